@@ -1,0 +1,231 @@
+/*
+ * mopac_b200.h -- C ABI of libmopac_b200.so, the B200 (sm_100a) build of
+ * MOPAC's semiempirical SCF hot path.
+ *
+ * Three layers, all plain C types (no torch, no C++):
+ *
+ *  (1) The reference GPU layer's bind(C) symbols with identical signatures
+ *      (src/gpu/cuda_wrappers.cu in the reference), so a Fortran build that
+ *      links the reference's wrappers links this library instead.  Host
+ *      pointers, synchronous, like the originals; the arithmetic runs in this
+ *      library's own kernels.
+ *  (2) Fortran-callable shims (by-reference arguments, gfortran mangling) for
+ *      the routines iter calls: fock2_, helect_, cnvg_, density_for_gpu_,
+ *      eigenvectors_lapack_, diag_for_gpu_.
+ *  (3) A device-resident native API (mb_*): an SCF context keeps H, W, F, P,
+ *      C and the eigenvalues in HBM across iterations and returns int status
+ *      codes.  Device-pointer kernel entry points (mb_*_dev) are exported for
+ *      callers that manage their own device memory.
+ *
+ * Packed matrices follow MOPAC: lower triangle by rows, element (i, j), i >= j
+ * (1-based) at i*(i-1)/2 + j, identical to the column-major upper triangle.
+ * Square matrices are column-major.  Orbital and atom indices passed as
+ * nfirst/nlast are 1-based like the reference; everything else is 0-based.
+ *
+ * Thread safety: one context must not be used from two threads at once
+ * (the reference is not thread-safe either, README.md:254-255); separate
+ * contexts are independent.
+ */
+#ifndef MOPAC_B200_H
+#define MOPAC_B200_H
+
+#include <stddef.h>
+#include <stdbool.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* CUDA stream handle without pulling in cuda_runtime.h */
+#ifndef __CUDA_RUNTIME_H__
+typedef struct CUstream_st* cudaStream_t;
+#endif
+
+/* ---------------------------------------------------------------- status */
+#define MB_OK 0
+#define MB_ERR_ARG 1          /* bad argument or size                         */
+#define MB_ERR_CUDA 2         /* CUDA runtime error (message in mb_last_error) */
+#define MB_ERR_NOCONV 3       /* SCF did not reach self-consistence in itrmax  */
+#define MB_ERR_TIMEOUT 4      /* a bounded device-side wait gave up            */
+#define MB_ERR_UNSUPPORTED 5  /* element or option outside this build          */
+#define MB_ERR_NUMERIC 6      /* NaN/Inf detected or eigensolver failure       */
+#define MB_ERR_NOMEM 7        /* device allocation failed                      */
+
+int mb_version(void);                 /* 10000*major + 100*minor + patch       */
+long long mb_launch_count(void);      /* kernels this library has launched     */
+const char* mb_last_error(void);      /* thread-local text of the last failure */
+
+/* ------------------------------------------------ (3) device-resident API */
+
+/* Device-side atom layout used by the dense kernels (see mb_atoms_create). */
+typedef struct MbAtomsDev {
+  int numat;
+  const int* first;      /* 0-based first orbital of each atom               */
+  const int* nor;        /* orbitals on the atom (1 or 4)                    */
+  const int* lim;        /* orbital pairs on the atom (1 or 10)              */
+  const long long* wrow; /* offset of the atom's first two-centre W block    */
+  const int* cum;        /* prefix sum of lim over lower-numbered atoms      */
+} MbAtomsDev;
+
+typedef struct mb_ctx mb_ctx; /* opaque SCF context */
+
+typedef struct mb_scf_opts {
+  int pseudo;        /* 1: pseudo-diagonalise once newdg is set (reference's
+                        commented-out path, SCF/iter.F90:847-861); 0: full
+                        diagonalisation every iteration like the fork     */
+  int itrmax;        /* iteration cap (ITRY), reference default 2000      */
+  double scfcrt;     /* SCF criterion, reference default 1e-4 kcal/mol    */
+  int precision;     /* 0: all FP64; 1: split-precision GEMMs until
+                        max|dP| < switch_pl, FP64 after                   */
+  double switch_pl;  /* precision switch threshold (default 1e-4)         */
+  int verbose;       /* print one line per iteration to stderr            */
+} mb_scf_opts;
+
+typedef struct mb_scf_result {
+  double escf;       /* heat of formation from iter, kcal/mol (no post-SCF
+                        geometry terms)                                  */
+  double ee;         /* electronic energy, eV                              */
+  int niter;
+  int converged;
+  int n_full_diag;   /* full eigensolves performed                         */
+  int n_pseudo_diag; /* pseudo-diagonalisations performed                  */
+  double pl;         /* last max|dP_ii|                                    */
+  double t_fock_ms, t_diag_ms, t_density_ms, t_other_ms; /* device-timed  */
+  double t_total_ms; /* CUDA events on the context stream around the SCF   */
+} mb_scf_result;
+
+void mb_scf_opts_default(mb_scf_opts* o);
+
+/* numat atoms with atomic numbers nat (H, C, O in this build); coordinates
+ * in Angstrom (numat x 3, host).  Computes nothing yet. */
+int mb_ctx_create(int numat, const int* nat, const double* coord, mb_ctx** out);
+int mb_ctx_destroy(mb_ctx* ctx);
+int mb_ctx_norbs(const mb_ctx* ctx);
+long long mb_ctx_n2elec(const mb_ctx* ctx);
+int mb_ctx_nclose(const mb_ctx* ctx);
+
+/* One-electron matrix H, two-electron integrals W and core-core energy from
+ * the coordinates, on the GPU (hcore, integrals/hcore.F90:150-297). */
+int mb_ctx_hcore(mb_ctx* ctx);
+/* Or supply them (host pointers): h[mpack], w[n2elec]. */
+int mb_ctx_set_hw(mb_ctx* ctx, const double* h, const double* w, double enuclr);
+/* Copy out H (mpack), W (n2elec), enuclr to host. */
+int mb_ctx_get_hw(mb_ctx* ctx, double* h, double* w, double* enuclr);
+
+/* Closed-shell RHF SCF (iter, SCF/iter.F90) from the standard diagonal guess
+ * (moldat.F90:731-760).  The whole loop runs on the device; only scalars
+ * cross to the host each iteration. */
+int mb_scf_run(mb_ctx* ctx, const mb_scf_opts* opts, mb_scf_result* res);
+
+/* Results to host: density P (mpack), eigenvectors C (norbs x norbs,
+ * column-major), eigenvalues (norbs), Fock matrix F (mpack). */
+int mb_ctx_get_density(mb_ctx* ctx, double* p);
+int mb_ctx_get_vectors(mb_ctx* ctx, double* c, double* eigs);
+int mb_ctx_get_fock(mb_ctx* ctx, double* f);
+/* Device pointers owned by the context (valid until destroy). */
+int mb_ctx_device_ptrs(mb_ctx* ctx, double** h, double** w, double** f, double** p,
+                       double** c, double** eigs);
+int mb_ctx_atoms_dev(mb_ctx* ctx, MbAtomsDev* out);
+
+/* --------------------------------------------- device-pointer kernels */
+/* Atom layout on the device from host nfirst/nlast (1-based). */
+int mb_atoms_create(int numat, const int* nfirst, const int* nlast, MbAtomsDev* out);
+int mb_atoms_destroy(MbAtomsDev* atoms);
+
+/* F = start + two-centre + one-centre terms (fock2 mode 2 with fock1).
+ * start = H (use_shift = 0) or H + shift*PA + 1e-16*i, F_ii -= shift.
+ * Bit-identical to the reference loop order.  All pointers device. */
+int mb_fock2_dev(const MbAtomsDev* atoms, double* f, const double* h, const double* ptot,
+                 const double* pa, const double* w, double shift, int use_shift,
+                 cudaStream_t stream);
+
+/* helect: sum_{i>j} P(H+F) + 0.5 sum_i P(H+F), written to *out (device). */
+int mb_helect_dev(int n, const double* p, const double* h, const double* f, double* out,
+                  cudaStream_t stream);
+
+/* cnvg (SCF/cnvg.F90) for RHF.  pnew is extrapolated in place, p and p1 are
+ * the history; *pl_out (device) receives max|dP_ii|.  Bit-identical. */
+int mb_cnvg_dev(int norbs, double* pnew, double* p, double* p1, int niter, double* pl_out,
+                cudaStream_t stream);
+
+/* P (packed) = occ * C[:, 0:nocc] C[:, 0:nocc]^T, FP64. */
+int mb_density_dev(int n, int nocc, double occ, const double* c, int ldc, double* p,
+                   cudaStream_t stream);
+
+/* Full eigensolve of a packed symmetric matrix after adding i*1e-10 to
+ * diagonal element i (eigenvectors_LAPACK.F90:53-55; the packed input is
+ * modified like the reference's xmat).  Ascending eigenvalues, vectors in
+ * columns.  Returns MB_ERR_NUMERIC if the solver fails. */
+int mb_eigh_packed_dev(int n, double* fpacked, double* c, double* eigs, cudaStream_t stream);
+
+/* Pseudo-diagonalisation (diag_for_GPU.F90): Fmo = C_v^T F C_o and the
+ * ordered 2x2 rotation sweep on C.  *nrot_out (host) gets the rotations
+ * applied.  Bit-identical rotation arithmetic. */
+int mb_pseudo_diag_dev(int n, int nocc, const double* fpacked, double* c, const double* eigs,
+                       long long* nrot_out, cudaStream_t stream);
+
+/* FP64 GEMM, column-major: C = alpha*op(A)*op(B) + beta*C. */
+int mb_dgemm_dev(char transa, char transb, int m, int n, int k, double alpha, const double* a,
+                 int lda, const double* b, int ldb, double beta, double* c, int ldc,
+                 cudaStream_t stream);
+
+/* ------------------------------------- (1) reference bind(C) symbols */
+/* src/gpu/cuda_wrappers.cu:192 (cublas_interfaces.F90:9-21) */
+void call_gemm_cublas(char tra, char trb, int m, int n, int k, double alpha, const double* A,
+                      int lda, const double* B, int ldb, double beta, double* C, int ldc);
+/* src/gpu/cuda_wrappers.cu:229 */
+void call_syrk_cublas(char uplo, char tra, int n, int k, double alpha, const double* A, int lda,
+                      double beta, double* C, int ldc);
+/* src/gpu/cuda_wrappers.cu:272, :372 -- one GPU here: same as the above */
+void call_gemm_cublas_2gpu(char tra, char trb, int m, int n, int k, double alpha, const double* A,
+                           int lda, const double* B, int ldb, double beta, double* C, int ldc);
+void call_syrk_cublas_2gpu(char uplo, char tra, int n, int k, double alpha, const double* A,
+                           int lda, double beta, double* C, int ldc);
+/* src/gpu/cuda_wrappers.cu:469 (eigenvectors_cuda.F90:9-20): full symmetric
+ * eigensolve, upper triangle of A (lda x n, column-major) on entry,
+ * eigenvectors on exit, eigenvalues in W, info = 0 on success. */
+void mopac_cuda_dsyevd(int n, double* A, int lda, double* W, int* info);
+/* src/gpu/cuda_wrappers.cu:547: rotation sweep of diag_for_GPU; lumo is
+ * 1-based; ci0/ca0 are unused (as in the reference). */
+void call_rot_cuda_gpu(const double* fmo, const double* eig, double* vector, const double* ci0,
+                       const double* ca0, int nocc, int lumo, int n, double bigeps, double tiny);
+void call_rot_cuda_2gpu_gpu(const double* fmo, const double* eig, double* vector,
+                            const double* ci0, const double* ca0, int nocc, int lumo, int n,
+                            double bigeps, double tiny);
+/* src/gpu/cuda_wrappers.cu:71, :115, :58, :158, :176, :830 */
+void getGPUInfo(bool* hasGpu, bool* hasDouble, int* nDevices, char (*name)[256], int* name_size,
+                size_t* totalMem, int* clockRate, int* major, int* minor);
+void setDevice(int idevice, bool* stat);
+void set_mozyme_gpu_pair(int dev0, int dev1);
+void create_handle(void);
+void destroy_handle(void);
+void mopac_cuda_destroy_resources(void);
+
+/* ------------------------------------------ (2) Fortran-level shims */
+/* fock2(f, ptot, p, w, wj, wk, numat, nfirst, nlast, mode), SCF/fock2.F90:16;
+ * host arrays, mode 2 only (fock1 included), numat > 0. */
+void fock2_(double* f, const double* ptot, const double* p, const double* w, const double* wj,
+            const double* wk, const int* numat, const int* nfirst, const int* nlast,
+            const int* mode);
+/* helect(n, p, h, f), integrals/helect.F90:16 */
+double helect_(const int* n, const double* p, const double* h, const double* f);
+/* cnvg(pnew, p, p1, niter, pl), SCF/cnvg.F90:16 (RHF).  norbs comes from
+ * molkst_C in the reference; a Fortran host sets it once with mb_set_norbs. */
+void cnvg_(double* pnew, double* p, double* p1, const int* niter, double* pl);
+void mb_set_norbs_(const int* norbs);
+/* density_for_GPU(c, fract, ndubl, nsingl, occ, mpack, norbs, mode, pp, iopc),
+ * matrix/density_for_GPU.F90:16; closed shell (fract = 0) */
+void density_for_gpu_(const double* c, const double* fract, const int* ndubl, const int* nsingl,
+                      const double* occ, const int* mpack, const int* norbs, const int* mode,
+                      double* pp, const int* iopc);
+/* eigenvectors_LAPACK(eigenvecs, xmat, eigvals, ndim),
+ * matrix/eigenvectors_LAPACK.F90:16; modifies xmat like the reference */
+void eigenvectors_lapack_(double* eigenvecs, double* xmat, double* eigvals, const int* ndim);
+/* diag_for_GPU(fao, vector, nocc, eig, norbs, mpack), matrix/diag_for_GPU.F90:16 */
+void diag_for_gpu_(const double* fao, double* vector, const int* nocc, const double* eig,
+                   const int* norbs, const int* mpack);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MOPAC_B200_H */

@@ -1,0 +1,120 @@
+"""ctypes binding of libmopac_b200.so.
+
+The library is built in-tree (``python -m mopac_gpu_b200.build``).  Loading
+fails loudly when it is missing: there is no CPU fallback for any entry point.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libmopac_b200.so")
+
+MB_OK = 0
+ERRORS = {1: "MB_ERR_ARG", 2: "MB_ERR_CUDA", 3: "MB_ERR_NOCONV", 4: "MB_ERR_TIMEOUT",
+          5: "MB_ERR_UNSUPPORTED", 6: "MB_ERR_NUMERIC", 7: "MB_ERR_NOMEM"}
+
+
+class LibraryError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class MbAtomsDev(ctypes.Structure):
+    _fields_ = [("numat", ctypes.c_int), ("first", ctypes.c_void_p), ("nor", ctypes.c_void_p),
+                ("lim", ctypes.c_void_p), ("wrow", ctypes.c_void_p), ("cum", ctypes.c_void_p)]
+
+
+class ScfOpts(ctypes.Structure):
+    _fields_ = [("pseudo", ctypes.c_int), ("itrmax", ctypes.c_int), ("scfcrt", ctypes.c_double),
+                ("precision", ctypes.c_int), ("switch_pl", ctypes.c_double), ("verbose", ctypes.c_int)]
+
+
+class ScfRes(ctypes.Structure):
+    _fields_ = [("escf", ctypes.c_double), ("ee", ctypes.c_double), ("niter", ctypes.c_int),
+                ("converged", ctypes.c_int), ("n_full_diag", ctypes.c_int), ("n_pseudo_diag", ctypes.c_int),
+                ("pl", ctypes.c_double), ("t_fock_ms", ctypes.c_double), ("t_diag_ms", ctypes.c_double),
+                ("t_density_ms", ctypes.c_double), ("t_other_ms", ctypes.c_double), ("t_total_ms", ctypes.c_double)]
+
+
+_lib = None
+
+_P = ctypes.c_void_p
+_I = ctypes.c_int
+_D = ctypes.c_double
+_LL = ctypes.c_longlong
+_C = ctypes.c_char
+
+SIGNATURES = {
+    "mb_version": ([], _I),
+    "mb_launch_count": ([], _LL),
+    "mb_last_error": ([], ctypes.c_char_p),
+    "mb_scf_opts_default": ([ctypes.POINTER(ScfOpts)], None),
+    "mb_ctx_create": ([_I, _P, _P, ctypes.POINTER(_P)], _I),
+    "mb_ctx_destroy": ([_P], _I),
+    "mb_ctx_norbs": ([_P], _I),
+    "mb_ctx_n2elec": ([_P], _LL),
+    "mb_ctx_nclose": ([_P], _I),
+    "mb_ctx_hcore": ([_P], _I),
+    "mb_ctx_set_hw": ([_P, _P, _P, _D], _I),
+    "mb_ctx_get_hw": ([_P, _P, _P, ctypes.POINTER(_D)], _I),
+    "mb_scf_run": ([_P, ctypes.POINTER(ScfOpts), ctypes.POINTER(ScfRes)], _I),
+    "mb_ctx_get_density": ([_P, _P], _I),
+    "mb_ctx_get_vectors": ([_P, _P, _P], _I),
+    "mb_ctx_get_fock": ([_P, _P], _I),
+    "mb_ctx_device_ptrs": ([_P] + [ctypes.POINTER(_P)] * 6, _I),
+    "mb_ctx_atoms_dev": ([_P, ctypes.POINTER(MbAtomsDev)], _I),
+    "mb_atoms_create": ([_I, _P, _P, ctypes.POINTER(MbAtomsDev)], _I),
+    "mb_atoms_destroy": ([ctypes.POINTER(MbAtomsDev)], _I),
+    "mb_fock2_dev": ([ctypes.POINTER(MbAtomsDev), _P, _P, _P, _P, _P, _D, _I, _P], _I),
+    "mb_helect_dev": ([_I, _P, _P, _P, _P, _P], _I),
+    "mb_cnvg_dev": ([_I, _P, _P, _P, _I, _P, _P], _I),
+    "mb_density_dev": ([_I, _I, _D, _P, _I, _P, _P], _I),
+    "mb_eigh_packed_dev": ([_I, _P, _P, _P, _P], _I),
+    "mb_pseudo_diag_dev": ([_I, _I, _P, _P, _P, ctypes.POINTER(_LL), _P], _I),
+    "mb_dgemm_dev": ([_C, _C, _I, _I, _I, _D, _P, _I, _P, _I, _D, _P, _I, _P], _I),
+    "call_gemm_cublas": ([_C, _C, _I, _I, _I, _D, _P, _I, _P, _I, _D, _P, _I], None),
+    "call_syrk_cublas": ([_C, _C, _I, _I, _D, _P, _I, _D, _P, _I], None),
+    "call_gemm_cublas_2gpu": ([_C, _C, _I, _I, _I, _D, _P, _I, _P, _I, _D, _P, _I], None),
+    "call_syrk_cublas_2gpu": ([_C, _C, _I, _I, _D, _P, _I, _D, _P, _I], None),
+    "mopac_cuda_dsyevd": ([_I, _P, _I, _P, _P], None),
+    "call_rot_cuda_gpu": ([_P, _P, _P, _P, _P, _I, _I, _I, _D, _D], None),
+    "call_rot_cuda_2gpu_gpu": ([_P, _P, _P, _P, _P, _I, _I, _I, _D, _D], None),
+    "getGPUInfo": ([_P] * 9, None),
+    "setDevice": ([_I, _P], None),
+    "set_mozyme_gpu_pair": ([_I, _I], None),
+    "create_handle": ([], None),
+    "destroy_handle": ([], None),
+    "mopac_cuda_destroy_resources": ([], None),
+    "fock2_": ([_P] * 10, None),
+    "helect_": ([_P] * 4, _D),
+    "cnvg_": ([_P] * 5, None),
+    "mb_set_norbs_": ([_P], None),
+    "density_for_gpu_": ([_P] * 10, None),
+    "eigenvectors_lapack_": ([_P] * 4, None),
+    "diag_for_gpu_": ([_P] * 6, None),
+}
+
+
+def lib():
+    """Load libmopac_b200.so (built in-tree); raise if it is absent."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise FileNotFoundError(
+                f"{LIB_PATH} is missing: build it with `python -m mopac_gpu_b200.build` "
+                "(there is no CPU fallback)")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (args, res) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = res
+        _lib = L
+    return _lib
+
+
+def check(rc: int) -> None:
+    if rc != MB_OK:
+        raise LibraryError(rc, lib().mb_last_error().decode(errors="replace"))

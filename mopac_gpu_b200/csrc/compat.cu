@@ -1,0 +1,416 @@
+// Reference-facing entry points.
+//
+// (1) The bind(C) symbols of the reference's src/gpu/cuda_wrappers.cu with
+//     identical signatures (host pointers, synchronous, void return), so a
+//     Fortran build that links the reference's wrappers links this library
+//     instead.  Device buffers are cached grow-only, like the reference's
+//     DevBuf (cuda_wrappers.cu:11-28); errors, which the reference ignores,
+//     are reported through mb_last_error() and, for the eigensolver, info.
+// (2) Fortran-callable shims (gfortran mangling, by-reference arguments) for
+//     the routines iter calls, so a gfortran-built iter can link them.
+#include <string.h>
+
+#include <mutex>
+#include <vector>
+
+#include "mb_common.cuh"
+
+extern "C" int mb_eigh_ws(int n, double* fpacked, int perturb, double* c, double* eigs, void* ws, int* status_dev,
+                          cudaStream_t stream);
+extern "C" size_t mb_eigh_ws_bytes(int n);
+extern "C" size_t mb_pseudo_ws_bytes(int n, int nocc);
+extern "C" int mb_pseudo_diag_ws(int n, int nocc, const double* fpacked, double* c, const double* eigs,
+                                 unsigned long long* nrot_dev, void* ws, cudaStream_t stream);
+extern "C" int mb_rot_sweep_ws(int n, int nocc, const double* fmo, const double* eigs, double* c, double bigeps,
+                               double tiny, unsigned long long* nrot_dev, void* ws, cudaStream_t stream);
+extern "C" int mb_cnvg_ws(int norbs, double* pnew, double* p, double* p1, int niter, double* pl_out, double* ws,
+                          cudaStream_t stream);
+extern "C" int mb_helect_ws(int n, const double* p, const double* h, const double* f, double* out, double* ws,
+                            cudaStream_t stream);
+
+namespace {
+
+// Grow-only device buffer cache (one set per process, serialised by a mutex;
+// the reference layer is not thread-safe at all).
+struct Buf {
+  void* p = nullptr;
+  size_t cap = 0;
+  int get(size_t bytes) {
+    if (bytes <= cap) return MB_OK;
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    MB_CUDA(cudaMalloc(&p, bytes));
+    cap = bytes;
+    return MB_OK;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+  }
+};
+
+std::mutex g_mu;
+Buf g_a, g_b, g_c, g_d, g_ws;
+cudaStream_t g_stream = nullptr;
+int g_norbs_fortran = 0;
+
+int ensure_stream() {
+  if (!g_stream) MB_CUDA(cudaStreamCreateWithFlags(&g_stream, cudaStreamNonBlocking));
+  return MB_OK;
+}
+
+// copy a (rows x cols, leading dim ld) host matrix to a dense device one (ld = rows)
+int h2d_mat(double* dst, const double* src, int rows, int cols, int ld) {
+  if (rows <= 0 || cols <= 0) return MB_OK;
+  MB_CUDA(cudaMemcpy2DAsync(dst, sizeof(double) * rows, src, sizeof(double) * ld, sizeof(double) * rows, cols,
+                            cudaMemcpyHostToDevice, g_stream));
+  return MB_OK;
+}
+int d2h_mat(double* dst, const double* src, int rows, int cols, int ld) {
+  if (rows <= 0 || cols <= 0) return MB_OK;
+  MB_CUDA(cudaMemcpy2DAsync(dst, sizeof(double) * ld, src, sizeof(double) * rows, sizeof(double) * rows, cols,
+                            cudaMemcpyDeviceToHost, g_stream));
+  return MB_OK;
+}
+
+bool is_t(char c) { return c == 'T' || c == 't' || c == 'C' || c == 'c'; }
+
+int gemm_host(char tra, char trb, int m, int n, int k, double alpha, const double* A, int lda, const double* B,
+              int ldb, double beta, double* C, int ldc) {
+  if (m <= 0 || n <= 0) return MB_OK;
+  MB_TRY(ensure_stream());
+  const int ar = is_t(tra) ? k : m, ac = is_t(tra) ? m : k;
+  const int br = is_t(trb) ? n : k, bc = is_t(trb) ? k : n;
+  MB_TRY(g_a.get(sizeof(double) * (size_t)ar * ac + 8));
+  MB_TRY(g_b.get(sizeof(double) * (size_t)br * bc + 8));
+  MB_TRY(g_c.get(sizeof(double) * (size_t)m * n));
+  MB_TRY(h2d_mat((double*)g_a.p, A, ar, ac, lda));
+  MB_TRY(h2d_mat((double*)g_b.p, B, br, bc, ldb));
+  if (beta != 0.0) MB_TRY(h2d_mat((double*)g_c.p, C, m, n, ldc));
+  MB_TRY(mb_dgemm_dev(tra, trb, m, n, k, alpha, (const double*)g_a.p, ar > 0 ? ar : 1, (const double*)g_b.p,
+                      br > 0 ? br : 1, beta, (double*)g_c.p, m, g_stream));
+  MB_TRY(d2h_mat(C, (const double*)g_c.p, m, n, ldc));
+  MB_CUDA(cudaStreamSynchronize(g_stream));
+  return MB_OK;
+}
+
+__global__ void keep_triangle(int n, const double* __restrict__ full, double* __restrict__ c, int upper) {
+  const int col = blockIdx.y;
+  for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < n; row += gridDim.x * blockDim.x)
+    if (upper ? row <= col : row >= col) c[(long long)col * n + row] = full[(long long)col * n + row];
+}
+
+int syrk_host(char uplo, char tra, int n, int k, double alpha, const double* A, int lda, double beta, double* C,
+              int ldc) {
+  if (n <= 0) return MB_OK;
+  MB_TRY(ensure_stream());
+  const bool t = is_t(tra);
+  const int ar = t ? k : n, ac = t ? n : k;
+  MB_TRY(g_a.get(sizeof(double) * (size_t)ar * ac + 8));
+  MB_TRY(g_c.get(sizeof(double) * (size_t)n * n));
+  MB_TRY(g_d.get(sizeof(double) * (size_t)n * n));
+  MB_TRY(h2d_mat((double*)g_a.p, A, ar, ac, lda));
+  MB_TRY(h2d_mat((double*)g_c.p, C, n, n, ldc));
+  MB_CUDA(cudaMemcpyAsync(g_d.p, g_c.p, sizeof(double) * (size_t)n * n, cudaMemcpyDeviceToDevice, g_stream));
+  // full product into d (both triangles), then keep only the requested one
+  MB_TRY(mb_dgemm_dev(t ? 'T' : 'N', t ? 'N' : 'T', n, n, k, alpha, (const double*)g_a.p, ar > 0 ? ar : 1,
+                      (const double*)g_a.p, ar > 0 ? ar : 1, beta, (double*)g_d.p, n, g_stream));
+  dim3 grid((n + 255) / 256, n);
+  keep_triangle<<<grid, 256, 0, g_stream>>>(n, (const double*)g_d.p, (double*)g_c.p,
+                                            (uplo == 'U' || uplo == 'u') ? 1 : 0);
+  MB_LAUNCH_CHECK();
+  MB_TRY(d2h_mat(C, (const double*)g_c.p, n, n, ldc));
+  MB_CUDA(cudaStreamSynchronize(g_stream));
+  return MB_OK;
+}
+
+__global__ void pack_upper(int n, const double* __restrict__ a, int lda, double* __restrict__ pk) {
+  const int col = blockIdx.y;
+  for (int row = blockIdx.x * blockDim.x + threadIdx.x; row <= col; row += gridDim.x * blockDim.x)
+    pk[mb_tri(col, row)] = a[(long long)col * lda + row];
+}
+
+int eigh_host(int n, const double* A_upper, int lda, double* vecs, int ldv, double* w, double* fpacked_host,
+              int perturb) {
+  MB_TRY(ensure_stream());
+  const size_t mp = (size_t)n * (n + 1) / 2, nn = (size_t)n * n;
+  MB_TRY(g_a.get(sizeof(double) * (nn > mp ? nn : mp)));
+  MB_TRY(g_b.get(sizeof(double) * mp));
+  MB_TRY(g_c.get(sizeof(double) * (nn + n)));
+  MB_TRY(g_ws.get(mb_eigh_ws_bytes(n) + 64));
+  double* pk = (double*)g_b.p;
+  if (fpacked_host) {
+    MB_CUDA(cudaMemcpyAsync(pk, fpacked_host, sizeof(double) * mp, cudaMemcpyHostToDevice, g_stream));
+  } else {
+    MB_TRY(h2d_mat((double*)g_a.p, A_upper, n, n, lda));
+    dim3 grid((n + 255) / 256, n);
+    pack_upper<<<grid, 256, 0, g_stream>>>(n, (const double*)g_a.p, n, pk);
+    MB_LAUNCH_CHECK();
+  }
+  double* cv = (double*)g_c.p;
+  double* ev = cv + nn;
+  int* st = (int*)((char*)g_ws.p + mb_eigh_ws_bytes(n));
+  MB_TRY(mb_eigh_ws(n, pk, perturb, cv, ev, g_ws.p, st, g_stream));
+  int hst = 0;
+  MB_CUDA(cudaMemcpyAsync(&hst, st, sizeof(int), cudaMemcpyDeviceToHost, g_stream));
+  MB_TRY(d2h_mat(vecs, cv, n, n, ldv));
+  MB_CUDA(cudaMemcpyAsync(w, ev, sizeof(double) * n, cudaMemcpyDeviceToHost, g_stream));
+  if (fpacked_host && perturb)
+    MB_CUDA(cudaMemcpyAsync(fpacked_host, pk, sizeof(double) * mp, cudaMemcpyDeviceToHost, g_stream));
+  MB_CUDA(cudaStreamSynchronize(g_stream));
+  if (hst != 0) return mb_set_error(MB_ERR_NUMERIC, "eigensolver: inverse iteration failed");
+  return MB_OK;
+}
+
+void report(int rc, const char* where) {
+  if (rc != MB_OK) fprintf(stderr, "mopac_b200 %s: %s\n", where, mb_last_error());
+}
+
+}  // namespace
+
+// ============================================================ (1) bind(C)
+extern "C" void call_gemm_cublas(char tra, char trb, int m, int n, int k, double alpha, const double* A, int lda,
+                                 const double* B, int ldb, double beta, double* C, int ldc) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  report(gemm_host(tra, trb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc), "call_gemm_cublas");
+}
+
+extern "C" void call_syrk_cublas(char uplo, char tra, int n, int k, double alpha, const double* A, int lda,
+                                 double beta, double* C, int ldc) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  report(syrk_host(uplo, tra, n, k, alpha, A, lda, beta, C, ldc), "call_syrk_cublas");
+}
+
+extern "C" void call_gemm_cublas_2gpu(char tra, char trb, int m, int n, int k, double alpha, const double* A,
+                                      int lda, const double* B, int ldb, double beta, double* C, int ldc) {
+  call_gemm_cublas(tra, trb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+}
+
+extern "C" void call_syrk_cublas_2gpu(char uplo, char tra, int n, int k, double alpha, const double* A, int lda,
+                                      double beta, double* C, int ldc) {
+  call_syrk_cublas(uplo, tra, n, k, alpha, A, lda, beta, C, ldc);
+}
+
+extern "C" void mopac_cuda_dsyevd(int n, double* A, int lda, double* W, int* info) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  int rc = (n <= 0 || lda < n) ? mb_set_error(MB_ERR_ARG, "mopac_cuda_dsyevd: bad size")
+                               : eigh_host(n, A, lda, A, lda, W, nullptr, 0);
+  report(rc, "mopac_cuda_dsyevd");
+  if (info) *info = rc == MB_OK ? 0 : -rc;
+}
+
+extern "C" void call_rot_cuda_gpu(const double* fmo, const double* eig, double* vector, const double* ci0,
+                                  const double* ca0, int nocc, int lumo, int n, double bigeps, double tiny) {
+  (void)ci0; (void)ca0;
+  std::lock_guard<std::mutex> lk(g_mu);
+  int rc = MB_OK;
+  const int nv = n - (lumo - 1);
+  if (nocc <= 0 || nv <= 0 || lumo - 1 != nocc) {
+    rc = (nocc <= 0 || nv <= 0) ? MB_OK : mb_set_error(MB_ERR_ARG, "call_rot_cuda_gpu: lumo must be nocc + 1");
+  } else {
+    rc = ensure_stream();
+    if (rc == MB_OK) rc = g_a.get(sizeof(double) * (size_t)nocc * nv);
+    if (rc == MB_OK) rc = g_b.get(sizeof(double) * (size_t)n + 64);
+    if (rc == MB_OK) rc = g_c.get(sizeof(double) * (size_t)n * n);
+    if (rc == MB_OK) rc = g_ws.get(mb_pseudo_ws_bytes(n, nocc) + 64);
+    unsigned long long* nr = (unsigned long long*)((char*)g_b.p + sizeof(double) * (size_t)n);
+    if (rc == MB_OK && cudaMemcpyAsync(g_a.p, fmo, sizeof(double) * (size_t)nocc * nv, cudaMemcpyHostToDevice, g_stream) != cudaSuccess) rc = MB_ERR_CUDA;
+    if (rc == MB_OK && cudaMemcpyAsync(g_b.p, eig, sizeof(double) * (size_t)n, cudaMemcpyHostToDevice, g_stream) != cudaSuccess) rc = MB_ERR_CUDA;
+    if (rc == MB_OK && cudaMemcpyAsync(g_c.p, vector, sizeof(double) * (size_t)n * n, cudaMemcpyHostToDevice, g_stream) != cudaSuccess) rc = MB_ERR_CUDA;
+    if (rc == MB_OK)
+      rc = mb_rot_sweep_ws(n, nocc, (const double*)g_a.p, (const double*)g_b.p, (double*)g_c.p, bigeps, tiny, nr,
+                           g_ws.p, g_stream);
+    if (rc == MB_OK && cudaMemcpyAsync(vector, g_c.p, sizeof(double) * (size_t)n * n, cudaMemcpyDeviceToHost, g_stream) != cudaSuccess) rc = MB_ERR_CUDA;
+    if (rc == MB_OK && cudaStreamSynchronize(g_stream) != cudaSuccess) rc = MB_ERR_CUDA;
+  }
+  report(rc, "call_rot_cuda_gpu");
+}
+
+extern "C" void call_rot_cuda_2gpu_gpu(const double* fmo, const double* eig, double* vector, const double* ci0,
+                                       const double* ca0, int nocc, int lumo, int n, double bigeps, double tiny) {
+  call_rot_cuda_gpu(fmo, eig, vector, ci0, ca0, nocc, lumo, n, bigeps, tiny);
+}
+
+extern "C" void getGPUInfo(bool* hasGpu, bool* hasDouble, int* nDevices, char (*name)[256], int* name_size,
+                           size_t* totalMem, int* clockRate, int* major, int* minor) {
+  int nd = 0;
+  if (cudaGetDeviceCount(&nd) != cudaSuccess) nd = 0;
+  if (hasGpu) *hasGpu = nd > 0;
+  if (nDevices) *nDevices = nd;
+  for (int i = 0; i < nd && i < 6; ++i) {
+    cudaDeviceProp pr;
+    if (cudaGetDeviceProperties(&pr, i) != cudaSuccess) continue;
+    if (hasDouble) hasDouble[i] = pr.major >= 2;
+    if (name) {
+      strncpy(name[i], pr.name, 255);
+      name[i][255] = 0;
+    }
+    if (name_size) name_size[i] = (int)strlen(pr.name);
+    if (totalMem) totalMem[i] = pr.totalGlobalMem;
+    int clk = 0;
+    cudaDeviceGetAttribute(&clk, cudaDevAttrClockRate, i);
+    if (clockRate) clockRate[i] = clk;
+    if (major) major[i] = pr.major;
+    if (minor) minor[i] = pr.minor;
+  }
+}
+
+extern "C" void setDevice(int idevice, bool* stat) {
+  cudaError_t e = cudaSetDevice(idevice);
+  if (stat) *stat = e == cudaSuccess;
+}
+
+extern "C" void set_mozyme_gpu_pair(int dev0, int dev1) { (void)dev0; (void)dev1; }
+extern "C" void create_handle(void) {}
+extern "C" void destroy_handle(void) {}
+
+extern "C" void mopac_cuda_destroy_resources(void) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  g_a.release(); g_b.release(); g_c.release(); g_d.release(); g_ws.release();
+  if (g_stream) { cudaStreamDestroy(g_stream); g_stream = nullptr; }
+}
+
+// ====================================================== (2) Fortran shims
+// molkst_C's norbs for cnvg_, which takes it from the module, not an argument.
+extern "C" void mb_set_norbs_(const int* norbs) { g_norbs_fortran = norbs ? *norbs : 0; }
+
+extern "C" void fock2_(double* f, const double* ptot, const double* p, const double* w, const double* wj,
+                       const double* wk, const int* numat, const int* nfirst, const int* nlast, const int* mode) {
+  (void)wj; (void)wk;
+  std::lock_guard<std::mutex> lk(g_mu);
+  int rc = MB_OK;
+  const int na = numat ? *numat : 0;
+  if (na <= 0 || !mode || *mode != 2) {
+    report(mb_set_error(MB_ERR_UNSUPPORTED, "fock2_: numat > 0 and mode 2 only"), "fock2_");
+    return;
+  }
+  MbAtomsDev at{};
+  rc = mb_atoms_create(na, nfirst, nlast, &at);
+  const int norbs = nlast[na - 1];
+  const size_t mp = (size_t)norbs * (norbs + 1) / 2;
+  long long n2 = 0;
+  for (int a = 0; a < na; ++a) {
+    long long li = (long long)(nlast[a] - nfirst[a] + 1) * (nlast[a] - nfirst[a] + 2) / 2, s = 0;
+    for (int b = 0; b < a; ++b) s += (long long)(nlast[b] - nfirst[b] + 1) * (nlast[b] - nfirst[b] + 2) / 2;
+    n2 += li * s + li * li;
+  }
+  if (rc == MB_OK) rc = ensure_stream();
+  if (rc == MB_OK) rc = g_a.get(sizeof(double) * mp * 3);
+  if (rc == MB_OK) rc = g_b.get(sizeof(double) * (size_t)n2);
+  double *df = (double*)g_a.p, *dpt = df + mp, *dpa = dpt + mp;
+  if (rc == MB_OK && (cudaMemcpyAsync(df, f, sizeof(double) * mp, cudaMemcpyHostToDevice, g_stream) != cudaSuccess ||
+                      cudaMemcpyAsync(dpt, ptot, sizeof(double) * mp, cudaMemcpyHostToDevice, g_stream) != cudaSuccess ||
+                      cudaMemcpyAsync(dpa, p, sizeof(double) * mp, cudaMemcpyHostToDevice, g_stream) != cudaSuccess ||
+                      cudaMemcpyAsync(g_b.p, w, sizeof(double) * (size_t)n2, cudaMemcpyHostToDevice, g_stream) != cudaSuccess))
+    rc = MB_ERR_CUDA;
+  // F arrives holding the start value; use_shift = 0 with h = f reproduces "f += ..."
+  if (rc == MB_OK) rc = mb_fock2_dev(&at, df, df, dpt, dpa, (const double*)g_b.p, 0.0, 0, g_stream);
+  if (rc == MB_OK && cudaMemcpyAsync(f, df, sizeof(double) * mp, cudaMemcpyDeviceToHost, g_stream) != cudaSuccess)
+    rc = MB_ERR_CUDA;
+  if (rc == MB_OK && cudaStreamSynchronize(g_stream) != cudaSuccess) rc = MB_ERR_CUDA;
+  mb_atoms_destroy(&at);
+  report(rc, "fock2_");
+}
+
+extern "C" double helect_(const int* n, const double* p, const double* h, const double* f) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  const int nn = *n;
+  const size_t mp = (size_t)nn * (nn + 1) / 2;
+  double out = 0.0;
+  int rc = ensure_stream();
+  if (rc == MB_OK) rc = g_a.get(sizeof(double) * (mp * 3 + 2 * (size_t)nn + 2));
+  double* d = (double*)g_a.p;
+  if (rc == MB_OK && (cudaMemcpyAsync(d, p, sizeof(double) * mp, cudaMemcpyHostToDevice, g_stream) != cudaSuccess ||
+                      cudaMemcpyAsync(d + mp, h, sizeof(double) * mp, cudaMemcpyHostToDevice, g_stream) != cudaSuccess ||
+                      cudaMemcpyAsync(d + 2 * mp, f, sizeof(double) * mp, cudaMemcpyHostToDevice, g_stream) != cudaSuccess))
+    rc = MB_ERR_CUDA;
+  if (rc == MB_OK) rc = mb_helect_ws(nn, d, d + mp, d + 2 * mp, d + 3 * mp + 2 * nn, d + 3 * mp, g_stream);
+  if (rc == MB_OK && cudaMemcpyAsync(&out, d + 3 * mp + 2 * nn, sizeof(double), cudaMemcpyDeviceToHost, g_stream) != cudaSuccess)
+    rc = MB_ERR_CUDA;
+  if (rc == MB_OK && cudaStreamSynchronize(g_stream) != cudaSuccess) rc = MB_ERR_CUDA;
+  report(rc, "helect_");
+  return out;
+}
+
+extern "C" void cnvg_(double* pnew, double* p, double* p1, const int* niter, double* pl) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  const int n = g_norbs_fortran;
+  if (n <= 0) {
+    report(mb_set_error(MB_ERR_ARG, "cnvg_: call mb_set_norbs_ first"), "cnvg_");
+    return;
+  }
+  const size_t mp = (size_t)n * (n + 1) / 2;
+  int rc = ensure_stream();
+  if (rc == MB_OK) rc = g_a.get(sizeof(double) * (2 * mp + (size_t)n + 8));
+  double* d = (double*)g_a.p;
+  double *dpn = d, *dp = d + mp, *dp1 = d + 2 * mp, *ws = dp1 + n;
+  if (rc == MB_OK && (cudaMemcpyAsync(dpn, pnew, sizeof(double) * mp, cudaMemcpyHostToDevice, g_stream) != cudaSuccess ||
+                      cudaMemcpyAsync(dp, p, sizeof(double) * mp, cudaMemcpyHostToDevice, g_stream) != cudaSuccess ||
+                      cudaMemcpyAsync(dp1, p1, sizeof(double) * n, cudaMemcpyHostToDevice, g_stream) != cudaSuccess))
+    rc = MB_ERR_CUDA;
+  if (rc == MB_OK) rc = mb_cnvg_ws(n, dpn, dp, dp1, *niter, ws + 4, ws, g_stream);
+  if (rc == MB_OK && (cudaMemcpyAsync(pnew, dpn, sizeof(double) * mp, cudaMemcpyDeviceToHost, g_stream) != cudaSuccess ||
+                      cudaMemcpyAsync(p, dp, sizeof(double) * mp, cudaMemcpyDeviceToHost, g_stream) != cudaSuccess ||
+                      cudaMemcpyAsync(p1, dp1, sizeof(double) * n, cudaMemcpyDeviceToHost, g_stream) != cudaSuccess ||
+                      cudaMemcpyAsync(pl, ws + 4, sizeof(double), cudaMemcpyDeviceToHost, g_stream) != cudaSuccess))
+    rc = MB_ERR_CUDA;
+  if (rc == MB_OK && cudaStreamSynchronize(g_stream) != cudaSuccess) rc = MB_ERR_CUDA;
+  report(rc, "cnvg_");
+}
+
+extern "C" void density_for_gpu_(const double* c, const double* fract, const int* ndubl, const int* nsingl,
+                                 const double* occ, const int* mpack, const int* norbs, const int* mode, double* pp,
+                                 const int* iopc) {
+  (void)nsingl; (void)mode; (void)iopc; (void)mpack;
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (fract && *fract >= 1.0e-2) {
+    report(mb_set_error(MB_ERR_UNSUPPORTED, "density_for_gpu_: fractional occupancy not in this build"),
+           "density_for_gpu_");
+    return;
+  }
+  const int n = *norbs, k = *ndubl;
+  const size_t mp = (size_t)n * (n + 1) / 2;
+  int rc = ensure_stream();
+  if (rc == MB_OK) rc = g_a.get(sizeof(double) * ((size_t)n * (k > 0 ? k : 1)));
+  if (rc == MB_OK) rc = g_b.get(sizeof(double) * mp);
+  if (rc == MB_OK && k > 0 && cudaMemcpyAsync(g_a.p, c, sizeof(double) * (size_t)n * k, cudaMemcpyHostToDevice, g_stream) != cudaSuccess)
+    rc = MB_ERR_CUDA;
+  if (rc == MB_OK) rc = mb_density_dev(n, k, *occ, (const double*)g_a.p, n, (double*)g_b.p, g_stream);
+  if (rc == MB_OK && cudaMemcpyAsync(pp, g_b.p, sizeof(double) * mp, cudaMemcpyDeviceToHost, g_stream) != cudaSuccess)
+    rc = MB_ERR_CUDA;
+  if (rc == MB_OK && cudaStreamSynchronize(g_stream) != cudaSuccess) rc = MB_ERR_CUDA;
+  report(rc, "density_for_gpu_");
+}
+
+extern "C" void eigenvectors_lapack_(double* eigenvecs, double* xmat, double* eigvals, const int* ndim) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  const int n = *ndim;
+  report(eigh_host(n, nullptr, n, eigenvecs, n, eigvals, xmat, 1), "eigenvectors_lapack_");
+}
+
+extern "C" void diag_for_gpu_(const double* fao, double* vector, const int* nocc, const double* eig, const int* norbs,
+                              const int* mpack) {
+  (void)mpack;
+  std::lock_guard<std::mutex> lk(g_mu);
+  const int n = *norbs, k = *nocc;
+  if (k == n || k == 0) return;
+  const size_t mp = (size_t)n * (n + 1) / 2;
+  int rc = ensure_stream();
+  if (rc == MB_OK) rc = g_a.get(sizeof(double) * mp);
+  if (rc == MB_OK) rc = g_b.get(sizeof(double) * (size_t)n + 64);
+  if (rc == MB_OK) rc = g_c.get(sizeof(double) * (size_t)n * n);
+  if (rc == MB_OK) rc = g_ws.get(mb_pseudo_ws_bytes(n, k) + 64);
+  unsigned long long* nr = (unsigned long long*)((char*)g_b.p + sizeof(double) * (size_t)n);
+  if (rc == MB_OK && (cudaMemcpyAsync(g_a.p, fao, sizeof(double) * mp, cudaMemcpyHostToDevice, g_stream) != cudaSuccess ||
+                      cudaMemcpyAsync(g_b.p, eig, sizeof(double) * n, cudaMemcpyHostToDevice, g_stream) != cudaSuccess ||
+                      cudaMemcpyAsync(g_c.p, vector, sizeof(double) * (size_t)n * n, cudaMemcpyHostToDevice, g_stream) != cudaSuccess))
+    rc = MB_ERR_CUDA;
+  if (rc == MB_OK)
+    rc = mb_pseudo_diag_ws(n, k, (const double*)g_a.p, (double*)g_c.p, (const double*)g_b.p, nr, g_ws.p, g_stream);
+  if (rc == MB_OK && cudaMemcpyAsync(vector, g_c.p, sizeof(double) * (size_t)n * n, cudaMemcpyDeviceToHost, g_stream) != cudaSuccess)
+    rc = MB_ERR_CUDA;
+  if (rc == MB_OK && cudaStreamSynchronize(g_stream) != cudaSuccess) rc = MB_ERR_CUDA;
+  report(rc, "diag_for_gpu_");
+}

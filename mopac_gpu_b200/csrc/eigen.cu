@@ -1,0 +1,568 @@
+// Full symmetric eigensolver in FP64 on the device, replacing the LAPACK /
+// cuSOLVER dsyevd call of eigenvectors_LAPACK (matrix/eigenvectors_LAPACK.F90
+// :53-121, cuda_wrappers.cu:469-505).
+//
+//   1. i*1e-10 added to diagonal element i of the packed input (the
+//      reference's parity-critical perturbation, eigenvectors_LAPACK.F90:53-55),
+//      then unpacked to a full column-major matrix.
+//   2. Householder tridiagonalisation, blocked: a cooperative kernel forms each
+//      panel of NB reflectors (three grid barriers per column: column update,
+//      reflector + symmetric matrix-vector product, correction), and the
+//      trailing matrix gets the rank-2*NB update A -= V W^T + W V^T as FP64 GEMM.
+//   3. Eigenvalues of the tridiagonal matrix by bisection on Sturm counts, one
+//      thread per eigenvalue.
+//   4. Eigenvectors of the tridiagonal matrix by inverse iteration with partial
+//      pivoting; eigenvalues closer than 1e-8 * ||T|| form clusters whose
+//      vectors are re-orthogonalised inside the iteration (one thread per
+//      cluster, members in order).
+//   5. Back-transformation C = Q Z with the compact WY form of each panel,
+//      Z -= V (T (V^T Z)), as FP64 GEMMs.
+// Eigenvalues ascend; eigenvectors are the columns of C.
+#include <cooperative_groups.h>
+
+#include "mb_common.cuh"
+
+namespace cg = cooperative_groups;
+
+namespace {
+
+constexpr int NB = 32;         // panel width
+constexpr int TPB = 256;       // threads per CTA in the panel kernel
+
+struct PanelArgs {
+  int n, k, ib, lda;
+  double* a;
+  double* vp;      // n x NB, panel reflectors (v_j[j+1] = 1, zero above)
+  double* wp;      // n x NB
+  double* vall;    // n x n, all reflectors (column j holds v_j)
+  double* d;
+  double* e;
+  double* tau;
+  double* part;    // gridDim partial norms (column j)
+  double* partd;   // gridDim partial dots (w.v)
+  double* tvec;    // 2*NB: t1 = W^T v, t2 = V^T v
+  double* wvec;    // n
+};
+
+__device__ double block_sum(double v, double* sh) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  if (lane == 0) sh[wid] = v;
+  __syncthreads();
+  double r = 0.0;
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) r += sh[i];
+  }
+  __syncthreads();
+  return r;  // valid in thread 0
+}
+
+__global__ void __launch_bounds__(TPB) tridiag_panel(PanelArgs p) {
+  cg::grid_group grid = cg::this_grid();
+  __shared__ double sh[32];
+  __shared__ double s_scal[4];
+  const int n = p.n, lda = p.lda;
+  const long long gtid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long gstride = (long long)gridDim.x * blockDim.x;
+  const int gwarp = (int)(gtid >> 5), nwarps = (int)(gstride >> 5), lane = threadIdx.x & 31;
+  double* A = p.a;
+#define AE(r, c) A[(long long)(c) * lda + (r)]
+#define VP(r, c) p.vp[(long long)(c) * n + (r)]
+#define WP(r, c) p.wp[(long long)(c) * n + (r)]
+  double prev_tau = 0.0;
+  for (int i = 0; i < p.ib; ++i) {
+    const int j = p.k + i;
+    // ---- phase A: finish W(:, i-1), update column j, partial norm
+    double alpha_prev = 0.0;
+    if (i > 0) {
+      double s = 0.0;
+      for (int b = 0; b < (int)gridDim.x; ++b) s += p.partd[b];
+      alpha_prev = -0.5 * prev_tau * s;
+    }
+    double wj[NB], vj[NB];
+    for (int l = 0; l < i; ++l) {
+      vj[l] = VP(j, l);
+      wj[l] = (l == i - 1) ? p.wvec[j] + alpha_prev * VP(j, l) : WP(j, l);
+    }
+    double sig = 0.0;
+    for (long long r = gtid; r < n; r += gstride) {
+      if (i > 0) {
+        double wr_last = (r >= j) ? p.wvec[r] + alpha_prev * VP(r, i - 1) : 0.0;
+        if (r >= j) WP(r, i - 1) = wr_last;
+        if (r >= j) {
+          double acc = AE(r, j);
+          for (int l = 0; l < i; ++l) {
+            double wrl = (l == i - 1) ? wr_last : WP(r, l);
+            acc -= VP(r, l) * wj[l] + wrl * vj[l];
+          }
+          AE(r, j) = acc;
+        }
+      }
+      if (r == j) p.d[j] = AE(j, j);
+      if (r >= j + 2) {
+        double x = AE(r, j);
+        sig += x * x;
+      }
+    }
+    double bs = block_sum(sig, sh);
+    if (threadIdx.x == 0) p.part[blockIdx.x] = bs;
+    grid.sync();
+    // ---- phase D: reflector, v, symmetric product p = A22 v, t1/t2
+    if (threadIdx.x == 0) {
+      double s = 0.0;
+      for (int b = 0; b < (int)gridDim.x; ++b) s += p.part[b];
+      double alpha = AE(j + 1, j);
+      double beta, tau, scal;
+      if (s == 0.0) {
+        beta = alpha; tau = 0.0; scal = 0.0;
+      } else {
+        beta = -copysign(sqrt(alpha * alpha + s), alpha);
+        tau = (beta - alpha) / beta;
+        scal = 1.0 / (alpha - beta);
+      }
+      s_scal[0] = tau;
+      s_scal[1] = scal;
+      s_scal[2] = beta;
+    }
+    __syncthreads();
+    const double tau = s_scal[0], scal = s_scal[1];
+    if (gtid == 0) {
+      p.e[j] = s_scal[2];
+      p.tau[j] = tau;
+    }
+    for (long long r = gtid; r < n; r += gstride) {
+      double v = (r == j + 1) ? 1.0 : (r > j + 1 ? AE(r, j) * scal : 0.0);
+      VP(r, i) = v;
+      p.vall[(long long)j * n + r] = v;
+    }
+    // p(r) = sum_{c > j} A(c, r) v(c), one warp per row r > j
+    for (int r = j + 1 + gwarp; r < n; r += nwarps) {
+      double acc = 0.0;
+      for (int c = j + 1 + lane; c < n; c += 32) {
+        double v = (c == j + 1) ? 1.0 : AE(c, j) * scal;
+        acc += AE(c, r) * v;
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+      if (lane == 0) p.wvec[r] = acc;
+    }
+    // t1[l] = sum_r W(r,l) v(r), t2[l] = sum_r V(r,l) v(r) over r > j; warp 0..2i-1
+    for (int q = gwarp; q < 2 * i; q += nwarps) {
+      const int l = q >> 1;
+      const bool isw = (q & 1) == 0;
+      double acc = 0.0;
+      for (int r = j + 1 + lane; r < n; r += 32) {
+        double v = (r == j + 1) ? 1.0 : AE(r, j) * scal;
+        acc += (isw ? WP(r, l) : VP(r, l)) * v;
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+      if (lane == 0) p.tvec[(isw ? 0 : NB) + l] = acc;
+    }
+    grid.sync();
+    // ---- phase E: corrections, w = tau (p - corr), partial w.v
+    double dot = 0.0;
+    for (long long r = gtid; r < n; r += gstride) {
+      if (r <= j) {
+        p.wvec[r] = 0.0;
+        continue;
+      }
+      double corr = 0.0;
+      for (int l = 0; l < i; ++l) corr += VP(r, l) * p.tvec[l] + WP(r, l) * p.tvec[NB + l];
+      double w = tau * (p.wvec[r] - corr);
+      p.wvec[r] = w;
+      dot += w * VP(r, i);
+    }
+    bs = block_sum(dot, sh);
+    if (threadIdx.x == 0) p.partd[blockIdx.x] = bs;
+    prev_tau = tau;
+    grid.sync();
+  }
+  // finish W(:, ib-1)
+  {
+    double s = 0.0;
+    for (int b = 0; b < (int)gridDim.x; ++b) s += p.partd[b];
+    const double alpha_prev = -0.5 * prev_tau * s;
+    const int last = p.ib - 1;
+    for (long long r = gtid; r < n; r += gstride)
+      WP(r, last) = p.wvec[r] + alpha_prev * VP(r, last);
+  }
+#undef AE
+#undef VP
+#undef WP
+}
+
+__global__ void copy_last_diag(int n, const double* a, int lda, double* d) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) d[n - 1] = a[(long long)(n - 1) * lda + (n - 1)];
+}
+
+// ---------------------------------------------------------------- bisection
+__device__ __forceinline__ int sturm_count(int n, const double* __restrict__ d, const double* __restrict__ e2,
+                                           double x, double pivmin) {
+  int cnt = 0;
+  double q = d[0] - x;
+  if (fabs(q) < pivmin) q = -pivmin;
+  cnt += q < 0.0;
+  for (int i = 1; i < n; ++i) {
+    q = d[i] - x - e2[i - 1] / q;
+    if (fabs(q) < pivmin) q = -pivmin;
+    cnt += q < 0.0;
+  }
+  return cnt;
+}
+
+__global__ void tri_bounds(int n, const double* d, const double* e, double* e2, double* bnd) {
+  __shared__ double slo[1024], shi[1024], se[1024];
+  double lo = 1e300, hi = -1e300, em = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    double r = (i > 0 ? fabs(e[i - 1]) : 0.0) + (i < n - 1 ? fabs(e[i]) : 0.0);
+    lo = fmin(lo, d[i] - r);
+    hi = fmax(hi, d[i] + r);
+    if (i < n - 1) {
+      e2[i] = e[i] * e[i];
+      em = fmax(em, e2[i]);
+    }
+  }
+  slo[threadIdx.x] = lo; shi[threadIdx.x] = hi; se[threadIdx.x] = em;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) {
+      slo[threadIdx.x] = fmin(slo[threadIdx.x], slo[threadIdx.x + s]);
+      shi[threadIdx.x] = fmax(shi[threadIdx.x], shi[threadIdx.x + s]);
+      se[threadIdx.x] = fmax(se[threadIdx.x], se[threadIdx.x + s]);
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    double tnorm = fmax(fabs(slo[0]), fabs(shi[0]));
+    double pad = 2.0 * 2.220446049250313e-16 * tnorm * n + 1e-300;
+    bnd[0] = slo[0] - pad;
+    bnd[1] = shi[0] + pad;
+    bnd[2] = fmax(1e-290, 2.2250738585072014e-308 * fmax(1.0, se[0]));  // pivmin
+    bnd[3] = tnorm;
+  }
+}
+
+__global__ void bisect_kernel(int n, const double* __restrict__ d, const double* __restrict__ e2,
+                              const double* __restrict__ bnd, double* __restrict__ w) {
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= n) return;
+  double lo = bnd[0], hi = bnd[1];
+  const double pivmin = bnd[2];
+  const double eps = 2.220446049250313e-16;
+  for (int it = 0; it < 200; ++it) {
+    double mid = 0.5 * (lo + hi);
+    if (hi - lo <= 2.0 * eps * fmax(fabs(lo), fabs(hi)) + pivmin || mid <= lo || mid >= hi) break;
+    int c = sturm_count(n, d, e2, mid, pivmin);
+    if (c > m) hi = mid; else lo = mid;
+  }
+  w[m] = 0.5 * (lo + hi);
+}
+
+// --------------------------------------------------------- inverse iteration
+// LU with partial pivoting of T - lam I and solve, in place on x (stride ld).
+// u0/u1/u2 (stride ld) receive the U factor; pivots are re-derived per solve.
+__device__ void tri_solve(int n, const double* __restrict__ d, const double* __restrict__ e, double lam,
+                          double tiny, double* u0, double* u1, double* u2, double* x, long long ld) {
+  // factorisation and forward substitution in one pass
+  double dd = d[0] - lam;      // current pivot row diagonal
+  double du = n > 1 ? e[0] : 0.0;  // current pivot row super-diagonal
+  double du2 = 0.0;
+  double xr = x[0];
+  for (int i = 0; i < n - 1; ++i) {
+    const double sub = e[i];           // T(i+1, i)
+    const double dn = d[i + 1] - lam;  // T(i+1, i+1)
+    const double en = (i + 1 < n - 1) ? e[i + 1] : 0.0;
+    const double xn = x[(long long)(i + 1) * ld];
+    if (fabs(dd) >= fabs(sub)) {
+      // no interchange
+      double piv_ = dd;
+      if (fabs(piv_) < tiny) piv_ = copysign(tiny, piv_ == 0.0 ? 1.0 : piv_);
+      const double l = sub / piv_;
+      u0[(long long)i * ld] = piv_;
+      u1[(long long)i * ld] = du;
+      u2[(long long)i * ld] = du2;
+      x[(long long)i * ld] = xr;
+      dd = dn - l * du;
+      du = en;
+      du2 = 0.0;
+      xr = xn - l * xr;
+    } else {
+      // interchange rows i and i+1
+      const double l = dd / sub;
+      u0[(long long)i * ld] = sub;
+      u1[(long long)i * ld] = dn;
+      u2[(long long)i * ld] = en;
+      x[(long long)i * ld] = xn;
+      const double ndd = du - l * dn;
+      const double ndu = -l * en;
+      dd = ndd;
+      du = ndu;
+      du2 = 0.0;
+      xr = xr - l * xn;
+    }
+  }
+  double last = dd;
+  if (fabs(last) < tiny) last = copysign(tiny, last == 0.0 ? 1.0 : last);
+  u0[(long long)(n - 1) * ld] = last;
+  // back substitution
+  double x1 = xr / last;  // x[n-1]
+  x[(long long)(n - 1) * ld] = x1;
+  double x2 = 0.0;        // x[i+2]
+  for (int i = n - 2; i >= 0; --i) {
+    const double v = (x[(long long)i * ld] - u1[(long long)i * ld] * x1 - u2[(long long)i * ld] * x2) /
+                     u0[(long long)i * ld];
+    x[(long long)i * ld] = v;
+    x2 = x1;
+    x1 = v;
+  }
+}
+
+// x (stride ld) normalised to unit 2-norm; returns the norm before scaling.
+__device__ double normalise(int n, double* x, long long ld) {
+  double s = 0.0, mx = 0.0;
+  for (int i = 0; i < n; ++i) mx = fmax(mx, fabs(x[(long long)i * ld]));
+  if (mx == 0.0) return 0.0;
+  const double inv = 1.0 / mx;
+  for (int i = 0; i < n; ++i) {
+    double v = x[(long long)i * ld] * inv;
+    s += v * v;
+  }
+  const double sc = inv / sqrt(s);
+  for (int i = 0; i < n; ++i) x[(long long)i * ld] *= sc;
+  return mx * sqrt(s);
+}
+
+// One thread per cluster start; X is n x n with X[i*n + m] = component i of
+// vector m (so consecutive threads touch consecutive addresses).
+__global__ void inverse_iteration(int n, const double* __restrict__ d, const double* __restrict__ e,
+                                  const double* __restrict__ w, const double* __restrict__ bnd,
+                                  double* __restrict__ X, double* __restrict__ U0, double* __restrict__ U1,
+                                  double* __restrict__ U2, int* status) {
+  const int m0 = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m0 >= n) return;
+  const double tnorm = bnd[3];
+  const double ortol = 1.0e-8 * tnorm;
+  if (m0 > 0 && !(w[m0] - w[m0 - 1] > ortol)) return;  // not a cluster start
+  int m1 = m0 + 1;
+  while (m1 < n && !(w[m1] - w[m1 - 1] > ortol)) ++m1;
+  const double eps = 2.220446049250313e-16;
+  const double tiny = eps * fmax(tnorm, 1e-300);
+  const long long ld = n;
+  double* u0 = U0 + m0;
+  double* u1 = U1 + m0;
+  double* u2 = U2 + m0;
+  double lam_prev = 0.0;
+  for (int m = m0; m < m1; ++m) {
+    double lam = w[m];
+    if (m > m0) {  // separate exactly coincident shifts (dstein's perturbation)
+      const double pertol = 10.0 * fabs(eps * lam) + tiny;
+      if (lam - lam_prev < pertol) lam = lam_prev + pertol;
+    }
+    lam_prev = lam;
+    double* x = X + m;
+    // deterministic start vector
+    unsigned long long s = 0x9E3779B97F4A7C15ull ^ (unsigned long long)(m + 1) * 0xBF58476D1CE4E5B9ull;
+    for (int i = 0; i < n; ++i) {
+      s ^= s >> 31; s *= 0x94D049BB133111EBull; s ^= s >> 29;
+      x[(long long)i * ld] = ((double)(s >> 11) * (1.0 / 9007199254740992.0)) - 0.5;
+    }
+    normalise(n, x, ld);
+    for (int it = 0; it < 4; ++it) {
+      tri_solve(n, d, e, lam, tiny, u0, u1, u2, x, ld);
+      // re-orthogonalise against earlier members of the cluster (MGS)
+      for (int q = m0; q < m; ++q) {
+        const double* y = X + q;
+        double dt = 0.0;
+        for (int i = 0; i < n; ++i) dt += y[(long long)i * ld] * x[(long long)i * ld];
+        for (int i = 0; i < n; ++i) x[(long long)i * ld] -= dt * y[(long long)i * ld];
+      }
+      double nr = normalise(n, x, ld);
+      if (!(nr > 0.0) || !isfinite(nr)) { atomicExch(status, MB_ERR_NUMERIC); return; }
+    }
+  }
+}
+
+// Z (column-major n x n) = X^T in the X[i*n + m] layout, i.e. plain copy with
+// swapped meaning: Z(i, m) = X[i*n + m].
+__global__ void transpose_kernel(int n, const double* __restrict__ X, double* __restrict__ Z) {
+  __shared__ double t[32][33];
+  const int bx = blockIdx.x * 32, by = blockIdx.y * 32;
+  // X viewed as row-major [i][m]: tile rows i = by.., cols m = bx..
+  for (int yy = threadIdx.y; yy < 32; yy += blockDim.y) {
+    int i = by + yy, m = bx + threadIdx.x;
+    if (i < n && m < n) t[yy][threadIdx.x] = X[(long long)i * n + m];
+  }
+  __syncthreads();
+  // Z column-major: Z(i, m) at m*n + i; write with i fastest
+  for (int yy = threadIdx.y; yy < 32; yy += blockDim.y) {
+    int m = bx + yy, i = by + threadIdx.x;
+    if (i < n && m < n) Z[(long long)m * n + i] = t[threadIdx.x][yy];
+  }
+}
+
+// T factor of a panel (dlarft, forward columnwise): T(i,i) = tau_i,
+// T(0:i, i) = -tau_i T(0:i, 0:i) S(0:i, i) with S = V^T V.
+__global__ void larft_kernel(int ib, const double* __restrict__ S, const double* __restrict__ tau,
+                             double* __restrict__ T) {
+  __shared__ double st[NB][NB + 1];
+  __shared__ double sv[NB][NB + 1];
+  for (int q = threadIdx.x; q < ib * ib; q += blockDim.x) {
+    int r = q % ib, c = q / ib;
+    sv[r][c] = S[c * ib + r];
+    st[r][c] = 0.0;
+  }
+  __syncthreads();
+  for (int i = 0; i < ib; ++i) {
+    const double ti = tau[i];
+    if (threadIdx.x < (unsigned)i) {
+      const int r = threadIdx.x;
+      double acc = 0.0;
+      for (int c = r; c < i; ++c) acc += st[r][c] * sv[c][i];
+      st[r][i] = -ti * acc;
+    }
+    if (threadIdx.x == 0) st[i][i] = ti;
+    __syncthreads();
+  }
+  for (int q = threadIdx.x; q < ib * ib; q += blockDim.x) {
+    int r = q % ib, c = q / ib;
+    T[c * ib + r] = st[r][c];
+  }
+}
+
+}  // namespace
+
+extern "C" int mb_unpack_dev(int n, const double* pk, double* a, int lda, int perturb, double* pk_mut,
+                             cudaStream_t stream);
+
+// Workspace: A n*n | V n*n | Z n*n | X n*n | U0,U1,U2 3*n*n | vp,wp 2*n*NB |
+// d,e,e2,tau,wvec 5n | small scratch
+extern "C" size_t mb_eigh_ws_bytes(int n) {
+  size_t nn = (size_t)n * n;
+  return sizeof(double) * (7 * nn + 2 * (size_t)n * NB + 5 * (size_t)n + 2 * NB + 4096 + NB * NB * 2 +
+                           (size_t)NB * n) + 256;
+}
+
+extern "C" int mb_eigh_ws(int n, double* fpacked, int perturb, double* c, double* eigs, void* ws, int* status_dev,
+                          cudaStream_t stream) {
+  const size_t nn = (size_t)n * n;
+  double* b = (double*)ws;
+  double* A = b; b += nn;
+  double* V = b; b += nn;
+  double* Z = b; b += nn;
+  double* X = b; b += nn;
+  double* U0 = b; b += nn;
+  double* U1 = b; b += nn;
+  double* U2 = b; b += nn;
+  double* vp = b; b += (size_t)n * NB;
+  double* wp = b; b += (size_t)n * NB;
+  double* d = b; b += n;
+  double* e = b; b += n;
+  double* e2 = b; b += n;
+  double* tau = b; b += n;
+  double* wvec = b; b += n;
+  double* tvec = b; b += 2 * NB;
+  double* part = b; b += 4096;
+  double* S = b; b += NB * NB;
+  double* Tm = b; b += NB * NB;
+  double* Y = b; b += (size_t)NB * n;
+  double* bnd = part + 2048;
+
+  if (n == 1) {
+    MB_TRY(mb_unpack_dev(1, fpacked, A, 1, perturb, fpacked, stream));
+    MB_CUDA(cudaMemcpyAsync(eigs, A, sizeof(double), cudaMemcpyDeviceToDevice, stream));
+    const double one = 1.0;
+    MB_CUDA(cudaMemcpyAsync(c, &one, sizeof(double), cudaMemcpyHostToDevice, stream));
+    return MB_OK;
+  }
+  MB_TRY(mb_unpack_dev(n, fpacked, A, n, perturb, fpacked, stream));
+  MB_CUDA(cudaMemsetAsync(V, 0, sizeof(double) * nn, stream));
+  MB_CUDA(cudaMemsetAsync(e, 0, sizeof(double) * n, stream));
+
+  // cooperative grid size: co-resident CTAs
+  static int grid_cached = 0;
+  if (grid_cached == 0) {
+    int dev = 0, sms = 0, per = 0;
+    MB_CUDA(cudaGetDevice(&dev));
+    MB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    MB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, tridiag_panel, TPB, 0));
+    if (per > 2) per = 2;
+    if (per < 1) return mb_set_error(MB_ERR_CUDA, "tridiag_panel: cannot be co-resident");
+    grid_cached = sms * per;
+    if (grid_cached > 1024) grid_cached = 1024;
+  }
+  const int grid = grid_cached;
+  for (int k = 0; k < n - 1; k += NB) {
+    const int ib = (NB < n - 1 - k) ? NB : n - 1 - k;
+    MB_CUDA(cudaMemsetAsync(vp, 0, sizeof(double) * (size_t)n * NB, stream));
+    MB_CUDA(cudaMemsetAsync(wp, 0, sizeof(double) * (size_t)n * NB, stream));
+    PanelArgs pa;
+    pa.n = n; pa.k = k; pa.ib = ib; pa.lda = n;
+    pa.a = A; pa.vp = vp; pa.wp = wp; pa.vall = V; pa.d = d; pa.e = e; pa.tau = tau;
+    pa.part = part; pa.partd = part + 1024; pa.tvec = tvec; pa.wvec = wvec;
+    void* args[] = {&pa};
+    MB_CUDA(cudaLaunchCooperativeKernel((void*)tridiag_panel, grid, TPB, args, 0, stream));
+    mb_count_launch();
+    const int t = k + ib;
+    if (t < n) {
+      const int m = n - t;
+      double* At = A + (size_t)t * n + t;
+      MB_TRY(mb_dgemm_dev('N', 'T', m, m, ib, -1.0, vp + t, n, wp + t, n, 1.0, At, n, stream));
+      MB_TRY(mb_dgemm_dev('N', 'T', m, m, ib, -1.0, wp + t, n, vp + t, n, 1.0, At, n, stream));
+    }
+  }
+  copy_last_diag<<<1, 32, 0, stream>>>(n, A, n, d);
+  MB_LAUNCH_CHECK();
+  // eigenvalues
+  tri_bounds<<<1, 1024, 0, stream>>>(n, d, e, e2, bnd);
+  MB_LAUNCH_CHECK();
+  bisect_kernel<<<(n + 127) / 128, 128, 0, stream>>>(n, d, e2, bnd, eigs);
+  MB_LAUNCH_CHECK();
+  // eigenvectors of T
+  MB_CUDA(cudaMemsetAsync(status_dev, 0, sizeof(int), stream));
+  inverse_iteration<<<(n + 127) / 128, 128, 0, stream>>>(n, d, e, eigs, bnd, X, U0, U1, U2, status_dev);
+  MB_LAUNCH_CHECK();
+  {
+    dim3 g((n + 31) / 32, (n + 31) / 32), blk(32, 8);
+    transpose_kernel<<<g, blk, 0, stream>>>(n, X, Z);
+    MB_LAUNCH_CHECK();
+  }
+  // back-transformation, panels in reverse order: Z <- (I - V T V^T) Z
+  int last_k = ((n - 2) / NB) * NB;
+  for (int k = last_k; k >= 0; k -= NB) {
+    const int ib = (NB < n - 1 - k) ? NB : n - 1 - k;
+    if (ib <= 0) continue;
+    const int r0 = k + 1;           // first nonzero row of the panel's reflectors
+    const int m = n - r0;
+    const double* Vk = V + (size_t)k * n + r0;
+    MB_TRY(mb_dgemm_dev('T', 'N', ib, ib, m, 1.0, Vk, n, Vk, n, 0.0, S, ib, stream));
+    larft_kernel<<<1, 64, 0, stream>>>(ib, S, tau + k, Tm);
+    MB_LAUNCH_CHECK();
+    MB_TRY(mb_dgemm_dev('T', 'N', ib, n, m, 1.0, Vk, n, Z + r0, n, 0.0, Y, ib, stream));
+    MB_TRY(mb_dgemm_dev('N', 'N', ib, n, ib, 1.0, Tm, ib, Y, ib, 0.0, X, ib, stream));
+    MB_TRY(mb_dgemm_dev('N', 'N', m, n, ib, -1.0, Vk, n, X, ib, 1.0, Z + r0, n, stream));
+  }
+  MB_CUDA(cudaMemcpyAsync(c, Z, sizeof(double) * nn, cudaMemcpyDeviceToDevice, stream));
+  return MB_OK;
+}
+
+extern "C" int mb_eigh_packed_dev(int n, double* fpacked, double* c, double* eigs, cudaStream_t stream) {
+  if (n <= 0) return mb_set_error(MB_ERR_ARG, "mb_eigh_packed_dev: n <= 0");
+  void* ws = nullptr;
+  int* st = nullptr;
+  MB_CUDA(cudaMalloc(&ws, mb_eigh_ws_bytes(n)));
+  cudaError_t ce = cudaMalloc((void**)&st, sizeof(int));
+  if (ce != cudaSuccess) { cudaFree(ws); return mb_set_cuda_error(ce, "cudaMalloc", __FILE__, __LINE__); }
+  int rc = mb_eigh_ws(n, fpacked, 1, c, eigs, ws, st, stream);
+  int hst = 0;
+  if (rc == MB_OK) {
+    ce = cudaMemcpyAsync(&hst, st, sizeof(int), cudaMemcpyDeviceToHost, stream);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(stream);
+    if (ce != cudaSuccess) rc = mb_set_cuda_error(ce, "eigh status", __FILE__, __LINE__);
+    else if (hst != 0) rc = mb_set_error(MB_ERR_NUMERIC, "eigensolver: inverse iteration failed");
+  }
+  cudaFree(ws);
+  cudaFree(st);
+  return rc;
+}

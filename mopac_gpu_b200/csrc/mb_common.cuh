@@ -1,0 +1,59 @@
+// Shared helpers for the mopac_gpu_b200 CUDA sources (sm_100a only).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+
+#include "mopac_b200.h"
+
+// Record a CUDA failure in the library's last-error slot and return MB_ERR_CUDA.
+int mb_set_cuda_error(cudaError_t e, const char* what, const char* file, int line);
+int mb_set_error(int code, const char* msg);
+
+#define MB_CUDA(call)                                                        \
+  do {                                                                       \
+    cudaError_t _e = (call);                                                 \
+    if (_e != cudaSuccess) return mb_set_cuda_error(_e, #call, __FILE__, __LINE__); \
+  } while (0)
+
+// Every kernel launch of the library is followed by MB_LAUNCH_CHECK, which
+// also counts it (mb_launch_count()).
+void mb_count_launch();
+#define MB_LAUNCH_CHECK()                                                    \
+  do {                                                                       \
+    mb_count_launch();                                                       \
+    cudaError_t _e = cudaGetLastError();                                     \
+    if (_e != cudaSuccess) return mb_set_cuda_error(_e, "kernel launch", __FILE__, __LINE__); \
+  } while (0)
+
+#define MB_TRY(expr)            \
+  do {                          \
+    int _rc = (expr);           \
+    if (_rc != MB_OK) return _rc; \
+  } while (0)
+
+// Packed lower triangle, row-major: element (r, c) with r >= c, 0-based.
+__host__ __device__ __forceinline__ long long mb_tri(long long r, long long c) {
+  return r * (r + 1) / 2 + c;
+}
+
+// Unrounded-product-free arithmetic: these keep the operation order of the
+// reference's Fortran loops with one rounding per operation (no FMA).
+#define DMUL(a, b) __dmul_rn((a), (b))
+#define DADD(a, b) __dadd_rn((a), (b))
+#define DSUB(a, b) __dsub_rn((a), (b))
+
+// Per-atom layout shared by the dense kernels.  Atoms are 0-based; `first`
+// is the 0-based first orbital, `nor` the orbital count (1 or 4), `lim` the
+// pair count (1 or 10), `wrow` the offset of the atom's first two-centre W
+// block and `cum` the prefix sum of `lim` over lower-numbered atoms, so the W
+// block of pair (a, b), b < a, starts at wrow[a] + lim[a] * cum[b] and the
+// one-centre block at wrow[a] + lim[a] * cum[a].
+struct MbAtoms {
+  int numat;
+  const int* first;
+  const int* nor;
+  const int* lim;
+  const long long* wrow;
+  const int* cum;
+};

@@ -1,0 +1,552 @@
+// Device-resident SCF context and driver.
+//
+// mb_scf_run restates the control flow of iter (SCF/iter.F90:16-1107) for
+// closed-shell RHF with default keywords and 1SCF settings: the level-shift
+// logic (:273-325), Fock build (:553), energy and heat (:641-659), the
+// convergence test (:675-690), the newdg/oknewd switches (:1022-1041), full
+// diagonalisation (:849) or -- with opts.pseudo -- the pseudo-diagonalisation
+// the reference comments out (:847-861), the density (:897), cnvg (:899-901)
+// and the exit diagonalisation (:1052-1106).  All matrices stay in HBM; the
+// host only sees the scalars the control flow branches on (energy, max|dP|,
+// HOMO/LUMO eigenvalues), a handful of bytes per iteration.
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <string>
+#include <vector>
+
+#include "mb_common.cuh"
+#include "pm7_params.h"
+
+// kernels defined in other translation units
+extern "C" int mb_helect_ws(int n, const double* p, const double* h, const double* f, double* out, double* ws,
+                            cudaStream_t stream);
+extern "C" int mb_cnvg_ws(int norbs, double* pnew, double* p, double* p1, int niter, double* pl_out, double* ws,
+                          cudaStream_t stream);
+extern "C" size_t mb_eigh_ws_bytes(int n);
+extern "C" int mb_eigh_ws(int n, double* fpacked, int perturb, double* c, double* eigs, void* ws, int* status_dev,
+                          cudaStream_t stream);
+extern "C" size_t mb_pseudo_ws_bytes(int n, int nocc);
+extern "C" int mb_pseudo_diag_ws(int n, int nocc, const double* fpacked, double* c, const double* eigs,
+                                 unsigned long long* nrot_dev, void* ws, cudaStream_t stream);
+extern "C" int mb_hcore_dev(const int* nat_d, const double* coord_d, const MbAtomsDev* at, int numat, double* h,
+                            double* w, double* enuc_pairs, cudaStream_t stream);
+extern "C" int mb_hcore_finish(int numat, const MbAtomsDev* at, const int* nat_d, double* h, const double* e1b,
+                               double* enuclr_dev, const double* enuc_pairs, cudaStream_t stream);
+
+// ------------------------------------------------------------------ errors
+static thread_local std::string g_last_error;
+
+int mb_set_error(int code, const char* msg) {
+  g_last_error = msg ? msg : "";
+  return code;
+}
+
+int mb_set_cuda_error(cudaError_t e, const char* what, const char* file, int line) {
+  char buf[512];
+  snprintf(buf, sizeof(buf), "%s failed: %s (%s:%d)", what, cudaGetErrorString(e), file, line);
+  g_last_error = buf;
+  if (e == cudaErrorMemoryAllocation) return MB_ERR_NOMEM;
+  return MB_ERR_CUDA;
+}
+
+extern "C" const char* mb_last_error(void) { return g_last_error.c_str(); }
+
+static unsigned long long g_launches = 0;
+void mb_count_launch() { __atomic_add_fetch(&g_launches, 1ull, __ATOMIC_RELAXED); }
+extern "C" long long mb_launch_count(void) { return (long long)__atomic_load_n(&g_launches, __ATOMIC_RELAXED); }
+extern "C" int mb_version(void) { return 100; }
+
+// ------------------------------------------------------------ atom layout
+static int build_layout(int numat, const int* nfirst, const int* nlast, std::vector<int>& first,
+                        std::vector<int>& nor, std::vector<int>& lim, std::vector<long long>& wrow,
+                        std::vector<int>& cum, long long* n2elec) {
+  first.resize(numat); nor.resize(numat); lim.resize(numat); wrow.resize(numat); cum.resize(numat);
+  long long off = 0;
+  int c = 0;
+  for (int a = 0; a < numat; ++a) {
+    first[a] = nfirst[a] - 1;
+    nor[a] = nlast[a] - nfirst[a] + 1;
+    if (nor[a] != 1 && nor[a] != 4) return mb_set_error(MB_ERR_UNSUPPORTED, "only s and sp atoms are supported");
+    lim[a] = nor[a] * (nor[a] + 1) / 2;
+    cum[a] = c;
+    wrow[a] = off;
+    off += (long long)lim[a] * c + (long long)lim[a] * lim[a];
+    c += lim[a];
+  }
+  *n2elec = off;
+  return MB_OK;
+}
+
+extern "C" int mb_atoms_create(int numat, const int* nfirst, const int* nlast, MbAtomsDev* out) {
+  if (numat <= 0 || !nfirst || !nlast || !out) return mb_set_error(MB_ERR_ARG, "mb_atoms_create: bad args");
+  std::vector<int> first, nor, lim, cum;
+  std::vector<long long> wrow;
+  long long n2 = 0;
+  MB_TRY(build_layout(numat, nfirst, nlast, first, nor, lim, wrow, cum, &n2));
+  int *d_first, *d_nor, *d_lim, *d_cum;
+  long long* d_wrow;
+  MB_CUDA(cudaMalloc(&d_first, sizeof(int) * numat));
+  MB_CUDA(cudaMalloc(&d_nor, sizeof(int) * numat));
+  MB_CUDA(cudaMalloc(&d_lim, sizeof(int) * numat));
+  MB_CUDA(cudaMalloc(&d_cum, sizeof(int) * numat));
+  MB_CUDA(cudaMalloc(&d_wrow, sizeof(long long) * numat));
+  MB_CUDA(cudaMemcpy(d_first, first.data(), sizeof(int) * numat, cudaMemcpyHostToDevice));
+  MB_CUDA(cudaMemcpy(d_nor, nor.data(), sizeof(int) * numat, cudaMemcpyHostToDevice));
+  MB_CUDA(cudaMemcpy(d_lim, lim.data(), sizeof(int) * numat, cudaMemcpyHostToDevice));
+  MB_CUDA(cudaMemcpy(d_cum, cum.data(), sizeof(int) * numat, cudaMemcpyHostToDevice));
+  MB_CUDA(cudaMemcpy(d_wrow, wrow.data(), sizeof(long long) * numat, cudaMemcpyHostToDevice));
+  out->numat = numat;
+  out->first = d_first;
+  out->nor = d_nor;
+  out->lim = d_lim;
+  out->cum = d_cum;
+  out->wrow = d_wrow;
+  return MB_OK;
+}
+
+extern "C" int mb_atoms_destroy(MbAtomsDev* a) {
+  if (!a) return MB_OK;
+  cudaFree((void*)a->first);
+  cudaFree((void*)a->nor);
+  cudaFree((void*)a->lim);
+  cudaFree((void*)a->cum);
+  cudaFree((void*)a->wrow);
+  memset(a, 0, sizeof(*a));
+  return MB_OK;
+}
+
+// ------------------------------------------------------------------ context
+struct mb_ctx {
+  int numat = 0, norbs = 0, nclose = 0;
+  long long mpack = 0, n2elec = 0;
+  std::vector<int> nat, nfirst, nlast;
+  std::vector<double> coord, pdiag;
+  double atheat = 0.0, enuclr = 0.0;
+  bool have_hw = false;
+  MbAtomsDev atoms{};
+  int* d_nat = nullptr;
+  double* d_coord = nullptr;
+  double *h = nullptr, *w = nullptr, *f = nullptr, *p = nullptr, *pa = nullptr, *pold = nullptr, *pold2 = nullptr,
+         *c = nullptr, *eigs = nullptr, *fdiag = nullptr;
+  double* scal = nullptr;   // device scalars: [0] ee, [1] pl, [8..] scratch
+  double* hws = nullptr;    // helect workspace (2n)
+  int* status = nullptr;
+  unsigned long long* nrot = nullptr;
+  void* eig_ws = nullptr;
+  void* pseudo_ws = nullptr;
+  cudaStream_t stream = nullptr;
+};
+
+static void ctx_free(mb_ctx* c) {
+  if (!c) return;
+  mb_atoms_destroy(&c->atoms);
+  void* ptrs[] = {c->d_nat, c->d_coord, c->h, c->w, c->f, c->p, c->pa, c->pold, c->pold2, c->c, c->eigs,
+                  c->fdiag, c->scal, c->hws, c->status, c->nrot, c->eig_ws, c->pseudo_ws};
+  for (void* q : ptrs)
+    if (q) cudaFree(q);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+}
+
+extern "C" void mb_scf_opts_default(mb_scf_opts* o) {
+  o->pseudo = 0;
+  o->itrmax = 2000;
+  o->scfcrt = 1.0e-4;
+  o->precision = 0;
+  o->switch_pl = 1.0e-4;
+  o->verbose = 0;
+}
+
+extern "C" int mb_ctx_create(int numat, const int* nat, const double* coord, mb_ctx** out) {
+  if (numat <= 0 || !nat || !out) return mb_set_error(MB_ERR_ARG, "mb_ctx_create: bad args");
+  *out = nullptr;
+  static Pm7Params P;
+  static bool pinit = false;
+  if (!pinit) { pm7_init(&P); pinit = true; }
+  mb_ctx* c = new mb_ctx();
+  c->numat = numat;
+  c->nat.assign(nat, nat + numat);
+  if (coord) c->coord.assign(coord, coord + 3 * (size_t)numat);
+  else c->coord.assign(3 * (size_t)numat, 0.0);
+  c->nfirst.resize(numat);
+  c->nlast.resize(numat);
+  int ia = 1, nelec = 0;
+  for (int a = 0; a < numat; ++a) {
+    if (!pm7_supported(nat[a])) { delete c; return mb_set_error(MB_ERR_UNSUPPORTED, "element outside H, C, O"); }
+    const Pm7Elem& e = P.el[nat[a]];
+    c->nfirst[a] = ia;
+    c->nlast[a] = ia + e.natorb - 1;
+    ia += e.natorb;
+    nelec += (int)e.tore;
+  }
+  if (nelec % 2) { delete c; return mb_set_error(MB_ERR_UNSUPPORTED, "closed-shell RHF needs an even electron count"); }
+  c->norbs = ia - 1;
+  c->nclose = nelec / 2;
+  c->mpack = (long long)c->norbs * (c->norbs + 1) / 2;
+  // diagonal guess (moldat.F90:731-760) and atomic heat (mopac_api_initialize.F90:340-350)
+  c->pdiag.resize(c->norbs);
+  double atheat = 0.0, eat = 0.0;
+  for (int a = 0; a < numat; ++a) {
+    const Pm7Elem& e = P.el[nat[a]];
+    for (int q = c->nfirst[a] - 1; q < c->nlast[a]; ++q) c->pdiag[q] = e.natorb == 1 ? e.tore : e.tore * 0.25;
+    atheat += e.eheat;
+  }
+  for (int a = 0; a < numat; ++a) eat += P.el[nat[a]].eisol;
+  c->atheat = atheat - eat * PM7_FPC9;
+  int rc = mb_atoms_create(numat, c->nfirst.data(), c->nlast.data(), &c->atoms);
+  if (rc != MB_OK) { ctx_free(c); return rc; }
+  {
+    std::vector<int> first, nor, lim, cum;
+    std::vector<long long> wrow;
+    build_layout(numat, c->nfirst.data(), c->nlast.data(), first, nor, lim, wrow, cum, &c->n2elec);
+  }
+  const int n = c->norbs;
+  const size_t mp = (size_t)c->mpack, nn = (size_t)n * n;
+  cudaError_t e = cudaSuccess;
+#define ALLOC(ptr, bytes) if (e == cudaSuccess) e = cudaMalloc((void**)&(ptr), (bytes))
+  ALLOC(c->d_nat, sizeof(int) * numat);
+  ALLOC(c->d_coord, sizeof(double) * 3 * numat);
+  ALLOC(c->h, sizeof(double) * mp);
+  ALLOC(c->w, sizeof(double) * (size_t)c->n2elec);
+  ALLOC(c->f, sizeof(double) * mp);
+  ALLOC(c->p, sizeof(double) * mp);
+  ALLOC(c->pa, sizeof(double) * mp);
+  ALLOC(c->pold, sizeof(double) * mp);
+  ALLOC(c->pold2, sizeof(double) * n);
+  ALLOC(c->c, sizeof(double) * nn);
+  ALLOC(c->eigs, sizeof(double) * n);
+  ALLOC(c->fdiag, sizeof(double) * mp);
+  ALLOC(c->scal, sizeof(double) * 64);
+  ALLOC(c->hws, sizeof(double) * 2 * n);
+  ALLOC(c->status, sizeof(int) * 4);
+  ALLOC(c->nrot, sizeof(unsigned long long) * 2);
+  ALLOC(c->eig_ws, mb_eigh_ws_bytes(n));
+#undef ALLOC
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaMemcpy(c->d_nat, nat, sizeof(int) * numat, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(c->d_coord, c->coord.data(), sizeof(double) * 3 * numat, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemset(c->c, 0, sizeof(double) * nn);
+  if (e == cudaSuccess) e = cudaMemset(c->eigs, 0, sizeof(double) * n);
+  if (e != cudaSuccess) {
+    int r = mb_set_cuda_error(e, "mb_ctx_create", __FILE__, __LINE__);
+    ctx_free(c);
+    return r;
+  }
+  *out = c;
+  return MB_OK;
+}
+
+extern "C" int mb_ctx_destroy(mb_ctx* c) {
+  if (c) {
+    cudaStreamSynchronize(c->stream);
+    ctx_free(c);
+  }
+  return MB_OK;
+}
+
+extern "C" int mb_ctx_norbs(const mb_ctx* c) { return c ? c->norbs : 0; }
+extern "C" long long mb_ctx_n2elec(const mb_ctx* c) { return c ? c->n2elec : 0; }
+extern "C" int mb_ctx_nclose(const mb_ctx* c) { return c ? c->nclose : 0; }
+
+extern "C" int mb_ctx_set_hw(mb_ctx* c, const double* h, const double* w, double enuclr) {
+  if (!c || !h || !w) return mb_set_error(MB_ERR_ARG, "mb_ctx_set_hw: bad args");
+  MB_CUDA(cudaMemcpyAsync(c->h, h, sizeof(double) * (size_t)c->mpack, cudaMemcpyHostToDevice, c->stream));
+  MB_CUDA(cudaMemcpyAsync(c->w, w, sizeof(double) * (size_t)c->n2elec, cudaMemcpyHostToDevice, c->stream));
+  MB_CUDA(cudaStreamSynchronize(c->stream));
+  c->enuclr = enuclr;
+  c->have_hw = true;
+  return MB_OK;
+}
+
+extern "C" int mb_ctx_get_hw(mb_ctx* c, double* h, double* w, double* enuclr) {
+  if (!c || !c->have_hw) return mb_set_error(MB_ERR_ARG, "mb_ctx_get_hw: no integrals yet");
+  if (h) MB_CUDA(cudaMemcpyAsync(h, c->h, sizeof(double) * (size_t)c->mpack, cudaMemcpyDeviceToHost, c->stream));
+  if (w) MB_CUDA(cudaMemcpyAsync(w, c->w, sizeof(double) * (size_t)c->n2elec, cudaMemcpyDeviceToHost, c->stream));
+  MB_CUDA(cudaStreamSynchronize(c->stream));
+  if (enuclr) *enuclr = c->enuclr;
+  return MB_OK;
+}
+
+extern "C" int mb_ctx_hcore(mb_ctx* c) {
+  if (!c) return mb_set_error(MB_ERR_ARG, "mb_ctx_hcore: null context");
+  // pair energies and e1b/e2a staging live in the eigensolver workspace (idle here)
+  double* enuc_pairs = (double*)c->eig_ws;
+  MB_TRY(mb_hcore_dev(c->d_nat, c->d_coord, &c->atoms, c->numat, c->h, c->w, enuc_pairs, c->stream));
+  MB_TRY(mb_hcore_finish(c->numat, &c->atoms, c->d_nat, c->h, nullptr, c->scal + 16, enuc_pairs, c->stream));
+  double en = 0.0;
+  MB_CUDA(cudaMemcpyAsync(&en, c->scal + 16, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  MB_CUDA(cudaStreamSynchronize(c->stream));
+  c->enuclr = en;
+  c->have_hw = true;
+  return MB_OK;
+}
+
+extern "C" int mb_ctx_get_density(mb_ctx* c, double* p) {
+  if (!c || !p) return mb_set_error(MB_ERR_ARG, "mb_ctx_get_density: bad args");
+  MB_CUDA(cudaMemcpyAsync(p, c->p, sizeof(double) * (size_t)c->mpack, cudaMemcpyDeviceToHost, c->stream));
+  MB_CUDA(cudaStreamSynchronize(c->stream));
+  return MB_OK;
+}
+
+extern "C" int mb_ctx_get_vectors(mb_ctx* c, double* cv, double* eigs) {
+  if (!c) return mb_set_error(MB_ERR_ARG, "mb_ctx_get_vectors: null context");
+  if (cv) MB_CUDA(cudaMemcpyAsync(cv, c->c, sizeof(double) * (size_t)c->norbs * c->norbs, cudaMemcpyDeviceToHost, c->stream));
+  if (eigs) MB_CUDA(cudaMemcpyAsync(eigs, c->eigs, sizeof(double) * (size_t)c->norbs, cudaMemcpyDeviceToHost, c->stream));
+  MB_CUDA(cudaStreamSynchronize(c->stream));
+  return MB_OK;
+}
+
+extern "C" int mb_ctx_get_fock(mb_ctx* c, double* f) {
+  if (!c || !f) return mb_set_error(MB_ERR_ARG, "mb_ctx_get_fock: bad args");
+  MB_CUDA(cudaMemcpyAsync(f, c->f, sizeof(double) * (size_t)c->mpack, cudaMemcpyDeviceToHost, c->stream));
+  MB_CUDA(cudaStreamSynchronize(c->stream));
+  return MB_OK;
+}
+
+extern "C" int mb_ctx_device_ptrs(mb_ctx* c, double** h, double** w, double** f, double** p, double** cv,
+                                  double** eigs) {
+  if (!c) return mb_set_error(MB_ERR_ARG, "null context");
+  if (h) *h = c->h;
+  if (w) *w = c->w;
+  if (f) *f = c->f;
+  if (p) *p = c->p;
+  if (cv) *cv = c->c;
+  if (eigs) *eigs = c->eigs;
+  return MB_OK;
+}
+
+extern "C" int mb_ctx_atoms_dev(mb_ctx* c, MbAtomsDev* out) {
+  if (!c || !out) return mb_set_error(MB_ERR_ARG, "null context");
+  *out = c->atoms;
+  return MB_OK;
+}
+
+// ---------------------------------------------------------------- kernels
+namespace {
+__global__ void half_kernel(long long n, const double* __restrict__ p, double* __restrict__ pa) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    pa[i] = p[i] * 0.5;
+}
+__global__ void add_tail_kernel(int n, int from, double* e, double s) {
+  int i = from + blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) e[i] = e[i] + s;
+}
+}  // namespace
+
+static int d2h(mb_ctx* c, double* dst, const double* src, int count) {
+  MB_CUDA(cudaMemcpyAsync(dst, src, sizeof(double) * count, cudaMemcpyDeviceToHost, c->stream));
+  MB_CUDA(cudaStreamSynchronize(c->stream));
+  return MB_OK;
+}
+
+struct PhaseTimer {
+  cudaEvent_t a, b;
+  float total = 0.f;
+  cudaStream_t s;
+  explicit PhaseTimer(cudaStream_t st) : s(st) { cudaEventCreate(&a); cudaEventCreate(&b); }
+  ~PhaseTimer() { cudaEventDestroy(a); cudaEventDestroy(b); }
+  void start() { cudaEventRecord(a, s); }
+  void stop() {
+    cudaEventRecord(b, s);
+    cudaEventSynchronize(b);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, a, b);
+    total += ms;
+  }
+};
+
+static int full_diag(mb_ctx* c, double* fpacked, double* eig_homo, double* eig_lumo, int ihomo) {
+  MB_TRY(mb_eigh_ws(c->norbs, fpacked, 1, c->c, c->eigs, c->eig_ws, c->status, c->stream));
+  int st = 0;
+  MB_CUDA(cudaMemcpyAsync(&st, c->status, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  double hl[2] = {0.0, 0.0};
+  const int n = c->norbs;
+  MB_CUDA(cudaMemcpyAsync(hl, c->eigs + (ihomo - 1), sizeof(double) * (ihomo < n ? 2 : 1), cudaMemcpyDeviceToHost,
+                          c->stream));
+  MB_CUDA(cudaStreamSynchronize(c->stream));
+  if (st != 0) return mb_set_error(MB_ERR_NUMERIC, "eigensolver failed (inverse iteration)");
+  *eig_homo = hl[0];
+  *eig_lumo = hl[1];
+  return MB_OK;
+}
+
+extern "C" int mb_scf_run(mb_ctx* c, const mb_scf_opts* opts_in, mb_scf_result* res) {
+  if (!c || !res) return mb_set_error(MB_ERR_ARG, "mb_scf_run: bad args");
+  if (!c->have_hw) return mb_set_error(MB_ERR_ARG, "mb_scf_run: call mb_ctx_hcore or mb_ctx_set_hw first");
+  mb_scf_opts opts;
+  if (opts_in) opts = *opts_in; else mb_scf_opts_default(&opts);
+  memset(res, 0, sizeof(*res));
+  const int n = c->norbs;
+  const long long mpack = c->mpack;
+  const int nclose = c->nclose;
+  cudaStream_t s = c->stream;
+  if (opts.pseudo && !c->pseudo_ws) MB_CUDA(cudaMalloc(&c->pseudo_ws, mb_pseudo_ws_bytes(n, nclose)));
+  PhaseTimer t_fock(s), t_diag(s), t_dens(s);
+  cudaEvent_t ev_begin, ev_end;
+  MB_CUDA(cudaEventCreate(&ev_begin));
+  MB_CUDA(cudaEventCreate(&ev_end));
+  MB_CUDA(cudaEventRecord(ev_begin, s));
+
+  // ---- first-call setup (iter.F90:123-221)
+  const double enrgy = PM7_FPC9;
+  double shift = 1.0, shfmax = 20.0, pl = 1.0, bshift = -80.0, ten = bshift, shfto = 0.0, shftbo = 0.0,
+         shiftb = 0.0;
+  const double plchek = 0.005, trans = 0.2;
+  bool newdg = false, oknewd = fabs(bshift) < 0.001;
+  const bool okpuly = false, halfe = false, camkin = false;
+  const int na1el = nclose, nb1el = nclose;
+  const int ihomo = nclose > 1 ? nclose : 1;
+  {
+    std::vector<double> hp(mpack, 0.0), hpa(mpack, 0.0), hpd(n);
+    const double w1 = na1el / (na1el + 1.0e-6 + nb1el);
+    double random = 1.0;
+    for (int i = 0; i < n; ++i) {
+      long long j = (long long)i * (i + 1) / 2 + i;
+      hp[j] = c->pdiag[i];
+      hpa[j] = hp[j] * w1 * random;
+      random = 1.0 / random;
+      hpd[i] = hpa[j];
+    }
+    MB_CUDA(cudaMemcpyAsync(c->p, hp.data(), sizeof(double) * mpack, cudaMemcpyHostToDevice, s));
+    MB_CUDA(cudaMemcpyAsync(c->pa, hpa.data(), sizeof(double) * mpack, cudaMemcpyHostToDevice, s));
+    MB_CUDA(cudaMemcpyAsync(c->pold, hpa.data(), sizeof(double) * mpack, cudaMemcpyHostToDevice, s));
+    MB_CUDA(cudaMemcpyAsync(c->pold2, hpd.data(), sizeof(double) * n, cudaMemcpyHostToDevice, s));
+    MB_CUDA(cudaStreamSynchronize(s));
+  }
+  const double gnorm = 0.0;
+  double selcon = opts.scfcrt;
+  selcon = fmin(fmin(opts.scfcrt * 100.0, 0.1), fmax(opts.scfcrt * gnorm * gnorm * gnorm, opts.scfcrt));
+  const double pltest = 0.05 * sqrt(fabs(selcon));
+  int iredy = 1, niter = 0;
+  double eold = 1.0e2, diff = 0.0, escf = 0.0, ee = 0.0, sellim = 0.0;
+  const double scorr = 0.0;
+  bool ready = false, converged = false;
+  double eig_homo = 0.0, eig_lumo = 0.0;  // host copies of eigs(ihomo), eigs(ihomo+1)
+  const int hblocks = (int)((mpack + 255) / 256 > 148 * 16 ? 148 * 16 : (mpack + 255) / 256);
+
+  for (;;) {  // label 250
+    ++niter;
+    if (niter > opts.itrmax) break;
+    bool use_shift = false;
+    if (fabs(shift) > 1.0e-10 && bshift != 0.0) {
+      if (niter > 1) {
+        if (newdg && !(halfe || camkin)) {
+          if (diff > 0.0) {
+            shift = 1.0;
+            if (diff > 1) newdg = false;
+          } else {
+            shift = -0.1;
+          }
+        } else {
+          shift = (ihomo < n) ? ten + eig_lumo - eig_homo + shift : 0.0;
+        }
+        if (diff > 0.0) {
+          if (shift > 4.0) shfmax = 4.5;
+          if (shift > shfmax) shfmax = fmax(shfmax - 0.5, 0.0);
+        }
+        shift = fmax(-20.0, fmin(shfmax, shift));
+        if (fabs(shift - shfmax) < 1.0e-5) shfmax = shfmax + 0.01;
+        if (okpuly || fabs(bshift - 4.44) < 1.0e-5) {
+          shift = -8.0;
+          if (newdg) shift = 0.0;
+        }
+      }
+      if (pl > plchek) {
+        shftbo = shiftb;
+        shfto = shift;
+      } else {
+        shiftb = shftbo;
+        shift = shfto;
+      }
+      if (ihomo < n) {
+        add_tail_kernel<<<(n - ihomo + 255) / 256, 256, 0, s>>>(n, ihomo, c->eigs, shift);
+        MB_LAUNCH_CHECK();
+        eig_lumo = eig_lumo + shift;
+      }
+      use_shift = true;
+    }
+    double cur_shift = shift;
+    for (;;) {  // label 320
+      t_fock.start();
+      MB_TRY(mb_fock2_dev(&c->atoms, c->f, c->h, c->p, c->pa, c->w, cur_shift, use_shift ? 1 : 0, s));
+      t_fock.stop();
+      MB_TRY(mb_helect_ws(n, c->pa, c->h, c->f, c->scal, c->hws, s));
+      double hee = 0.0;
+      MB_TRY(d2h(c, &hee, c->scal, 1));
+      ee = hee * 2.0;
+      escf = (ee + c->enuclr) * enrgy + c->atheat + scorr;
+      diff = escf - eold;
+      if (diff > 0) ten = ten - 1.0;
+      else ten = ten * 0.975 + 0.05;
+      sellim = fmax(selcon, 1.0e-15 * fmax(fabs(ee), 1.0));
+      const bool conv = niter > 4 && (pl == 0.0 || (pl < pltest && fabs(diff) < sellim)) && ready;
+      if (conv) {
+        if (fabs(shift) < 1.0e-10) { converged = true; break; }
+        shift = 0.0;
+        shiftb = 0.0;
+        use_shift = false;
+        cur_shift = 0.0;
+        continue;
+      }
+      break;
+    }
+    if (converged) break;
+    ready = iredy > 0 && (fabs(diff) < sellim * 10.0 || pl == 0.0);
+    ++iredy;
+    eold = escf;
+    if (opts.verbose)
+      fprintf(stderr, " ITERATION %4d PLS=%10.3e ENERGY %14.6f DELTAE %13.7f shift %8.3f %s\n", niter, pl, escf, diff,
+              shift, newdg ? "newdg" : "");
+    t_diag.start();
+    if (newdg && opts.pseudo && !(halfe || camkin)) {
+      MB_TRY(mb_pseudo_diag_ws(n, na1el, c->f, c->c, c->eigs, c->nrot, c->pseudo_ws, s));
+      res->n_pseudo_diag++;
+    } else {
+      MB_TRY(full_diag(c, c->f, &eig_homo, &eig_lumo, ihomo));
+      res->n_full_diag++;
+    }
+    t_diag.stop();
+    t_dens.start();
+    MB_TRY(mb_density_dev(n, nclose, 2.0, c->c, n, c->p, s));
+    MB_TRY(mb_cnvg_ws(n, c->p, c->pold, c->pold2, niter, c->scal + 1, c->scal + 8, s));
+    half_kernel<<<hblocks, 256, 0, s>>>(mpack, c->p, c->pa);
+    MB_LAUNCH_CHECK();
+    t_dens.stop();
+    MB_TRY(d2h(c, &pl, c->scal + 1, 1));
+    if (!isfinite(pl)) return mb_set_error(MB_ERR_NUMERIC, "non-finite density change");
+    oknewd = pl < sellim || oknewd;
+    newdg = (pl < trans && oknewd) || newdg;
+    if (pl < trans * 0.3333) oknewd = true;
+  }
+  // ---- label 600: final energy and exit diagonalisation
+  MB_TRY(mb_helect_ws(n, c->pa, c->h, c->f, c->scal, c->hws, s));
+  double hee = 0.0;
+  MB_TRY(d2h(c, &hee, c->scal, 1));
+  ee = hee * 2.0;
+  MB_CUDA(cudaMemcpyAsync(c->fdiag, c->f, sizeof(double) * mpack, cudaMemcpyDeviceToDevice, s));
+  t_diag.start();
+  MB_TRY(full_diag(c, c->fdiag, &eig_homo, &eig_lumo, ihomo));
+  t_diag.stop();
+  res->n_full_diag++;
+  escf = (ee + c->enuclr) * enrgy + c->atheat;
+  res->escf = escf;
+  res->ee = ee;
+  res->niter = niter;
+  res->converged = converged ? 1 : 0;
+  res->pl = pl;
+  res->t_fock_ms = t_fock.total;
+  res->t_diag_ms = t_diag.total;
+  res->t_density_ms = t_dens.total;
+  MB_CUDA(cudaEventRecord(ev_end, s));
+  MB_CUDA(cudaEventSynchronize(ev_end));
+  float tot = 0.f;
+  MB_CUDA(cudaEventElapsedTime(&tot, ev_begin, ev_end));
+  cudaEventDestroy(ev_begin);
+  cudaEventDestroy(ev_end);
+  res->t_total_ms = tot;
+  res->t_other_ms = tot - res->t_fock_ms - res->t_diag_ms - res->t_density_ms;
+  if (!converged) return mb_set_error(MB_ERR_NOCONV, "UNABLE TO ACHIEVE SELF-CONSISTENCE");
+  return MB_OK;
+}

@@ -1,0 +1,474 @@
+// SCF step kernels other than the Fock build and the eigensolver:
+//   helect   integrals/helect.F90          electronic energy
+//   cnvg     SCF/cnvg.F90                  density extrapolation / damping
+//   unpack   dtpttr('u') as used by eigenvectors_LAPACK.F90:56 and
+//            diag_for_GPU.F90:101-114
+//   pseudo-diagonalisation, diag_for_GPU.F90:116-206: Fmo = C_v^T F C_o by
+//            FP64 GEMM, tiny = 0.05 max|Fmo|, rotation coefficients and the
+//            ordered 2x2 rotation sweep over the columns of C.
+#include "mb_common.cuh"
+
+namespace {
+
+// ------------------------------------------------------------------ helect
+// Row sums of P(H+F) below the diagonal and the diagonal terms; one warp/row.
+__global__ void helect_rows(int n, const double* __restrict__ p, const double* __restrict__ h,
+                            const double* __restrict__ f, double* __restrict__ rows,
+                            double* __restrict__ diag) {
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (warp >= n) return;
+  const long long base = (long long)warp * (warp + 1) / 2;
+  double s = 0.0;
+  for (int c = lane; c < warp; c += 32) s += p[base + c] * (h[base + c] + f[base + c]);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if (lane == 0) {
+    rows[warp] = s;
+    diag[warp] = p[base + warp] * (h[base + warp] + f[base + warp]);
+  }
+}
+
+// ee = sum(rows) + 0.5 * sum(diag), fixed-order block reduction.
+__global__ void helect_final(int n, const double* __restrict__ rows, const double* __restrict__ diag,
+                             double* __restrict__ out) {
+  __shared__ double sr[1024], sd[1024];
+  double a = 0.0, b = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) { a += rows[i]; b += diag[i]; }
+  sr[threadIdx.x] = a;
+  sd[threadIdx.x] = b;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) { sr[threadIdx.x] += sr[threadIdx.x + s]; sd[threadIdx.x] += sd[threadIdx.x + s]; }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *out = sr[0] + 0.5 * sd[0];
+}
+
+// -------------------------------------------------------------------- cnvg
+// Scalars shared between the three cnvg phases (device scratch).
+struct CnvgState {
+  double fac;
+  double pl;
+};
+
+// Phase 1 (one CTA): diagonal statistics in reference order (thread 0), the
+// history update p1 <- p_ii and p_ii <- pnew_ii, and the extrapolation factor.
+__global__ void cnvg_diag1(int norbs, const double* __restrict__ pnew, double* __restrict__ p,
+                           double* __restrict__ p1, int niter, CnvgState* st, double* sum1_out) {
+  extern __shared__ double sh[];
+  double* sa_new = sh;           // pnew_ii
+  double* sa_old = sh + norbs;   // p_ii
+  for (int i = threadIdx.x; i < norbs; i += blockDim.x) {
+    long long k = mb_tri(i, i);
+    sa_new[i] = pnew[k];
+    sa_old[i] = p[k];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const bool extrap = (niter % 3) != 0;
+    double pl = 0.0, faca = 0.0, facb = 0.0, sum1 = 0.0;
+    for (int i = 0; i < norbs; ++i) {
+      double a = sa_new[i];
+      sum1 = DADD(sum1, a);
+      double sa = fabs(DSUB(a, sa_old[i]));
+      if (sa > pl) pl = sa;
+      if (!extrap) {
+        faca = DADD(faca, DMUL(sa, sa));
+        double t = DADD(DSUB(a, DMUL(2.0, sa_old[i])), p1[i]);
+        facb = DADD(facb, DMUL(t, t));
+      }
+    }
+    double fac = 0.0;
+    if (facb > 1.0e-10 && faca < DMUL(100.0, facb)) fac = sqrt(faca / facb);
+    st->fac = fac;
+    st->pl = pl;
+    *sum1_out = sum1;
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < norbs; i += blockDim.x) {
+    long long k = mb_tri(i, i);
+    p1[i] = sa_old[i];
+    p[k] = sa_new[i];
+  }
+}
+
+// Phase 2 (one CTA per row): off-diagonal extrapolation p = a + fac (a - p).
+__global__ void cnvg_offdiag(int norbs, double* __restrict__ pnew, double* __restrict__ p,
+                             const CnvgState* __restrict__ st) {
+  const double fac = st->fac;
+  for (int r = blockIdx.x; r < norbs; r += gridDim.x) {
+    const long long base = (long long)r * (r + 1) / 2;
+    for (int c = threadIdx.x; c < r; c += blockDim.x) {
+      const long long idx = base + c;
+      double a = pnew[idx];
+      double v = DADD(a, DMUL(fac, DSUB(a, p[idx])));
+      p[idx] = v;
+      pnew[idx] = v;
+    }
+  }
+}
+
+// Phase 3 (one CTA, thread 0 sequential): diagonal damping, clamp to [0, 2],
+// trace renormalisation loop; exactly the reference's order.
+__global__ void cnvg_diag2(int norbs, double* __restrict__ pnew, double* __restrict__ p,
+                           const double* __restrict__ p1, int niter, const CnvgState* st,
+                           const double* sum1_in, double* pl_out) {
+  extern __shared__ double sh[];
+  double* pd = sh;
+  double* p1s = sh + norbs;
+  for (int i = threadIdx.x; i < norbs; i += blockDim.x) {
+    pd[i] = p[mb_tri(i, i)];
+    p1s[i] = p1[i];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const double rhfuhf = 2.0;
+    const double damp = (niter > 3) ? 0.05 : 1.0e10;
+    const double fac = st->fac;
+    double sum2 = 0.0;
+    for (int i = 0; i < norbs; ++i) {
+      double v = pd[i];
+      double dlt = DSUB(v, p1s[i]);
+      if (fabs(dlt) > damp) v = DADD(p1s[i], copysign(damp, dlt));
+      else v = DADD(v, DMUL(fac, dlt));
+      double t = v > 0.0 ? v : 0.0;
+      v = t < rhfuhf ? t : rhfuhf;
+      sum2 = DADD(sum2, v);
+      pd[i] = v;
+    }
+    double sum0 = *sum1_in, sum1 = sum0;
+    for (int guard = 0; guard < 1000; ++guard) {
+      double sum = sum2 > 1.0e-3 ? sum1 / sum2 : 0.0;
+      sum1 = sum0;
+      if (sum2 < 1.0e-3 || fabs(DSUB(sum, 1.0)) < 1.0e-5) break;
+      sum2 = 0.0;
+      for (int i = 0; i < norbs; ++i) {
+        double v = DADD(DMUL(pd[i], sum), 1.0e-20);
+        v = v > 0.0 ? v : 0.0;
+        if (v > rhfuhf) {
+          v = rhfuhf;
+          sum1 = DSUB(sum1, rhfuhf);
+        } else {
+          sum2 = DADD(sum2, v);
+        }
+        pd[i] = v;
+      }
+    }
+    *pl_out = st->pl;
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < norbs; i += blockDim.x) {
+    long long k = mb_tri(i, i);
+    p[k] = pd[i];
+    pnew[k] = pd[i];
+  }
+}
+
+// ------------------------------------------------------------------ unpack
+// Full symmetric column-major matrix from packed lower storage.
+__global__ void unpack_sym(int n, const double* __restrict__ pk, double* __restrict__ a, int lda) {
+  const int col = blockIdx.y;
+  for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < n; row += gridDim.x * blockDim.x) {
+    long long idx = row >= col ? mb_tri(row, col) : mb_tri(col, row);
+    a[(long long)col * lda + row] = pk[idx];
+  }
+}
+
+__global__ void perturb_diag(int n, double* __restrict__ pk) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    long long k = mb_tri(i, i);
+    pk[k] = DADD(pk[k], DMUL((double)(i + 1), 1.0e-10));
+  }
+}
+
+// -------------------------------------------------------- pseudo-diag sweep
+constexpr int RT = 16;          // rotation tile: 16 occupied x 16 virtual columns
+constexpr int ROWS = 64;        // rows of C per CTA (one row per thread)
+
+__global__ void absmax_kernel(long long len, const double* __restrict__ x, unsigned long long* out) {
+  double m = 0.0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < len; i += (long long)gridDim.x * blockDim.x)
+    m = fmax(m, fabs(x[i]));
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, __double_as_longlong(m));  // m >= 0: bit order == value order
+}
+
+// Rotation coefficients for every (occupied i, virtual a) pair in the
+// reference's arithmetic (diag_for_GPU.F90:176-206).  act = 0 means skipped.
+__global__ void rot_coeff_kernel(int nocc, int nvirt, const double* __restrict__ fmo,
+                                 const double* __restrict__ eig, const unsigned long long* tinybits,
+                                 double tiny_direct, double bigeps, double* __restrict__ alpha, double* __restrict__ beta,
+                                 unsigned char* __restrict__ act, unsigned int* __restrict__ tile_cnt,
+                                 unsigned long long* __restrict__ nrot, int ntile_v) {
+  // tiny = 0.05 * max|Fmo| (diag_for_GPU.F90:151-152) unless given directly
+  const double tiny = tiny_direct >= 0.0 ? tiny_direct : __longlong_as_double(*tinybits) * 0.05;
+  const long long total = (long long)nocc * nvirt;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < total; q += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(q / nvirt), av = (int)(q % nvirt);
+    const double x = fmo[av + (long long)nvirt * i];
+    unsigned char on = 0;
+    double al = 1.0, be = 0.0;
+    if (!(fabs(x) < tiny)) {
+      const double d = DSUB(eig[i], eig[nocc + av]);
+      if (!(fabs(x / d) < bigeps)) {
+        const double e = copysign(sqrt(DADD(DMUL(DMUL(4.0, x), x), DMUL(d, d))), d);
+        al = sqrt(DMUL(0.5, DADD(1.0, d / e)));
+        be = -copysign(sqrt(DSUB(1.0, DMUL(al, al))), x);
+        on = 1;
+      }
+    }
+    alpha[q] = al;
+    beta[q] = be;
+    act[q] = on;
+    if (on) {
+      atomicAdd(&tile_cnt[(i / RT) * ntile_v + av / RT], 1u);
+      atomicAdd(nrot, 1ull);
+    }
+  }
+}
+
+// Apply all active rotations to C in the reference order.  Each thread owns one
+// row of C.  Tiles are visited occupied-block outer, virtual-block inner; inside
+// a tile, occupied column i outer, virtual column j inner.  That keeps the order
+// of operations on every column identical to the sequential sweep (rotations on
+// disjoint column pairs commute exactly), so the result is bit-identical.
+__global__ void __launch_bounds__(ROWS) rot_sweep_kernel(int n, int nocc, int nvirt, double* __restrict__ c,
+                                                         const double* __restrict__ alpha,
+                                                         const double* __restrict__ beta,
+                                                         const unsigned char* __restrict__ act,
+                                                         const unsigned int* __restrict__ tile_cnt,
+                                                         int ntile_o, int ntile_v) {
+  __shared__ double s_al[RT][RT], s_be[RT][RT];
+  __shared__ unsigned char s_on[RT][RT];
+  const int r = blockIdx.x * ROWS + threadIdx.x;
+  const bool live = r < n;
+  for (int ti = 0; ti < ntile_o; ++ti) {
+    const int i0 = ti * RT;
+    bool any = false;
+    for (int tj = 0; tj < ntile_v; ++tj) any |= tile_cnt[ti * ntile_v + tj] != 0;
+    if (!any) continue;
+    double xi[RT];
+#pragma unroll
+    for (int u = 0; u < RT; ++u) xi[u] = (live && i0 + u < nocc) ? c[(long long)(i0 + u) * n + r] : 0.0;
+    for (int tj = 0; tj < ntile_v; ++tj) {
+      if (tile_cnt[ti * ntile_v + tj] == 0) continue;
+      const int j0 = tj * RT;
+      __syncthreads();
+      for (int e = threadIdx.x; e < RT * RT; e += ROWS) {
+        int u = e / RT, v = e % RT;
+        bool in = (i0 + u < nocc) && (j0 + v < nvirt);
+        long long q = (long long)(i0 + u) * nvirt + (j0 + v);
+        s_on[u][v] = in ? act[q] : 0;
+        s_al[u][v] = in ? alpha[q] : 1.0;
+        s_be[u][v] = in ? beta[q] : 0.0;
+      }
+      __syncthreads();
+      double xj[RT];
+#pragma unroll
+      for (int v = 0; v < RT; ++v) xj[v] = (live && j0 + v < nvirt) ? c[(long long)(nocc + j0 + v) * n + r] : 0.0;
+#pragma unroll
+      for (int u = 0; u < RT; ++u)
+#pragma unroll
+        for (int v = 0; v < RT; ++v) {
+          if (s_on[u][v]) {
+            const double al = s_al[u][v], be = s_be[u][v];
+            const double a = xi[u], b = xj[v];
+            xi[u] = DADD(DMUL(al, a), DMUL(be, b));
+            xj[v] = DSUB(DMUL(al, b), DMUL(be, a));
+          }
+        }
+      if (live) {
+#pragma unroll
+        for (int v = 0; v < RT; ++v)
+          if (j0 + v < nvirt) c[(long long)(nocc + j0 + v) * n + r] = xj[v];
+      }
+    }
+    if (live) {
+#pragma unroll
+      for (int u = 0; u < RT; ++u)
+        if (i0 + u < nocc) c[(long long)(i0 + u) * n + r] = xi[u];
+    }
+  }
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------- C ABI
+extern "C" int mb_helect_dev(int n, const double* p, const double* h, const double* f, double* out,
+                             cudaStream_t stream) {
+  if (n <= 0) return mb_set_error(MB_ERR_ARG, "mb_helect_dev: n <= 0");
+  double* tmp = nullptr;
+  MB_CUDA(cudaMallocAsync(&tmp, sizeof(double) * 2 * (size_t)n, stream));
+  const int threads = 256;
+  const int blocks = (int)(((long long)n * 32 + threads - 1) / threads);
+  helect_rows<<<blocks, threads, 0, stream>>>(n, p, h, f, tmp, tmp + n);
+  MB_LAUNCH_CHECK();
+  helect_final<<<1, 1024, 0, stream>>>(n, tmp, tmp + n, out);
+  MB_LAUNCH_CHECK();
+  MB_CUDA(cudaFreeAsync(tmp, stream));
+  return MB_OK;
+}
+
+// Workspace-taking variants used by the SCF driver (no allocation per call).
+extern "C" int mb_helect_ws(int n, const double* p, const double* h, const double* f, double* out,
+                            double* ws /* 2n */, cudaStream_t stream) {
+  const int threads = 256;
+  const int blocks = (int)(((long long)n * 32 + threads - 1) / threads);
+  helect_rows<<<blocks, threads, 0, stream>>>(n, p, h, f, ws, ws + n);
+  MB_LAUNCH_CHECK();
+  helect_final<<<1, 1024, 0, stream>>>(n, ws, ws + n, out);
+  MB_LAUNCH_CHECK();
+  return MB_OK;
+}
+
+extern "C" int mb_cnvg_ws(int norbs, double* pnew, double* p, double* p1, int niter, double* pl_out,
+                          double* ws /* 4 doubles */, cudaStream_t stream) {
+  CnvgState* st = reinterpret_cast<CnvgState*>(ws);
+  double* sum1 = ws + 2;
+  size_t sh = sizeof(double) * 2 * (size_t)norbs;
+  if (sh > 200 * 1024) return mb_set_error(MB_ERR_ARG, "mb_cnvg: norbs too large for one CTA");
+  if (sh > 48 * 1024) {
+    MB_CUDA(cudaFuncSetAttribute(cnvg_diag1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh));
+    MB_CUDA(cudaFuncSetAttribute(cnvg_diag2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh));
+  }
+  cnvg_diag1<<<1, 1024, sh, stream>>>(norbs, pnew, p, p1, niter, st, sum1);
+  MB_LAUNCH_CHECK();
+  cnvg_offdiag<<<norbs, 256, 0, stream>>>(norbs, pnew, p, st);
+  MB_LAUNCH_CHECK();
+  cnvg_diag2<<<1, 1024, sh, stream>>>(norbs, pnew, p, p1, niter, st, sum1, pl_out);
+  MB_LAUNCH_CHECK();
+  return MB_OK;
+}
+
+extern "C" int mb_cnvg_dev(int norbs, double* pnew, double* p, double* p1, int niter, double* pl_out,
+                           cudaStream_t stream) {
+  if (norbs <= 0) return mb_set_error(MB_ERR_ARG, "mb_cnvg_dev: norbs <= 0");
+  double* ws = nullptr;
+  MB_CUDA(cudaMallocAsync(&ws, sizeof(double) * 4, stream));
+  int rc = mb_cnvg_ws(norbs, pnew, p, p1, niter, pl_out, ws, stream);
+  cudaFreeAsync(ws, stream);
+  return rc;
+}
+
+extern "C" int mb_unpack_dev(int n, const double* pk, double* a, int lda, int perturb, double* pk_mut,
+                             cudaStream_t stream) {
+  if (perturb) {
+    perturb_diag<<<(n + 255) / 256, 256, 0, stream>>>(n, pk_mut);
+    MB_LAUNCH_CHECK();
+  }
+  dim3 grid((n + 255) / 256, n);
+  unpack_sym<<<grid, 256, 0, stream>>>(n, pk, a, lda);
+  MB_LAUNCH_CHECK();
+  return MB_OK;
+}
+
+// Every workspace region starts on a 256-byte boundary.
+static inline size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+// Workspace layout for the pseudo-diagonalisation (bytes):
+//   F full n*n | fck n*max(k,v) | fmo v*k | alpha k*v | beta k*v | act k*v |
+//   tile counts | tiny bits | nrot
+extern "C" size_t mb_pseudo_ws_bytes(int n, int nocc) {
+  size_t v = (size_t)(n - nocc), k = (size_t)nocc;
+  size_t kv = k * v;
+  size_t to = (k + RT - 1) / RT, tv = (v + RT - 1) / RT;
+  size_t b = 0;
+  b += align256(sizeof(double) * (size_t)n * n);
+  b += align256(sizeof(double) * (size_t)n * (k > v ? k : v));
+  b += 3 * align256(sizeof(double) * kv);
+  b += align256(kv);
+  b += align256(sizeof(unsigned int) * (to * tv + 64));
+  b += 256;
+  return b;
+}
+
+extern "C" int mb_pseudo_diag_ws(int n, int nocc, const double* fpacked, double* c, const double* eigs,
+                                 unsigned long long* nrot_dev, void* ws, cudaStream_t stream) {
+  const int nvirt = n - nocc;
+  if (nocc <= 0 || nvirt <= 0) return MB_OK;
+  if (((uintptr_t)ws & 255) != 0) return mb_set_error(MB_ERR_ARG, "pseudo-diag workspace must be 256-byte aligned");
+  const size_t kv = (size_t)nocc * nvirt;
+  char* b = (char*)ws;
+  double* ff = (double*)b; b += align256(sizeof(double) * (size_t)n * n);
+  double* fck = (double*)b; b += align256(sizeof(double) * (size_t)n * (nocc > nvirt ? nocc : nvirt));
+  double* fmo = (double*)b; b += align256(sizeof(double) * kv);
+  double* al = (double*)b; b += align256(sizeof(double) * kv);
+  double* be = (double*)b; b += align256(sizeof(double) * kv);
+  unsigned char* act = (unsigned char*)b; b += align256(kv);
+  const int to = (nocc + RT - 1) / RT, tv = (nvirt + RT - 1) / RT;
+  unsigned int* tcnt = (unsigned int*)b; b += align256(sizeof(unsigned int) * ((size_t)to * tv + 64));
+  unsigned long long* tiny = (unsigned long long*)b;
+  MB_TRY(mb_unpack_dev(n, fpacked, ff, n, 0, nullptr, stream));
+  // diag_for_GPU.F90:116-150
+  if (nocc < nvirt) {
+    MB_TRY(mb_dgemm_dev('N', 'N', n, nocc, n, 1.0, ff, n, c, n, 0.0, fck, n, stream));
+    MB_TRY(mb_dgemm_dev('T', 'N', nvirt, nocc, n, 1.0, c + (size_t)nocc * n, n, fck, n, 0.0, fmo, nvirt, stream));
+  } else {
+    MB_TRY(mb_dgemm_dev('N', 'N', n, nvirt, n, 1.0, ff, n, c + (size_t)nocc * n, n, 0.0, fck, n, stream));
+    MB_TRY(mb_dgemm_dev('T', 'N', nvirt, nocc, n, 1.0, fck, n, c, n, 0.0, fmo, nvirt, stream));
+  }
+  MB_CUDA(cudaMemsetAsync(tiny, 0, sizeof(unsigned long long), stream));
+  MB_CUDA(cudaMemsetAsync(tcnt, 0, sizeof(unsigned int) * (size_t)to * tv, stream));
+  MB_CUDA(cudaMemsetAsync(nrot_dev, 0, sizeof(unsigned long long), stream));
+  int blocks = (int)((kv + 255) / 256);
+  if (blocks > 148 * 8) blocks = 148 * 8;
+  absmax_kernel<<<blocks, 256, 0, stream>>>((long long)kv, fmo, tiny);
+  MB_LAUNCH_CHECK();
+  rot_coeff_kernel<<<blocks, 256, 0, stream>>>(nocc, nvirt, fmo, eigs, tiny, -1.0, 1.5e-7, al, be, act, tcnt, nrot_dev, tv);
+  MB_LAUNCH_CHECK();
+  rot_sweep_kernel<<<(n + ROWS - 1) / ROWS, ROWS, 0, stream>>>(n, nocc, nvirt, c, al, be, act, tcnt, to, tv);
+  MB_LAUNCH_CHECK();
+  return MB_OK;
+}
+
+// Rotation sweep alone with caller-given Fmo, tiny and bigeps (the arguments
+// of the reference's call_rot_cuda_gpu).  ws as for mb_pseudo_diag_ws.
+extern "C" int mb_rot_sweep_ws(int n, int nocc, const double* fmo, const double* eigs, double* c, double bigeps,
+                               double tiny, unsigned long long* nrot_dev, void* ws, cudaStream_t stream) {
+  const int nvirt = n - nocc;
+  if (nocc <= 0 || nvirt <= 0) return MB_OK;
+  if (((uintptr_t)ws & 255) != 0) return mb_set_error(MB_ERR_ARG, "rotation workspace must be 256-byte aligned");
+  const size_t kvs = (size_t)nocc * nvirt;
+  char* b = (char*)ws;
+  b += align256(sizeof(double) * (size_t)n * n);
+  b += align256(sizeof(double) * (size_t)n * (nocc > nvirt ? nocc : nvirt));
+  b += align256(sizeof(double) * kvs);
+  double* al = (double*)b; b += align256(sizeof(double) * kvs);
+  double* be = (double*)b; b += align256(sizeof(double) * kvs);
+  unsigned char* act = (unsigned char*)b; b += align256(kvs);
+  const int to = (nocc + RT - 1) / RT, tv = (nvirt + RT - 1) / RT;
+  unsigned int* tcnt = (unsigned int*)b;
+  MB_CUDA(cudaMemsetAsync(tcnt, 0, sizeof(unsigned int) * (size_t)to * tv, stream));
+  MB_CUDA(cudaMemsetAsync(nrot_dev, 0, sizeof(unsigned long long), stream));
+  const long long kv = (long long)nocc * nvirt;
+  int blocks = (int)((kv + 255) / 256);
+  if (blocks > 148 * 8) blocks = 148 * 8;
+  rot_coeff_kernel<<<blocks, 256, 0, stream>>>(nocc, nvirt, fmo, eigs, nullptr, tiny, bigeps, al, be, act, tcnt, nrot_dev, tv);
+  MB_LAUNCH_CHECK();
+  rot_sweep_kernel<<<(n + ROWS - 1) / ROWS, ROWS, 0, stream>>>(n, nocc, nvirt, c, al, be, act, tcnt, to, tv);
+  MB_LAUNCH_CHECK();
+  return MB_OK;
+}
+
+extern "C" int mb_pseudo_diag_dev(int n, int nocc, const double* fpacked, double* c, const double* eigs,
+                                  long long* nrot_out, cudaStream_t stream) {
+  if (n <= 0 || nocc < 0 || nocc > n) return mb_set_error(MB_ERR_ARG, "mb_pseudo_diag_dev: bad size");
+  void* ws = nullptr;
+  unsigned long long* nrot = nullptr;
+  MB_CUDA(cudaMallocAsync(&ws, mb_pseudo_ws_bytes(n, nocc), stream));
+  MB_CUDA(cudaMallocAsync((void**)&nrot, sizeof(unsigned long long), stream));
+  MB_CUDA(cudaMemsetAsync(nrot, 0, sizeof(unsigned long long), stream));
+  int rc = mb_pseudo_diag_ws(n, nocc, fpacked, c, eigs, nrot, ws, stream);
+  unsigned long long h = 0;
+  if (rc == MB_OK) {
+    cudaError_t e = cudaMemcpyAsync(&h, nrot, sizeof(h), cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    if (e != cudaSuccess) rc = mb_set_cuda_error(e, "pseudo_diag nrot", __FILE__, __LINE__);
+  }
+  cudaFreeAsync(ws, stream);
+  cudaFreeAsync(nrot, stream);
+  if (nrot_out) *nrot_out = (long long)h;
+  return rc;
+}

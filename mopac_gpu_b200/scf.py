@@ -1,0 +1,127 @@
+"""Host-side mirror of the reference's SCF entry point.
+
+``ScfContext`` owns a device-resident SCF context (H, W, F, P, C and the
+eigenvalues stay in HBM).  ``run`` is the counterpart of ``iter``
+(SCF/iter.F90) for closed-shell PM7: it returns the heat of formation
+``escf`` as iter computes it (kcal/mol, without the post-SCF geometry
+terms), the electronic energy, and the iteration count; errors surface as
+``LibraryError`` (MB_ERR_NOCONV is the reference's "UNABLE TO ACHIEVE
+SELF-CONSISTENCE").
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+
+from ._lib import ScfOpts, ScfRes, check, lib
+
+
+@dataclass
+class ScfResult:
+    escf: float
+    ee: float
+    niter: int
+    converged: bool
+    n_full_diag: int
+    n_pseudo_diag: int
+    pl: float
+    t_fock_ms: float
+    t_diag_ms: float
+    t_density_ms: float
+    t_other_ms: float
+    t_total_ms: float
+
+
+class ScfContext:
+    def __init__(self, nat, coord):
+        self.nat = np.ascontiguousarray(nat, dtype=np.int32)
+        self.coord = np.ascontiguousarray(coord, dtype=np.float64).reshape(-1, 3)
+        L = lib()
+        h = ctypes.c_void_p()
+        check(L.mb_ctx_create(int(self.nat.shape[0]), self.nat.ctypes.data, self.coord.ctypes.data,
+                              ctypes.byref(h)))
+        self._h = h
+        self.norbs = L.mb_ctx_norbs(h)
+        self.nclose = L.mb_ctx_nclose(h)
+        self.n2elec = L.mb_ctx_n2elec(h)
+        self.mpack = self.norbs * (self.norbs + 1) // 2
+
+    # -- integrals
+    def hcore(self) -> None:
+        check(lib().mb_ctx_hcore(self._h))
+
+    def set_hw(self, h: np.ndarray, w: np.ndarray, enuclr: float) -> None:
+        h = np.ascontiguousarray(h, dtype=np.float64)
+        w = np.ascontiguousarray(w, dtype=np.float64)
+        assert h.size == self.mpack and w.size == self.n2elec
+        check(lib().mb_ctx_set_hw(self._h, h.ctypes.data, w.ctypes.data, float(enuclr)))
+
+    def get_hw(self):
+        h = np.empty(self.mpack)
+        w = np.empty(self.n2elec)
+        e = ctypes.c_double()
+        check(lib().mb_ctx_get_hw(self._h, h.ctypes.data, w.ctypes.data, ctypes.byref(e)))
+        return h, w, e.value
+
+    # -- SCF
+    def run(self, pseudo: bool = False, scfcrt: float = 1.0e-4, itrmax: int = 2000, precision: int = 0,
+            switch_pl: float = 1.0e-4, verbose: bool = False) -> ScfResult:
+        o = ScfOpts()
+        lib().mb_scf_opts_default(ctypes.byref(o))
+        o.pseudo = int(pseudo)
+        o.scfcrt = scfcrt
+        o.itrmax = itrmax
+        o.precision = precision
+        o.switch_pl = switch_pl
+        o.verbose = int(verbose)
+        r = ScfRes()
+        check(lib().mb_scf_run(self._h, ctypes.byref(o), ctypes.byref(r)))
+        return ScfResult(r.escf, r.ee, r.niter, bool(r.converged), r.n_full_diag, r.n_pseudo_diag, r.pl,
+                         r.t_fock_ms, r.t_diag_ms, r.t_density_ms, r.t_other_ms, r.t_total_ms)
+
+    def density(self) -> np.ndarray:
+        p = np.empty(self.mpack)
+        check(lib().mb_ctx_get_density(self._h, p.ctypes.data))
+        return p
+
+    def vectors(self):
+        c = np.empty((self.norbs, self.norbs), order="F")
+        e = np.empty(self.norbs)
+        check(lib().mb_ctx_get_vectors(self._h, c.ctypes.data, e.ctypes.data))
+        return c, e
+
+    def fock(self) -> np.ndarray:
+        f = np.empty(self.mpack)
+        check(lib().mb_ctx_get_fock(self._h, f.ctypes.data))
+        return f
+
+    def device_ptrs(self):
+        ps = [ctypes.c_void_p() for _ in range(6)]
+        check(lib().mb_ctx_device_ptrs(self._h, *[ctypes.byref(p) for p in ps]))
+        return dict(zip(["h", "w", "f", "p", "c", "eigs"], [p.value for p in ps]))
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) is not None and self._h.value:
+            lib().mb_ctx_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+def run_scf(nat, coord, pseudo: bool = False, **kw):
+    """Integrals on the GPU, then the SCF; returns (ScfResult, context)."""
+    ctx = ScfContext(nat, coord)
+    ctx.hcore()
+    return ctx.run(pseudo=pseudo, **kw), ctx

@@ -1,0 +1,405 @@
+"""CPU oracle for the PM7 dense SCF path (test infrastructure only).
+
+Only tests/, __graft_entry__.smoke() and the CPU legs of bench.py may import
+this module; the product package never does.  It is the checker, not the
+thing measured or shipped.
+
+What it restates:
+  * ``iter`` (SCF/iter.F90:16-1107) for closed-shell RHF with the default
+    keywords (no UHF, no Camp-King, no C.I., id = 0): level-shift control
+    (:273-325), Fock build (:553), energy (:641-659), convergence test
+    (:675-690), full diagonalisation (:849) or, in ``pseudo`` mode, the
+    pseudo-diagonalisation the reference comments out (:847-861), density
+    (:897), ``cnvg`` (:899-901) and the exit diagonalisation (:1052-1106);
+  * ``eigenvectors_LAPACK`` (matrix/eigenvectors_LAPACK.F90:53-121): adds
+    i*1e-10 to diagonal element i, then LAPACK dsyevd (numpy.linalg.eigh calls
+    the same LAPACK driver);
+  * ``density_for_GPU`` iopc 5 (matrix/density_for_GPU.F90:102-108):
+    P = 2 C_occ C_occ^T;
+  * ``diag_for_GPU`` (matrix/diag_for_GPU.F90:101-206): Fmo = C_v^T F C_o and
+    the ordered 2x2 rotation sweep.
+The integral, Fock, energy and extrapolation kernels live in the C part
+(mopac_oracle.c) and are reached through ctypes.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from dataclasses import dataclass, field
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "_build", "liboracle.so")
+_lib = None
+
+FPC9 = 23.060547830619029
+EV = 27.211386245988
+
+
+def build() -> str:
+    """Compile the C oracle (gcc, -ffp-contract=off) into oracle/_build."""
+    src = os.path.join(_HERE, "mopac_oracle.c")
+    if (not os.path.exists(_LIB_PATH)) or os.path.getmtime(_LIB_PATH) < os.path.getmtime(src):
+        subprocess.check_call(["make", "-s", "-C", _HERE])
+    return _LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        L = ctypes.CDLL(_LIB_PATH)
+        i32p = np.ctypeslib.ndpointer(np.int32, flags="C")
+        f64p = np.ctypeslib.ndpointer(np.float64, flags="C")
+        L.orc_layout.argtypes = [ctypes.c_int, i32p, i32p, i32p]
+        L.orc_layout.restype = ctypes.c_int
+        L.orc_n2elec.argtypes = [ctypes.c_int, i32p]
+        L.orc_n2elec.restype = ctypes.c_longlong
+        L.orc_hcore.argtypes = [ctypes.c_int, i32p, f64p, f64p, f64p, ctypes.POINTER(ctypes.c_double)]
+        L.orc_fock2.argtypes = [ctypes.c_int, i32p, i32p, f64p, f64p, f64p, f64p]
+        L.orc_helect.argtypes = [ctypes.c_int, f64p, f64p, f64p]
+        L.orc_helect.restype = ctypes.c_double
+        L.orc_cnvg.argtypes = [ctypes.c_int, f64p, f64p, f64p, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+        L.orc_pdiag.argtypes = [ctypes.c_int, i32p, f64p]
+        L.orc_atheat.argtypes = [ctypes.c_int, i32p]
+        L.orc_atheat.restype = ctypes.c_double
+        L.orc_disp_pm7.argtypes = [ctypes.c_int, i32p, f64p]
+        L.orc_disp_pm7.restype = ctypes.c_double
+        L.orc_param.argtypes = [ctypes.c_int, ctypes.c_char_p]
+        L.orc_param.restype = ctypes.c_double
+        _lib = L
+    return _lib
+
+
+# ---------------------------------------------------------------- packing
+def tri_index(n: int):
+    """(row, col) of packed lower-triangle storage, row-major: i(i-1)/2 + j."""
+    return np.tril_indices(n)
+
+
+def unpack(p: np.ndarray, n: int) -> np.ndarray:
+    a = np.zeros((n, n))
+    r, c = tri_index(n)
+    a[r, c] = p
+    a[c, r] = p
+    return a
+
+
+def pack(a: np.ndarray) -> np.ndarray:
+    r, c = tri_index(a.shape[0])
+    return np.ascontiguousarray(a[r, c])
+
+
+def diag_index(n: int) -> np.ndarray:
+    i = np.arange(1, n + 1)
+    return i * (i + 1) // 2 - 1
+
+
+# ---------------------------------------------------------------- system
+@dataclass
+class System:
+    nat: np.ndarray          # atomic numbers (int32)
+    coord: np.ndarray        # (numat, 3) Angstrom
+    nfirst: np.ndarray = field(default=None)  # 1-based
+    nlast: np.ndarray = field(default=None)
+    norbs: int = 0
+    nclose: int = 0
+    h: np.ndarray = field(default=None)
+    w: np.ndarray = field(default=None)
+    enuclr: float = 0.0
+    atheat: float = 0.0
+    pdiag: np.ndarray = field(default=None)
+
+    @property
+    def numat(self) -> int:
+        return int(self.nat.shape[0])
+
+    @property
+    def mpack(self) -> int:
+        return self.norbs * (self.norbs + 1) // 2
+
+
+def make_system(nat, coord, integrals: bool = True) -> System:
+    L = lib()
+    nat = np.ascontiguousarray(nat, dtype=np.int32)
+    coord = np.ascontiguousarray(coord, dtype=np.float64).reshape(-1, 3)
+    n = nat.shape[0]
+    nfirst = np.zeros(n, np.int32)
+    nlast = np.zeros(n, np.int32)
+    norbs = L.orc_layout(n, nat, nfirst, nlast)
+    if norbs < 0:
+        raise ValueError("oracle supports H, C and O only")
+    tore = {1: 1, 6: 4, 8: 6}
+    nelec = int(sum(tore[int(z)] for z in nat))
+    if nelec % 2:
+        raise ValueError("closed-shell RHF needs an even electron count")
+    s = System(nat=nat, coord=coord, nfirst=nfirst, nlast=nlast, norbs=norbs, nclose=nelec // 2)
+    s.pdiag = np.zeros(norbs)
+    L.orc_pdiag(n, nat, s.pdiag)
+    s.atheat = L.orc_atheat(n, nat)
+    if integrals:
+        hcore(s)
+    return s
+
+
+def hcore(s: System) -> None:
+    L = lib()
+    n2 = L.orc_n2elec(s.numat, s.nat)
+    s.h = np.zeros(s.mpack)
+    s.w = np.zeros(n2)
+    e = ctypes.c_double(0.0)
+    L.orc_hcore(s.numat, s.nat, s.coord.reshape(-1), s.h, s.w, ctypes.byref(e))
+    s.enuclr = e.value
+
+
+def fock2(s: System, f: np.ndarray, ptot: np.ndarray, pa: np.ndarray) -> None:
+    lib().orc_fock2(s.numat, s.nfirst, s.nlast, f, ptot, pa, s.w)
+
+
+def helect(n: int, p, h, f) -> float:
+    return lib().orc_helect(n, p, h, f)
+
+
+def cnvg(norbs: int, pnew, p, p1, niter: int) -> float:
+    pl = ctypes.c_double(0.0)
+    lib().orc_cnvg(norbs, pnew, p, p1, niter, ctypes.byref(pl))
+    return pl.value
+
+
+def disp_correction(s: System) -> float:
+    return lib().orc_disp_pm7(s.numat, s.nat, s.coord.reshape(-1))
+
+
+def eigenvectors_lapack(f: np.ndarray, n: int):
+    """eigenvectors_LAPACK.F90:53-121; perturbs f in place like the reference."""
+    f[diag_index(n)] += np.arange(1, n + 1) * 1.0e-10
+    a = unpack(f, n)
+    w, v = np.linalg.eigh(a, UPLO="U")
+    return np.asfortranarray(v), w
+
+
+def density(c: np.ndarray, nclose: int) -> np.ndarray:
+    co = c[:, :nclose]
+    return pack(2.0 * (co @ co.T))
+
+
+def fmo_block(f: np.ndarray, c: np.ndarray, nocc: int) -> np.ndarray:
+    """diag_for_GPU.F90:101-150: Fmo (nvirt x nocc) = C_v^T F C_o."""
+    n = c.shape[0]
+    F = unpack(f, n)
+    if nocc < n - nocc:
+        return c[:, nocc:].T @ (F @ c[:, :nocc])
+    return (F @ c[:, nocc:]).T @ c[:, :nocc]
+
+
+def rotation_sweep(c: np.ndarray, fmo: np.ndarray, eig: np.ndarray, nocc: int,
+                   bigeps: float = 1.5e-7, tiny: float | None = None) -> int:
+    """diag_for_GPU.F90:151-206 (CPU branch).  Rotates columns of c in place in
+    the reference order (occupied i outer, virtual j inner); returns the count
+    of rotations applied."""
+    n = c.shape[0]
+    if tiny is None:
+        tiny = float(np.max(np.abs(fmo))) * 0.05
+    done = 0
+    for i in range(nocc):
+        for jv in range(n - nocc):
+            x = fmo[jv, i]
+            if abs(x) < tiny:
+                continue
+            a = eig[i]
+            b = eig[nocc + jv]
+            d = a - b
+            if abs(x / d) < bigeps:
+                continue
+            e = np.copysign(np.sqrt(4.0 * x * x + d * d), d)
+            alpha = np.sqrt(0.5 * (1.0 + d / e))
+            beta = -np.copysign(np.sqrt(1.0 - alpha * alpha), x)
+            ci = c[:, i].copy()
+            cj = c[:, nocc + jv].copy()
+            c[:, i] = alpha * ci + beta * cj
+            c[:, nocc + jv] = alpha * cj - beta * ci
+            done += 1
+    return done
+
+
+def pseudo_diag(f, c, nocc, eig):
+    fmo = fmo_block(f, c, nocc)
+    return rotation_sweep(c, fmo, eig, nocc)
+
+
+# ---------------------------------------------------------------- iter
+@dataclass
+class ScfResult:
+    escf: float             # heat of formation from iter, kcal/mol (no post-SCF terms)
+    ee: float               # electronic energy, eV
+    eigs: np.ndarray
+    c: np.ndarray
+    p: np.ndarray
+    niter: int
+    converged: bool
+    history: list
+
+
+def iter_scf(s: System, pseudo: bool = False, scfcrt: float = 1.0e-4, itrmax: int = 2000,
+             gnorm: float = 0.0, trace: bool = False) -> ScfResult:
+    """Closed-shell restatement of iter (SCF/iter.F90), 1SCF settings
+    (last = 1, nscf = 0, fulscf = .true.)."""
+    n = s.norbs
+    mpack = s.mpack
+    nclose = s.nclose
+    h, w = s.h, s.w
+    enrgy = FPC9
+    # -- first-call setup (iter.F90:123-221) --
+    shift = 1.0
+    shfmax = 20.0
+    newdg = False
+    plchek = 0.005
+    pl = 1.0
+    bshift = -80.0
+    ten = bshift
+    tenold = ten
+    shfto = 0.0
+    shftbo = 0.0
+    shiftb = 0.0
+    oknewd = abs(bshift) < 0.001
+    okpuly = False
+    halfe = False
+    camkin = False
+    trans = 0.2
+    na1el = nclose
+    nb1el = nclose
+    ihomo = max(1, nclose)
+    p = np.zeros(mpack)
+    pa = np.zeros(mpack)
+    w1 = na1el / (na1el + 1.0e-6 + nb1el)
+    random = 1.0
+    dix = diag_index(n)
+    for i in range(n):
+        j = dix[i]
+        p[j] = s.pdiag[i]
+        pa[j] = p[j] * w1 * random
+        random = 1.0 / random
+    pold = pa.copy()
+    pold2 = pold[dix].copy()
+    gs = True
+    selcon = scfcrt
+    if gs:
+        selcon = min(min(scfcrt * 100.0, 0.1), max(scfcrt * gnorm ** 3, scfcrt))
+    pltest = 0.05 * np.sqrt(abs(selcon))
+    iredy = 1
+    niter = 0
+    eold = 1.0e2
+    ready = False
+    diff = 0.0
+    scorr = 0.0
+    eigs = np.zeros(n)
+    c = np.zeros((n, n), order="F")
+    history = []
+    ramp = np.arange(1, mpack + 1) * 1.0e-16
+    f = None
+    converged = False
+    while True:  # label 250
+        niter += 1
+        if niter > itrmax:
+            break
+        if abs(shift) > 1.0e-10 and bshift != 0.0:
+            if niter > 1:
+                if newdg and not (halfe or camkin):
+                    if diff > 0.0:
+                        shift = 1.0
+                        if diff > 1:
+                            newdg = False
+                    else:
+                        shift = -0.1
+                else:
+                    if ihomo < n:
+                        shift = ten + eigs[ihomo] - eigs[ihomo - 1] + shift
+                    else:
+                        shift = 0.0
+                if diff > 0.0:
+                    if shift > 4.0:
+                        shfmax = 4.5
+                    if shift > shfmax:
+                        shfmax = max(shfmax - 0.5, 0.0)
+                shift = max(-20.0, min(shfmax, shift))
+                if abs(shift - shfmax) < 1.0e-5:
+                    shfmax = shfmax + 0.01
+                if okpuly or abs(bshift - 4.44) < 1.0e-5:
+                    shift = -8.0
+                    if newdg:
+                        shift = 0.0
+            tenold = ten
+            if pl > plchek:
+                shftbo = shiftb
+                shfto = shift
+            else:
+                shiftb = shftbo
+                shift = shfto
+            eigs[ihomo:] = eigs[ihomo:] + shift
+            f = h + shift * pa + ramp
+            f[dix] = f[dix] - shift
+        else:
+            f = h.copy()
+        while True:  # label 320
+            fock2(s, f, p, pa)
+            ee = helect(n, pa, h, f) * 2.0
+            escf = (ee + s.enuclr) * enrgy + s.atheat + scorr
+            diff = escf - eold
+            if diff > 0:
+                ten = ten - 1.0
+            else:
+                ten = ten * 0.975 + 0.05
+            sellim = max(selcon, 1.0e-15 * max(abs(ee), 1.0))
+            conv = niter > 4 and (pl == 0.0 or (pl < pltest and abs(diff) < sellim)) and ready
+            if conv:
+                if abs(shift) < 1.0e-10:
+                    converged = True
+                    break
+                shift = 0.0
+                shiftb = 0.0
+                f = h.copy()
+                continue
+            break
+        if converged:
+            break
+        ready = iredy > 0 and (abs(diff) < sellim * 10.0 or pl == 0.0)
+        iredy += 1
+        eold = escf
+        if trace:
+            history.append(dict(niter=niter, escf=escf, pl=pl, shift=shift, newdg=newdg))
+        if newdg and pseudo and not (halfe or camkin):
+            pseudo_diag(f, c, na1el, eigs)
+        else:
+            c, eigs = eigenvectors_lapack(f, n)
+        p = density(c, nclose)
+        pl = cnvg(n, p, pold, pold2, niter)
+        pa = p * 0.5
+        oknewd = pl < sellim or oknewd
+        newdg = (pl < trans and oknewd) or newdg
+        if pl < trans * 0.3333:
+            oknewd = True
+    # -- label 600 --
+    ee = helect(n, pa, h, f) * 2.0
+    fcopy = f.copy()
+    c, eigs = eigenvectors_lapack(fcopy, n)
+    escf = (ee + s.enuclr) * enrgy + s.atheat
+    return ScfResult(escf=escf, ee=ee, eigs=eigs, c=c, p=p, niter=niter, converged=converged,
+                     history=history)
+
+
+# ---------------------------------------------------------------- properties
+def mulliken_charges(s: System, p: np.ndarray) -> np.ndarray:
+    """NDDO net charges: core charge minus the diagonal density on the atom."""
+    tore = {1: 1.0, 6: 4.0, 8: 6.0}
+    pd = p[diag_index(s.norbs)]
+    q = np.zeros(s.numat)
+    for a in range(s.numat):
+        q[a] = tore[int(s.nat[a])] - pd[s.nfirst[a] - 1:s.nlast[a]].sum()
+    return q
+
+
+def heat_of_formation(s: System, res: ScfResult) -> float:
+    """Final heat = iter's escf + the PM7 post-SCF dispersion term (compfg)."""
+    return res.escf + disp_correction(s)

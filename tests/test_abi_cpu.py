@@ -1,0 +1,66 @@
+"""CPU checks of the C ABI: the library builds for sm_100a, loads, and exports
+every function include/mopac_b200.h declares.  No compute is called."""
+import ctypes
+import os
+import re
+import subprocess
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared_functions():
+    txt = open(os.path.join(ROOT, "include", "mopac_b200.h")).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    names = re.findall(r"^\s*(?:const\s+)?(?:void|int|double|size_t|long long|char\s*\*|const char\s*\*)\s*\**\s*(\w+)\s*\(",
+                       txt, flags=re.M)
+    return sorted(set(names))
+
+
+@pytest.fixture(scope="module")
+def libpath():
+    from mopac_gpu_b200 import build
+    return build.build()
+
+
+def test_header_declares_reference_symbols():
+    names = _declared_functions()
+    for ref in ["call_gemm_cublas", "call_syrk_cublas", "call_gemm_cublas_2gpu", "call_syrk_cublas_2gpu",
+                "mopac_cuda_dsyevd", "call_rot_cuda_gpu", "call_rot_cuda_2gpu_gpu", "getGPUInfo", "setDevice",
+                "set_mozyme_gpu_pair", "create_handle", "destroy_handle", "mopac_cuda_destroy_resources",
+                "fock2_", "helect_", "cnvg_", "density_for_gpu_", "eigenvectors_lapack_", "diag_for_gpu_",
+                "mb_scf_run", "mb_ctx_create", "mb_fock2_dev", "mb_eigh_packed_dev"]:
+        assert ref in names, ref
+
+
+def test_library_exports_every_declared_symbol(libpath):
+    names = _declared_functions()
+    out = subprocess.run(["nm", "-D", "--defined-only", libpath], capture_output=True, text=True).stdout
+    exported = {l.split()[-1] for l in out.splitlines() if l.strip()}
+    missing = [n for n in names if n not in exported]
+    assert not missing, missing
+
+
+def test_library_loads_and_reports_version(libpath):
+    L = ctypes.CDLL(libpath)
+    L.mb_version.restype = ctypes.c_int
+    assert L.mb_version() >= 100
+
+
+def test_python_loader_binds_all_signatures(libpath):
+    from mopac_gpu_b200 import _lib
+    L = _lib.lib()
+    for name in _lib.SIGNATURES:
+        assert getattr(L, name) is not None
+
+
+def test_bad_arguments_fail_loudly_without_gpu_work(libpath):
+    from mopac_gpu_b200 import _lib
+    L = _lib.lib()
+    h = ctypes.c_void_p()
+    import numpy as np
+    nat = np.array([9], np.int32)  # fluorine: outside this build
+    rc = L.mb_ctx_create(1, nat.ctypes.data, None, ctypes.byref(h))
+    assert rc == 5
+    assert b"element" in L.mb_last_error()

@@ -1,0 +1,187 @@
+"""Kernel-level parity on the GPU against the CPU oracle (same inputs).
+
+Bit-exact where the kernel keeps the reference's operation order (Fock build,
+cnvg, rotation sweep); tolerance-based for reductions and the eigensolver.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+from oracle import scf_oracle as so
+from tests.helpers import mixed_density, oracle_system, small_systems
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+SYSTEMS = small_systems()
+
+
+def _dev(a):
+    return torch.as_tensor(np.ascontiguousarray(a), dtype=torch.float64, device="cuda")
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _need_gpu():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from mopac_gpu_b200 import build
+    build.build()
+
+
+@pytest.mark.parametrize("name", sorted(SYSTEMS))
+@pytest.mark.parametrize("use_shift", [False, True])
+def test_fock2_bit_identical(name, use_shift):
+    from mopac_gpu_b200 import kernels as K
+    s = oracle_system(*SYSTEMS[name])
+    p = mixed_density(s)
+    pa = p * 0.5
+    shift = -20.0 if use_shift else 0.0
+    if use_shift:
+        f = s.h + shift * pa + np.arange(1, s.mpack + 1) * 1.0e-16
+        f[so.diag_index(s.norbs)] -= shift
+    else:
+        f = s.h.copy()
+    so.fock2(s, f, p, pa)
+    at = K.Atoms(s.nfirst, s.nlast)
+    fd = torch.empty(s.mpack, dtype=torch.float64, device="cuda")
+    K.fock2(at, fd, _dev(s.h), _dev(p), _dev(pa), _dev(s.w), shift, use_shift)
+    got = fd.cpu().numpy()
+    assert np.array_equal(got, f), np.abs(got - f).max()
+
+
+def test_cnvg_bit_identical():
+    from mopac_gpu_b200 import kernels as K
+    rng = np.random.default_rng(3)
+    n = 257
+    mp = n * (n + 1) // 2
+    for niter in (2, 3, 4, 6, 9):
+        pnew = rng.uniform(0, 1, mp)
+        p = pnew + rng.normal(scale=0.02, size=mp)
+        p1 = p[so.diag_index(n)] + rng.normal(scale=0.01, size=n)
+        a, b, c = pnew.copy(), p.copy(), p1.copy()
+        pl_ref = so.cnvg(n, a, b, c, niter)
+        da, db, dc = _dev(pnew), _dev(p), _dev(p1)
+        pl = K.cnvg(n, da, db, dc, niter)
+        assert pl == pl_ref
+        assert np.array_equal(da.cpu().numpy(), a)
+        assert np.array_equal(db.cpu().numpy(), b)
+        assert np.array_equal(dc.cpu().numpy(), c)
+
+
+@pytest.mark.parametrize("name", ["water16", "propane"])
+def test_helect_matches(name):
+    from mopac_gpu_b200 import kernels as K
+    s = oracle_system(*SYSTEMS[name])
+    p = mixed_density(s)
+    f = s.h.copy()
+    so.fock2(s, f, p, p * 0.5)
+    ref = so.helect(s.norbs, p * 0.5, s.h, f)
+    got = K.helect(s.norbs, _dev(p * 0.5), _dev(s.h), _dev(f))
+    assert abs(got - ref) <= 1e-12 * abs(ref)
+
+
+@pytest.mark.parametrize("n,k", [(96, 64), (200, 37), (513, 300)])
+def test_density_fp64(n, k):
+    from mopac_gpu_b200 import kernels as K
+    rng = np.random.default_rng(n)
+    c = np.asfortranarray(rng.normal(size=(n, n)) / np.sqrt(n))
+    ref = so.density(c, k)
+    got = K.density(torch.as_tensor(np.ascontiguousarray(c.T), device="cuda").t(), k).cpu().numpy()
+    np.testing.assert_allclose(got, ref, atol=1e-13, rtol=1e-12)
+
+
+@pytest.mark.parametrize("m,n,k,ta,tb", [(70, 50, 33, "N", "N"), (64, 64, 64, "T", "N"), (129, 17, 200, "N", "T"),
+                                         (31, 77, 45, "T", "T")])
+def test_dgemm(m, n, k, ta, tb):
+    from mopac_gpu_b200 import kernels as K
+    rng = np.random.default_rng(m + n)
+    A = rng.normal(size=(k, m) if ta == "T" else (m, k))
+    B = rng.normal(size=(n, k) if tb == "T" else (k, n))
+    C = rng.normal(size=(m, n))
+    opA = A.T if ta == "T" else A
+    opB = B.T if tb == "T" else B
+    ref = 0.7 * opA @ opB - 0.3 * C
+    dA = _dev(np.asfortranarray(A).ravel(order="F"))
+    dB = _dev(np.asfortranarray(B).ravel(order="F"))
+    dC = _dev(np.asfortranarray(C).ravel(order="F"))
+    K.dgemm(ta, tb, m, n, k, 0.7, dA, A.shape[0], dB, B.shape[0], -0.3, dC, m)
+    got = dC.cpu().numpy().reshape(n, m).T
+    np.testing.assert_allclose(got, ref, atol=1e-12, rtol=1e-12)
+
+
+@pytest.mark.parametrize("n", [1, 2, 5, 12, 96, 331, 700])
+def test_eigh_packed(n):
+    from mopac_gpu_b200 import kernels as K
+    rng = np.random.default_rng(n)
+    a = rng.normal(size=(n, n))
+    a = (a + a.T) * 5.0
+    if n >= 12:  # exact degeneracies, as in symmetric molecules
+        a[:4, :] = 0.0
+        a[:, :4] = 0.0
+        a[0, 0] = a[1, 1] = 3.0
+        a[2, 2] = a[3, 3] = -7.0
+    fp = so.pack(a)
+    ref_f = fp.copy()
+    cref, wref = so.eigenvectors_lapack(ref_f, n)
+    dfp = _dev(fp)
+    c, w = K.eigh_packed(dfp)
+    w = w.cpu().numpy()
+    c = c.cpu().numpy()
+    assert np.array_equal(dfp.cpu().numpy(), ref_f)  # same in-place perturbation
+    np.testing.assert_allclose(w, wref, atol=1e-10 * max(1, np.abs(wref).max()))
+    apert = so.unpack(ref_f, n)
+    resid = np.abs(apert @ c - c * w).max()
+    assert resid < 1e-9 * max(1, np.abs(wref).max())
+    assert np.abs(c.T @ c - np.eye(n)).max() < 1e-10
+
+
+def test_rotation_sweep_bit_identical_through_reference_symbol():
+    """call_rot_cuda_gpu (reference signature) vs the oracle's sequential sweep."""
+    from mopac_gpu_b200._lib import lib
+    rng = np.random.default_rng(11)
+    n, nocc = 150, 53
+    nv = n - nocc
+    c = np.asfortranarray(np.linalg.qr(rng.normal(size=(n, n)))[0])
+    eig = np.sort(rng.normal(size=n) * 10)
+    fmo = np.asfortranarray(rng.normal(size=(nv, nocc)) * 0.1)
+    fmo[np.abs(fmo) < 0.08] *= 1e-3  # a mix of skipped and applied rotations
+    tiny = float(np.abs(fmo).max() * 0.05)
+    ref = c.copy(order="F")
+    nrot = so.rotation_sweep(ref, fmo, eig, nocc, tiny=tiny)
+    got = c.copy(order="F")
+    lib().call_rot_cuda_gpu(fmo.ctypes.data, eig.ctypes.data, got.ctypes.data, None, None, nocc, nocc + 1, n,
+                            1.5e-7, tiny)
+    assert nrot > 100
+    assert np.array_equal(got, ref), np.abs(got - ref).max()
+
+
+def test_pseudo_diag_matches_oracle():
+    from mopac_gpu_b200 import kernels as K
+    s = oracle_system(*SYSTEMS["water16"])
+    r = so.iter_scf(s, itrmax=6)
+    f = s.h.copy()
+    so.fock2(s, f, r.p, r.p * 0.5)
+    c0, e0 = so.eigenvectors_lapack(f.copy(), s.norbs)
+    # perturb F a little so the sweep has work
+    f2 = f + np.random.default_rng(1).normal(scale=1e-3, size=f.shape)
+    ref = c0.copy(order="F")
+    nref = so.pseudo_diag(f2, ref, s.nclose, e0)
+    cT = torch.as_tensor(np.ascontiguousarray(c0.T), device="cuda")
+    nrot = K.pseudo_diag(_dev(f2), cT, _dev(e0), s.nclose)
+    got = cT.cpu().numpy().T
+    assert nrot == nref
+    np.testing.assert_allclose(got, ref, atol=1e-12)
+
+
+@pytest.mark.parametrize("name", sorted(SYSTEMS))
+def test_gpu_hcore_matches_oracle(name):
+    from mopac_gpu_b200 import ScfContext
+    nat, xyz = SYSTEMS[name]
+    s = oracle_system(nat, xyz)
+    ctx = ScfContext(nat, xyz)
+    ctx.hcore()
+    h, w, en = ctx.get_hw()
+    np.testing.assert_allclose(h, s.h, rtol=1e-12, atol=1e-12)
+    np.testing.assert_allclose(w, s.w, rtol=1e-12, atol=1e-12)
+    assert abs(en - s.enuclr) < 1e-9 * abs(s.enuclr)
