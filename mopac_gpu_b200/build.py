@@ -5,6 +5,7 @@ Usage: python -m mopac_gpu_b200.build [--force] [--verbose]
 from __future__ import annotations
 
 import concurrent.futures as cf
+import hashlib
 import os
 import subprocess
 import sys
@@ -39,8 +40,6 @@ def _headers_mtime():
 def _compile(src, force, verbose):
     obj = os.path.join(BUILD, src.replace(".cu", ".o"))
     srcp = os.path.join(CSRC, src)
-    if not force and os.path.exists(obj) and os.path.getmtime(obj) >= max(os.path.getmtime(srcp), _headers_mtime()):
-        return obj
     cmd = [NVCC, *ARCH, *COMMON, "-c", srcp, "-o", obj]
     if src in NO_FMA:
         cmd.insert(1, "-fmad=false")
@@ -55,8 +54,26 @@ def _compile(src, force, verbose):
     return obj
 
 
+def _stamp() -> str:
+    """Content hash of every source and header plus the flags."""
+    h = hashlib.sha256()
+    for d in (CSRC, os.path.join(ROOT, "include")):
+        for f in sorted(os.listdir(d)):
+            if f.endswith((".cu", ".cuh", ".h")):
+                h.update(f.encode())
+                h.update(open(os.path.join(d, f), "rb").read())
+    h.update(" ".join(ARCH + COMMON + sorted(NO_FMA)).encode())
+    return h.hexdigest()
+
+
 def build(force: bool = False, verbose: bool = False) -> str:
+    """Compile when the sources changed (content hash), else reuse the in-tree
+    library -- a prebuilt library is never rebuilt on a GPU host."""
     os.makedirs(BUILD, exist_ok=True)
+    stamp_file = os.path.join(BUILD, "stamp")
+    stamp = _stamp()
+    if not force and os.path.exists(LIB) and os.path.exists(stamp_file) and open(stamp_file).read() == stamp:
+        return LIB
     srcs = sources()
     with cf.ThreadPoolExecutor(max_workers=min(8, len(srcs))) as ex:
         objs = list(ex.map(lambda s: _compile(s, force, verbose), srcs))
@@ -65,6 +82,8 @@ def build(force: bool = False, verbose: bool = False) -> str:
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
+    with open(stamp_file, "w") as fh:
+        fh.write(stamp)
     return LIB
 
 

@@ -28,6 +28,7 @@ namespace {
 
 constexpr int NB = 32;         // panel width
 constexpr int TPB = 256;       // threads per CTA in the panel kernel
+constexpr int TCH = 16;        // row chunks per dot product in t1/t2
 
 struct PanelArgs {
   int n, k, ib, lda;
@@ -40,7 +41,8 @@ struct PanelArgs {
   double* tau;
   double* part;    // gridDim partial norms (column j)
   double* partd;   // gridDim partial dots (w.v)
-  double* tvec;    // 2*NB: t1 = W^T v, t2 = V^T v
+  double* tvec;    // unused
+  double* tpart;   // 2*NB*TCH chunk partials of t1 = W^T v, t2 = V^T v
   double* wvec;    // n
 };
 
@@ -58,10 +60,36 @@ __device__ double block_sum(double v, double* sh) {
   return r;  // valid in thread 0
 }
 
+// Sum of the gridDim.x per-CTA partials, computed by warp 0 of each CTA and
+// broadcast to the whole CTA (one load per lane per 32 partials).
+__device__ double grid_partials_sum(const double* part, double* sh_out) {
+  if (threadIdx.x < 32) {
+    double s = 0.0;
+    for (int b = threadIdx.x; b < (int)gridDim.x; b += 32) s += part[b];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if (threadIdx.x == 0) *sh_out = s;
+  }
+  __syncthreads();
+  const double r = *sh_out;
+  __syncthreads();
+  return r;
+}
+
 __global__ void __launch_bounds__(TPB) tridiag_panel(PanelArgs p) {
+  // Two grid barriers per column.  For column j = k + i:
+  //   phase A  finish W(:, i-1) for the CTA's rows (w = tau (p - corr) + alpha v,
+  //            with w.v = tau (p.v - 2 t1.t2) so no extra reduction is needed),
+  //            update column j with the panel's earlier reflectors, partial
+  //            norm of A(j+2:n, j).                                   -> barrier
+  //   phase D  reflector, v, p = A22 v (one warp per row), partial p.v and the
+  //            chunked t1 = W^T v, t2 = V^T v.                        -> barrier
   cg::grid_group grid = cg::this_grid();
   __shared__ double sh[32];
   __shared__ double s_scal[4];
+  __shared__ double s_sum;
+  __shared__ double s_vj[NB], s_wj[NB], s_t1[NB], s_t2[NB];
+  __shared__ double s_pv[TPB / 32];
   const int n = p.n, lda = p.lda;
   const long long gtid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long gstride = (long long)gridDim.x * blockDim.x;
@@ -71,53 +99,102 @@ __global__ void __launch_bounds__(TPB) tridiag_panel(PanelArgs p) {
 #define VP(r, c) p.vp[(long long)(c) * n + (r)]
 #define WP(r, c) p.wp[(long long)(c) * n + (r)]
   double prev_tau = 0.0;
-  for (int i = 0; i < p.ib; ++i) {
+  for (int i = 0; i <= p.ib; ++i) {
     const int j = p.k + i;
-    // ---- phase A: finish W(:, i-1), update column j, partial norm
+    // ---------------- phase A
     double alpha_prev = 0.0;
     if (i > 0) {
-      double s = 0.0;
-      for (int b = 0; b < (int)gridDim.x; ++b) s += p.partd[b];
-      alpha_prev = -0.5 * prev_tau * s;
-    }
-    double wj[NB], vj[NB];
-    for (int l = 0; l < i; ++l) {
-      vj[l] = VP(j, l);
-      wj[l] = (l == i - 1) ? p.wvec[j] + alpha_prev * VP(j, l) : WP(j, l);
-    }
-    double sig = 0.0;
-    for (long long r = gtid; r < n; r += gstride) {
-      if (i > 0) {
-        double wr_last = (r >= j) ? p.wvec[r] + alpha_prev * VP(r, i - 1) : 0.0;
-        if (r >= j) WP(r, i - 1) = wr_last;
-        if (r >= j) {
-          double acc = AE(r, j);
-          for (int l = 0; l < i; ++l) {
-            double wrl = (l == i - 1) ? wr_last : WP(r, l);
-            acc -= VP(r, l) * wj[l] + wrl * vj[l];
-          }
-          AE(r, j) = acc;
-        }
+      const int il = i - 1;  // the column whose W is finished here
+      if (threadIdx.x < (unsigned)(2 * il)) {
+        const int dotq = threadIdx.x, l = dotq >> 1;
+        double t = 0.0;
+        for (int ch = 0; ch < TCH; ++ch) t += p.tpart[dotq * TCH + ch];
+        if ((dotq & 1) == 0) s_t1[l] = t; else s_t2[l] = t;
       }
-      if (r == j) p.d[j] = AE(j, j);
-      if (r >= j + 2) {
-        double x = AE(r, j);
-        sig += x * x;
+      const double pv = grid_partials_sum(p.partd, &s_sum);  // also syncs s_t1/s_t2
+      double tt = 0.0;
+      for (int l = 0; l < il; ++l) tt += s_t1[l] * s_t2[l];
+      const double dot = prev_tau * (pv - 2.0 * tt);
+      alpha_prev = -0.5 * prev_tau * dot;
+      if (i == p.ib) {
+        // last column of the panel: finish W(:, il) and leave
+        for (long long r = gtid; r < n; r += gstride) {
+          if (r < j) continue;
+          double corr = 0.0;
+          for (int l = 0; l < il; ++l) corr += VP(r, l) * s_t1[l] + WP(r, l) * s_t2[l];
+          WP(r, il) = prev_tau * (p.wvec[r] - corr) + alpha_prev * VP(r, il);
+        }
+        break;
+      }
+      if (threadIdx.x == 0) {  // row j of W(:, il), needed by every CTA below
+        double corr = 0.0;
+        for (int l = 0; l < il; ++l) corr += VP(j, l) * s_t1[l] + WP(j, l) * s_t2[l];
+        s_wj[il] = prev_tau * (p.wvec[j] - corr) + alpha_prev * VP(j, il);
+      }
+    }
+    if (threadIdx.x < (unsigned)i) {
+      const int l = threadIdx.x;
+      s_vj[l] = VP(j, l);
+      if (l < i - 1) s_wj[l] = WP(j, l);
+    }
+    __syncthreads();
+    // Rows r >= j, eight lanes per row: lane q handles reflectors l = q, q+8, ...
+    // (independent loads), partial sums are combined with shuffles.  The group
+    // finishes W(r, i-1) and updates A(r, j); lane 0 accumulates the norm.
+    double sig = 0.0;
+    {
+      const int q = lane & 7;
+      const long long gstep = gstride >> 3;         // 8-lane groups in the grid
+      const long long gw0 = (gtid >> 5) << 2;       // first group of this warp
+      const int il = i - 1;
+      // the loop is warp-uniform (shuffles need every lane); each group checks
+      // its own row
+      for (long long base = j + gw0; base < n; base += gstep) {
+        const long long r = base + (lane >> 3);
+        const bool act = r < n;
+        if (i > 0) {
+          double corr = 0.0;
+          if (act)
+            for (int l = q; l < il; l += 8) corr += VP(r, l) * s_t1[l] + WP(r, l) * s_t2[l];
+          corr += __shfl_xor_sync(0xffffffffu, corr, 4);
+          corr += __shfl_xor_sync(0xffffffffu, corr, 2);
+          corr += __shfl_xor_sync(0xffffffffu, corr, 1);
+          const double wr_il = act ? prev_tau * (p.wvec[r] - corr) + alpha_prev * VP(r, il) : 0.0;
+          double upd = 0.0;
+          if (act)
+            for (int l = q; l < i; l += 8) {
+              const double wrl = (l == il) ? wr_il : WP(r, l);
+              upd += VP(r, l) * s_wj[l] + wrl * s_vj[l];
+            }
+          upd += __shfl_xor_sync(0xffffffffu, upd, 4);
+          upd += __shfl_xor_sync(0xffffffffu, upd, 2);
+          upd += __shfl_xor_sync(0xffffffffu, upd, 1);
+          if (act && q == 0) {
+            WP(r, il) = wr_il;
+            AE(r, j) = AE(r, j) - upd;
+          }
+        }
+        if (act && q == 0) {
+          if (r == j) p.d[j] = AE(j, j);
+          if (r >= j + 2) {
+            const double x = AE(r, j);
+            sig += x * x;
+          }
+        }
       }
     }
     double bs = block_sum(sig, sh);
     if (threadIdx.x == 0) p.part[blockIdx.x] = bs;
     grid.sync();
-    // ---- phase D: reflector, v, symmetric product p = A22 v, t1/t2
+    // ---------------- phase D
+    const double snorm = grid_partials_sum(p.part, &s_sum);
     if (threadIdx.x == 0) {
-      double s = 0.0;
-      for (int b = 0; b < (int)gridDim.x; ++b) s += p.part[b];
-      double alpha = AE(j + 1, j);
+      const double alpha = AE(j + 1, j);
       double beta, tau, scal;
-      if (s == 0.0) {
+      if (snorm == 0.0) {
         beta = alpha; tau = 0.0; scal = 0.0;
       } else {
-        beta = -copysign(sqrt(alpha * alpha + s), alpha);
+        beta = -copysign(sqrt(alpha * alpha + snorm), alpha);
         tau = (beta - alpha) / beta;
         scal = 1.0 / (alpha - beta);
       }
@@ -132,61 +209,78 @@ __global__ void __launch_bounds__(TPB) tridiag_panel(PanelArgs p) {
       p.tau[j] = tau;
     }
     for (long long r = gtid; r < n; r += gstride) {
-      double v = (r == j + 1) ? 1.0 : (r > j + 1 ? AE(r, j) * scal : 0.0);
+      const double v = (r == j + 1) ? 1.0 : (r > j + 1 ? AE(r, j) * scal : 0.0);
       VP(r, i) = v;
       p.vall[(long long)j * n + r] = v;
     }
-    // p(r) = sum_{c > j} A(c, r) v(c), one warp per row r > j
-    for (int r = j + 1 + gwarp; r < n; r += nwarps) {
-      double acc = 0.0;
-      for (int c = j + 1 + lane; c < n; c += 32) {
-        double v = (c == j + 1) ? 1.0 : AE(c, j) * scal;
-        acc += AE(c, r) * v;
-      }
+    // p(r) = sum_{c > j} A(c, r) v(c), one warp per row r > j, eight loads in
+    // flight per lane; the warp also accumulates p(r) v(r) for p.v.
+    double pvw = 0.0;
+    {
+      const double* colj = A + (long long)j * lda;
+      for (int r = j + 1 + gwarp; r < n; r += nwarps) {
+        const double* colr = A + (long long)r * lda;
+        double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0, acc3 = 0.0;
+        int c = j + 1 + lane;
+        for (; c + 224 < n; c += 256) {
+          double x[8], y[8];
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
-      if (lane == 0) p.wvec[r] = acc;
-    }
-    // t1[l] = sum_r W(r,l) v(r), t2[l] = sum_r V(r,l) v(r) over r > j; warp 0..2i-1
-    for (int q = gwarp; q < 2 * i; q += nwarps) {
-      const int l = q >> 1;
-      const bool isw = (q & 1) == 0;
-      double acc = 0.0;
-      for (int r = j + 1 + lane; r < n; r += 32) {
-        double v = (r == j + 1) ? 1.0 : AE(r, j) * scal;
-        acc += (isw ? WP(r, l) : VP(r, l)) * v;
-      }
+          for (int u = 0; u < 8; ++u) x[u] = __ldcs(colr + c + 32 * u);
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
-      if (lane == 0) p.tvec[(isw ? 0 : NB) + l] = acc;
-    }
-    grid.sync();
-    // ---- phase E: corrections, w = tau (p - corr), partial w.v
-    double dot = 0.0;
-    for (long long r = gtid; r < n; r += gstride) {
-      if (r <= j) {
-        p.wvec[r] = 0.0;
-        continue;
+          for (int u = 0; u < 8; ++u) y[u] = colj[c + 32 * u];
+#pragma unroll
+          for (int u = 0; u < 8; ++u) {
+            const double v = (c + 32 * u == j + 1) ? 1.0 : y[u] * scal;
+            if ((u & 3) == 0) acc0 += x[u] * v;
+            else if ((u & 3) == 1) acc1 += x[u] * v;
+            else if ((u & 3) == 2) acc2 += x[u] * v;
+            else acc3 += x[u] * v;
+          }
+        }
+        for (; c < n; c += 32) {
+          const double v = (c == j + 1) ? 1.0 : colj[c] * scal;
+          acc0 += colr[c] * v;
+        }
+        double acc = (acc0 + acc1) + (acc2 + acc3);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+        if (lane == 0) {
+          p.wvec[r] = acc;
+          const double vr = (r == j + 1) ? 1.0 : colj[r] * scal;
+          pvw += acc * vr;
+        }
       }
-      double corr = 0.0;
-      for (int l = 0; l < i; ++l) corr += VP(r, l) * p.tvec[l] + WP(r, l) * p.tvec[NB + l];
-      double w = tau * (p.wvec[r] - corr);
-      p.wvec[r] = w;
-      dot += w * VP(r, i);
+      for (int r = gtid; r <= j && r < n; r += (int)gstride) p.wvec[r] = 0.0;
     }
-    bs = block_sum(dot, sh);
-    if (threadIdx.x == 0) p.partd[blockIdx.x] = bs;
+    if (lane == 0) s_pv[threadIdx.x >> 5] = pvw;
+    // t1/t2 chunk partials (TCH row chunks per dot product)
+    {
+      const int rows = n - (j + 1);
+      const int chunk = (rows + TCH - 1) / TCH;
+      for (int q = nwarps - 1 - gwarp; q < 2 * i * TCH; q += nwarps) {
+        const int dotq = q / TCH, ch = q % TCH;
+        const int l = dotq >> 1;
+        const bool isw = (dotq & 1) == 0;
+        const double* col = isw ? p.wp + (long long)l * n : p.vp + (long long)l * n;
+        const int rb = j + 1 + ch * chunk, re = min(n, rb + chunk);
+        double acc = 0.0;
+        for (int r = rb + lane; r < re; r += 32) {
+          const double v = (r == j + 1) ? 1.0 : AE(r, j) * scal;
+          acc += col[r] * v;
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+        if (lane == 0) p.tpart[q] = acc;
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += s_pv[w];
+      p.partd[blockIdx.x] = t;
+    }
     prev_tau = tau;
     grid.sync();
-  }
-  // finish W(:, ib-1)
-  {
-    double s = 0.0;
-    for (int b = 0; b < (int)gridDim.x; ++b) s += p.partd[b];
-    const double alpha_prev = -0.5 * prev_tau * s;
-    const int last = p.ib - 1;
-    for (long long r = gtid; r < n; r += gstride)
-      WP(r, last) = p.wvec[r] + alpha_prev * VP(r, last);
   }
 #undef AE
 #undef VP
@@ -244,20 +338,35 @@ __global__ void tri_bounds(int n, const double* d, const double* e, double* e2, 
   }
 }
 
+// One warp per eigenvalue: each pass the 32 lanes evaluate Sturm counts at 32
+// interior points of the bracket, shrinking it 33-fold (about a dozen passes
+// instead of ~60 bisection steps, with 32x the parallelism).
 __global__ void bisect_kernel(int n, const double* __restrict__ d, const double* __restrict__ e2,
                               const double* __restrict__ bnd, double* __restrict__ w) {
-  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  const int m = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
   if (m >= n) return;
   double lo = bnd[0], hi = bnd[1];
   const double pivmin = bnd[2];
   const double eps = 2.220446049250313e-16;
-  for (int it = 0; it < 200; ++it) {
-    double mid = 0.5 * (lo + hi);
-    if (hi - lo <= 2.0 * eps * fmax(fabs(lo), fabs(hi)) + pivmin || mid <= lo || mid >= hi) break;
-    int c = sturm_count(n, d, e2, mid, pivmin);
-    if (c > m) hi = mid; else lo = mid;
+  for (int it = 0; it < 64; ++it) {
+    if (hi - lo <= 2.0 * eps * fmax(fabs(lo), fabs(hi)) + pivmin) break;
+    const double x = lo + (hi - lo) * ((double)(lane + 1) / 33.0);
+    const int cnt = sturm_count(n, d, e2, x, pivmin);
+    const unsigned above = __ballot_sync(0xffffffffu, cnt > m);  // lanes whose point lies above eigenvalue m
+    double nlo = lo, nhi = hi;
+    if (above == 0u) {
+      nlo = __shfl_sync(0xffffffffu, x, 31);
+    } else {
+      const int first = __ffs(above) - 1;
+      nhi = __shfl_sync(0xffffffffu, x, first);
+      if (first > 0) nlo = __shfl_sync(0xffffffffu, x, first - 1);
+    }
+    if (!(nlo > lo) && !(nhi < hi)) break;  // no representable progress
+    lo = nlo;
+    hi = nhi;
   }
-  w[m] = 0.5 * (lo + hi);
+  if (lane == 0) w[m] = 0.5 * (lo + hi);
 }
 
 // --------------------------------------------------------- inverse iteration
@@ -369,7 +478,8 @@ __global__ void inverse_iteration(int n, const double* __restrict__ d, const dou
       x[(long long)i * ld] = ((double)(s >> 11) * (1.0 / 9007199254740992.0)) - 0.5;
     }
     normalise(n, x, ld);
-    for (int it = 0; it < 4; ++it) {
+    const int nits = (m1 - m0 > 1) ? 4 : 2;
+    for (int it = 0; it < nits; ++it) {
       tri_solve(n, d, e, lam, tiny, u0, u1, u2, x, ld);
       // re-orthogonalise against earlier members of the cluster (MGS)
       for (int q = m0; q < m; ++q) {
@@ -402,32 +512,36 @@ __global__ void transpose_kernel(int n, const double* __restrict__ X, double* __
   }
 }
 
-// T factor of a panel (dlarft, forward columnwise): T(i,i) = tau_i,
-// T(0:i, i) = -tau_i T(0:i, 0:i) S(0:i, i) with S = V^T V.
+// T factor of a block of reflectors (dlarft, forward columnwise):
+// T(i,i) = tau_i, T(0:i, i) = -tau_i T(0:i, 0:i) S(0:i, i) with S = V^T V.
+// S and T both live in (dynamic) shared memory.
+constexpr int BT = 64;  // reflectors per back-transformation block
+constexpr size_t LARFT_SMEM = sizeof(double) * 2 * BT * (BT + 1);
+
 __global__ void larft_kernel(int ib, const double* __restrict__ S, const double* __restrict__ tau,
                              double* __restrict__ T) {
-  __shared__ double st[NB][NB + 1];
-  __shared__ double sv[NB][NB + 1];
+  extern __shared__ double larft_sh[];
+  double(*st)[BT + 1] = reinterpret_cast<double(*)[BT + 1]>(larft_sh);
+  double(*ss)[BT + 1] = reinterpret_cast<double(*)[BT + 1]>(larft_sh + BT * (BT + 1));
   for (int q = threadIdx.x; q < ib * ib; q += blockDim.x) {
-    int r = q % ib, c = q / ib;
-    sv[r][c] = S[c * ib + r];
+    const int r = q % ib, c = q / ib;
+    ss[r][c] = S[(long long)c * ib + r];
     st[r][c] = 0.0;
   }
   __syncthreads();
   for (int i = 0; i < ib; ++i) {
-    const double ti = tau[i];
     if (threadIdx.x < (unsigned)i) {
       const int r = threadIdx.x;
       double acc = 0.0;
-      for (int c = r; c < i; ++c) acc += st[r][c] * sv[c][i];
-      st[r][i] = -ti * acc;
+      for (int c = r; c < i; ++c) acc += st[r][c] * ss[c][i];
+      st[r][i] = -tau[i] * acc;
     }
-    if (threadIdx.x == 0) st[i][i] = ti;
+    if (threadIdx.x == 0) st[i][i] = tau[i];
     __syncthreads();
   }
   for (int q = threadIdx.x; q < ib * ib; q += blockDim.x) {
-    int r = q % ib, c = q / ib;
-    T[c * ib + r] = st[r][c];
+    const int r = q % ib, c = q / ib;
+    T[(long long)c * ib + r] = st[r][c];
   }
 }
 
@@ -435,13 +549,17 @@ __global__ void larft_kernel(int ib, const double* __restrict__ S, const double*
 
 extern "C" int mb_unpack_dev(int n, const double* pk, double* a, int lda, int perturb, double* pk_mut,
                              cudaStream_t stream);
+extern "C" int mb_dgemm_ws(char transa, char transb, int m, int n, int k, double alpha, const double* a, int lda,
+                           const double* b, int ldb, double beta, double* c, int ldc, double* ws, size_t ws_elems,
+                           cudaStream_t stream);
 
 // Workspace: A n*n | V n*n | Z n*n | X n*n | U0,U1,U2 3*n*n | vp,wp 2*n*NB |
 // d,e,e2,tau,wvec 5n | small scratch
 extern "C" size_t mb_eigh_ws_bytes(int n) {
   size_t nn = (size_t)n * n;
-  return sizeof(double) * (7 * nn + 2 * (size_t)n * NB + 5 * (size_t)n + 2 * NB + 4096 + NB * NB * 2 +
-                           (size_t)NB * n) + 256;
+  return sizeof(double) * (7 * nn + 3 * (size_t)n * NB + 5 * (size_t)n + 2 * NB + 2 * NB * TCH + 4096 +
+                           (size_t)BT * BT * 2 +
+                           (size_t)BT * n) + 256;
 }
 
 extern "C" int mb_eigh_ws(int n, double* fpacked, int perturb, double* c, double* eigs, void* ws, int* status_dev,
@@ -455,18 +573,20 @@ extern "C" int mb_eigh_ws(int n, double* fpacked, int perturb, double* c, double
   double* U0 = b; b += nn;
   double* U1 = b; b += nn;
   double* U2 = b; b += nn;
-  double* vp = b; b += (size_t)n * NB;
-  double* wp = b; b += (size_t)n * NB;
+  double* vwv = b; b += (size_t)n * 3 * NB;  // [V | W | V] panel columns
+  double* vp = vwv;
+  double* wp = vwv + (size_t)n * NB;
   double* d = b; b += n;
   double* e = b; b += n;
   double* e2 = b; b += n;
   double* tau = b; b += n;
   double* wvec = b; b += n;
   double* tvec = b; b += 2 * NB;
+  double* tpart = b; b += 2 * NB * TCH;
   double* part = b; b += 4096;
-  double* S = b; b += NB * NB;
-  double* Tm = b; b += NB * NB;
-  double* Y = b; b += (size_t)NB * n;
+  double* S = b; b += (size_t)BT * BT;
+  double* Tm = b; b += (size_t)BT * BT;
+  double* Y = b; b += (size_t)BT * n;
   double* bnd = part + 2048;
 
   if (n == 1) {
@@ -487,7 +607,7 @@ extern "C" int mb_eigh_ws(int n, double* fpacked, int perturb, double* c, double
     MB_CUDA(cudaGetDevice(&dev));
     MB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     MB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, tridiag_panel, TPB, 0));
-    if (per > 2) per = 2;
+    if (per > 4) per = 4;
     if (per < 1) return mb_set_error(MB_ERR_CUDA, "tridiag_panel: cannot be co-resident");
     grid_cached = sms * per;
     if (grid_cached > 1024) grid_cached = 1024;
@@ -495,12 +615,11 @@ extern "C" int mb_eigh_ws(int n, double* fpacked, int perturb, double* c, double
   const int grid = grid_cached;
   for (int k = 0; k < n - 1; k += NB) {
     const int ib = (NB < n - 1 - k) ? NB : n - 1 - k;
-    MB_CUDA(cudaMemsetAsync(vp, 0, sizeof(double) * (size_t)n * NB, stream));
-    MB_CUDA(cudaMemsetAsync(wp, 0, sizeof(double) * (size_t)n * NB, stream));
+    MB_CUDA(cudaMemsetAsync(vwv, 0, sizeof(double) * (size_t)n * 2 * NB, stream));
     PanelArgs pa;
     pa.n = n; pa.k = k; pa.ib = ib; pa.lda = n;
     pa.a = A; pa.vp = vp; pa.wp = wp; pa.vall = V; pa.d = d; pa.e = e; pa.tau = tau;
-    pa.part = part; pa.partd = part + 1024; pa.tvec = tvec; pa.wvec = wvec;
+    pa.part = part; pa.partd = part + 1024; pa.tvec = tvec; pa.tpart = tpart; pa.wvec = wvec;
     void* args[] = {&pa};
     MB_CUDA(cudaLaunchCooperativeKernel((void*)tridiag_panel, grid, TPB, args, 0, stream));
     mb_count_launch();
@@ -508,8 +627,15 @@ extern "C" int mb_eigh_ws(int n, double* fpacked, int perturb, double* c, double
     if (t < n) {
       const int m = n - t;
       double* At = A + (size_t)t * n + t;
-      MB_TRY(mb_dgemm_dev('N', 'T', m, m, ib, -1.0, vp + t, n, wp + t, n, 1.0, At, n, stream));
-      MB_TRY(mb_dgemm_dev('N', 'T', m, m, ib, -1.0, wp + t, n, vp + t, n, 1.0, At, n, stream));
+      if (ib == NB) {
+        // A -= [V W] [W V]^T as one GEMM with k = 2*NB
+        MB_CUDA(cudaMemcpyAsync(vwv + (size_t)n * 2 * NB, vp, sizeof(double) * (size_t)n * NB,
+                                cudaMemcpyDeviceToDevice, stream));
+        MB_TRY(mb_dgemm_dev('N', 'T', m, m, 2 * NB, -1.0, vwv + t, n, wp + t, n, 1.0, At, n, stream));
+      } else {
+        MB_TRY(mb_dgemm_dev('N', 'T', m, m, ib, -1.0, vp + t, n, wp + t, n, 1.0, At, n, stream));
+        MB_TRY(mb_dgemm_dev('N', 'T', m, m, ib, -1.0, wp + t, n, vp + t, n, 1.0, At, n, stream));
+      }
     }
   }
   copy_last_diag<<<1, 32, 0, stream>>>(n, A, n, d);
@@ -517,7 +643,7 @@ extern "C" int mb_eigh_ws(int n, double* fpacked, int perturb, double* c, double
   // eigenvalues
   tri_bounds<<<1, 1024, 0, stream>>>(n, d, e, e2, bnd);
   MB_LAUNCH_CHECK();
-  bisect_kernel<<<(n + 127) / 128, 128, 0, stream>>>(n, d, e2, bnd, eigs);
+  bisect_kernel<<<(n * 32 + 255) / 256, 256, 0, stream>>>(n, d, e2, bnd, eigs);
   MB_LAUNCH_CHECK();
   // eigenvectors of T
   MB_CUDA(cudaMemsetAsync(status_dev, 0, sizeof(int), stream));
@@ -528,20 +654,29 @@ extern "C" int mb_eigh_ws(int n, double* fpacked, int perturb, double* c, double
     transpose_kernel<<<g, blk, 0, stream>>>(n, X, Z);
     MB_LAUNCH_CHECK();
   }
-  // back-transformation, panels in reverse order: Z <- (I - V T V^T) Z
-  int last_k = ((n - 2) / NB) * NB;
-  for (int k = last_k; k >= 0; k -= NB) {
-    const int ib = (NB < n - 1 - k) ? NB : n - 1 - k;
-    if (ib <= 0) continue;
-    const int r0 = k + 1;           // first nonzero row of the panel's reflectors
-    const int m = n - r0;
-    const double* Vk = V + (size_t)k * n + r0;
-    MB_TRY(mb_dgemm_dev('T', 'N', ib, ib, m, 1.0, Vk, n, Vk, n, 0.0, S, ib, stream));
-    larft_kernel<<<1, 64, 0, stream>>>(ib, S, tau + k, Tm);
-    MB_LAUNCH_CHECK();
-    MB_TRY(mb_dgemm_dev('T', 'N', ib, n, m, 1.0, Vk, n, Z + r0, n, 0.0, Y, ib, stream));
-    MB_TRY(mb_dgemm_dev('N', 'N', ib, n, ib, 1.0, Tm, ib, Y, ib, 0.0, X, ib, stream));
-    MB_TRY(mb_dgemm_dev('N', 'N', m, n, ib, -1.0, Vk, n, X, ib, 1.0, Z + r0, n, stream));
+  // back-transformation, blocks of BT reflectors in reverse order:
+  // Z <- (I - V T V^T) Z
+  {
+    static bool larft_attr = false;
+    if (!larft_attr) {
+      MB_CUDA(cudaFuncSetAttribute(larft_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LARFT_SMEM));
+      larft_attr = true;
+    }
+    const int nref = n - 1;  // reflectors 0 .. n-2
+    const int last_k = ((nref - 1) / BT) * BT;
+    for (int k = last_k; k >= 0; k -= BT) {
+      const int ib = (BT < nref - k) ? BT : nref - k;
+      if (ib <= 0) continue;
+      const int r0 = k + 1;  // first nonzero row of the block's reflectors
+      const int m = n - r0;
+      const double* Vk = V + (size_t)k * n + r0;
+      MB_TRY(mb_dgemm_ws('T', 'N', ib, ib, m, 1.0, Vk, n, Vk, n, 0.0, S, ib, U0, 3 * nn, stream));
+      larft_kernel<<<1, BT, LARFT_SMEM, stream>>>(ib, S, tau + k, Tm);
+      MB_LAUNCH_CHECK();
+      MB_TRY(mb_dgemm_ws('T', 'N', ib, n, m, 1.0, Vk, n, Z + r0, n, 0.0, Y, ib, U0, 3 * nn, stream));
+      MB_TRY(mb_dgemm_dev('N', 'N', ib, n, ib, 1.0, Tm, ib, Y, ib, 0.0, X, ib, stream));
+      MB_TRY(mb_dgemm_dev('N', 'N', m, n, ib, -1.0, Vk, n, X, ib, 1.0, Z + r0, n, stream));
+    }
   }
   MB_CUDA(cudaMemcpyAsync(c, Z, sizeof(double) * nn, cudaMemcpyDeviceToDevice, stream));
   return MB_OK;

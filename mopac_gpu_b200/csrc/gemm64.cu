@@ -26,8 +26,9 @@ __device__ __forceinline__ double load_b(const double* b, int ldb, int n, int k,
 // C tile (bm, bn) accumulation, shared by dgemm and packed syrk.
 template <bool TA, bool TB>
 __device__ __forceinline__ void tile_mma(const double* __restrict__ a, int lda, const double* __restrict__ b,
-                                         int ldb, int m, int n, int k, int bm, int bn,
+                                         int ldb, int m, int n, int kbeg, int kend, int bm, int bn,
                                          double acc[TM][TN]) {
+  const int k = kend;
   __shared__ double As[2][BK][BM + 1];
   __shared__ double Bs[2][BK][BN + 1];
   const int tid = threadIdx.x;
@@ -70,13 +71,13 @@ __device__ __forceinline__ void tile_mma(const double* __restrict__ a, int lda, 
       Bs[buf][kk][c] = rb[q];
     }
   };
-  const int nk = (k + BK - 1) / BK;
-  gload(0);
+  const int nk = (kend - kbeg + BK - 1) / BK;
+  gload(kbeg);
   sstore(0);
   __syncthreads();
   for (int t = 0; t < nk; ++t) {
     const int cur = t & 1;
-    if (t + 1 < nk) gload((t + 1) * BK);
+    if (t + 1 < nk) gload(kbeg + (t + 1) * BK);
 #pragma unroll
     for (int kk = 0; kk < BK; ++kk) {
       double av[TM], bv[TN];
@@ -98,10 +99,17 @@ template <bool TA, bool TB>
 __global__ void __launch_bounds__(NT) dgemm_kernel(int m, int n, int k, double alpha, const double* __restrict__ a,
                                                    int lda, const double* __restrict__ b, int ldb, double beta,
                                                    double* __restrict__ c, int ldc) {
+  // split-K: slice z of gridDim.z covers k in [z*kchunk, min(k, (z+1)*kchunk))
+  // and, when gridDim.z > 1, writes its raw partial sum to c + z*m*n (ld = m)
   const int bm = blockIdx.y * BM, bn = blockIdx.x * BN;
+  const int kchunk = (k + gridDim.z - 1) / gridDim.z;
+  const int kb = blockIdx.z * kchunk, ke = min(k, kb + kchunk);
   double acc[TM][TN];
-  tile_mma<TA, TB>(a, lda, b, ldb, m, n, k, bm, bn, acc);
+  tile_mma<TA, TB>(a, lda, b, ldb, m, n, kb, ke, bm, bn, acc);
   const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+  const bool partial = gridDim.z > 1;
+  double* cz = partial ? c + (long long)blockIdx.z * m * n : c;
+  const int ldz = partial ? m : ldc;
 #pragma unroll
   for (int i = 0; i < TM; ++i) {
     int r = bm + ty + 16 * i;
@@ -110,9 +118,23 @@ __global__ void __launch_bounds__(NT) dgemm_kernel(int m, int n, int k, double a
     for (int j = 0; j < TN; ++j) {
       int cc = bn + tx + 16 * j;
       if (cc >= n) continue;
-      double* p = c + (long long)cc * ldc + r;
-      *p = (beta == 0.0) ? alpha * acc[i][j] : alpha * acc[i][j] + beta * (*p);
+      double* p = cz + (long long)cc * ldz + r;
+      if (partial) *p = acc[i][j];
+      else *p = (beta == 0.0) ? alpha * acc[i][j] : alpha * acc[i][j] + beta * (*p);
     }
+  }
+}
+
+// C = alpha * sum_z part[z] + beta * C, slices summed in order (deterministic).
+__global__ void splitk_reduce(int m, int n, int nz, double alpha, const double* __restrict__ part, double beta,
+                              double* __restrict__ c, int ldc) {
+  const long long mn = (long long)m * n;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < mn; q += (long long)gridDim.x * blockDim.x) {
+    double s = part[q];
+    for (int z = 1; z < nz; ++z) s += part[z * mn + q];
+    const int r = (int)(q % m), cc = (int)(q / m);
+    double* p = c + (long long)cc * ldc + r;
+    *p = (beta == 0.0) ? alpha * s : alpha * s + beta * (*p);
   }
 }
 
@@ -123,7 +145,7 @@ __global__ void __launch_bounds__(NT) syrk_packed_kernel(int n, int k, double oc
   const int bm = blockIdx.y * BM, bn = blockIdx.x * BN;
   if (bn > bm + BM - 1) return;  // tile entirely above the diagonal
   double acc[TM][TN];
-  tile_mma<false, true>(a, lda, a, lda, n, n, k, bm, bn, acc);
+  tile_mma<false, true>(a, lda, a, lda, n, n, 0, k, bm, bn, acc);
   const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
 #pragma unroll
   for (int i = 0; i < TM; ++i) {
@@ -140,20 +162,45 @@ __global__ void __launch_bounds__(NT) syrk_packed_kernel(int n, int k, double oc
 
 }  // namespace
 
-extern "C" int mb_dgemm_dev(char transa, char transb, int m, int n, int k, double alpha, const double* a,
-                            int lda, const double* b, int ldb, double beta, double* c, int ldc,
-                            cudaStream_t stream) {
-  if (m < 0 || n < 0 || k < 0) return mb_set_error(MB_ERR_ARG, "mb_dgemm_dev: negative size");
+// GEMM with optional split-K: when the output has too few 64x64 tiles to fill
+// the GPU and k is long, the k loop is cut into slices whose partial sums go to
+// ws (nsplit * m * n doubles) and are reduced in a fixed order.
+extern "C" int mb_dgemm_ws(char transa, char transb, int m, int n, int k, double alpha, const double* a, int lda,
+                           const double* b, int ldb, double beta, double* c, int ldc, double* ws, size_t ws_elems,
+                           cudaStream_t stream) {
+  if (m < 0 || n < 0 || k < 0) return mb_set_error(MB_ERR_ARG, "mb_dgemm: negative size");
   if (m == 0 || n == 0) return MB_OK;
   bool ta = (transa == 'T' || transa == 't' || transa == 'C' || transa == 'c');
   bool tb = (transb == 'T' || transb == 't' || transb == 'C' || transb == 'c');
-  dim3 grid((n + BN - 1) / BN, (m + BM - 1) / BM);
-  if (!ta && !tb) dgemm_kernel<false, false><<<grid, NT, 0, stream>>>(m, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
-  else if (!ta && tb) dgemm_kernel<false, true><<<grid, NT, 0, stream>>>(m, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
-  else if (ta && !tb) dgemm_kernel<true, false><<<grid, NT, 0, stream>>>(m, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
-  else dgemm_kernel<true, true><<<grid, NT, 0, stream>>>(m, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
+  const int tiles = ((n + BN - 1) / BN) * ((m + BM - 1) / BM);
+  int nz = 1;
+  if (ws && k >= 512 && tiles < 296) {
+    nz = (296 + tiles - 1) / tiles;
+    if (nz > k / 128) nz = k / 128;
+    if (nz > 32) nz = 32;
+    while (nz > 1 && (size_t)nz * m * n > ws_elems) --nz;
+  }
+  dim3 grid((n + BN - 1) / BN, (m + BM - 1) / BM, nz);
+  double* out = nz > 1 ? ws : c;
+  if (!ta && !tb) dgemm_kernel<false, false><<<grid, NT, 0, stream>>>(m, n, k, alpha, a, lda, b, ldb, beta, out, ldc);
+  else if (!ta && tb) dgemm_kernel<false, true><<<grid, NT, 0, stream>>>(m, n, k, alpha, a, lda, b, ldb, beta, out, ldc);
+  else if (ta && !tb) dgemm_kernel<true, false><<<grid, NT, 0, stream>>>(m, n, k, alpha, a, lda, b, ldb, beta, out, ldc);
+  else dgemm_kernel<true, true><<<grid, NT, 0, stream>>>(m, n, k, alpha, a, lda, b, ldb, beta, out, ldc);
   MB_LAUNCH_CHECK();
+  if (nz > 1) {
+    long long mn = (long long)m * n;
+    int blocks = (int)((mn + 255) / 256);
+    if (blocks > 148 * 8) blocks = 148 * 8;
+    splitk_reduce<<<blocks, 256, 0, stream>>>(m, n, nz, alpha, ws, beta, c, ldc);
+    MB_LAUNCH_CHECK();
+  }
   return MB_OK;
+}
+
+extern "C" int mb_dgemm_dev(char transa, char transb, int m, int n, int k, double alpha, const double* a,
+                            int lda, const double* b, int ldb, double beta, double* c, int ldc,
+                            cudaStream_t stream) {
+  return mb_dgemm_ws(transa, transb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, nullptr, 0, stream);
 }
 
 extern "C" int mb_density_dev(int n, int nocc, double occ, const double* c, int ldc, double* p,

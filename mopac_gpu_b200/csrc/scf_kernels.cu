@@ -184,7 +184,6 @@ __global__ void perturb_diag(int n, double* __restrict__ pk) {
 
 // -------------------------------------------------------- pseudo-diag sweep
 constexpr int RT = 16;          // rotation tile: 16 occupied x 16 virtual columns
-constexpr int ROWS = 64;        // rows of C per CTA (one row per thread)
 
 __global__ void absmax_kernel(long long len, const double* __restrict__ x, unsigned long long* out) {
   double m = 0.0;
@@ -229,68 +228,75 @@ __global__ void rot_coeff_kernel(int nocc, int nvirt, const double* __restrict__
   }
 }
 
-// Apply all active rotations to C in the reference order.  Each thread owns one
-// row of C.  Tiles are visited occupied-block outer, virtual-block inner; inside
-// a tile, occupied column i outer, virtual column j inner.  That keeps the order
-// of operations on every column identical to the sequential sweep (rotations on
-// disjoint column pairs commute exactly), so the result is bit-identical.
-__global__ void __launch_bounds__(ROWS) rot_sweep_kernel(int n, int nocc, int nvirt, double* __restrict__ c,
+// Apply all active rotations to C in the reference order, one anti-diagonal of
+// 16x16 (occupied block I, virtual block J) tiles per launch.  Tile (I, J)
+// touches columns I (occupied) and J (virtual) only; it must follow (I, J-1),
+// which last touched columns I, and (I-1, J), which last touched columns J.
+// Tiles on one anti-diagonal I + J = t touch disjoint columns, so they run in
+// parallel, and every column still sees its rotations in the sequential
+// sweep's order (occupied i outer, virtual j inner) -- rotations on disjoint
+// column pairs commute exactly, so C is bit-identical to the sequential sweep.
+// Each thread owns one row of C; a CTA covers WROWS rows of one tile.
+constexpr int WROWS = 64;
+
+__global__ void __launch_bounds__(WROWS) rot_wave_kernel(int n, int nocc, int nvirt, double* __restrict__ c,
                                                          const double* __restrict__ alpha,
                                                          const double* __restrict__ beta,
                                                          const unsigned char* __restrict__ act,
-                                                         const unsigned int* __restrict__ tile_cnt,
-                                                         int ntile_o, int ntile_v) {
+                                                         const unsigned int* __restrict__ tile_cnt, int ntile_o,
+                                                         int ntile_v, int t) {
+  const int jlo = t - (ntile_o - 1) > 0 ? t - (ntile_o - 1) : 0;
+  const int J = jlo + blockIdx.y;
+  const int I = t - J;
+  if (J >= ntile_v || I < 0 || I >= ntile_o) return;
+  if (tile_cnt[I * ntile_v + J] == 0) return;
   __shared__ double s_al[RT][RT], s_be[RT][RT];
   __shared__ unsigned char s_on[RT][RT];
-  const int r = blockIdx.x * ROWS + threadIdx.x;
-  const bool live = r < n;
-  for (int ti = 0; ti < ntile_o; ++ti) {
-    const int i0 = ti * RT;
-    bool any = false;
-    for (int tj = 0; tj < ntile_v; ++tj) any |= tile_cnt[ti * ntile_v + tj] != 0;
-    if (!any) continue;
-    double xi[RT];
-#pragma unroll
-    for (int u = 0; u < RT; ++u) xi[u] = (live && i0 + u < nocc) ? c[(long long)(i0 + u) * n + r] : 0.0;
-    for (int tj = 0; tj < ntile_v; ++tj) {
-      if (tile_cnt[ti * ntile_v + tj] == 0) continue;
-      const int j0 = tj * RT;
-      __syncthreads();
-      for (int e = threadIdx.x; e < RT * RT; e += ROWS) {
-        int u = e / RT, v = e % RT;
-        bool in = (i0 + u < nocc) && (j0 + v < nvirt);
-        long long q = (long long)(i0 + u) * nvirt + (j0 + v);
-        s_on[u][v] = in ? act[q] : 0;
-        s_al[u][v] = in ? alpha[q] : 1.0;
-        s_be[u][v] = in ? beta[q] : 0.0;
-      }
-      __syncthreads();
-      double xj[RT];
-#pragma unroll
-      for (int v = 0; v < RT; ++v) xj[v] = (live && j0 + v < nvirt) ? c[(long long)(nocc + j0 + v) * n + r] : 0.0;
-#pragma unroll
-      for (int u = 0; u < RT; ++u)
-#pragma unroll
-        for (int v = 0; v < RT; ++v) {
-          if (s_on[u][v]) {
-            const double al = s_al[u][v], be = s_be[u][v];
-            const double a = xi[u], b = xj[v];
-            xi[u] = DADD(DMUL(al, a), DMUL(be, b));
-            xj[v] = DSUB(DMUL(al, b), DMUL(be, a));
-          }
-        }
-      if (live) {
-#pragma unroll
-        for (int v = 0; v < RT; ++v)
-          if (j0 + v < nvirt) c[(long long)(nocc + j0 + v) * n + r] = xj[v];
-      }
-    }
-    if (live) {
-#pragma unroll
-      for (int u = 0; u < RT; ++u)
-        if (i0 + u < nocc) c[(long long)(i0 + u) * n + r] = xi[u];
-    }
+  const int i0 = I * RT, j0 = J * RT;
+  for (int e = threadIdx.x; e < RT * RT; e += WROWS) {
+    const int u = e / RT, v = e % RT;
+    const bool in = (i0 + u < nocc) && (j0 + v < nvirt);
+    const long long q = (long long)(i0 + u) * nvirt + (j0 + v);
+    s_on[u][v] = in ? act[q] : 0;
+    s_al[u][v] = in ? alpha[q] : 1.0;
+    s_be[u][v] = in ? beta[q] : 0.0;
   }
+  __syncthreads();
+  const int r = blockIdx.x * WROWS + threadIdx.x;
+  if (r >= n) return;
+  double xi[RT], xj[RT];
+#pragma unroll
+  for (int u = 0; u < RT; ++u) xi[u] = (i0 + u < nocc) ? c[(long long)(i0 + u) * n + r] : 0.0;
+#pragma unroll
+  for (int v = 0; v < RT; ++v) xj[v] = (j0 + v < nvirt) ? c[(long long)(nocc + j0 + v) * n + r] : 0.0;
+#pragma unroll
+  for (int u = 0; u < RT; ++u)
+#pragma unroll
+    for (int v = 0; v < RT; ++v) {
+      if (s_on[u][v]) {
+        const double al = s_al[u][v], be = s_be[u][v];
+        const double a = xi[u], b = xj[v];
+        xi[u] = DADD(DMUL(al, a), DMUL(be, b));
+        xj[v] = DSUB(DMUL(al, b), DMUL(be, a));
+      }
+    }
+#pragma unroll
+  for (int u = 0; u < RT; ++u)
+    if (i0 + u < nocc) c[(long long)(i0 + u) * n + r] = xi[u];
+#pragma unroll
+  for (int v = 0; v < RT; ++v)
+    if (j0 + v < nvirt) c[(long long)(nocc + j0 + v) * n + r] = xj[v];
+}
+
+int launch_wavefronts(int n, int nocc, int nvirt, double* c, const double* al, const double* be,
+                      const unsigned char* act, const unsigned int* tcnt, int to, int tv, cudaStream_t stream) {
+  const int diag_len = to < tv ? to : tv;
+  dim3 grid((n + WROWS - 1) / WROWS, diag_len);
+  for (int t = 0; t < to + tv - 1; ++t) {
+    rot_wave_kernel<<<grid, WROWS, 0, stream>>>(n, nocc, nvirt, c, al, be, act, tcnt, to, tv, t);
+    MB_LAUNCH_CHECK();
+  }
+  return MB_OK;
 }
 
 }  // namespace
@@ -418,9 +424,7 @@ extern "C" int mb_pseudo_diag_ws(int n, int nocc, const double* fpacked, double*
   MB_LAUNCH_CHECK();
   rot_coeff_kernel<<<blocks, 256, 0, stream>>>(nocc, nvirt, fmo, eigs, tiny, -1.0, 1.5e-7, al, be, act, tcnt, nrot_dev, tv);
   MB_LAUNCH_CHECK();
-  rot_sweep_kernel<<<(n + ROWS - 1) / ROWS, ROWS, 0, stream>>>(n, nocc, nvirt, c, al, be, act, tcnt, to, tv);
-  MB_LAUNCH_CHECK();
-  return MB_OK;
+  return launch_wavefronts(n, nocc, nvirt, c, al, be, act, tcnt, to, tv, stream);
 }
 
 // Rotation sweep alone with caller-given Fmo, tiny and bigeps (the arguments
@@ -447,9 +451,7 @@ extern "C" int mb_rot_sweep_ws(int n, int nocc, const double* fmo, const double*
   if (blocks > 148 * 8) blocks = 148 * 8;
   rot_coeff_kernel<<<blocks, 256, 0, stream>>>(nocc, nvirt, fmo, eigs, nullptr, tiny, bigeps, al, be, act, tcnt, nrot_dev, tv);
   MB_LAUNCH_CHECK();
-  rot_sweep_kernel<<<(n + ROWS - 1) / ROWS, ROWS, 0, stream>>>(n, nocc, nvirt, c, al, be, act, tcnt, to, tv);
-  MB_LAUNCH_CHECK();
-  return MB_OK;
+  return launch_wavefronts(n, nocc, nvirt, c, al, be, act, tcnt, to, tv, stream);
 }
 
 extern "C" int mb_pseudo_diag_dev(int n, int nocc, const double* fpacked, double* c, const double* eigs,
