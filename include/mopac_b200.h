@@ -143,6 +143,16 @@ int mb_fock2_dev(const MbAtomsDev* atoms, double* f, const double* h, const doub
 int mb_helect_dev(int n, const double* p, const double* h, const double* f, double* out,
                   cudaStream_t stream);
 
+/* helect without any device allocation.  No counterpart in the reference: it
+ * exists for callers that cannot allocate device memory where they need the
+ * energy (a host arena that owns all device memory, stream capture, hard
+ * latency loops).  Scratch is a fixed 256 KiB array inside the library, so
+ * n <= 16384 (larger n: MB_ERR_ARG); calls share that array and must not
+ * overlap on the GPU; the first call on a device resolves the array's address
+ * and should happen outside stream capture. */
+int mb_helect_noalloc(int n, const double* p, const double* h, const double* f, double* out,
+                      cudaStream_t stream);
+
 /* cnvg (SCF/cnvg.F90) for RHF.  pnew is extrapolated in place, p and p1 are
  * the history; *pl_out (device) receives max|dP_ii|.  Bit-identical. */
 int mb_cnvg_dev(int norbs, double* pnew, double* p, double* p1, int niter, double* pl_out,

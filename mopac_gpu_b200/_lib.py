@@ -70,6 +70,7 @@ SIGNATURES = {
     "mb_atoms_destroy": ([ctypes.POINTER(MbAtomsDev)], _I),
     "mb_fock2_dev": ([ctypes.POINTER(MbAtomsDev), _P, _P, _P, _P, _P, _D, _I, _P], _I),
     "mb_helect_dev": ([_I, _P, _P, _P, _P, _P], _I),
+    "mb_helect_noalloc": ([_I, _P, _P, _P, _P, _P], _I),
     "mb_cnvg_dev": ([_I, _P, _P, _P, _I, _P, _P], _I),
     "mb_density_dev": ([_I, _I, _D, _P, _I, _P, _P], _I),
     "mb_eigh_packed_dev": ([_I, _P, _P, _P, _P], _I),
