@@ -53,6 +53,11 @@ typedef struct CUstream_st* cudaStream_t;
 
 int mb_version(void);                 /* 10000*major + 100*minor + patch       */
 long long mb_launch_count(void);      /* kernels this library has launched     */
+/* Opt-in CUDA-event timing per kernel family, recorded on the launching
+ * stream: 0 Householder panel, 1 Fock build, 2 density, 3 full eigensolve,
+ * 4 pseudo-diagonalisation.  mb_kstats_read syncs, returns and clears id. */
+void mb_kstats_enable(int on);
+int mb_kstats_read(int id, long long* count, double* total_ms);
 const char* mb_last_error(void);      /* thread-local text of the last failure */
 
 /* ------------------------------------------------ (3) device-resident API */

@@ -50,6 +50,8 @@ _C = ctypes.c_char
 SIGNATURES = {
     "mb_version": ([], _I),
     "mb_launch_count": ([], _LL),
+    "mb_kstats_enable": ([_I], None),
+    "mb_kstats_read": ([_I, ctypes.POINTER(_LL), ctypes.POINTER(_D)], _I),
     "mb_last_error": ([], ctypes.c_char_p),
     "mb_scf_opts_default": ([ctypes.POINTER(ScfOpts)], None),
     "mb_ctx_create": ([_I, _P, _P, ctypes.POINTER(_P)], _I),

@@ -621,7 +621,9 @@ extern "C" int mb_eigh_ws(int n, double* fpacked, int perturb, double* c, double
     pa.a = A; pa.vp = vp; pa.wp = wp; pa.vall = V; pa.d = d; pa.e = e; pa.tau = tau;
     pa.part = part; pa.partd = part + 1024; pa.tvec = tvec; pa.tpart = tpart; pa.wvec = wvec;
     void* args[] = {&pa};
+    mb_kstat_mark(MB_KSTAT_TRIDIAG, stream, true);
     MB_CUDA(cudaLaunchCooperativeKernel((void*)tridiag_panel, grid, TPB, args, 0, stream));
+    mb_kstat_mark(MB_KSTAT_TRIDIAG, stream, false);
     mb_count_launch();
     const int t = k + ib;
     if (t < n) {

@@ -255,7 +255,9 @@ extern "C" int mb_fock2_dev(const MbAtomsDev* atoms, double* f, const double* h,
   a.w = w;
   a.shift = shift;
   a.use_shift = use_shift;
+  mb_kstat_mark(MB_KSTAT_FOCK, stream, true);
   fock2_kernel<<<atoms->numat, kChunk, 0, stream>>>(a);
+  mb_kstat_mark(MB_KSTAT_FOCK, stream, false);
   MB_LAUNCH_CHECK();
   return MB_OK;
 }

@@ -211,7 +211,9 @@ extern "C" int mb_density_dev(int n, int nocc, double occ, const double* c, int 
     return MB_OK;
   }
   dim3 grid((n + BN - 1) / BN, (n + BM - 1) / BM);
+  mb_kstat_mark(MB_KSTAT_DENSITY, stream, true);
   syrk_packed_kernel<<<grid, NT, 0, stream>>>(n, nocc, occ, c, ldc, p, grid.x);
+  mb_kstat_mark(MB_KSTAT_DENSITY, stream, false);
   MB_LAUNCH_CHECK();
   return MB_OK;
 }

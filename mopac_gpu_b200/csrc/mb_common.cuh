@@ -26,6 +26,15 @@ void mb_count_launch();
     if (_e != cudaSuccess) return mb_set_cuda_error(_e, "kernel launch", __FILE__, __LINE__); \
   } while (0)
 
+// Kernel-family ids for the opt-in event timing (mb_kstats_*).
+#define MB_KSTAT_TRIDIAG 0   // one tridiag_panel launch
+#define MB_KSTAT_FOCK 1      // one fock2_kernel launch
+#define MB_KSTAT_DENSITY 2   // one packed SYRK (density) launch
+#define MB_KSTAT_EIGH 3      // one full eigensolve
+#define MB_KSTAT_PSEUDO 4    // one pseudo-diagonalisation
+#define MB_KSTAT_IDS 8
+void mb_kstat_mark(int id, cudaStream_t s, bool begin);
+
 #define MB_TRY(expr)            \
   do {                          \
     int _rc = (expr);           \

@@ -358,7 +358,9 @@ struct PhaseTimer {
 };
 
 static int full_diag(mb_ctx* c, double* fpacked, double* eig_homo, double* eig_lumo, int ihomo) {
+  mb_kstat_mark(MB_KSTAT_EIGH, c->stream, true);
   MB_TRY(mb_eigh_ws(c->norbs, fpacked, 1, c->c, c->eigs, c->eig_ws, c->status, c->stream));
+  mb_kstat_mark(MB_KSTAT_EIGH, c->stream, false);
   int st = 0;
   MB_CUDA(cudaMemcpyAsync(&st, c->status, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   double hl[2] = {0.0, 0.0};
@@ -501,7 +503,9 @@ extern "C" int mb_scf_run(mb_ctx* c, const mb_scf_opts* opts_in, mb_scf_result* 
               shift, newdg ? "newdg" : "");
     t_diag.start();
     if (newdg && opts.pseudo && !(halfe || camkin)) {
+      mb_kstat_mark(MB_KSTAT_PSEUDO, s, true);
       MB_TRY(mb_pseudo_diag_ws(n, na1el, c->f, c->c, c->eigs, c->nrot, c->pseudo_ws, s));
+      mb_kstat_mark(MB_KSTAT_PSEUDO, s, false);
       res->n_pseudo_diag++;
     } else {
       MB_TRY(full_diag(c, c->f, &eig_homo, &eig_lumo, ihomo));
