@@ -84,6 +84,9 @@ typedef struct mb_scf_opts {
                         max|dP| < switch_pl, FP64 after                   */
   double switch_pl;  /* precision switch threshold (default 1e-4)         */
   int verbose;       /* print one line per iteration to stderr            */
+  int pulay;         /* 1: Pulay's converger once newdg is set, like the
+                        PULAY keyword (SCF/iter.F90:135, :815-831); cnvg is
+                        then skipped (:899) and the shift is -8 / 0 (:417) */
 } mb_scf_opts;
 
 typedef struct mb_scf_result {
@@ -97,6 +100,7 @@ typedef struct mb_scf_result {
   double pl;         /* last max|dP_ii|                                    */
   double t_fock_ms, t_diag_ms, t_density_ms, t_other_ms; /* device-timed  */
   double t_total_ms; /* CUDA events on the context stream around the SCF   */
+  int n_pulay;       /* Pulay extrapolation steps taken                    */
 } mb_scf_result;
 
 void mb_scf_opts_default(mb_scf_opts* o);
@@ -163,6 +167,25 @@ int mb_helect_noalloc(int n, const double* p, const double* h, const double* f, 
 int mb_cnvg_dev(int norbs, double* pnew, double* p, double* p1, int niter, double* pl_out,
                 cudaStream_t stream);
 
+/* One step of Pulay's converger, pulay(f, p, n, fppf, fock, emat, lfock,
+ * nfock, msize, start, pl) (SCF/pulay.F90:16-180), on device histories.
+ * f, p: packed n x n (device); f is replaced by the extrapolated Fock matrix
+ * once two entries are stored.  fppf, fock: device histories of mfock
+ * entries in the reference's layouts (commutator slot l is the block
+ * fppf[l*linear ...], Fock entry i of slot l is fock[l + i*mfock]).  emat:
+ * host, column-major ldemat x ldemat (ldemat >= mfock + 1).  lfock, nfock,
+ * start (0/1), pl: host scalars with the reference's meaning.  ws: device,
+ * 256-byte aligned, mb_pulay_ws_bytes(n) bytes.  mfock <= 16.  Synchronises
+ * the stream once (the B matrix is inverted on the host). */
+size_t mb_pulay_ws_bytes(int n);
+int mb_pulay_ws(int n, double* f, const double* p, double* fppf, double* fock, int mfock,
+                double* emat, int ldemat, int* lfock, int* nfock, int* start, double* pl, void* ws,
+                cudaStream_t stream);
+/* osinv(a, n, d) (matrix/osinv.F90): in-place Gauss-Jordan inverse with full
+ * pivoting of the column-major n x n host matrix a; returns d (0 when a pivot
+ * is below 1e-8). */
+double mb_osinv(double* a, int n);
+
 /* P (packed) = occ * C[:, 0:nocc] C[:, 0:nocc]^T, FP64. */
 int mb_density_dev(int n, int nocc, double occ, const double* c, int ldc, double* p,
                    cudaStream_t stream);
@@ -228,6 +251,13 @@ double helect_(const int* n, const double* p, const double* h, const double* f);
  * molkst_C in the reference; a Fortran host sets it once with mb_set_norbs. */
 void cnvg_(double* pnew, double* p, double* p1, const int* niter, double* pl);
 void mb_set_norbs_(const int* norbs);
+/* pulay(f, p, n, fppf, fock, emat, lfock, nfock, msize, start, pl),
+ * SCF/pulay.F90:16; host arrays; start is a Fortran LOGICAL (4 bytes).
+ * npulay comes from molkst_C in the reference (default 10, which this shim
+ * assumes); a Fortran host with another value sets it with mb_set_npulay. */
+void pulay_(double* f, const double* p, const int* n, double* fppf, double* fock, double* emat,
+            int* lfock, int* nfock, const int* msize, int* start, double* pl);
+void mb_set_npulay_(const int* npulay);
 /* density_for_GPU(c, fract, ndubl, nsingl, occ, mpack, norbs, mode, pp, iopc),
  * matrix/density_for_GPU.F90:16; closed shell (fract = 0) */
 void density_for_gpu_(const double* c, const double* fract, const int* ndubl, const int* nsingl,

@@ -29,14 +29,16 @@ class MbAtomsDev(ctypes.Structure):
 
 class ScfOpts(ctypes.Structure):
     _fields_ = [("pseudo", ctypes.c_int), ("itrmax", ctypes.c_int), ("scfcrt", ctypes.c_double),
-                ("precision", ctypes.c_int), ("switch_pl", ctypes.c_double), ("verbose", ctypes.c_int)]
+                ("precision", ctypes.c_int), ("switch_pl", ctypes.c_double), ("verbose", ctypes.c_int),
+                ("pulay", ctypes.c_int)]
 
 
 class ScfRes(ctypes.Structure):
     _fields_ = [("escf", ctypes.c_double), ("ee", ctypes.c_double), ("niter", ctypes.c_int),
                 ("converged", ctypes.c_int), ("n_full_diag", ctypes.c_int), ("n_pseudo_diag", ctypes.c_int),
                 ("pl", ctypes.c_double), ("t_fock_ms", ctypes.c_double), ("t_diag_ms", ctypes.c_double),
-                ("t_density_ms", ctypes.c_double), ("t_other_ms", ctypes.c_double), ("t_total_ms", ctypes.c_double)]
+                ("t_density_ms", ctypes.c_double), ("t_other_ms", ctypes.c_double), ("t_total_ms", ctypes.c_double),
+                ("n_pulay", ctypes.c_int)]
 
 
 _lib = None
@@ -75,6 +77,9 @@ SIGNATURES = {
     "mb_helect_noalloc": ([_I, _P, _P, _P, _P, _P], _I),
     "mb_cnvg_dev": ([_I, _P, _P, _P, _I, _P, _P], _I),
     "mb_density_dev": ([_I, _I, _D, _P, _I, _P, _P], _I),
+    "mb_pulay_ws_bytes": ([_I], ctypes.c_size_t),
+    "mb_pulay_ws": ([_I, _P, _P, _P, _P, _I, _P, _I, _P, _P, _P, _P, _P, _P], _I),
+    "mb_osinv": ([_P, _I], _D),
     "mb_eigh_packed_dev": ([_I, _P, _P, _P, _P], _I),
     "mb_pseudo_diag_dev": ([_I, _I, _P, _P, _P, ctypes.POINTER(_LL), _P], _I),
     "mb_dgemm_dev": ([_C, _C, _I, _I, _I, _D, _P, _I, _P, _I, _D, _P, _I, _P], _I),
@@ -95,6 +100,8 @@ SIGNATURES = {
     "helect_": ([_P] * 4, _D),
     "cnvg_": ([_P] * 5, None),
     "mb_set_norbs_": ([_P], None),
+    "pulay_": ([_P] * 11, None),
+    "mb_set_npulay_": ([_P], None),
     "density_for_gpu_": ([_P] * 10, None),
     "eigenvectors_lapack_": ([_P] * 4, None),
     "diag_for_gpu_": ([_P] * 6, None),

@@ -27,6 +27,9 @@ extern "C" int mb_cnvg_ws(int norbs, double* pnew, double* p, double* p1, int ni
                           cudaStream_t stream);
 extern "C" int mb_helect_ws(int n, const double* p, const double* h, const double* f, double* out, double* ws,
                             cudaStream_t stream);
+extern "C" size_t mb_pulay_ws_bytes(int n);
+extern "C" int mb_pulay_ws(int n, double* f, const double* p, double* fppf, double* fock, int mfock, double* emat,
+                           int ldemat, int* lfock, int* nfock, int* start, double* pl, void* ws, cudaStream_t stream);
 
 namespace {
 
@@ -55,6 +58,8 @@ std::mutex g_mu;
 Buf g_a, g_b, g_c, g_d, g_ws;
 cudaStream_t g_stream = nullptr;
 int g_norbs_fortran = 0;
+int g_npulay_fortran = 10;  // molkst_C.F90:114-115
+int g_mfock_fortran = 0;    // pulay's saved mfock (pulay.F90:40, :57-59)
 
 int ensure_stream() {
   if (!g_stream) MB_CUDA(cudaStreamCreateWithFlags(&g_stream, cudaStreamNonBlocking));
@@ -413,4 +418,54 @@ extern "C" void diag_for_gpu_(const double* fao, double* vector, const int* nocc
     rc = MB_ERR_CUDA;
   if (rc == MB_OK && cudaStreamSynchronize(g_stream) != cudaSuccess) rc = MB_ERR_CUDA;
   report(rc, "diag_for_gpu_");
+}
+
+extern "C" void mb_set_npulay_(const int* npulay) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (npulay && *npulay > 0) g_npulay_fortran = *npulay;
+}
+
+extern "C" void pulay_(double* f, const double* p, const int* n, double* fppf, double* fock, double* emat,
+                       int* lfock, int* nfock, const int* msize, int* start, double* pl) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (!n || *n <= 0 || !msize) {
+    report(mb_set_error(MB_ERR_ARG, "pulay_: bad size"), "pulay_");
+    return;
+  }
+  const int nn = *n;
+  const size_t lin = (size_t)nn * (nn + 1) / 2;
+  if (*start) {
+    int mf = (int)((size_t)*msize / lin);
+    g_mfock_fortran = mf < g_npulay_fortran ? mf : g_npulay_fortran;
+  }
+  const int mfock = g_mfock_fortran;
+  if (mfock < 1) {
+    report(mb_set_error(MB_ERR_ARG, "pulay_: msize holds no history entry"), "pulay_");
+    return;
+  }
+  const size_t hist = lin * (size_t)mfock;
+  auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
+  int rc = ensure_stream();
+  if (rc == MB_OK) rc = g_a.get(al(sizeof(double) * lin) * 2 + al(sizeof(double) * hist) * 2);
+  if (rc == MB_OK) rc = g_ws.get(mb_pulay_ws_bytes(nn));
+  if (rc != MB_OK) { report(rc, "pulay_"); return; }
+  char* b = (char*)g_a.p;
+  double* df = (double*)b; b += al(sizeof(double) * lin);
+  double* dp = (double*)b; b += al(sizeof(double) * lin);
+  double* dfppf = (double*)b; b += al(sizeof(double) * hist);
+  double* dfock = (double*)b;
+  if (cudaMemcpyAsync(df, f, sizeof(double) * lin, cudaMemcpyHostToDevice, g_stream) != cudaSuccess ||
+      cudaMemcpyAsync(dp, p, sizeof(double) * lin, cudaMemcpyHostToDevice, g_stream) != cudaSuccess ||
+      cudaMemcpyAsync(dfppf, fppf, sizeof(double) * hist, cudaMemcpyHostToDevice, g_stream) != cudaSuccess ||
+      cudaMemcpyAsync(dfock, fock, sizeof(double) * hist, cudaMemcpyHostToDevice, g_stream) != cudaSuccess)
+    rc = MB_ERR_CUDA;
+  if (rc == MB_OK)
+    rc = mb_pulay_ws(nn, df, dp, dfppf, dfock, mfock, emat, g_npulay_fortran + 1, lfock, nfock, start, pl, g_ws.p,
+                     g_stream);
+  if (rc == MB_OK && (cudaMemcpyAsync(f, df, sizeof(double) * lin, cudaMemcpyDeviceToHost, g_stream) != cudaSuccess ||
+                      cudaMemcpyAsync(fppf, dfppf, sizeof(double) * hist, cudaMemcpyDeviceToHost, g_stream) != cudaSuccess ||
+                      cudaMemcpyAsync(fock, dfock, sizeof(double) * hist, cudaMemcpyDeviceToHost, g_stream) != cudaSuccess))
+    rc = MB_ERR_CUDA;
+  if (rc == MB_OK && cudaStreamSynchronize(g_stream) != cudaSuccess) rc = MB_ERR_CUDA;
+  report(rc, "pulay_");
 }

@@ -6,6 +6,7 @@
 // convergence test (:675-690), the newdg/oknewd switches (:1022-1041), full
 // diagonalisation (:849) or -- with opts.pseudo -- the pseudo-diagonalisation
 // the reference comments out (:847-861), the density (:897), cnvg (:899-901)
+// or -- with opts.pulay, the PULAY keyword -- Pulay's converger (:815-831),
 // and the exit diagonalisation (:1052-1106).  All matrices stay in HBM; the
 // host only sees the scalars the control flow branches on (energy, max|dP|,
 // HOMO/LUMO eigenvalues), a handful of bytes per iteration.
@@ -30,6 +31,9 @@ extern "C" int mb_eigh_ws(int n, double* fpacked, int perturb, double* c, double
 extern "C" size_t mb_pseudo_ws_bytes(int n, int nocc);
 extern "C" int mb_pseudo_diag_ws(int n, int nocc, const double* fpacked, double* c, const double* eigs,
                                  unsigned long long* nrot_dev, void* ws, cudaStream_t stream);
+extern "C" size_t mb_pulay_ws_bytes(int n);
+extern "C" int mb_pulay_ws(int n, double* f, const double* p, double* fppf, double* fock, int mfock, double* emat,
+                           int ldemat, int* lfock, int* nfock, int* start, double* pl, void* ws, cudaStream_t stream);
 extern "C" int mb_hcore_dev(const int* nat_d, const double* coord_d, const MbAtomsDev* at, int numat, double* h,
                             double* w, double* enuc_pairs, cudaStream_t stream);
 extern "C" int mb_hcore_finish(int numat, const MbAtomsDev* at, const int* nat_d, double* h, const double* e1b,
@@ -136,14 +140,20 @@ struct mb_ctx {
   unsigned long long* nrot = nullptr;
   void* eig_ws = nullptr;
   void* pseudo_ws = nullptr;
+  // Pulay histories (npulay * mpack each), allocated on the first Pulay run
+  double *fppf_hist = nullptr, *fock_hist = nullptr;
   cudaStream_t stream = nullptr;
 };
+
+// History length of Pulay's converger: molkst_C.F90:114-115 sets npulay = 10.
+static const int kNpulay = 10;
 
 static void ctx_free(mb_ctx* c) {
   if (!c) return;
   mb_atoms_destroy(&c->atoms);
   void* ptrs[] = {c->d_nat, c->d_coord, c->h, c->w, c->f, c->p, c->pa, c->pold, c->pold2, c->c, c->eigs,
-                  c->fdiag, c->scal, c->hws, c->status, c->nrot, c->eig_ws, c->pseudo_ws};
+                  c->fdiag, c->scal, c->hws, c->status, c->nrot, c->eig_ws, c->pseudo_ws,
+                  c->fppf_hist, c->fock_hist};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -157,6 +167,7 @@ extern "C" void mb_scf_opts_default(mb_scf_opts* o) {
   o->precision = 0;
   o->switch_pl = 1.0e-4;
   o->verbose = 0;
+  o->pulay = 0;
 }
 
 extern "C" int mb_ctx_create(int numat, const int* nat, const double* coord, mb_ctx** out) {
@@ -385,6 +396,20 @@ extern "C" int mb_scf_run(mb_ctx* c, const mb_scf_opts* opts_in, mb_scf_result* 
   const int nclose = c->nclose;
   cudaStream_t s = c->stream;
   if (opts.pseudo && !c->pseudo_ws) MB_CUDA(cudaMalloc(&c->pseudo_ws, mb_pseudo_ws_bytes(n, nclose)));
+  const bool okpuly = opts.pulay != 0;
+  if (okpuly) {
+    if (!c->fppf_hist) MB_CUDA(cudaMalloc(&c->fppf_hist, sizeof(double) * kNpulay * (size_t)mpack));
+    if (!c->fock_hist) MB_CUDA(cudaMalloc(&c->fock_hist, sizeof(double) * kNpulay * (size_t)mpack));
+    // the commutator work runs in the eigensolver workspace, idle before the diagonalisation
+    if (mb_pulay_ws_bytes(n) > mb_eigh_ws_bytes(n))
+      return mb_set_error(MB_ERR_ARG, "mb_scf_run: Pulay workspace exceeds the eigensolver workspace");
+  }
+  // In the reference pold and pold2 are the heads of pulay's history arrays
+  // (setup_mopac_arrays.F90:148, iter.F90:826-831): keep that aliasing.
+  double* pold = okpuly ? c->fppf_hist : c->pold;
+  double* pold2 = okpuly ? c->fock_hist : c->pold2;
+  std::vector<double> emat((size_t)(kNpulay + 1) * (kNpulay + 1), 0.0);
+  int lfock = 0, nfock = 0, frst = 1;
   PhaseTimer t_fock(s), t_diag(s), t_dens(s);
   cudaEvent_t ev_begin, ev_end;
   MB_CUDA(cudaEventCreate(&ev_begin));
@@ -397,7 +422,7 @@ extern "C" int mb_scf_run(mb_ctx* c, const mb_scf_opts* opts_in, mb_scf_result* 
          shiftb = 0.0;
   const double plchek = 0.005, trans = 0.2;
   bool newdg = false, oknewd = fabs(bshift) < 0.001;
-  const bool okpuly = false, halfe = false, camkin = false;
+  const bool halfe = false, camkin = false;
   const int na1el = nclose, nb1el = nclose;
   const int ihomo = nclose > 1 ? nclose : 1;
   {
@@ -413,8 +438,8 @@ extern "C" int mb_scf_run(mb_ctx* c, const mb_scf_opts* opts_in, mb_scf_result* 
     }
     MB_CUDA(cudaMemcpyAsync(c->p, hp.data(), sizeof(double) * mpack, cudaMemcpyHostToDevice, s));
     MB_CUDA(cudaMemcpyAsync(c->pa, hpa.data(), sizeof(double) * mpack, cudaMemcpyHostToDevice, s));
-    MB_CUDA(cudaMemcpyAsync(c->pold, hpa.data(), sizeof(double) * mpack, cudaMemcpyHostToDevice, s));
-    MB_CUDA(cudaMemcpyAsync(c->pold2, hpd.data(), sizeof(double) * n, cudaMemcpyHostToDevice, s));
+    MB_CUDA(cudaMemcpyAsync(pold, hpa.data(), sizeof(double) * mpack, cudaMemcpyHostToDevice, s));
+    MB_CUDA(cudaMemcpyAsync(pold2, hpd.data(), sizeof(double) * n, cudaMemcpyHostToDevice, s));
     MB_CUDA(cudaStreamSynchronize(s));
   }
   const double gnorm = 0.0;
@@ -501,6 +526,11 @@ extern "C" int mb_scf_run(mb_ctx* c, const mb_scf_opts* opts_in, mb_scf_result* 
     if (opts.verbose)
       fprintf(stderr, " ITERATION %4d PLS=%10.3e ENERGY %14.6f DELTAE %13.7f shift %8.3f %s\n", niter, pl, escf, diff,
               shift, newdg ? "newdg" : "");
+    if (newdg && okpuly && iredy > 1) {  // iter.F90:815-831
+      MB_TRY(mb_pulay_ws(n, c->f, c->pa, c->fppf_hist, c->fock_hist, kNpulay, emat.data(), kNpulay + 1, &lfock,
+                         &nfock, &frst, &pl, c->eig_ws, s));
+      res->n_pulay++;
+    }
     t_diag.start();
     if (newdg && opts.pseudo && !(halfe || camkin)) {
       mb_kstat_mark(MB_KSTAT_PSEUDO, s, true);
@@ -514,11 +544,12 @@ extern "C" int mb_scf_run(mb_ctx* c, const mb_scf_opts* opts_in, mb_scf_result* 
     t_diag.stop();
     t_dens.start();
     MB_TRY(mb_density_dev(n, nclose, 2.0, c->c, n, c->p, s));
-    MB_TRY(mb_cnvg_ws(n, c->p, c->pold, c->pold2, niter, c->scal + 1, c->scal + 8, s));
+    const bool do_cnvg = !(newdg && okpuly);  // iter.F90:899
+    if (do_cnvg) MB_TRY(mb_cnvg_ws(n, c->p, pold, pold2, niter, c->scal + 1, c->scal + 8, s));
     half_kernel<<<hblocks, 256, 0, s>>>(mpack, c->p, c->pa);
     MB_LAUNCH_CHECK();
     t_dens.stop();
-    MB_TRY(d2h(c, &pl, c->scal + 1, 1));
+    if (do_cnvg) MB_TRY(d2h(c, &pl, c->scal + 1, 1));
     if (!isfinite(pl)) return mb_set_error(MB_ERR_NUMERIC, "non-finite density change");
     oknewd = pl < sellim || oknewd;
     newdg = (pl < trans && oknewd) || newdg;

@@ -55,6 +55,36 @@ def cnvg(norbs: int, pnew, p, p1, niter: int) -> float:
     return float(pl.item())
 
 
+class Pulay:
+    """Device histories and host state of Pulay's converger for one density
+    (the fppf, fock, emat, lfock, nfock, start arguments of
+    pulay(f, p, n, fppf, fock, emat, lfock, nfock, msize, start, pl),
+    SCF/pulay.F90:16).  ``step(f, p)`` extrapolates f in place and returns pl."""
+
+    def __init__(self, n: int, npulay: int = 10, device="cuda"):
+        self.n = n
+        self.linear = n * (n + 1) // 2
+        self.mfock = npulay
+        self.fppf = torch.zeros(npulay * self.linear, dtype=torch.float64, device=device)
+        self.fock = torch.zeros(npulay * self.linear, dtype=torch.float64, device=device)
+        self.emat = np.zeros((npulay + 1) * (npulay + 1))   # column-major, ld npulay + 1
+        nb = int(lib().mb_pulay_ws_bytes(n))
+        self.ws = torch.empty(nb // 8 + 32, dtype=torch.float64, device=device)
+        self.lfock = ctypes.c_int(0)
+        self.nfock = ctypes.c_int(0)
+        self.start = ctypes.c_int(1)
+
+    def step(self, f, p) -> float:
+        pl = ctypes.c_double(0.0)
+        base = self.ws.data_ptr()
+        ws = ctypes.c_void_p((base + 255) & ~255)
+        check(lib().mb_pulay_ws(self.n, _ptr(f), _ptr(p), _ptr(self.fppf), _ptr(self.fock), self.mfock,
+                                self.emat.ctypes.data, self.mfock + 1, ctypes.byref(self.lfock),
+                                ctypes.byref(self.nfock), ctypes.byref(self.start), ctypes.byref(pl), ws,
+                                _stream()))
+        return pl.value
+
+
 def density(c, nocc: int, occ: float = 2.0):
     """c: (n, n) column-major, i.e. a torch tensor whose .T is contiguous."""
     n = c.shape[0]

@@ -32,6 +32,7 @@ class ScfResult:
     t_density_ms: float
     t_other_ms: float
     t_total_ms: float
+    n_pulay: int = 0
 
 
 class ScfContext:
@@ -67,7 +68,7 @@ class ScfContext:
 
     # -- SCF
     def run(self, pseudo: bool = False, scfcrt: float = 1.0e-4, itrmax: int = 2000, precision: int = 0,
-            switch_pl: float = 1.0e-4, verbose: bool = False) -> ScfResult:
+            switch_pl: float = 1.0e-4, verbose: bool = False, pulay: bool = False) -> ScfResult:
         o = ScfOpts()
         lib().mb_scf_opts_default(ctypes.byref(o))
         o.pseudo = int(pseudo)
@@ -76,10 +77,11 @@ class ScfContext:
         o.precision = precision
         o.switch_pl = switch_pl
         o.verbose = int(verbose)
+        o.pulay = int(pulay)
         r = ScfRes()
         check(lib().mb_scf_run(self._h, ctypes.byref(o), ctypes.byref(r)))
         return ScfResult(r.escf, r.ee, r.niter, bool(r.converged), r.n_full_diag, r.n_pseudo_diag, r.pl,
-                         r.t_fock_ms, r.t_diag_ms, r.t_density_ms, r.t_other_ms, r.t_total_ms)
+                         r.t_fock_ms, r.t_diag_ms, r.t_density_ms, r.t_other_ms, r.t_total_ms, r.n_pulay)
 
     def density(self) -> np.ndarray:
         p = np.empty(self.mpack)

@@ -229,6 +229,186 @@ def pseudo_diag(f, c, nocc, eig):
     return rotation_sweep(c, fmo, eig, nocc)
 
 
+# ---------------------------------------------------------------- pulay
+def osinv(a: np.ndarray, n: int):
+    """matrix/osinv.F90: in-place Gauss-Jordan inverse with full pivoting of
+    the column-major n x n matrix stored flat in a; returns the clamped
+    determinant d (0 when a pivot falls below 1e-8)."""
+    tol = 1.0e-8
+    d = 1.0
+    L = [0] * (n + 1)
+    M = [0] * (n + 1)
+    A = a  # 1-based helper below
+    def g(i):
+        return A[i - 1]
+    def s_(i, v):
+        A[i - 1] = v
+    nk = -n
+    for k in range(1, n + 1):
+        nk = nk + n
+        L[k] = k
+        M[k] = k
+        kk = nk + k
+        biga = g(kk)
+        for j in range(k, n + 1):
+            iz = n * (j - 1)
+            for i in range(k, n + 1):
+                ij = iz + i
+                if abs(biga) - abs(g(ij)) >= 0.0:
+                    continue
+                biga = g(ij)
+                L[k] = i
+                M[k] = j
+        j = L[k]
+        if j - k > 0:
+            ki = k - n
+            for i in range(1, n + 1):
+                ki = ki + n
+                holo = -g(ki)
+                ji = ki - k + j
+                s_(ki, g(ji))
+                s_(ji, holo)
+        i = M[k]
+        if i - k > 0:
+            jp = n * (i - 1)
+            for j in range(1, n + 1):
+                jk = nk + j
+                ji = jp + j
+                holo = -g(jk)
+                s_(jk, g(ji))
+                s_(ji, holo)
+        if abs(biga) - tol < 0.0:
+            return 0.0
+        for i in range(1, n + 1):
+            if i - k == 0:
+                continue
+            ik = nk + i
+            s_(ik, g(ik) / (-biga))
+        for i in range(1, n + 1):
+            ik = nk + i
+            ij = i - n
+            if i - k != 0:
+                for j in range(1, n + 1):
+                    ij = ij + n
+                    if j - k == 0:
+                        continue
+                    kj = ij - i + k
+                    s_(ij, g(ik) * g(kj) + g(ij))
+        kj = k - n
+        for j in range(1, n + 1):
+            kj = kj + n
+            if j - k == 0:
+                continue
+            s_(kj, g(kj) / biga)
+        d = min(d * biga, 1.0e10)
+        s_(kk, 1.0 / biga)
+    k = n
+    while True:
+        k = k - 1
+        if k <= 0:
+            break
+        i = L[k]
+        if i - k > 0:
+            jq = n * (k - 1)
+            jr = n * (i - 1)
+            for j in range(1, n + 1):
+                jk = jq + j
+                holo = g(jk)
+                ji = jr + j
+                s_(jk, -g(ji))
+                s_(ji, holo)
+        j = M[k]
+        if j - k <= 0:
+            continue
+        ki = k - n
+        for i in range(1, n + 1):
+            ki = ki + n
+            holo = g(ki)
+            ji = ki + j - k
+            s_(ki, -g(ji))
+            s_(ji, holo)
+    return d
+
+
+class PulayState:
+    """Storage iter hands to pulay (SCF/pulay.F90:16).  As in the reference
+    (setup_mopac_arrays.F90:148, iter.F90:826-831) the commutator history is
+    ``pold`` and the Fock history is ``pold2``, both npulay*mpack long: slot l
+    of the commutators is the planar block fppf[l*linear:(l+1)*linear], entry
+    i of Fock slot l sits at fock[l + i*mfock] (interleaved).  iter's cnvg
+    uses the first mpack (resp. norbs) elements of the same two arrays."""
+
+    def __init__(self, n: int, npulay: int = 10):
+        self.n = n
+        self.linear = n * (n + 1) // 2
+        self.mfock = npulay
+        self.fppf = np.zeros(npulay * self.linear)
+        self.fock = np.zeros(npulay * self.linear)
+        self.emat = np.zeros((npulay + 1, npulay + 1))
+        self.start = True
+        self.lfock = 0
+        self.nfock = 0
+
+
+def commutator_packed(p: np.ndarray, f: np.ndarray, n: int) -> np.ndarray:
+    """sym_commute + pack_matrix (SCF/pulay.F90:219-247, 181-191): M = P F,
+    element (i, j), i <= j, becomes M(i, j) - M(j, i), packed 'U' by columns
+    (the same index as MOPAC's lower-triangle-by-rows layout)."""
+    P = unpack(p, n)
+    F = unpack(f, n)
+    m = P @ F
+    r, c = tri_index(n)          # r >= c: packed slot of (row c, col r) in 'U'
+    return np.ascontiguousarray(m[c, r] - m[r, c])
+
+
+def pulay(st: PulayState, f: np.ndarray, p: np.ndarray):
+    """SCF/pulay.F90:16-180.  f is replaced by the extrapolated Fock matrix
+    when at least two entries are stored; returns pl = |[P,F]|^2 / linear."""
+    lin = st.linear
+    if st.start:
+        st.nfock = 1
+        st.lfock = 1
+        st.start = False
+    else:
+        if st.nfock < st.mfock:
+            st.nfock += 1
+        st.lfock = st.lfock + 1 if st.lfock != st.mfock else 1
+    l0 = st.lfock - 1
+    st.fock[l0::st.mfock][:lin] = f[:lin]
+    st.fppf[l0 * lin:(l0 + 1) * lin] = commutator_packed(p, f, st.n)
+    nf = st.nfock
+    e = st.emat
+    cur = st.fppf[l0 * lin:(l0 + 1) * lin]
+    for i in range(nf):
+        e[nf, i] = -1.0
+        e[i, nf] = -1.0
+        e[l0, i] = float(np.dot(st.fppf[i * lin:(i + 1) * lin], cur))
+        e[i, l0] = e[l0, i]
+    pl = e[l0, l0] / lin
+    e[nf, nf] = 0.0
+    if e[l0, l0] < 1.0e-20:
+        return pl
+    const = 1.0 / e[l0, l0]
+    e[:nf, :nf] *= const
+    ev = list(e[:nf + 1, :nf + 1].ravel())   # row i of emat -> column i of evec
+    const = 1.0 / const
+    e[:nf, :nf] *= const
+    d = osinv(ev, nf + 1)
+    if abs(d) < 1.0e-6:
+        st.start = True
+        return pl
+    if nf < 2:
+        return pl
+    il = nf * (nf + 1)
+    coeffs = [-ev[il + j] for j in range(nf)]
+    hist = st.fock[:lin * st.mfock].reshape(lin, st.mfock)
+    out = np.zeros(lin)
+    for j in range(nf):
+        out = out + coeffs[j] * hist[:, j]
+    f[:lin] = out
+    return pl
+
+
 # ---------------------------------------------------------------- iter
 @dataclass
 class ScfResult:
@@ -243,7 +423,7 @@ class ScfResult:
 
 
 def iter_scf(s: System, pseudo: bool = False, scfcrt: float = 1.0e-4, itrmax: int = 2000,
-             gnorm: float = 0.0, trace: bool = False) -> ScfResult:
+             gnorm: float = 0.0, trace: bool = False, pulay_on: bool = False) -> ScfResult:
     """Closed-shell restatement of iter (SCF/iter.F90), 1SCF settings
     (last = 1, nscf = 0, fulscf = .true.)."""
     n = s.norbs
@@ -264,7 +444,8 @@ def iter_scf(s: System, pseudo: bool = False, scfcrt: float = 1.0e-4, itrmax: in
     shftbo = 0.0
     shiftb = 0.0
     oknewd = abs(bshift) < 0.001
-    okpuly = False
+    okpuly = pulay_on
+    pst = PulayState(s.norbs) if pulay_on else None
     halfe = False
     camkin = False
     trans = 0.2
@@ -281,8 +462,15 @@ def iter_scf(s: System, pseudo: bool = False, scfcrt: float = 1.0e-4, itrmax: in
         p[j] = s.pdiag[i]
         pa[j] = p[j] * w1 * random
         random = 1.0 / random
-    pold = pa.copy()
-    pold2 = pold[dix].copy()
+    if pst is not None:
+        # pold and pold2 are the heads of pulay's two history arrays
+        pold = pst.fppf[:mpack]
+        pold[:] = pa
+        pold2 = pst.fock[:n]
+        pold2[:] = pold[dix]
+    else:
+        pold = pa.copy()
+        pold2 = pold[dix].copy()
     gs = True
     selcon = scfcrt
     if gs:
@@ -369,12 +557,15 @@ def iter_scf(s: System, pseudo: bool = False, scfcrt: float = 1.0e-4, itrmax: in
         eold = escf
         if trace:
             history.append(dict(niter=niter, escf=escf, pl=pl, shift=shift, newdg=newdg))
+        if newdg and okpuly and iredy > 1:
+            pl = pulay(pst, f, pa)
         if newdg and pseudo and not (halfe or camkin):
             pseudo_diag(f, c, na1el, eigs)
         else:
             c, eigs = eigenvectors_lapack(f, n)
         p = density(c, nclose)
-        pl = cnvg(n, p, pold, pold2, niter)
+        if not (newdg and okpuly):
+            pl = cnvg(n, p, pold, pold2, niter)
         pa = p * 0.5
         oknewd = pl < sellim or oknewd
         newdg = (pl < trans and oknewd) or newdg
