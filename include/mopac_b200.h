@@ -80,8 +80,10 @@ typedef struct mb_scf_opts {
                         diagonalisation every iteration like the fork     */
   int itrmax;        /* iteration cap (ITRY), reference default 2000      */
   double scfcrt;     /* SCF criterion, reference default 1e-4 kcal/mol    */
-  int precision;     /* 0: all FP64; 1: split-precision GEMMs until
-                        max|dP| < switch_pl, FP64 after                   */
+  int precision;     /* 0: all FP64; 1: density and Fmo GEMMs in split BF16
+                        precision on the tensor cores until max|dP| <
+                        switch_pl, FP64 after (convergence is only
+                        declared in FP64)                                 */
   double switch_pl;  /* precision switch threshold (default 1e-4)         */
   int verbose;       /* print one line per iteration to stderr            */
   int pulay;         /* 1: Pulay's converger once newdg is set, like the
@@ -101,6 +103,8 @@ typedef struct mb_scf_result {
   double t_fock_ms, t_diag_ms, t_density_ms, t_other_ms; /* device-timed  */
   double t_total_ms; /* CUDA events on the context stream around the SCF   */
   int n_pulay;       /* Pulay extrapolation steps taken                    */
+  int n_split;       /* iterations whose density / Fmo GEMMs ran in the
+                        split BF16 precision (opts.precision = 1)          */
 } mb_scf_result;
 
 void mb_scf_opts_default(mb_scf_opts* o);
@@ -185,6 +189,22 @@ int mb_pulay_ws(int n, double* f, const double* p, double* fppf, double* fock, i
  * pivoting of the column-major n x n host matrix a; returns d (0 when a pivot
  * is below 1e-8). */
 double mb_osinv(double* a, int n);
+
+/* Split-precision GEMM on the tcgen05 tensor cores: C = alpha*op(A)*op(B) +
+ * beta*C (column-major, BLAS argument meaning), each FP64 operand split into
+ * two BF16 planes and three BF16 products accumulated in FP32 (relative error
+ * ~1e-5 of |A||B|).  ws: device, 1024-byte aligned, mb_gemm_split_ws_bytes
+ * bytes.  err_dev: device int the kernel sets to 1 if a pipeline wait ran out
+ * (results are then not written); the caller zeroes and reads it. */
+size_t mb_gemm_split_ws_bytes(int m, int n, int k);
+int mb_gemm_split_ws(char transa, char transb, int m, int n, int k, double alpha, const double* a,
+                     int lda, const double* b, int ldb, double beta, double* c, int ldc, void* ws,
+                     size_t ws_bytes, int* err_dev, cudaStream_t stream);
+/* Density with the same split arithmetic: packed P = occ * C_occ C_occ^T
+ * (lower tiles only, written straight into the packed layout). */
+size_t mb_density_split_ws_bytes(int n, int nocc);
+int mb_density_split_ws(int n, int nocc, double occ, const double* c, int ldc, double* p, void* ws,
+                        size_t ws_bytes, int* err_dev, cudaStream_t stream);
 
 /* P (packed) = occ * C[:, 0:nocc] C[:, 0:nocc]^T, FP64. */
 int mb_density_dev(int n, int nocc, double occ, const double* c, int ldc, double* p,

@@ -38,7 +38,7 @@ class ScfRes(ctypes.Structure):
                 ("converged", ctypes.c_int), ("n_full_diag", ctypes.c_int), ("n_pseudo_diag", ctypes.c_int),
                 ("pl", ctypes.c_double), ("t_fock_ms", ctypes.c_double), ("t_diag_ms", ctypes.c_double),
                 ("t_density_ms", ctypes.c_double), ("t_other_ms", ctypes.c_double), ("t_total_ms", ctypes.c_double),
-                ("n_pulay", ctypes.c_int)]
+                ("n_pulay", ctypes.c_int), ("n_split", ctypes.c_int)]
 
 
 _lib = None
@@ -80,6 +80,10 @@ SIGNATURES = {
     "mb_pulay_ws_bytes": ([_I], ctypes.c_size_t),
     "mb_pulay_ws": ([_I, _P, _P, _P, _P, _I, _P, _I, _P, _P, _P, _P, _P, _P], _I),
     "mb_osinv": ([_P, _I], _D),
+    "mb_gemm_split_ws_bytes": ([_I, _I, _I], ctypes.c_size_t),
+    "mb_gemm_split_ws": ([_C, _C, _I, _I, _I, _D, _P, _I, _P, _I, _D, _P, _I, _P, ctypes.c_size_t, _P, _P], _I),
+    "mb_density_split_ws_bytes": ([_I, _I], ctypes.c_size_t),
+    "mb_density_split_ws": ([_I, _I, _D, _P, _I, _P, _P, ctypes.c_size_t, _P, _P], _I),
     "mb_eigh_packed_dev": ([_I, _P, _P, _P, _P], _I),
     "mb_pseudo_diag_dev": ([_I, _I, _P, _P, _P, ctypes.POINTER(_LL), _P], _I),
     "mb_dgemm_dev": ([_C, _C, _I, _I, _I, _D, _P, _I, _P, _I, _D, _P, _I, _P], _I),

@@ -31,6 +31,13 @@ extern "C" int mb_eigh_ws(int n, double* fpacked, int perturb, double* c, double
 extern "C" size_t mb_pseudo_ws_bytes(int n, int nocc);
 extern "C" int mb_pseudo_diag_ws(int n, int nocc, const double* fpacked, double* c, const double* eigs,
                                  unsigned long long* nrot_dev, void* ws, cudaStream_t stream);
+extern "C" int mb_pseudo_diag_ex(int n, int nocc, const double* fpacked, double* c, const double* eigs,
+                                 unsigned long long* nrot_dev, void* ws, void* split_ws, size_t split_ws_bytes,
+                                 int* split_err, cudaStream_t stream);
+extern "C" size_t mb_gemm_split_ws_bytes(int m, int n, int k);
+extern "C" size_t mb_density_split_ws_bytes(int n, int nocc);
+extern "C" int mb_density_split_ws(int n, int nocc, double occ, const double* c, int ldc, double* p, void* ws,
+                                   size_t ws_bytes, int* err_dev, cudaStream_t stream);
 extern "C" size_t mb_pulay_ws_bytes(int n);
 extern "C" int mb_pulay_ws(int n, double* f, const double* p, double* fppf, double* fock, int mfock, double* emat,
                            int ldemat, int* lfock, int* nfock, int* start, double* pl, void* ws, cudaStream_t stream);
@@ -142,6 +149,10 @@ struct mb_ctx {
   void* pseudo_ws = nullptr;
   // Pulay histories (npulay * mpack each), allocated on the first Pulay run
   double *fppf_hist = nullptr, *fock_hist = nullptr;
+  // BF16 plane buffers of the split-precision GEMMs, allocated on first use
+  void* tc_ws_raw = nullptr;
+  void* tc_ws = nullptr;     // 1024-byte aligned inside tc_ws_raw
+  size_t tc_ws_bytes = 0;
   cudaStream_t stream = nullptr;
 };
 
@@ -153,7 +164,7 @@ static void ctx_free(mb_ctx* c) {
   mb_atoms_destroy(&c->atoms);
   void* ptrs[] = {c->d_nat, c->d_coord, c->h, c->w, c->f, c->p, c->pa, c->pold, c->pold2, c->c, c->eigs,
                   c->fdiag, c->scal, c->hws, c->status, c->nrot, c->eig_ws, c->pseudo_ws,
-                  c->fppf_hist, c->fock_hist};
+                  c->fppf_hist, c->fock_hist, c->tc_ws_raw};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -410,6 +421,25 @@ extern "C" int mb_scf_run(mb_ctx* c, const mb_scf_opts* opts_in, mb_scf_result* 
   double* pold2 = okpuly ? c->fock_hist : c->pold2;
   std::vector<double> emat((size_t)(kNpulay + 1) * (kNpulay + 1), 0.0);
   int lfock = 0, nfock = 0, frst = 1;
+  // Split precision: density and Fmo GEMMs on the tensor cores until pl falls
+  // below switch_pl; convergence is only accepted once FP64 has taken over.
+  bool use_split = opts.precision != 0 && nclose > 0 && nclose < n;
+  if (use_split) {
+    const int nv = n - nclose, kmin = nclose < nv ? nclose : nv;
+    size_t need = mb_density_split_ws_bytes(n, nclose);
+    size_t g1 = mb_gemm_split_ws_bytes(n, kmin, n), g2 = mb_gemm_split_ws_bytes(nv, nclose, n);
+    if (g1 > need) need = g1;
+    if (g2 > need) need = g2;
+    if (need > c->tc_ws_bytes) {
+      if (c->tc_ws_raw) cudaFree(c->tc_ws_raw);
+      c->tc_ws_raw = c->tc_ws = nullptr;
+      c->tc_ws_bytes = 0;
+      MB_CUDA(cudaMalloc(&c->tc_ws_raw, need + 1024));
+      c->tc_ws = (void*)(((uintptr_t)c->tc_ws_raw + 1023) & ~(uintptr_t)1023);
+      c->tc_ws_bytes = need;
+    }
+    MB_CUDA(cudaMemsetAsync(c->status + 1, 0, sizeof(int), s));
+  }
   PhaseTimer t_fock(s), t_diag(s), t_dens(s);
   cudaEvent_t ev_begin, ev_end;
   MB_CUDA(cudaEventCreate(&ev_begin));
@@ -508,7 +538,11 @@ extern "C" int mb_scf_run(mb_ctx* c, const mb_scf_opts* opts_in, mb_scf_result* 
       if (diff > 0) ten = ten - 1.0;
       else ten = ten * 0.975 + 0.05;
       sellim = fmax(selcon, 1.0e-15 * fmax(fabs(ee), 1.0));
-      const bool conv = niter > 4 && (pl == 0.0 || (pl < pltest && fabs(diff) < sellim)) && ready;
+      bool conv = niter > 4 && (pl == 0.0 || (pl < pltest && fabs(diff) < sellim)) && ready;
+      if (conv && use_split) {  // finish in FP64 before accepting convergence
+        use_split = false;
+        conv = false;
+      }
       if (conv) {
         if (fabs(shift) < 1.0e-10) { converged = true; break; }
         shift = 0.0;
@@ -534,7 +568,8 @@ extern "C" int mb_scf_run(mb_ctx* c, const mb_scf_opts* opts_in, mb_scf_result* 
     t_diag.start();
     if (newdg && opts.pseudo && !(halfe || camkin)) {
       mb_kstat_mark(MB_KSTAT_PSEUDO, s, true);
-      MB_TRY(mb_pseudo_diag_ws(n, na1el, c->f, c->c, c->eigs, c->nrot, c->pseudo_ws, s));
+      MB_TRY(mb_pseudo_diag_ex(n, na1el, c->f, c->c, c->eigs, c->nrot, c->pseudo_ws, use_split ? c->tc_ws : nullptr,
+                               c->tc_ws_bytes, c->status + 1, s));
       mb_kstat_mark(MB_KSTAT_PSEUDO, s, false);
       res->n_pseudo_diag++;
     } else {
@@ -543,13 +578,25 @@ extern "C" int mb_scf_run(mb_ctx* c, const mb_scf_opts* opts_in, mb_scf_result* 
     }
     t_diag.stop();
     t_dens.start();
-    MB_TRY(mb_density_dev(n, nclose, 2.0, c->c, n, c->p, s));
+    if (use_split) {
+      MB_TRY(mb_density_split_ws(n, nclose, 2.0, c->c, n, c->p, c->tc_ws, c->tc_ws_bytes, c->status + 1, s));
+      res->n_split++;
+    } else {
+      MB_TRY(mb_density_dev(n, nclose, 2.0, c->c, n, c->p, s));
+    }
     const bool do_cnvg = !(newdg && okpuly);  // iter.F90:899
     if (do_cnvg) MB_TRY(mb_cnvg_ws(n, c->p, pold, pold2, niter, c->scal + 1, c->scal + 8, s));
     half_kernel<<<hblocks, 256, 0, s>>>(mpack, c->p, c->pa);
     MB_LAUNCH_CHECK();
     t_dens.stop();
     if (do_cnvg) MB_TRY(d2h(c, &pl, c->scal + 1, 1));
+    if (opts.precision != 0 && res->n_split > 0) {
+      int terr = 0;
+      MB_CUDA(cudaMemcpyAsync(&terr, c->status + 1, sizeof(int), cudaMemcpyDeviceToHost, s));
+      MB_CUDA(cudaStreamSynchronize(s));
+      if (terr) return mb_set_error(MB_ERR_CUDA, "tensor-core GEMM pipeline wait expired");
+    }
+    if (use_split && pl < opts.switch_pl) use_split = false;
     if (!isfinite(pl)) return mb_set_error(MB_ERR_NUMERIC, "non-finite density change");
     oknewd = pl < sellim || oknewd;
     newdg = (pl < trans && oknewd) || newdg;

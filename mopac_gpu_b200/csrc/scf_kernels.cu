@@ -390,8 +390,15 @@ extern "C" size_t mb_pseudo_ws_bytes(int n, int nocc) {
   return b;
 }
 
-extern "C" int mb_pseudo_diag_ws(int n, int nocc, const double* fpacked, double* c, const double* eigs,
-                                 unsigned long long* nrot_dev, void* ws, cudaStream_t stream) {
+extern "C" int mb_gemm_split_ws(char transa, char transb, int m, int n, int k, double alpha, const double* a, int lda,
+                                const double* b, int ldb, double beta, double* c, int ldc, void* ws, size_t ws_bytes,
+                                int* err_dev, cudaStream_t stream);
+
+// The Fmo GEMMs run in FP64, or -- when split_ws is given -- with the
+// three-product BF16 split on the tensor cores (mb_gemm_split_ws).
+extern "C" int mb_pseudo_diag_ex(int n, int nocc, const double* fpacked, double* c, const double* eigs,
+                                 unsigned long long* nrot_dev, void* ws, void* split_ws, size_t split_ws_bytes,
+                                 int* split_err, cudaStream_t stream) {
   const int nvirt = n - nocc;
   if (nocc <= 0 || nvirt <= 0) return MB_OK;
   if (((uintptr_t)ws & 255) != 0) return mb_set_error(MB_ERR_ARG, "pseudo-diag workspace must be 256-byte aligned");
@@ -408,12 +415,19 @@ extern "C" int mb_pseudo_diag_ws(int n, int nocc, const double* fpacked, double*
   unsigned long long* tiny = (unsigned long long*)b;
   MB_TRY(mb_unpack_dev(n, fpacked, ff, n, 0, nullptr, stream));
   // diag_for_GPU.F90:116-150
+  auto gemm = [&](char ta, char tb, int m, int nn, int k, const double* a, int lda, const double* bb, int ldb,
+                  double* cc, int ldc) -> int {
+    if (split_ws)
+      return mb_gemm_split_ws(ta, tb, m, nn, k, 1.0, a, lda, bb, ldb, 0.0, cc, ldc, split_ws, split_ws_bytes, split_err,
+                              stream);
+    return mb_dgemm_dev(ta, tb, m, nn, k, 1.0, a, lda, bb, ldb, 0.0, cc, ldc, stream);
+  };
   if (nocc < nvirt) {
-    MB_TRY(mb_dgemm_dev('N', 'N', n, nocc, n, 1.0, ff, n, c, n, 0.0, fck, n, stream));
-    MB_TRY(mb_dgemm_dev('T', 'N', nvirt, nocc, n, 1.0, c + (size_t)nocc * n, n, fck, n, 0.0, fmo, nvirt, stream));
+    MB_TRY(gemm('N', 'N', n, nocc, n, ff, n, c, n, fck, n));
+    MB_TRY(gemm('T', 'N', nvirt, nocc, n, c + (size_t)nocc * n, n, fck, n, fmo, nvirt));
   } else {
-    MB_TRY(mb_dgemm_dev('N', 'N', n, nvirt, n, 1.0, ff, n, c + (size_t)nocc * n, n, 0.0, fck, n, stream));
-    MB_TRY(mb_dgemm_dev('T', 'N', nvirt, nocc, n, 1.0, fck, n, c, n, 0.0, fmo, nvirt, stream));
+    MB_TRY(gemm('N', 'N', n, nvirt, n, ff, n, c + (size_t)nocc * n, n, fck, n));
+    MB_TRY(gemm('T', 'N', nvirt, nocc, n, fck, n, c, n, fmo, nvirt));
   }
   MB_CUDA(cudaMemsetAsync(tiny, 0, sizeof(unsigned long long), stream));
   MB_CUDA(cudaMemsetAsync(tcnt, 0, sizeof(unsigned int) * (size_t)to * tv, stream));
@@ -425,6 +439,11 @@ extern "C" int mb_pseudo_diag_ws(int n, int nocc, const double* fpacked, double*
   rot_coeff_kernel<<<blocks, 256, 0, stream>>>(nocc, nvirt, fmo, eigs, tiny, -1.0, 1.5e-7, al, be, act, tcnt, nrot_dev, tv);
   MB_LAUNCH_CHECK();
   return launch_wavefronts(n, nocc, nvirt, c, al, be, act, tcnt, to, tv, stream);
+}
+
+extern "C" int mb_pseudo_diag_ws(int n, int nocc, const double* fpacked, double* c, const double* eigs,
+                                 unsigned long long* nrot_dev, void* ws, cudaStream_t stream) {
+  return mb_pseudo_diag_ex(n, nocc, fpacked, c, eigs, nrot_dev, ws, nullptr, 0, nullptr, stream);
 }
 
 // Rotation sweep alone with caller-given Fmo, tiny and bigeps (the arguments

@@ -116,3 +116,45 @@ def pseudo_diag(fpacked, cT, eigs, nocc: int) -> int:
 def dgemm(transa: str, transb: str, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc) -> None:
     check(lib().mb_dgemm_dev(transa.encode(), transb.encode(), m, n, k, alpha, _ptr(a), lda, _ptr(b), ldb, beta,
                              _ptr(c), ldc, _stream()))
+
+
+def _aligned_ws(nbytes: int, device, align: int = 1024):
+    buf = torch.empty(nbytes + align, dtype=torch.uint8, device=device)
+    return buf, ctypes.c_void_p((buf.data_ptr() + align - 1) & ~(align - 1))
+
+
+def matmul_split(a, b, alpha: float = 1.0):
+    """alpha * a @ b for row-major float64 CUDA tensors through the
+    split-precision tensor-core GEMM (mb_gemm_split_ws)."""
+    m, k = a.shape
+    k2, n = b.shape
+    assert k == k2
+    a = a.contiguous()
+    b = b.contiguous()
+    c = torch.empty((m, n), dtype=torch.float64, device=a.device)
+    nb = int(lib().mb_gemm_split_ws_bytes(n, m, k))
+    buf, ws = _aligned_ws(nb, a.device)
+    err = torch.zeros(1, dtype=torch.int32, device=a.device)
+    # row-major C = A B is column-major C^T = B^T A^T
+    check(lib().mb_gemm_split_ws(b"N", b"N", n, m, k, float(alpha), _ptr(b), n, _ptr(a), k, 0.0, _ptr(c), n, ws,
+                                 nb, ctypes.c_void_p(err.data_ptr()), _stream()))
+    if int(err.item()) != 0:
+        raise RuntimeError("tensor-core GEMM pipeline wait expired")
+    del buf
+    return c
+
+
+def density_split(c, nocc: int, occ: float = 2.0):
+    """density() with the split-precision tensor-core product."""
+    n = c.shape[0]
+    ct = c.t().contiguous() if not c.t().is_contiguous() else c.t()
+    p = torch.empty(n * (n + 1) // 2, dtype=torch.float64, device=c.device)
+    nb = int(lib().mb_density_split_ws_bytes(n, nocc))
+    buf, ws = _aligned_ws(nb, c.device)
+    err = torch.zeros(1, dtype=torch.int32, device=c.device)
+    check(lib().mb_density_split_ws(n, nocc, float(occ), ctypes.c_void_p(ct.data_ptr()), n, _ptr(p), ws, nb,
+                                    ctypes.c_void_p(err.data_ptr()), _stream()))
+    if int(err.item()) != 0:
+        raise RuntimeError("tensor-core GEMM pipeline wait expired")
+    del buf
+    return p

@@ -33,6 +33,7 @@ class ScfResult:
     t_other_ms: float
     t_total_ms: float
     n_pulay: int = 0
+    n_split: int = 0
 
 
 class ScfContext:
@@ -81,7 +82,7 @@ class ScfContext:
         r = ScfRes()
         check(lib().mb_scf_run(self._h, ctypes.byref(o), ctypes.byref(r)))
         return ScfResult(r.escf, r.ee, r.niter, bool(r.converged), r.n_full_diag, r.n_pseudo_diag, r.pl,
-                         r.t_fock_ms, r.t_diag_ms, r.t_density_ms, r.t_other_ms, r.t_total_ms, r.n_pulay)
+                         r.t_fock_ms, r.t_diag_ms, r.t_density_ms, r.t_other_ms, r.t_total_ms, r.n_pulay, r.n_split)
 
     def density(self) -> np.ndarray:
         p = np.empty(self.mpack)

@@ -1,0 +1,120 @@
+"""Split-precision tensor-core GEMMs (tcgen05, three BF16 products) and the
+SCF's precision switch.
+
+Tolerance of the split products: |C - C_fp64| <= 1e-4 * (|A| |B|) element by
+element (three BF16 products leave ~2^-16 relative per product; FP32
+accumulation adds ~k 2^-24 in the worst case).  The SCF with the switch on
+takes a different trajectory from the FP64 one, so it lands on the same
+self-consistent state only to within the SCF's own convergence test: heat
+1e-4 kcal/mol, density and orbital energies 1e-4 (the bar the pseudo- and
+full-diagonalisation paths are held to against each other); convergence is
+only accepted after FP64 has taken over.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+from oracle import scf_oracle as so
+from tests.helpers import oracle_system, small_systems
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+SYSTEMS = small_systems()
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _need_gpu():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+
+
+def _dev_colmajor(a):
+    return torch.from_numpy(np.ascontiguousarray(np.asfortranarray(a).ravel(order="F"))).cuda()
+
+
+def _gemm_split(ta, tb, a, b, alpha=1.0, beta=0.0, c0=None):
+    from mopac_gpu_b200._lib import check, lib
+    opa = a.T if ta == "T" else a
+    opb = b.T if tb == "T" else b
+    m, k = opa.shape
+    n = opb.shape[1]
+    da, db = _dev_colmajor(a), _dev_colmajor(b)
+    c = c0 if c0 is not None else np.zeros((m, n))
+    dc = _dev_colmajor(c)
+    nb = int(lib().mb_gemm_split_ws_bytes(m, n, k))
+    buf = torch.empty(nb + 1024, dtype=torch.uint8, device="cuda")
+    ws = ctypes.c_void_p((buf.data_ptr() + 1023) & ~1023)
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    s = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    check(lib().mb_gemm_split_ws(ta.encode(), tb.encode(), m, n, k, alpha, ctypes.c_void_p(da.data_ptr()),
+                                 a.shape[0], ctypes.c_void_p(db.data_ptr()), b.shape[0], beta,
+                                 ctypes.c_void_p(dc.data_ptr()), m, ws, nb, ctypes.c_void_p(err.data_ptr()), s))
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
+    return dc.cpu().numpy().reshape(n, m).T, opa, opb
+
+
+@pytest.mark.parametrize("ta,tb", [("N", "N"), ("T", "N"), ("N", "T"), ("T", "T")])
+@pytest.mark.parametrize("m,n,k", [(128, 128, 64), (200, 77, 130), (1, 300, 5), (513, 257, 1000)])
+def test_gemm_split_matches_fp64(ta, tb, m, n, k):
+    rng = np.random.default_rng(m * 7 + n * 3 + k)
+    a = rng.normal(size=(k, m) if ta == "T" else (m, k))
+    b = rng.normal(size=(n, k) if tb == "T" else (k, n))
+    c, opa, opb = _gemm_split(ta, tb, a, b, alpha=0.75)
+    ref = 0.75 * opa @ opb
+    bound = 1e-4 * 0.75 * (np.abs(opa) @ np.abs(opb)) + 1e-12
+    assert np.all(np.abs(c - ref) <= bound)
+
+
+def test_gemm_split_beta_accumulates():
+    rng = np.random.default_rng(11)
+    a, b, c0 = rng.normal(size=(150, 90)), rng.normal(size=(90, 140)), rng.normal(size=(150, 140))
+    c, opa, opb = _gemm_split("N", "N", a, b, alpha=2.0, beta=-0.5, c0=c0)
+    ref = 2.0 * a @ b - 0.5 * c0
+    assert np.all(np.abs(c - ref) <= 2e-4 * (np.abs(a) @ np.abs(b)) + 1e-12)
+
+
+@pytest.mark.parametrize("n,nocc", [(96, 64), (300, 131), (1000, 700), (3072, 2048)])
+def test_density_split_matches_fp64(n, nocc):
+    from mopac_gpu_b200 import kernels
+    rng = np.random.default_rng(n)
+    q, _ = np.linalg.qr(rng.normal(size=(n, n)))
+    c = torch.from_numpy(np.ascontiguousarray(q)).cuda()          # row-major storage of C
+    cc = c.t().contiguous().t()                                    # column-major view
+    p64 = kernels.density(cc, nocc).cpu().numpy()
+    psp = kernels.density_split(cc, nocc).cpu().numpy()
+    co = q[:, :nocc]
+    ref = so.pack(2.0 * co @ co.T)
+    np.testing.assert_allclose(p64, ref, atol=1e-12)
+    bound = so.pack(1e-4 * 2.0 * np.abs(co) @ np.abs(co).T) + 1e-12
+    assert np.all(np.abs(psp - ref) <= bound)
+
+
+def test_matmul_split_wrapper():
+    from mopac_gpu_b200 import kernels
+    rng = np.random.default_rng(2)
+    a, b = rng.normal(size=(64, 33)), rng.normal(size=(33, 250))
+    c = kernels.matmul_split(torch.from_numpy(a).cuda(), torch.from_numpy(b).cuda()).cpu().numpy()
+    assert np.all(np.abs(c - a @ b) <= 1e-4 * (np.abs(a) @ np.abs(b)) + 1e-12)
+
+
+@pytest.mark.parametrize("name", ["water16", "propane", "heptane"])
+@pytest.mark.parametrize("pseudo", [False, True])
+def test_split_precision_scf_lands_on_fp64_oracle(name, pseudo):
+    from mopac_gpu_b200 import ScfContext
+    nat, xyz = SYSTEMS[name]
+    s = oracle_system(nat, xyz)
+    ref = so.iter_scf(s, pseudo=pseudo)
+    ctx = ScfContext(nat, xyz)
+    ctx.set_hw(s.h, s.w, s.enuclr)
+    r = ctx.run(pseudo=pseudo, precision=1, switch_pl=1e-4)
+    p = ctx.density()
+    _, e = ctx.vectors()
+    ctx.close()
+    assert r.converged and r.n_split > 0
+    print(f"{name} pseudo={pseudo}: dHf {r.escf - ref.escf:.2e} kcal/mol, max|dP| {np.abs(p - ref.p).max():.2e}, "
+          f"max|de| {np.abs(e - ref.eigs).max():.2e} eV, split iterations {r.n_split} of {r.niter}")
+    assert abs(r.escf - ref.escf) < 1e-4
+    np.testing.assert_allclose(p, ref.p, atol=1e-4)
+    np.testing.assert_allclose(e, ref.eigs, atol=1e-4)
