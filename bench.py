@@ -9,12 +9,18 @@ between steps anyway).  The headline metric is SCF single points per second
 (whole job); scf_wall_s is the time of one SCF.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--mode fast|plain]
-                  [--impl mine|reference]
+                  [--precision split|fp64] [--impl mine|reference]
 
 --mode fast   pseudo-diagonalisation once the reference's newdg switch is set
               (the path the reference comments out), full FP64 eigensolves
               otherwise -- the product path.
 --mode plain  full FP64 eigensolve every iteration, like the fork's iter.
+--precision split (default) density and Fmo GEMMs as three BF16 products on
+              the tensor cores until max|dP| < 1e-4, FP64 after (convergence
+              is only accepted in FP64); fp64: FP64 throughout.  The line
+              states |dHf| of the timed SCF against the FP64 SCF and the time
+              of the plain FP64 path (full eigensolve every iteration, FP64
+              GEMMs) on the same box.
 --impl reference
               times the CPU implementation of the same SCF (the oracle's C
               kernels with LAPACK dsyevd through numpy) on the host cores on a
@@ -50,6 +56,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--mode", choices=["fast", "plain"], default="fast")
+    ap.add_argument("--precision", choices=["split", "fp64"], default="split")
     ap.add_argument("--impl", choices=["mine", "reference"], default="mine")
     ap.add_argument("--nwater", type=int, default=512)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -186,6 +193,7 @@ def run_mine(args):
     L = lib()
     nat, xyz, edge = workloads.water_box(args.nwater)
     pseudo = args.mode == "fast"
+    prec = 1 if args.precision == "split" else 0
     ctx = ScfContext(nat, xyz)
     ctx.hcore()
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
@@ -196,7 +204,7 @@ def run_mine(args):
             dist.barrier()
 
     for _ in range(args.warmup):
-        r = ctx.run(pseudo=pseudo)
+        r = ctx.run(pseudo=pseudo, precision=prec)
     # ---- timed region (device-resident inputs)
     clocks = ClockSampler(local)
     barrier()
@@ -209,7 +217,7 @@ def run_mine(args):
     for _ in range(args.steps):
         flush.fill_(1.0)
         torch.cuda.synchronize()
-        r = ctx.run(pseudo=pseudo)
+        r = ctx.run(pseudo=pseudo, precision=prec)
         times.append(r.t_total_ms)
         results.append(r)
     barrier()
@@ -240,7 +248,7 @@ def run_mine(args):
             barrier()
             t0 = time.perf_counter()
             L.mb_ctx_set_hw(ctx._h, hp.data_ptr(), wp.data_ptr(), enuc)
-            rr = ctx.run(pseudo=pseudo)
+            rr = ctx.run(pseudo=pseudo, precision=prec)
             L.mb_ctx_get_density(ctx._h, pout.data_ptr())
             torch.cuda.synchronize()
             if step > 0:
@@ -256,6 +264,19 @@ def run_mine(args):
     # recorded on its stream inside the timed region, and the Fock build
     roof = panel_roofline(ctx, kst)
     roof_fock = fock_roofline(ctx)
+    # ---- the plain FP64 GPU path on the same input (reference point of the
+    # metric) and |dHf| of the timed SCF against FP64
+    plain_ms = []
+    r64 = None
+    for i in range(3):
+        flush.fill_(1.0)
+        torch.cuda.synchronize()
+        rp = ctx.run(pseudo=False, precision=0)
+        if i > 0:
+            plain_ms.append(rp.t_total_ms)
+        r64 = rp
+    plain = {"scf_wall_s": statistics.mean(plain_ms) / 1000.0, "niter": r64.niter, "escf_kcal_mol": r64.escf,
+             "mode": "full FP64 eigensolve every iteration, FP64 GEMMs", "steps": len(plain_ms)}
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         os.environ.setdefault("OPENBLAS_NUM_THREADS", str(os.cpu_count()))
@@ -268,16 +289,22 @@ def run_mine(args):
         line = {
             "metric": METRIC, "value": ws * 1000.0 / t_ms, "unit": "SCF/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_ms, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded water box, random sequential insertion)",
-            "config": {"workload": WORKLOAD, "mode": args.mode, "parallelism": f"replicas x{ws}",
+            "vs_baseline": None, "dtype": "f64" if prec == 0 else "f64+bf16x3",
+            "data": "synthetic (seeded water box, random sequential insertion)",
+            "config": {"workload": WORKLOAD, "mode": args.mode, "precision": args.precision,
+                       "parallelism": f"replicas x{ws}",
                        "l2": "flushed between steps (256 MB write); W = 151 MB > L2",
                        "cell_edge_A": round(edge, 3)},
             "scf_wall_s": t_ms / 1000.0,
             "scf": {"escf_kcal_mol": r.escf, "niter": r.niter, "full_diag": r.n_full_diag,
-                    "pseudo_diag": r.n_pseudo_diag, "converged": r.converged,
+                    "pseudo_diag": r.n_pseudo_diag, "split_iterations": r.n_split, "converged": r.converged,
+                    "abs_dHf_vs_fp64_kcal_mol": abs(r.escf - r64.escf),
                     "phase_ms": {"fock": r.t_fock_ms, "diag": r.t_diag_ms, "density_cnvg": r.t_density_ms,
                                  "other": r.t_other_ms}},
-            "gpu_launches": int(launches // max(1, args.steps)),
+            "plain_fp64_gpu": plain,
+            "speedup_vs_plain_fp64": plain["scf_wall_s"] / (t_ms / 1000.0),
+            "gpu_launches": int(launches),
+            "gpu_launches_per_step": int(launches // max(1, args.steps)),
             "clocks": clk,
             "roofline": roof,
             "roofline_fock": roof_fock,
