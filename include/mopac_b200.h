@@ -206,6 +206,64 @@ size_t mb_density_split_ws_bytes(int n, int nocc);
 int mb_density_split_ws(int n, int nocc, double occ, const double* c, int ldc, double* p, void* ws,
                         size_t ws_bytes, int* err_dev, cudaStream_t stream);
 
+/* ------------------------------------------------ MOZYME (sparse blocks) */
+/* Pair-block storage of P, H, F (MOZYME/fillij.F90:20-230, first call,
+ * molecular): for atom i in order, partners j < i with r^2 < cutof2 (block
+ * iorbs(i) x iorbs(j), i's orbitals outer), then i's lower triangle.  Device
+ * arrays; pair entries of atom i are pair_ptr[i] .. pair_ptr[i+1]-1, partners
+ * ascending, the diagonal block last; pair_off = the reference's nijbo. */
+typedef struct MbMzLayout {
+  int numat;
+  long long mpack, npairs;
+  const int* iorbs;
+  const int* pair_ptr;
+  const int* pair_i;
+  const int* pair_j;
+  const long long* pair_off;
+} MbMzLayout;
+/* Occupied LMOs on the device: cocc as in MOZYME_C plus, per atom, the LMOs
+ * containing it (ascending) and the offset of its coefficients in cocc. */
+typedef struct MbMzLmos {
+  int nlmo;
+  const int* atom_ptr;
+  const int* atom_lmo;
+  const int* atom_coff;
+  const double* cocc;
+} MbMzLmos;
+/* Builds the layout (host coordinates in Angstrom, cutoffs squared, as
+ * cutof1/cutof2 in fillij); nijbo (optional, host numat x numat) receives the
+ * reference's table: offset, -2 (cutof2 <= r^2 < cutof1) or -1. */
+int mb_mz_layout_create(int numat, const int* iorbs, const double* coord, double cutof1, double cutof2,
+                        MbMzLayout* out, long long* nijbo);
+int mb_mz_layout_destroy(MbMzLayout* layout);
+/* idiag (host, norbs): 1-based position of each orbital's diagonal element,
+ * as iter_for_MOZYME.F90:183-190. */
+int mb_mz_idiag(const MbMzLayout* layout, long long* idiag);
+/* Uploads LMOs given in the reference's arrays (host; icocc 1-based atoms,
+ * nncf/ncocc 0-based starts). */
+int mb_mz_lmos_create(int numat, const int* iorbs, int nlmo, const int* ncf, const int* nncf,
+                      const int* icocc, const int* ncocc, const double* cocc, long long ncocc_total,
+                      MbMzLmos* out);
+int mb_mz_lmos_destroy(MbMzLmos* lmos);
+/* density_for_MOZYME(p, mode, nclose, partp) (MOZYME/density_for_MOZYME.F90:16):
+ * mode 0: P = 2 sum_LMO c c^T; -1: P = -2 (sum - partp/2); 1: P = 2 (sum +
+ * partp/2); other: P = sum + partp/2.  Bit-identical to the reference's
+ * loop. */
+int mb_mz_density_dev(const MbMzLayout* layout, const MbMzLmos* lmos, int mode, const double* partp,
+                      double* p, cudaStream_t stream);
+/* helecz() (MOZYME/helecz.F90:16): sum p(h+f) with diagonal elements
+ * weighted 1/2; *out (device).  Fixed-order parallel reduction. */
+size_t mb_mz_helecz_ws_bytes(void);
+int mb_mz_helecz_ws(long long mpack, int norbs, const long long* idiag, const double* p,
+                    const double* h, const double* f, double* out, double* ws, cudaStream_t stream);
+/* cnvgz(pnew, p, p1, p2, p3, niter, idiag) (MOZYME/cnvgz.F90:16), device
+ * arrays; use3 = use_three_point_extrap; *pmax_out (device) = max|pnew - p|
+ * before extrapolation.  Bit-identical. */
+size_t mb_mz_cnvgz_ws_bytes(void);
+int mb_mz_cnvgz_ws(int norbs, long long mpack, double* pnew, double* p, double* p1, double* p2,
+                   double* p3, int niter, const long long* idiag, int use3, double* pmax_out, void* ws,
+                   cudaStream_t stream);
+
 /* P (packed) = occ * C[:, 0:nocc] C[:, 0:nocc]^T, FP64. */
 int mb_density_dev(int n, int nocc, double occ, const double* c, int ldc, double* p,
                    cudaStream_t stream);

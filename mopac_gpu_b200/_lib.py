@@ -27,6 +27,17 @@ class MbAtomsDev(ctypes.Structure):
                 ("lim", ctypes.c_void_p), ("wrow", ctypes.c_void_p), ("cum", ctypes.c_void_p)]
 
 
+class MbMzLayout(ctypes.Structure):
+    _fields_ = [("numat", ctypes.c_int), ("mpack", ctypes.c_longlong), ("npairs", ctypes.c_longlong),
+                ("iorbs", ctypes.c_void_p), ("pair_ptr", ctypes.c_void_p), ("pair_i", ctypes.c_void_p),
+                ("pair_j", ctypes.c_void_p), ("pair_off", ctypes.c_void_p)]
+
+
+class MbMzLmos(ctypes.Structure):
+    _fields_ = [("nlmo", ctypes.c_int), ("atom_ptr", ctypes.c_void_p), ("atom_lmo", ctypes.c_void_p),
+                ("atom_coff", ctypes.c_void_p), ("cocc", ctypes.c_void_p)]
+
+
 class ScfOpts(ctypes.Structure):
     _fields_ = [("pseudo", ctypes.c_int), ("itrmax", ctypes.c_int), ("scfcrt", ctypes.c_double),
                 ("precision", ctypes.c_int), ("switch_pl", ctypes.c_double), ("verbose", ctypes.c_int),
@@ -80,6 +91,16 @@ SIGNATURES = {
     "mb_pulay_ws_bytes": ([_I], ctypes.c_size_t),
     "mb_pulay_ws": ([_I, _P, _P, _P, _P, _I, _P, _I, _P, _P, _P, _P, _P, _P], _I),
     "mb_osinv": ([_P, _I], _D),
+    "mb_mz_layout_create": ([_I, _P, _P, _D, _D, ctypes.POINTER(MbMzLayout), _P], _I),
+    "mb_mz_layout_destroy": ([ctypes.POINTER(MbMzLayout)], _I),
+    "mb_mz_idiag": ([ctypes.POINTER(MbMzLayout), _P], _I),
+    "mb_mz_lmos_create": ([_I, _P, _I, _P, _P, _P, _P, _P, _LL, ctypes.POINTER(MbMzLmos)], _I),
+    "mb_mz_lmos_destroy": ([ctypes.POINTER(MbMzLmos)], _I),
+    "mb_mz_density_dev": ([ctypes.POINTER(MbMzLayout), ctypes.POINTER(MbMzLmos), _I, _P, _P, _P], _I),
+    "mb_mz_helecz_ws_bytes": ([], ctypes.c_size_t),
+    "mb_mz_helecz_ws": ([_LL, _I, _P, _P, _P, _P, _P, _P, _P], _I),
+    "mb_mz_cnvgz_ws_bytes": ([], ctypes.c_size_t),
+    "mb_mz_cnvgz_ws": ([_I, _LL, _P, _P, _P, _P, _P, _I, _P, _I, _P, _P, _P], _I),
     "mb_gemm_split_ws_bytes": ([_I, _I, _I], ctypes.c_size_t),
     "mb_gemm_split_ws": ([_C, _C, _I, _I, _I, _D, _P, _I, _P, _I, _D, _P, _I, _P, ctypes.c_size_t, _P, _P], _I),
     "mb_density_split_ws_bytes": ([_I, _I], ctypes.c_size_t),

@@ -1,0 +1,106 @@
+"""MOZYME sparse pair-block kernels on torch CUDA tensors.
+
+Mirrors the reference's MOZYME routines that the SCF loop (iter_for_MOZYME,
+MOZYME/iter_for_MOZYME.F90) calls on the block-sparse P, H and F:
+``density`` = density_for_MOZYME, ``helecz`` = helecz, ``cnvgz`` = cnvgz.
+``Layout`` is fillij's storage, ``Lmos`` the occupied LMOs of MOZYME_C.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import torch
+
+from ._lib import MbMzLayout, MbMzLmos, check, lib
+
+
+def _stream():
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def _ptr(t: torch.Tensor):
+    assert t.is_cuda and t.is_contiguous()
+    return ctypes.c_void_p(t.data_ptr())
+
+
+class Layout:
+    """Pair-block storage for atoms with iorbs orbitals at coord (Angstrom);
+    cutof1, cutof2 squared as in fillij."""
+
+    def __init__(self, iorbs, coord, cutof1: float, cutof2: float, want_nijbo: bool = False):
+        self.iorbs = np.ascontiguousarray(iorbs, np.int32)
+        c = np.ascontiguousarray(coord, np.float64).reshape(-1)
+        n = self.iorbs.size
+        self.nijbo = np.zeros(n * n, np.int64) if want_nijbo else None
+        self.s = MbMzLayout()
+        check(lib().mb_mz_layout_create(n, self.iorbs.ctypes.data, c.ctypes.data, float(cutof1), float(cutof2),
+                                        ctypes.byref(self.s),
+                                        self.nijbo.ctypes.data if want_nijbo else None))
+        if want_nijbo:
+            self.nijbo = self.nijbo.reshape(n, n)
+        self.mpack = int(self.s.mpack)
+        self.norbs = int(self.iorbs.sum())
+        idg = np.zeros(self.norbs, np.int64)
+        check(lib().mb_mz_idiag(ctypes.byref(self.s), idg.ctypes.data))
+        self.idiag_host = idg
+        self.idiag = torch.from_numpy(idg).cuda()
+
+    def close(self):
+        if self.s is not None:
+            lib().mb_mz_layout_destroy(ctypes.byref(self.s))
+            self.s = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Lmos:
+    """Occupied LMOs given as the reference's (ncf, nncf, icocc, ncocc, cocc)."""
+
+    def __init__(self, layout: Layout, lmos):
+        ncf, nncf, icocc, ncocc, cocc = (np.ascontiguousarray(x) for x in lmos)
+        self._keep = (ncf.astype(np.int32), nncf.astype(np.int32), icocc.astype(np.int32),
+                      ncocc.astype(np.int32), cocc.astype(np.float64))
+        ncf, nncf, icocc, ncocc, cocc = self._keep
+        self.s = MbMzLmos()
+        check(lib().mb_mz_lmos_create(layout.iorbs.size, layout.iorbs.ctypes.data, int(ncf.size), ncf.ctypes.data,
+                                      nncf.ctypes.data, icocc.ctypes.data, ncocc.ctypes.data, cocc.ctypes.data,
+                                      int(cocc.size), ctypes.byref(self.s)))
+
+    def close(self):
+        if self.s is not None:
+            lib().mb_mz_lmos_destroy(ctypes.byref(self.s))
+            self.s = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def density(layout: Layout, lmos: Lmos, mode: int = 0, partp=None, out=None):
+    p = out if out is not None else torch.empty(layout.mpack, dtype=torch.float64, device="cuda")
+    check(lib().mb_mz_density_dev(ctypes.byref(layout.s), ctypes.byref(lmos.s), int(mode),
+                                  _ptr(partp) if partp is not None else None, _ptr(p), _stream()))
+    return p
+
+
+def helecz(layout: Layout, p, h, f) -> float:
+    out = torch.zeros(1, dtype=torch.float64, device="cuda")
+    ws = torch.empty(int(lib().mb_mz_helecz_ws_bytes()) // 8 + 1, dtype=torch.float64, device="cuda")
+    check(lib().mb_mz_helecz_ws(layout.mpack, layout.norbs, _ptr(layout.idiag), _ptr(p), _ptr(h), _ptr(f),
+                                _ptr(out), _ptr(ws), _stream()))
+    return float(out.item())
+
+
+def cnvgz(layout: Layout, pnew, p, p1, p2, p3, niter: int, use3: bool = True) -> float:
+    pm = torch.zeros(1, dtype=torch.float64, device="cuda")
+    ws = torch.empty(int(lib().mb_mz_cnvgz_ws_bytes()) // 8, dtype=torch.float64, device="cuda")
+    check(lib().mb_mz_cnvgz_ws(layout.norbs, layout.mpack, _ptr(pnew), _ptr(p), _ptr(p1), _ptr(p2), _ptr(p3),
+                               int(niter), _ptr(layout.idiag), int(use3), _ptr(pm), _ptr(ws), _stream()))
+    return float(pm.item())

@@ -215,3 +215,32 @@ def formula(nat) -> str:
     c = Counter(int(z) for z in nat)
     sym = {1: "H", 6: "C", 8: "O"}
     return "".join(f"{sym[z]}{c[z]}" for z in (6, 1, 8) if c[z])
+
+
+def mozyme_lmos(nat, xyz, radius: float = 4.0, seed: int = 11, per_heavy: int = 4):
+    """Synthetic occupied LMOs in the reference's MOZYME_C arrays, for kernel
+    tests and timing: every O or C atom owns `per_heavy` LMOs that cover the
+    atom itself, then every other atom within `radius` Angstrom in order of
+    distance (the way diagg2 grows an LMO outward); coefficients decay with
+    distance.  Returns (iorbs, (ncf, nncf, icocc, ncocc, cocc)) with icocc
+    1-based and nncf/ncocc 0-based starts."""
+    nat = np.asarray(nat)
+    xyz = np.asarray(xyz, float).reshape(-1, 3)
+    rng = np.random.default_rng(seed)
+    iorbs = np.where(nat == 1, 1, 4).astype(np.int32)
+    ncf, nncf, icocc, ncocc, cocc = [], [], [], [], []
+    heavy = np.nonzero(nat != 1)[0]
+    for a in heavy:
+        d = np.linalg.norm(xyz - xyz[a], axis=1)
+        near = np.nonzero(d < radius)[0]
+        near = near[np.argsort(d[near], kind="stable")]
+        for _ in range(per_heavy):
+            nncf.append(len(icocc))
+            ncocc.append(len(cocc))
+            ncf.append(len(near))
+            for b in near:
+                icocc.append(int(b) + 1)
+                cocc.extend((rng.normal(size=iorbs[b]) * np.exp(-d[b] / 1.5)).tolist())
+    lmos = (np.array(ncf, np.int32), np.array(nncf, np.int32), np.array(icocc, np.int32),
+            np.array(ncocc, np.int32), np.array(cocc, np.float64))
+    return iorbs, lmos

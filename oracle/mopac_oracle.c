@@ -1309,3 +1309,168 @@ double orc_const(const char *name) {
   if (!strcmp(name, "a0")) return A0;
   return 0.0;
 }
+
+/* ======================================================================
+ * MOZYME sparse pair-block storage and the kernels on it.
+ * ====================================================================== */
+
+/* fillij (MOZYME/fillij.F90:20-230), first call, molecular (id = 0), full
+ * nijbo table (lijbo): for atom i in order, the blocks of its partners j < i
+ * with r^2 < cutof2 (iorbs(i) x iorbs(j), atom i's orbitals outer), then its
+ * own lower triangle.  nijbo (numat x numat, row-major here, symmetric) gets
+ * the 0-based block offset, -2 for cutof2 <= r^2 < cutof1 and -1 beyond.
+ * Returns mpack. */
+long long orc_mz_layout(int numat, const int *iorbs, const double *coord, double cutof1, double cutof2,
+                        long long *nijbo) {
+    long long mpack = 0;
+    for (int i = 0; i < numat; ++i) {
+        const int io = iorbs[i];
+        const double x1 = coord[3 * i], x2 = coord[3 * i + 1], x3 = coord[3 * i + 2];
+        for (int j = 0; j < i; ++j) {
+            const int jo = iorbs[j];
+            const double dx = x1 - coord[3 * j], dy = x2 - coord[3 * j + 1], dz = x3 - coord[3 * j + 2];
+            const double r = dx * dx + dy * dy + dz * dz;
+            long long v;
+            if (r < cutof2) {
+                v = mpack;
+                mpack += (long long)io * jo;
+            } else if (r < cutof1) {
+                v = -2;
+            } else {
+                v = -1;
+            }
+            nijbo[(long long)i * numat + j] = v;
+            nijbo[(long long)j * numat + i] = v;
+        }
+        nijbo[(long long)i * numat + i] = mpack;
+        mpack += (long long)io * (io + 1) / 2;
+    }
+    return mpack;
+}
+
+/* density_for_MOZYME (MOZYME/density_for_MOZYME.F90:16-342), lijbo branch,
+ * CPU arithmetic.  LMO i (0-based) covers the ncf[i] atoms icocc[nncf[i] ..]
+ * (1-based atom numbers), its coefficients start at cocc[ncocc[i]] in the
+ * order of that atom list, iorbs[atom] per atom. */
+void orc_mz_density(int numat, const int *iorbs, const long long *nijbo, int nclose, const int *ncf,
+                    const int *nncf, const int *icocc, const int *ncocc, const double *cocc, int mode,
+                    long long mpack, const double *partp, double *p) {
+    if (mode == 0) {
+        for (long long l = 0; l < mpack; ++l) p[l] = 0.0;
+    } else if (mode == -1) {
+        for (long long l = 0; l < mpack; ++l) p[l] = -0.5 * partp[l];
+    } else {
+        for (long long l = 0; l < mpack; ++l) p[l] = 0.5 * partp[l];
+    }
+    for (int i = 0; i < nclose; ++i) {
+        const int loop = ncocc[i];
+        int ja = 0;
+        for (int jj = nncf[i]; jj < nncf[i] + ncf[i]; ++jj) {
+            const int j = icocc[jj] - 1;
+            const int nj = iorbs[j];
+            int ka = loop;
+            for (int kk = nncf[i]; kk < nncf[i] + ncf[i]; ++kk) {
+                const int k = icocc[kk] - 1;
+                const long long base = nijbo[(long long)j * numat + k];
+                if (j == k) {
+                    long long l = base;
+                    for (int j1 = 0; j1 < nj; ++j1) {
+                        const double sum = cocc[ja + j1 + loop];
+                        for (int k1 = 0; k1 <= j1; ++k1) {
+                            p[l] = p[l] + cocc[ka + k1] * sum;
+                            ++l;
+                        }
+                    }
+                } else if (j > k && base >= 0) {
+                    long long l = base;
+                    for (int j1 = 0; j1 < nj; ++j1) {
+                        const double sum = cocc[ja + j1 + loop];
+                        for (int k1 = 0; k1 < iorbs[k]; ++k1) {
+                            p[l] = p[l] + cocc[ka + k1] * sum;
+                            ++l;
+                        }
+                    }
+                }
+                ka += iorbs[k];
+            }
+            ja += nj;
+        }
+    }
+    double spinfa;
+    if (mode == 0 || mode == 1) spinfa = 2.0;
+    else if (mode == -1) spinfa = -2.0;
+    else spinfa = 1.0;
+    if (fabs(spinfa - 1.0) > 1.0e-10)
+        for (long long l = 0; l < mpack; ++l) p[l] = spinfa * p[l];
+}
+
+/* helecz (MOZYME/helecz.F90:16-52) */
+double orc_mz_helecz(int numat, const int *iorbs, const long long *nijbo, const double *p, const double *h,
+                     const double *f) {
+    double ed = 0.0, ee = 0.0;
+    for (int i = 0; i < numat; ++i) {
+        for (int j = 0; j < i; ++j) {
+            const long long k = nijbo[(long long)i * numat + j];
+            if (k >= 0) {
+                const long long l = k + (long long)iorbs[i] * iorbs[j];
+                for (long long m = k; m < l; ++m) ee = ee + p[m] * (h[m] + f[m]);
+            }
+        }
+        long long k = nijbo[(long long)i * numat + i];
+        for (int l1 = 0; l1 < iorbs[i]; ++l1) {
+            for (int l2 = 0; l2 < l1; ++l2) {
+                ee = ee + p[k] * (h[k] + f[k]);
+                ++k;
+            }
+            ed = ed + p[k] * (h[k] + f[k]);
+            ++k;
+        }
+    }
+    return ee + 0.5 * ed;
+}
+
+/* cnvgz (MOZYME/cnvgz.F90:16-85); idiag is 1-based like the reference's. */
+void orc_mz_cnvgz(int norbs, long long mpack, double *pnew, double *p, double *p1, double *p2, double *p3,
+                  int niter, const long long *idiag, int use3, double *pmax_out) {
+    for (int i = 0; i < norbs; ++i) {
+        const long long j = idiag[i] - 1;
+        p3[i] = pnew[j];
+        p2[i] = p[j];
+    }
+    double pmax = 0.0;
+    for (long long i = 0; i < mpack; ++i) {
+        const double sa = fabs(pnew[i] - p[i]);
+        pmax = pmax > sa ? pmax : sa;
+    }
+    if (use3) {
+        if (niter % 3 == 0) {
+            double faca = 0.0, facb = 0.0;
+            for (int i = 0; i < norbs; ++i) {
+                const double sa = fabs(p3[i] - p2[i]);
+                faca = faca + sa * sa;
+                const double t = p3[i] - 2.0 * p2[i] + p1[i];
+                facb = facb + t * t;
+            }
+            if (facb > 0.0 && faca < 100.0 * facb) {
+                const double fac = sqrt(faca / facb);
+                for (long long i = 0; i < mpack; ++i) pnew[i] = pnew[i] + fac * (pnew[i] - p[i]);
+            }
+        }
+        if (niter > 3) {
+            const double damp = 0.05;
+            if (pmax > damp) {
+                for (int i = 0; i < norbs; ++i) {
+                    const long long j = idiag[i] - 1;
+                    if (fabs(p3[i] - p2[i]) > damp) {
+                        pnew[j] = p2[i] + copysign(damp, p3[i] - p2[i]);
+                        const double v = pnew[j] > 0.0 ? pnew[j] : 0.0;
+                        pnew[j] = v < 2.0 ? v : 2.0;
+                    }
+                }
+            }
+        }
+    }
+    for (int i = 0; i < norbs; ++i) p1[i] = p2[i];
+    for (long long i = 0; i < mpack; ++i) p[i] = pnew[i];
+    *pmax_out = pmax;
+}

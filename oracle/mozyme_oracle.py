@@ -1,0 +1,107 @@
+"""CPU oracle for the MOZYME sparse-block kernels (test infrastructure only).
+
+Only tests/ and the CPU legs of bench.py may import this module.  It binds the
+C restatements in mopac_oracle.c:
+  * orc_mz_layout   -- fillij (MOZYME/fillij.F90:20-230), first call, id = 0;
+  * orc_mz_density  -- density_for_MOZYME (MOZYME/density_for_MOZYME.F90:16-342);
+  * orc_mz_helecz   -- helecz (MOZYME/helecz.F90:16-52);
+  * orc_mz_cnvgz    -- cnvgz (MOZYME/cnvgz.F90:16-85).
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from oracle import scf_oracle as so
+
+_bound = False
+
+
+def _lib():
+    global _bound
+    L = so.lib()
+    if not _bound:
+        i32p = np.ctypeslib.ndpointer(np.int32, flags="C")
+        i64p = np.ctypeslib.ndpointer(np.int64, flags="C")
+        f64p = np.ctypeslib.ndpointer(np.float64, flags="C")
+        L.orc_mz_layout.argtypes = [ctypes.c_int, i32p, f64p, ctypes.c_double, ctypes.c_double, i64p]
+        L.orc_mz_layout.restype = ctypes.c_longlong
+        L.orc_mz_density.argtypes = [ctypes.c_int, i32p, i64p, ctypes.c_int, i32p, i32p, i32p, i32p, f64p,
+                                     ctypes.c_int, ctypes.c_longlong, f64p, f64p]
+        L.orc_mz_helecz.argtypes = [ctypes.c_int, i32p, i64p, f64p, f64p, f64p]
+        L.orc_mz_helecz.restype = ctypes.c_double
+        L.orc_mz_cnvgz.argtypes = [ctypes.c_int, ctypes.c_longlong, f64p, f64p, f64p, f64p, f64p, ctypes.c_int,
+                                   i64p, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+        _bound = True
+    return L
+
+
+def cutoffs(numat: int, cutofp: float | None = None):
+    """cutof1, cutof2 (squared) as fillij sets them (MOZYME/fillij.F90:59-80)."""
+    c1, c2 = 10.0 ** 2, 9.9 ** 2
+    if cutofp is not None and cutofp < 100.0:
+        c1, c2 = cutofp ** 2 + 1e-4, cutofp ** 2
+    if numat < 30:
+        c1, c2 = 1.0e6 + 10, 1.0e6
+    return c1, c2
+
+
+def layout(iorbs, coord, cutof1: float, cutof2: float):
+    iorbs = np.ascontiguousarray(iorbs, np.int32)
+    coord = np.ascontiguousarray(coord, np.float64).reshape(-1)
+    n = iorbs.size
+    nijbo = np.zeros(n * n, np.int64)
+    mpack = _lib().orc_mz_layout(n, iorbs, coord, cutof1, cutof2, nijbo)
+    return int(mpack), nijbo.reshape(n, n)
+
+
+def idiag(iorbs, nijbo) -> np.ndarray:
+    """iter_for_MOZYME.F90:183-190 (1-based positions)."""
+    out = []
+    for i, io in enumerate(iorbs):
+        j = int(nijbo[i, i])
+        for k in range(1, int(io) + 1):
+            j += k
+            out.append(j)
+    return np.array(out, np.int64)
+
+
+def density(iorbs, nijbo, lmos, mode: int, mpack: int, partp=None) -> np.ndarray:
+    ncf, nncf, icocc, ncocc, cocc = lmos
+    p = np.zeros(mpack)
+    pp = np.zeros(mpack) if partp is None else np.ascontiguousarray(partp, np.float64)
+    _lib().orc_mz_density(len(iorbs), np.ascontiguousarray(iorbs, np.int32), np.ascontiguousarray(nijbo.ravel()),
+                          len(ncf), ncf, nncf, icocc, ncocc, cocc, mode, mpack, pp, p)
+    return p
+
+
+def helecz(iorbs, nijbo, p, h, f) -> float:
+    return _lib().orc_mz_helecz(len(iorbs), np.ascontiguousarray(iorbs, np.int32),
+                                np.ascontiguousarray(nijbo.ravel()), p, h, f)
+
+
+def cnvgz(pnew, p, p1, p2, p3, niter: int, idg, use3: bool = True) -> float:
+    pm = ctypes.c_double()
+    _lib().orc_mz_cnvgz(p1.size, pnew.size, pnew, p, p1, p2, p3, niter, idg, int(use3), ctypes.byref(pm))
+    return pm.value
+
+
+def dense_to_blocks(a: np.ndarray, iorbs, nijbo, mpack: int) -> np.ndarray:
+    """Gather a full symmetric matrix into the pair-block storage."""
+    first = np.concatenate([[0], np.cumsum(iorbs)[:-1]])
+    out = np.zeros(mpack)
+    n = len(iorbs)
+    for i in range(n):
+        for j in range(i + 1):
+            off = int(nijbo[i, j])
+            if off < 0:
+                continue
+            bi = a[first[i]:first[i] + iorbs[i], first[j]:first[j] + iorbs[j]]
+            if i == j:
+                r, c = np.tril_indices(iorbs[i])
+                vals = bi[r, c]
+            else:
+                vals = bi.ravel()
+            out[off:off + vals.size] = vals
+    return out

@@ -1,0 +1,166 @@
+"""MOZYME sparse-block rows: storage (fillij), LMO density
+(density_for_MOZYME), energy (helecz) and extrapolation (cnvgz).
+
+CPU: the oracle's sparse restatements against the pinned dense path -- with
+every pair inside the cutoff (fewer than 30 atoms, as fillij sets it) and
+canonical MOs as LMOs, the MOZYME density and energy equal the dense ones
+rearranged into blocks.  GPU: the library against the oracle on synthetic
+LMOs over a seeded water box with the 9 A cutoff: layout identical, density
+and cnvgz bit-identical, helecz to 1e-12 relative.
+"""
+import numpy as np
+import pytest
+
+from mopac_gpu_b200 import workloads
+from oracle import mozyme_oracle as mo
+from oracle import scf_oracle as so
+from tests.helpers import oracle_system, small_systems
+
+
+def _canonical_lmos(s, c):
+    """Occupied canonical MOs as LMOs over all atoms (atom order 1..numat)."""
+    iorbs = (s.nlast - s.nfirst + 1).astype(np.int32)
+    nocc = s.nclose
+    ncf = np.full(nocc, s.numat, np.int32)
+    nncf = (np.arange(nocc) * s.numat).astype(np.int32)
+    icocc = np.tile(np.arange(1, s.numat + 1, dtype=np.int32), nocc)
+    ncocc = (np.arange(nocc) * s.norbs).astype(np.int32)
+    cocc = np.ascontiguousarray(c[:, :nocc].T).ravel()
+    return iorbs, (ncf, nncf, icocc, ncocc, cocc)
+
+
+@pytest.mark.parametrize("name", ["water16", "propane"])
+def test_oracle_mozyme_density_and_energy_equal_dense(name):
+    nat, xyz = small_systems()[name]
+    s = oracle_system(nat, xyz)
+    r = so.iter_scf(s)
+    iorbs, lmos = _canonical_lmos(s, r.c)
+    mpack, nijbo = mo.layout(iorbs, s.coord, 1.0e6 + 10, 1.0e6)   # every pair stored
+    assert mpack == s.mpack
+    p = mo.density(iorbs, nijbo, lmos, 0, mpack)
+    pdense = so.density(r.c, s.nclose)
+    pd = so.unpack(pdense, s.norbs)
+    np.testing.assert_allclose(p, mo.dense_to_blocks(pd, iorbs, nijbo, mpack), atol=1e-12)
+    f = so.unpack(s.h, s.norbs)  # any symmetric pair works for the energy identity
+    h = so.unpack(s.h, s.norbs) * 0.5
+    e_sparse = mo.helecz(iorbs, nijbo, p, mo.dense_to_blocks(h, iorbs, nijbo, mpack),
+                         mo.dense_to_blocks(f, iorbs, nijbo, mpack))
+    e_dense = so.helect(s.norbs, pdense, so.pack(h), so.pack(f))
+    assert e_sparse == pytest.approx(e_dense, rel=1e-12)
+
+
+def test_oracle_mozyme_density_modes():
+    nat, xyz = small_systems()["water16"]
+    iorbs, lmos = workloads.mozyme_lmos(nat, xyz, radius=3.5)
+    mpack, nijbo = mo.layout(iorbs, xyz, 9.0 ** 2 + 1e-4, 9.0 ** 2)
+    p0 = mo.density(iorbs, nijbo, lmos, 0, mpack)
+    part = np.random.default_rng(0).normal(size=mpack)
+    pm = mo.density(iorbs, nijbo, lmos, -1, mpack, part)
+    pp = mo.density(iorbs, nijbo, lmos, 1, mpack, part)
+    np.testing.assert_allclose(pm, -(p0 - part), atol=1e-12)
+    np.testing.assert_allclose(pp, p0 + part, atol=1e-12)
+
+
+def test_oracle_cnvgz_damps_and_extrapolates():
+    rng = np.random.default_rng(4)
+    iorbs = np.array([4, 1, 1, 4], np.int32)
+    xyz = rng.normal(size=(4, 3))
+    mpack, nijbo = mo.layout(iorbs, xyz, 1e6, 1e6)
+    idg = mo.idiag(iorbs, nijbo)
+    p = rng.uniform(0, 2, mpack)
+    pnew = p + rng.normal(scale=0.2, size=mpack)
+    p1 = rng.uniform(0, 2, 10)
+    p2, p3 = np.zeros(10), np.zeros(10)
+    pn = pnew.copy()
+    pmax = mo.cnvgz(pn, p.copy(), p1.copy(), p2, p3, 6, idg)
+    assert pmax == pytest.approx(np.abs(pnew - p).max())
+    d = pn[idg - 1]
+    assert np.all(d >= 0) and np.all(d <= 2)
+
+
+# ------------------------------------------------------------------ GPU
+def _need_gpu():
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return torch
+
+
+def _water_case(nwater, radius=4.0):
+    nat, xyz, _ = workloads.water_box(nwater)
+    iorbs, lmos = workloads.mozyme_lmos(nat, xyz, radius=radius)
+    return nat, xyz, iorbs, lmos
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("nwater", [16, 128, 512])
+def test_gpu_layout_matches_fillij(nwater):
+    _need_gpu()
+    from mopac_gpu_b200.mozyme import Layout
+    nat, xyz, iorbs, _ = _water_case(nwater)
+    c1, c2 = mo.cutoffs(len(nat), 9.0)
+    mp, nijbo = mo.layout(iorbs, xyz, c1, c2)
+    L = Layout(iorbs, xyz, c1, c2, want_nijbo=True)
+    assert L.mpack == mp
+    np.testing.assert_array_equal(L.nijbo, nijbo)
+    np.testing.assert_array_equal(L.idiag_host, mo.idiag(iorbs, nijbo))
+    L.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("nwater,mode", [(16, 0), (128, 0), (128, -1), (128, 1), (512, 0)])
+def test_gpu_mozyme_density_bit_identical(nwater, mode):
+    torch = _need_gpu()
+    from mopac_gpu_b200 import mozyme
+    nat, xyz, iorbs, lmos = _water_case(nwater)
+    c1, c2 = mo.cutoffs(len(nat), 9.0)
+    mp, nijbo = mo.layout(iorbs, xyz, c1, c2)
+    part = np.random.default_rng(1).normal(size=mp) if mode != 0 else None
+    ref = mo.density(iorbs, nijbo, lmos, mode, mp, part)
+    L = mozyme.Layout(iorbs, xyz, c1, c2)
+    Q = mozyme.Lmos(L, lmos)
+    p = mozyme.density(L, Q, mode, torch.from_numpy(part).cuda() if part is not None else None)
+    np.testing.assert_array_equal(p.cpu().numpy(), ref)
+    Q.close()
+    L.close()
+
+
+@pytest.mark.gpu
+def test_gpu_helecz_matches_oracle():
+    torch = _need_gpu()
+    from mopac_gpu_b200 import mozyme
+    nat, xyz, iorbs, lmos = _water_case(256)
+    c1, c2 = mo.cutoffs(len(nat), 9.0)
+    mp, nijbo = mo.layout(iorbs, xyz, c1, c2)
+    rng = np.random.default_rng(3)
+    p, h, f = rng.normal(size=mp), rng.normal(size=mp), rng.normal(size=mp)
+    ref = mo.helecz(iorbs, nijbo, p, h, f)
+    L = mozyme.Layout(iorbs, xyz, c1, c2)
+    e = mozyme.helecz(L, *(torch.from_numpy(x).cuda() for x in (p, h, f)))
+    assert e == pytest.approx(ref, rel=1e-12, abs=1e-9)
+    L.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("niter", [2, 3, 4, 6, 7])
+def test_gpu_cnvgz_bit_identical(niter):
+    torch = _need_gpu()
+    from mopac_gpu_b200 import mozyme
+    nat, xyz, iorbs, _ = _water_case(128)
+    c1, c2 = mo.cutoffs(len(nat), 9.0)
+    mp, nijbo = mo.layout(iorbs, xyz, c1, c2)
+    idg = mo.idiag(iorbs, nijbo)
+    n = idg.size
+    rng = np.random.default_rng(niter)
+    p = rng.uniform(0, 2, mp)
+    pnew = p + rng.normal(scale=0.1, size=mp)
+    p1 = rng.uniform(0, 2, n)
+    arrays = [pnew.copy(), p.copy(), p1.copy(), np.zeros(n), np.zeros(n)]
+    pmax_ref = mo.cnvgz(*arrays, niter, idg)
+    L = mozyme.Layout(iorbs, xyz, c1, c2)
+    dev = [torch.from_numpy(x).cuda() for x in (pnew, p, p1, np.zeros(n), np.zeros(n))]
+    pmax = mozyme.cnvgz(L, *dev, niter)
+    assert pmax == pmax_ref
+    for a, d in zip(arrays, dev):
+        np.testing.assert_array_equal(d.cpu().numpy(), a)
+    L.close()
