@@ -273,6 +273,13 @@ int mb_density_dev(int n, int nocc, double occ, const double* c, int ldc, double
  * modified like the reference's xmat).  Ascending eigenvalues, vectors in
  * columns.  Returns MB_ERR_NUMERIC if the solver fails. */
 int mb_eigh_packed_dev(int n, double* fpacked, double* c, double* eigs, cudaStream_t stream);
+/* The same with a caller-owned workspace (mb_eigh_ws_bytes(n) bytes, 256-byte
+ * aligned) and no host synchronisation: perturb = 1 adds the i*1e-10
+ * diagonal; *status_dev (device int) is set nonzero if inverse iteration
+ * fails. */
+size_t mb_eigh_ws_bytes(int n);
+int mb_eigh_ws(int n, double* fpacked, int perturb, double* c, double* eigs, void* ws, int* status_dev,
+               cudaStream_t stream);
 
 /* Pseudo-diagonalisation (diag_for_GPU.F90): Fmo = C_v^T F C_o and the
  * ordered 2x2 rotation sweep on C.  *nrot_out (host) gets the rotations

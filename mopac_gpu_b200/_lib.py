@@ -106,6 +106,8 @@ SIGNATURES = {
     "mb_density_split_ws_bytes": ([_I, _I], ctypes.c_size_t),
     "mb_density_split_ws": ([_I, _I, _D, _P, _I, _P, _P, ctypes.c_size_t, _P, _P], _I),
     "mb_eigh_packed_dev": ([_I, _P, _P, _P, _P], _I),
+    "mb_eigh_ws_bytes": ([_I], ctypes.c_size_t),
+    "mb_eigh_ws": ([_I, _P, _I, _P, _P, _P, _P, _P], _I),
     "mb_pseudo_diag_dev": ([_I, _I, _P, _P, _P, ctypes.POINTER(_LL), _P], _I),
     "mb_dgemm_dev": ([_C, _C, _I, _I, _I, _D, _P, _I, _P, _I, _D, _P, _I, _P], _I),
     "call_gemm_cublas": ([_C, _C, _I, _I, _I, _D, _P, _I, _P, _I, _D, _P, _I], None),

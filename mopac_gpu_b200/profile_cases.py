@@ -1,0 +1,300 @@
+"""Per-kernel timing cases for the SCF rows, at the benchmark sizes.
+
+  python -m mopac_gpu_b200.profile_cases [case ...] [--reps R] [--out FILE]
+
+Each case times one library entry point with CUDA events on the current
+stream (warm-up first, L2 flushed by a 256 MB write before every timed
+repetition) and prints one JSON line: the time per call, the algorithmic
+bytes or flops of one call, the achieved rate and its fraction of the peak
+it is bound by.  Peaks: HBM and BF16 from MEASURED_PEAKS.json at the
+repository root (fallback 6650 GB/s, 1590 TFLOP/s); FP64 is measured here as
+torch's float64 matmul at 8192^3 (cuBLAS DGEMM) because the pool's peak file
+has no FP64 figure.
+
+Cases (sizes of the benchmark configurations):
+  fock2         Fock build, (H2O)512: 8 (n2elec + 4 mpack) bytes
+  helect, cnvg  energy and extrapolation, n = 3072: 24 mpack / 24 mpack + 8 n bytes
+  density64     P = 2 C_o C_o^T FP64, n = 3072, k = 2048: n^2 k flops
+  density_split same with the three-product BF16 split on tcgen05
+  gemm64, gemm_split   3072^3 GEMM, 2 n^3 flops
+  eigh          full eigensolve n = 3072 (the SCF's Fock matrix)
+  pseudo_diag   Fmo + rotation sweep, n = 3072, k = 2048
+  pulay         one Pulay step with a full 10-entry history, n = 3072
+  mz_density, mz_helecz, mz_cnvgz   MOZYME blocks, (H2O)4096, 9 A cutoff,
+                synthetic LMOs over 4 A
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import sys
+
+import numpy as np
+import torch
+
+from . import kernels, mozyme, workloads
+from ._lib import MbAtomsDev, check, lib
+from .scf import ScfContext
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        d = json.load(open(path))
+        return {"hbm_gbs": d["hbm_gbs"], "bf16_tflops": d["bf16_tflops"], "source": "measured"}
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "source": "fallback"}
+
+
+_flush = None
+
+
+def flush_l2():
+    global _flush
+    if _flush is None:
+        _flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    _flush.fill_(1.0)
+
+
+def timed(fn, reps: int, warm: int = 2, setup=None):
+    for _ in range(warm):
+        if setup:
+            setup()
+        fn()
+    torch.cuda.synchronize()
+    ts = []
+    for _ in range(reps):
+        if setup:
+            setup()
+        flush_l2()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        fn()
+        b.record()
+        torch.cuda.synchronize()
+        ts.append(a.elapsed_time(b))
+    return float(np.median(ts))
+
+
+def s():
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def vp(t):
+    return ctypes.c_void_p(t.data_ptr())
+
+
+_fp64_peak = None
+
+
+def fp64_peak_tflops():
+    global _fp64_peak
+    if _fp64_peak is None:
+        a = torch.randn(8192, 8192, dtype=torch.float64, device="cuda")
+        b = torch.randn(8192, 8192, dtype=torch.float64, device="cuda")
+        ms = timed(lambda: torch.matmul(a, b), 3, 1)
+        _fp64_peak = 2 * 8192 ** 3 / (ms * 1e-3) / 1e12
+        del a, b
+    return _fp64_peak
+
+
+def line(case, ms, work, unit, bound, peak, peak_src, **extra):
+    scale = 1e9 if unit == "GB/s" else 1e12
+    ach = work / (ms * 1e-3) / scale
+    d = {"case": case, "ms": round(ms, 4), "achieved": round(ach, 2), "unit": unit, "bound": bound,
+         "peak": round(peak, 1), "frac": round(ach / peak, 4), "peak_source": peak_src,
+         "work_per_call": work}
+    d.update(extra)
+    return d
+
+
+class C1:
+    """(H2O)512 context converged once, plus device copies for the kernels."""
+
+    def __init__(self):
+        nat, xyz, _ = workloads.water_box(512)
+        self.ctx = ScfContext(nat, xyz)
+        self.ctx.hcore()
+        self.ctx.run(pseudo=True)
+        self.n = self.ctx.norbs
+        self.k = self.ctx.nclose
+        self.mpack = self.ctx.mpack
+        ptr = self.ctx.device_ptrs()
+        self.ptr = ptr
+        mp, n = self.mpack, self.n
+
+        def wrap(addr, count):
+            # torch views of library-owned device memory through __cuda_array_interface__
+            class _A:
+                __cuda_array_interface__ = {"shape": (count,), "typestr": "<f8", "data": (addr, False),
+                                            "version": 3, "strides": None}
+            return torch.as_tensor(_A(), device="cuda")
+
+        self.h = wrap(ptr["h"], mp)
+        self.w = wrap(ptr["w"], self.ctx.n2elec)
+        self.f = wrap(ptr["f"], mp)
+        self.p = wrap(ptr["p"], mp)
+        self.c = wrap(ptr["c"], n * n)
+        self.eigs = wrap(ptr["eigs"], n)
+        self.pa = (self.p * 0.5).contiguous()
+        self.atoms = MbAtomsDev()
+        check(lib().mb_ctx_atoms_dev(self.ctx._h, ctypes.byref(self.atoms)))
+
+
+def run_cases(names, reps):
+    L = lib()
+    pk = peaks()
+    out = []
+    hbm, bf16, src = pk["hbm_gbs"], pk["bf16_tflops"], pk["source"]
+    need_c1 = any(c in names for c in ("fock2", "helect", "cnvg", "density64", "density_split", "eigh",
+                                       "pseudo_diag", "pulay"))
+    c1 = C1() if need_c1 else None
+    fp64 = fp64_peak_tflops() if any(c in names for c in ("density64", "gemm64", "eigh")) else None
+    if "fock2" in names:
+        f = c1.f.clone()
+        ms = timed(lambda: check(L.mb_fock2_dev(ctypes.byref(c1.atoms), vp(f), vp(c1.h), vp(c1.p), vp(c1.pa),
+                                                vp(c1.w), 0.0, 0, s())), reps)
+        out.append(line("fock2", ms, 8 * (c1.ctx.n2elec + 4 * c1.mpack), "GB/s", "hbm", hbm, src,
+                        config="(H2O)512, n = 3072"))
+    if "helect" in names:
+        o = torch.zeros(1, dtype=torch.float64, device="cuda")
+        ms = timed(lambda: check(L.mb_helect_dev(c1.n, vp(c1.pa), vp(c1.h), vp(c1.f), vp(o), s())), reps)
+        out.append(line("helect", ms, 24 * c1.mpack, "GB/s", "hbm", hbm, src, config="n = 3072"))
+    if "cnvg" in names:
+        pn, po, p1 = c1.p.clone(), c1.p.clone() * 0.999, torch.ones(c1.n, dtype=torch.float64, device="cuda")
+        pl = torch.zeros(1, dtype=torch.float64, device="cuda")
+        ms = timed(lambda: check(L.mb_cnvg_dev(c1.n, vp(pn), vp(po), vp(p1), 5, vp(pl), s())), reps)
+        out.append(line("cnvg", ms, 24 * c1.mpack + 8 * c1.n, "GB/s", "hbm", hbm, src, config="n = 3072"))
+    if "density64" in names or "density_split" in names:
+        ct = c1.c.view(c1.n, c1.n)  # row-major view of column-major C: row index = column of C
+        cc = ct.t()
+        if "density64" in names:
+            ms = timed(lambda: kernels.density(cc, c1.k), reps)
+            out.append(line("density64", ms, c1.n ** 2 * c1.k, "TFLOP/s", "fp64", fp64, "cuBLAS DGEMM here",
+                            config="n = 3072, k = 2048"))
+        if "density_split" in names:
+            ms = timed(lambda: kernels.density_split(cc, c1.k), reps)
+            out.append(line("density_split", ms, c1.n ** 2 * c1.k, "TFLOP/s", "tensor", bf16, src,
+                            config="n = 3072, k = 2048", note="algorithmic n^2 k against the BF16 peak; the "
+                            "tensor pipe does 3x that (three BF16 products) on the lower tiles only"))
+    if "gemm64" in names or "gemm_split" in names:
+        n = 3072
+        a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+        b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+        cm = torch.empty(n, n, dtype=torch.float64, device="cuda")
+        if "gemm64" in names:
+            ms = timed(lambda: check(L.mb_dgemm_dev(b"N", b"N", n, n, n, 1.0, vp(a), n, vp(b), n, 0.0, vp(cm), n,
+                                                    s())), reps)
+            out.append(line("gemm64", ms, 2 * n ** 3, "TFLOP/s", "fp64", fp64, "cuBLAS DGEMM here", config="3072^3"))
+        if "gemm_split" in names:
+            nb = int(L.mb_gemm_split_ws_bytes(n, n, n))
+            buf, ws = kernels._aligned_ws(nb, "cuda")
+            err = torch.zeros(1, dtype=torch.int32, device="cuda")
+            ms = timed(lambda: check(L.mb_gemm_split_ws(b"N", b"N", n, n, n, 1.0, vp(a), n, vp(b), n, 0.0, vp(cm),
+                                                        n, ws, nb, vp(err), s())), reps)
+            assert int(err.item()) == 0
+            out.append(line("gemm_split", ms, 2 * n ** 3, "TFLOP/s", "tensor", bf16, src, config="3072^3",
+                            note="algorithmic 2 n^3 against the BF16 peak (the pipe does 3x)"))
+    if "eigh" in names:
+        fpk = c1.f.clone()
+        work = fpk.clone()
+        cv = torch.empty(c1.n * c1.n, dtype=torch.float64, device="cuda")
+        ev = torch.empty(c1.n, dtype=torch.float64, device="cuda")
+        nb = int(L.mb_eigh_ws_bytes(c1.n))
+        buf, ws = kernels._aligned_ws(nb, "cuda", 256)
+        st = torch.zeros(4, dtype=torch.int32, device="cuda")
+        ms = timed(lambda: check(L.mb_eigh_ws(c1.n, vp(work), 1, vp(cv), vp(ev), ws, vp(st), s())),
+                   max(2, reps // 2), setup=lambda: work.copy_(fpk))
+        assert int(st[0].item()) == 0
+        out.append(line("eigh", ms, 4.5 * c1.n ** 3, "TFLOP/s", "fp64", fp64, "cuBLAS DGEMM here",
+                        config="n = 3072 Fock matrix of (H2O)512", note="4.5 n^3 flop convention of the "
+                        "reference's gpu_bench"))
+    if "pseudo_diag" in names:
+        cv = c1.c.clone()
+        nrot = ctypes.c_longlong(0)
+        ms = timed(lambda: check(L.mb_pseudo_diag_dev(c1.n, c1.k, vp(c1.f), vp(cv), vp(c1.eigs), ctypes.byref(nrot),
+                                                      s())), reps, setup=lambda: cv.copy_(c1.c))
+        v = c1.n - c1.k
+        fl = 2 * c1.n * c1.n * v + 2 * v * c1.k * c1.n
+        out.append(line("pseudo_diag", ms, fl, "TFLOP/s", "fp64", fp64_peak_tflops(), "cuBLAS DGEMM here",
+                        config="n = 3072, k = 2048", rotations=int(nrot.value),
+                        note="flops of the two Fmo GEMMs; the rotation sweep moves 32 n bytes per rotation"))
+    if "pulay" in names:
+        pu = kernels.Pulay(c1.n)
+        f = c1.f.clone()
+        for _ in range(10):
+            pu.step(f, c1.pa)
+        ms = timed(lambda: pu.step(f, c1.pa), reps, setup=lambda: f.copy_(c1.f))
+        out.append(line("pulay", ms, 2 * c1.n ** 3, "TFLOP/s", "fp64", fp64_peak_tflops(), "cuBLAS DGEMM here",
+                        config="n = 3072, 10 stored entries",
+                        note="dominated by the n^3 commutator GEMM; history traffic 2 x 10 x 8 mpack bytes"))
+    if any(c.startswith("mz_") for c in names):
+        nat, xyz, _ = workloads.water_box(4096)
+        iorbs, lmos = workloads.mozyme_lmos(nat, xyz, radius=4.0)
+        c1c, c2c = 9.0 ** 2 + 1e-4, 9.0 ** 2
+        lay = mozyme.Layout(iorbs, xyz, c1c, c2c)
+        q = mozyme.Lmos(lay, lmos)
+        mp = lay.mpack
+        cfg = f"(H2O)4096, 9 A cutoff: mpack = {mp}, {len(lmos[0])} LMOs, {len(lmos[4])} coefficients"
+        p = torch.empty(mp, dtype=torch.float64, device="cuda")
+        mozyme.density(lay, q, 0, None, p)
+        if "mz_density" in names:
+            ms = timed(lambda: mozyme.density(lay, q, 0, None, p), reps)
+            out.append(line("mz_density", ms, 8 * mp + 8 * len(lmos[4]), "GB/s", "hbm", hbm, src, config=cfg,
+                            note="P written once and the coefficients read once; the merges re-read "
+                            "coefficients from L2"))
+        rng = np.random.default_rng(0)
+        h = torch.from_numpy(rng.normal(size=mp)).cuda()
+        f = torch.from_numpy(rng.normal(size=mp)).cuda()
+        if "mz_helecz" in names:
+            ws = torch.empty(int(L.mb_mz_helecz_ws_bytes()) // 8 + 1, dtype=torch.float64, device="cuda")
+            o = torch.zeros(1, dtype=torch.float64, device="cuda")
+            ms = timed(lambda: check(L.mb_mz_helecz_ws(mp, lay.norbs, vp(lay.idiag), vp(p), vp(h), vp(f), vp(o),
+                                                       vp(ws), s())), reps)
+            out.append(line("mz_helecz", ms, 24 * mp, "GB/s", "hbm", hbm, src, config=cfg))
+        if "mz_cnvgz" in names:
+            n = lay.norbs
+            pn, po = p.clone(), p.clone() * 0.999
+            p1, p2, p3 = (torch.zeros(n, dtype=torch.float64, device="cuda") for _ in range(3))
+            pm = torch.zeros(1, dtype=torch.float64, device="cuda")
+            ws = torch.empty(32, dtype=torch.float64, device="cuda")
+            ms = timed(lambda: check(L.mb_mz_cnvgz_ws(n, mp, vp(pn), vp(po), vp(p1), vp(p2), vp(p3), 6,
+                                                      vp(lay.idiag), 1, vp(pm), vp(ws), s())), reps,
+                       setup=lambda: (pn.copy_(p), po.copy_(p * 0.999)))
+            out.append(line("mz_cnvgz", ms, 8 * 5 * mp + 8 * 5 * n, "GB/s", "hbm", hbm, src, config=cfg,
+                            note="niter = 6: gather + max, one-thread factor, extrapolation, damping, copy"))
+        q.close()
+        lay.close()
+    if c1 is not None:
+        c1.ctx.close()
+    return out
+
+
+ALL = ["fock2", "helect", "cnvg", "density64", "density_split", "gemm64", "gemm_split", "eigh", "pseudo_diag",
+       "pulay", "mz_density", "mz_helecz", "mz_cnvgz"]
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("cases", nargs="*", default=ALL)
+    ap.add_argument("--reps", type=int, default=5)
+    ap.add_argument("--out", default=None)
+    a = ap.parse_args(argv)
+    bad = [c for c in a.cases if c not in ALL]
+    if bad:
+        raise SystemExit(f"unknown cases {bad}; known: {ALL}")
+    res = run_cases(a.cases, a.reps)
+    for d in res:
+        print(json.dumps(d), flush=True)
+    if a.out:
+        with open(a.out, "w") as fh:
+            for d in res:
+                fh.write(json.dumps(d) + "\n")
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())
