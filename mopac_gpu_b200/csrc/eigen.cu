@@ -287,6 +287,261 @@ __global__ void __launch_bounds__(TPB) tridiag_panel(PanelArgs p) {
 #undef WP
 }
 
+// Second form of the panel kernel, used when every row of the matrix can own
+// an 8-lane group of the grid for the whole panel (n <= grid * TPB / 8).
+// Row r belongs to group r throughout, so the group keeps its own V(r, l) and
+// W(r, l) in registers (lane q holds l = q, q+8, q+16, q+24), prefetches
+// A(r, j+1) before the column's last barrier, and updates A(r, j) with no
+// global loads but p(r).  After each barrier the loads that remain (the
+// per-CTA partials, the broadcast row j, p(r)) are issued by different warps at
+// once.  The symmetric matrix-vector product gives each row 1, 2, 4 or 8
+// warps of one CTA as the trailing matrix shrinks, so late columns are not
+// bound by one warp's chain of loads.  Arithmetic per element follows the
+// first form, except that p(r) is summed in wpr column slices for wpr > 1.
+__global__ void __launch_bounds__(TPB, 3) tridiag_panel2(PanelArgs p) {
+  cg::grid_group grid = cg::this_grid();
+  __shared__ double sh[32];
+  __shared__ double s_scal[4];
+  __shared__ double s_sum, s_alpha, s_wjr;
+  __shared__ double s_vj[NB], s_wj[NB], s_t1[NB], s_t2[NB];
+  __shared__ double s_pv[TPB / 32];
+  __shared__ double s_symv[TPB / 32];
+  const int n = p.n, lda = p.lda;
+  const long long gtid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long gstride = (long long)gridDim.x * blockDim.x;
+  const int gwarp = (int)(gtid >> 5), nwarps = (int)(gstride >> 5), lane = threadIdx.x & 31;
+  const int wid = threadIdx.x >> 5, q = lane & 7, gbase = lane & ~7;
+  double* A = p.a;
+#define AE(r, c) A[(long long)(c) * lda + (r)]
+#define VP(r, c) p.vp[(long long)(c) * n + (r)]
+#define WP(r, c) p.wp[(long long)(c) * n + (r)]
+  const int r = (int)(gtid >> 3);  // the row this group owns
+  const bool own = r < n;
+  double vreg[4] = {0.0, 0.0, 0.0, 0.0}, wreg[4] = {0.0, 0.0, 0.0, 0.0};
+  double a_cur = (own && r >= p.k) ? AE(r, p.k) : 0.0;  // A(r, j) as the panel found it
+  double prev_tau = 0.0;
+  for (int i = 0; i <= p.ib; ++i) {
+    const int j = p.k + i;
+    const bool act = own && r >= j;
+    double anew = a_cur;
+    // ---------------- phase A
+    if (i > 0) {
+      const int il = i - 1;
+      double wv = act ? p.wvec[r] : 0.0;
+      if (wid == 0) {
+        double sacc = 0.0;
+        for (int b = lane; b < (int)gridDim.x; b += 32) sacc += p.partd[b];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) sacc += __shfl_down_sync(0xffffffffu, sacc, o);
+        if (lane == 0) s_sum = sacc;
+      } else if (threadIdx.x >= 32 && threadIdx.x < (unsigned)(32 + 2 * il)) {
+        const int dotq = threadIdx.x - 32, l = dotq >> 1;
+        double t = 0.0;
+        for (int ch = 0; ch < TCH; ++ch) t += p.tpart[dotq * TCH + ch];
+        if ((dotq & 1) == 0) s_t1[l] = t; else s_t2[l] = t;
+      } else if (wid == TPB / 32 - 1) {
+        for (int l = lane; l < i; l += 32) {
+          s_vj[l] = VP(j, l);
+          if (l < il) s_wj[l] = WP(j, l);
+        }
+        if (lane == 0) s_wjr = p.wvec[j];
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        double tt = 0.0;
+        for (int l = 0; l < il; ++l) tt += s_t1[l] * s_t2[l];
+        const double dot = prev_tau * (s_sum - 2.0 * tt);
+        const double ap = -0.5 * prev_tau * dot;
+        double corr = 0.0;
+        for (int l = 0; l < il; ++l) corr += s_vj[l] * s_t1[l] + s_wj[l] * s_t2[l];
+        s_wj[il] = prev_tau * (s_wjr - corr) + ap * s_vj[il];
+        s_scal[3] = ap;
+      }
+      __syncthreads();
+      const double alpha_prev = s_scal[3];
+      // W(r, il) from the group's registers
+      double corr = 0.0;
+      if (act) {
+#pragma unroll
+        for (int sl = 0; sl < 4; ++sl) {
+          const int l = q + 8 * sl;
+          if (l < il) corr += vreg[sl] * s_t1[l] + wreg[sl] * s_t2[l];
+        }
+      }
+      corr += __shfl_xor_sync(0xffffffffu, corr, 4);
+      corr += __shfl_xor_sync(0xffffffffu, corr, 2);
+      corr += __shfl_xor_sync(0xffffffffu, corr, 1);
+      const int sil = il >> 3;
+      const double vsel = sil == 0 ? vreg[0] : (sil == 1 ? vreg[1] : (sil == 2 ? vreg[2] : vreg[3]));
+      const double v_il = __shfl_sync(0xffffffffu, vsel, gbase + (il & 7));
+      const double wr_il = act ? prev_tau * (wv - corr) + alpha_prev * v_il : 0.0;
+      if (q == (il & 7)) {
+        if (sil == 0) wreg[0] = wr_il; else if (sil == 1) wreg[1] = wr_il;
+        else if (sil == 2) wreg[2] = wr_il; else wreg[3] = wr_il;
+      }
+      if (act && q == 0) WP(r, il) = wr_il;
+      if (i == p.ib) break;  // last column of the panel: W(:, il) was all that was left
+      double upd = 0.0;
+      if (act) {
+#pragma unroll
+        for (int sl = 0; sl < 4; ++sl) {
+          const int l = q + 8 * sl;
+          if (l < i) upd += vreg[sl] * s_wj[l] + wreg[sl] * s_vj[l];
+        }
+      }
+      upd += __shfl_xor_sync(0xffffffffu, upd, 4);
+      upd += __shfl_xor_sync(0xffffffffu, upd, 2);
+      upd += __shfl_xor_sync(0xffffffffu, upd, 1);
+      anew = a_cur - upd;
+      if (act && q == 0) AE(r, j) = anew;
+    }
+    double sig = 0.0;
+    if (act && q == 0) {
+      if (r == j) p.d[j] = anew;
+      if (r >= j + 2) sig = anew * anew;
+    }
+    const double bs = block_sum(sig, sh);
+    if (threadIdx.x == 0) p.part[blockIdx.x] = bs;
+    grid.sync();
+    // ---------------- phase D
+    if (wid == 0) {
+      double sacc = 0.0;
+      for (int b = lane; b < (int)gridDim.x; b += 32) sacc += p.part[b];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) sacc += __shfl_down_sync(0xffffffffu, sacc, o);
+      if (lane == 0) s_sum = sacc;
+    } else if (wid == 1 && lane == 0) {
+      s_alpha = AE(j + 1, j);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      const double snorm = s_sum, alpha = s_alpha;
+      double beta, tau, scal;
+      if (snorm == 0.0) {
+        beta = alpha; tau = 0.0; scal = 0.0;
+      } else {
+        beta = -copysign(sqrt(alpha * alpha + snorm), alpha);
+        tau = (beta - alpha) / beta;
+        scal = 1.0 / (alpha - beta);
+      }
+      s_scal[0] = tau;
+      s_scal[1] = scal;
+      s_scal[2] = beta;
+    }
+    __syncthreads();
+    const double tau = s_scal[0], scal = s_scal[1];
+    if (gtid == 0) {
+      p.e[j] = s_scal[2];
+      p.tau[j] = tau;
+    }
+    {
+      const double v = !own ? 0.0 : (r == j + 1 ? 1.0 : (r > j + 1 ? anew * scal : 0.0));
+      const int si = i >> 3;
+      if (q == (i & 7)) {
+        if (si == 0) vreg[0] = v; else if (si == 1) vreg[1] = v; else if (si == 2) vreg[2] = v; else vreg[3] = v;
+      }
+      if (own && q == 0) {
+        VP(r, i) = v;
+        p.vall[(long long)j * n + r] = v;
+      }
+    }
+    // p(r) = sum_{c > j} A(c, r) v(c) with wpr warps of one CTA per row
+    double pvw = 0.0;
+    {
+      const int R = n - j - 1;
+      int wpr = 1;
+      while (wpr < 8 && (long long)gridDim.x * (TPB / 32 / (wpr * 2)) >= R) wpr *= 2;
+      const int rpc = (TPB / 32) / wpr;
+      const int sub = wid % wpr;
+      const double* colj = A + (long long)j * lda;
+      const int rounds = (R + (int)gridDim.x * rpc - 1) / ((int)gridDim.x * rpc);
+      for (int t = 0; t < rounds; ++t) {
+        const int rho = (t * (int)gridDim.x + (int)blockIdx.x) * rpc + wid / wpr;
+        const int rr = j + 1 + rho;
+        double acc = 0.0;
+        if (rho < R) {
+          const double* colr = A + (long long)rr * lda;
+          double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0, acc3 = 0.0;
+          const int step = 32 * wpr;
+          int c = j + 1 + lane + 32 * sub;
+          for (; c + 7 * step < n; c += 8 * step) {
+            double x[8], y[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) x[u] = __ldcs(colr + c + step * u);
+#pragma unroll
+            for (int u = 0; u < 8; ++u) y[u] = colj[c + step * u];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+              const double v = (c + step * u == j + 1) ? 1.0 : y[u] * scal;
+              if ((u & 3) == 0) acc0 += x[u] * v;
+              else if ((u & 3) == 1) acc1 += x[u] * v;
+              else if ((u & 3) == 2) acc2 += x[u] * v;
+              else acc3 += x[u] * v;
+            }
+          }
+          for (; c < n; c += step) {
+            const double v = (c == j + 1) ? 1.0 : colj[c] * scal;
+            acc0 += colr[c] * v;
+          }
+          acc = (acc0 + acc1) + (acc2 + acc3);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+        if (wpr > 1) {
+          if (lane == 0) s_symv[wid] = acc;
+          __syncthreads();
+          if (sub == 0 && lane == 0 && rho < R) {
+            double tot = 0.0;
+            for (int u = 0; u < wpr; ++u) tot += s_symv[wid + u];
+            acc = tot;
+          }
+          __syncthreads();
+        }
+        if (sub == 0 && lane == 0 && rho < R) {
+          p.wvec[rr] = acc;
+          const double vr = (rr == j + 1) ? 1.0 : colj[rr] * scal;
+          pvw += acc * vr;
+        }
+      }
+      for (int rz = (int)gtid; rz <= j && rz < n; rz += (int)gstride) p.wvec[rz] = 0.0;
+    }
+    if (lane == 0) s_pv[wid] = pvw;
+    // t1/t2 chunk partials (TCH row chunks per dot product)
+    {
+      const int rows = n - (j + 1);
+      const int chunk = (rows + TCH - 1) / TCH;
+      for (int qq = nwarps - 1 - gwarp; qq < 2 * i * TCH; qq += nwarps) {
+        const int dotq = qq / TCH, ch = qq % TCH;
+        const int l = dotq >> 1;
+        const bool isw = (dotq & 1) == 0;
+        const double* col = isw ? p.wp + (long long)l * n : p.vp + (long long)l * n;
+        const int rb = j + 1 + ch * chunk, re = min(n, rb + chunk);
+        double acc = 0.0;
+        for (int rw = rb + lane; rw < re; rw += 32) {
+          const double v = (rw == j + 1) ? 1.0 : AE(rw, j) * scal;
+          acc += col[rw] * v;
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+        if (lane == 0) p.tpart[qq] = acc;
+      }
+    }
+    // the next column of A for this row, in flight across the barrier
+    a_cur = (own && r >= j + 1 && i < p.ib) ? AE(r, j + 1) : 0.0;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += s_pv[w];
+      p.partd[blockIdx.x] = t;
+    }
+    prev_tau = tau;
+    grid.sync();
+  }
+#undef AE
+#undef VP
+#undef WP
+}
+
 __global__ void copy_last_diag(int n, const double* a, int lda, double* d) {
   if (threadIdx.x == 0 && blockIdx.x == 0) d[n - 1] = a[(long long)(n - 1) * lda + (n - 1)];
 }
@@ -606,7 +861,10 @@ extern "C" int mb_eigh_ws(int n, double* fpacked, int perturb, double* c, double
     int dev = 0, sms = 0, per = 0;
     MB_CUDA(cudaGetDevice(&dev));
     MB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    int per2 = 0;
     MB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, tridiag_panel, TPB, 0));
+    MB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per2, tridiag_panel2, TPB, 0));
+    if (per2 < per) per = per2;
     if (per > 4) per = 4;
     if (per < 1) return mb_set_error(MB_ERR_CUDA, "tridiag_panel: cannot be co-resident");
     grid_cached = sms * per;
@@ -622,7 +880,9 @@ extern "C" int mb_eigh_ws(int n, double* fpacked, int perturb, double* c, double
     pa.part = part; pa.partd = part + 1024; pa.tvec = tvec; pa.tpart = tpart; pa.wvec = wvec;
     void* args[] = {&pa};
     mb_kstat_mark(MB_KSTAT_TRIDIAG, stream, true);
-    MB_CUDA(cudaLaunchCooperativeKernel((void*)tridiag_panel, grid, TPB, args, 0, stream));
+    // rows own 8-lane groups when the grid has enough of them
+    void* kfn = ((long long)grid * TPB / 8 >= n) ? (void*)tridiag_panel2 : (void*)tridiag_panel;
+    MB_CUDA(cudaLaunchCooperativeKernel(kfn, grid, TPB, args, 0, stream));
     mb_kstat_mark(MB_KSTAT_TRIDIAG, stream, false);
     mb_count_launch();
     const int t = k + ib;
