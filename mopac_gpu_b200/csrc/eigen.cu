@@ -29,6 +29,7 @@ namespace {
 constexpr int NB = 32;         // panel width
 constexpr int TPB = 256;       // threads per CTA in the panel kernel
 constexpr int TCH = 16;        // row chunks per dot product in t1/t2
+constexpr int PANEL2_SMEM_MAX = 8192 * 8;  // dynamic shared memory of the second panel form (v, n <= 8192)
 
 struct PanelArgs {
   int n, k, ib, lda;
@@ -298,7 +299,7 @@ __global__ void __launch_bounds__(TPB) tridiag_panel(PanelArgs p) {
 // warps of one CTA as the trailing matrix shrinks, so late columns are not
 // bound by one warp's chain of loads.  Arithmetic per element follows the
 // first form, except that p(r) is summed in wpr column slices for wpr > 1.
-__global__ void __launch_bounds__(TPB, 3) tridiag_panel2(PanelArgs p) {
+__global__ void __launch_bounds__(TPB) tridiag_panel2(PanelArgs p) {
   cg::grid_group grid = cg::this_grid();
   __shared__ double sh[32];
   __shared__ double s_scal[4];
@@ -306,18 +307,22 @@ __global__ void __launch_bounds__(TPB, 3) tridiag_panel2(PanelArgs p) {
   __shared__ double s_vj[NB], s_wj[NB], s_t1[NB], s_t2[NB];
   __shared__ double s_pv[TPB / 32];
   __shared__ double s_symv[TPB / 32];
+  __shared__ double s_gv[TPB / 8][NB], s_gw[TPB / 8][NB];  // V(r, l), W(r, l) of the CTA's rows
+  extern __shared__ double s_v[];                          // v of the current column, n entries
   const int n = p.n, lda = p.lda;
   const long long gtid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long gstride = (long long)gridDim.x * blockDim.x;
   const int gwarp = (int)(gtid >> 5), nwarps = (int)(gstride >> 5), lane = threadIdx.x & 31;
-  const int wid = threadIdx.x >> 5, q = lane & 7, gbase = lane & ~7;
+  const int wid = threadIdx.x >> 5, q = lane & 7;
   double* A = p.a;
 #define AE(r, c) A[(long long)(c) * lda + (r)]
 #define VP(r, c) p.vp[(long long)(c) * n + (r)]
 #define WP(r, c) p.wp[(long long)(c) * n + (r)]
   const int r = (int)(gtid >> 3);  // the row this group owns
   const bool own = r < n;
-  double vreg[4] = {0.0, 0.0, 0.0, 0.0}, wreg[4] = {0.0, 0.0, 0.0, 0.0};
+  const int g = threadIdx.x >> 3;
+  double* gv = s_gv[g];
+  double* gw = s_gw[g];
   double a_cur = (own && r >= p.k) ? AE(r, p.k) : 0.0;  // A(r, j) as the panel found it
   double prev_tau = 0.0;
   for (int i = 0; i <= p.ib; ++i) {
@@ -361,34 +366,22 @@ __global__ void __launch_bounds__(TPB, 3) tridiag_panel2(PanelArgs p) {
       const double alpha_prev = s_scal[3];
       // W(r, il) from the group's registers
       double corr = 0.0;
-      if (act) {
-#pragma unroll
-        for (int sl = 0; sl < 4; ++sl) {
-          const int l = q + 8 * sl;
-          if (l < il) corr += vreg[sl] * s_t1[l] + wreg[sl] * s_t2[l];
-        }
-      }
+      if (act)
+        for (int l = q; l < il; l += 8) corr += gv[l] * s_t1[l] + gw[l] * s_t2[l];
       corr += __shfl_xor_sync(0xffffffffu, corr, 4);
       corr += __shfl_xor_sync(0xffffffffu, corr, 2);
       corr += __shfl_xor_sync(0xffffffffu, corr, 1);
-      const int sil = il >> 3;
-      const double vsel = sil == 0 ? vreg[0] : (sil == 1 ? vreg[1] : (sil == 2 ? vreg[2] : vreg[3]));
-      const double v_il = __shfl_sync(0xffffffffu, vsel, gbase + (il & 7));
-      const double wr_il = act ? prev_tau * (wv - corr) + alpha_prev * v_il : 0.0;
-      if (q == (il & 7)) {
-        if (sil == 0) wreg[0] = wr_il; else if (sil == 1) wreg[1] = wr_il;
-        else if (sil == 2) wreg[2] = wr_il; else wreg[3] = wr_il;
-      }
+      const double wr_il = act ? prev_tau * (wv - corr) + alpha_prev * gv[il] : 0.0;
       if (act && q == 0) WP(r, il) = wr_il;
       if (i == p.ib) break;  // last column of the panel: W(:, il) was all that was left
       double upd = 0.0;
-      if (act) {
-#pragma unroll
-        for (int sl = 0; sl < 4; ++sl) {
-          const int l = q + 8 * sl;
-          if (l < i) upd += vreg[sl] * s_wj[l] + wreg[sl] * s_vj[l];
+      if (act)
+        for (int l = q; l < i; l += 8) {
+          const double wrl = (l == il) ? wr_il : gw[l];
+          upd += gv[l] * s_wj[l] + wrl * s_vj[l];
         }
-      }
+      __syncwarp();
+      if (q == (il & 7)) gw[il] = wr_il;
       upd += __shfl_xor_sync(0xffffffffu, upd, 4);
       upd += __shfl_xor_sync(0xffffffffu, upd, 2);
       upd += __shfl_xor_sync(0xffffffffu, upd, 1);
@@ -436,15 +429,21 @@ __global__ void __launch_bounds__(TPB, 3) tridiag_panel2(PanelArgs p) {
     }
     {
       const double v = !own ? 0.0 : (r == j + 1 ? 1.0 : (r > j + 1 ? anew * scal : 0.0));
-      const int si = i >> 3;
-      if (q == (i & 7)) {
-        if (si == 0) vreg[0] = v; else if (si == 1) vreg[1] = v; else if (si == 2) vreg[2] = v; else vreg[3] = v;
-      }
-      if (own && q == 0) {
-        VP(r, i) = v;
-        p.vall[(long long)j * n + r] = v;
+      if (q == 0) {
+        gv[i] = v;
+        if (own) {
+          VP(r, i) = v;
+          p.vall[(long long)j * n + r] = v;
+        }
       }
     }
+    // v(c) for the whole column, once per CTA (A(c, j) was final at the barrier)
+    {
+      const double* colj = A + (long long)j * lda;
+      for (int c = threadIdx.x; c < n; c += TPB)
+        s_v[c] = c <= j ? 0.0 : (c == j + 1 ? 1.0 : colj[c] * scal);
+    }
+    __syncthreads();
     // p(r) = sum_{c > j} A(c, r) v(c) with wpr warps of one CTA per row
     double pvw = 0.0;
     {
@@ -453,7 +452,6 @@ __global__ void __launch_bounds__(TPB, 3) tridiag_panel2(PanelArgs p) {
       while (wpr < 8 && (long long)gridDim.x * (TPB / 32 / (wpr * 2)) >= R) wpr *= 2;
       const int rpc = (TPB / 32) / wpr;
       const int sub = wid % wpr;
-      const double* colj = A + (long long)j * lda;
       const int rounds = (R + (int)gridDim.x * rpc - 1) / ((int)gridDim.x * rpc);
       for (int t = 0; t < rounds; ++t) {
         const int rho = (t * (int)gridDim.x + (int)blockIdx.x) * rpc + wid / wpr;
@@ -465,24 +463,19 @@ __global__ void __launch_bounds__(TPB, 3) tridiag_panel2(PanelArgs p) {
           const int step = 32 * wpr;
           int c = j + 1 + lane + 32 * sub;
           for (; c + 7 * step < n; c += 8 * step) {
-            double x[8], y[8];
+            double x[8];
 #pragma unroll
             for (int u = 0; u < 8; ++u) x[u] = __ldcs(colr + c + step * u);
 #pragma unroll
-            for (int u = 0; u < 8; ++u) y[u] = colj[c + step * u];
-#pragma unroll
             for (int u = 0; u < 8; ++u) {
-              const double v = (c + step * u == j + 1) ? 1.0 : y[u] * scal;
+              const double v = s_v[c + step * u];
               if ((u & 3) == 0) acc0 += x[u] * v;
               else if ((u & 3) == 1) acc1 += x[u] * v;
               else if ((u & 3) == 2) acc2 += x[u] * v;
               else acc3 += x[u] * v;
             }
           }
-          for (; c < n; c += step) {
-            const double v = (c == j + 1) ? 1.0 : colj[c] * scal;
-            acc0 += colr[c] * v;
-          }
+          for (; c < n; c += step) acc0 += colr[c] * s_v[c];
           acc = (acc0 + acc1) + (acc2 + acc3);
         }
 #pragma unroll
@@ -499,8 +492,7 @@ __global__ void __launch_bounds__(TPB, 3) tridiag_panel2(PanelArgs p) {
         }
         if (sub == 0 && lane == 0 && rho < R) {
           p.wvec[rr] = acc;
-          const double vr = (rr == j + 1) ? 1.0 : colj[rr] * scal;
-          pvw += acc * vr;
+          pvw += acc * s_v[rr];
         }
       }
       for (int rz = (int)gtid; rz <= j && rz < n; rz += (int)gstride) p.wvec[rz] = 0.0;
@@ -517,10 +509,7 @@ __global__ void __launch_bounds__(TPB, 3) tridiag_panel2(PanelArgs p) {
         const double* col = isw ? p.wp + (long long)l * n : p.vp + (long long)l * n;
         const int rb = j + 1 + ch * chunk, re = min(n, rb + chunk);
         double acc = 0.0;
-        for (int rw = rb + lane; rw < re; rw += 32) {
-          const double v = (rw == j + 1) ? 1.0 : AE(rw, j) * scal;
-          acc += col[rw] * v;
-        }
+        for (int rw = rb + lane; rw < re; rw += 32) acc += col[rw] * s_v[rw];
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
         if (lane == 0) p.tpart[qq] = acc;
@@ -855,22 +844,30 @@ extern "C" int mb_eigh_ws(int n, double* fpacked, int perturb, double* c, double
   MB_CUDA(cudaMemsetAsync(V, 0, sizeof(double) * nn, stream));
   MB_CUDA(cudaMemsetAsync(e, 0, sizeof(double) * n, stream));
 
-  // cooperative grid size: co-resident CTAs
-  static int grid_cached = 0;
-  if (grid_cached == 0) {
-    int dev = 0, sms = 0, per = 0;
+  // cooperative grid size: co-resident CTAs of the panel form in use
+  static int sms = 0, per1 = 0;
+  if (sms == 0) {
+    int dev = 0;
     MB_CUDA(cudaGetDevice(&dev));
     MB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    int per2 = 0;
-    MB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, tridiag_panel, TPB, 0));
-    MB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per2, tridiag_panel2, TPB, 0));
-    if (per2 < per) per = per2;
-    if (per > 4) per = 4;
-    if (per < 1) return mb_set_error(MB_ERR_CUDA, "tridiag_panel: cannot be co-resident");
-    grid_cached = sms * per;
-    if (grid_cached > 1024) grid_cached = 1024;
+    MB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per1, tridiag_panel, TPB, 0));
+    if (per1 > 4) per1 = 4;
+    if (per1 < 1) return mb_set_error(MB_ERR_CUDA, "tridiag_panel: cannot be co-resident");
+    MB_CUDA(cudaFuncSetAttribute(tridiag_panel2, cudaFuncAttributeMaxDynamicSharedMemorySize, PANEL2_SMEM_MAX));
   }
-  const int grid = grid_cached;
+  const size_t smem2 = sizeof(double) * (size_t)n;
+  bool v2 = smem2 <= (size_t)PANEL2_SMEM_MAX;
+  int per = per1;
+  if (v2) {
+    int per2 = 0;
+    MB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per2, tridiag_panel2, TPB, smem2));
+    if (per2 > 4) per2 = 4;
+    // every row needs its own 8-lane group
+    if (per2 >= 1 && (long long)sms * per2 * TPB / 8 >= n) per = per2;
+    else v2 = false;
+  }
+  int grid = sms * per;
+  if (grid > 1024) grid = 1024;
   for (int k = 0; k < n - 1; k += NB) {
     const int ib = (NB < n - 1 - k) ? NB : n - 1 - k;
     MB_CUDA(cudaMemsetAsync(vwv, 0, sizeof(double) * (size_t)n * 2 * NB, stream));
@@ -881,8 +878,8 @@ extern "C" int mb_eigh_ws(int n, double* fpacked, int perturb, double* c, double
     void* args[] = {&pa};
     mb_kstat_mark(MB_KSTAT_TRIDIAG, stream, true);
     // rows own 8-lane groups when the grid has enough of them
-    void* kfn = ((long long)grid * TPB / 8 >= n) ? (void*)tridiag_panel2 : (void*)tridiag_panel;
-    MB_CUDA(cudaLaunchCooperativeKernel(kfn, grid, TPB, args, 0, stream));
+    void* kfn = v2 ? (void*)tridiag_panel2 : (void*)tridiag_panel;
+    MB_CUDA(cudaLaunchCooperativeKernel(kfn, grid, TPB, args, v2 ? smem2 : 0, stream));
     mb_kstat_mark(MB_KSTAT_TRIDIAG, stream, false);
     mb_count_launch();
     const int t = k + ib;
