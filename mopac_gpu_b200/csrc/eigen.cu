@@ -29,7 +29,6 @@ namespace {
 constexpr int NB = 32;         // panel width
 constexpr int TPB = 256;       // threads per CTA in the panel kernel
 constexpr int TCH = 16;        // row chunks per dot product in t1/t2
-constexpr int PANEL2_SMEM_MAX = 8192 * 8;  // dynamic shared memory of the second panel form (v, n <= 8192)
 
 struct PanelArgs {
   int n, k, ib, lda;
@@ -308,7 +307,6 @@ __global__ void __launch_bounds__(TPB) tridiag_panel2(PanelArgs p) {
   __shared__ double s_pv[TPB / 32];
   __shared__ double s_symv[TPB / 32];
   __shared__ double s_gv[TPB / 8][NB], s_gw[TPB / 8][NB];  // V(r, l), W(r, l) of the CTA's rows
-  extern __shared__ double s_v[];                          // v of the current column, n entries
   const int n = p.n, lda = p.lda;
   const long long gtid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long gstride = (long long)gridDim.x * blockDim.x;
@@ -437,13 +435,7 @@ __global__ void __launch_bounds__(TPB) tridiag_panel2(PanelArgs p) {
         }
       }
     }
-    // v(c) for the whole column, once per CTA (A(c, j) was final at the barrier)
-    {
-      const double* colj = A + (long long)j * lda;
-      for (int c = threadIdx.x; c < n; c += TPB)
-        s_v[c] = c <= j ? 0.0 : (c == j + 1 ? 1.0 : colj[c] * scal);
-    }
-    __syncthreads();
+    const double* colj = A + (long long)j * lda;
     // p(r) = sum_{c > j} A(c, r) v(c) with wpr warps of one CTA per row
     double pvw = 0.0;
     {
@@ -463,19 +455,24 @@ __global__ void __launch_bounds__(TPB) tridiag_panel2(PanelArgs p) {
           const int step = 32 * wpr;
           int c = j + 1 + lane + 32 * sub;
           for (; c + 7 * step < n; c += 8 * step) {
-            double x[8];
+            double x[8], y[8];
 #pragma unroll
             for (int u = 0; u < 8; ++u) x[u] = __ldcs(colr + c + step * u);
 #pragma unroll
+            for (int u = 0; u < 8; ++u) y[u] = colj[c + step * u];
+#pragma unroll
             for (int u = 0; u < 8; ++u) {
-              const double v = s_v[c + step * u];
+              const double v = (c + step * u == j + 1) ? 1.0 : y[u] * scal;
               if ((u & 3) == 0) acc0 += x[u] * v;
               else if ((u & 3) == 1) acc1 += x[u] * v;
               else if ((u & 3) == 2) acc2 += x[u] * v;
               else acc3 += x[u] * v;
             }
           }
-          for (; c < n; c += step) acc0 += colr[c] * s_v[c];
+          for (; c < n; c += step) {
+            const double v = (c == j + 1) ? 1.0 : colj[c] * scal;
+            acc0 += colr[c] * v;
+          }
           acc = (acc0 + acc1) + (acc2 + acc3);
         }
 #pragma unroll
@@ -492,7 +489,8 @@ __global__ void __launch_bounds__(TPB) tridiag_panel2(PanelArgs p) {
         }
         if (sub == 0 && lane == 0 && rho < R) {
           p.wvec[rr] = acc;
-          pvw += acc * s_v[rr];
+          const double vr = (rr == j + 1) ? 1.0 : colj[rr] * scal;
+          pvw += acc * vr;
         }
       }
       for (int rz = (int)gtid; rz <= j && rz < n; rz += (int)gstride) p.wvec[rz] = 0.0;
@@ -509,7 +507,10 @@ __global__ void __launch_bounds__(TPB) tridiag_panel2(PanelArgs p) {
         const double* col = isw ? p.wp + (long long)l * n : p.vp + (long long)l * n;
         const int rb = j + 1 + ch * chunk, re = min(n, rb + chunk);
         double acc = 0.0;
-        for (int rw = rb + lane; rw < re; rw += 32) acc += col[rw] * s_v[rw];
+        for (int rw = rb + lane; rw < re; rw += 32) {
+          const double v = (rw == j + 1) ? 1.0 : AE(rw, j) * scal;
+          acc += col[rw] * v;
+        }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
         if (lane == 0) p.tpart[qq] = acc;
@@ -853,15 +854,14 @@ extern "C" int mb_eigh_ws(int n, double* fpacked, int perturb, double* c, double
     MB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per1, tridiag_panel, TPB, 0));
     if (per1 > 4) per1 = 4;
     if (per1 < 1) return mb_set_error(MB_ERR_CUDA, "tridiag_panel: cannot be co-resident");
-    MB_CUDA(cudaFuncSetAttribute(tridiag_panel2, cudaFuncAttributeMaxDynamicSharedMemorySize, PANEL2_SMEM_MAX));
   }
-  const size_t smem2 = sizeof(double) * (size_t)n;
-  bool v2 = smem2 <= (size_t)PANEL2_SMEM_MAX;
+  const size_t smem2 = 0;
+  bool v2 = true;
   int per = per1;
   if (v2) {
     int per2 = 0;
     MB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per2, tridiag_panel2, TPB, smem2));
-    if (per2 > 4) per2 = 4;
+    if (per2 > 3) per2 = 3;  // wider grids cost more per barrier than they add in bandwidth
     // every row needs its own 8-lane group
     if (per2 >= 1 && (long long)sms * per2 * TPB / 8 >= n) per = per2;
     else v2 = false;
@@ -879,7 +879,7 @@ extern "C" int mb_eigh_ws(int n, double* fpacked, int perturb, double* c, double
     mb_kstat_mark(MB_KSTAT_TRIDIAG, stream, true);
     // rows own 8-lane groups when the grid has enough of them
     void* kfn = v2 ? (void*)tridiag_panel2 : (void*)tridiag_panel;
-    MB_CUDA(cudaLaunchCooperativeKernel(kfn, grid, TPB, args, v2 ? smem2 : 0, stream));
+    MB_CUDA(cudaLaunchCooperativeKernel(kfn, grid, TPB, args, 0, stream));
     mb_kstat_mark(MB_KSTAT_TRIDIAG, stream, false);
     mb_count_launch();
     const int t = k + ib;
