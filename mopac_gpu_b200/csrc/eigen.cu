@@ -543,10 +543,22 @@ __device__ __forceinline__ int sturm_count(int n, const double* __restrict__ d, 
   double q = d[0] - x;
   if (fabs(q) < pivmin) q = -pivmin;
   cnt += q < 0.0;
-  for (int i = 1; i < n; ++i) {
-    q = d[i] - x - e2[i - 1] / q;
-    if (fabs(q) < pivmin) q = -pivmin;
-    cnt += q < 0.0;
+  // operands of eight rows are fetched ahead of the dependent recurrence
+  for (int i0 = 1; i0 < n; i0 += 8) {
+    double db[8], eb[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int i = i0 + u;
+      db[u] = i < n ? d[i] : 0.0;
+      eb[u] = i < n ? e2[i - 1] : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      if (i0 + u >= n) break;
+      q = db[u] - x - eb[u] / q;
+      if (fabs(q) < pivmin) q = -pivmin;
+      cnt += q < 0.0;
+    }
   }
   return cnt;
 }
@@ -617,44 +629,63 @@ __global__ void bisect_kernel(int n, const double* __restrict__ d, const double*
 // --------------------------------------------------------- inverse iteration
 // LU with partial pivoting of T - lam I and solve, in place on x (stride ld).
 // u0/u1/u2 (stride ld) receive the U factor; pivots are re-derived per solve.
+// Both sweeps fetch eight rows of operands ahead of the dependent chain, so
+// the chain waits on arithmetic, not on one L2 round trip per row.
 __device__ void tri_solve(int n, const double* __restrict__ d, const double* __restrict__ e, double lam,
                           double tiny, double* u0, double* u1, double* u2, double* x, long long ld) {
+  constexpr int B = 8;
   // factorisation and forward substitution in one pass
-  double dd = d[0] - lam;      // current pivot row diagonal
+  double dd = d[0] - lam;          // current pivot row diagonal
   double du = n > 1 ? e[0] : 0.0;  // current pivot row super-diagonal
   double du2 = 0.0;
   double xr = x[0];
-  for (int i = 0; i < n - 1; ++i) {
-    const double sub = e[i];           // T(i+1, i)
-    const double dn = d[i + 1] - lam;  // T(i+1, i+1)
-    const double en = (i + 1 < n - 1) ? e[i + 1] : 0.0;
-    const double xn = x[(long long)(i + 1) * ld];
-    if (fabs(dd) >= fabs(sub)) {
-      // no interchange
-      double piv_ = dd;
-      if (fabs(piv_) < tiny) piv_ = copysign(tiny, piv_ == 0.0 ? 1.0 : piv_);
-      const double l = sub / piv_;
-      u0[(long long)i * ld] = piv_;
-      u1[(long long)i * ld] = du;
-      u2[(long long)i * ld] = du2;
-      x[(long long)i * ld] = xr;
-      dd = dn - l * du;
-      du = en;
-      du2 = 0.0;
-      xr = xn - l * xr;
-    } else {
-      // interchange rows i and i+1
-      const double l = dd / sub;
-      u0[(long long)i * ld] = sub;
-      u1[(long long)i * ld] = dn;
-      u2[(long long)i * ld] = en;
-      x[(long long)i * ld] = xn;
-      const double ndd = du - l * dn;
-      const double ndu = -l * en;
-      dd = ndd;
-      du = ndu;
-      du2 = 0.0;
-      xr = xr - l * xn;
+  for (int i0 = 0; i0 < n - 1; i0 += B) {
+    double sb[B], dnb[B], enb[B], xnb[B];
+#pragma unroll
+    for (int u = 0; u < B; ++u) {
+      const int i = i0 + u;
+      if (i < n - 1) {
+        sb[u] = e[i];
+        dnb[u] = d[i + 1];
+        enb[u] = (i + 1 < n - 1) ? e[i + 1] : 0.0;
+        xnb[u] = x[(long long)(i + 1) * ld];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < B; ++u) {
+      const int i = i0 + u;
+      if (i >= n - 1) break;
+      const double sub = sb[u];          // T(i+1, i)
+      const double dn = dnb[u] - lam;    // T(i+1, i+1)
+      const double en = enb[u];
+      const double xn = xnb[u];
+      if (fabs(dd) >= fabs(sub)) {
+        // no interchange
+        double piv_ = dd;
+        if (fabs(piv_) < tiny) piv_ = copysign(tiny, piv_ == 0.0 ? 1.0 : piv_);
+        const double l = sub / piv_;
+        u0[(long long)i * ld] = piv_;
+        u1[(long long)i * ld] = du;
+        u2[(long long)i * ld] = du2;
+        x[(long long)i * ld] = xr;
+        dd = dn - l * du;
+        du = en;
+        du2 = 0.0;
+        xr = xn - l * xr;
+      } else {
+        // interchange rows i and i+1
+        const double l = dd / sub;
+        u0[(long long)i * ld] = sub;
+        u1[(long long)i * ld] = dn;
+        u2[(long long)i * ld] = en;
+        x[(long long)i * ld] = xn;
+        const double ndd = du - l * dn;
+        const double ndu = -l * en;
+        dd = ndd;
+        du = ndu;
+        du2 = 0.0;
+        xr = xr - l * xn;
+      }
     }
   }
   double last = dd;
@@ -664,27 +695,64 @@ __device__ void tri_solve(int n, const double* __restrict__ d, const double* __r
   double x1 = xr / last;  // x[n-1]
   x[(long long)(n - 1) * ld] = x1;
   double x2 = 0.0;        // x[i+2]
-  for (int i = n - 2; i >= 0; --i) {
-    const double v = (x[(long long)i * ld] - u1[(long long)i * ld] * x1 - u2[(long long)i * ld] * x2) /
-                     u0[(long long)i * ld];
-    x[(long long)i * ld] = v;
-    x2 = x1;
-    x1 = v;
+  for (int i0 = n - 2; i0 >= 0; i0 -= B) {
+    double xb[B], a0[B], a1[B], a2[B];
+#pragma unroll
+    for (int u = 0; u < B; ++u) {
+      const int i = i0 - u;
+      if (i >= 0) {
+        xb[u] = x[(long long)i * ld];
+        a0[u] = u0[(long long)i * ld];
+        a1[u] = u1[(long long)i * ld];
+        a2[u] = u2[(long long)i * ld];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < B; ++u) {
+      const int i = i0 - u;
+      if (i < 0) break;
+      const double v = (xb[u] - a1[u] * x1 - a2[u] * x2) / a0[u];
+      x[(long long)i * ld] = v;
+      x2 = x1;
+      x1 = v;
+    }
   }
 }
 
 // x (stride ld) normalised to unit 2-norm; returns the norm before scaling.
+// Eight independent loads per step keep the three sweeps bandwidth-bound.
 __device__ double normalise(int n, double* x, long long ld) {
-  double s = 0.0, mx = 0.0;
-  for (int i = 0; i < n; ++i) mx = fmax(mx, fabs(x[(long long)i * ld]));
+  constexpr int B = 8;
+  double mx = 0.0;
+  for (int i0 = 0; i0 < n; i0 += B) {
+    double t[B];
+#pragma unroll
+    for (int u = 0; u < B; ++u) t[u] = (i0 + u < n) ? x[(long long)(i0 + u) * ld] : 0.0;
+#pragma unroll
+    for (int u = 0; u < B; ++u) mx = fmax(mx, fabs(t[u]));
+  }
   if (mx == 0.0) return 0.0;
   const double inv = 1.0 / mx;
-  for (int i = 0; i < n; ++i) {
-    double v = x[(long long)i * ld] * inv;
-    s += v * v;
+  double s = 0.0;
+  for (int i0 = 0; i0 < n; i0 += B) {
+    double t[B];
+#pragma unroll
+    for (int u = 0; u < B; ++u) t[u] = (i0 + u < n) ? x[(long long)(i0 + u) * ld] : 0.0;
+#pragma unroll
+    for (int u = 0; u < B; ++u) {
+      const double v = t[u] * inv;
+      s += v * v;
+    }
   }
   const double sc = inv / sqrt(s);
-  for (int i = 0; i < n; ++i) x[(long long)i * ld] *= sc;
+  for (int i0 = 0; i0 < n; i0 += B) {
+    double t[B];
+#pragma unroll
+    for (int u = 0; u < B; ++u) t[u] = (i0 + u < n) ? x[(long long)(i0 + u) * ld] : 0.0;
+#pragma unroll
+    for (int u = 0; u < B; ++u)
+      if (i0 + u < n) x[(long long)(i0 + u) * ld] = t[u] * sc;
+  }
   return mx * sqrt(s);
 }
 
