@@ -18,6 +18,8 @@ Cases (sizes of the benchmark configurations):
   density_split same with the three-product BF16 split on tcgen05
   gemm64, gemm_split   3072^3 GEMM, 2 n^3 flops
   eigh          full eigensolve n = 3072 (the SCF's Fock matrix)
+  eigh_rand     full eigensolve of a seeded random symmetric 3072 x 3072 matrix
+                (no SCF before it: the case to run under a launch-list capture)
   pseudo_diag   Fmo + rotation sweep, n = 3072, k = 2048
   pulay         one Pulay step with a full 10-entry history, n = 3072
   mz_density, mz_helecz, mz_cnvgz   MOZYME blocks, (H2O)4096, 9 A cutoff,
@@ -212,6 +214,23 @@ def run_cases(names, reps):
         out.append(line("eigh", ms, 4.5 * c1.n ** 3, "TFLOP/s", "fp64", fp64, "cuBLAS DGEMM here",
                         config="n = 3072 Fock matrix of (H2O)512", note="4.5 n^3 flop convention of the "
                         "reference's gpu_bench"))
+    if "eigh_rand" in names:
+        n = 3072
+        rng = np.random.default_rng(0)
+        a = rng.normal(size=(n, n))
+        rr, cc = np.tril_indices(n)
+        fpk = torch.from_numpy(np.ascontiguousarray((0.5 * (a + a.T))[rr, cc])).cuda()
+        work = fpk.clone()
+        cv = torch.empty(n * n, dtype=torch.float64, device="cuda")
+        ev = torch.empty(n, dtype=torch.float64, device="cuda")
+        nb = int(L.mb_eigh_ws_bytes(n))
+        buf, ws = kernels._aligned_ws(nb, "cuda", 256)
+        st = torch.zeros(4, dtype=torch.int32, device="cuda")
+        ms = timed(lambda: check(L.mb_eigh_ws(n, vp(work), 1, vp(cv), vp(ev), ws, vp(st), s())), reps, warm=1,
+                   setup=lambda: work.copy_(fpk))
+        assert int(st[0].item()) == 0
+        out.append(line("eigh_rand", ms, 4.5 * n ** 3, "TFLOP/s", "fp64", fp64_peak_tflops(), "cuBLAS DGEMM here",
+                        config="n = 3072 seeded random symmetric"))
     if "pseudo_diag" in names:
         cv = c1.c.clone()
         nrot = ctypes.c_longlong(0)
@@ -273,7 +292,8 @@ def run_cases(names, reps):
     return out
 
 
-ALL = ["fock2", "helect", "cnvg", "density64", "density_split", "gemm64", "gemm_split", "eigh", "pseudo_diag",
+ALL = ["fock2", "helect", "cnvg", "density64", "density_split", "gemm64", "gemm_split", "eigh", "eigh_rand",
+       "pseudo_diag",
        "pulay", "mz_density", "mz_helecz", "mz_cnvgz"]
 
 
