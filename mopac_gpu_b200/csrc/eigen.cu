@@ -537,6 +537,20 @@ __global__ void copy_last_diag(int n, const double* a, int lda, double* d) {
 }
 
 // ---------------------------------------------------------------- bisection
+// 1/q from the hardware's approximate reciprocal refined by two Newton steps,
+// r <- r + r (1 - q r): about 1e-16 relative, cheaper than the IEEE division.
+// |q| >= pivmin (a normal number) here, so flushing subnormals loses nothing.
+// A Sturm count is exact for a matrix within a few ulps of T, so the
+// eigenvalue bounds keep the bisection's accuracy.
+__device__ __forceinline__ double recip_nr2(double q) {
+  double r;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(q));
+  double e = fma(-q, r, 1.0);
+  r = fma(r, e, r);
+  e = fma(-q, r, 1.0);
+  return fma(r, e, r);
+}
+
 __device__ __forceinline__ int sturm_count(int n, const double* __restrict__ d, const double* __restrict__ e2,
                                            double x, double pivmin) {
   int cnt = 0;
@@ -555,7 +569,7 @@ __device__ __forceinline__ int sturm_count(int n, const double* __restrict__ d, 
 #pragma unroll
     for (int u = 0; u < 8; ++u) {
       if (i0 + u >= n) break;
-      q = db[u] - x - eb[u] / q;
+      q = db[u] - x - eb[u] * recip_nr2(q);
       if (fabs(q) < pivmin) q = -pivmin;
       cnt += q < 0.0;
     }
@@ -831,9 +845,17 @@ __global__ void transpose_kernel(int n, const double* __restrict__ X, double* __
 constexpr int BT = 64;  // reflectors per back-transformation block
 constexpr size_t LARFT_SMEM = sizeof(double) * 2 * BT * (BT + 1);
 
-__global__ void larft_kernel(int ib, const double* __restrict__ S, const double* __restrict__ tau,
-                             double* __restrict__ T) {
+// One CTA per block of reflectors: block b holds reflectors k = b*BT ..
+// k+ib-1 of nref, S and T at b*BT*BT.
+__global__ void larft_kernel(int nref, const double* __restrict__ Sall, const double* __restrict__ tau_all,
+                             double* __restrict__ Tall) {
   extern __shared__ double larft_sh[];
+  const int k = blockIdx.x * BT;
+  const int ib = (BT < nref - k) ? BT : nref - k;
+  if (ib <= 0) return;
+  const double* S = Sall + (size_t)blockIdx.x * BT * BT;
+  const double* tau = tau_all + k;
+  double* T = Tall + (size_t)blockIdx.x * BT * BT;
   double(*st)[BT + 1] = reinterpret_cast<double(*)[BT + 1]>(larft_sh);
   double(*ss)[BT + 1] = reinterpret_cast<double(*)[BT + 1]>(larft_sh + BT * (BT + 1));
   for (int q = threadIdx.x; q < ib * ib; q += blockDim.x) {
@@ -871,7 +893,7 @@ extern "C" int mb_dgemm_ws(char transa, char transb, int m, int n, int k, double
 extern "C" size_t mb_eigh_ws_bytes(int n) {
   size_t nn = (size_t)n * n;
   return sizeof(double) * (7 * nn + 3 * (size_t)n * NB + 5 * (size_t)n + 2 * NB + 2 * NB * TCH + 4096 +
-                           (size_t)BT * BT * 2 +
+                           (size_t)BT * BT * 2 * (size_t)((n + BT - 1) / BT) +
                            (size_t)BT * n) + 256;
 }
 
@@ -897,8 +919,9 @@ extern "C" int mb_eigh_ws(int n, double* fpacked, int perturb, double* c, double
   double* tvec = b; b += 2 * NB;
   double* tpart = b; b += 2 * NB * TCH;
   double* part = b; b += 4096;
-  double* S = b; b += (size_t)BT * BT;
-  double* Tm = b; b += (size_t)BT * BT;
+  const int nblk_bt = (n + BT - 1) / BT;
+  double* S = b; b += (size_t)BT * BT * nblk_bt;   // S_b = V_b^T V_b of every back-transformation block
+  double* Tm = b; b += (size_t)BT * BT * nblk_bt;  // their T factors
   double* Y = b; b += (size_t)BT * n;
   double* bnd = part + 2048;
 
@@ -991,17 +1014,26 @@ extern "C" int mb_eigh_ws(int n, double* fpacked, int perturb, double* c, double
     }
     const int nref = n - 1;  // reflectors 0 .. n-2
     const int last_k = ((nref - 1) / BT) * BT;
+    const int nblk = last_k / BT + 1;
+    // every block's T factor first (they depend on V only), in one launch
+    for (int k = 0; k <= last_k; k += BT) {
+      const int ib = (BT < nref - k) ? BT : nref - k;
+      const int r0 = k + 1;
+      const double* Vk = V + (size_t)k * n + r0;
+      MB_TRY(mb_dgemm_ws('T', 'N', ib, ib, n - r0, 1.0, Vk, n, Vk, n, 0.0, S + (size_t)(k / BT) * BT * BT, ib, U0,
+                         3 * nn, stream));
+    }
+    larft_kernel<<<nblk, BT, LARFT_SMEM, stream>>>(nref, S, tau, Tm);
+    MB_LAUNCH_CHECK();
     for (int k = last_k; k >= 0; k -= BT) {
       const int ib = (BT < nref - k) ? BT : nref - k;
       if (ib <= 0) continue;
       const int r0 = k + 1;  // first nonzero row of the block's reflectors
       const int m = n - r0;
       const double* Vk = V + (size_t)k * n + r0;
-      MB_TRY(mb_dgemm_ws('T', 'N', ib, ib, m, 1.0, Vk, n, Vk, n, 0.0, S, ib, U0, 3 * nn, stream));
-      larft_kernel<<<1, BT, LARFT_SMEM, stream>>>(ib, S, tau + k, Tm);
-      MB_LAUNCH_CHECK();
+      const double* Tk = Tm + (size_t)(k / BT) * BT * BT;
       MB_TRY(mb_dgemm_ws('T', 'N', ib, n, m, 1.0, Vk, n, Z + r0, n, 0.0, Y, ib, U0, 3 * nn, stream));
-      MB_TRY(mb_dgemm_dev('N', 'N', ib, n, ib, 1.0, Tm, ib, Y, ib, 0.0, X, ib, stream));
+      MB_TRY(mb_dgemm_dev('N', 'N', ib, n, ib, 1.0, Tk, ib, Y, ib, 0.0, X, ib, stream));
       MB_TRY(mb_dgemm_dev('N', 'N', m, n, ib, -1.0, Vk, n, X, ib, 1.0, Z + r0, n, stream));
     }
   }
