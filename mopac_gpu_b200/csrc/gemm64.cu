@@ -1,10 +1,14 @@
-// FP64 GEMM / packed SYRK on the CUDA cores (column-major, LAPACK argument
-// conventions).  B200 has the same FP64 rate on DMMA and FFMA, so a register-
-// tiled FFMA kernel is the FP64 baseline; the split-precision tensor-core path
-// lives in gemm_split.cu.
+// FP64 GEMM / packed SYRK (column-major, LAPACK argument conventions).
 //
-// Tile: 64 x 64 per CTA, BK = 16, 256 threads, 4 x 4 outputs per thread,
-// double-buffered shared memory fed by register staging.
+// Two tile engines:
+//  * DMMA: 128 x 128 per CTA, BK = 16, 8 warps of 64 x 32, each warp issuing
+//    mma.sync m8n8k4 f64 on the FP64 tensor path (8 x 4 fragments, 64
+//    accumulators per lane).  Used for every product whose output has more
+//    than 64 rows and columns.
+//  * FFMA: 64 x 64 per CTA, 4 x 4 outputs per thread; its 8 shared loads per
+//    16 FMAs bind it at half the FP64 rate, so it only serves skinny outputs.
+// Both double-buffer shared memory through register staging.  The
+// split-precision tensor-core path lives in gemm_tc.cu.
 #include "mb_common.cuh"
 
 namespace {
@@ -125,6 +129,159 @@ __global__ void __launch_bounds__(NT) dgemm_kernel(int m, int n, int k, double a
   }
 }
 
+// ------------------------------------------------------------------ DMMA
+constexpr int DBM = 128, DBN = 128, DBK = 16, DPAD = 4;  // row stride 132 doubles: conflict-free fragments
+constexpr int DMMA_SMEM = (int)sizeof(double) * 2 * DBK * (DBM + DPAD + DBN + DPAD);
+
+__device__ __forceinline__ void dmma(double (&c)[2], double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+               : "+d"(c[0]), "+d"(c[1])
+               : "d"(a), "d"(b));
+}
+
+// 128 x 128 tile of op(A) op(B) over k in [kbeg, kend).  Warp w covers rows
+// (w % 2) * 64 .. +64 and columns (w / 2) * 32 .. +32; fragment (i, j) of a
+// lane holds C(row0 + 8 i + lane / 4, col0 + 8 j + 2 (lane % 4) + {0, 1}).
+template <bool TA, bool TB>
+__device__ __forceinline__ void tile_dmma(const double* __restrict__ a, int lda, const double* __restrict__ b,
+                                          int ldb, int m, int n, int kbeg, int kend, int bm, int bn,
+                                          double (&acc)[8][4][2]) {
+  extern __shared__ double dmma_sh[];  // DMMA_SMEM bytes: As[2][DBK][DBM+DPAD], Bs[2][DBK][DBN+DPAD]
+  double(*As)[DBK][DBM + DPAD] = reinterpret_cast<double(*)[DBK][DBM + DPAD]>(dmma_sh);
+  double(*Bs)[DBK][DBN + DPAD] = reinterpret_cast<double(*)[DBK][DBN + DPAD]>(dmma_sh + 2 * DBK * (DBM + DPAD));
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int wm = (warp & 1) * 64, wn = (warp >> 1) * 32;
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+  double ra[8], rb[8];  // 128 x 16 tiles: 8 elements per thread each
+  auto gload = [&](int k0) {
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int e = tid + q * NT;
+      int r, kk;
+      if (TA) { kk = e % DBK; r = e / DBK; } else { r = e % DBM; kk = e / DBM; }
+      ra[q] = load_a<TA>(a, lda, m, kend, bm + r, k0 + kk);
+    }
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int e = tid + q * NT;
+      int cc, kk;
+      if (TB) { cc = e % DBN; kk = e / DBN; } else { kk = e % DBK; cc = e / DBK; }
+      rb[q] = load_b<TB>(b, ldb, n, kend, k0 + kk, bn + cc);
+    }
+  };
+  auto sstore = [&](int buf) {
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int e = tid + q * NT;
+      int r, kk;
+      if (TA) { kk = e % DBK; r = e / DBK; } else { r = e % DBM; kk = e / DBM; }
+      As[buf][kk][r] = ra[q];
+    }
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int e = tid + q * NT;
+      int cc, kk;
+      if (TB) { cc = e % DBN; kk = e / DBN; } else { kk = e % DBK; cc = e / DBK; }
+      Bs[buf][kk][cc] = rb[q];
+    }
+  };
+  const int nk = (kend - kbeg + DBK - 1) / DBK;
+  gload(kbeg);
+  sstore(0);
+  __syncthreads();
+  const int fr = lane >> 2, fk = lane & 3;
+  for (int t = 0; t < nk; ++t) {
+    const int cur = t & 1;
+    if (t + 1 < nk) gload(kbeg + (t + 1) * DBK);
+#pragma unroll
+    for (int kk = 0; kk < DBK; kk += 4) {
+      double av[8], bv[4];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) av[i] = As[cur][kk + fk][wm + 8 * i + fr];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) bv[j] = Bs[cur][kk + fk][wn + 8 * j + fr];
+#pragma unroll
+      for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) dmma(acc[i][j], av[i], bv[j]);
+    }
+    if (t + 1 < nk) sstore(cur ^ 1);
+    __syncthreads();
+  }
+}
+
+template <bool TA, bool TB>
+__global__ void __launch_bounds__(NT) dgemm_dmma_kernel(int m, int n, int k, double alpha,
+                                                        const double* __restrict__ a, int lda,
+                                                        const double* __restrict__ b, int ldb, double beta,
+                                                        double* __restrict__ c, int ldc) {
+  const int bm = blockIdx.y * DBM, bn = blockIdx.x * DBN;
+  const int kchunk = (k + gridDim.z - 1) / gridDim.z;
+  const int kb = blockIdx.z * kchunk, ke = min(k, kb + kchunk);
+  double acc[8][4][2];
+  tile_dmma<TA, TB>(a, lda, b, ldb, m, n, kb, ke, bm, bn, acc);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int r0 = bm + (warp & 1) * 64 + (lane >> 2), c0 = bn + (warp >> 1) * 32 + 2 * (lane & 3);
+  const bool partial = gridDim.z > 1;
+  double* cz = partial ? c + (long long)blockIdx.z * m * n : c;
+  const int ldz = partial ? m : ldc;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    const int r = r0 + 8 * i;
+    if (r >= m) continue;
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int t = 0; t < 2; ++t) {
+        const int cc = c0 + 8 * j + t;
+        if (cc >= n) continue;
+        double* p = cz + (long long)cc * ldz + r;
+        if (partial) *p = acc[i][j][t];
+        else *p = (beta == 0.0) ? alpha * acc[i][j][t] : alpha * acc[i][j][t] + beta * (*p);
+      }
+  }
+}
+
+// Packed lower P = occ * A A^T on the DMMA engine (tiles meeting the lower triangle).
+__global__ void __launch_bounds__(NT) syrk_packed_dmma_kernel(int n, int k, double occ, const double* __restrict__ a,
+                                                              int lda, double* __restrict__ p) {
+  const int bm = blockIdx.y * DBM, bn = blockIdx.x * DBN;
+  if (bn > bm + DBM - 1) return;
+  double acc[8][4][2];
+  tile_dmma<false, true>(a, lda, a, lda, n, n, 0, k, bm, bn, acc);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int r0 = bm + (warp & 1) * 64 + (lane >> 2), c0 = bn + (warp >> 1) * 32 + 2 * (lane & 3);
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    const int r = r0 + 8 * i;
+    if (r >= n) continue;
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int t = 0; t < 2; ++t) {
+        const int cc = c0 + 8 * j + t;
+        if (cc > r) continue;
+        p[mb_tri(r, cc)] = occ * acc[i][j][t];
+      }
+  }
+}
+
+// Opt the DMMA kernels into their dynamic shared memory once per process.
+int dmma_attrs() {
+  static bool done = false;
+  if (done) return MB_OK;
+  MB_CUDA(cudaFuncSetAttribute(dgemm_dmma_kernel<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, DMMA_SMEM));
+  MB_CUDA(cudaFuncSetAttribute(dgemm_dmma_kernel<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, DMMA_SMEM));
+  MB_CUDA(cudaFuncSetAttribute(dgemm_dmma_kernel<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, DMMA_SMEM));
+  MB_CUDA(cudaFuncSetAttribute(dgemm_dmma_kernel<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, DMMA_SMEM));
+  MB_CUDA(cudaFuncSetAttribute(syrk_packed_dmma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, DMMA_SMEM));
+  done = true;
+  return MB_OK;
+}
+
 // C = alpha * sum_z part[z] + beta * C, slices summed in order (deterministic).
 __global__ void splitk_reduce(int m, int n, int nz, double alpha, const double* __restrict__ part, double beta,
                               double* __restrict__ c, int ldc) {
@@ -172,20 +329,31 @@ extern "C" int mb_dgemm_ws(char transa, char transb, int m, int n, int k, double
   if (m == 0 || n == 0) return MB_OK;
   bool ta = (transa == 'T' || transa == 't' || transa == 'C' || transa == 'c');
   bool tb = (transb == 'T' || transb == 't' || transb == 'C' || transb == 'c');
-  const int tiles = ((n + BN - 1) / BN) * ((m + BM - 1) / BM);
+  const bool wide = m > BM && n > BN;  // DMMA engine for all but skinny outputs
+  const int tbm = wide ? DBM : BM, tbn = wide ? DBN : BN;
+  const int tiles = ((n + tbn - 1) / tbn) * ((m + tbm - 1) / tbm);
+  const int target = wide ? 148 : 296;
   int nz = 1;
-  if (ws && k >= 512 && tiles < 296) {
-    nz = (296 + tiles - 1) / tiles;
+  if (ws && k >= 512 && tiles < target) {
+    nz = (target + tiles - 1) / tiles;
     if (nz > k / 128) nz = k / 128;
     if (nz > 32) nz = 32;
     while (nz > 1 && (size_t)nz * m * n > ws_elems) --nz;
   }
-  dim3 grid((n + BN - 1) / BN, (m + BM - 1) / BM, nz);
+  dim3 grid((n + tbn - 1) / tbn, (m + tbm - 1) / tbm, nz);
   double* out = nz > 1 ? ws : c;
-  if (!ta && !tb) dgemm_kernel<false, false><<<grid, NT, 0, stream>>>(m, n, k, alpha, a, lda, b, ldb, beta, out, ldc);
-  else if (!ta && tb) dgemm_kernel<false, true><<<grid, NT, 0, stream>>>(m, n, k, alpha, a, lda, b, ldb, beta, out, ldc);
-  else if (ta && !tb) dgemm_kernel<true, false><<<grid, NT, 0, stream>>>(m, n, k, alpha, a, lda, b, ldb, beta, out, ldc);
-  else dgemm_kernel<true, true><<<grid, NT, 0, stream>>>(m, n, k, alpha, a, lda, b, ldb, beta, out, ldc);
+  if (wide) {
+    MB_TRY(dmma_attrs());
+    if (!ta && !tb) dgemm_dmma_kernel<false, false><<<grid, NT, DMMA_SMEM, stream>>>(m, n, k, alpha, a, lda, b, ldb, beta, out, ldc);
+    else if (!ta && tb) dgemm_dmma_kernel<false, true><<<grid, NT, DMMA_SMEM, stream>>>(m, n, k, alpha, a, lda, b, ldb, beta, out, ldc);
+    else if (ta && !tb) dgemm_dmma_kernel<true, false><<<grid, NT, DMMA_SMEM, stream>>>(m, n, k, alpha, a, lda, b, ldb, beta, out, ldc);
+    else dgemm_dmma_kernel<true, true><<<grid, NT, DMMA_SMEM, stream>>>(m, n, k, alpha, a, lda, b, ldb, beta, out, ldc);
+  } else {
+    if (!ta && !tb) dgemm_kernel<false, false><<<grid, NT, 0, stream>>>(m, n, k, alpha, a, lda, b, ldb, beta, out, ldc);
+    else if (!ta && tb) dgemm_kernel<false, true><<<grid, NT, 0, stream>>>(m, n, k, alpha, a, lda, b, ldb, beta, out, ldc);
+    else if (ta && !tb) dgemm_kernel<true, false><<<grid, NT, 0, stream>>>(m, n, k, alpha, a, lda, b, ldb, beta, out, ldc);
+    else dgemm_kernel<true, true><<<grid, NT, 0, stream>>>(m, n, k, alpha, a, lda, b, ldb, beta, out, ldc);
+  }
   MB_LAUNCH_CHECK();
   if (nz > 1) {
     long long mn = (long long)m * n;
@@ -210,9 +378,15 @@ extern "C" int mb_density_dev(int n, int nocc, double occ, const double* c, int 
     MB_CUDA(cudaMemsetAsync(p, 0, sizeof(double) * (size_t)n * (n + 1) / 2, stream));
     return MB_OK;
   }
-  dim3 grid((n + BN - 1) / BN, (n + BM - 1) / BM);
   mb_kstat_mark(MB_KSTAT_DENSITY, stream, true);
-  syrk_packed_kernel<<<grid, NT, 0, stream>>>(n, nocc, occ, c, ldc, p, grid.x);
+  if (n > BM) {
+    dim3 grid((n + DBN - 1) / DBN, (n + DBM - 1) / DBM);
+    MB_TRY(dmma_attrs());
+    syrk_packed_dmma_kernel<<<grid, NT, DMMA_SMEM, stream>>>(n, nocc, occ, c, ldc, p);
+  } else {
+    dim3 grid((n + BN - 1) / BN, (n + BM - 1) / BM);
+    syrk_packed_kernel<<<grid, NT, 0, stream>>>(n, nocc, occ, c, ldc, p, grid.x);
+  }
   mb_kstat_mark(MB_KSTAT_DENSITY, stream, false);
   MB_LAUNCH_CHECK();
   return MB_OK;

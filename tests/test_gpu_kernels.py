@@ -92,7 +92,10 @@ def test_density_fp64(n, k):
 
 
 @pytest.mark.parametrize("m,n,k,ta,tb", [(70, 50, 33, "N", "N"), (64, 64, 64, "T", "N"), (129, 17, 200, "N", "T"),
-                                         (31, 77, 45, "T", "T")])
+                                         (31, 77, 45, "T", "T"),
+                                         # DMMA engine (both output sides above 64)
+                                         (200, 150, 70, "N", "N"), (200, 150, 70, "T", "T"),
+                                         (513, 257, 1000, "N", "T"), (257, 513, 129, "T", "N"), (65, 65, 1, "N", "N")])
 def test_dgemm(m, n, k, ta, tb):
     from mopac_gpu_b200 import kernels as K
     rng = np.random.default_rng(m + n)
