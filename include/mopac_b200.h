@@ -220,6 +220,17 @@ typedef struct MbMzLayout {
   const int* pair_i;
   const int* pair_j;
   const long long* pair_off;
+  /* two-electron integrals of the stored pairs: entry e's block (100, 10 or
+   * 1 values for a pair, ilim^2 for an atom's own entry) at pair_woff[e], nw
+   * in all -- the dense W's order with the pairs outside cutof2 left out */
+  const long long* pair_woff;
+  long long nw;
+  /* every stored partner of atom a, both directions, ascending:
+   * nbr_atom[nbr_ptr[a] ..], with the pair entry of (max, min) in nbr_entry */
+  const int* nbr_ptr;
+  const int* nbr_atom;
+  const long long* nbr_entry;
+  double cutof1, cutof2;
 } MbMzLayout;
 /* Occupied LMOs on the device: cocc as in MOZYME_C plus, per atom, the LMOs
  * containing it (ascending) and the offset of its coefficients in cocc. */
@@ -251,6 +262,18 @@ int mb_mz_lmos_destroy(MbMzLmos* lmos);
  * loop. */
 int mb_mz_density_dev(const MbMzLayout* layout, const MbMzLmos* lmos, int mode, const double* partp,
                       double* p, cudaStream_t stream);
+/* buildf(f, partf, 0) -> fock2z (MOZYME/buildf.F90:16, fock2z.F90:669-1293),
+ * whole-F mode, direct and semi-direct (the reference's defaults), s/p atoms:
+ * F = H + the two-electron terms of the stored pairs (w: their integrals in
+ * pair_woff order), the point-charge monopole qe(b) ev a0 / r of every
+ * other pair, then each atom's one-centre terms.  coord: device, numat x 3
+ * Angstrom.  Needs cutof2 >= 49 (7 A), where the reference's feathering
+ * weight is exactly zero for every pair outside the cutoff, so its dipole
+ * terms vanish.  Bit-identical to the reference's loop. */
+size_t mb_mz_fock_ws_bytes(const MbMzLayout* layout);
+int mb_mz_fock_dev(const MbMzLayout* layout, const double* coord, const double* w, const double* ptot,
+                   const double* h, double* f, void* ws, cudaStream_t stream);
+
 /* helecz() (MOZYME/helecz.F90:16): sum p(h+f) with diagonal elements
  * weighted 1/2; *out (device).  Fixed-order parallel reduction. */
 size_t mb_mz_helecz_ws_bytes(void);

@@ -30,7 +30,9 @@ class MbAtomsDev(ctypes.Structure):
 class MbMzLayout(ctypes.Structure):
     _fields_ = [("numat", ctypes.c_int), ("mpack", ctypes.c_longlong), ("npairs", ctypes.c_longlong),
                 ("iorbs", ctypes.c_void_p), ("pair_ptr", ctypes.c_void_p), ("pair_i", ctypes.c_void_p),
-                ("pair_j", ctypes.c_void_p), ("pair_off", ctypes.c_void_p)]
+                ("pair_j", ctypes.c_void_p), ("pair_off", ctypes.c_void_p), ("pair_woff", ctypes.c_void_p),
+                ("nw", ctypes.c_longlong), ("nbr_ptr", ctypes.c_void_p), ("nbr_atom", ctypes.c_void_p),
+                ("nbr_entry", ctypes.c_void_p), ("cutof1", ctypes.c_double), ("cutof2", ctypes.c_double)]
 
 
 class MbMzLmos(ctypes.Structure):
@@ -97,6 +99,8 @@ SIGNATURES = {
     "mb_mz_lmos_create": ([_I, _P, _I, _P, _P, _P, _P, _P, _LL, ctypes.POINTER(MbMzLmos)], _I),
     "mb_mz_lmos_destroy": ([ctypes.POINTER(MbMzLmos)], _I),
     "mb_mz_density_dev": ([ctypes.POINTER(MbMzLayout), ctypes.POINTER(MbMzLmos), _I, _P, _P, _P], _I),
+    "mb_mz_fock_ws_bytes": ([ctypes.POINTER(MbMzLayout)], ctypes.c_size_t),
+    "mb_mz_fock_dev": ([ctypes.POINTER(MbMzLayout), _P, _P, _P, _P, _P, _P, _P], _I),
     "mb_mz_helecz_ws_bytes": ([], ctypes.c_size_t),
     "mb_mz_helecz_ws": ([_LL, _I, _P, _P, _P, _P, _P, _P, _P], _I),
     "mb_mz_cnvgz_ws_bytes": ([], ctypes.c_size_t),

@@ -192,6 +192,184 @@ __global__ void __launch_bounds__(256) copy_kernel(long long n, const double* __
     dst[i] = src[i];
 }
 
+// ------------------------------------------------------------- fock2z
+constexpr double MZ_EV = 27.211386245988;
+constexpr double MZ_A0 = 0.529177210903;
+__constant__ int c_pidx[16] = {1, 2, 4, 7, 2, 3, 5, 8, 4, 5, 6, 9, 7, 8, 9, 10};
+
+__device__ __forceinline__ int tri1(int i, int j) {  // 1-based packed index of (i, j)
+  const int a = i > j ? i : j, b = i < j ? i : j;
+  return (a * (a - 1)) / 2 + b;
+}
+
+// qe(a): electrons on each atom, chrge_for_MOZYME (MOZYME/chrge_for_MOZYME.F90).
+__global__ void mz_chrge(MbMzLayout L, const double* __restrict__ p, double* __restrict__ qe) {
+  for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < L.numat; a += gridDim.x * blockDim.x) {
+    long long ii = L.pair_off[L.pair_ptr[a + 1] - 1];
+    double sum = 0.0;
+    for (int j = 1; j <= L.iorbs[a]; ++j) {
+      ii += j;
+      sum = DADD(sum, p[ii - 1]);
+    }
+    qe[a] = sum;
+  }
+}
+
+// Contribution of stored partner b to element t (0-based triangle position) of
+// atom a's diagonal block, as fz2n adds it during pair (max(a,b), min(a,b)).
+__device__ double mz_pair_diag_term(int a, int b, int t, const MbMzLayout& L, const double* __restrict__ wk,
+                                    const double* __restrict__ p) {
+  const int ia = L.iorbs[a], ib = L.iorbs[b];
+  const long long db = L.pair_off[L.pair_ptr[b + 1] - 1];
+  if (ia >= 3 && ib >= 3) {
+    // jab: the higher atom gets sumb (the lower atom's density), the lower one suma
+    int i5 = 1;
+    while ((i5 * (i5 + 1)) / 2 <= t) ++i5;  // row of triangle position t (0-based t)
+    const int i6 = t - (i5 * (i5 - 1)) / 2 + 1;
+    const int i = (i5 * (i5 - 1)) / 2 + i6 - 1;  // running index of jab's output loop = t
+    double s = 0.0;
+    for (int j = 0; j < 16; ++j) {
+      const int jr = j / 4 + 1, jc = j % 4 + 1;
+      const double pb = p[db + tri1(jr, jc) - 1];
+      const double wv = (a > b) ? wk[i * 10 + c_pidx[j] - 1] : wk[(c_pidx[j] - 1) * 10 + i];
+      s = DADD(s, DMUL(pb, wv));
+    }
+    return s;
+  }
+  if (ia >= 3) {  // a heavy, b light: a's element t gets ptot(b) w(t+1)
+    return DMUL(p[db], wk[t]);
+  }
+  if (ib >= 3) {  // a light, b heavy: sumoff * 2 + sumdia over b's triangle
+    double sumoff = 0.0, sumdia = 0.0;
+    int k = 0;
+    for (int i = 1; i <= 4; ++i) {
+      for (int j = 1; j <= i - 1; ++j) {
+        ++k;
+        sumoff = DADD(sumoff, DMUL(p[db + tri1(i, j) - 1], wk[k - 1]));
+      }
+      ++k;
+      sumdia = DADD(sumdia, DMUL(p[db + tri1(i, i) - 1], wk[k - 1]));
+    }
+    return DADD(DMUL(sumoff, 2.0), sumdia);
+  }
+  return DMUL(p[db], wk[0]);  // light-light
+}
+
+// Diagonal blocks: one warp per atom.  Lanes evaluate 32 partners at a time
+// (stored pairs: their integral terms; the others: qe(b) ev a0 / r on the s
+// and p diagonal), then lane t folds element t over the 32 partners in
+// ascending order -- the order in which fz2n's pair loop reaches atom a -- and
+// the one-centre terms come last.
+__global__ void __launch_bounds__(128) mz_fock_diag(MbMzLayout L, const double* __restrict__ coord,
+                                                   const double* __restrict__ w, const double* __restrict__ p,
+                                                   const double* __restrict__ qe, const double* __restrict__ h,
+                                                   double* __restrict__ f) {
+  __shared__ double s_c[4][32][10];
+  __shared__ unsigned short s_m[4][32];
+  const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
+  const int a = blockIdx.x * 4 + wl;
+  if (a >= L.numat) return;
+  const int ia = L.iorbs[a];
+  const int ne = ia * (ia + 1) / 2;
+  const long long da = L.pair_off[L.pair_ptr[a + 1] - 1];
+  double acc = lane < ne ? h[da + lane] : 0.0;
+  const int nb0 = L.nbr_ptr[a], nb1 = L.nbr_ptr[a + 1];
+  const double evA0 = DMUL(MZ_EV, MZ_A0);
+  for (int base = 0; base < L.numat; base += 32) {
+    const int b = base + lane;
+    unsigned short mask = 0;
+    if (b < L.numat && b != a) {
+      // r^2 as fillij forms it (higher atom minus lower atom), so the stored test agrees with the layout
+      const int hi = a > b ? a : b, lo = a > b ? b : a;
+      const double dx = DSUB(coord[3 * hi], coord[3 * lo]);
+      const double dy = DSUB(coord[3 * hi + 1], coord[3 * lo + 1]);
+      const double dz = DSUB(coord[3 * hi + 2], coord[3 * lo + 2]);
+      const double r2 = DADD(DADD(DMUL(dx, dx), DMUL(dy, dy)), DMUL(dz, dz));
+      if (r2 < L.cutof2) {
+        int lo_i = nb0, hi_i = nb1 - 1, e = -1;
+        while (lo_i <= hi_i) {
+          const int mid = (lo_i + hi_i) >> 1;
+          const int v = L.nbr_atom[mid];
+          if (v == b) { e = mid; break; }
+          if (v < b) lo_i = mid + 1; else hi_i = mid - 1;
+        }
+        if (e >= 0) {
+          const double* wk = w + L.pair_woff[L.nbr_entry[e]];
+          for (int t = 0; t < ne; ++t) s_c[wl][lane][t] = mz_pair_diag_term(a, b, t, L, wk, p);
+          mask = (unsigned short)((1u << ne) - 1u);
+        }
+      } else {
+        // point-charge monopole (feathering weight zero beyond 7 A): w1 = ev a0 / r
+        const double point = evA0 / sqrt(r2);
+        const double c = DMUL(qe[b], point);
+        const int dg[4] = {0, 2, 5, 9};
+        for (int q = 0; q < ia; ++q) {
+          s_c[wl][lane][dg[q]] = c;
+          mask |= (unsigned short)(1u << dg[q]);
+        }
+      }
+    }
+    s_m[wl][lane] = mask;
+    __syncwarp();
+    if (lane < ne) {
+      const int nt = min(32, L.numat - base);
+      for (int t = 0; t < nt; ++t)
+        if (s_m[wl][t] & (1u << lane)) acc = DADD(acc, s_c[wl][t][lane]);
+    }
+    __syncwarp();
+  }
+  // fock1_for_MOZYME
+  if (lane < ne) {
+    const int ilim = ne;
+    const double* wo = w + L.pair_woff[L.pair_ptr[a + 1] - 1];
+    int i = 1;
+    while ((i * (i + 1)) / 2 <= lane) ++i;
+    const int j = lane - (i * (i - 1)) / 2 + 1;
+    const int ijw = (i * (i - 1)) / 2 + j;
+    double sum = 0.0;
+    for (int k = 1; k <= ia; ++k)
+      for (int l = 1; l <= ia; ++l) {
+        const int ijp = tri1(k, l);
+        const int ikw = tri1(k, j), jlw = tri1(l, i);
+        const double pv = p[da + ijp - 1];
+        sum = DSUB(DADD(sum, DMUL(pv, wo[(ijw - 1) + ilim * (ijp - 1)])), DMUL(DMUL(0.5, pv), wo[(ikw - 1) + ilim * (jlw - 1)]));
+      }
+    f[da + lane] = DADD(acc, sum);
+  }
+}
+
+// Off-diagonal blocks of stored pairs: F = H - exchange, 16 lanes per pair.
+__global__ void __launch_bounds__(256) mz_fock_pairs(MbMzLayout L, const double* __restrict__ w,
+                                                    const double* __restrict__ p, const double* __restrict__ h,
+                                                    double* __restrict__ f) {
+  const long long g = (blockIdx.x * (long long)blockDim.x + threadIdx.x);
+  const long long e = g >> 4;
+  const int t = (int)(g & 15);
+  if (e >= L.npairs) return;
+  const int ii = L.pair_i[e], jj = L.pair_j[e];
+  if (ii == jj) return;
+  const int ia = L.iorbs[ii], ib = L.iorbs[jj];
+  const long long off = L.pair_off[e];
+  const double* wk = w + L.pair_woff[e];
+  if (ia >= 3 && ib >= 3) {
+    const int mu = t / 4 + 1, nu = t % 4 + 1;
+    double s = 0.0;
+    for (int i2 = 0; i2 < 16; ++i2) {
+      const int lam = i2 / 4 + 1, sig = i2 % 4 + 1;
+      s = DADD(s, DMUL(p[off + i2], wk[(tri1(mu, lam) - 1) * 10 + tri1(nu, sig) - 1]));
+    }
+    f[off + t] = DSUB(h[off + t], DMUL(s, 0.5));
+  } else if (ia >= 3 || ib >= 3) {
+    if (t >= 4) return;
+    double s = 0.0;
+    for (int j = 1; j <= 4; ++j) s = DADD(s, DMUL(p[off + j - 1], wk[c_pidx[t * 4 + j - 1] - 1]));
+    f[off + t] = DSUB(h[off + t], DMUL(s, 0.5));
+  } else {
+    if (t != 0) return;
+    f[off] = DSUB(h[off], DMUL(DMUL(p[off], wk[0]), 0.5));
+  }
+}
+
 int grid_for(long long n) {
   long long b = (n + 255) / 256;
   return (int)(b > 148 * 8 ? 148 * 8 : (b < 1 ? 1 : b));
@@ -245,15 +423,49 @@ extern "C" int mb_mz_layout_create(int numat, const int* iorbs, const double* co
     mpack += (long long)io * (io + 1) / 2;
   }
   ptr[numat] = (int)pi.size();
+  // integral blocks in entry order: the dense W's layout without the far pairs
+  std::vector<long long> woff(pi.size());
+  long long nw = 0;
+  for (size_t e = 0; e < pi.size(); ++e) {
+    woff[e] = nw;
+    const int a = iorbs[pi[e]], b = iorbs[pj[e]];
+    if (pi[e] == pj[e]) {
+      const long long il = (long long)a * (a + 1) / 2;
+      nw += il * il;
+    } else {
+      nw += (a >= 3 && b >= 3) ? 100 : ((a >= 3 || b >= 3) ? 10 : 1);
+    }
+  }
+  // stored partners of every atom in both directions, ascending
+  std::vector<int> ncount(numat + 1, 0);
+  for (size_t e = 0; e < pi.size(); ++e)
+    if (pi[e] != pj[e]) { ncount[pi[e] + 1]++; ncount[pj[e] + 1]++; }
+  for (int a = 0; a < numat; ++a) ncount[a + 1] += ncount[a];
+  std::vector<int> nat_(ncount[numat]), nfill(ncount.begin(), ncount.end() - 1);
+  std::vector<long long> nent(ncount[numat]);
+  for (int a = 0; a < numat; ++a) {  // partners b < a from a's own entries, then b > a from later atoms
+    for (int e = ptr[a]; e < ptr[a + 1]; ++e)
+      if (pj[e] != a) { nat_[nfill[a]] = pj[e]; nent[nfill[a]] = e; nfill[a]++; }
+  }
+  for (int b = 0; b < numat; ++b)
+    for (int e = ptr[b]; e < ptr[b + 1]; ++e)
+      if (pj[e] != b) { const int a = pj[e]; nat_[nfill[a]] = b; nent[nfill[a]] = e; nfill[a]++; }
   std::vector<int> io(iorbs, iorbs + numat);
   out->numat = numat;
   out->mpack = mpack;
   out->npairs = (long long)pi.size();
+  out->nw = nw;
+  out->cutof1 = cutof1;
+  out->cutof2 = cutof2;
   int rc = upload(io, &out->iorbs);
   if (rc == MB_OK) rc = upload(ptr, &out->pair_ptr);
   if (rc == MB_OK) rc = upload(pi, &out->pair_i);
   if (rc == MB_OK) rc = upload(pj, &out->pair_j);
   if (rc == MB_OK) rc = upload(po, &out->pair_off);
+  if (rc == MB_OK) rc = upload(woff, &out->pair_woff);
+  if (rc == MB_OK) rc = upload(ncount, &out->nbr_ptr);
+  if (rc == MB_OK) rc = upload(nat_, &out->nbr_atom);
+  if (rc == MB_OK) rc = upload(nent, &out->nbr_entry);
   if (rc != MB_OK) mb_mz_layout_destroy(out);
   return rc;
 }
@@ -265,6 +477,10 @@ extern "C" int mb_mz_layout_destroy(MbMzLayout* L) {
   cudaFree((void*)L->pair_i);
   cudaFree((void*)L->pair_j);
   cudaFree((void*)L->pair_off);
+  cudaFree((void*)L->pair_woff);
+  cudaFree((void*)L->nbr_ptr);
+  cudaFree((void*)L->nbr_atom);
+  cudaFree((void*)L->nbr_entry);
   memset(L, 0, sizeof(*L));
   return MB_OK;
 }
@@ -380,5 +596,25 @@ extern "C" int mb_mz_cnvgz_ws(int norbs, long long mpack, double* pnew, double* 
   copy_kernel<<<grid_for(mpack), 256, 0, stream>>>(mpack, pnew, p);
   MB_LAUNCH_CHECK();
   MB_CUDA(cudaMemcpyAsync(pmax_out, bits, sizeof(double), cudaMemcpyDeviceToDevice, stream));
+  return MB_OK;
+}
+
+extern "C" size_t mb_mz_fock_ws_bytes(const MbMzLayout* L) {
+  return L ? sizeof(double) * (size_t)L->numat : 0;
+}
+
+extern "C" int mb_mz_fock_dev(const MbMzLayout* L, const double* coord, const double* w, const double* ptot,
+                              const double* h, double* f, void* ws, cudaStream_t stream) {
+  if (!L || !coord || !w || !ptot || !h || !f || !ws) return mb_set_error(MB_ERR_ARG, "mb_mz_fock_dev: bad args");
+  if (!(L->cutof2 >= 49.0))
+    return mb_set_error(MB_ERR_UNSUPPORTED, "mb_mz_fock_dev: needs cutof2 >= 49 (7 A); shorter cutoffs feather");
+  double* qe = (double*)ws;
+  mz_chrge<<<grid_for(L->numat), 256, 0, stream>>>(*L, ptot, qe);
+  MB_LAUNCH_CHECK();
+  mz_fock_diag<<<(L->numat + 3) / 4, 128, 0, stream>>>(*L, coord, w, ptot, qe, h, f);
+  MB_LAUNCH_CHECK();
+  const long long thr = L->npairs * 16;
+  mz_fock_pairs<<<(unsigned)((thr + 255) / 256), 256, 0, stream>>>(*L, w, ptot, h, f);
+  MB_LAUNCH_CHECK();
   return MB_OK;
 }

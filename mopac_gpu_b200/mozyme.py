@@ -104,3 +104,16 @@ def cnvgz(layout: Layout, pnew, p, p1, p2, p3, niter: int, use3: bool = True) ->
     check(lib().mb_mz_cnvgz_ws(layout.norbs, layout.mpack, _ptr(pnew), _ptr(p), _ptr(p1), _ptr(p2), _ptr(p3),
                                int(niter), _ptr(layout.idiag), int(use3), _ptr(pm), _ptr(ws), _stream()))
     return float(pm.item())
+
+
+def fock(layout: Layout, coord, w, ptot, h, out=None):
+    """buildf(f, partf, 0): F = H + G(P) over the pair-block storage.  coord
+    (numat x 3, Angstrom), w (the stored pairs' integrals, layout.nw), ptot
+    and h: CUDA float64 tensors."""
+    f = out if out is not None else torch.empty(layout.mpack, dtype=torch.float64, device="cuda")
+    ws = torch.empty(int(lib().mb_mz_fock_ws_bytes(ctypes.byref(layout.s))) // 8 + 1, dtype=torch.float64,
+                     device="cuda")
+    c = coord.contiguous()
+    check(lib().mb_mz_fock_dev(ctypes.byref(layout.s), _ptr(c), _ptr(w), _ptr(ptot), _ptr(h), _ptr(f), _ptr(ws),
+                               _stream()))
+    return f

@@ -1474,3 +1474,265 @@ void orc_mz_cnvgz(int norbs, long long mpack, double *pnew, double *p, double *p
     for (long long i = 0; i < mpack; ++i) p[i] = pnew[i];
     *pmax_out = pmax;
 }
+
+/* Offsets of the dense W blocks (hcore's sequential layout): pair (i, j),
+ * j < i, at woff[i*numat + j], the one-centre block of i at woff[i*numat + i]. */
+static void dense_w_offsets(int numat, const int *iorbs, long long *woff) {
+    long long kk = 0;
+    for (int i = 0; i < numat; ++i) {
+        for (int j = 0; j < i; ++j) {
+            woff[(long long)i * numat + j] = kk;
+            const int a = iorbs[i] >= 3, b = iorbs[j] >= 3;
+            kk += (a && b) ? 100 : ((a || b) ? 10 : 1);
+        }
+        woff[(long long)i * numat + i] = kk;
+        const int il = iorbs[i] * (iorbs[i] + 1) / 2;
+        kk += (long long)il * il;
+    }
+}
+
+/* fz2n (MOZYME/fock2z.F90:669-1293), mode 0 (the whole F), direct and
+ * semi-direct (the defaults), molecular, s/p atoms, no COSMO.  f holds H on
+ * entry and F on exit, in the pair-block storage of nijbo.  The integrals of
+ * a stored pair are the pair's block of the dense W (the reference computes
+ * them on the fly with the same rotate), the one-centre blocks are the
+ * atoms' blocks of the dense W.  Pairs outside cutof2 get the point-charge
+ * monopole, and those inside cutof1 also the dipole terms; all one-centre
+ * terms come after the pair loop, as in the direct path. */
+void orc_mz_fock(int numat, const int *nat, const double *coord, const int *iorbs, const long long *nijbo,
+                 const double *w, const double *ptot, double *f, double *qe_out) {
+    static const int pidx[16] = {1, 2, 4, 7, 2, 3, 5, 8, 4, 5, 6, 9, 7, 8, 9, 10};
+    long long *woff = (long long *)malloc(sizeof(long long) * (size_t)numat * numat);
+    double *qe = (double *)malloc(sizeof(double) * numat);
+    double *pt2 = (double *)malloc(sizeof(double) * 16 * (size_t)numat);
+    dense_w_offsets(numat, iorbs, woff);
+#define NB_(i, j) nijbo[(long long)(i) * numat + (j)]
+    for (int i = 0; i < numat; ++i) {  /* chrge_for_MOZYME */
+        long long ii = NB_(i, i);
+        double sum = 0.0;
+        for (int j = 1; j <= iorbs[i]; ++j) {
+            ii += j;
+            sum = sum + ptot[ii - 1];
+        }
+        qe[i] = sum;
+        const long long b = NB_(i, i);
+        int m = 0;
+        for (int j = 1; j <= iorbs[i]; ++j)
+            for (int k = 1; k <= iorbs[i]; ++k) {
+                const int jk = j < k ? j : k, kj = j + k - jk;
+                pt2[16 * i + m] = ptot[b + (kj * (kj - 1)) / 2 + jk - 1];
+                ++m;
+            }
+    }
+    double w2 = 0.0, w3 = 0.0, w4 = 0.0, w5 = 0.0, w6 = 0.0, w7 = 0.0;
+    for (int ii = 0; ii < numat; ++ii) {
+        const int iab = iorbs[ii];
+        if (iab == 0) continue;
+        for (int jj = 0; jj < ii; ++jj) {
+            const int jba = iorbs[jj];
+            const long long off = NB_(ii, jj);
+            if (off >= 0) {
+                const double *wk = w + woff[(long long)ii * numat + jj];
+                if (iab >= 3 && jba >= 3) {
+                    /* jab_for_MOZYME(1, 1, ptot2(ii), ptot2(jj), w, F(ii ii), F(jj jj)) */
+                    double suma[10], sumb[10];
+                    for (int i = 0; i < 10; ++i) { suma[i] = 0.0; sumb[i] = 0.0; }
+                    for (int j = 0; j < 16; ++j)
+                        for (int i = 0; i < 10; ++i) {
+                            suma[i] = suma[i] + pt2[16 * ii + j] * wk[(pidx[j] - 1) * 10 + i];
+                            sumb[i] = sumb[i] + pt2[16 * jj + j] * wk[i * 10 + pidx[j] - 1];
+                        }
+                    const long long fi = NB_(ii, ii), fj = NB_(jj, jj);
+                    int i = 0;
+                    for (int i5 = 1; i5 <= 4; ++i5) {
+                        long long ioff = (i5 * (i5 - 1)) / 2, joff = ioff;
+                        for (int i6 = 1; i6 <= i5; ++i6) {
+                            ++ioff; ++joff;
+                            f[fi + ioff - 1] = f[fi + ioff - 1] + sumb[i];
+                            f[fj + joff - 1] = f[fj + joff - 1] + suma[i];
+                            ++i;
+                        }
+                    }
+                    /* kab_for_MOZYME(0, 0, ptot(l), w, f(l)) */
+                    double sum[16];
+                    for (int j = 0; j < 16; ++j) {
+                        const int mu = j / 4 + 1, nu = j % 4 + 1;
+                        sum[j] = 0.0;
+                        for (int i2 = 0; i2 < 16; ++i2) {
+                            const int lam = i2 / 4 + 1, sig = i2 % 4 + 1;
+                            sum[j] = sum[j] + ptot[off + i2] * wk[(indx_(mu, lam) - 1) * 10 + indx_(nu, sig) - 1];
+                        }
+                    }
+                    for (int i2 = 0; i2 < 16; ++i2) f[off + i2] = f[off + i2] - sum[i2] * 0.5;
+                } else if (iab >= 3 && jba == 1) {
+                    double sumdia = 0.0, sumoff = 0.0;
+                    const long long lj = NB_(jj, jj) + 1;
+                    long long li = NB_(ii, ii);
+                    int k = 0;
+                    for (int i = 1; i <= 4; ++i) {
+                        for (int j = 1; j <= i - 1; ++j) {
+                            ++li; ++k;
+                            f[li - 1] = f[li - 1] + ptot[lj - 1] * wk[k - 1];
+                            sumoff = sumoff + ptot[li - 1] * wk[k - 1];
+                        }
+                        ++li; ++k;
+                        f[li - 1] = f[li - 1] + ptot[lj - 1] * wk[k - 1];
+                        sumdia = sumdia + ptot[li - 1] * wk[k - 1];
+                    }
+                    f[lj - 1] = f[lj - 1] + sumoff * 2.0 + sumdia;
+                    k = 0;
+                    for (int i = 1; i <= 4; ++i) {
+                        double s = 0.0;
+                        for (int j = 1; j <= 4; ++j) {
+                            ++k;
+                            s = s + ptot[off + j - 1] * wk[pidx[k - 1] - 1];
+                        }
+                        f[off + i - 1] = f[off + i - 1] - s * 0.5;
+                    }
+                } else if (jba >= 3 && iab == 1) {
+                    double sumdia = 0.0, sumoff = 0.0;
+                    long long lj = NB_(jj, jj);
+                    const long long li = NB_(ii, ii) + 1;
+                    int k = 0;
+                    for (int i = 1; i <= 4; ++i) {
+                        for (int j = 1; j <= i - 1; ++j) {
+                            ++k; ++lj;
+                            f[lj - 1] = f[lj - 1] + ptot[li - 1] * wk[k - 1];
+                            sumoff = sumoff + ptot[lj - 1] * wk[k - 1];
+                        }
+                        ++lj; ++k;
+                        f[lj - 1] = f[lj - 1] + ptot[li - 1] * wk[k - 1];
+                        sumdia = sumdia + ptot[lj - 1] * wk[k - 1];
+                    }
+                    f[li - 1] = f[li - 1] + sumoff * 2.0 + sumdia;
+                    k = 0;
+                    for (int i = 1; i <= 4; ++i) {
+                        double s = 0.0;
+                        for (int j = 1; j <= 4; ++j) {
+                            ++k;
+                            s = s + ptot[off + j - 1] * wk[pidx[k - 1] - 1];
+                        }
+                        f[off + i - 1] = f[off + i - 1] - s * 0.5;
+                    }
+                } else if (iab == 1 && jba == 1) {
+                    const long long lii = NB_(ii, ii) + 1, lij = off + 1, ljj = NB_(jj, jj) + 1;
+                    f[lii - 1] = f[lii - 1] + ptot[ljj - 1] * wk[0];
+                    f[ljj - 1] = f[ljj - 1] + ptot[lii - 1] * wk[0];
+                    f[lij - 1] = f[lij - 1] - ptot[lij - 1] * wk[0] * 0.5;
+                }
+            } else {
+                long long i1 = NB_(ii, ii), j1 = NB_(jj, jj);
+                double dx = coord[3 * ii] - coord[3 * jj];
+                double dy = coord[3 * ii + 1] - coord[3 * jj + 1];
+                double dz = coord[3 * ii + 2] - coord[3 * jj + 2];
+                const double r2 = dx * dx + dy * dy + dz * dz;
+                const int ni = nat[ii], nj = nat[jj];
+                const double aee = 0.5 / E[ni].am + 0.5 / E[nj].am;
+                double point, cst;
+                const double rij = sqrt(r2);
+                to_point(rij, &point, &cst);
+                double w1 = EV / sqrt(r2 / (A0 * A0) + aee * aee);
+                w1 = w1 * cst + (1.0 - cst) * point;
+                for (int i = 1; i <= iab; ++i) {
+                    i1 += i;
+                    f[i1 - 1] = f[i1 - 1] + qe[jj] * w1;
+                }
+                for (int j = 1; j <= jba; ++j) {
+                    j1 += j;
+                    f[j1 - 1] = f[j1 - 1] + qe[ii] * w1;
+                }
+                i1 = NB_(ii, ii);
+                j1 = NB_(jj, jj);
+                if (off == -2) {
+                    const double r = sqrt(r2);
+                    dx = dx / r; dy = dy / r; dz = dz / r;
+                    if (fabs(dz) > 0.99999999) dz = copysign(1.0, dz);
+                    if (iab > 1) {
+                        const double da = E[ni].dd, ade = 0.5 / E[ni].ad + 0.5 / E[nj].am;
+                        const double rp = sqrt((r / A0 + da) * (r / A0 + da) + ade * ade);
+                        const double rm = sqrt((r / A0 - da) * (r / A0 - da) + ade * ade);
+                        double ri2 = EV * (0.5 / rp - 0.5 / rm);
+                        to_point(r, &point, &cst);
+                        ri2 = ri2 * cst;
+                        w5 = ri2 * dx; w6 = ri2 * dy; w7 = ri2 * dz;
+                    }
+                    if (jba > 1) {
+                        const double da = E[nj].dd, ade = 0.5 / E[ni].am + 0.5 / E[nj].ad;
+                        const double rp = sqrt((r / A0 + da) * (r / A0 + da) + ade * ade);
+                        const double rm = sqrt((r / A0 - da) * (r / A0 - da) + ade * ade);
+                        double ri5 = -EV * (0.5 / rp - 0.5 / rm);
+                        to_point(r, &point, &cst);
+                        ri5 = ri5 * cst;
+                        w2 = ri5 * dx; w3 = ri5 * dy; w4 = ri5 * dz;
+                    }
+#define FA(x) f[(x) - 1]
+#define PA(x) ptot[(x) - 1]
+                    if (iab > 1 && jba > 1) {
+                        FA(j1 + 2) = FA(j1 + 2) + qe[ii] * w2;
+                        FA(j1 + 4) = FA(j1 + 4) + qe[ii] * w3;
+                        FA(j1 + 7) = FA(j1 + 7) + qe[ii] * w4;
+                        FA(i1 + 2) = FA(i1 + 2) + qe[jj] * w5;
+                        FA(i1 + 4) = FA(i1 + 4) + qe[jj] * w6;
+                        FA(i1 + 7) = FA(i1 + 7) + qe[jj] * w7;
+                        const int dg[4] = {1, 3, 6, 10};
+                        for (int q = 0; q < 4; ++q) FA(j1 + dg[q]) = FA(j1 + dg[q]) + PA(i1 + 2) * w5 * 2;
+                        for (int q = 0; q < 4; ++q) FA(j1 + dg[q]) = FA(j1 + dg[q]) + PA(i1 + 4) * w6 * 2;
+                        for (int q = 0; q < 4; ++q) FA(j1 + dg[q]) = FA(j1 + dg[q]) + PA(i1 + 7) * w7 * 2;
+                        for (int q = 0; q < 4; ++q) FA(i1 + dg[q]) = FA(i1 + dg[q]) + PA(j1 + 2) * w2 * 2;
+                        for (int q = 0; q < 4; ++q) FA(i1 + dg[q]) = FA(i1 + dg[q]) + PA(j1 + 4) * w3 * 2;
+                        for (int q = 0; q < 4; ++q) FA(i1 + dg[q]) = FA(i1 + dg[q]) + PA(j1 + 7) * w4 * 2;
+                    } else if (iab > 1) {
+                        FA(i1 + 2) = FA(i1 + 2) + qe[jj] * w5;
+                        FA(i1 + 4) = FA(i1 + 4) + qe[jj] * w6;
+                        FA(i1 + 7) = FA(i1 + 7) + qe[jj] * w7;
+                        FA(j1 + 1) = FA(j1 + 1) + PA(i1 + 2) * w5 * 2;
+                        FA(j1 + 1) = FA(j1 + 1) + PA(i1 + 4) * w6 * 2;
+                        FA(j1 + 1) = FA(j1 + 1) + PA(i1 + 7) * w7 * 2;
+                    } else if (jba > 1) {
+                        FA(j1 + 2) = FA(j1 + 2) + qe[ii] * w2;
+                        FA(j1 + 4) = FA(j1 + 4) + qe[ii] * w3;
+                        FA(j1 + 7) = FA(j1 + 7) + qe[ii] * w4;
+                        FA(i1 + 1) = FA(i1 + 1) + PA(j1 + 2) * w2 * 2;
+                        FA(i1 + 1) = FA(i1 + 1) + PA(j1 + 4) * w3 * 2;
+                        FA(i1 + 1) = FA(i1 + 1) + PA(j1 + 7) * w4 * 2;
+                    }
+#undef FA
+#undef PA
+                }
+            }
+        }
+    }
+    /* fock1_for_MOZYME for every atom, after the pairs (direct path) */
+    for (int ii = 0; ii < numat; ++ii) {
+        const int iab = iorbs[ii];
+        if (iab == 0) continue;
+        const int ilim = iab * (iab + 1) / 2;
+        const double *wo = w + woff[(long long)ii * numat + ii];
+        const long long base = NB_(ii, ii);
+#define WF(a, b) wo[((a) - 1) + ilim * ((b) - 1)]
+        for (int i = 1; i <= iab; ++i)
+            for (int j = 1; j <= i; ++j) {
+                const int ij = (i * (i - 1)) / 2 + j, ijw = ij;
+                double sum = 0.0;
+                for (int k = 1; k <= iab; ++k)
+                    for (int l = 1; l <= iab; ++l) {
+                        const int ip = k > l ? k : l, jp = k < l ? k : l;
+                        const int ijp = (ip * (ip - 1)) / 2 + jp;
+                        const int klw = ijp;
+                        int im = k > j ? k : j, jm = k < j ? k : j;
+                        const int ikw = (im * (im - 1)) / 2 + jm;
+                        im = l > i ? l : i; jm = l < i ? l : i;
+                        const int jlw = (im * (im - 1)) / 2 + jm;
+                        sum = sum + ptot[base + ijp - 1] * WF(ijw, klw) - 0.5 * ptot[base + ijp - 1] * WF(ikw, jlw);
+                    }
+                f[base + ij - 1] = f[base + ij - 1] + sum;
+            }
+#undef WF
+    }
+#undef NB_
+    if (qe_out)
+        for (int i = 0; i < numat; ++i) qe_out[i] = qe[i];
+    free(woff);
+    free(qe);
+    free(pt2);
+}

@@ -105,3 +105,54 @@ def dense_to_blocks(a: np.ndarray, iorbs, nijbo, mpack: int) -> np.ndarray:
                 vals = bi.ravel()
             out[off:off + vals.size] = vals
     return out
+
+
+def dense_w_offsets(iorbs) -> np.ndarray:
+    """Offsets of the dense W blocks (hcore's order): pair (i, j), j < i, and
+    the one-centre block (i, i)."""
+    n = len(iorbs)
+    off = np.zeros((n, n), np.int64)
+    kk = 0
+    for i in range(n):
+        for j in range(i):
+            off[i, j] = kk
+            a, b = iorbs[i] >= 3, iorbs[j] >= 3
+            kk += 100 if (a and b) else (10 if (a or b) else 1)
+        off[i, i] = kk
+        il = iorbs[i] * (iorbs[i] + 1) // 2
+        kk += il * il
+    return off
+
+
+def w_stored(iorbs, nijbo, w_dense) -> np.ndarray:
+    """The dense W with the blocks of pairs outside cutof2 left out: the
+    integrals fock2z uses, in the layout's entry order."""
+    off = dense_w_offsets(iorbs)
+    out = []
+    n = len(iorbs)
+    for i in range(n):
+        for j in range(i):
+            if nijbo[i, j] >= 0:
+                a, b = iorbs[i] >= 3, iorbs[j] >= 3
+                sz = 100 if (a and b) else (10 if (a or b) else 1)
+                out.append(w_dense[off[i, j]:off[i, j] + sz])
+        il = iorbs[i] * (iorbs[i] + 1) // 2
+        out.append(w_dense[off[i, i]:off[i, i] + il * il])
+    return np.ascontiguousarray(np.concatenate(out))
+
+
+def fock(nat, coord, iorbs, nijbo, w_dense, ptot, h):
+    """fz2n mode 0: F from H (both in the pair-block storage)."""
+    L = _lib()
+    if not hasattr(L, "_mz_fock_bound"):
+        i32p = np.ctypeslib.ndpointer(np.int32, flags="C")
+        i64p = np.ctypeslib.ndpointer(np.int64, flags="C")
+        f64p = np.ctypeslib.ndpointer(np.float64, flags="C")
+        L.orc_mz_fock.argtypes = [ctypes.c_int, i32p, f64p, i32p, i64p, f64p, f64p, f64p, f64p]
+        L._mz_fock_bound = True
+    f = np.ascontiguousarray(h, np.float64).copy()
+    qe = np.zeros(len(iorbs))
+    L.orc_mz_fock(len(iorbs), np.ascontiguousarray(nat, np.int32), np.ascontiguousarray(coord, np.float64).ravel(),
+                  np.ascontiguousarray(iorbs, np.int32), np.ascontiguousarray(nijbo.ravel()),
+                  np.ascontiguousarray(w_dense, np.float64), np.ascontiguousarray(ptot, np.float64), f, qe)
+    return f

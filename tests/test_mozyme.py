@@ -49,6 +49,25 @@ def test_oracle_mozyme_density_and_energy_equal_dense(name):
     assert e_sparse == pytest.approx(e_dense, rel=1e-12)
 
 
+@pytest.mark.parametrize("name", ["water16", "propane"])
+def test_oracle_mozyme_fock_equals_dense_when_all_pairs_stored(name):
+    """With every pair stored, fz2n is fock2 + fock1 in another summation
+    order: the sparse F equals the pinned dense F to rounding."""
+    nat, xyz = small_systems()[name]
+    s = oracle_system(nat, xyz)
+    r = so.iter_scf(s)
+    iorbs = (s.nlast - s.nfirst + 1).astype(np.int32)
+    mpack, nijbo = mo.layout(iorbs, s.coord, 1.0e6 + 10, 1.0e6)
+    pd = so.unpack(r.p, s.norbs)
+    hb = mo.dense_to_blocks(so.unpack(s.h, s.norbs), iorbs, nijbo, mpack)
+    pb = mo.dense_to_blocks(pd, iorbs, nijbo, mpack)
+    fz = mo.fock(s.nat, s.coord, iorbs, nijbo, s.w, pb, hb)
+    fd = s.h.copy()
+    so.fock2(s, fd, r.p, r.p * 0.5)
+    ref = mo.dense_to_blocks(so.unpack(fd, s.norbs), iorbs, nijbo, mpack)
+    np.testing.assert_allclose(fz, ref, rtol=0, atol=1e-11 * np.abs(ref).max())
+
+
 def test_oracle_mozyme_density_modes():
     nat, xyz = small_systems()["water16"]
     iorbs, lmos = workloads.mozyme_lmos(nat, xyz, radius=3.5)
@@ -122,6 +141,45 @@ def test_gpu_mozyme_density_bit_identical(nwater, mode):
     p = mozyme.density(L, Q, mode, torch.from_numpy(part).cuda() if part is not None else None)
     np.testing.assert_array_equal(p.cpu().numpy(), ref)
     Q.close()
+    L.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("nwater,cut", [(16, 9.0), (64, 9.0), (64, 7.5), (128, 9.0)])
+def test_gpu_mozyme_fock_bit_identical(nwater, cut):
+    torch = _need_gpu()
+    from mopac_gpu_b200 import mozyme
+    nat, xyz, _ = workloads.water_box(nwater) if nwater != 16 else (*small_systems()["water16"], None)
+    s = oracle_system(nat, xyz)
+    iorbs = (s.nlast - s.nfirst + 1).astype(np.int32)
+    c1, c2 = cut ** 2 + 1e-4, cut ** 2
+    mp, nb = mo.layout(iorbs, s.coord, c1, c2)
+    rng = np.random.default_rng(nwater)
+    x = rng.normal(size=(s.norbs, s.norbs)) * 0.1
+    pd = x + x.T + np.diag(rng.uniform(0.2, 1.8, s.norbs))
+    pb = mo.dense_to_blocks(pd, iorbs, nb, mp)
+    hb = mo.dense_to_blocks(so.unpack(s.h, s.norbs), iorbs, nb, mp)
+    ref = mo.fock(s.nat, s.coord, iorbs, nb, s.w, pb, hb)
+    L = mozyme.Layout(iorbs, s.coord, c1, c2)
+    wz = mo.w_stored(iorbs, nb, s.w)
+    assert wz.size == L.s.nw
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    f = mozyme.fock(L, dev(s.coord), dev(wz), dev(pb), dev(hb)).cpu().numpy()
+    np.testing.assert_array_equal(f, ref)
+    L.close()
+
+
+@pytest.mark.gpu
+def test_gpu_mozyme_fock_rejects_short_cutoff():
+    torch = _need_gpu()
+    from mopac_gpu_b200 import mozyme
+    from mopac_gpu_b200._lib import LibraryError
+    nat, xyz = small_systems()["water16"]
+    iorbs = np.where(np.asarray(nat) == 1, 1, 4).astype(np.int32)
+    L = mozyme.Layout(iorbs, xyz, 6.0 ** 2 + 1e-4, 6.0 ** 2)
+    z = torch.zeros(max(L.mpack, int(L.s.nw), 3 * len(nat)), dtype=torch.float64, device="cuda")
+    with pytest.raises(LibraryError):
+        mozyme.fock(L, z[:3 * len(nat)], z, z[:L.mpack], z[:L.mpack])
     L.close()
 
 
