@@ -217,8 +217,12 @@ __global__ void mz_chrge(MbMzLayout L, const double* __restrict__ p, double* __r
 
 // Contribution of stored partner b to element t (0-based triangle position) of
 // atom a's diagonal block, as fz2n adds it during pair (max(a,b), min(a,b)).
+// A light atom with a heavy partner receives two additions in a row,
+// f = (f + sumoff * 2) + sumdia, as Fortran evaluates the statement; the
+// second one comes back in *second (and true).
 __device__ double mz_pair_diag_term(int a, int b, int t, const MbMzLayout& L, const double* __restrict__ wk,
-                                    const double* __restrict__ p) {
+                                    const double* __restrict__ p, double* second, bool* has_second) {
+  *has_second = false;
   const int ia = L.iorbs[a], ib = L.iorbs[b];
   const long long db = L.pair_off[L.pair_ptr[b + 1] - 1];
   if (ia >= 3 && ib >= 3) {
@@ -250,7 +254,9 @@ __device__ double mz_pair_diag_term(int a, int b, int t, const MbMzLayout& L, co
       ++k;
       sumdia = DADD(sumdia, DMUL(p[db + tri1(i, i) - 1], wk[k - 1]));
     }
-    return DADD(DMUL(sumoff, 2.0), sumdia);
+    *second = sumdia;
+    *has_second = true;
+    return DMUL(sumoff, 2.0);
   }
   return DMUL(p[db], wk[0]);  // light-light
 }
@@ -265,7 +271,8 @@ __global__ void __launch_bounds__(128) mz_fock_diag(MbMzLayout L, const double* 
                                                    const double* __restrict__ qe, const double* __restrict__ h,
                                                    double* __restrict__ f) {
   __shared__ double s_c[4][32][10];
-  __shared__ unsigned short s_m[4][32];
+  __shared__ double s_x[4][32];          // second addition (light atom, heavy partner)
+  __shared__ unsigned short s_m[4][32];  // bit t: element t gets s_c; bit 15: then s_x on element 0
   const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
   const int a = blockIdx.x * 4 + wl;
   if (a >= L.numat) return;
@@ -295,8 +302,14 @@ __global__ void __launch_bounds__(128) mz_fock_diag(MbMzLayout L, const double* 
         }
         if (e >= 0) {
           const double* wk = w + L.pair_woff[L.nbr_entry[e]];
-          for (int t = 0; t < ne; ++t) s_c[wl][lane][t] = mz_pair_diag_term(a, b, t, L, wk, p);
+          double second = 0.0;
+          bool two = false;
+          for (int t = 0; t < ne; ++t) s_c[wl][lane][t] = mz_pair_diag_term(a, b, t, L, wk, p, &second, &two);
           mask = (unsigned short)((1u << ne) - 1u);
+          if (two) {
+            s_x[wl][lane] = second;
+            mask |= (unsigned short)0x8000u;
+          }
         }
       } else {
         // point-charge monopole (feathering weight zero beyond 7 A): w1 = ev a0 / r
@@ -313,8 +326,11 @@ __global__ void __launch_bounds__(128) mz_fock_diag(MbMzLayout L, const double* 
     __syncwarp();
     if (lane < ne) {
       const int nt = min(32, L.numat - base);
-      for (int t = 0; t < nt; ++t)
-        if (s_m[wl][t] & (1u << lane)) acc = DADD(acc, s_c[wl][t][lane]);
+      for (int t = 0; t < nt; ++t) {
+        const unsigned mk = s_m[wl][t];
+        if (mk & (1u << lane)) acc = DADD(acc, s_c[wl][t][lane]);
+        if ((mk & 0x8000u) && lane == 0) acc = DADD(acc, s_x[wl][t]);
+      }
     }
     __syncwarp();
   }
