@@ -231,6 +231,8 @@ typedef struct MbMzLayout {
   const int* nbr_atom;
   const long long* nbr_entry;
   double cutof1, cutof2;
+  const int* first;   /* 0-based first orbital of each atom */
+  int norbs;
 } MbMzLayout;
 /* Occupied LMOs on the device: cocc as in MOZYME_C plus, per atom, the LMOs
  * containing it (ascending) and the offset of its coefficients in cocc. */
@@ -240,6 +242,13 @@ typedef struct MbMzLmos {
   const int* atom_lmo;
   const int* atom_coff;
   const double* cocc;
+  /* the reference's own arrays: ncf (atoms per LMO), nncf (0-based start in
+   * icocc), icocc (1-based atom numbers), ncocc (0-based start in cocc) */
+  const int* ncf;
+  const int* nncf;
+  const int* icocc;
+  const int* ncocc;
+  long long nentries;  /* length of icocc */
 } MbMzLmos;
 /* Builds the layout (host coordinates in Angstrom, cutoffs squared, as
  * cutof1/cutof2 in fillij); nijbo (optional, host numat x numat) receives the
@@ -273,6 +282,25 @@ int mb_mz_density_dev(const MbMzLayout* layout, const MbMzLmos* lmos, int mode, 
 size_t mb_mz_fock_ws_bytes(const MbMzLayout* layout);
 int mb_mz_fock_dev(const MbMzLayout* layout, const double* coord, const double* w, const double* ptot,
                    const double* h, double* f, void* ws, cudaStream_t stream);
+
+/* diagg1 (MOZYME/diagg1.F90:16-503): F psi for every virtual LMO, the virtual
+ * LMO energies eigv, the occupied-virtual interaction list (fmo) -- rebuilt
+ * when idiagg <= 5 or even, recomputed on the previous list otherwise -- and,
+ * when idiagg <= 2 or divisible by 4, the occupied LMO energies eigs.  All
+ * cutoffs and orders as the reference; fao and p in the block storage.
+ * state[4] (host, in/out): fref, safety, oldlim, tiny of the previous call
+ * (start with 10, 1, 0, 0).  nfmo (device, nvir), ifmo (device, 2 x cap,
+ * 1-based LMO numbers) and fmo (device, cap) carry the list between calls;
+ * *nij: capacity in, entries out (MB_ERR_UNSUPPORTED if a rebuilt list would
+ * not fit, where the reference truncates).  *eigs_done: 1 if eigs was
+ * computed.  *sumt: the sum of |fmo| over the evaluated pairs (a fixed-order
+ * parallel sum; diagnostic only in the reference).  Bit-identical fmo, eigv,
+ * eigs and tiny. */
+size_t mb_mz_diagg1_ws_bytes(const MbMzLayout* layout, const MbMzLmos* occ, const MbMzLmos* vir);
+int mb_mz_diagg1_dev(const MbMzLayout* layout, const MbMzLmos* occ, const MbMzLmos* vir, const double* fao,
+                     const double* p, int idiagg, double* state, int* nfmo, int* ifmo, double* fmo,
+                     long long* nij, double* eigv, double* eigs, int* eigs_done, double* sumt, void* ws,
+                     cudaStream_t stream);
 
 /* helecz() (MOZYME/helecz.F90:16): sum p(h+f) with diagonal elements
  * weighted 1/2; *out (device).  Fixed-order parallel reduction. */

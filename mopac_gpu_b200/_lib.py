@@ -32,12 +32,15 @@ class MbMzLayout(ctypes.Structure):
                 ("iorbs", ctypes.c_void_p), ("pair_ptr", ctypes.c_void_p), ("pair_i", ctypes.c_void_p),
                 ("pair_j", ctypes.c_void_p), ("pair_off", ctypes.c_void_p), ("pair_woff", ctypes.c_void_p),
                 ("nw", ctypes.c_longlong), ("nbr_ptr", ctypes.c_void_p), ("nbr_atom", ctypes.c_void_p),
-                ("nbr_entry", ctypes.c_void_p), ("cutof1", ctypes.c_double), ("cutof2", ctypes.c_double)]
+                ("nbr_entry", ctypes.c_void_p), ("cutof1", ctypes.c_double), ("cutof2", ctypes.c_double),
+                ("first", ctypes.c_void_p), ("norbs", ctypes.c_int)]
 
 
 class MbMzLmos(ctypes.Structure):
     _fields_ = [("nlmo", ctypes.c_int), ("atom_ptr", ctypes.c_void_p), ("atom_lmo", ctypes.c_void_p),
-                ("atom_coff", ctypes.c_void_p), ("cocc", ctypes.c_void_p)]
+                ("atom_coff", ctypes.c_void_p), ("cocc", ctypes.c_void_p), ("ncf", ctypes.c_void_p),
+                ("nncf", ctypes.c_void_p), ("icocc", ctypes.c_void_p), ("ncocc", ctypes.c_void_p),
+                ("nentries", ctypes.c_longlong)]
 
 
 class ScfOpts(ctypes.Structure):
@@ -100,6 +103,11 @@ SIGNATURES = {
     "mb_mz_lmos_destroy": ([ctypes.POINTER(MbMzLmos)], _I),
     "mb_mz_density_dev": ([ctypes.POINTER(MbMzLayout), ctypes.POINTER(MbMzLmos), _I, _P, _P, _P], _I),
     "mb_mz_fock_ws_bytes": ([ctypes.POINTER(MbMzLayout)], ctypes.c_size_t),
+    "mb_mz_diagg1_ws_bytes": ([ctypes.POINTER(MbMzLayout), ctypes.POINTER(MbMzLmos), ctypes.POINTER(MbMzLmos)],
+                              ctypes.c_size_t),
+    "mb_mz_diagg1_dev": ([ctypes.POINTER(MbMzLayout), ctypes.POINTER(MbMzLmos), ctypes.POINTER(MbMzLmos), _P, _P,
+                          _I, _P, _P, _P, _P, ctypes.POINTER(_LL), _P, _P, ctypes.POINTER(_I),
+                          ctypes.POINTER(_D), _P, _P], _I),
     "mb_mz_fock_dev": ([ctypes.POINTER(MbMzLayout), _P, _P, _P, _P, _P, _P, _P], _I),
     "mb_mz_helecz_ws_bytes": ([], ctypes.c_size_t),
     "mb_mz_helecz_ws": ([_LL, _I, _P, _P, _P, _P, _P, _P, _P], _I),

@@ -467,6 +467,10 @@ extern "C" int mb_mz_layout_create(int numat, const int* iorbs, const double* co
     for (int e = ptr[b]; e < ptr[b + 1]; ++e)
       if (pj[e] != b) { const int a = pj[e]; nat_[nfill[a]] = b; nent[nfill[a]] = e; nfill[a]++; }
   std::vector<int> io(iorbs, iorbs + numat);
+  std::vector<int> fst(numat);
+  int norbs = 0;
+  for (int a = 0; a < numat; ++a) { fst[a] = norbs; norbs += iorbs[a]; }
+  out->norbs = norbs;
   out->numat = numat;
   out->mpack = mpack;
   out->npairs = (long long)pi.size();
@@ -482,6 +486,7 @@ extern "C" int mb_mz_layout_create(int numat, const int* iorbs, const double* co
   if (rc == MB_OK) rc = upload(ncount, &out->nbr_ptr);
   if (rc == MB_OK) rc = upload(nat_, &out->nbr_atom);
   if (rc == MB_OK) rc = upload(nent, &out->nbr_entry);
+  if (rc == MB_OK) rc = upload(fst, &out->first);
   if (rc != MB_OK) mb_mz_layout_destroy(out);
   return rc;
 }
@@ -497,6 +502,7 @@ extern "C" int mb_mz_layout_destroy(MbMzLayout* L) {
   cudaFree((void*)L->nbr_ptr);
   cudaFree((void*)L->nbr_atom);
   cudaFree((void*)L->nbr_entry);
+  cudaFree((void*)L->first);
   memset(L, 0, sizeof(*L));
   return MB_OK;
 }
@@ -545,11 +551,20 @@ extern "C" int mb_mz_lmos_create(int numat, const int* iorbs, int nlmo, const in
     if (c > ncocc_total) return mb_set_error(MB_ERR_ARG, "mb_mz_lmos_create: cocc too short for the atom lists");
   }
   std::vector<double> cv(cocc, cocc + ncocc_total);
+  long long nent = 0;
+  for (int i = 0; i < nlmo; ++i) nent = std::max<long long>(nent, (long long)nncf[i] + ncf[i]);
+  std::vector<int> vncf(ncf, ncf + nlmo), vnncf(nncf, nncf + nlmo), vic(icocc, icocc + nent),
+      vnco(ncocc, ncocc + nlmo);
   out->nlmo = nlmo;
+  out->nentries = nent;
   int rc = upload(cnt, &out->atom_ptr);
   if (rc == MB_OK) rc = upload(lmo, &out->atom_lmo);
   if (rc == MB_OK) rc = upload(coff, &out->atom_coff);
   if (rc == MB_OK) rc = upload(cv, &out->cocc);
+  if (rc == MB_OK) rc = upload(vncf, &out->ncf);
+  if (rc == MB_OK) rc = upload(vnncf, &out->nncf);
+  if (rc == MB_OK) rc = upload(vic, &out->icocc);
+  if (rc == MB_OK) rc = upload(vnco, &out->ncocc);
   if (rc != MB_OK) mb_mz_lmos_destroy(out);
   return rc;
 }
@@ -560,6 +575,10 @@ extern "C" int mb_mz_lmos_destroy(MbMzLmos* Q) {
   cudaFree((void*)Q->atom_lmo);
   cudaFree((void*)Q->atom_coff);
   cudaFree((void*)Q->cocc);
+  cudaFree((void*)Q->ncf);
+  cudaFree((void*)Q->nncf);
+  cudaFree((void*)Q->icocc);
+  cudaFree((void*)Q->ncocc);
   memset(Q, 0, sizeof(*Q));
   return MB_OK;
 }

@@ -1,0 +1,468 @@
+// diagg1 (MOZYME/diagg1.F90:16-503) on the device: for every virtual LMO psi_i
+// the product ws = F psi_i on the LMO's atoms, the LMO energy eigv(i), and
+// its interactions fmo(i, j) = <psi_j | ws> with the occupied LMOs, under the
+// reference's cutoffs and in its order; optionally the occupied LMO energies.
+//
+// One CTA per virtual LMO.  Its atoms, their squared coefficients (avir),
+// ws and aov live in shared memory; three bitmaps over the atoms (the LMO's
+// atoms, the partners of its first atom, the partners of its second atom)
+// answer the reference's pair tests in O(1).  Every ws element, eigv and
+// every fmo(i, j) is one thread's sequential sum in the reference's term
+// order, so all of them are bit-identical.  The interaction list is written
+// in two passes: a count per virtual LMO, an exclusive scan on the host, and
+// the ordered write (entries for LMO i in ascending j, LMOs in order), which
+// reproduces the reference's running counter ijc without a sequential loop.
+#include <math.h>
+#include <string.h>
+
+#include <vector>
+
+#include "mb_common.cuh"
+
+namespace {
+
+constexpr int MZ_MAXA = 256;  // atoms per virtual LMO handled by one CTA
+constexpr int MZ_T = 128;
+
+__device__ long long pair_offset(const MbMzLayout& L, int a, int b) {
+  if (a == b) return L.pair_off[L.pair_ptr[a + 1] - 1];
+  int lo = L.nbr_ptr[a], hi = L.nbr_ptr[a + 1] - 1;
+  while (lo <= hi) {
+    const int mid = (lo + hi) >> 1;
+    const int v = L.nbr_atom[mid];
+    if (v == b) return L.pair_off[L.nbr_entry[mid]];
+    if (v < b) lo = mid + 1; else hi = mid - 1;
+  }
+  return -1;  // outside cutof2: the reference's nijbo is -1 or -2, tested as < 0
+}
+
+// aocc(kk) = sum of squared coefficients of entry kk (one thread per LMO).
+__global__ void mzd_aocc(MbMzLmos Q, const int* __restrict__ iorbs, double* __restrict__ aocc) {
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < Q.nlmo; j += gridDim.x * blockDim.x) {
+    const int loopj = Q.ncocc[j];
+    int kl = 0;
+    for (int kk = Q.nncf[j]; kk < Q.nncf[j] + Q.ncf[j]; ++kk) {
+      const int k1 = Q.icocc[kk] - 1;
+      double sum = 0.0;
+      for (int k = 0; k < iorbs[k1]; ++k) {
+        const double c = Q.cocc[loopj + kl];
+        sum = DADD(sum, DMUL(c, c));
+        ++kl;
+      }
+      aocc[kk] = sum;
+    }
+  }
+}
+
+struct DiagArgs {
+  MbMzLayout L;
+  MbMzLmos occ, vir;
+  const double* fao;
+  const double* p;
+  const double* aocc;
+  double cutoff, flim, oldlim;
+  int mode;                       // 0: count, 1: write (rebuild), 2: recompute on the old list
+  const long long* list_off;      // write / recompute: first list position of each virtual LMO
+  int* nfmo;                      // count pass: entries per virtual LMO
+  int* ifmo;
+  double* fmo;
+  double* eigv;
+  double* sumt_part;              // per virtual LMO, sum of |fmo| in j order
+  unsigned long long* tiny_bits;  // max |fmo| (non-negative doubles order like their bits)
+  int* err;
+};
+
+__device__ __forceinline__ bool bit_test(const unsigned* bm, int a) { return (bm[a >> 5] >> (a & 31)) & 1u; }
+
+// Local index of atom a in the LMO's atom list (sorted copy), or -1.
+__device__ __forceinline__ int local_of(const int* s_sorted, const int* s_sidx, int n, int a) {
+  int lo = 0, hi = n - 1;
+  while (lo <= hi) {
+    const int mid = (lo + hi) >> 1;
+    const int v = s_sorted[mid];
+    if (v == a) return s_sidx[mid];
+    if (v < a) lo = mid + 1; else hi = mid - 1;
+  }
+  return -1;
+}
+
+// fmo(i, j) over occupied LMO j's atoms that belong to virtual LMO i.
+__device__ double mzd_fmo(const DiagArgs& A, int j, const unsigned* lat, const int* s_sorted, const int* s_sidx,
+                          int nce, const double* s_aov, const int* s_wpos, const double* s_ws, bool* lij) {
+  const int loopj = A.occ.ncocc[j];
+  double sum = 0.0;
+  int kl = 0;
+  *lij = false;
+  for (int kk = A.occ.nncf[j]; kk < A.occ.nncf[j] + A.occ.ncf[j]; ++kk) {
+    const int k1 = A.occ.icocc[kk] - 1;
+    const int nk = A.L.iorbs[k1];
+    if (!bit_test(lat, k1)) { kl += nk; continue; }
+    const int li = local_of(s_sorted, s_sidx, nce, k1);
+    if (DMUL(A.aocc[kk], s_aov[li]) < A.cutoff) { kl += nk; continue; }
+    *lij = true;
+    for (int k = 0; k < nk; ++k) {
+      sum = DADD(sum, DMUL(s_ws[s_wpos[li] + k], A.occ.cocc[loopj + kl]));
+      ++kl;
+    }
+  }
+  return sum;
+}
+
+__global__ void __launch_bounds__(MZ_T) mzd_virtual(DiagArgs A) {
+  extern __shared__ unsigned s_bits[];  // lat | near1 | near2, ceil(numat/32) words each
+  __shared__ int s_atom[MZ_MAXA], s_wpos[MZ_MAXA + 1], s_sorted[MZ_MAXA], s_sidx[MZ_MAXA];
+  __shared__ double s_avir[MZ_MAXA], s_aov[MZ_MAXA], s_ws[4 * MZ_MAXA];
+  __shared__ int s_eat[4 * MZ_MAXA];
+  __shared__ double s_val[MZ_T];
+  __shared__ int s_flag[MZ_T], s_scan[MZ_T];
+  __shared__ long long s_base;
+  __shared__ double s_sumt, s_tiny;
+  const int i = blockIdx.x, tid = threadIdx.x;
+  const MbMzLayout& L = A.L;
+  const int nce = A.vir.ncf[i], nn = A.vir.nncf[i], loopi = A.vir.ncocc[i];
+  if (nce > MZ_MAXA) {  // uniform over the CTA
+    if (tid == 0) atomicExch(A.err, 1);
+    return;
+  }
+  const int words = (L.numat + 31) >> 5;
+  unsigned* lat = s_bits;
+  unsigned* near1 = s_bits + words;
+  unsigned* near2 = s_bits + 2 * words;
+  for (int w = tid; w < 3 * words; w += MZ_T) s_bits[w] = 0u;
+  __syncthreads();
+  if (tid == 0) {
+    int pos = 0;
+    for (int t = 0; t < nce; ++t) {
+      const int a = A.vir.icocc[nn + t] - 1;
+      s_atom[t] = a;
+      s_wpos[t] = pos;
+      for (int x = 0; x < L.iorbs[a]; ++x) s_eat[pos + x] = t;
+      pos += L.iorbs[a];
+      // insertion into the sorted copy (short lists)
+      int q = t;
+      while (q > 0 && s_sorted[q - 1] > a) { s_sorted[q] = s_sorted[q - 1]; s_sidx[q] = s_sidx[q - 1]; --q; }
+      s_sorted[q] = a;
+      s_sidx[q] = t;
+    }
+    s_wpos[nce] = pos;
+    s_sumt = 0.0;
+    s_tiny = 0.0;
+  }
+  __syncthreads();
+  for (int t = tid; t < nce; t += MZ_T) {
+    const int a = s_atom[t];
+    double sum = 0.0;
+    for (int k = 0; k < L.iorbs[a]; ++k) {
+      const double c = A.vir.cocc[loopi + s_wpos[t] + k];
+      sum = DADD(sum, DMUL(c, c));
+    }
+    s_avir[t] = sum;
+    atomicOr(&lat[a >> 5], 1u << (a & 31));
+  }
+  __syncthreads();
+  // ws(orbital of atom j1, jx) = sum over the LMO's atoms k1 (in order) of F(k1, j1) psi(k1)
+  const int nws = s_wpos[nce];
+  for (int e = tid; e < nws; e += MZ_T) {
+    const int jjl = s_eat[e];
+    const int j1 = s_atom[jjl], jx = e - s_wpos[jjl] + 1;
+    const int nj = L.iorbs[j1];
+    double acc = 0.0;
+    for (int kk = 0; kk < nce; ++kk) {
+      const int k1 = s_atom[kk];
+      const long long kj = pair_offset(L, k1, j1);
+      if (kj < 0 || !(DMUL(s_avir[kk], A.p[kj]) > A.cutoff)) continue;
+      const int nk = L.iorbs[k1];
+      const double* cv = A.vir.cocc + loopi + s_wpos[kk];
+      for (int i4 = 1; i4 <= nk; ++i4) {
+        long long ii;
+        if (nk == 1 && nj == 1) ii = kj + 1;
+        else if (k1 > j1) ii = kj + (long long)(i4 - 1) * nj + jx;
+        else if (k1 < j1) ii = kj + (long long)(jx - 1) * nk + i4;
+        else ii = i4 > jx ? kj + (i4 * (i4 - 1)) / 2 + jx : kj + (jx * (jx - 1)) / 2 + i4;
+        acc = DADD(acc, DMUL(A.fao[ii - 1], cv[i4 - 1]));
+      }
+    }
+    s_ws[e] = acc;
+  }
+  __syncthreads();
+  for (int t = tid; t < nce; t += MZ_T) {
+    double sum = 0.0;
+    for (int k = 0; k < L.iorbs[s_atom[t]]; ++k) sum = DADD(sum, DMUL(s_ws[s_wpos[t] + k], s_ws[s_wpos[t] + k]));
+    s_aov[t] = sum;
+  }
+  __syncthreads();
+  if (tid == 0) {  // eigv(i)
+    double sum = 0.0;
+    for (int kk = 0; kk < nce; ++kk) {
+      if (!(DMUL(s_aov[kk], s_avir[kk]) > A.cutoff)) continue;
+      for (int k = 0; k < L.iorbs[s_atom[kk]]; ++k)
+        sum = DADD(sum, DMUL(s_ws[s_wpos[kk] + k], A.vir.cocc[loopi + s_wpos[kk] + k]));
+    }
+    A.eigv[i] = sum;
+  }
+  if (A.mode == 2) {
+    // recompute on the previous list: entries of LMO i at list_off[i] ..
+    const long long b0 = A.list_off[i];
+    const int cnt = A.nfmo[i];
+    double lmax = 0.0;
+    for (int q = tid; q < cnt; q += MZ_T) {
+      const int j = A.ifmo[2 * (b0 + q) + 1] - 1;
+      bool lij;
+      const double v = mzd_fmo(A, j, lat, s_sorted, s_sidx, nce, s_aov, s_wpos, s_ws, &lij);
+      A.fmo[b0 + q] = v;
+      lmax = fmax(lmax, fabs(v));
+    }
+    // |fmo| in list order for sumt, and the maximum
+    for (int q0 = 0; q0 < cnt; q0 += MZ_T) {
+      __syncthreads();
+      const int q = q0 + tid;
+      s_val[tid] = q < cnt ? fabs(A.fmo[b0 + q]) : 0.0;
+      __syncthreads();
+      if (tid == 0) {
+        const int m = min(MZ_T, cnt - q0);
+        for (int t = 0; t < m; ++t) s_sumt = DADD(s_sumt, s_val[t]);
+      }
+    }
+    if (lmax > 0.0) atomicMax(A.tiny_bits, (unsigned long long)__double_as_longlong(lmax));
+    __syncthreads();
+    if (tid == 0) A.sumt_part[i] = s_sumt;
+    return;
+  }
+  // rebuild: candidate occupied LMOs j in ascending order
+  const int i1 = s_atom[0], i2 = nce > 1 ? s_atom[1] : s_atom[0];
+  for (int q = L.nbr_ptr[i1] + tid; q < L.nbr_ptr[i1 + 1]; q += MZ_T) atomicOr(&near1[L.nbr_atom[q] >> 5], 1u << (L.nbr_atom[q] & 31));
+  for (int q = L.nbr_ptr[i2] + tid; q < L.nbr_ptr[i2 + 1]; q += MZ_T) atomicOr(&near2[L.nbr_atom[q] >> 5], 1u << (L.nbr_atom[q] & 31));
+  if (tid == 0) {
+    atomicOr(&near1[i1 >> 5], 1u << (i1 & 31));
+    atomicOr(&near2[i2 >> 5], 1u << (i2 & 31));
+    s_base = A.mode == 1 ? A.list_off[i] : 0;
+  }
+  __syncthreads();
+  int count = 0;
+  const int nocc = A.occ.nlmo;
+  for (int j0 = 0; j0 < nocc; j0 += MZ_T) {
+    const int j = j0 + tid;
+    int app = 0, ev = 0;
+    double val = 0.0;
+    if (j < nocc) {
+      const int j1 = A.occ.icocc[A.occ.nncf[j]] - 1;
+      const int j2 = A.occ.ncf[j] > 1 ? A.occ.icocc[A.occ.nncf[j] + 1] - 1 : j1;
+      const bool b11 = bit_test(near1, j1), b12 = bit_test(near1, j2), b21 = bit_test(near2, j1),
+                 b22 = bit_test(near2, j2);
+      if (b11 || b12 || b21 || b22) {
+        double s = 0.0;
+        if (b11) s = fabs(A.fao[pair_offset(L, i1, j1)]);
+        if (b12) s = DADD(s, fabs(A.fao[pair_offset(L, i1, j2)]));
+        if (b21) s = DADD(s, fabs(A.fao[pair_offset(L, i2, j1)]));
+        if (b22) s = DADD(s, fabs(A.fao[pair_offset(L, i2, j2)]));
+        if (s >= A.flim) {
+          bool lij;
+          val = mzd_fmo(A, j, lat, s_sorted, s_sidx, nce, s_aov, s_wpos, s_ws, &lij);
+          ev = 1;
+          app = (lij && fabs(val) > A.oldlim) ? 1 : 0;
+        }
+      }
+    }
+    __syncthreads();
+    s_val[tid] = ev ? fabs(val) : -1.0;
+    s_flag[tid] = app;
+    __syncthreads();
+    if (tid == 0) {  // ordered fold of |fmo| for sumt, max for tiny, running ranks
+      int run = 0;
+      const int m = min(MZ_T, nocc - j0);
+      for (int t = 0; t < m; ++t) {
+        if (s_val[t] >= 0.0) {
+          s_sumt = DADD(s_sumt, s_val[t]);
+          s_tiny = fmax(s_tiny, s_val[t]);
+        }
+        s_scan[t] = run;
+        run += s_flag[t];
+      }
+    }
+    __syncthreads();
+    if (A.mode == 1 && app) {
+      const long long pos = s_base + count + s_scan[tid];
+      A.ifmo[2 * pos] = i + 1;
+      A.ifmo[2 * pos + 1] = j + 1;
+      A.fmo[pos] = val;
+    }
+    const int m = min(MZ_T, nocc - j0);
+    count += s_scan[m - 1] + s_flag[m - 1];
+  }
+  __syncthreads();
+  if (tid == 0) {
+    if (A.mode == 0) A.nfmo[i] = count;
+    A.sumt_part[i] = s_sumt;
+    if (s_tiny > 0.0) atomicMax(A.tiny_bits, (unsigned long long)__double_as_longlong(s_tiny));
+  }
+}
+
+// Occupied LMO energies psi^T F psi with the reference's cutoff (one thread per LMO).
+__global__ void mzd_occ_energy(MbMzLayout L, MbMzLmos Q, const double* __restrict__ fao, const double* __restrict__ p,
+                               const double* __restrict__ aocc, double cutoff, double* __restrict__ eigs) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < Q.nlmo; i += gridDim.x * blockDim.x) {
+    const int loopi = Q.ncocc[i], nn = Q.nncf[i], nc = Q.ncf[i];
+    double sum = 0.0;
+    int jl = loopi;
+    for (int j = nn; j < nn + nc; ++j) {
+      const int j1 = Q.icocc[j] - 1;
+      const int nj = L.iorbs[j1];
+      int kl = loopi;
+      for (int k = nn; k < nn + nc; ++k) {
+        const int k1 = Q.icocc[k] - 1;
+        const int nk = L.iorbs[k1];
+        const long long k1j1 = pair_offset(L, k1, j1);
+        // avir(k1) of this LMO equals aocc of k1's entry
+        if (k1j1 >= 0 && DMUL(DMUL(aocc[k], p[k1j1]), aocc[k]) >= cutoff) {
+          for (int jx = 1; jx <= nj; ++jx) {
+            double sum1 = 0.0;
+            if (k1 > j1) {
+              for (int i4 = 1; i4 <= nk; ++i4)
+                sum1 = DADD(sum1, DMUL(fao[k1j1 + (long long)(i4 - 1) * nj + jx - 1], Q.cocc[kl + i4 - 1]));
+            } else if (k1 < j1) {
+              for (int i4 = 1; i4 <= nk; ++i4)
+                sum1 = DADD(sum1, DMUL(fao[k1j1 + (long long)(jx - 1) * nk + i4 - 1], Q.cocc[kl + i4 - 1]));
+            } else {
+              for (int j4 = 1; j4 <= jx; ++j4)
+                sum1 = DADD(sum1, DMUL(fao[k1j1 + (jx * (jx - 1)) / 2 + j4 - 1], Q.cocc[kl + j4 - 1]));
+              for (int i4 = jx + 1; i4 <= nk; ++i4)
+                sum1 = DADD(sum1, DMUL(fao[k1j1 + (i4 * (i4 - 1)) / 2 + jx - 1], Q.cocc[kl + i4 - 1]));
+            }
+            sum = DADD(sum, DMUL(Q.cocc[jl + jx - 1], sum1));
+          }
+        }
+        kl += nk;
+      }
+      jl += nj;
+    }
+    eigs[i] = sum;
+  }
+}
+
+inline size_t al256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+}  // namespace
+
+extern "C" size_t mb_mz_diagg1_ws_bytes(const MbMzLayout* L, const MbMzLmos* occ, const MbMzLmos* vir) {
+  if (!L || !occ || !vir) return 0;
+  return al256(sizeof(double) * (size_t)(occ->nentries + 1)) + al256(sizeof(double) * (size_t)(vir->nlmo + 1)) +
+         al256(sizeof(long long) * (size_t)(vir->nlmo + 1)) + al256(sizeof(unsigned long long)) + al256(sizeof(int)) +
+         256;
+}
+
+extern "C" int mb_mz_diagg1_dev(const MbMzLayout* L, const MbMzLmos* occ, const MbMzLmos* vir, const double* fao,
+                                const double* p, int idiagg, double* state, int* nfmo, int* ifmo, double* fmo,
+                                long long* nij, double* eigv, double* eigs, int* eigs_done, double* sumt, void* ws,
+                                cudaStream_t stream) {
+  if (!L || !occ || !vir || !fao || !p || !state || !nfmo || !ifmo || !fmo || !nij || !eigv || !eigs || !eigs_done ||
+      !sumt || !ws)
+    return mb_set_error(MB_ERR_ARG, "mb_mz_diagg1_dev: bad args");
+  const int nvir = vir->nlmo;
+  double fref = state[0], safety = state[1], oldlim = state[2], tiny = state[3];
+  const long long cap = *nij;
+  char* b = (char*)ws;
+  double* aocc = (double*)b; b += al256(sizeof(double) * (size_t)(occ->nentries + 1));
+  double* sumt_part = (double*)b; b += al256(sizeof(double) * (size_t)(nvir + 1));
+  long long* list_off = (long long*)b; b += al256(sizeof(long long) * (size_t)(nvir + 1));
+  unsigned long long* tiny_bits = (unsigned long long*)b; b += al256(sizeof(unsigned long long));
+  int* err = (int*)b;
+  // scalars as the reference sets them on entry (diagg1.F90:85-94)
+  const double cutlim = 1.0e-8;
+  double cutoff = cutlim > tiny * 10.0 * cutlim ? cutlim : tiny * 10.0 * cutlim;
+  const double flim = 3.0 < fref * 0.5 ? 3.0 : fref * 0.5;
+  fref = 0.0;
+  if (idiagg <= 5) cutoff = cutlim;
+  MB_CUDA(cudaMemsetAsync(tiny_bits, 0, sizeof(unsigned long long), stream));
+  MB_CUDA(cudaMemsetAsync(err, 0, sizeof(int), stream));
+  mzd_aocc<<<(occ->nlmo + 127) / 128, 128, 0, stream>>>(*occ, L->iorbs, aocc);
+  MB_LAUNCH_CHECK();
+  DiagArgs A;
+  A.L = *L;
+  A.occ = *occ;
+  A.vir = *vir;
+  A.fao = fao;
+  A.p = p;
+  A.aocc = aocc;
+  A.cutoff = cutoff;
+  A.flim = flim;
+  A.oldlim = oldlim;
+  A.list_off = list_off;
+  A.nfmo = nfmo;
+  A.ifmo = ifmo;
+  A.fmo = fmo;
+  A.eigv = eigv;
+  A.sumt_part = sumt_part;
+  A.tiny_bits = tiny_bits;
+  A.err = err;
+  const size_t smem = sizeof(unsigned) * 3 * (size_t)((L->numat + 31) / 32);
+  if (smem > 160 * 1024) return mb_set_error(MB_ERR_UNSUPPORTED, "mb_mz_diagg1_dev: too many atoms for the bitmaps");
+  static bool attr = false;
+  if (!attr) {
+    MB_CUDA(cudaFuncSetAttribute(mzd_virtual, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
+    attr = true;
+  }
+  const bool rebuild = idiagg <= 5 || idiagg % 2 == 0;
+  std::vector<int> cnt(nvir);
+  std::vector<long long> off(nvir + 1, 0);
+  long long total = 0;
+  if (rebuild) {
+    A.mode = 0;
+    mzd_virtual<<<nvir, MZ_T, smem, stream>>>(A);
+    MB_LAUNCH_CHECK();
+    MB_CUDA(cudaMemcpyAsync(cnt.data(), nfmo, sizeof(int) * nvir, cudaMemcpyDeviceToHost, stream));
+    MB_CUDA(cudaStreamSynchronize(stream));
+    for (int i = 0; i < nvir; ++i) off[i + 1] = off[i] + cnt[i];
+    total = off[nvir];
+    if (total > cap)
+      return mb_set_error(MB_ERR_UNSUPPORTED, "mb_mz_diagg1_dev: interaction list exceeds its capacity");
+    MB_CUDA(cudaMemcpyAsync(list_off, off.data(), sizeof(long long) * nvir, cudaMemcpyHostToDevice, stream));
+    MB_CUDA(cudaMemsetAsync(tiny_bits, 0, sizeof(unsigned long long), stream));
+    A.mode = 1;
+    mzd_virtual<<<nvir, MZ_T, smem, stream>>>(A);
+    MB_LAUNCH_CHECK();
+  } else {
+    MB_CUDA(cudaMemcpyAsync(cnt.data(), nfmo, sizeof(int) * nvir, cudaMemcpyDeviceToHost, stream));
+    MB_CUDA(cudaStreamSynchronize(stream));
+    for (int i = 0; i < nvir; ++i) off[i + 1] = off[i] + cnt[i];
+    total = off[nvir] < cap ? off[nvir] : cap;
+    MB_CUDA(cudaMemcpyAsync(list_off, off.data(), sizeof(long long) * nvir, cudaMemcpyHostToDevice, stream));
+    A.mode = 2;
+    mzd_virtual<<<nvir, MZ_T, smem, stream>>>(A);
+    MB_LAUNCH_CHECK();
+  }
+  std::vector<double> sp(nvir);
+  unsigned long long tb = 0;
+  int herr = 0;
+  MB_CUDA(cudaMemcpyAsync(sp.data(), sumt_part, sizeof(double) * nvir, cudaMemcpyDeviceToHost, stream));
+  MB_CUDA(cudaMemcpyAsync(&tb, tiny_bits, sizeof(tb), cudaMemcpyDeviceToHost, stream));
+  MB_CUDA(cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, stream));
+  MB_CUDA(cudaStreamSynchronize(stream));
+  if (herr) return mb_set_error(MB_ERR_UNSUPPORTED, "mb_mz_diagg1_dev: a virtual LMO covers more than 256 atoms");
+  double st = 0.0;
+  for (int i = 0; i < nvir; ++i) st += sp[i];
+  *sumt = st;
+  double tnew;
+  memcpy(&tnew, &tb, sizeof(tnew));
+  tiny = tnew;
+  const long long ijc = total;
+  if (ijc == cap) safety = safety * 2.0;
+  else safety = safety * 0.5 > 1.0 ? safety * 0.5 : 1.0;
+  *nij = ijc;
+  *eigs_done = 0;
+  if (idiagg > 2 && idiagg % 4 != 0) {
+    const double t2 = tiny * tiny;
+    fref = t2 * t2;
+  } else {
+    mzd_occ_energy<<<(occ->nlmo + 127) / 128, 128, 0, stream>>>(*L, *occ, fao, p, aocc, cutoff, eigs);
+    MB_LAUNCH_CHECK();
+    oldlim = tiny * safety * 1.0e-3;
+    const double t2 = tiny * tiny;
+    fref = t2 * t2;
+    *eigs_done = 1;
+  }
+  state[0] = fref;
+  state[1] = safety;
+  state[2] = oldlim;
+  state[3] = tiny;
+  return MB_OK;
+}

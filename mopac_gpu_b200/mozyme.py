@@ -117,3 +117,34 @@ def fock(layout: Layout, coord, w, ptot, h, out=None):
     check(lib().mb_mz_fock_dev(ctypes.byref(layout.s), _ptr(c), _ptr(w), _ptr(ptot), _ptr(h), _ptr(f), _ptr(ws),
                                _stream()))
     return f
+
+
+class Diagg1:
+    """diagg1's saved state (MOZYME/diagg1.F90: fref, safety, oldlim, tiny
+    and the interaction list) for one SCF, on the device."""
+
+    def __init__(self, layout: Layout, occ: Lmos, vir: Lmos, cap: int):
+        self.layout, self.occ, self.vir, self.cap = layout, occ, vir, int(cap)
+        self.state = np.array([10.0, 1.0, 0.0, 0.0])
+        nv = int(vir.s.nlmo)
+        self.nfmo = torch.zeros(nv, dtype=torch.int32, device="cuda")
+        self.ifmo = torch.zeros(2 * self.cap, dtype=torch.int32, device="cuda")
+        self.fmo = torch.zeros(self.cap, dtype=torch.float64, device="cuda")
+        self.eigv = torch.zeros(nv, dtype=torch.float64, device="cuda")
+        self.eigs = torch.zeros(int(occ.s.nlmo), dtype=torch.float64, device="cuda")
+        nb = int(lib().mb_mz_diagg1_ws_bytes(ctypes.byref(layout.s), ctypes.byref(occ.s), ctypes.byref(vir.s)))
+        self.ws = torch.empty(nb // 8 + 64, dtype=torch.float64, device="cuda")
+        self.nij = 0
+
+    def __call__(self, fao, p, idiagg: int):
+        nij = ctypes.c_longlong(self.cap)
+        done = ctypes.c_int(0)
+        sumt = ctypes.c_double(0.0)
+        base = (self.ws.data_ptr() + 255) & ~255
+        check(lib().mb_mz_diagg1_dev(ctypes.byref(self.layout.s), ctypes.byref(self.occ.s), ctypes.byref(self.vir.s),
+                                     _ptr(fao), _ptr(p), int(idiagg), self.state.ctypes.data, _ptr(self.nfmo),
+                                     _ptr(self.ifmo), _ptr(self.fmo), ctypes.byref(nij), _ptr(self.eigv),
+                                     _ptr(self.eigs), ctypes.byref(done), ctypes.byref(sumt), ctypes.c_void_p(base),
+                                     _stream()))
+        self.nij = nij.value
+        return nij.value, bool(done.value), sumt.value

@@ -1736,3 +1736,253 @@ void orc_mz_fock(int numat, const int *nat, const double *coord, const int *iorb
     free(qe);
     free(pt2);
 }
+
+/* diagg1 (MOZYME/diagg1.F90:16-503), lijbo path, s/p atoms.  LMO arrays as in
+ * MOZYME_C with 0-based starts (nncf, ncocc, nnce, ncvir) and 1-based atom
+ * numbers (icocc, icvir); first[a] is the 0-based first orbital of atom a.
+ * st[0..3] = fref, safety, oldlim, tiny of the previous call (in/out); the
+ * interaction list (ifmo as pairs of 1-based LMO numbers, fmo) and nfmo are
+ * in/out like the reference's saved arrays; *nij: capacity in, count out.
+ * eigv (virtual LMO energies) out; eigs (occupied) out when recomputed.
+ * Returns sumt. */
+double orc_mz_diagg1(int numat, const int *iorbs, const int *first, int norbs, const long long *nijbo,
+                     const double *fao, const double *p, int nocc, const int *ncf, const int *nncf, const int *icocc,
+                     const int *ncocc, const double *cocc, int nvir, const int *nce, const int *nnce,
+                     const int *icvir, const int *ncvir, const double *cvir, int idiagg, double *st, int *nfmo,
+                     int *ifmo, double *fmo, long long *nij_io, double *eigv, double *eigs, int *eigs_done) {
+#define NB_(i, j) nijbo[(long long)(i) * numat + (j)]
+    double fref = st[0], safety = st[1], oldlim = st[2], tiny = st[3];
+    const long long nij = *nij_io;
+    int ncocc_tot = 0;
+    for (int j = 0; j < nocc; ++j) ncocc_tot = nncf[j] + ncf[j] > ncocc_tot ? nncf[j] + ncf[j] : ncocc_tot;
+    double *aocc = (double *)calloc((size_t)ncocc_tot + 1, sizeof(double));
+    double *avir = (double *)calloc((size_t)numat, sizeof(double));
+    double *aov = (double *)calloc((size_t)numat, sizeof(double));
+    double *ws = (double *)calloc((size_t)norbs, sizeof(double));
+    char *latoms = (char *)calloc((size_t)numat, 1);
+    for (int j = 0; j < nocc; ++j) {
+        const int loopj = ncocc[j];
+        int kl = 0;
+        for (int kk = nncf[j]; kk < nncf[j] + ncf[j]; ++kk) {
+            const int k1 = icocc[kk] - 1;
+            double sum = 0.0;
+            for (int k = 0; k < iorbs[k1]; ++k) {
+                ++kl;
+                sum = sum + cocc[kl + loopj - 1] * cocc[kl + loopj - 1];
+            }
+            aocc[kk] = sum;
+        }
+    }
+    const double cutlim = 1.0e-8;
+    double cutoff = cutlim > tiny * 10.0 * cutlim ? cutlim : tiny * 10.0 * cutlim;
+    const double flim = 3.0 < fref * 0.5 ? 3.0 : fref * 0.5;
+    fref = 0.0;
+    if (idiagg <= 5) cutoff = cutlim;
+    double sumt = 0.0;
+    long long ijc = 0;
+    tiny = 0.0;
+    for (int i = 0; i < nvir; ++i) {
+        const int loopi = ncvir[i];
+        for (int a = 0; a < numat; ++a) latoms[a] = 0;
+        int l = 0;
+        for (int j = nnce[i]; j < nnce[i] + nce[i]; ++j) {
+            const int j1 = icvir[j] - 1;
+            double sum = 0.0;
+            for (int k = l + 1; k <= l + iorbs[j1]; ++k) sum = sum + cvir[k + loopi - 1] * cvir[k + loopi - 1];
+            l += iorbs[j1];
+            avir[j1] = sum;
+            latoms[j1] = 1;
+        }
+        for (int jj = nnce[i]; jj < nnce[i] + nce[i]; ++jj) {
+            const int j1 = icvir[jj] - 1;
+            for (int jx = 1; jx <= iorbs[j1]; ++jx) ws[first[j1] + jx - 1] = 0.0;
+            int kl = loopi;
+            for (int kk = nnce[i]; kk < nnce[i] + nce[i]; ++kk) {
+                const int k1 = icvir[kk] - 1;
+                const long long kj = NB_(k1, j1);
+                if (kj >= 0 && avir[k1] * p[kj] > cutoff) {
+                    if (iorbs[k1] == 1 && iorbs[j1] == 1) {
+                        ws[first[j1]] = ws[first[j1]] + fao[kj] * cvir[kl];
+                    } else if (k1 > j1) {
+                        long long ii = kj;
+                        for (int i4 = 1; i4 <= iorbs[k1]; ++i4)
+                            for (int jx = 1; jx <= iorbs[j1]; ++jx) {
+                                ++ii;
+                                ws[first[j1] + jx - 1] = ws[first[j1] + jx - 1] + fao[ii - 1] * cvir[kl + i4 - 1];
+                            }
+                    } else if (k1 < j1) {
+                        long long ii = kj;
+                        for (int jx = 1; jx <= iorbs[j1]; ++jx)
+                            for (int i4 = 1; i4 <= iorbs[k1]; ++i4) {
+                                ++ii;
+                                ws[first[j1] + jx - 1] = ws[first[j1] + jx - 1] + fao[ii - 1] * cvir[kl + i4 - 1];
+                            }
+                    } else {
+                        for (int jx = 1; jx <= iorbs[j1]; ++jx)
+                            for (int i4 = 1; i4 <= iorbs[j1]; ++i4) {
+                                const long long ii = i4 > jx ? kj + (i4 * (i4 - 1)) / 2 + jx : kj + (jx * (jx - 1)) / 2 + i4;
+                                ws[first[j1] + jx - 1] = ws[first[j1] + jx - 1] + fao[ii - 1] * cvir[kl + i4 - 1];
+                            }
+                    }
+                }
+                kl += iorbs[k1];
+            }
+        }
+        for (int j = 0; j < numat; ++j) {
+            if (latoms[j]) {
+                double sum = 0.0;
+                for (int k = first[j]; k < first[j] + iorbs[j]; ++k) sum = sum + ws[k] * ws[k];
+                aov[j] = sum;
+            } else {
+                aov[j] = 0.0;
+            }
+        }
+        {
+            double sum = 0.0;
+            int kl = loopi;
+            for (int kk = nnce[i]; kk < nnce[i] + nce[i]; ++kk) {
+                const int k1 = icvir[kk] - 1;
+                if (aov[k1] * avir[k1] > cutoff) {
+                    for (int k = first[k1]; k < first[k1] + iorbs[k1]; ++k) {
+                        ++kl;
+                        sum = sum + ws[k] * cvir[kl - 1];
+                    }
+                } else {
+                    kl += iorbs[k1];
+                }
+            }
+            eigv[i] = sum;
+        }
+        if (idiagg <= 5 || idiagg % 2 == 0) {
+            int nf = 0;
+            const int i1 = icvir[nnce[i]] - 1;
+            const int i2 = nce[i] > 1 ? icvir[nnce[i] + 1] - 1 : i1;
+            for (int j = 0; j < nocc; ++j) {
+                if (ijc == nij) continue;
+                const int j1 = icocc[nncf[j]] - 1;
+                const int j2 = ncf[j] > 1 ? icocc[nncf[j] + 1] - 1 : j1;
+                const long long a11 = NB_(i1, j1), a12 = NB_(i1, j2), a21 = NB_(i2, j1), a22 = NB_(i2, j2);
+                if (a11 >= 0 || a12 >= 0 || a21 >= 0 || a22 >= 0) {
+                    double sum = 0.0;
+                    if (a11 >= 0) sum = fabs(fao[a11]);
+                    if (a12 >= 0) sum = sum + fabs(fao[a12]);
+                    if (a21 >= 0) sum = sum + fabs(fao[a21]);
+                    if (a22 >= 0) sum = sum + fabs(fao[a22]);
+                    if (sum >= flim) {
+                        const int loopj = ncocc[j];
+                        int lij = 0, kl = 0;
+                        sum = 0.0;
+                        for (int kk = nncf[j]; kk < nncf[j] + ncf[j]; ++kk) {
+                            const int k1 = icocc[kk] - 1;
+                            if (aocc[kk] * aov[k1] < cutoff || !latoms[k1]) {
+                                kl += iorbs[k1];
+                            } else {
+                                lij = 1;
+                                for (int k = first[k1]; k < first[k1] + iorbs[k1]; ++k) {
+                                    ++kl;
+                                    sum = sum + ws[k] * cocc[kl + loopj - 1];
+                                }
+                            }
+                        }
+                        sumt = sumt + fabs(sum);
+                        tiny = tiny > fabs(sum) ? tiny : fabs(sum);
+                        if (lij && fabs(sum) > oldlim) {
+                            ++nf;
+                            ifmo[2 * ijc] = i + 1;
+                            ifmo[2 * ijc + 1] = j + 1;
+                            fmo[ijc] = sum;
+                            ++ijc;
+                        }
+                    }
+                }
+            }
+            nfmo[i] = nf;
+        } else {
+            const long long ij0 = ijc;
+            for (int jj = 1; jj <= nfmo[i]; ++jj) {
+                if (ijc == nij) break;
+                const int j = ifmo[2 * (ij0 + jj - 1) + 1] - 1;
+                const int loopj = ncocc[j];
+                double sum = 0.0;
+                int kl = 0;
+                for (int kk = nncf[j]; kk < nncf[j] + ncf[j]; ++kk) {
+                    const int k1 = icocc[kk] - 1;
+                    if (aov[k1] * aocc[kk] < cutoff || !latoms[k1]) {
+                        kl += iorbs[k1];
+                    } else {
+                        for (int k = first[k1]; k < first[k1] + iorbs[k1]; ++k) {
+                            ++kl;
+                            sum = sum + ws[k] * cocc[kl + loopj - 1];
+                        }
+                    }
+                }
+                sumt = sumt + fabs(sum);
+                tiny = tiny > fabs(sum) ? tiny : fabs(sum);
+                fmo[ijc] = sum;
+                ++ijc;
+            }
+        }
+    }
+    if (ijc == nij) safety = safety * 2.0;
+    else safety = safety * 0.5 > 1.0 ? safety * 0.5 : 1.0;
+    *nij_io = ijc;
+    *eigs_done = 0;
+    if (idiagg > 2 && idiagg % 4 != 0) {
+        const double t2 = tiny * tiny;  /* tiny**4 as gfortran expands it: (t t)(t t) */
+        fref = t2 * t2;
+    } else {
+        for (int i = 0; i < nocc; ++i) {
+            const int loopi = ncocc[i];
+            int l = 0;
+            for (int j = nncf[i]; j < nncf[i] + ncf[i]; ++j) {
+                const int j1 = icocc[j] - 1;
+                double sum = 0.0;
+                for (int k = l + 1; k <= l + iorbs[j1]; ++k) sum = sum + cocc[k + loopi - 1] * cocc[k + loopi - 1];
+                l += iorbs[j1];
+                avir[j1] = sum;
+            }
+            double sum = 0.0;
+            int jl = loopi;
+            for (int j = nncf[i]; j < nncf[i] + ncf[i]; ++j) {
+                const int j1 = icocc[j] - 1;
+                int kl = loopi;
+                for (int k = nncf[i]; k < nncf[i] + ncf[i]; ++k) {
+                    const int k1 = icocc[k] - 1;
+                    const long long k1j1 = NB_(k1, j1);
+                    if (k1j1 >= 0 && avir[k1] * p[k1j1] * aocc[k] >= cutoff) {
+                        for (int jx = 1; jx <= iorbs[j1]; ++jx) {
+                            double sum1 = 0.0;
+                            if (k1 > j1) {
+                                for (int i4 = 1; i4 <= iorbs[k1]; ++i4)
+                                    sum1 = sum1 + fao[k1j1 + (long long)(i4 - 1) * iorbs[j1] + jx - 1] * cocc[kl + i4 - 1];
+                            } else if (k1 < j1) {
+                                for (int i4 = 1; i4 <= iorbs[k1]; ++i4)
+                                    sum1 = sum1 + fao[k1j1 + (long long)(jx - 1) * iorbs[k1] + i4 - 1] * cocc[kl + i4 - 1];
+                            } else {
+                                for (int j4 = 1; j4 <= jx; ++j4)
+                                    sum1 = sum1 + fao[k1j1 + (jx * (jx - 1)) / 2 + j4 - 1] * cocc[kl + j4 - 1];
+                                for (int i4 = jx + 1; i4 <= iorbs[k1]; ++i4)
+                                    sum1 = sum1 + fao[k1j1 + (i4 * (i4 - 1)) / 2 + jx - 1] * cocc[kl + i4 - 1];
+                            }
+                            sum = sum + cocc[jl + jx - 1] * sum1;
+                        }
+                    }
+                    kl += iorbs[k1];
+                }
+                jl += iorbs[j1];
+            }
+            eigs[i] = sum;
+        }
+        oldlim = tiny * safety * 1.0e-3;
+        const double t2 = tiny * tiny;
+        fref = t2 * t2;
+        *eigs_done = 1;
+    }
+    st[0] = fref;
+    st[1] = safety;
+    st[2] = oldlim;
+    st[3] = tiny;
+    free(aocc); free(avir); free(aov); free(ws); free(latoms);
+#undef NB_
+    return sumt;
+}

@@ -156,3 +156,33 @@ def fock(nat, coord, iorbs, nijbo, w_dense, ptot, h):
                   np.ascontiguousarray(iorbs, np.int32), np.ascontiguousarray(nijbo.ravel()),
                   np.ascontiguousarray(w_dense, np.float64), np.ascontiguousarray(ptot, np.float64), f, qe)
     return f
+
+
+def diagg1(iorbs, nijbo, fao, p, occ, vir, idiagg, state, nfmo, ifmo, fmo, cap):
+    """diagg1 (MOZYME/diagg1.F90:16-503), lijbo path.  state = [fref, safety,
+    oldlim, tiny] (updated in place); nfmo, ifmo (2 x cap), fmo (cap) carry
+    the list between calls.  Returns (nij, eigv, eigs or None, sumt)."""
+    L = _lib()
+    if not hasattr(L, "_mz_diagg1_bound"):
+        i32p = np.ctypeslib.ndpointer(np.int32, flags="C")
+        i64p = np.ctypeslib.ndpointer(np.int64, flags="C")
+        f64p = np.ctypeslib.ndpointer(np.float64, flags="C")
+        L.orc_mz_diagg1.argtypes = ([ctypes.c_int, i32p, i32p, ctypes.c_int, i64p, f64p, f64p, ctypes.c_int]
+                                    + [i32p] * 4 + [f64p, ctypes.c_int] + [i32p] * 4
+                                    + [f64p, ctypes.c_int, f64p, i32p, i32p, f64p, ctypes.POINTER(ctypes.c_longlong),
+                                       f64p, f64p, ctypes.POINTER(ctypes.c_int)])
+        L.orc_mz_diagg1.restype = ctypes.c_double
+        L._mz_diagg1_bound = True
+    iorbs = np.ascontiguousarray(iorbs, np.int32)
+    first = np.ascontiguousarray(np.concatenate([[0], np.cumsum(iorbs)[:-1]]), np.int32)
+    ncf, nncf, icocc, ncocc, cocc = occ
+    nce, nnce, icvir, ncvir, cvir = vir
+    eigv = np.zeros(len(nce))
+    eigs = np.zeros(len(ncf))
+    nij = ctypes.c_longlong(cap)
+    done = ctypes.c_int(0)
+    sumt = L.orc_mz_diagg1(len(iorbs), iorbs, first, int(iorbs.sum()), np.ascontiguousarray(nijbo.ravel()),
+                           np.ascontiguousarray(fao), np.ascontiguousarray(p), len(ncf), ncf, nncf, icocc, ncocc,
+                           cocc, len(nce), nce, nnce, icvir, ncvir, cvir, idiagg, state, nfmo, ifmo, fmo,
+                           ctypes.byref(nij), eigv, eigs, ctypes.byref(done))
+    return nij.value, eigv, (eigs if done.value else None), sumt

@@ -169,6 +169,66 @@ def test_gpu_mozyme_fock_bit_identical(nwater, cut):
     L.close()
 
 
+def _diagg_case(nwater):
+    nat, xyz, _ = workloads.water_box(nwater)
+    s = oracle_system(nat, xyz)
+    iorbs = (s.nlast - s.nfirst + 1).astype(np.int32)
+    c1, c2 = mo.cutoffs(len(nat), 9.0)
+    mp, nb = mo.layout(iorbs, s.coord, c1, c2)
+    _, occ = workloads.mozyme_lmos(nat, xyz, radius=4.0, seed=3, per_heavy=4)
+    _, vir = workloads.mozyme_lmos(nat, xyz, radius=3.2, seed=4, per_heavy=2)
+    p = mo.density(iorbs, nb, occ, 0, mp)
+    fao = mo.dense_to_blocks(so.unpack(s.h, s.norbs), iorbs, nb, mp)
+    return s, iorbs, nb, mp, occ, vir, p, fao
+
+
+def test_oracle_diagg1_sequence_runs():
+    s, iorbs, nb, mp, occ, vir, p, fao = _diagg_case(32)
+    cap = 300 * s.norbs
+    st = np.array([10.0, 1.0, 0.0, 0.0])
+    nfmo = np.zeros(len(vir[0]), np.int32)
+    ifmo = np.zeros(2 * cap, np.int32)
+    fmo = np.zeros(cap)
+    for idg in range(0, 8):
+        nij, eigv, eigs, sumt = mo.diagg1(iorbs, nb, fao, p, occ, vir, idg, st, nfmo, ifmo, fmo, cap)
+        assert nij == nfmo.sum() and nij > 0
+        assert st[3] == pytest.approx(np.abs(fmo[:nij]).max() if idg % 2 == 1 and idg > 5 else st[3])
+        assert (eigs is not None) == (idg <= 2 or idg % 4 == 0)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("nwater", [32, 96])
+def test_gpu_diagg1_bit_identical_over_iterations(nwater):
+    torch = _need_gpu()
+    from mopac_gpu_b200 import mozyme
+    s, iorbs, nb, mp, occ, vir, p, fao = _diagg_case(nwater)
+    cap = 300 * s.norbs
+    st = np.array([10.0, 1.0, 0.0, 0.0])
+    nfmo = np.zeros(len(vir[0]), np.int32)
+    ifmo = np.zeros(2 * cap, np.int32)
+    fmo = np.zeros(cap)
+    c1, c2 = mo.cutoffs(len(iorbs), 9.0)
+    L = mozyme.Layout(iorbs, s.coord, c1, c2)
+    Qo, Qv = mozyme.Lmos(L, occ), mozyme.Lmos(L, vir)
+    D = mozyme.Diagg1(L, Qo, Qv, cap)
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    fd, pd = dev(fao), dev(p)
+    for idg in range(0, 9):
+        nij, eigv, eigs, sumt = mo.diagg1(iorbs, nb, fao, p, occ, vir, idg, st, nfmo, ifmo, fmo, cap)
+        gn, done, gsum = D(fd, pd, idg)
+        assert gn == nij
+        np.testing.assert_array_equal(D.nfmo.cpu().numpy(), nfmo)
+        np.testing.assert_array_equal(D.ifmo[:2 * nij].cpu().numpy(), ifmo[:2 * nij])
+        np.testing.assert_array_equal(D.fmo[:nij].cpu().numpy(), fmo[:nij])
+        np.testing.assert_array_equal(D.eigv.cpu().numpy(), eigv)
+        assert done == (eigs is not None)
+        if done:
+            np.testing.assert_array_equal(D.eigs.cpu().numpy(), eigs)
+        np.testing.assert_array_equal(D.state, st)
+        assert gsum == pytest.approx(sumt, rel=1e-12)
+    L.close()
+
+
 @pytest.mark.gpu
 def test_gpu_mozyme_fock_rejects_short_cutoff():
     torch = _need_gpu()
