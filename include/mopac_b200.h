@@ -248,7 +248,8 @@ typedef struct MbMzLmos {
   const int* nncf;
   const int* icocc;
   const int* ncocc;
-  long long nentries;  /* length of icocc */
+  long long nentries;  /* length of icocc (icocc_dim) */
+  long long ncoeff;    /* length of cocc (cocc_dim) */
 } MbMzLmos;
 /* Builds the layout (host coordinates in Angstrom, cutoffs squared, as
  * cutof1/cutof2 in fillij); nijbo (optional, host numat x numat) receives the
@@ -260,10 +261,15 @@ int mb_mz_layout_destroy(MbMzLayout* layout);
  * as iter_for_MOZYME.F90:183-190. */
 int mb_mz_idiag(const MbMzLayout* layout, long long* idiag);
 /* Uploads LMOs given in the reference's arrays (host; icocc 1-based atoms,
- * nncf/ncocc 0-based starts). */
+ * nncf/ncocc 0-based starts).  icocc_dim and cocc_dim are the arrays'
+ * lengths: the space between one LMO's end and the next LMO's start (and,
+ * for the last, up to these lengths) is where diagg2 may grow the LMO. */
 int mb_mz_lmos_create(int numat, const int* iorbs, int nlmo, const int* ncf, const int* nncf,
-                      const int* icocc, const int* ncocc, const double* cocc, long long ncocc_total,
-                      MbMzLmos* out);
+                      const int* icocc, const int* ncocc, const double* cocc, long long icocc_dim,
+                      long long cocc_dim, MbMzLmos* out);
+/* Rebuilds the per-atom index after diagg2 has grown LMOs (mb_mz_density_dev
+ * reads it). */
+int mb_mz_lmos_refresh(int numat, const int* iorbs_host, MbMzLmos* lmos);
 int mb_mz_lmos_destroy(MbMzLmos* lmos);
 /* density_for_MOZYME(p, mode, nclose, partp) (MOZYME/density_for_MOZYME.F90:16):
  * mode 0: P = 2 sum_LMO c c^T; -1: P = -2 (sum - partp/2); 1: P = 2 (sum +
@@ -301,6 +307,22 @@ int mb_mz_diagg1_dev(const MbMzLayout* layout, const MbMzLmos* occ, const MbMzLm
                      const double* p, int idiagg, double* state, int* nfmo, int* ifmo, double* fmo,
                      long long* nij, double* eigv, double* eigs, int* eigs_done, double* sumt, void* ws,
                      cudaStream_t stream);
+
+/* diagg2 (MOZYME/diagg2.F90:16-359): the 2x2 rotations of diagg1's list in
+ * list order, with the reference's growth of LMOs by atoms whose new
+ * coefficients exceed thresh and its rejection of rotations that would
+ * overflow an LMO's space (retried with alpha <- (alpha + 1)/2 when the
+ * last two calls rejected equally often).  Rotations touching disjoint LMO
+ * pairs commute, so the list runs in dependency levels, each level's
+ * rotations in parallel: bit-identical coefficients and atom lists.
+ * occ/vir are modified in place (call mb_mz_lmos_refresh on occ before the
+ * next density).  eigs/eigv: occupied / virtual LMO energies (device);
+ * ctl[5] (host): damping constant, shift, thresh, diagg1's tiny, bigeps;
+ * nrejct[2] (host, in/out) the rejection counts of the last two calls.
+ * *sumb: the sum of |beta| (fixed-order, diagnostic in the reference). */
+int mb_mz_diagg2_dev(const MbMzLayout* layout, MbMzLmos* occ, MbMzLmos* vir, const int* ifmo,
+                     const double* fmo, long long nij, const double* eigs, const double* eigv, int idiagg,
+                     const double* ctl, int* nrejct, double* sumb, long long* nrej, cudaStream_t stream);
 
 /* helecz() (MOZYME/helecz.F90:16): sum p(h+f) with diagonal elements
  * weighted 1/2; *out (device).  Fixed-order parallel reduction. */

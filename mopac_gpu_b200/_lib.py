@@ -40,7 +40,7 @@ class MbMzLmos(ctypes.Structure):
     _fields_ = [("nlmo", ctypes.c_int), ("atom_ptr", ctypes.c_void_p), ("atom_lmo", ctypes.c_void_p),
                 ("atom_coff", ctypes.c_void_p), ("cocc", ctypes.c_void_p), ("ncf", ctypes.c_void_p),
                 ("nncf", ctypes.c_void_p), ("icocc", ctypes.c_void_p), ("ncocc", ctypes.c_void_p),
-                ("nentries", ctypes.c_longlong)]
+                ("nentries", ctypes.c_longlong), ("ncoeff", ctypes.c_longlong)]
 
 
 class ScfOpts(ctypes.Structure):
@@ -99,7 +99,10 @@ SIGNATURES = {
     "mb_mz_layout_create": ([_I, _P, _P, _D, _D, ctypes.POINTER(MbMzLayout), _P], _I),
     "mb_mz_layout_destroy": ([ctypes.POINTER(MbMzLayout)], _I),
     "mb_mz_idiag": ([ctypes.POINTER(MbMzLayout), _P], _I),
-    "mb_mz_lmos_create": ([_I, _P, _I, _P, _P, _P, _P, _P, _LL, ctypes.POINTER(MbMzLmos)], _I),
+    "mb_mz_lmos_create": ([_I, _P, _I, _P, _P, _P, _P, _P, _LL, _LL, ctypes.POINTER(MbMzLmos)], _I),
+    "mb_mz_lmos_refresh": ([_I, _P, ctypes.POINTER(MbMzLmos)], _I),
+    "mb_mz_diagg2_dev": ([ctypes.POINTER(MbMzLayout), ctypes.POINTER(MbMzLmos), ctypes.POINTER(MbMzLmos), _P, _P,
+                          _LL, _P, _P, _I, _P, _P, ctypes.POINTER(_D), ctypes.POINTER(_LL), _P], _I),
     "mb_mz_lmos_destroy": ([ctypes.POINTER(MbMzLmos)], _I),
     "mb_mz_density_dev": ([ctypes.POINTER(MbMzLayout), ctypes.POINTER(MbMzLmos), _I, _P, _P, _P], _I),
     "mb_mz_fock_ws_bytes": ([ctypes.POINTER(MbMzLayout)], ctypes.c_size_t),

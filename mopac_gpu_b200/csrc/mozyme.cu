@@ -525,38 +525,49 @@ extern "C" int mb_mz_idiag(const MbMzLayout* L, long long* idiag) {
   return MB_OK;
 }
 
-extern "C" int mb_mz_lmos_create(int numat, const int* iorbs, int nlmo, const int* ncf, const int* nncf,
-                                 const int* icocc, const int* ncocc, const double* cocc, long long ncocc_total,
-                                 MbMzLmos* out) {
-  if (numat <= 0 || nlmo < 0 || !out) return mb_set_error(MB_ERR_ARG, "mb_mz_lmos_create: bad args");
-  memset(out, 0, sizeof(*out));
-  std::vector<int> cnt(numat + 1, 0);
+static int build_atom_index(int numat, const int* iorbs, int nlmo, const int* ncf, const int* nncf,
+                            const int* icocc, const int* ncocc, long long cocc_dim, std::vector<int>& cnt,
+                            std::vector<int>& lmo, std::vector<int>& coff) {
+  cnt.assign(numat + 1, 0);
   for (int i = 0; i < nlmo; ++i)
     for (int jj = nncf[i]; jj < nncf[i] + ncf[i]; ++jj) {
       const int a = icocc[jj] - 1;
-      if (a < 0 || a >= numat) return mb_set_error(MB_ERR_ARG, "mb_mz_lmos_create: atom number out of range");
+      if (a < 0 || a >= numat) return mb_set_error(MB_ERR_ARG, "MOZYME LMOs: atom number out of range");
       cnt[a + 1]++;
     }
   for (int a = 0; a < numat; ++a) cnt[a + 1] += cnt[a];
-  std::vector<int> fill(cnt.begin(), cnt.end() - 1), lmo(cnt[numat]), coff(cnt[numat]);
+  std::vector<int> fill(cnt.begin(), cnt.end() - 1);
+  lmo.assign(cnt[numat], 0);
+  coff.assign(cnt[numat], 0);
   for (int i = 0; i < nlmo; ++i) {  // ascending LMO order per atom by construction
-    int c = ncocc[i];
+    long long c = ncocc[i];
     for (int jj = nncf[i]; jj < nncf[i] + ncf[i]; ++jj) {
       const int a = icocc[jj] - 1;
       lmo[fill[a]] = i;
-      coff[fill[a]] = c;
+      coff[fill[a]] = (int)c;
       fill[a]++;
       c += iorbs[a];
     }
-    if (c > ncocc_total) return mb_set_error(MB_ERR_ARG, "mb_mz_lmos_create: cocc too short for the atom lists");
+    if (c > cocc_dim) return mb_set_error(MB_ERR_ARG, "MOZYME LMOs: cocc too short for the atom lists");
   }
-  std::vector<double> cv(cocc, cocc + ncocc_total);
-  long long nent = 0;
-  for (int i = 0; i < nlmo; ++i) nent = std::max<long long>(nent, (long long)nncf[i] + ncf[i]);
-  std::vector<int> vncf(ncf, ncf + nlmo), vnncf(nncf, nncf + nlmo), vic(icocc, icocc + nent),
+  return MB_OK;
+}
+
+extern "C" int mb_mz_lmos_create(int numat, const int* iorbs, int nlmo, const int* ncf, const int* nncf,
+                                 const int* icocc, const int* ncocc, const double* cocc, long long icocc_dim,
+                                 long long cocc_dim, MbMzLmos* out) {
+  if (numat <= 0 || nlmo < 0 || !out) return mb_set_error(MB_ERR_ARG, "mb_mz_lmos_create: bad args");
+  memset(out, 0, sizeof(*out));
+  for (int i = 0; i < nlmo; ++i)
+    if ((long long)nncf[i] + ncf[i] > icocc_dim) return mb_set_error(MB_ERR_ARG, "mb_mz_lmos_create: icocc too short");
+  std::vector<int> cnt, lmo, coff;
+  MB_TRY(build_atom_index(numat, iorbs, nlmo, ncf, nncf, icocc, ncocc, cocc_dim, cnt, lmo, coff));
+  std::vector<double> cv(cocc, cocc + cocc_dim);
+  std::vector<int> vncf(ncf, ncf + nlmo), vnncf(nncf, nncf + nlmo), vic(icocc, icocc + icocc_dim),
       vnco(ncocc, ncocc + nlmo);
   out->nlmo = nlmo;
-  out->nentries = nent;
+  out->nentries = icocc_dim;
+  out->ncoeff = cocc_dim;
   int rc = upload(cnt, &out->atom_ptr);
   if (rc == MB_OK) rc = upload(lmo, &out->atom_lmo);
   if (rc == MB_OK) rc = upload(coff, &out->atom_coff);
@@ -567,6 +578,27 @@ extern "C" int mb_mz_lmos_create(int numat, const int* iorbs, int nlmo, const in
   if (rc == MB_OK) rc = upload(vnco, &out->ncocc);
   if (rc != MB_OK) mb_mz_lmos_destroy(out);
   return rc;
+}
+
+extern "C" int mb_mz_lmos_refresh(int numat, const int* iorbs, MbMzLmos* Q) {
+  if (!Q || !iorbs) return mb_set_error(MB_ERR_ARG, "mb_mz_lmos_refresh: bad args");
+  const int n = Q->nlmo;
+  std::vector<int> ncf(n), nncf(n), ncocc(n), ic(Q->nentries);
+  MB_CUDA(cudaMemcpy(ncf.data(), Q->ncf, sizeof(int) * n, cudaMemcpyDeviceToHost));
+  MB_CUDA(cudaMemcpy(nncf.data(), Q->nncf, sizeof(int) * n, cudaMemcpyDeviceToHost));
+  MB_CUDA(cudaMemcpy(ncocc.data(), Q->ncocc, sizeof(int) * n, cudaMemcpyDeviceToHost));
+  MB_CUDA(cudaMemcpy(ic.data(), Q->icocc, sizeof(int) * Q->nentries, cudaMemcpyDeviceToHost));
+  std::vector<int> cnt, lmo, coff;
+  MB_TRY(build_atom_index(numat, iorbs, n, ncf.data(), nncf.data(), ic.data(), ncocc.data(), Q->ncoeff, cnt, lmo,
+                          coff));
+  cudaFree((void*)Q->atom_ptr);
+  cudaFree((void*)Q->atom_lmo);
+  cudaFree((void*)Q->atom_coff);
+  Q->atom_ptr = Q->atom_lmo = Q->atom_coff = nullptr;
+  MB_TRY(upload(cnt, &Q->atom_ptr));
+  MB_TRY(upload(lmo, &Q->atom_lmo));
+  MB_TRY(upload(coff, &Q->atom_coff));
+  return MB_OK;
 }
 
 extern "C" int mb_mz_lmos_destroy(MbMzLmos* Q) {

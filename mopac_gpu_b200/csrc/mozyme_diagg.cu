@@ -466,3 +466,290 @@ extern "C" int mb_mz_diagg1_dev(const MbMzLayout* L, const MbMzLmos* occ, const 
   state[3] = tiny;
   return MB_OK;
 }
+
+// ------------------------------------------------------------------ diagg2
+namespace {
+
+struct D2Args {
+  MbMzLmos occ, vir;
+  const int* iorbs;
+  const int* ifmo;
+  const double* fmo;
+  const double* eigs;
+  const double* eigv;
+  const long long* order;
+  long long lo, hi;
+  double cst, shift, thresh, tiny, biglim;
+  int retry, nocc, nvir, norbs;
+  double* beta_sum;
+  int* rej;
+};
+
+// Offset of atom a's coefficients in LMO q's block (atoms nn .. nn+cnt), or -1.
+__device__ __forceinline__ int find_atom(const int* ic, int nn, int cnt, const int* iorbs, int a) {
+  int off = 0;
+  for (int t = nn; t < nn + cnt; ++t) {
+    const int b = ic[t] - 1;
+    if (b == a) return off;
+    off += iorbs[b];
+  }
+  return -1;
+}
+
+// One thread per rotation of the level.  Whether a rotation is rejected
+// depends only on coefficients it has not yet touched (those of atoms in one
+// LMO only), so a dry run decides it first; modifying and then restoring, as
+// the reference does, leaves the same state as not modifying.
+__global__ void mzd2_level(D2Args A) {
+  const long long q = A.lo + blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (q >= A.hi) return;
+  const long long e = A.order[q];
+  const int i = A.ifmo[2 * e] - 1, j = A.ifmo[2 * e + 1] - 1;
+  double bs = 0.0;
+  int rj = 0;
+  const double fm = A.fmo[e];
+  if (!(fabs(fm) >= A.tiny)) { A.beta_sum[e] = 0.0; A.rej[e] = 0; return; }
+  const double c = DMUL(fm, A.cst);
+  const double d = DSUB(DSUB(A.eigs[j], A.eigv[i]), A.shift);
+  if (!(fabs(c / d) >= A.biglim)) { A.beta_sum[e] = 0.0; A.rej[e] = 0; return; }
+  int* ncf = const_cast<int*>(A.occ.ncf);
+  int* icocc = const_cast<int*>(A.occ.icocc);
+  double* cocc = const_cast<double*>(A.occ.cocc);
+  int* nce = const_cast<int*>(A.vir.ncf);
+  int* icvir = const_cast<int*>(A.vir.icocc);
+  double* cvir = const_cast<double*>(A.vir.cocc);
+  const int* nncf = A.occ.nncf;
+  const int* nnce = A.vir.nncf;
+  const long long loopj = A.occ.ncocc[j], loopi = A.vir.ncocc[i];
+  // spaces, 1-based ends as in the reference
+  const long long jlr = loopj + 1, ilr = loopi + 1;
+  long long jur = (j != A.nocc - 1) ? A.occ.ncocc[j + 1] : A.occ.ncoeff;
+  const long long jncf = (j != A.nocc - 1) ? nncf[j + 1] : A.occ.nentries;
+  long long iur = (i != A.nvir - 1) ? A.vir.ncocc[i + 1] : A.vir.ncoeff;
+  const long long incv = (i != A.nvir - 1) ? nnce[i + 1] : A.vir.nentries;
+  jur = jlr + A.norbs - 1 < jur ? jlr + A.norbs - 1 : jur;
+  iur = ilr + A.norbs - 1 < iur ? ilr + A.norbs - 1 : iur;
+  const int ncf0 = ncf[j], nce0 = nce[i];
+  const double ee = copysign(sqrt(DADD(DMUL(DMUL(4.0, c), c), DMUL(d, d))), d);
+  double alpha = sqrt(DMUL(0.5, DADD(1.0, d / ee)));
+  for (;;) {
+    const double beta = -copysign(sqrt(DSUB(1.0, DMUL(alpha, alpha))), c);
+    bs = DADD(bs, fabs(beta));
+    // ---- dry run: growth decisions and the space checks, in the reference's order
+    bool rejected = false;
+    long long mlf = 0;
+    for (int t = nncf[j]; t < nncf[j] + ncf0; ++t) mlf += A.iorbs[icocc[t] - 1];
+    long long nfj = ncf0, mle = 0;
+    for (int le = nnce[i]; le < nnce[i] + nce0; ++le) {
+      const int mie = icvir[le] - 1;
+      const int no = A.iorbs[mie];
+      if (find_atom(icocc, nncf[j], ncf0, A.iorbs, mie) < 0) {
+        double sum = 0.0;
+        for (int k = 0; k < no; ++k) {
+          const double t = DMUL(beta, cvir[loopi + mle + k]);
+          sum = DADD(sum, DMUL(t, t));
+        }
+        if (sum > A.thresh) {
+          if (nncf[j] + nfj >= jncf || mlf + no + loopj > jur) { rejected = true; break; }
+          ++nfj;
+          mlf += no;
+        }
+      }
+      mle += no;
+    }
+    long long nfi = nce0;
+    if (!rejected) {
+      long long off = 0;
+      for (int lf = nncf[j]; lf < nncf[j] + ncf0; ++lf) {
+        const int ii = icocc[lf] - 1;
+        const int no = A.iorbs[ii];
+        if (find_atom(icvir, nnce[i], nce0, A.iorbs, ii) < 0) {
+          double sum = 0.0;
+          for (int k = 0; k < no; ++k) {
+            const double t = DMUL(beta, cocc[loopj + off + k]);
+            sum = DADD(sum, DMUL(t, t));
+          }
+          if (sum > A.thresh) {
+            if (nnce[i] + nfi >= incv || mle + no + loopi > iur) { rejected = true; break; }
+            ++nfi;
+            mle += no;
+          }
+        }
+        off += no;
+      }
+    }
+    if (rejected) {
+      ++rj;
+      if (A.retry) { alpha = DMUL(0.5, DADD(alpha, 1.0)); continue; }
+      break;
+    }
+    // ---- apply: rotations and the atoms added to LMO j (loop over LMO i's atoms)
+    mlf = 0;
+    for (int t = nncf[j]; t < nncf[j] + ncf0; ++t) mlf += A.iorbs[icocc[t] - 1];
+    mle = 0;
+    for (int le = nnce[i]; le < nnce[i] + nce0; ++le) {
+      const int mie = icvir[le] - 1;
+      const int no = A.iorbs[mie];
+      const int uj = find_atom(icocc, nncf[j], ncf0, A.iorbs, mie);
+      if (uj >= 0) {
+        for (int k = 0; k < no; ++k) {
+          const long long pj = loopj + uj + k, pi = loopi + mle + k;
+          const double a = cocc[pj], b = cvir[pi];
+          cocc[pj] = DADD(DMUL(alpha, a), DMUL(beta, b));
+          cvir[pi] = DSUB(DMUL(alpha, b), DMUL(beta, a));
+        }
+      } else {
+        double sum = 0.0;
+        for (int k = 0; k < no; ++k) {
+          const double t = DMUL(beta, cvir[loopi + mle + k]);
+          sum = DADD(sum, DMUL(t, t));
+        }
+        if (sum > A.thresh) {
+          ncf[j] = ncf[j] + 1;
+          icocc[nncf[j] + ncf[j] - 1] = mie + 1;
+          for (int k = 0; k < no; ++k) {
+            const long long pi = loopi + mle + k;
+            cocc[loopj + mlf + k] = DMUL(beta, cvir[pi]);
+            cvir[pi] = DMUL(alpha, cvir[pi]);
+          }
+          mlf += no;
+        }
+      }
+      mle += no;
+    }
+    // atoms added to LMO i (loop over LMO j's original atoms not in LMO i)
+    long long off = 0;
+    for (int lf = nncf[j]; lf < nncf[j] + ncf0; ++lf) {
+      const int ii = icocc[lf] - 1;
+      const int no = A.iorbs[ii];
+      if (find_atom(icvir, nnce[i], nce0, A.iorbs, ii) < 0) {
+        double sum = 0.0;
+        for (int k = 0; k < no; ++k) {
+          const double t = DMUL(beta, cocc[loopj + off + k]);
+          sum = DADD(sum, DMUL(t, t));
+        }
+        if (sum > A.thresh) {
+          nce[i] = nce[i] + 1;
+          icvir[nnce[i] + nce[i] - 1] = ii + 1;
+          for (int k = 0; k < no; ++k) {
+            const long long pj = loopj + off + k;
+            cvir[loopi + mle + k] = DMUL(-beta, cocc[pj]);
+            cocc[pj] = DMUL(alpha, cocc[pj]);
+          }
+          mle += no;
+        }
+      }
+      off += no;
+    }
+    break;
+  }
+  A.beta_sum[e] = bs;
+  A.rej[e] = rj;
+}
+
+}  // namespace
+
+extern "C" int mb_mz_diagg2_dev(const MbMzLayout* L, MbMzLmos* occ, MbMzLmos* vir, const int* ifmo, const double* fmo,
+                                long long nij, const double* eigs, const double* eigv, int idiagg, const double* ctl,
+                                int* nrejct, double* sumb, long long* nrej, cudaStream_t stream) {
+  if (!L || !occ || !vir || !ctl || !nrejct || !sumb || !nrej || nij < 0)
+    return mb_set_error(MB_ERR_ARG, "mb_mz_diagg2_dev: bad args");
+  *sumb = 0.0;
+  *nrej = 0;
+  const int retry = (nrejct[0] == nrejct[1] && nrejct[0] != 0 && nrejct[0] < 20);
+  double tiny, biglim;
+  if (idiagg % 5 == 0 || idiagg <= 5) {
+    tiny = -1.0;
+    biglim = -1.0;
+  } else {
+    tiny = 0.01 * ctl[3];
+    biglim = ctl[4];
+  }
+  if (nij == 0) {
+    nrejct[1] = nrejct[0];
+    nrejct[0] = 0;
+    return MB_OK;
+  }
+  // dependency levels: an entry follows the last earlier entry of its virtual and of its occupied LMO
+  std::vector<int> hl(2 * (size_t)nij);
+  MB_CUDA(cudaMemcpyAsync(hl.data(), ifmo, sizeof(int) * 2 * (size_t)nij, cudaMemcpyDeviceToHost, stream));
+  MB_CUDA(cudaStreamSynchronize(stream));
+  std::vector<int> lastv(vir->nlmo, 0), lasto(occ->nlmo, 0), lvl(nij);
+  int nlev = 0;
+  for (long long e = 0; e < nij; ++e) {
+    const int i = hl[2 * e] - 1, j = hl[2 * e + 1] - 1;
+    if (i < 0 || i >= vir->nlmo || j < 0 || j >= occ->nlmo) return mb_set_error(MB_ERR_ARG, "diagg2: bad list entry");
+    const int lv = 1 + (lastv[i] > lasto[j] ? lastv[i] : lasto[j]);
+    lastv[i] = lasto[j] = lv;
+    lvl[e] = lv;
+    if (lv > nlev) nlev = lv;
+  }
+  std::vector<long long> start(nlev + 2, 0), order(nij);
+  for (long long e = 0; e < nij; ++e) start[lvl[e] + 1]++;
+  for (int v = 1; v <= nlev + 1; ++v) start[v] += start[v - 1];
+  {
+    std::vector<long long> fill(start.begin(), start.end());
+    for (long long e = 0; e < nij; ++e) order[fill[lvl[e]]++] = e;
+  }
+  long long* d_order = nullptr;
+  double* d_bs = nullptr;
+  int* d_rej = nullptr;
+  MB_CUDA(cudaMallocAsync((void**)&d_order, sizeof(long long) * nij, stream));
+  MB_CUDA(cudaMallocAsync((void**)&d_bs, sizeof(double) * nij, stream));
+  MB_CUDA(cudaMallocAsync((void**)&d_rej, sizeof(int) * nij, stream));
+  int rc = MB_OK;
+  if (cudaMemcpyAsync(d_order, order.data(), sizeof(long long) * nij, cudaMemcpyHostToDevice, stream) != cudaSuccess)
+    rc = mb_set_error(MB_ERR_CUDA, "diagg2: upload");
+  D2Args A;
+  A.occ = *occ;
+  A.vir = *vir;
+  A.iorbs = L->iorbs;
+  A.ifmo = ifmo;
+  A.fmo = fmo;
+  A.eigs = eigs;
+  A.eigv = eigv;
+  A.order = d_order;
+  A.cst = ctl[0];
+  A.shift = ctl[1];
+  A.thresh = ctl[2];
+  A.tiny = tiny;
+  A.biglim = biglim;
+  A.retry = retry;
+  A.nocc = occ->nlmo;
+  A.nvir = vir->nlmo;
+  A.norbs = L->norbs;
+  A.beta_sum = d_bs;
+  A.rej = d_rej;
+  for (int v = 1; v <= nlev && rc == MB_OK; ++v) {
+    A.lo = start[v];
+    A.hi = start[v + 1];
+    const long long cnt = A.hi - A.lo;
+    if (cnt <= 0) continue;
+    mzd2_level<<<(unsigned)((cnt + 127) / 128), 128, 0, stream>>>(A);
+    mb_count_launch();
+    if (cudaGetLastError() != cudaSuccess) rc = mb_set_error(MB_ERR_CUDA, "diagg2: launch");
+  }
+  std::vector<double> bs(nij);
+  std::vector<int> rj(nij);
+  if (rc == MB_OK && (cudaMemcpyAsync(bs.data(), d_bs, sizeof(double) * nij, cudaMemcpyDeviceToHost, stream) !=
+                          cudaSuccess ||
+                      cudaMemcpyAsync(rj.data(), d_rej, sizeof(int) * nij, cudaMemcpyDeviceToHost, stream) !=
+                          cudaSuccess ||
+                      cudaStreamSynchronize(stream) != cudaSuccess))
+    rc = mb_set_error(MB_ERR_CUDA, "diagg2: results");
+  cudaFreeAsync(d_order, stream);
+  cudaFreeAsync(d_bs, stream);
+  cudaFreeAsync(d_rej, stream);
+  if (rc != MB_OK) return rc;
+  double sb = 0.0;
+  long long nr = 0;
+  for (long long e = 0; e < nij; ++e) {
+    sb += bs[e];
+    nr += rj[e];
+  }
+  *sumb = sb;
+  *nrej = nr;
+  nrejct[1] = nrejct[0];
+  nrejct[0] = (int)nr;
+  return MB_OK;
+}

@@ -24,6 +24,14 @@ def _ptr(t: torch.Tensor):
     return ctypes.c_void_p(t.data_ptr())
 
 
+def _device_view(addr: int, count: int, typestr: str) -> torch.Tensor:
+    """A torch view of library-owned device memory (no copy)."""
+    class _A:
+        __cuda_array_interface__ = {"shape": (count,), "typestr": typestr, "data": (addr, False), "version": 3,
+                                    "strides": None}
+    return torch.as_tensor(_A(), device="cuda")
+
+
 class Layout:
     """Pair-block storage for atoms with iorbs orbitals at coord (Angstrom);
     cutof1, cutof2 squared as in fillij."""
@@ -67,9 +75,22 @@ class Lmos:
                       ncocc.astype(np.int32), cocc.astype(np.float64))
         ncf, nncf, icocc, ncocc, cocc = self._keep
         self.s = MbMzLmos()
+        self.numat = int(layout.iorbs.size)
+        self._iorbs = layout.iorbs
         check(lib().mb_mz_lmos_create(layout.iorbs.size, layout.iorbs.ctypes.data, int(ncf.size), ncf.ctypes.data,
                                       nncf.ctypes.data, icocc.ctypes.data, ncocc.ctypes.data, cocc.ctypes.data,
-                                      int(cocc.size), ctypes.byref(self.s)))
+                                      int(icocc.size), int(cocc.size), ctypes.byref(self.s)))
+
+    def refresh(self):
+        """Rebuild the per-atom index after diagg2 grew LMOs."""
+        check(lib().mb_mz_lmos_refresh(self.numat, self._iorbs.ctypes.data, ctypes.byref(self.s)))
+
+    def to_host(self):
+        """(ncf, icocc, cocc) as they are on the device now."""
+        n = int(self.s.nlmo)
+        return (_device_view(self.s.ncf, n, "<i4").cpu().numpy(),
+                _device_view(self.s.icocc, int(self.s.nentries), "<i4").cpu().numpy(),
+                _device_view(self.s.cocc, int(self.s.ncoeff), "<f8").cpu().numpy())
 
     def close(self):
         if self.s is not None:
@@ -148,3 +169,17 @@ class Diagg1:
                                      _stream()))
         self.nij = nij.value
         return nij.value, bool(done.value), sumt.value
+
+
+def diagg2(layout: Layout, occ: Lmos, vir: Lmos, d1: "Diagg1", idiagg: int, ctl, nrejct):
+    """diagg2 on diagg1's list: rotates occ and vir in place.  ctl = (damping
+    constant, shift, thresh, diagg1's tiny, bigeps); nrejct (int32[2]) is
+    updated.  Returns (sumb, nrej)."""
+    c = np.ascontiguousarray(ctl, np.float64)
+    sumb = ctypes.c_double(0.0)
+    nrej = ctypes.c_longlong(0)
+    check(lib().mb_mz_diagg2_dev(ctypes.byref(layout.s), ctypes.byref(occ.s), ctypes.byref(vir.s), _ptr(d1.ifmo),
+                                 _ptr(d1.fmo), int(d1.nij), _ptr(d1.eigs), _ptr(d1.eigv), int(idiagg),
+                                 c.ctypes.data, nrejct.ctypes.data, ctypes.byref(sumb), ctypes.byref(nrej),
+                                 _stream()))
+    return sumb.value, nrej.value

@@ -217,13 +217,14 @@ def formula(nat) -> str:
     return "".join(f"{sym[z]}{c[z]}" for z in (6, 1, 8) if c[z])
 
 
-def mozyme_lmos(nat, xyz, radius: float = 4.0, seed: int = 11, per_heavy: int = 4):
+def mozyme_lmos(nat, xyz, radius: float = 4.0, seed: int = 11, per_heavy: int = 4, pad_atoms: int = 0):
     """Synthetic occupied LMOs in the reference's MOZYME_C arrays, for kernel
     tests and timing: every O or C atom owns `per_heavy` LMOs that cover the
     atom itself, then every other atom within `radius` Angstrom in order of
     distance (the way diagg2 grows an LMO outward); coefficients decay with
-    distance.  Returns (iorbs, (ncf, nncf, icocc, ncocc, cocc)) with icocc
-    1-based and nncf/ncocc 0-based starts."""
+    distance.  pad_atoms empty atom slots (and 4 coefficients each) follow
+    every LMO, the room diagg2 may grow it into.  Returns (iorbs, (ncf, nncf,
+    icocc, ncocc, cocc)) with icocc 1-based and nncf/ncocc 0-based starts."""
     nat = np.asarray(nat)
     xyz = np.asarray(xyz, float).reshape(-1, 3)
     rng = np.random.default_rng(seed)
@@ -238,9 +239,14 @@ def mozyme_lmos(nat, xyz, radius: float = 4.0, seed: int = 11, per_heavy: int = 
             nncf.append(len(icocc))
             ncocc.append(len(cocc))
             ncf.append(len(near))
+            vec = []
             for b in near:
                 icocc.append(int(b) + 1)
-                cocc.extend((rng.normal(size=iorbs[b]) * np.exp(-d[b] / 1.5)).tolist())
+                vec.extend((rng.normal(size=iorbs[b]) * np.exp(-d[b] / 1.5)).tolist())
+            vec = np.asarray(vec)
+            cocc.extend((vec / np.linalg.norm(vec)).tolist())  # unit LMOs
+            icocc.extend([0] * pad_atoms)
+            cocc.extend([0.0] * (4 * pad_atoms))
     lmos = (np.array(ncf, np.int32), np.array(nncf, np.int32), np.array(icocc, np.int32),
             np.array(ncocc, np.int32), np.array(cocc, np.float64))
     return iorbs, lmos

@@ -1986,3 +1986,146 @@ double orc_mz_diagg1(int numat, const int *iorbs, const int *first, int norbs, c
 #undef NB_
     return sumt;
 }
+
+/* diagg2 (MOZYME/diagg2.F90:16-359): the 2x2 rotations of the interaction
+ * list in order, growing an LMO by an atom whose new coefficients exceed
+ * thresh and rejecting (restoring both LMOs) a rotation that would overflow
+ * their space.  LMO arrays 0-based starts as in orc_mz_diagg1; nncf/ncocc
+ * (nnce/ncvir) of LMO k+1 bound LMO k's space, icocc_dim/cocc_dim
+ * (icvir_dim/cvir_dim) the last one's.  ctl[0..4] = const (damping), shift,
+ * thresh, tiny (diagg1's, in: scaled here as the reference does), bigeps;
+ * nrejct[2] saved between calls.  eigs: occupied LMO energies, eigv: virtual.
+ * Returns sumb (sum of |beta|). */
+double orc_mz_diagg2(int numat, const int *iorbs, int norbs, int nocc, int *ncf, const int *nncf, int *icocc,
+                     const int *ncocc, double *cocc, long long icocc_dim, long long cocc_dim, int nvir, int *nce,
+                     const int *nnce, int *icvir, const int *ncvir, double *cvir, long long icvir_dim,
+                     long long cvir_dim, const int *ifmo, const double *fmo, long long nij, const double *eigs,
+                     const double *eigv, int idiagg, const double *ctl, int *nrejct, long long *nrej_out) {
+    const double cst = ctl[0], shift = ctl[1], thresh = ctl[2], bigeps = ctl[4];
+    double tiny = ctl[3], biglim;
+    const int retry = (nrejct[0] == nrejct[1] && nrejct[0] != 0 && nrejct[0] < 20);
+    if (idiagg % 5 == 0 || idiagg <= 5) {
+        tiny = -1.0;
+        biglim = -1.0;
+    } else {
+        tiny = 0.01 * tiny;
+        biglim = bigeps;
+    }
+    int *iused = (int *)malloc(sizeof(int) * numat);
+    char *latoms = (char *)calloc(numat, 1);
+    double *storei = (double *)malloc(sizeof(double) * norbs);
+    double *storej = (double *)malloc(sizeof(double) * norbs);
+    for (int a = 0; a < numat; ++a) iused[a] = -1;
+    double sumb = 0.0;
+    long long nrej = 0;
+    for (long long ij = 0; ij < nij; ++ij) {
+        const int i = ifmo[2 * ij] - 1, j = ifmo[2 * ij + 1] - 1;
+        if (!(fabs(fmo[ij]) >= tiny)) continue;
+        const double c = fmo[ij] * cst;
+        const double d = eigs[j] - eigv[i] - shift;
+        if (!(fabs(c / d) >= biglim)) continue;
+        const int ncfj = ncf[j], ncei = nce[i];
+        const long long jlr = ncocc[j] + 1;  /* 1-based, as the reference */
+        long long jur, jncf;
+        if (j != nocc - 1) { jur = ncocc[j + 1]; jncf = nncf[j + 1]; } else { jur = cocc_dim; jncf = icocc_dim; }
+        jur = jlr + norbs - 1 < jur ? jlr + norbs - 1 : jur;
+        const long long ilr = ncvir[i] + 1;
+        long long iur, incv;
+        if (i != nvir - 1) { iur = ncvir[i + 1]; incv = nnce[i + 1]; } else { iur = cvir_dim; incv = icvir_dim; }
+        iur = ilr + norbs - 1 < iur ? ilr + norbs - 1 : iur;
+        for (long long k = jlr, l = 0; k <= jur; ++k, ++l) storej[l] = cocc[k - 1];
+        for (long long k = ilr, l = 0; k <= iur; ++k, ++l) storei[l] = cvir[k - 1];
+        const double e = copysign(sqrt(4.0 * c * c + d * d), d);
+        double alpha = sqrt(0.5 * (1.0 + d / e));
+        for (;;) {
+            const double beta = -copysign(sqrt(1.0 - alpha * alpha), c);
+            sumb = sumb + fabs(beta);
+            int mlf = 0, rejected = 0;
+            for (int lf = nncf[j]; lf < nncf[j] + ncf[j]; ++lf) {
+                const int ii = icocc[lf] - 1;
+                iused[ii] = mlf;
+                mlf += iorbs[ii];
+            }
+            const long long loopi = ncvir[i], loopj = ncocc[j];
+            long long mle = 0;
+            for (int le = nnce[i]; le < nnce[i] + nce[i] && !rejected; ++le) {
+                const int mie = icvir[le] - 1;
+                latoms[mie] = 1;
+                long long mlff = iused[mie] + loopj;
+                if (iused[mie] >= 0) {
+                    for (long long mlee = mle + 1 + loopi; mlee <= mle + iorbs[mie] + loopi; ++mlee) {
+                        ++mlff;
+                        const double a = cocc[mlff - 1], b = cvir[mlee - 1];
+                        cocc[mlff - 1] = alpha * a + beta * b;
+                        cvir[mlee - 1] = alpha * b - beta * a;
+                    }
+                } else {
+                    double sum = 0.0;
+                    for (long long mlee = mle + 1 + loopi; mlee <= mle + iorbs[mie] + loopi; ++mlee) {
+                        const double t = beta * cvir[mlee - 1];
+                        sum = sum + t * t;
+                    }
+                    if (sum > thresh) {
+                        if (nncf[j] + ncf[j] >= jncf || mlf + iorbs[mie] + loopj > jur) { rejected = 1; break; }
+                        ncf[j] = ncf[j] + 1;
+                        icocc[nncf[j] + ncf[j] - 1] = mie + 1;
+                        iused[mie] = mlf;
+                        mlf += iorbs[mie];
+                        mlff = iused[mie] + loopj;
+                        for (long long mlee = mle + 1 + loopi; mlee <= mle + iorbs[mie] + loopi; ++mlee) {
+                            ++mlff;
+                            cocc[mlff - 1] = beta * cvir[mlee - 1];
+                            cvir[mlee - 1] = alpha * cvir[mlee - 1];
+                        }
+                    }
+                }
+                mle += iorbs[mie];
+            }
+            if (!rejected) {
+                for (int lf = nncf[j]; lf < nncf[j] + ncf[j]; ++lf) {
+                    const int ii = icocc[lf] - 1;
+                    if (latoms[ii]) continue;
+                    double sum = 0.0;
+                    for (long long mlff = iused[ii] + loopj + 1; mlff <= iused[ii] + loopj + iorbs[ii]; ++mlff) {
+                        const double t = beta * cocc[mlff - 1];
+                        sum = sum + t * t;
+                    }
+                    if (sum > thresh) {
+                        if (nnce[i] + nce[i] >= incv || mle + iorbs[ii] + loopi > iur) { rejected = 1; break; }
+                        nce[i] = nce[i] + 1;
+                        icvir[nnce[i] + nce[i] - 1] = ii + 1;
+                        latoms[ii] = 1;
+                        long long mlff = iused[ii] + loopj;
+                        for (long long mlee = mle + 1 + loopi; mlee <= mle + iorbs[ii] + loopi; ++mlee) {
+                            ++mlff;
+                            cvir[mlee - 1] = -beta * cocc[mlff - 1];
+                            cocc[mlff - 1] = alpha * cocc[mlff - 1];
+                        }
+                        mle += iorbs[ii];
+                    }
+                }
+            }
+            if (!rejected) break;
+            /* label 1000 */
+            ++nrej;
+            for (long long k = jlr, l = 0; k <= jur; ++k, ++l) cocc[k - 1] = storej[l];
+            for (long long k = ilr, l = 0; k <= iur; ++k, ++l) cvir[k - 1] = storei[l];
+            ncf[j] = ncfj;
+            nce[i] = ncei;
+            for (int k = 0; k < numat; ++k) { iused[k] = -1; latoms[k] = 0; }
+            if (retry) {
+                alpha = 0.5 * (alpha + 1.0);
+            } else {
+                goto next_ij;
+            }
+        }
+        for (int le = nnce[i]; le < nnce[i] + nce[i]; ++le) latoms[icvir[le] - 1] = 0;
+        for (int lf = nncf[j]; lf < nncf[j] + ncf[j]; ++lf) iused[icocc[lf] - 1] = -1;
+    next_ij:;
+    }
+    nrejct[1] = nrejct[0];
+    nrejct[0] = (int)nrej;
+    *nrej_out = nrej;
+    free(iused); free(latoms); free(storei); free(storej);
+    return sumb;
+}

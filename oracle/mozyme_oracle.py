@@ -186,3 +186,29 @@ def diagg1(iorbs, nijbo, fao, p, occ, vir, idiagg, state, nfmo, ifmo, fmo, cap):
                            cocc, len(nce), nce, nnce, icvir, ncvir, cvir, idiagg, state, nfmo, ifmo, fmo,
                            ctypes.byref(nij), eigv, eigs, ctypes.byref(done))
     return nij.value, eigv, (eigs if done.value else None), sumt
+
+
+def diagg2(iorbs, occ, vir, ifmo, fmo, nij, eigs, eigv, idiagg, ctl, nrejct):
+    """diagg2 (MOZYME/diagg2.F90:16-359).  occ/vir tuples of numpy arrays are
+    modified in place (ncf, icocc, cocc / nce, icvir, cvir); nrejct (int32[2])
+    updated.  Returns (sumb, nrej)."""
+    L = _lib()
+    if not hasattr(L, "_mz_diagg2_bound"):
+        i32p = np.ctypeslib.ndpointer(np.int32, flags="C")
+        f64p = np.ctypeslib.ndpointer(np.float64, flags="C")
+        L.orc_mz_diagg2.argtypes = ([ctypes.c_int, i32p, ctypes.c_int, ctypes.c_int, i32p, i32p, i32p, i32p, f64p,
+                                     ctypes.c_longlong, ctypes.c_longlong, ctypes.c_int, i32p, i32p, i32p, i32p, f64p,
+                                     ctypes.c_longlong, ctypes.c_longlong, i32p, f64p, ctypes.c_longlong, f64p, f64p,
+                                     ctypes.c_int, f64p, i32p, ctypes.POINTER(ctypes.c_longlong)])
+        L.orc_mz_diagg2.restype = ctypes.c_double
+        L._mz_diagg2_bound = True
+    iorbs = np.ascontiguousarray(iorbs, np.int32)
+    ncf, nncf, icocc, ncocc, cocc = occ
+    nce, nnce, icvir, ncvir, cvir = vir
+    nrej = ctypes.c_longlong(0)
+    sumb = L.orc_mz_diagg2(len(iorbs), iorbs, int(iorbs.sum()), len(ncf), ncf, nncf, icocc, ncocc, cocc,
+                           icocc.size, cocc.size, len(nce), nce, nnce, icvir, ncvir, cvir, icvir.size, cvir.size,
+                           np.ascontiguousarray(ifmo, np.int32), np.ascontiguousarray(fmo, np.float64), int(nij),
+                           np.ascontiguousarray(eigs), np.ascontiguousarray(eigv), int(idiagg),
+                           np.ascontiguousarray(ctl, np.float64), nrejct, ctypes.byref(nrej))
+    return sumb, nrej.value

@@ -229,6 +229,78 @@ def test_gpu_diagg1_bit_identical_over_iterations(nwater):
     L.close()
 
 
+def _copy_lmos(t):
+    return tuple(np.array(x, copy=True) for x in t)
+
+
+def test_oracle_diagg2_grows_and_rejects():
+    s, iorbs, nb, mp, occ, vir, p, fao = _diagg_case(32)
+    _, occ = workloads.mozyme_lmos(*workloads.water_box(32)[:2], radius=4.0, seed=3, per_heavy=4, pad_atoms=2)
+    cap = 300 * s.norbs
+    ctl0 = [1.0, 0.0, 1e-13, 0.0, 50 * np.sqrt(1e-39)]
+    for padv in (0, 8):
+        _, vir = workloads.mozyme_lmos(*workloads.water_box(32)[:2], radius=3.2, seed=4, per_heavy=2,
+                                       pad_atoms=padv)
+        st = np.array([10.0, 1.0, 0.0, 0.0])
+        nfmo = np.zeros(len(vir[0]), np.int32)
+        ifmo = np.zeros(2 * cap, np.int32)
+        fmo = np.zeros(cap)
+        nij, eigv, eigs, _ = mo.diagg1(iorbs, nb, fao, p, occ, vir, 0, st, nfmo, ifmo, fmo, cap)
+        o2, v2 = _copy_lmos(occ), _copy_lmos(vir)
+        nrejct = np.zeros(2, np.int32)
+        ctl0[3] = st[3]
+        sumb, nrej = mo.diagg2(iorbs, o2, v2, ifmo, fmo, nij, eigs, eigv, 0, ctl0, nrejct)
+        assert nij > 0 and sumb > 0 and nrejct[0] == nrej
+        if padv == 0:
+            assert nrej > 0                            # no room to grow: rejected
+        else:
+            assert not np.array_equal(o2[4], occ[4])   # rotated
+            assert (v2[0] > vir[0]).any()              # virtual LMOs grew
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("nwater,padv", [(32, 0), (32, 2), (96, 1)])
+def test_gpu_diagg2_bit_identical(nwater, padv):
+    torch = _need_gpu()
+    from mopac_gpu_b200 import mozyme
+    s, iorbs, nb, mp, _, _, p, fao = _diagg_case(nwater)
+    nat, xyz, _ = workloads.water_box(nwater)
+    _, occ = workloads.mozyme_lmos(nat, xyz, radius=4.0, seed=3, per_heavy=4, pad_atoms=2)
+    _, vir = workloads.mozyme_lmos(nat, xyz, radius=3.2, seed=4, per_heavy=2, pad_atoms=padv)
+    cap = 300 * s.norbs
+    c1, c2 = mo.cutoffs(len(iorbs), 9.0)
+    L = mozyme.Layout(iorbs, s.coord, c1, c2)
+    Qo, Qv = mozyme.Lmos(L, occ), mozyme.Lmos(L, vir)
+    D = mozyme.Diagg1(L, Qo, Qv, cap)
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    fd, pd = dev(fao), dev(p)
+    o_ref, v_ref = _copy_lmos(occ), _copy_lmos(vir)
+    st = np.array([10.0, 1.0, 0.0, 0.0])
+    nfmo = np.zeros(len(vir[0]), np.int32)
+    ifmo = np.zeros(2 * cap, np.int32)
+    fmo = np.zeros(cap)
+    nrej_o, nrej_g = np.zeros(2, np.int32), np.zeros(2, np.int32)
+    for idg in (0, 1, 6, 7):
+        nij, eigv, eigs, _ = mo.diagg1(iorbs, nb, fao, p, o_ref, v_ref, idg, st, nfmo, ifmo, fmo, cap)
+        gn, _, _ = D(fd, pd, idg)
+        assert gn == nij
+        ctl = [1.0, 0.0, 1e-13, st[3], 50 * np.sqrt(1e-39)]
+        if eigs is None:
+            eigs = D.eigs.cpu().numpy()
+        sb_o, nr_o = mo.diagg2(iorbs, o_ref, v_ref, ifmo, fmo, nij, eigs, eigv, idg, ctl, nrej_o)
+        sb_g, nr_g = mozyme.diagg2(L, Qo, Qv, D, idg, ctl, nrej_g)
+        Qo.refresh()
+        Qv.refresh()
+        assert nr_g == nr_o and np.array_equal(nrej_g, nrej_o)
+        assert sb_g == pytest.approx(sb_o, rel=1e-13)
+        for ref, q in ((o_ref, Qo), (v_ref, Qv)):
+            n_, ic_, c_ = q.to_host()
+            np.testing.assert_array_equal(n_, ref[0])
+            np.testing.assert_array_equal(ic_, ref[2])
+            np.testing.assert_array_equal(c_, ref[4])
+    L.close()
+
+
 @pytest.mark.gpu
 def test_gpu_mozyme_fock_rejects_short_cutoff():
     torch = _need_gpu()
