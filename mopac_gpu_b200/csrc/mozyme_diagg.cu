@@ -499,7 +499,10 @@ __device__ __forceinline__ int find_atom(const int* ic, int nn, int cnt, const i
 // One thread per rotation of the level.  Whether a rotation is rejected
 // depends only on coefficients it has not yet touched (those of atoms in one
 // LMO only), so a dry run decides it first; modifying and then restoring, as
-// the reference does, leaves the same state as not modifying.
+// the reference does, leaves the same coefficients as not modifying.  The
+// atom numbers it appends before a rejection stay in the LMOs' spare slots
+// in the reference (it restores the counts, not the slots); the dry run
+// writes them too.
 __global__ void mzd2_level(D2Args A) {
   const long long q = A.lo + blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (q >= A.hi) return;
@@ -552,6 +555,7 @@ __global__ void mzd2_level(D2Args A) {
         if (sum > A.thresh) {
           if (nncf[j] + nfj >= jncf || mlf + no + loopj > jur) { rejected = true; break; }
           ++nfj;
+          icocc[nncf[j] + nfj - 1] = mie + 1;  // the reference leaves these in place if it rejects later
           mlf += no;
         }
       }
@@ -572,6 +576,7 @@ __global__ void mzd2_level(D2Args A) {
           if (sum > A.thresh) {
             if (nnce[i] + nfi >= incv || mle + no + loopi > iur) { rejected = true; break; }
             ++nfi;
+            icvir[nnce[i] + nfi - 1] = ii + 1;
             mle += no;
           }
         }
