@@ -22,8 +22,10 @@ Cases (sizes of the benchmark configurations):
                 (no SCF before it: the case to run under a launch-list capture)
   pseudo_diag   Fmo + rotation sweep, n = 3072, k = 2048
   pulay         one Pulay step with a full 10-entry history, n = 3072
-  mz_density, mz_helecz, mz_cnvgz   MOZYME blocks, (H2O)4096, 9 A cutoff,
-                synthetic LMOs over 4 A
+  mz_density, mz_helecz, mz_cnvgz, mz_fock, mz_diagg1, mz_diagg2
+                MOZYME blocks, (H2O)4096, 9 A cutoff, synthetic unit LMOs
+                (occupied over 4 A, virtual over 3.2 A, two spare atom slots),
+                seeded random integrals for the Fock build (timing only)
 """
 from __future__ import annotations
 
@@ -285,6 +287,46 @@ def run_cases(names, reps):
                        setup=lambda: (pn.copy_(p), po.copy_(p * 0.999)))
             out.append(line("mz_cnvgz", ms, 8 * 5 * mp + 8 * 5 * n, "GB/s", "hbm", hbm, src, config=cfg,
                             note="niter = 6: gather + max, one-thread factor, extrapolation, damping, copy"))
+        if "mz_fock" in names:
+            nw = int(lay.s.nw)
+            wv = torch.from_numpy(rng.normal(size=nw) * 0.1).cuda()
+            xyz_d = torch.from_numpy(np.ascontiguousarray(xyz, np.float64)).cuda()
+            fo = torch.empty(mp, dtype=torch.float64, device="cuda")
+            ms = timed(lambda: mozyme.fock(lay, xyz_d, wv, p, h, fo), reps)
+            out.append(line("mz_fock", ms, 8 * nw + 8 * 3 * mp, "GB/s", "hbm", hbm, src, config=cfg,
+                            note=f"stored-pair integrals ({nw} values) read once, P and H read, F written; "
+                                 "every atom also scans all others for the point-charge terms"))
+        if "mz_diagg1" in names or "mz_diagg2" in names:
+            _, occ = workloads.mozyme_lmos(nat, xyz, radius=4.0, seed=3, per_heavy=4, pad_atoms=2)
+            _, vir = workloads.mozyme_lmos(nat, xyz, radius=3.2, seed=4, per_heavy=2, pad_atoms=2)
+            qo, qv = mozyme.Lmos(lay, occ), mozyme.Lmos(lay, vir)
+            pz = mozyme.density(lay, qo, 0)
+            cap = 300 * lay.norbs
+            d1 = mozyme.Diagg1(lay, qo, qv, cap)
+            if "mz_diagg1" in names:
+                ms = timed(lambda: d1(h, pz, 0), max(2, reps // 2))
+                out.append(line("mz_diagg1", ms, 8 * (mp + len(occ[4]) + len(vir[4])), "GB/s", "latency", hbm, src,
+                                config=cfg, list_entries=int(d1.nij),
+                                note="rebuild of the interaction list (idiagg = 0) over all occupied x virtual "
+                                     "pairs; bytes = F once plus the coefficients once"))
+            if "mz_diagg2" in names:
+                d1(h, pz, 0)
+                nrejct = np.zeros(2, np.int32)
+                ctl = [1.0, 0.0, 1e-13, float(d1.state[3]), 50 * np.sqrt(1e-39)]
+                t0 = torch.cuda.Event(enable_timing=True)
+                t1 = torch.cuda.Event(enable_timing=True)
+                flush_l2()
+                t0.record()
+                sb, nrej = mozyme.diagg2(lay, qo, qv, d1, 0, ctl, nrejct)
+                t1.record()
+                torch.cuda.synchronize()
+                ms = t0.elapsed_time(t1)
+                out.append(line("mz_diagg2", ms, 32 * int(d1.nij) * 4 * 20, "GB/s", "latency", hbm, src, config=cfg,
+                                rotations=int(d1.nij), rejected=int(nrej),
+                                note="one pass over the list in dependency levels (host level build included); "
+                                     "bytes: nominal 2 LMOs x 20 atoms x 4 orbitals read+write per rotation"))
+            qo.close()
+            qv.close()
         q.close()
         lay.close()
     if c1 is not None:
@@ -294,7 +336,7 @@ def run_cases(names, reps):
 
 ALL = ["fock2", "helect", "cnvg", "density64", "density_split", "gemm64", "gemm_split", "eigh", "eigh_rand",
        "pseudo_diag",
-       "pulay", "mz_density", "mz_helecz", "mz_cnvgz"]
+       "pulay", "mz_density", "mz_helecz", "mz_cnvgz", "mz_fock", "mz_diagg1", "mz_diagg2"]
 
 
 def main(argv=None):
