@@ -206,6 +206,25 @@ size_t mb_density_split_ws_bytes(int n, int nocc);
 int mb_density_split_ws(int n, int nocc, double occ, const double* c, int ldc, double* p, void* ws,
                         size_t ws_bytes, int* err_dev, cudaStream_t stream);
 
+/* ----------------------------------------------- batched small molecules */
+/* Many closed-shell molecules (n <= 128 basis functions, n * nocc <= 11008)
+ * in one persistent launch, one CTA per molecule SCF at a time (iter with a
+ * full diagonalisation every iteration, SCF/iter.F90:16-1107; Fock and cnvg
+ * bit-identical to the oracle's).  numat[m] atoms of molecule m; nat and
+ * coord (Angstrom, 3 per atom) concatenated over the molecules, host arrays.
+ * Integrals are computed on the GPU at creation. */
+typedef struct mb_batch mb_batch;
+int mb_batch_create(int nmol, const int* numat, const int* nat, const double* coord, mb_batch** out);
+int mb_batch_destroy(mb_batch* batch);
+int mb_batch_nmol(const mb_batch* batch);
+/* Runs every molecule's SCF; per molecule escf (kcal/mol, iter's), niter,
+ * converged (host arrays of nmol, each optional); *t_ms: CUDA-event time of
+ * the launch. */
+int mb_batch_run(mb_batch* batch, const mb_scf_opts* opts, double* escf, int* niter, int* converged,
+                 double* t_ms);
+int mb_batch_get_density(mb_batch* batch, int m, double* p);
+int mb_batch_get_hw(mb_batch* batch, int m, double* h, double* w, double* enuclr);
+
 /* ------------------------------------------------ MOZYME (sparse blocks) */
 /* Pair-block storage of P, H, F (MOZYME/fillij.F90:20-230, first call,
  * molecular): for atom i in order, partners j < i with r^2 < cutof2 (block

@@ -96,6 +96,12 @@ SIGNATURES = {
     "mb_pulay_ws_bytes": ([_I], ctypes.c_size_t),
     "mb_pulay_ws": ([_I, _P, _P, _P, _P, _I, _P, _I, _P, _P, _P, _P, _P, _P], _I),
     "mb_osinv": ([_P, _I], _D),
+    "mb_batch_create": ([_I, _P, _P, _P, ctypes.POINTER(_P)], _I),
+    "mb_batch_destroy": ([_P], _I),
+    "mb_batch_nmol": ([_P], _I),
+    "mb_batch_run": ([_P, ctypes.POINTER(ScfOpts), _P, _P, _P, ctypes.POINTER(_D)], _I),
+    "mb_batch_get_density": ([_P, _I, _P], _I),
+    "mb_batch_get_hw": ([_P, _I, _P, _P, ctypes.POINTER(_D)], _I),
     "mb_mz_layout_create": ([_I, _P, _P, _D, _D, ctypes.POINTER(MbMzLayout), _P], _I),
     "mb_mz_layout_destroy": ([ctypes.POINTER(MbMzLayout)], _I),
     "mb_mz_idiag": ([ctypes.POINTER(MbMzLayout), _P], _I),

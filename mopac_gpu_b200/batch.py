@@ -1,0 +1,58 @@
+"""Batched SCF over many small molecules (one persistent launch).
+
+``Batch(molecules)`` takes a list of (atomic numbers, coordinates) pairs,
+computes every molecule's integrals on the GPU, and ``run()`` performs every
+molecule's SCF (iter, SCF/iter.F90, full diagonalisation each iteration) in
+one launch; it returns the heats of formation as iter computes them.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from ._lib import ScfOpts, check, lib
+
+
+class Batch:
+    def __init__(self, molecules):
+        nats = [np.asarray(m[0], np.int32) for m in molecules]
+        xyzs = [np.asarray(m[1], np.float64).reshape(-1, 3) for m in molecules]
+        self.nmol = len(nats)
+        self.numat = np.array([len(n) for n in nats], np.int32)
+        nat = np.ascontiguousarray(np.concatenate(nats), np.int32)
+        xyz = np.ascontiguousarray(np.concatenate(xyzs), np.float64)
+        self._h = ctypes.c_void_p()
+        check(lib().mb_batch_create(self.nmol, self.numat.ctypes.data, nat.ctypes.data, xyz.ctypes.data,
+                                    ctypes.byref(self._h)))
+        self.norbs = [int(np.where(n == 1, 1, 4).sum()) for n in nats]
+
+    def run(self, scfcrt: float = 1.0e-4, itrmax: int = 2000):
+        o = ScfOpts()
+        lib().mb_scf_opts_default(ctypes.byref(o))
+        o.scfcrt = scfcrt
+        o.itrmax = itrmax
+        escf = np.zeros(self.nmol)
+        niter = np.zeros(self.nmol, np.int32)
+        conv = np.zeros(self.nmol, np.int32)
+        t = ctypes.c_double()
+        check(lib().mb_batch_run(self._h, ctypes.byref(o), escf.ctypes.data, niter.ctypes.data, conv.ctypes.data,
+                                 ctypes.byref(t)))
+        return escf, niter, conv.astype(bool), t.value
+
+    def density(self, m: int) -> np.ndarray:
+        n = self.norbs[m]
+        p = np.empty(n * (n + 1) // 2)
+        check(lib().mb_batch_get_density(self._h, int(m), p.ctypes.data))
+        return p
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            lib().mb_batch_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
