@@ -223,6 +223,11 @@ int mb_batch_nmol(const mb_batch* batch);
 int mb_batch_run(mb_batch* batch, const mb_scf_opts* opts, double* escf, int* niter, int* converged,
                  double* t_ms);
 int mb_batch_get_density(mb_batch* batch, int m, double* p);
+/* Phase timing (off by default): SM cycles summed over all CTAs of the last
+ * run, out[8] = Fock, energy and control, Householder, bisection, inverse
+ * iteration, back-transformation, density, cnvg. */
+int mb_batch_set_phase_timing(mb_batch* batch, int on);
+int mb_batch_phase_cycles(mb_batch* batch, unsigned long long* out);
 int mb_batch_get_hw(mb_batch* batch, int m, double* h, double* w, double* enuclr);
 
 /* ------------------------------------------------ MOZYME (sparse blocks) */

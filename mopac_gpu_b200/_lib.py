@@ -101,6 +101,8 @@ SIGNATURES = {
     "mb_batch_nmol": ([_P], _I),
     "mb_batch_run": ([_P, ctypes.POINTER(ScfOpts), _P, _P, _P, ctypes.POINTER(_D)], _I),
     "mb_batch_get_density": ([_P, _I, _P], _I),
+    "mb_batch_set_phase_timing": ([_P, _I], _I),
+    "mb_batch_phase_cycles": ([_P, _P], _I),
     "mb_batch_get_hw": ([_P, _I, _P, _P, ctypes.POINTER(_D)], _I),
     "mb_mz_layout_create": ([_I, _P, _P, _D, _D, ctypes.POINTER(MbMzLayout), _P], _I),
     "mb_mz_layout_destroy": ([ctypes.POINTER(MbMzLayout)], _I),

@@ -40,6 +40,18 @@ class Batch:
                                  ctypes.byref(t)))
         return escf, niter, conv.astype(bool), t.value
 
+    PHASES = ("fock", "energy", "householder", "bisection", "inverse_iteration", "back_transform", "density",
+              "cnvg")
+
+    def set_phase_timing(self, on: bool = True):
+        check(lib().mb_batch_set_phase_timing(self._h, int(on)))
+
+    def phase_cycles(self) -> dict:
+        """SM cycles per phase summed over all CTAs of the last run."""
+        out = np.zeros(len(self.PHASES), np.uint64)
+        check(lib().mb_batch_phase_cycles(self._h, out.ctypes.data))
+        return dict(zip(self.PHASES, out.tolist()))
+
     def density(self, m: int) -> np.ndarray:
         n = self.norbs[m]
         p = np.empty(n * (n + 1) // 2)

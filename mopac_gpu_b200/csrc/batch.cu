@@ -8,18 +8,22 @@
 // exit diagonalisation.  Every thread computes the control scalars from the
 // same CTA-wide values (so they agree bit for bit); the CTA runs the phases
 // between barriers:
-//   * Fock: thread per atom folds its diagonal block's contributions in the
-//     reference order (pairs with lower atoms, its one-centre terms, pairs
-//     with higher atoms) and writes the exchange blocks of its lower pairs --
-//     the operation order of fock2/fock1, so F is bit-identical to the oracle;
-//   * eigensolve of the packed F in shared memory: Householder reduction to
-//     tridiagonal form, eigenvalues 0..nocc by 5-section Sturm counts (four
-//     lanes per eigenvalue), occupied eigenvectors of T by inverse iteration
-//     (thread per vector, clusters re-orthogonalised), back-transformation;
+//   * Fock: P staged in shared memory; a thread per diagonal-block element
+//     folds that element's contributions in the reference order (pairs with
+//     lower atoms, the one-centre terms, pairs with higher atoms) and a thread
+//     per off-diagonal element forms its exchange sum -- the operation order
+//     of fock2/fock1, so F is bit-identical to the oracle;
+//   * eigensolve in shared memory: Householder reduction to tridiagonal form
+//     (warp per row, two barriers per column), eigenvalues through the LUMO
+//     by 5-section Sturm counts (four lanes per eigenvalue), the occupied
+//     eigenvectors of T by inverse iteration (thread per vector, clusters
+//     re-orthogonalised), back-transformation (a lane group per vector);
 //   * density P = 2 Z Z^T over the occupied vectors; cnvg with its diagonal
 //     statistics in the reference's order (bit-identical).
-// Matrices live in shared memory (packed F, the n x nocc vectors) and in a
-// CTA-private global scratch (the packed F, P, PA, P_old, the LU factors).
+// Shared memory holds the packed matrix (P, then F, then the n x nocc
+// eigenvectors when they fit) and the tridiagonal; 77 KB, two CTAs per SM.
+// Each molecule's F, P, P_old live in global memory; each CTA has a global
+// scratch for the LU factors, the reflectors and oversized eigenvectors.
 #include <math.h>
 #include <string.h>
 
@@ -36,9 +40,18 @@ extern "C" int mb_hcore_finish(int numat, const MbAtomsDev* at, const int* nat_d
 
 namespace {
 
-constexpr int BT_T = 256;         // threads per CTA
-constexpr int BT_NMAX = 128;      // basis functions per molecule
-constexpr int BT_ZMAX = 11008;    // n * nocc doubles in shared memory
+constexpr int BT_T = 256;                                 // threads per CTA
+constexpr int BT_W = BT_T / 32;                           // warps per CTA
+constexpr int BT_NMAX = 128;                              // basis functions per molecule
+constexpr int BT_AMAX = BT_NMAX * (BT_NMAX + 1) / 2;      // packed lower triangle
+constexpr int BT_ZMAX = 11008;                            // n * nocc
+constexpr int BT_IMAX = 320;                              // diagonal-block elements, <= 2.5 n
+constexpr long long BT_LU = 5LL * BT_ZMAX;                // LU factors of T - lambda I, 5 n per vector
+constexpr long long BT_SCR = BT_LU + BT_AMAX + BT_ZMAX;   // + reflectors + oversized Z: doubles per CTA
+constexpr int BT_NB = 8;                                  // reflectors per back-transformation block
+constexpr int BT_TW = ((BT_NMAX - 2 + BT_NB - 1) / BT_NB) * BT_NB * BT_NB;  // T of every block
+constexpr int BT_PHASES = 8;
+static_assert(BT_T == 256, "the reduction tile is 16 x 16 threads");  // fock, energy, householder, bisection, inverse iteration, back-transform, density, cnvg
 
 struct Mol {
   int n, nclose, numat, aoff;  // aoff: first atom in the concatenated atom tables
@@ -56,15 +69,13 @@ struct BatchArgs {
   const double* h;
   const double* w;
   const long long* wrow;     // molecule-local W offsets of each atom's first pair block
-  const int* lim;
   const int* cum;
   const double* pdiag;
   double* f;
   double* p;
-  double* pa;
   double* pold;
   double* pold2;
-  double* scratch;           // per CTA: 3 * BT_NMAX * BT_NMAX doubles (LU factors)
+  double* scratch;           // per CTA: BT_SCR doubles (LU factors, reflectors, Z when it is too big)
   double* escf;
   double* ee;
   int* niter;
@@ -72,178 +83,251 @@ struct BatchArgs {
   double* homo;
   double* lumo;
   int* next;
-  int* status;
+  unsigned long long* phase;  // optional: SM cycles per phase, summed over CTAs
   int itrmax;
   double scfcrt;
 };
 
 __device__ __forceinline__ long long tri(long long r, long long c) { return r * (r + 1) / 2 + c; }
 __device__ __forceinline__ int indx1(int i, int j) { if (i < j) { int t = i; i = j; j = t; } return (i * (i - 1)) / 2 + j; }
+// (row, column) of packed lower-triangle index q < 2^24
+__device__ __forceinline__ void tri_rc(int q, int& r, int& c) {
+  r = (int)((sqrtf(8.0f * (float)q + 1.0f) - 1.0f) * 0.5f);
+  while (r * (r + 1) / 2 > q) --r;
+  while ((r + 1) * (r + 2) / 2 <= q) ++r;
+  c = q - r * (r + 1) / 2;
+}
 
 __constant__ int c_bpidx[16] = {1, 2, 4, 7, 2, 3, 5, 8, 4, 5, 6, 9, 7, 8, 9, 10};
 
-// ------------------------------------------------------------ Fock (one atom)
-// F(a's diagonal block) and the exchange blocks of pairs (a, b < a), in the
-// operation order of fock2 (SCF/fock2.F90:149-298) and fock1 (SCF/fock1.F90).
-__device__ void fock_atom(const BatchArgs& B, const Mol& M, int a, const double* __restrict__ ptot,
-                          const double* __restrict__ p, double* __restrict__ f) {
-  const int* first = B.first + M.aoff;
-  const int* nor = B.nor + M.aoff;
-  const long long* wrow = B.wrow + M.aoff;
-  const int* lim = B.lim + M.aoff;
-  const int* cum = B.cum + M.aoff;
-  const double* w = B.w + M.woff;
-  const int ia = first[a] + 1, ib = first[a] + nor[a];  // 1-based orbitals
-  const int na = nor[a];
-  const int nd = na * (na + 1) / 2;
-  double acc[10];
-  for (int t = 0; t < nd; ++t) {
-    int r = 0;
-    while ((r + 1) * (r + 2) / 2 <= t) ++r;
-    const int c = t - r * (r + 1) / 2;
-    acc[t] = f[tri(ia - 1 + r, ia - 1 + c)];
-  }
-  auto pairw = [&](int hi, int lo) { return w + wrow[hi] + (long long)lim[hi] * cum[lo]; };
-  auto pk = [&](int r1, int c1) -> double {  // packed element, 1-based orbitals
-    const int mx = r1 > c1 ? r1 : c1, mn = r1 < c1 ? r1 : c1;
-    return ptot[tri(mx - 1, mn - 1)];
-  };
-  // contribution of pair (hi, lo) to atom a's diagonal block
-  auto pair_terms = [&](int hi, int lo) {
-    const double* wk = pairw(hi, lo);
-    const int ha = first[hi] + 1, hb = first[hi] + nor[hi];
-    const int la = first[lo] + 1, lb = first[lo] + nor[lo];
-    if (hb - ha >= 3 && lb - la >= 3) {
-      // jab: hi's block gets sumb (from lo's density), lo's block gets suma
-      const int oa = (a == hi) ? la : ha;  // the other atom's first orbital
-      for (int q = 0; q < 10; ++q) {
-        double s;
-        if (a == hi) {
-          s = DMUL(pk(oa + 0, oa + 0), wk[q * 10 + c_bpidx[0] - 1]);
-          for (int m = 1; m < 16; ++m) s = DADD(s, DMUL(pk(oa + m / 4, oa + m % 4), wk[q * 10 + c_bpidx[m] - 1]));
-        } else {
-          s = DMUL(pk(oa + 0, oa + 0), wk[(c_bpidx[0] - 1) * 10 + q]);
-          for (int m = 1; m < 16; ++m) s = DADD(s, DMUL(pk(oa + m / 4, oa + m % 4), wk[(c_bpidx[m] - 1) * 10 + q]));
-        }
-        acc[q] = DADD(acc[q], s);
-      }
-    } else if (hb - ha >= 3 && la == lb) {  // hi heavy, lo light
-      const double pl = ptot[tri(la - 1, la - 1)];
-      if (a == hi) {
-        int k = 0;
-        for (int i = 0; i <= 3; ++i) {
-          for (int j = 1; j <= i; ++j) {
-            acc[i * (i + 1) / 2 + j - 1] = DADD(acc[i * (i + 1) / 2 + j - 1], DMUL(pl, wk[j + k - 1]));
-          }
-          if (i > 0) k += i;
-          k += 1;
-          acc[i * (i + 1) / 2 + i] = DADD(acc[i * (i + 1) / 2 + i], DMUL(pl, wk[k - 1]));
-        }
-      } else {
-        double sumdia = 0.0, sumoff = 0.0;
-        int k = 0;
-        for (int i = 0; i <= 3; ++i) {
-          for (int j = 1; j <= i; ++j) sumoff = DADD(sumoff, DMUL(pk(ha + i, ha + j - 1), wk[j + k - 1]));
-          if (i > 0) k += i;
-          k += 1;
-          sumdia = DADD(sumdia, DMUL(pk(ha + i, ha + i), wk[k - 1]));
-        }
-        acc[0] = DADD(DADD(acc[0], DMUL(sumoff, 2.0)), sumdia);
-      }
-    } else if (lb - la >= 3 && ha == hb) {  // hi light, lo heavy
-      const double ph = ptot[tri(ha - 1, ha - 1)];
-      if (a == lo) {
-        int k = 0;
-        for (int i = 0; i <= 3; ++i) {
-          for (int j = 1; j <= i; ++j) acc[i * (i + 1) / 2 + j - 1] = DADD(acc[i * (i + 1) / 2 + j - 1], DMUL(ph, wk[j + k - 1]));
-          if (i > 0) k += i;
-          k += 1;
-          acc[i * (i + 1) / 2 + i] = DADD(acc[i * (i + 1) / 2 + i], DMUL(ph, wk[k - 1]));
-        }
-      } else {
-        double sumdia = 0.0, sumoff = 0.0;
-        int k = 0;
-        for (int i = 0; i <= 3; ++i) {
-          for (int j = 1; j <= i; ++j) sumoff = DADD(sumoff, DMUL(pk(la + i, la + j - 1), wk[j + k - 1]));
-          if (i > 0) k += i;
-          k += 1;
-          sumdia = DADD(sumdia, DMUL(pk(la + i, la + i), wk[k - 1]));
-        }
-        acc[0] = DADD(DADD(acc[0], DMUL(sumoff, 2.0)), sumdia);
-      }
-    } else {  // light-light
-      const double po = (a == hi) ? ptot[tri(la - 1, la - 1)] : ptot[tri(ha - 1, ha - 1)];
-      acc[0] = DADD(acc[0], DMUL(po, wk[0]));
-    }
-  };
-  for (int b = 0; b < a; ++b) pair_terms(a, b);
-  // fock1: one-centre terms of atom a
-  {
-    const int il = nd;
-    const double* wo = w + wrow[a] + (long long)lim[a] * cum[a];
-    for (int i = ia; i <= ib; ++i) {
-      const int iw = i - ia + 1;
-      for (int j = ia; j <= i; ++j) {
-        const int jw = j - ia + 1;
-        const int ijw = (iw * (iw - 1)) / 2 + jw;
-        double sum = 0.0;
-        for (int k = ia; k <= ib; ++k) {
-          const int kw = k - ia + 1;
-          for (int l = ia; l <= ib; ++l) {
-            const int lw = l - ia + 1;
-            const int klw = indx1(kw, lw), ikw = indx1(kw, jw), jlw = indx1(lw, iw);
-            const double pt = pk(k, l), ps = p[tri((k > l ? k : l) - 1, (k < l ? k : l) - 1)];
-            sum = DSUB(DADD(sum, DMUL(pt, wo[(ijw - 1) + il * (klw - 1)])), DMUL(ps, wo[(ikw - 1) + il * (jlw - 1)]));
-          }
-        }
-        acc[ijw - 1] = DADD(acc[ijw - 1], sum);
-      }
-    }
-  }
-  for (int b = a + 1; b < M.numat; ++b) pair_terms(b, a);
-  for (int t = 0; t < nd; ++t) {
-    int r = 0;
-    while ((r + 1) * (r + 2) / 2 <= t) ++r;
-    const int c = t - r * (r + 1) / 2;
-    f[tri(ia - 1 + r, ia - 1 + c)] = acc[t];
-  }
-  // exchange blocks of the pairs (a, b < a): one subtraction per element
-  for (int b = 0; b < a; ++b) {
-    const double* wk = pairw(a, b);
-    const int ja = first[b] + 1, jb = first[b] + nor[b];
-    if (ib - ia >= 3 && jb - ja >= 3) {
-      for (int mu = 1; mu <= 4; ++mu)
-        for (int nu = 1; nu <= 4; ++nu) {
-          double s = 0.0;
-          bool firstt = true;
-          for (int lam = 1; lam <= 4; ++lam)
-            for (int sig = 1; sig <= 4; ++sig) {
-              const double t = DMUL(p[tri(ia + lam - 2, ja + sig - 2)], wk[(indx1(mu, lam) - 1) * 10 + indx1(nu, sig) - 1]);
-              if (firstt) { s = t; firstt = false; } else s = DADD(s, t);
-            }
-          const long long idx = tri(ia + mu - 2, ja + nu - 2);
-          f[idx] = DSUB(f[idx], s);
-        }
-    } else if (ib - ia >= 3 && ja == jb) {
-      for (int i = ia; i <= ib; ++i) {
-        double sum = 0.0;
-        for (int j = 1; j <= ib - ia + 1; ++j) sum = DADD(sum, DMUL(p[tri(j - 1 + ia - 1, ja - 1)], wk[indx1(i - ia + 1, j) - 1]));
-        const long long idx = tri(i - 1, ja - 1);
-        f[idx] = DSUB(f[idx], sum);
-      }
-    } else if (jb - ja >= 3 && ia == ib) {
-      for (int i = 0; i < 4; ++i) {
-        double sum = 0.0;
-        for (int l = 1; l <= 4; ++l) sum = DADD(sum, DMUL(p[tri(ia - 1, ja - 1) + l - 1], wk[indx1(i + 1, l) - 1]));
-        const long long idx = tri(ia - 1, ja - 1) + i;
-        f[idx] = DSUB(f[idx], sum);
-      }
-    } else {
-      const long long ij = tri(ia - 1, ja - 1);
-      f[ij] = DSUB(f[ij], DMUL(p[ij], wk[0]));
-    }
+// 1/q: hardware estimate and two Newton steps (relative error a few ulps);
+// used where an eigenvalue search or inverse iteration divides, both of which
+// tolerate that.
+__device__ __forceinline__ double recip_nr2(double q) {
+  double r;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(q));
+  double e = fma(-q, r, 1.0);
+  r = fma(r, e, r);
+  e = fma(-q, r, 1.0);
+  return fma(r, e, r);
+}
+
+__device__ __forceinline__ double warp_sum(double x) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+  return x;
+}
+
+// Phase clock (thread 0): charges the cycles since the last mark to phase i.
+// ph[BT_PHASES] holds the last mark; ph == nullptr when phase timing is off.
+__device__ __forceinline__ void ph_mark(long long* ph, int i) {
+  if (ph && threadIdx.x == 0) {
+    const long long now = clock64();
+    ph[i] += now - ph[BT_PHASES];
+    ph[BT_PHASES] = now;
   }
 }
+
+struct Smem {
+  double* A;      // packed lower (BT_AMAX): P during the Fock build, the matrix during the reduction, Z after it
+  double* Z;      // n x nz eigenvectors, Z[i * nz + m]: the A region when n * nz fits, else global scratch
+  double* d;
+  double* e;
+  double* e2;
+  double* tau;
+  double* pv;
+  double* v;
+  double* eig;    // eigenvalues 0 .. LUMO
+  double* red;    // two sets of BT_W warp partials
+  double* scal;
+  double* tw;     // the back-transformation blocks' T
+  int* afirst;    // the molecule's atom tables
+  int* anor;
+  int* acum;
+  int* orb_atom;  // atom of each orbital
+  int* item;      // diagonal-block elements: atom << 4 | element
+  long long* awrow;
+};
+
+// Sum over the CTA, the same value in every thread: butterfly within each
+// warp (commutative pairs, so every lane holds the same bits), then the warp
+// sums in a fixed order.
+__device__ double block_sum_all(double x, double* red) {
+  x = warp_sum(x);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = x;
+  __syncthreads();
+  double r = red[0];
+#pragma unroll
+  for (int q = 1; q < BT_W; ++q) r += red[q];
+  __syncthreads();
+  return r;
+}
+
+// ------------------------------------------------------------------- Fock
+// F = H (+ the level-shift start) + G(P), P staged in S.A, PA = cpa * P
+// exactly (the reference's PA is P/2 after every density and w1 * P for the
+// diagonal guess).  Every element is written once, in the operation order of
+// fock2 (SCF/fock2.F90:149-298) and fock1 (SCF/fock1.F90):
+//   * a diagonal-block element of atom a folds the Coulomb terms of the
+//     pairs (a, b < a) in b order, a's one-centre terms, then the pairs
+//     (b > a, a) in b order;
+//   * an element of the block of atoms a > b is its start value minus the
+//     exchange sum over a's and b's orbitals.
+
+__device__ __forceinline__ double f_start(const double* __restrict__ h, long long idx, bool diag, double ptot,
+                                          double cpa, double shift, bool use_shift) {
+  if (!use_shift) return h[idx];
+  double v = DADD(DADD(h[idx], DMUL(shift, DMUL(ptot, cpa))), DMUL((double)(idx + 1), 1.0e-16));
+  if (diag) v = DSUB(v, shift);
+  return v;
+}
+
+__device__ __forceinline__ double pk(const double* P, int r, int c) {  // 0-based orbitals
+  return r >= c ? P[tri(r, c)] : P[tri(c, r)];
+}
+
+// Coulomb contribution of pair (hi > lo) to element q of atom a's block.
+__device__ __forceinline__ double pair_q(const Smem& S, const double* __restrict__ w, int hi, int lo, int a, int q,
+                                         double acc) {
+  const double* P = S.A;
+  const int nh = S.anor[hi], nl = S.anor[lo];
+  const double* wk = w + S.awrow[hi] + (long long)(nh == 1 ? 1 : 10) * S.acum[lo];
+  const int fh = S.afirst[hi], fl = S.afirst[lo];
+  if (nh == 4 && nl == 4) {
+    const int o = (a == hi) ? fl : fh;
+    double s;
+    if (a == hi) {
+      s = DMUL(pk(P, o, o), wk[q * 10 + c_bpidx[0] - 1]);
+#pragma unroll
+      for (int m = 1; m < 16; ++m) s = DADD(s, DMUL(pk(P, o + m / 4, o + m % 4), wk[q * 10 + c_bpidx[m] - 1]));
+    } else {
+      s = DMUL(pk(P, o, o), wk[(c_bpidx[0] - 1) * 10 + q]);
+#pragma unroll
+      for (int m = 1; m < 16; ++m) s = DADD(s, DMUL(pk(P, o + m / 4, o + m % 4), wk[(c_bpidx[m] - 1) * 10 + q]));
+    }
+    return DADD(acc, s);
+  }
+  if (nh != nl) {  // one heavy atom (four orbitals), one hydrogen
+    const int fheavy = nh == 4 ? fh : fl, flight = nh == 4 ? fl : fh;
+    const bool a_heavy = (a == hi) == (nh == 4);
+    if (a_heavy) return DADD(acc, DMUL(P[tri(flight, flight)], wk[q]));
+    double sumdia = 0.0, sumoff = 0.0;
+#pragma unroll
+    for (int i = 0; i <= 3; ++i) {
+#pragma unroll
+      for (int j = 0; j < i; ++j) sumoff = DADD(sumoff, DMUL(P[tri(fheavy + i, fheavy + j)], wk[i * (i + 1) / 2 + j]));
+      sumdia = DADD(sumdia, DMUL(P[tri(fheavy + i, fheavy + i)], wk[i * (i + 1) / 2 + i]));
+    }
+    return DADD(DADD(acc, DMUL(sumoff, 2.0)), sumdia);
+  }
+  const int o = (a == hi) ? fl : fh;  // two hydrogens
+  return DADD(acc, DMUL(P[tri(o, o)], wk[0]));
+}
+
+// Final value of element q of atom a's diagonal block.
+__device__ double fock_item(const Smem& S, const Mol& M, const double* __restrict__ w, const double* __restrict__ h,
+                            int a, int q, double cpa, double shift, bool use_shift) {
+  const double* P = S.A;
+  const int fa = S.afirst[a], na = S.anor[a];
+  int r, c;
+  tri_rc(q, r, c);
+  const long long idx = tri(fa + r, fa + c);
+  double acc = f_start(h, idx, r == c, P[idx], cpa, shift, use_shift);
+  for (int b = 0; b < a; ++b) acc = pair_q(S, w, a, b, a, q, acc);
+  {  // fock1: one-centre terms
+    const int il = na == 1 ? 1 : 10;
+    const double* wo = w + S.awrow[a] + (long long)il * S.acum[a];
+    const int iw = r + 1, jw = c + 1, ijw = q + 1;
+    double sum = 0.0;
+    for (int k = 1; k <= na; ++k)
+      for (int l = 1; l <= na; ++l) {
+        const int klw = indx1(k, l), ikw = indx1(k, jw), jlw = indx1(l, iw);
+        const double pt = pk(P, fa + k - 1, fa + l - 1);
+        sum = DSUB(DADD(sum, DMUL(pt, wo[(ijw - 1) + il * (klw - 1)])), DMUL(DMUL(pt, cpa), wo[(ikw - 1) + il * (jlw - 1)]));
+      }
+    acc = DADD(acc, sum);
+  }
+  for (int b = a + 1; b < M.numat; ++b) acc = pair_q(S, w, b, a, a, q, acc);
+  return acc;
+}
+
+// Final value of element (r, c) of the block of atoms a > b.
+__device__ double fock_exchange(const Smem& S, const double* __restrict__ w, const double* __restrict__ h, int r,
+                                int c, int a, int b, double cpa, double shift, bool use_shift) {
+  const double* P = S.A;
+  const long long idx = tri(r, c);
+  const int na = S.anor[a], nb = S.anor[b], fa = S.afirst[a], fb = S.afirst[b];
+  const double* wk = w + S.awrow[a] + (long long)(na == 1 ? 1 : 10) * S.acum[b];
+  const int mu = r - fa, nu = c - fb;
+  double s;
+  if (na == 4 && nb == 4) {
+    s = 0.0;
+#pragma unroll
+    for (int lam = 0; lam < 4; ++lam)
+#pragma unroll
+      for (int sig = 0; sig < 4; ++sig) {
+        const double t = DMUL(DMUL(P[tri(fa + lam, fb + sig)], cpa),
+                              wk[(indx1(mu + 1, lam + 1) - 1) * 10 + indx1(nu + 1, sig + 1) - 1]);
+        s = (lam == 0 && sig == 0) ? t : DADD(s, t);
+      }
+  } else if (na == 4) {
+    s = 0.0;
+#pragma unroll
+    for (int j = 1; j <= 4; ++j) s = DADD(s, DMUL(DMUL(P[tri(fa + j - 1, fb)], cpa), wk[indx1(mu + 1, j) - 1]));
+  } else if (nb == 4) {
+    s = 0.0;
+#pragma unroll
+    for (int l = 1; l <= 4; ++l) s = DADD(s, DMUL(DMUL(P[tri(fa, fb) + l - 1], cpa), wk[indx1(nu + 1, l) - 1]));
+  } else {
+    s = DMUL(DMUL(P[idx], cpa), wk[0]);
+  }
+  return DSUB(f_start(h, idx, false, P[idx], cpa, shift, use_shift), s);
+}
+
+__device__ void cta_fock(const BatchArgs& B, const Mol& M, const Smem& S, int nitems, double cpa, double shift,
+                         bool use_shift, double* __restrict__ f, const double* __restrict__ p,
+                         const double* __restrict__ h) {
+  const int mp = M.n * (M.n + 1) / 2;
+  for (int q = threadIdx.x; q < mp; q += BT_T) S.A[q] = p[q];
+  __syncthreads();
+  const double* w = B.w + M.woff;
+  // the diagonal-block elements (the long folds) first, then the exchange elements
+  for (int u = threadIdx.x; u < nitems + mp; u += BT_T) {
+    if (u < nitems) {
+      const int it = S.item[u], a = it >> 4, q = it & 15;
+      const double v = fock_item(S, M, w, h, a, q, cpa, shift, use_shift);
+      int r, c;
+      tri_rc(q, r, c);
+      f[tri(S.afirst[a] + r, S.afirst[a] + c)] = v;
+    } else {
+      int r, c;
+      tri_rc(u - nitems, r, c);
+      const int a = S.orb_atom[r], b = S.orb_atom[c];
+      if (a != b) f[tri(r, c)] = fock_exchange(S, w, h, r, c, a, b, cpa, shift, use_shift);
+    }
+  }
+  __syncthreads();
+}
+
+// helect: sum_{i>j} pa (h + f) + 0.5 sum_i pa_ii (h_ii + f_ii), pa = cpa * p.
+__device__ double cta_helect(int n, const double* p, double cpa, const double* h, const double* f, double* red) {
+  double s = 0.0, dsum = 0.0;
+  for (int r = threadIdx.x; r < n; r += BT_T) {
+    const long long base = (long long)r * (r + 1) / 2;
+    double a = 0.0;
+    for (int c = 0; c < r; ++c) a += DMUL(p[base + c], cpa) * (h[base + c] + f[base + c]);
+    s += a;
+    dsum += DMUL(p[base + r], cpa) * (h[base + r] + f[base + r]);
+  }
+  const double a = block_sum_all(s, red);
+  const double b = block_sum_all(dsum, red);
+  return a + 0.5 * b;
+}
+
+// ------------------------------------------------------------ eigensolver
+// Eigenvalues 0 .. max(nz, 1) of the packed symmetric matrix in S.A (lost)
+// and, when vectors, the eigenvectors of the lowest nz in S.Z.  scr: the
+// CTA's global scratch (LU factors, then the reflectors when Z overlays A).
 
 // Sturm count of T - x I (d, e2 = e^2).
 __device__ int sturm(int n, const double* d, const double* e2, double x, double pivmin) {
@@ -252,119 +336,152 @@ __device__ int sturm(int n, const double* d, const double* e2, double x, double 
   if (fabs(q) < pivmin) q = -pivmin;
   cnt += q < 0.0;
   for (int i = 1; i < n; ++i) {
-    q = d[i] - x - e2[i - 1] / q;
+    q = d[i] - x - e2[i - 1] * recip_nr2(q);
     if (fabs(q) < pivmin) q = -pivmin;
     cnt += q < 0.0;
   }
   return cnt;
 }
 
-struct Smem {
-  double* A;     // packed lower, n(n+1)/2
-  double* Z;     // n x nz, Z[i * nz + m]
-  double* d;
-  double* e;
-  double* e2;
-  double* tau;
-  double* pv;    // p / w vector
-  double* v;     // current Householder vector (full length n)
-  double* eig;   // eigenvalues 0 .. nz
-  double* red;   // reduction scratch (BT_T)
-  double* scal;  // scalars
-};
-
-// Sum over the CTA, the same value in every thread: butterfly within each
-// warp (commutative pairs, so every lane holds the same bits), then the warp
-// sums in a fixed order.
-__device__ double block_sum_all(double x, double* red) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = x;
-  __syncthreads();
-  double r = red[0];
-#pragma unroll
-  for (int q = 1; q < BT_T / 32; ++q) r += red[q];
-  __syncthreads();
-  return r;
-}
-
-// Eigenvalues 0..nz of the packed symmetric matrix in S.A (destroyed) and the
-// eigenvectors of the lowest nz (in S.Z), using U (3 * n * nz doubles,
-// global) for the LU factors.
-__device__ void cta_eigh(int n, int nz, Smem& S, double* U) {
-  const int tid = threadIdx.x;
-  // ---- Householder reduction (lower, column k below the diagonal)
-  for (int k = 0; k < n - 2; ++k) {
+// reltol: relative width at which an eigenvalue's bracket stops shrinking.
+__device__ void cta_eigh(int n, int nz, bool vectors, double reltol, Smem& S, double* scr, long long* ph) {
+  const int tid = threadIdx.x, lane = tid & 31, wp = tid >> 5, tr = tid >> 4, tc = tid & 15;
+  double* A = S.A;
+  double* redA = S.red;
+  double* redB = S.red + BT_W;
+  // ---- Householder reduction to tridiagonal form, lower, two barriers per
+  // column: the reflector's norm comes from the previous column's update.
+  // The 16 x 16 tile covers n - 1 <= 127 rows and columns in 8 steps.
+  {
     double part = 0.0;
-    for (int i = k + 2 + tid; i < n; i += BT_T) {
-      const double x = S.A[tri(i, k)];
-      part += x * x;
+    for (int i = 2 + tid; i < n; i += BT_T) part += A[tri(i, 0)] * A[tri(i, 0)];
+    part = warp_sum(part);
+    if (lane == 0) redA[wp] = part;
+    __syncthreads();
+  }
+  for (int k = 0; k < n - 2; ++k) {
+    double sigma = redA[0];
+#pragma unroll
+    for (int q = 1; q < BT_W; ++q) sigma += redA[q];
+    const double alpha = A[tri(k + 1, k)];
+    double beta, tau, scal;
+    if (sigma == 0.0) { beta = alpha; tau = 0.0; scal = 0.0; }
+    else {
+      beta = -copysign(sqrt(alpha * alpha + sigma), alpha);
+      tau = (beta - alpha) / beta;
+      scal = 1.0 / (alpha - beta);
     }
-    const double sigma = block_sum_all(part, S.red);
     if (tid == 0) {
-      const double alpha = S.A[tri(k + 1, k)];
-      double beta, tau, scal;
-      if (sigma == 0.0) { beta = alpha; tau = 0.0; scal = 0.0; }
-      else {
-        beta = -copysign(sqrt(alpha * alpha + sigma), alpha);
-        tau = (beta - alpha) / beta;
-        scal = 1.0 / (alpha - beta);
-      }
-      S.scal[0] = tau;
-      S.scal[1] = scal;
       S.e[k] = beta;
       S.tau[k] = tau;
-      S.d[k] = S.A[tri(k, k)];
+      S.d[k] = A[tri(k, k)];
     }
-    __syncthreads();
-    const double tau = S.scal[0], scal = S.scal[1];
-    for (int i = tid; i < n; i += BT_T) {
-      double vi = 0.0;
-      if (i == k + 1) vi = 1.0;
-      else if (i > k + 1) {
-        vi = S.A[tri(i, k)] * scal;
-        S.A[tri(i, k)] = vi;  // reflector kept below the subdiagonal
-      }
-      S.v[i] = vi;
+    // p = tau A22 v on a 16 x 16 thread tile: thread (tr, tc) sums rows
+    // k+1+tr+16a over columns k+1+tc+16b, v on the fly from column k; the
+    // row sums are reduced over the 16 lanes of a half-warp.
+    const int k1 = k + 1;
+    // tile rows i = k1 + tr + 16 a < n, columns j = k1 + tc + 16 b < n; nrw
+    // bounds a for both half-warps of this warp (the shuffles stay uniform)
+    const int nrw = (n - k1 - 2 * wp + 15) >> 4;
+    double vr[8];
+#pragma unroll
+    for (int b = 0; b < 8; ++b) {
+      const int j = k1 + tc + 16 * b;
+      vr[b] = 0.0;
+      if (j < n) vr[b] = (j == k1) ? 1.0 : A[j * (j + 1) / 2 + k] * scal;
     }
-    __syncthreads();
-    if (tau == 0.0) continue;
-    // p = tau A22 v over rows k+1..n-1
-    double pvp = 0.0;
-    for (int i = k + 1 + tid; i < n; i += BT_T) {
+    double acc[8];
+#pragma unroll
+    for (int a = 0; a < 8; ++a) {
+      acc[a] = 0.0;
+      const int i = k1 + tr + 16 * a;
+      if (i >= n) break;
+      const int rbase = i * (i + 1) / 2;
       double s = 0.0;
-      for (int j = k + 1; j <= i; ++j) s += S.A[tri(i, j)] * S.v[j];
-      for (int j = i + 1; j < n; ++j) s += S.A[tri(j, i)] * S.v[j];
-      s *= tau;
-      S.pv[i] = s;
-      pvp += s * S.v[i];
+#pragma unroll
+      for (int b = 0; b < 8; ++b) {
+        const int j = k1 + tc + 16 * b;
+        if (j >= n) break;
+        s += (j <= i ? A[rbase + j] : A[j * (j + 1) / 2 + i]) * vr[b];
+      }
+      acc[a] = s;
     }
-    const double dot = block_sum_all(pvp, S.red);
-    const double kk = 0.5 * tau * dot;
-    for (int i = k + 1 + tid; i < n; i += BT_T) S.pv[i] = S.pv[i] - kk * S.v[i];
+#pragma unroll
+    for (int a = 0; a < 8; ++a) {
+      if (a >= nrw) break;
+#pragma unroll
+      for (int o = 8; o > 0; o >>= 1) acc[a] += __shfl_xor_sync(0xffffffffu, acc[a], o);
+    }
+    double dot = 0.0;
+    if (tc == 0) {
+#pragma unroll
+      for (int a = 0; a < 8; ++a) {
+        const int i = k1 + tr + 16 * a;
+        if (i >= n) break;
+        const double vi = (i == k1) ? 1.0 : A[i * (i + 1) / 2 + k] * scal;
+        const double s = acc[a] * tau;
+        S.pv[i] = s;
+        S.v[i] = vi;
+        dot += s * vi;
+      }
+    }
+    dot = warp_sum(dot);
+    if (lane == 0) redB[wp] = dot;
     __syncthreads();
-    // A22 -= v w^T + w v^T (lower triangle)
-    const int m = n - k - 1;
-    const long long cnt = (long long)m * (m + 1) / 2;
-    for (long long q = tid; q < cnt; q += BT_T) {
-      int r = (int)((sqrt(8.0 * (double)q + 1.0) - 1.0) * 0.5);
-      while ((long long)r * (r + 1) / 2 > q) --r;
-      while ((long long)(r + 1) * (r + 2) / 2 <= q) ++r;
-      const int c = (int)(q - (long long)r * (r + 1) / 2);
-      const int i = k + 1 + r, j = k + 1 + c;
-      S.A[tri(i, j)] -= S.v[i] * S.pv[j] + S.pv[i] * S.v[j];
+    double dt = redB[0];
+#pragma unroll
+    for (int q = 1; q < BT_W; ++q) dt += redB[q];
+    const double kk = 0.5 * tau * dt;
+    // A22 -= v w^T + w v^T, w = p - kk v, on the same tile; the reflector
+    // replaces column k; squares of the new column k + 1 below its
+    // subdiagonal give the next norm
+    double wr[8];
+#pragma unroll
+    for (int b = 0; b < 8; ++b) {
+      const int j = k1 + tc + 16 * b;
+      vr[b] = 0.0;
+      wr[b] = 0.0;
+      if (j < n) {
+        vr[b] = S.v[j];
+        wr[b] = S.pv[j] - kk * vr[b];
+      }
     }
+    double nxt = 0.0;
+#pragma unroll
+    for (int a = 0; a < 8; ++a) {
+      const int i = k1 + tr + 16 * a;
+      if (i >= n) break;
+      const int rbase = i * (i + 1) / 2;
+      const double vi = S.v[i], wi = S.pv[i] - kk * vi;
+#pragma unroll
+      for (int b = 0; b < 8; ++b) {
+        const int j = k1 + tc + 16 * b;
+        if (j > i) break;
+        const double x = A[rbase + j] - (vi * wr[b] + wi * vr[b]);
+        A[rbase + j] = x;
+        if (b == 0 && tc == 0 && i >= k + 3) nxt += x * x;
+      }
+      if (tc == 0 && i >= k + 2) A[rbase + k] = vi;
+    }
+    nxt = warp_sum(nxt);
+    if (lane == 0) redA[wp] = nxt;
     __syncthreads();
   }
   if (tid == 0) {
     if (n >= 2) {
-      S.d[n - 2] = S.A[tri(n - 2, n - 2)];
-      S.e[n - 2] = S.A[tri(n - 1, n - 2)];
+      S.d[n - 2] = A[tri(n - 2, n - 2)];
+      S.e[n - 2] = A[tri(n - 1, n - 2)];
       S.tau[n - 2] = 0.0;
     }
-    S.d[n - 1] = S.A[tri(n - 1, n - 1)];
+    S.d[n - 1] = A[tri(n - 1, n - 1)];
   }
+  // reflectors to global scratch when Z is to overlay A
+  const bool zshared = S.Z == S.A;
+  double* refl = zshared ? scr + BT_LU : A;
+  if (vectors && zshared)
+    for (int q = tid; q < n * (n + 1) / 2; q += BT_T) refl[q] = A[q];
   __syncthreads();
+  ph_mark(ph, 2);
   // ---- bounds, e^2
   if (tid == 0) {
     double lo = 1e300, hi = -1e300, em = 0.0;
@@ -382,14 +499,15 @@ __device__ void cta_eigh(int n, int nz, Smem& S, double* U) {
     S.scal[7] = tnorm;
   }
   __syncthreads();
-  // ---- eigenvalues 0..nz by 5-section, four lanes per eigenvalue.  Every
+  // ---- eigenvalues 0 .. LUMO by 5-section, four lanes per eigenvalue.  Every
   // lane runs the same rounds and steps (groups that have converged idle), so
   // the 4-lane shuffles always see a converged warp.
   {
     const int grp = tid >> 2, ln = tid & 3, base = tid & 31 & ~3;
     const double pivmin = S.scal[6];
-    const double eps = 2.220446049250313e-16;
-    const int nev = ((nz > 1 ? nz : 1) + 1 < n ? (nz > 1 ? nz : 1) + 1 : n);  // through the LUMO
+    const double atol = 2.220446049250313e-16 * S.scal[7] + pivmin;
+    const int nlo = nz > 1 ? nz : 1;
+    const int nev = nlo + 1 < n ? nlo + 1 : n;
     const int rounds = (nev + BT_T / 4 - 1) / (BT_T / 4);
     for (int rd = 0; rd < rounds; ++rd) {
       const int mm = rd * (BT_T / 4) + grp;
@@ -397,7 +515,7 @@ __device__ void cta_eigh(int n, int nz, Smem& S, double* U) {
       double lo = S.scal[4], hi = S.scal[5];
       bool done = !active;
       for (int it = 0; it < 100; ++it) {
-        if (!done && hi - lo <= 2.0 * eps * fmax(fabs(lo), fabs(hi)) + pivmin) done = true;
+        if (!done && hi - lo <= reltol * fmax(fabs(lo), fabs(hi)) + atol) done = true;
         const double x = lo + (hi - lo) * ((double)(ln + 1) / 5.0);
         const int cnt = done ? 0 : sturm(n, S.d, S.e2, x, pivmin);
         const int flag = cnt > mm ? 1 : 0;
@@ -408,17 +526,17 @@ __device__ void cta_eigh(int n, int nz, Smem& S, double* U) {
 #pragma unroll
         for (int q = 0; q < 4; ++q) xs[q] = __shfl_sync(0xffffffffu, x, base + q);
         if (!done) {
-          double nlo = lo, nhi = hi;
+          double nl = lo, nh = hi;
           if (above == 0) {
-            nlo = xs[3];
+            nl = xs[3];
           } else {
             const int firstl = __ffs(above) - 1;
-            nhi = xs[firstl];
-            if (firstl > 0) nlo = xs[firstl - 1];
+            nh = xs[firstl];
+            if (firstl > 0) nl = xs[firstl - 1];
           }
-          if (!(nlo > lo) && !(nhi < hi)) done = true;
-          lo = nlo;
-          hi = nhi;
+          if (!(nl > lo) && !(nh < hi)) done = true;
+          lo = nl;
+          hi = nh;
         }
         if (__all_sync(0xffffffffu, done)) break;
       }
@@ -426,19 +544,27 @@ __device__ void cta_eigh(int n, int nz, Smem& S, double* U) {
     }
   }
   __syncthreads();
+  ph_mark(ph, 3);
+  if (!vectors) return;
   // ---- eigenvectors 0..nz-1 of T by inverse iteration (thread per cluster start)
   {
     const double tnorm = S.scal[7];
-    const double ortol = 1.0e-8 * tnorm;
+    // vectors whose eigenvalues lie closer than ortol are a cluster
+    // (iterated together, re-orthogonalised); farther pairs converge apart in
+    // two solves even from eigenvalues good to 1e-11 relative
+    const double ortol = 1.0e-7 * tnorm;
     const double eps = 2.220446049250313e-16;
     const double tiny = eps * fmax(tnorm, 1e-300);
+    double* Z = S.Z;
     for (int m0 = tid; m0 < nz; m0 += BT_T) {
       if (m0 > 0 && !(S.eig[m0] - S.eig[m0 - 1] > ortol)) continue;
       int m1 = m0 + 1;
       while (m1 < nz && !(S.eig[m1] - S.eig[m1 - 1] > ortol)) ++m1;
-      double* u0 = U + (long long)m0 * 3 * n;
+      double* u0 = scr + (long long)m0 * 5 * n;
       double* u1 = u0 + n;
       double* u2 = u1 + n;
+      double* ul = u2 + n;
+      double* us = ul + n;
       double lam_prev = 0.0;
       for (int mv = m0; mv < m1; ++mv) {
         double lam = S.eig[mv];
@@ -447,170 +573,231 @@ __device__ void cta_eigh(int n, int nz, Smem& S, double* U) {
           if (lam - lam_prev < pertol) lam = lam_prev + pertol;
         }
         lam_prev = lam;
-        double* x = S.Z + mv;  // stride nz
-        unsigned long long s = 0x9E3779B97F4A7C15ull ^ (unsigned long long)(mv + 1) * 0xBF58476D1CE4E5B9ull;
-        for (int i = 0; i < n; ++i) {
-          s ^= s >> 31; s *= 0x94D049BB133111EBull; s ^= s >> 29;
-          x[(long long)i * nz] = ((double)(s >> 11) * (1.0 / 9007199254740992.0)) - 0.5;
-        }
-        const int nits = (m1 - m0 > 1) ? 4 : 2;
-        for (int itr = 0; itr < nits; ++itr) {
-          // LU with partial pivoting of T - lam I, forward and back substitution
-          double dd = S.d[0] - lam, du = n > 1 ? S.e[0] : 0.0, du2 = 0.0, xr = x[0];
+        double* x = Z + mv;  // stride nz
+        // LU with partial pivoting of T - lam I, once per vector: 1 / pivot,
+        // the two entries right of it, the multiplier, whether rows swapped
+        {
+          double dd = S.d[0] - lam, du = n > 1 ? S.e[0] : 0.0;
           for (int i = 0; i < n - 1; ++i) {
             const double sub = S.e[i], dn = S.d[i + 1] - lam, en = (i + 1 < n - 1) ? S.e[i + 1] : 0.0;
-            const double xn = x[(long long)(i + 1) * nz];
             if (fabs(dd) >= fabs(sub)) {
               double pv = dd;
               if (fabs(pv) < tiny) pv = copysign(tiny, pv == 0.0 ? 1.0 : pv);
-              const double l = sub / pv;
-              u0[i] = pv; u1[i] = du; u2[i] = du2;
-              x[(long long)i * nz] = xr;
-              dd = dn - l * du; du = en; du2 = 0.0; xr = xn - l * xr;
+              const double rp = recip_nr2(pv);
+              const double l = sub * rp;
+              u0[i] = rp; u1[i] = du; u2[i] = 0.0; ul[i] = l; us[i] = 0.0;
+              dd = dn - l * du;
+              du = en;
             } else {
-              const double l = dd / sub;
-              u0[i] = sub; u1[i] = dn; u2[i] = en;
-              x[(long long)i * nz] = xn;
-              const double ndd = du - l * dn, ndu = -l * en;
-              dd = ndd; du = ndu; du2 = 0.0; xr = xr - l * xn;
+              const double rs = recip_nr2(sub);
+              const double l = dd * rs;
+              u0[i] = rs; u1[i] = dn; u2[i] = en; ul[i] = l; us[i] = 1.0;
+              dd = du - l * dn;
+              du = -l * en;
             }
           }
           double last = dd;
           if (fabs(last) < tiny) last = copysign(tiny, last == 0.0 ? 1.0 : last);
-          u0[n - 1] = last;
-          double x1 = xr / last, x2 = 0.0;
-          x[(long long)(n - 1) * nz] = x1;
+          u0[n - 1] = recip_nr2(last);
+        }
+        const int nits = (m1 - m0 > 1) ? 4 : 2;
+        for (int itr = 0; itr < nits; ++itr) {
+          // forward (row swaps and multipliers) and back substitution; the
+          // first pass starts from a pseudo-random vector made on the way
+          unsigned long long rs = 0x9E3779B97F4A7C15ull ^ (unsigned long long)(mv + 1) * 0xBF58476D1CE4E5B9ull;
+          auto rnd = [&]() {
+            rs ^= rs >> 31; rs *= 0x94D049BB133111EBull; rs ^= rs >> 29;
+            return ((double)(rs >> 11) * (1.0 / 9007199254740992.0)) - 0.5;
+          };
+          double xr = itr == 0 ? rnd() : x[0];
+          for (int i = 0; i < n - 1; ++i) {
+            const double xn = itr == 0 ? rnd() : x[(i + 1) * nz];
+            if (us[i] != 0.0) {
+              x[i * nz] = xn;
+              xr = xr - ul[i] * xn;
+            } else {
+              x[i * nz] = xr;
+              xr = xn - ul[i] * xr;
+            }
+          }
+          double x1 = xr * u0[n - 1], x2 = 0.0;
+          x[(n - 1) * nz] = x1;
           for (int i = n - 2; i >= 0; --i) {
-            const double vv = (x[(long long)i * nz] - u1[i] * x1 - u2[i] * x2) / u0[i];
-            x[(long long)i * nz] = vv;
+            const double vv = (x[i * nz] - u1[i] * x1 - u2[i] * x2) * u0[i];
+            x[i * nz] = vv;
             x2 = x1;
             x1 = vv;
           }
           for (int q = m0; q < mv; ++q) {  // re-orthogonalise against earlier members
-            double dt = 0.0;
-            for (int i = 0; i < n; ++i) dt += S.Z[(long long)i * nz + q] * x[(long long)i * nz];
-            for (int i = 0; i < n; ++i) x[(long long)i * nz] -= dt * S.Z[(long long)i * nz + q];
+            double dq = 0.0;
+            for (int i = 0; i < n; ++i) dq += Z[i * nz + q] * x[i * nz];
+            for (int i = 0; i < n; ++i) x[i * nz] -= dq * Z[i * nz + q];
           }
-          double mx = 0.0, ss = 0.0;
-          for (int i = 0; i < n; ++i) mx = fmax(mx, fabs(x[(long long)i * nz]));
-          const double inv = mx > 0.0 ? 1.0 / mx : 0.0;
-          for (int i = 0; i < n; ++i) { const double t = x[(long long)i * nz] * inv; ss += t * t; }
-          const double sc = ss > 0.0 ? inv / sqrt(ss) : 0.0;
-          for (int i = 0; i < n; ++i) x[(long long)i * nz] *= sc;
+          // normalise (one solve from a unit vector grows it by at most
+          // n / tiny, far inside the double range)
+          double ss = 0.0;
+          for (int i = 0; i < n; ++i) ss += x[i * nz] * x[i * nz];
+          const double sc = ss > 0.0 ? 1.0 / sqrt(ss) : 0.0;
+          for (int i = 0; i < n; ++i) x[i * nz] *= sc;
         }
       }
     }
   }
   __syncthreads();
-  // ---- back-transformation Z <- H_0 ... H_{n-3} Z (thread per vector column)
-  for (int k = n - 3; k >= 0; --k) {
-    const double tau = S.tau[k];
-    if (tau != 0.0) {
-      for (int mcol = tid; mcol < nz; mcol += BT_T) {
-        double s = S.Z[(long long)(k + 1) * nz + mcol];
-        for (int i = k + 2; i < n; ++i) s += S.A[tri(i, k)] * S.Z[(long long)i * nz + mcol];
-        s *= tau;
-        S.Z[(long long)(k + 1) * nz + mcol] -= s;
-        for (int i = k + 2; i < n; ++i) S.Z[(long long)i * nz + mcol] -= s * S.A[tri(i, k)];
+  ph_mark(ph, 4);
+  // ---- back-transformation Z <- H_0 ... H_{n-3} Z in blocks of BT_NB
+  // reflectors, each block as I - V T V^T (the compact WY form; T upper
+  // triangular, T(0:c, c) = -tau_c T(0:c, 0:c) V(:, 0:c)^T v_c).  T of every
+  // block first (a warp per block), then g lanes per column apply the blocks
+  // from the last to the first with no barriers: a column belongs to one
+  // lane group.
+  {
+    double* Z = S.Z;
+    const int nr = n - 2;  // reflectors 0 .. n-3
+    const int nblk = nr > 0 ? (nr + BT_NB - 1) / BT_NB : 0;
+    auto vref = [&](int i, int kr) -> double {  // element i of reflector kr
+      return i == kr + 1 ? 1.0 : (i > kr + 1 ? refl[i * (i + 1) / 2 + kr] : 0.0);
+    };
+    for (int blk = wp; blk < nblk; blk += BT_W) {
+      double* T = S.tw + blk * BT_NB * BT_NB;
+      const int kb = blk * BT_NB, nbb = min(BT_NB, nr - kb);
+      for (int q = lane; q < BT_NB * BT_NB; q += 32) T[q] = 0.0;
+      __syncwarp();
+      // Gram entries V(:, j)^T v_c, j < c < nbb, one lane each (28 pairs)
+      if (lane < BT_NB * (BT_NB - 1) / 2) {
+        int c = 1, j = lane;
+        while (j >= c) { j -= c; ++c; }
+        if (c < nbb) {
+          double g = 0.0;
+          for (int i = kb + c + 1; i < n; ++i) g += vref(i, kb + j) * vref(i, kb + c);
+          T[j * BT_NB + c] = g;
+        }
+      }
+      __syncwarp();
+      if (lane == 0) {
+        for (int c = 0; c < nbb; ++c) {
+          const double tc_ = S.tau[kb + c];
+          double t[BT_NB];
+#pragma unroll
+          for (int j = 0; j < BT_NB; ++j) {
+            double s = 0.0;
+            if (j < c)
+              for (int l = j; l < c; ++l) s += T[j * BT_NB + l] * T[l * BT_NB + c];
+            t[j] = s;
+          }
+#pragma unroll
+          for (int j = 0; j < BT_NB; ++j)
+            if (j < c) T[j * BT_NB + c] = -tc_ * t[j];
+          T[c * BT_NB + c] = tc_;
+        }
+      }
+      __syncwarp();
+    }
+    __syncthreads();
+    const int g = nz <= 32 ? 8 : (nz <= 64 ? 4 : 2);
+    const int col = tid / g, gl = tid % g;
+    const bool act = col < nz;
+    for (int blk = nblk - 1; blk >= 0; --blk) {
+      const double* T = S.tw + blk * BT_NB * BT_NB;
+      const int kb = blk * BT_NB;
+      double acc[BT_NB];
+#pragma unroll
+      for (int c = 0; c < BT_NB; ++c) acc[c] = 0.0;
+      // rows kb+1 .. kb+BT_NB meet the reflectors' leading ones and zeros;
+      // below them every element is a stored reflector entry.  Reflectors
+      // past n-3 have zero T rows and columns and no stored entries here.
+      if (act) {
+        int i = kb + 1 + gl;
+        for (; i < n && i <= kb + BT_NB; i += g) {
+          const double z = Z[i * nz + col];
+#pragma unroll
+          for (int c = 0; c < BT_NB; ++c) acc[c] += vref(i, kb + c) * z;
+        }
+        for (; i < n; i += g) {
+          const double z = Z[i * nz + col];
+          const double* rr = refl + i * (i + 1) / 2 + kb;
+#pragma unroll
+          for (int c = 0; c < BT_NB; ++c) acc[c] += rr[c] * z;
+        }
+      }
+#pragma unroll
+      for (int o = 1; o < 8; o <<= 1)
+        if (o < g)
+#pragma unroll
+          for (int c = 0; c < BT_NB; ++c) acc[c] += __shfl_xor_sync(0xffffffffu, acc[c], o);
+      double wv[BT_NB];
+#pragma unroll
+      for (int c = 0; c < BT_NB; ++c) {
+        double s = 0.0;
+#pragma unroll
+        for (int j = c; j < BT_NB; ++j) s += T[c * BT_NB + j] * acc[j];
+        wv[c] = s;
+      }
+      if (act) {
+        int i = kb + 1 + gl;
+        for (; i < n && i <= kb + BT_NB; i += g) {
+          double s = 0.0;
+#pragma unroll
+          for (int c = 0; c < BT_NB; ++c) s += vref(i, kb + c) * wv[c];
+          Z[i * nz + col] -= s;
+        }
+        for (; i < n; i += g) {
+          const double* rr = refl + i * (i + 1) / 2 + kb;
+          double s = 0.0;
+#pragma unroll
+          for (int c = 0; c < BT_NB; ++c) s += rr[c] * wv[c];
+          Z[i * nz + col] -= s;
+        }
       }
     }
   }
   __syncthreads();
-}
-
-// F of the molecule (H, the shifted start when use_shift, then fock2 + fock1).
-__device__ void cta_fock(const BatchArgs& B, const Mol& M, double shift, bool use_shift, double* f,
-                         const double* p, const double* pa, const double* h) {
-  const long long mp = (long long)M.n * (M.n + 1) / 2;
-  for (long long idx = threadIdx.x; idx < mp; idx += BT_T) {
-    double v = h[idx];
-    if (use_shift) {
-      v = DADD(DADD(h[idx], DMUL(shift, pa[idx])), DMUL((double)(idx + 1), 1.0e-16));
-      long long r = (long long)((sqrt(8.0 * (double)idx + 1.0) - 1.0) * 0.5);
-      while (r * (r + 1) / 2 > idx) --r;
-      while ((r + 1) * (r + 2) / 2 <= idx) ++r;
-      if (idx - r * (r + 1) / 2 == r) v = DSUB(v, shift);
-    }
-    f[idx] = v;
-  }
-  __syncthreads();
-  for (int a = threadIdx.x; a < M.numat; a += BT_T) fock_atom(B, M, a, p, pa, f);
-  __syncthreads();
-}
-
-// helect: sum_{i>j} p (h + f) + 0.5 sum_i p_ii (h_ii + f_ii), fixed order.
-__device__ double cta_helect(int n, const double* p, const double* h, const double* f, double* red) {
-  double s = 0.0, dsum = 0.0;
-  for (int r = threadIdx.x; r < n; r += BT_T) {
-    const long long base = (long long)r * (r + 1) / 2;
-    double a = 0.0;
-    for (int c = 0; c < r; ++c) a += p[base + c] * (h[base + c] + f[base + c]);
-    s += a;
-    dsum += p[base + r] * (h[base + r] + f[base + r]);
-  }
-  const double a = block_sum_all(s, red);
-  const double b = block_sum_all(dsum, red);
-  return a + 0.5 * b;
+  ph_mark(ph, 5);
 }
 
 // cnvg (SCF/cnvg.F90:16-145) on the molecule's packed arrays; returns pl.
-__device__ double cta_cnvg(int n, double* pnew, double* p, double* p1, int niter, double* red, double* scal) {
+// The diagonal statistics run on thread 0 in the reference's order over
+// copies staged in shared memory (S.d, S.e, S.e2, S.pv: free after the
+// eigensolve); the off-diagonal extrapolation is elementwise.
+__device__ double cta_cnvg(int n, double* pnew, double* p, double* p1, int niter, Smem& S) {
+  double *xn = S.d, *xo = S.e, *x1 = S.e2, *pd = S.pv;
+  for (int i = threadIdx.x; i < n; i += BT_T) {
+    xn[i] = pnew[tri(i, i)];
+    xo[i] = p[tri(i, i)];
+    x1[i] = p1[i];
+  }
+  __syncthreads();
   if (threadIdx.x == 0) {
     const bool extrap = (niter % 3) != 0;
     double pl = 0.0, faca = 0.0, facb = 0.0, sum1 = 0.0;
     for (int i = 0; i < n; ++i) {
-      const long long k = tri(i, i);
-      const double a = pnew[k];
+      const double a = xn[i];
       sum1 = DADD(sum1, a);
-      const double sa = fabs(DSUB(a, p[k]));
+      const double sa = fabs(DSUB(a, xo[i]));
       if (sa > pl) pl = sa;
       if (!extrap) {
         faca = DADD(faca, DMUL(sa, sa));
-        const double t = DADD(DSUB(a, DMUL(2.0, p[k])), p1[i]);
+        const double t = DADD(DSUB(a, DMUL(2.0, xo[i])), x1[i]);
         facb = DADD(facb, DMUL(t, t));
       }
     }
     double fac = 0.0;
     if (facb > 1.0e-10 && faca < DMUL(100.0, facb)) fac = sqrt(faca / facb);
-    scal[8] = fac;
-    scal[9] = pl;
-    scal[10] = sum1;
-    for (int i = 0; i < n; ++i) {
-      const long long k = tri(i, i);
-      p1[i] = p[k];
-      p[k] = pnew[k];
-    }
-  }
-  __syncthreads();
-  const double fac = scal[8];
-  for (int r = 0; r < n; ++r) {
-    const long long base = (long long)r * (r + 1) / 2;
-    for (int c = threadIdx.x; c < r; c += BT_T) {
-      const long long idx = base + c;
-      const double a = pnew[idx];
-      const double v = DADD(a, DMUL(fac, DSUB(a, p[idx])));
-      p[idx] = v;
-      pnew[idx] = v;
-    }
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
+    // diagonal: damped extrapolation from the old diagonal (now P1), clamp, renormalise
     const double rhfuhf = 2.0;
     const double damp = (niter > 3) ? 0.05 : 1.0e10;
     double sum2 = 0.0;
-    double* pd = red;  // n <= 128 <= BT_T
     for (int i = 0; i < n; ++i) {
-      double v = p[tri(i, i)];
-      const double dlt = DSUB(v, p1[i]);
-      if (fabs(dlt) > damp) v = DADD(p1[i], copysign(damp, dlt));
+      double v = xn[i];
+      const double dlt = DSUB(v, xo[i]);
+      if (fabs(dlt) > damp) v = DADD(xo[i], copysign(damp, dlt));
       else v = DADD(v, DMUL(fac, dlt));
       const double t = v > 0.0 ? v : 0.0;
       v = t < rhfuhf ? t : rhfuhf;
       sum2 = DADD(sum2, v);
       pd[i] = v;
     }
-    const double sum0 = scal[10];
-    double sum1 = sum0;
+    const double sum0 = sum1;
     for (int guard = 0; guard < 1000; ++guard) {
       const double sum = sum2 > 1.0e-3 ? sum1 / sum2 : 0.0;
       sum1 = sum0;
@@ -628,51 +815,86 @@ __device__ double cta_cnvg(int n, double* pnew, double* p, double* p1, int niter
         pd[i] = v;
       }
     }
-    for (int i = 0; i < n; ++i) {
-      p[tri(i, i)] = pd[i];
-      pnew[tri(i, i)] = pd[i];
+    S.scal[8] = fac;
+    S.scal[9] = pl;
+  }
+  __syncthreads();
+  const double fac = S.scal[8];
+  const int mp = n * (n + 1) / 2;
+  for (int q = threadIdx.x; q < mp; q += BT_T) {
+    int r, c;
+    tri_rc(q, r, c);
+    if (r == c) {
+      p[q] = pd[r];
+      pnew[q] = pd[r];
+      p1[r] = xo[r];
+    } else {
+      const double a = pnew[q];
+      const double v = DADD(a, DMUL(fac, DSUB(a, p[q])));
+      p[q] = v;
+      pnew[q] = v;
     }
   }
   __syncthreads();
-  return scal[9];
+  return S.scal[9];
 }
 
-// Full diagonalisation of the molecule's F (packed, perturbed i*1e-10 in place
-// as eigenvectors_LAPACK does), occupied vectors in S.Z, eigenvalues in S.eig.
-__device__ void cta_diag(const Mol& M, double* f, Smem& S, double* U) {
-  const int n = M.n;
-  const long long mp = (long long)n * (n + 1) / 2;
-  for (int i = threadIdx.x; i < n; i += BT_T) {
-    const long long k = tri(i, i);
-    f[k] = DADD(f[k], DMUL((double)(i + 1), 1.0e-10));
+// The molecule's F (packed, perturbed i*1e-10 in place as eigenvectors_LAPACK
+// does) into S.A.
+__device__ void load_perturbed(int n, double* f, Smem& S, bool in_place) {
+  const int mp = n * (n + 1) / 2;
+  if (in_place)
+    for (int i = threadIdx.x; i < n; i += BT_T) {
+      const long long k = tri(i, i);
+      f[k] = DADD(f[k], DMUL((double)(i + 1), 1.0e-10));
+    }
+  __syncthreads();
+  for (int q = threadIdx.x; q < mp; q += BT_T) {
+    int r, c;
+    tri_rc(q, r, c);
+    S.A[q] = (r == c && !in_place) ? DADD(f[q], DMUL((double)(r + 1), 1.0e-10)) : f[q];
   }
   __syncthreads();
-  for (long long q = threadIdx.x; q < mp; q += BT_T) S.A[q] = f[q];
-  __syncthreads();
-  cta_eigh(n, M.nclose, S, U);
 }
 
-__device__ void cta_density(const Mol& M, const Smem& S, double* p, double* pa) {
-  const int n = M.n, nz = M.nclose;
-  const long long mp = (long long)n * (n + 1) / 2;
-  for (long long q = threadIdx.x; q < mp; q += BT_T) {
-    long long r = (long long)((sqrt(8.0 * (double)q + 1.0) - 1.0) * 0.5);
-    while (r * (r + 1) / 2 > q) --r;
-    while ((r + 1) * (r + 2) / 2 <= q) ++r;
-    const long long c = q - r * (r + 1) / 2;
+// P = 2 Z Z^T over the occupied vectors.
+__device__ void cta_density(int n, int nz, const Smem& S, double* p) {
+  const int mp = n * (n + 1) / 2;
+  for (int q = threadIdx.x; q < mp; q += BT_T) {
+    int r, c;
+    tri_rc(q, r, c);
     double s = 0.0;
     for (int m = 0; m < nz; ++m) s += S.Z[r * nz + m] * S.Z[c * nz + m];
     p[q] = 2.0 * s;
   }
   __syncthreads();
-  (void)pa;
 }
 
-__global__ void __launch_bounds__(BT_T, 1) scf_batch_kernel(BatchArgs B) {
+__global__ void __launch_bounds__(BT_T, 2) scf_batch_kernel(BatchArgs B) {
   extern __shared__ double smem[];
-  __shared__ int s_m;
+  __shared__ int s_m, s_nitems;
+  __shared__ long long s_ph[BT_PHASES + 1];
   const int tid = threadIdx.x;
-  double* Ushared = B.scratch + (long long)blockIdx.x * 3 * BT_NMAX * BT_NMAX;
+  long long* ph = B.phase ? s_ph : nullptr;
+  double* scr = B.scratch + (long long)blockIdx.x * BT_SCR;
+  Smem S;
+  S.A = smem;
+  S.d = S.A + BT_AMAX;
+  S.e = S.d + BT_NMAX;
+  S.e2 = S.e + BT_NMAX;
+  S.tau = S.e2 + BT_NMAX;
+  S.pv = S.tau + BT_NMAX;
+  S.v = S.pv + BT_NMAX;
+  S.eig = S.v + BT_NMAX;
+  S.red = S.eig + BT_NMAX + 2;
+  S.scal = S.red + 2 * BT_W;
+  S.tw = S.scal + 16;
+  S.awrow = (long long*)(S.tw + BT_TW);
+  S.afirst = (int*)(S.awrow + BT_NMAX);
+  S.anor = S.afirst + BT_NMAX;
+  S.acum = S.anor + BT_NMAX;
+  S.orb_atom = S.acum + BT_NMAX;
+  S.item = S.orb_atom + BT_NMAX;
   for (;;) {
     if (tid == 0) s_m = atomicAdd(B.next, 1);
     __syncthreads();
@@ -681,37 +903,48 @@ __global__ void __launch_bounds__(BT_T, 1) scf_batch_kernel(BatchArgs B) {
     if (m >= B.nmol) break;
     const int mi = B.order[m];
     const Mol M = B.mol[mi];
+    if (ph && tid == 0) {
+      for (int q = 0; q < BT_PHASES; ++q) s_ph[q] = 0;
+      s_ph[BT_PHASES] = clock64();
+    }
     const int n = M.n, nclose = M.nclose;
-    const long long mp = (long long)n * (n + 1) / 2;
-    Smem S;
-    S.A = smem;
-    S.Z = S.A + (BT_NMAX * (BT_NMAX + 1)) / 2;
-    S.d = S.Z + BT_ZMAX;
-    S.e = S.d + BT_NMAX;
-    S.e2 = S.e + BT_NMAX;
-    S.tau = S.e2 + BT_NMAX;
-    S.pv = S.tau + BT_NMAX;
-    S.v = S.pv + BT_NMAX;
-    S.eig = S.v + BT_NMAX;
-    S.red = S.eig + BT_NMAX + 1;
-    S.scal = S.red + BT_T;
+    const int mp = n * (n + 1) / 2;
+    S.Z = (n * nclose <= BT_AMAX) ? S.A : scr + BT_LU + BT_AMAX;
+    // the molecule's atom tables
+    for (int a = tid; a < M.numat; a += BT_T) {
+      S.afirst[a] = B.first[M.aoff + a];
+      S.anor[a] = B.nor[M.aoff + a];
+      S.acum[a] = B.cum[M.aoff + a];
+      S.awrow[a] = B.wrow[M.aoff + a];
+    }
+    __syncthreads();
+    for (int a = tid; a < M.numat; a += BT_T)
+      for (int o = 0; o < S.anor[a]; ++o) S.orb_atom[S.afirst[a] + o] = a;
+    if (tid == 0) {
+      int it = 0;
+      for (int a = 0; a < M.numat; ++a) {
+        const int nd = S.anor[a] * (S.anor[a] + 1) / 2;
+        for (int q = 0; q < nd; ++q) S.item[it++] = (a << 4) | q;
+      }
+      s_nitems = it;
+    }
     double* f = B.f + M.hoff;
     double* p = B.p + M.hoff;
-    double* pa = B.pa + M.hoff;
     double* pold = B.pold + M.hoff;
     double* pold2 = B.pold2 + M.doff;
     const double* h = B.h + M.hoff;
-    // ---- first-call setup (iter.F90:123-221): diagonal guess
+    // ---- first-call setup (iter.F90:123-221): diagonal guess; PA = w1 * P
     const double w1 = (double)nclose / ((double)nclose + 1.0e-6 + (double)nclose);
-    for (long long q = tid; q < mp; q += BT_T) { p[q] = 0.0; pa[q] = 0.0; pold[q] = 0.0; }
+    double cpa = w1;
+    for (int q = tid; q < mp; q += BT_T) { p[q] = 0.0; pold[q] = 0.0; }
     __syncthreads();
+    const int nitems = s_nitems;
     for (int i = tid; i < n; i += BT_T) {
       const long long j = tri(i, i);
       const double pd = B.pdiag[M.doff + i];
       p[j] = pd;
-      pa[j] = DMUL(DMUL(pd, w1), 1.0);
-      pold[j] = pa[j];
-      pold2[i] = pa[j];
+      pold[j] = DMUL(pd, w1);
+      pold2[i] = pold[j];
     }
     __syncthreads();
     // control scalars: every thread holds the same copy
@@ -752,8 +985,10 @@ __global__ void __launch_bounds__(BT_T, 1) scf_batch_kernel(BatchArgs B) {
       }
       double cur_shift = shift;
       for (;;) {  // label 320
-        cta_fock(B, M, cur_shift, use_shift, f, p, pa, h);
-        ee = cta_helect(n, pa, h, f, S.red) * 2.0;
+        ph_mark(ph, 7);
+        cta_fock(B, M, S, nitems, cpa, cur_shift, use_shift, f, p, h);
+        ph_mark(ph, 0);
+        ee = cta_helect(n, p, cpa, h, f, S.red) * 2.0;
         escf = (ee + M.enuclr) * enrgy + M.atheat;
         diff = escf - eold;
         if (diff > 0) ten = ten - 1.0; else ten = ten * 0.975 + 0.05;
@@ -773,25 +1008,28 @@ __global__ void __launch_bounds__(BT_T, 1) scf_batch_kernel(BatchArgs B) {
       ready = iredy > 0 && (fabs(diff) < sellim * 10.0 || pl == 0.0);
       ++iredy;
       eold = escf;
-      cta_diag(M, f, S, Ushared);
+      ph_mark(ph, 1);
+      load_perturbed(n, f, S, true);
+      cta_eigh(n, nclose, true, 1.0e-11, S, scr, ph);
       eig_homo = S.eig[ihomo - 1];
       eig_lumo = ihomo < n ? S.eig[ihomo] : 0.0;
-      cta_density(M, S, p, pa);
-      pl = cta_cnvg(n, p, pold, pold2, niter, S.red, S.scal);
-      for (long long q = tid; q < mp; q += BT_T) pa[q] = p[q] * 0.5;
-      __syncthreads();
+      cta_density(n, nclose, S, p);
+      ph_mark(ph, 6);
+      pl = cta_cnvg(n, p, pold, pold2, niter, S);
+      cpa = 0.5;
       if (!isfinite(pl)) break;
       oknewd = pl < sellim || oknewd;
       newdg = (pl < trans && oknewd) || newdg;
       if (pl < trans * 0.3333) oknewd = true;
     }
-    // ---- label 600: final energy and exit diagonalisation
-    ee = cta_helect(n, pa, h, f, S.red) * 2.0;
-    for (long long q = tid; q < mp; q += BT_T) S.A[q] = f[q];
-    __syncthreads();
-    for (int i = tid; i < n; i += BT_T) S.A[tri(i, i)] = DADD(S.A[tri(i, i)], DMUL((double)(i + 1), 1.0e-10));
-    __syncthreads();
-    cta_eigh(n, nclose, S, Ushared);
+    // ---- label 600: final energy and the exit eigenvalues
+    ph_mark(ph, 7);
+    ee = cta_helect(n, p, cpa, h, f, S.red) * 2.0;
+    load_perturbed(n, f, S, false);
+    ph_mark(ph, 1);
+    cta_eigh(n, nclose, false, 4.4e-16, S, scr, ph);
+    if (ph && tid == 0)
+      for (int q = 0; q < BT_PHASES; ++q) atomicAdd(B.phase + q, (unsigned long long)s_ph[q]);
     if (tid == 0) {
       B.escf[mi] = (ee + M.enuclr) * enrgy + M.atheat;
       B.ee[mi] = ee;
@@ -805,7 +1043,8 @@ __global__ void __launch_bounds__(BT_T, 1) scf_batch_kernel(BatchArgs B) {
 }
 
 size_t batch_smem() {
-  return sizeof(double) * ((size_t)(BT_NMAX * (BT_NMAX + 1)) / 2 + BT_ZMAX + 7 * BT_NMAX + 1 + BT_T + 32);
+  return sizeof(double) * ((size_t)BT_AMAX + 6 * BT_NMAX + BT_NMAX + 2 + 2 * BT_W + 16 + BT_TW) +
+         sizeof(long long) * BT_NMAX + sizeof(int) * (4 * BT_NMAX + BT_IMAX);
 }
 
 }  // namespace
@@ -816,8 +1055,10 @@ struct mb_batch {
   Mol* mol = nullptr;
   int *order = nullptr, *first = nullptr, *nor = nullptr, *lim = nullptr, *cum = nullptr, *nat = nullptr, *next = nullptr,
       *niter = nullptr, *conv = nullptr, *status = nullptr;
+  unsigned long long* phase = nullptr;
+  bool timing = false;
   long long* wrow = nullptr;
-  double *coord = nullptr, *h = nullptr, *w = nullptr, *pdiag = nullptr, *f = nullptr, *p = nullptr, *pa = nullptr,
+  double *coord = nullptr, *h = nullptr, *w = nullptr, *pdiag = nullptr, *f = nullptr, *p = nullptr,
          *pold = nullptr, *pold2 = nullptr, *scratch = nullptr, *escf = nullptr, *ee = nullptr, *homo = nullptr,
          *lumo = nullptr, *enuc = nullptr, *epairs = nullptr;
   long long tot_mp = 0, tot_w = 0;
@@ -828,8 +1069,8 @@ struct mb_batch {
 static void batch_free(mb_batch* b) {
   if (!b) return;
   void* ptrs[] = {b->mol, b->order, b->first, b->nor, b->lim, b->cum, b->nat, b->next, b->niter, b->conv, b->status, b->wrow,
-                  b->coord, b->h, b->w, b->pdiag, b->f, b->p, b->pa, b->pold, b->pold2, b->scratch, b->escf, b->ee,
-                  b->homo, b->lumo, b->enuc, b->epairs};
+                  b->coord, b->h, b->w, b->pdiag, b->f, b->p, b->pold, b->pold2, b->scratch, b->escf, b->ee,
+                  b->homo, b->lumo, b->enuc, b->epairs, b->phase};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   if (b->stream) cudaStreamDestroy(b->stream);
@@ -917,7 +1158,6 @@ extern "C" int mb_batch_create(int nmol, const int* numat, const int* nat, const
   BALLOC(b->pdiag, sizeof(double) * doff);
   BALLOC(b->f, sizeof(double) * hoff);
   BALLOC(b->p, sizeof(double) * hoff);
-  BALLOC(b->pa, sizeof(double) * hoff);
   BALLOC(b->pold, sizeof(double) * hoff);
   BALLOC(b->pold2, sizeof(double) * doff);
   BALLOC(b->escf, sizeof(double) * nmol);
@@ -929,6 +1169,7 @@ extern "C" int mb_batch_create(int nmol, const int* numat, const int* nat, const
   BALLOC(b->conv, sizeof(int) * nmol);
   BALLOC(b->next, sizeof(int));
   BALLOC(b->status, sizeof(int));
+  BALLOC(b->phase, sizeof(unsigned long long) * BT_PHASES);
   BALLOC(b->epairs, sizeof(double) * (maxpairs + 1));
 #undef BALLOC
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
@@ -989,7 +1230,7 @@ extern "C" int mb_batch_create(int nmol, const int* numat, const int* nat, const
     return r;
   }
   b->grid = std::min(nmol, sms * per);
-  e = cudaMalloc((void**)&b->scratch, sizeof(double) * 3 * BT_NMAX * BT_NMAX * (size_t)b->grid);
+  e = cudaMalloc((void**)&b->scratch, sizeof(double) * BT_SCR * (size_t)b->grid);
   if (e != cudaSuccess) {
     int r = mb_set_cuda_error(e, "mb_batch_create scratch", __FILE__, __LINE__);
     batch_free(b);
@@ -1023,12 +1264,10 @@ extern "C" int mb_batch_run(mb_batch* b, const mb_scf_opts* opts_in, double* esc
   A.h = b->h;
   A.w = b->w;
   A.wrow = b->wrow;
-  A.lim = b->lim;
   A.cum = b->cum;
   A.pdiag = b->pdiag;
   A.f = b->f;
   A.p = b->p;
-  A.pa = b->pa;
   A.pold = b->pold;
   A.pold2 = b->pold2;
   A.scratch = b->scratch;
@@ -1039,7 +1278,8 @@ extern "C" int mb_batch_run(mb_batch* b, const mb_scf_opts* opts_in, double* esc
   A.homo = b->homo;
   A.lumo = b->lumo;
   A.next = b->next;
-  A.status = b->status;
+  A.phase = b->timing ? b->phase : nullptr;
+  if (b->timing) MB_CUDA(cudaMemsetAsync(b->phase, 0, sizeof(unsigned long long) * BT_PHASES, b->stream));
   A.itrmax = o.itrmax;
   A.scfcrt = o.scfcrt;
   cudaEvent_t e0, e1;
@@ -1059,6 +1299,18 @@ extern "C" int mb_batch_run(mb_batch* b, const mb_scf_opts* opts_in, double* esc
   if (escf) MB_CUDA(cudaMemcpy(escf, b->escf, sizeof(double) * b->nmol, cudaMemcpyDeviceToHost));
   if (niter) MB_CUDA(cudaMemcpy(niter, b->niter, sizeof(int) * b->nmol, cudaMemcpyDeviceToHost));
   if (converged) MB_CUDA(cudaMemcpy(converged, b->conv, sizeof(int) * b->nmol, cudaMemcpyDeviceToHost));
+  return MB_OK;
+}
+
+extern "C" int mb_batch_set_phase_timing(mb_batch* b, int on) {
+  if (!b) return mb_set_error(MB_ERR_ARG, "mb_batch_set_phase_timing: null batch");
+  b->timing = on != 0;
+  return MB_OK;
+}
+
+extern "C" int mb_batch_phase_cycles(mb_batch* b, unsigned long long* out) {
+  if (!b || !out) return mb_set_error(MB_ERR_ARG, "mb_batch_phase_cycles: bad args");
+  MB_CUDA(cudaMemcpy(out, b->phase, sizeof(unsigned long long) * BT_PHASES, cudaMemcpyDeviceToHost));
   return MB_OK;
 }
 
