@@ -25,6 +25,12 @@ between steps anyway).  The headline metric is SCF single points per second
               times the CPU implementation of the same SCF (the oracle's C
               kernels with LAPACK dsyevd through numpy) on the host cores on a
               bounded sample and extrapolates to one SCF; N > 1: rank 0 only.
+--batch N     also measure the batched workload (default 4096 seeded linear
+              alkanes C3-C20, one persistent launch, a CTA per molecule SCF):
+              batched SCFs/s on device-resident integrals, the same through
+              the C ABI from host coordinates (integrals included), the plain
+              FP64 GPU path (one molecule at a time) and the CPU oracle on
+              samples; reported under "batched".  0 skips it.
 Multi-GPU: replicas only (independent SCFs per rank, no data-path collective).
 """
 from __future__ import annotations
@@ -44,6 +50,8 @@ sys.path.insert(0, ROOT)
 
 WORKLOAD = "(H2O)512 water box, PM7 1SCF, RHF closed shell, 1536 atoms, 3072 basis functions, 2048 occupied"
 METRIC = "scf_single_points_per_s"
+BATCH_WORKLOAD = ("linear alkanes C3H8..C20H42, seeded random staggered conformers (no syn-pentane pairs), "
+                  "PM7 1SCF each, RHF closed shell, 11-62 atoms, 20-122 basis functions")
 # Iterations the reference algorithm needs on this input from the standard
 # guess with full diagonalisation each iteration (same for the CPU oracle and
 # the GPU plain path; used to scale the CPU sample to one SCF).
@@ -61,6 +69,7 @@ def parse():
     ap.add_argument("--nwater", type=int, default=512)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--batch", type=int, default=4096)
     return ap.parse_args()
 
 
@@ -148,6 +157,117 @@ def cpu_sample(nwater: int, iters: int = 1):
     return (time.perf_counter() - t0) / iters
 
 
+def _cpu_one(mol):
+    """One molecule's SCF with the CPU oracle (a pool worker's task)."""
+    from oracle import scf_oracle as so
+    r = so.iter_scf(so.make_system(mol[0], mol[1]))
+    return r.escf
+
+
+def cpu_batch_rate(mols, nsample: int, workers: int):
+    """SCF/s of the CPU oracle over an evenly spaced sample of the molecules,
+    `workers` processes (spawned) each running whole SCFs with one BLAS
+    thread; the pool is warmed on one molecule per worker first."""
+    import multiprocessing as mp
+    step = max(1, len(mols) // nsample)
+    sample = mols[::step][:nsample]
+    old = os.environ.get("OPENBLAS_NUM_THREADS")
+    os.environ["OPENBLAS_NUM_THREADS"] = "1"
+    try:
+        with mp.get_context("spawn").Pool(workers) as pool:
+            pool.map(_cpu_one, mols[:workers], chunksize=1)
+            t0 = time.perf_counter()
+            pool.map(_cpu_one, sample, chunksize=1)
+            dt = time.perf_counter() - t0
+    finally:
+        if old is None:
+            os.environ.pop("OPENBLAS_NUM_THREADS", None)
+        else:
+            os.environ["OPENBLAS_NUM_THREADS"] = old
+    return len(sample) / dt, len(sample)
+
+
+def run_batch(args, flush, L):
+    """The batched workload on this GPU; returns the "batched" object."""
+    import numpy as np
+    import torch
+    from mopac_gpu_b200 import ScfContext, workloads
+    from mopac_gpu_b200.batch import Batch
+    mols = workloads.alkane_batch(args.batch)
+    nat_tot = sum(len(m[0]) for m in mols)
+    b = Batch(mols)
+    for _ in range(args.warmup):
+        b.run()
+    times = []
+    l0 = L.mb_launch_count()
+    for _ in range(args.steps):
+        flush.fill_(1.0)
+        torch.cuda.synchronize()
+        escf, niter, conv, t_ms = b.run()
+        times.append(t_ms)
+    launches = L.mb_launch_count() - l0
+    t_ms = statistics.mean(times)
+    b.set_phase_timing(True)
+    b.run()
+    ph = b.phase_cycles()
+    b.set_phase_timing(False)
+    tot = max(1, sum(ph.values()))
+    b.close()
+    # through the C ABI from host coordinates: create (H2D of the atoms,
+    # integrals on the GPU), run, read the heats back, destroy
+    e2e_t = []
+    for step in range(args.steps + 1):
+        flush.fill_(1.0)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        bb = Batch(mols)
+        e2, _, _, _ = bb.run()
+        bb.close()
+        torch.cuda.synchronize()
+        if step > 0:
+            e2e_t.append(time.perf_counter() - t0)
+    te = statistics.mean(e2e_t)
+    # the plain FP64 GPU path, one molecule at a time, on a sample
+    nplain = min(32, len(mols))
+    stepp = max(1, len(mols) // nplain)
+    idx = list(range(0, len(mols), stepp))[:nplain]
+    plain_ms, dhf = [], []
+    for m in idx:
+        ctx = ScfContext(*mols[m])
+        ctx.hcore()
+        ctx.run(pseudo=False, precision=0)
+        r = ctx.run(pseudo=False, precision=0)
+        plain_ms.append(r.t_total_ms)
+        dhf.append(abs(r.escf - escf[m]))
+        ctx.close()
+    plain_rate = len(idx) / (sum(plain_ms) / 1000.0)
+    out = {
+        "workload": f"{len(mols)} {BATCH_WORKLOAD}",
+        "metric": "batched_scfs_per_s", "value": len(mols) / (t_ms / 1000.0), "unit": "SCF/s",
+        "ms_per_step": t_ms, "steps": args.steps, "warmup": args.warmup, "dtype": "f64",
+        "l2": "flushed between steps (256 MB write)",
+        "atoms": nat_tot, "niter_mean": float(np.mean(niter)), "niter_max": int(niter.max()),
+        "converged_fraction": float(conv.mean()),
+        "gpu_launches_per_step": int(launches // max(1, args.steps)),
+        "phase_share": {k: round(v / tot, 4) for k, v in ph.items()},
+        "plain_fp64_gpu": {"value": plain_rate, "unit": "SCF/s", "sample": len(idx),
+                           "mode": "one molecule at a time through mb_scf_run, full FP64 eigensolve every "
+                                   "iteration, integrals resident",
+                           "max_abs_dHf_vs_batched_kcal_mol": float(max(dhf))},
+        "speedup_vs_plain_fp64": (len(mols) / (t_ms / 1000.0)) / plain_rate,
+        "e2e": {"value": len(mols) / te, "unit": "SCF/s", "h2d_bytes_per_step": 28 * nat_tot + 4 * len(mols),
+                "d2h_bytes_per_step": 8 * len(mols), "wall_s": te,
+                "includes": "batch creation (atoms to the device, integrals on the GPU), SCFs, heats to the host"},
+    }
+    if not args.no_cpu_baseline:
+        workers = os.cpu_count() or 1
+        rate, ns = cpu_batch_rate(mols, 8 * workers, workers)
+        out["cpu_baseline"] = {"value": rate, "unit": "SCF/s", "cores": workers, "kind": "port",
+                               "sample": f"{ns} evenly spaced molecules of the batch, one whole oracle SCF per "
+                                         f"task, {workers} spawned processes"}
+    return out
+
+
 def run_reference(args):
     ws, rank, _ = dist_init()
     if rank != 0:
@@ -174,6 +294,14 @@ def run_reference(args):
                                    f"scaled by {CPU_NITER_FALLBACK} iterations to one SCF"},
         "e2e": {"value": val, "unit": "SCF/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    if args.batch > 0:
+        from mopac_gpu_b200 import workloads
+        mols = workloads.alkane_batch(args.batch)
+        rate, ns = cpu_batch_rate(mols, 8 * cores, cores)
+        line["batched"] = {"workload": f"{len(mols)} {BATCH_WORKLOAD}", "metric": "batched_scfs_per_s",
+                           "value": rate, "unit": "SCF/s", "cores": cores, "kind": "port",
+                           "sample": f"{ns} evenly spaced molecules of the batch, one whole oracle SCF per "
+                                     f"task, {cores} spawned processes"}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -285,6 +413,8 @@ def run_mine(args):
         cpu = {"value": 1.0 / t_scf, "unit": "SCF/s", "cores": os.cpu_count(), "kind": "port",
                "sample": f"one SCF iteration of the CPU oracle (fock2 in C, LAPACK dsyevd, density, cnvg) "
                          f"scaled by {CPU_NITER_FALLBACK} iterations", "scf_wall_s": t_scf}
+    # the batched workload is a one-GPU measurement (skipped under torchrun)
+    batched = run_batch(args, flush, L) if args.batch > 0 and ws == 1 else None
     if rank == 0:
         line = {
             "metric": METRIC, "value": ws * 1000.0 / t_ms, "unit": "SCF/s", "n_gpus": ws, "steps": args.steps,
@@ -311,6 +441,7 @@ def run_mine(args):
             "kernel_ms": {k: v["total_ms"] / max(1, args.steps) for k, v in kst.items()},
             "cpu_baseline": cpu,
             "e2e": e2e,
+            "batched": batched,
         }
         print(json.dumps(line), flush=True)
     ctx.close()

@@ -26,6 +26,7 @@ class Batch:
         check(lib().mb_batch_create(self.nmol, self.numat.ctypes.data, nat.ctypes.data, xyz.ctypes.data,
                                     ctypes.byref(self._h)))
         self.norbs = [int(np.where(n == 1, 1, 4).sum()) for n in nats]
+        self._nats = nats
 
     def run(self, scfcrt: float = 1.0e-4, itrmax: int = 2000):
         o = ScfOpts()
@@ -57,6 +58,18 @@ class Batch:
         p = np.empty(n * (n + 1) // 2)
         check(lib().mb_batch_get_density(self._h, int(m), p.ctypes.data))
         return p
+
+    def hw(self, m: int):
+        """(H packed, W, enuclr) of molecule m as the batch computed them."""
+        lim = np.where(self._nats[m] == 1, 1, 10)
+        cum = np.concatenate([[0], np.cumsum(lim)[:-1]])
+        n2 = int((lim * (cum + lim)).sum())
+        n = self.norbs[m]
+        h = np.empty(n * (n + 1) // 2)
+        w = np.empty(n2)
+        en = ctypes.c_double()
+        check(lib().mb_batch_get_hw(self._h, int(m), h.ctypes.data, w.ctypes.data, ctypes.byref(en)))
+        return h, w, en.value
 
     def close(self):
         if getattr(self, "_h", None) is not None and self._h.value:

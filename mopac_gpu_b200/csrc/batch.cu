@@ -33,10 +33,7 @@
 #include "mb_common.cuh"
 #include "pm7_params.h"
 
-extern "C" int mb_hcore_dev(const int* nat_d, const double* coord_d, const MbAtomsDev* at, int numat, double* h,
-                            double* w, double* enuc_pairs, cudaStream_t stream);
-extern "C" int mb_hcore_finish(int numat, const MbAtomsDev* at, const int* nat_d, double* h, const double* e1b,
-                               double* enuclr_dev, const double* enuc_pairs, cudaStream_t stream);
+extern "C" int mb_hcore_batch_dev(const MbHcoreBatch* b, cudaStream_t stream);
 
 namespace {
 
@@ -1057,7 +1054,7 @@ struct mb_batch {
       *niter = nullptr, *conv = nullptr, *status = nullptr;
   unsigned long long* phase = nullptr;
   bool timing = false;
-  long long* wrow = nullptr;
+  long long *wrow = nullptr, *offs = nullptr;  // offs: pair, atom prefixes (nmol + 1 each), hoff, woff
   double *coord = nullptr, *h = nullptr, *w = nullptr, *pdiag = nullptr, *f = nullptr, *p = nullptr,
          *pold = nullptr, *pold2 = nullptr, *scratch = nullptr, *escf = nullptr, *ee = nullptr, *homo = nullptr,
          *lumo = nullptr, *enuc = nullptr, *epairs = nullptr;
@@ -1070,7 +1067,7 @@ static void batch_free(mb_batch* b) {
   if (!b) return;
   void* ptrs[] = {b->mol, b->order, b->first, b->nor, b->lim, b->cum, b->nat, b->next, b->niter, b->conv, b->status, b->wrow,
                   b->coord, b->h, b->w, b->pdiag, b->f, b->p, b->pold, b->pold2, b->scratch, b->escf, b->ee,
-                  b->homo, b->lumo, b->enuc, b->epairs, b->phase};
+                  b->homo, b->lumo, b->enuc, b->epairs, b->phase, b->offs};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   if (b->stream) cudaStreamDestroy(b->stream);
@@ -1089,7 +1086,8 @@ extern "C" int mb_batch_create(int nmol, const int* numat, const int* nat, const
   std::vector<int> first, nor, lim, cum;
   std::vector<long long> wrow;
   std::vector<double> pdiag;
-  long long hoff = 0, woff = 0, maxpairs = 0;
+  long long hoff = 0, woff = 0, npair = 0;
+  std::vector<long long> offs(4 * (size_t)nmol + 2);  // pair_off, atom_off, hoff, woff
   int aoff = 0, doff = 0;
   for (int m = 0; m < nmol; ++m) {
     Mol& M = b->hmol[m];
@@ -1132,12 +1130,18 @@ extern "C" int mb_batch_create(int nmol, const int* numat, const int* nat, const
     M.doff = doff;
     M.enuclr = 0.0;
     M.atheat = atheat - eat * PM7_FPC9;
+    offs[m] = npair;
+    offs[nmol + 1 + m] = aoff;
+    offs[2 * nmol + 2 + m] = hoff;
+    offs[3 * nmol + 2 + m] = woff;
+    npair += (long long)na * (na - 1) / 2;
     hoff += (long long)ia * (ia + 1) / 2;
     woff += wr;
     doff += ia;
     aoff += na;
-    maxpairs = std::max<long long>(maxpairs, (long long)na * (na - 1) / 2);
   }
+  offs[nmol] = npair;
+  offs[2 * nmol + 1] = aoff;
   b->tot_mp = hoff;
   b->tot_w = woff;
   b->tot_n = doff;
@@ -1170,7 +1174,8 @@ extern "C" int mb_batch_create(int nmol, const int* numat, const int* nat, const
   BALLOC(b->next, sizeof(int));
   BALLOC(b->status, sizeof(int));
   BALLOC(b->phase, sizeof(unsigned long long) * BT_PHASES);
-  BALLOC(b->epairs, sizeof(double) * (maxpairs + 1));
+  BALLOC(b->epairs, sizeof(double) * (npair + 1));
+  BALLOC(b->offs, sizeof(long long) * offs.size());
 #undef BALLOC
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaMemcpy(b->first, first.data(), sizeof(int) * aoff, cudaMemcpyHostToDevice);
@@ -1181,25 +1186,34 @@ extern "C" int mb_batch_create(int nmol, const int* numat, const int* nat, const
   if (e == cudaSuccess) e = cudaMemcpy(b->nat, nat, sizeof(int) * aoff, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(b->coord, coord, sizeof(double) * 3 * aoff, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(b->pdiag, pdiag.data(), sizeof(double) * doff, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(b->offs, offs.data(), sizeof(long long) * offs.size(), cudaMemcpyHostToDevice);
   if (e != cudaSuccess) {
     int r = mb_set_cuda_error(e, "mb_batch_create", __FILE__, __LINE__);
     batch_free(b);
     return r;
   }
-  // integrals per molecule on the GPU (hcore), then E_nuc
-  for (int m = 0; m < nmol; ++m) {
-    const Mol& M = b->hmol[m];
-    MbAtomsDev at;
-    at.numat = M.numat;
-    at.first = b->first + M.aoff;
-    at.nor = b->nor + M.aoff;
-    at.lim = b->lim + M.aoff;
-    at.wrow = b->wrow + M.aoff;
-    at.cum = b->cum + M.aoff;
-    int rc = mb_hcore_dev(b->nat + M.aoff, b->coord + 3 * M.aoff, &at, M.numat, b->h + M.hoff, b->w + M.woff,
-                          b->epairs, b->stream);
-    if (rc == MB_OK)
-      rc = mb_hcore_finish(M.numat, &at, b->nat + M.aoff, b->h + M.hoff, nullptr, b->enuc + m, b->epairs, b->stream);
+  // integrals of every molecule on the GPU in three launches, then E_nuc
+  {
+    MbHcoreBatch hb;
+    hb.nmol = nmol;
+    hb.npair_tot = npair;
+    hb.natom_tot = aoff;
+    hb.pair_off = b->offs;
+    hb.atom_off = b->offs + nmol + 1;
+    hb.hoff = b->offs + 2 * nmol + 2;
+    hb.woff = b->offs + 3 * nmol + 2;
+    hb.nat = b->nat;
+    hb.coord = b->coord;
+    hb.first = b->first;
+    hb.nor = b->nor;
+    hb.lim = b->lim;
+    hb.wrow = b->wrow;
+    hb.cum = b->cum;
+    hb.h = b->h;
+    hb.w = b->w;
+    hb.enuc_pairs = b->epairs;
+    hb.enuclr = b->enuc;
+    const int rc = mb_hcore_batch_dev(&hb, b->stream);
     if (rc != MB_OK) { batch_free(b); return rc; }
   }
   std::vector<double> en(nmol);

@@ -12,6 +12,8 @@
 //                the reference's order (partners below A, then above A), and
 //                the one-centre W block (wstore).
 //   enuc_sum     fixed-order reduction of the pair energies.
+#include <algorithm>
+
 #include "mb_common.cuh"
 #include "pm7_params.h"
 
@@ -585,10 +587,11 @@ __device__ void w_block(int ni, int nj, const double p[4][4], const double ri[23
   }
 }
 
-__global__ void hcore_pairs(int numat, const int* __restrict__ nat, const double* __restrict__ coord, MbAtomsDev at,
-                            double* __restrict__ h, double* __restrict__ w, double* __restrict__ enuc_pairs) {
-  const long long npair = (long long)numat * (numat - 1) / 2;
-  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < npair; q += (long long)gridDim.x * blockDim.x) {
+// Off-diagonal H block, two-centre W block and core-core energy of pair q.
+__device__ void hcore_pair_one(long long q, const int* __restrict__ nat, const double* __restrict__ coord,
+                               const MbAtomsDev& at, double* __restrict__ h, double* __restrict__ w,
+                               double* __restrict__ enuc_pairs) {
+  {
     // pair q -> (i, j), i > j, in the reference loop order
     long long i = (long long)((sqrt(8.0 * (double)q + 1.0) + 1.0) * 0.5);
     while (i * (i - 1) / 2 > q) --i;
@@ -607,7 +610,7 @@ __global__ void hcore_pairs(int numat, const int* __restrict__ nat, const double
     if (dx * dx + dy * dy + dz * dz < 0.00002) {
       for (int x = 0; x < at.lim[ia] * at.lim[ja]; ++x) wb[x] = 0.0;
       enuc_pairs[q] = 0.0;
-      continue;
+      return;
     }
     double p[4][4];
     const double r = rotmat(xi, xj, p);
@@ -618,11 +621,16 @@ __global__ void hcore_pairs(int numat, const int* __restrict__ nat, const double
   }
 }
 
+__global__ void hcore_pairs(int numat, const int* __restrict__ nat, const double* __restrict__ coord, MbAtomsDev at,
+                            double* __restrict__ h, double* __restrict__ w, double* __restrict__ enuc_pairs) {
+  const long long npair = (long long)numat * (numat - 1) / 2;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < npair; q += (long long)gridDim.x * blockDim.x)
+    hcore_pair_one(q, nat, coord, at, h, w, enuc_pairs);
+}
+
 // Diagonal H block of atom A in reference accumulation order + one-centre W.
-__global__ void hcore_diag(int numat, const int* __restrict__ nat, const double* __restrict__ coord, MbAtomsDev at,
-                           double* __restrict__ h, double* __restrict__ w) {
-  const int A = blockIdx.x * blockDim.x + threadIdx.x;
-  if (A >= numat) return;
+__device__ void hcore_atom_one(int A, int numat, const int* __restrict__ nat, const double* __restrict__ coord,
+                               const MbAtomsDev& at, double* __restrict__ h, double* __restrict__ w) {
   const int nA = nat[A], fA = at.first[A], noA = at.nor[A], lA = at.lim[A];
   const Pm7Elem& E = c_P.el[nA];
   double blk[10];
@@ -669,6 +677,56 @@ __global__ void hcore_diag(int numat, const int* __restrict__ nat, const double*
 #undef WS
 }
 
+__global__ void hcore_diag(int numat, const int* __restrict__ nat, const double* __restrict__ coord, MbAtomsDev at,
+                           double* __restrict__ h, double* __restrict__ w) {
+  const int A = blockIdx.x * blockDim.x + threadIdx.x;
+  if (A < numat) hcore_atom_one(A, numat, nat, coord, at, h, w);
+}
+
+// ---- many molecules in one launch: a global pair or atom index is mapped to
+// its molecule by a binary search over the prefix offsets.
+__device__ __forceinline__ int batch_find(const long long* off, int nmol, long long q) {
+  int lo = 0, hi = nmol;  // largest m < nmol with off[m] <= q
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (off[mid] <= q) lo = mid; else hi = mid;
+  }
+  return lo;
+}
+
+__device__ __forceinline__ MbAtomsDev batch_atoms(const MbHcoreBatch& B, int m) {
+  const long long a0 = B.atom_off[m];
+  MbAtomsDev at;
+  at.numat = (int)(B.atom_off[m + 1] - a0);
+  at.first = B.first + a0;
+  at.nor = B.nor + a0;
+  at.lim = B.lim + a0;
+  at.wrow = B.wrow + a0;
+  at.cum = B.cum + a0;
+  return at;
+}
+
+__global__ void hcore_pairs_batch(MbHcoreBatch B) {
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < B.pair_off[B.nmol];
+       q += (long long)gridDim.x * blockDim.x) {
+    const int m = batch_find(B.pair_off, B.nmol, q);
+    const MbAtomsDev at = batch_atoms(B, m);
+    const long long a0 = B.atom_off[m];
+    hcore_pair_one(q - B.pair_off[m], B.nat + a0, B.coord + 3 * a0, at, B.h + B.hoff[m], B.w + B.woff[m],
+                   B.enuc_pairs + B.pair_off[m]);
+  }
+}
+
+__global__ void hcore_diag_batch(MbHcoreBatch B) {
+  for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < B.atom_off[B.nmol];
+       g += (long long)gridDim.x * blockDim.x) {
+    const int m = batch_find(B.atom_off, B.nmol, g);
+    const MbAtomsDev at = batch_atoms(B, m);
+    const long long a0 = B.atom_off[m];
+    hcore_atom_one((int)(g - a0), at.numat, B.nat + a0, B.coord + 3 * a0, at, B.h + B.hoff[m], B.w + B.woff[m]);
+  }
+}
+
 // Fixed-order two-level reduction of the pair energies.
 __global__ void enuc_sum(long long npair, const double* __restrict__ e, double* __restrict__ out) {
   __shared__ double sh[1024];
@@ -681,6 +739,22 @@ __global__ void enuc_sum(long long npair, const double* __restrict__ e, double* 
     __syncthreads();
   }
   if (threadIdx.x == 0) *out = sh[0];
+}
+
+// enuc_sum for every molecule (block m: molecule m, the same order).
+__global__ void enuc_sum_batch(MbHcoreBatch B) {
+  const int m = blockIdx.x;
+  const long long p0 = B.pair_off[m], np = B.pair_off[m + 1] - p0;
+  __shared__ double sh[1024];
+  double s = 0.0;
+  for (long long q = threadIdx.x; q < np; q += blockDim.x) s += B.enuc_pairs[p0 + q];
+  sh[threadIdx.x] = s;
+  __syncthreads();
+  for (int st = blockDim.x / 2; st > 0; st >>= 1) {
+    if (threadIdx.x < st) sh[threadIdx.x] += sh[threadIdx.x + st];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) B.enuclr[m] = np > 0 ? sh[0] : 0.0;
 }
 
 bool g_params_uploaded = false;
@@ -712,6 +786,23 @@ extern "C" int mb_hcore_dev(const int* nat_d, const double* coord_d, const MbAto
     MB_LAUNCH_CHECK();
   }
   hcore_diag<<<(numat + 63) / 64, 64, 0, stream>>>(numat, nat_d, coord_d, *at, h, w);
+  MB_LAUNCH_CHECK();
+  return MB_OK;
+}
+
+extern "C" int mb_hcore_batch_dev(const MbHcoreBatch* b, cudaStream_t stream) {
+  if (!b || b->nmol <= 0) return mb_set_error(MB_ERR_ARG, "mb_hcore_batch_dev: bad args");
+  MB_TRY(upload_params());
+  const long long npair = b->npair_tot, natom = b->natom_tot;
+  if (npair > 0) {
+    const int blocks = (int)std::min<long long>((npair + 127) / 128, 148LL * 32);
+    hcore_pairs_batch<<<blocks, 128, 0, stream>>>(*b);
+    MB_LAUNCH_CHECK();
+  }
+  const int blocks = (int)std::min<long long>((natom + 63) / 64, 148LL * 32);
+  hcore_diag_batch<<<blocks, 64, 0, stream>>>(*b);
+  MB_LAUNCH_CHECK();
+  enuc_sum_batch<<<b->nmol, 1024, 0, stream>>>(*b);
   MB_LAUNCH_CHECK();
   return MB_OK;
 }

@@ -66,3 +66,28 @@ struct MbAtoms {
   const long long* wrow;
   const int* cum;
 };
+
+// Integrals of many molecules in one launch (device pointers): molecule m
+// owns atoms atom_off[m] .. atom_off[m+1]-1 of the concatenated tables
+// (molecule-local first/wrow/cum), pairs pair_off[m] .. pair_off[m+1]-1 of
+// enuc_pairs, and its packed H and W at hoff[m], woff[m].
+struct MbHcoreBatch {
+  int nmol;
+  long long npair_tot, natom_tot;
+  const long long* pair_off;
+  const long long* atom_off;
+  const long long* hoff;
+  const long long* woff;
+  const int* nat;
+  const double* coord;
+  const int* first;
+  const int* nor;
+  const int* lim;
+  const long long* wrow;
+  const int* cum;
+  double* h;
+  double* w;
+  double* enuc_pairs;
+  double* enuclr;
+};
+

@@ -174,8 +174,13 @@ def _alkane_once(nc: int, rng: np.random.Generator):
     carbons = [np.zeros(3), np.array([cc, 0.0, 0.0])]
     if nc >= 3:
         carbons.append(carbons[1] + cc * np.array([-np.cos(TETRA), np.sin(TETRA), 0.0]))
+    prev = 180.0
     for i in range(3, nc):
-        tor = np.deg2rad(rng.choice([60.0, 180.0, 300.0]) + rng.uniform(-10.0, 10.0))
+        # trans or gauche, never a gauche+ gauche- pair (the syn-pentane clash)
+        choices = [180.0, prev] if prev != 180.0 else [60.0, 180.0, 300.0]
+        t = float(rng.choice(choices))
+        prev = t
+        tor = np.deg2rad(t + rng.uniform(-10.0, 10.0))
         carbons.append(_zmat_place(carbons[i - 3], carbons[i - 2], carbons[i - 1], cc, TETRA, tor))
     carbons = carbons[:nc]
     hs = []

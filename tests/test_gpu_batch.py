@@ -45,6 +45,23 @@ def test_batch_matches_oracle_per_molecule():
     b.close()
 
 
+def test_batch_integrals_match_single_molecule_path():
+    """One launch over all molecules gives each molecule's H, W and E_nuc bit
+    for bit as the one-molecule integral path."""
+    from mopac_gpu_b200 import ScfContext
+    from mopac_gpu_b200.batch import Batch
+    mols = _molecules()
+    b = Batch(mols)
+    for m, (nat, xyz) in enumerate(mols):
+        h, w, en = b.hw(m)
+        ctx = ScfContext(nat, xyz)
+        ctx.hcore()
+        h1, w1, en1 = ctx.get_hw()
+        ctx.close()
+        assert np.array_equal(h, h1) and np.array_equal(w, w1) and en == en1, m
+    b.close()
+
+
 def test_batch_repeat_is_deterministic():
     from mopac_gpu_b200.batch import Batch
     mols = _molecules()[:4] * 3
