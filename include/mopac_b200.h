@@ -89,6 +89,10 @@ typedef struct mb_scf_opts {
   int pulay;         /* 1: Pulay's converger once newdg is set, like the
                         PULAY keyword (SCF/iter.F90:135, :815-831); cnvg is
                         then skipped (:899) and the shift is -8 / 0 (:417) */
+  int guess;         /* 1: start from the density given by mb_ctx_set_guess
+                        or predicted by mb_ctx_guess, entered like an OLDENS
+                        density (SCF/iter.F90:151-158); 0: the standard
+                        diagonal guess                                     */
 } mb_scf_opts;
 
 typedef struct mb_scf_result {
@@ -129,6 +133,11 @@ int mb_ctx_get_hw(mb_ctx* ctx, double* h, double* w, double* enuclr);
  * (moldat.F90:731-760).  The whole loop runs on the device; only scalars
  * cross to the host each iteration. */
 int mb_scf_run(mb_ctx* ctx, const mb_scf_opts* opts, mb_scf_result* res);
+
+/* Starting density for opts.guess = 1: a host packed total density (mpack)
+ * such as a previous SCF's P -- the reference reads one with OLDENS
+ * (SCF/iter.F90:151-158, den_in_out) -- or the learned guess (below). */
+int mb_ctx_set_guess(mb_ctx* ctx, const double* p);
 
 /* Results to host: density P (mpack), eigenvectors C (norbs x norbs,
  * column-major), eigenvalues (norbs), Fock matrix F (mpack). */
@@ -388,6 +397,77 @@ int mb_pseudo_diag_dev(int n, int nocc, const double* fpacked, double* c, const 
 int mb_dgemm_dev(char transa, char transb, int m, int n, int k, double alpha, const double* a,
                  int lda, const double* b, int ldb, double beta, double* c, int ldc,
                  cudaStream_t stream);
+
+/* ------------------------------------------------ learned initial guess
+ * No counterpart in the reference (which starts from moldat.F90:731-760 or an
+ * OLDENS density): an atom-pair MLP predicts each pair's density block in a
+ * local frame from radial/angular descriptors within 6 A.  Five pair types
+ * (0 heavy atom's own block, 1 hydrogen's own block, 2 heavy-heavy,
+ * 3 heavy-hydrogen, 4 hydrogen-hydrogen), each with its own network
+ * DIN -> 128 -> 128 -> 128 -> 16 (SiLU), BF16 weights and activations, FP32
+ * accumulation.  The parameter blob is NTYPES consecutive blocks of
+ * MB_GUESS_PER_TYPE floats: in_mean[DIN], in_std[DIN], W1[128][DIN], b1[128],
+ * W2[128][128], b2, W3[128][128], b3, W4[16][128], b4[16], out_mean[16],
+ * out_std[16]. */
+#define MB_GUESS_DIN 336
+#define MB_GUESS_HID 128
+#define MB_GUESS_DOUT 16
+#define MB_GUESS_NTYPES 5
+#define MB_GUESS_PER_TYPE 78928
+typedef struct mb_guess_model mb_guess_model;
+size_t mb_guess_blob_floats(void);
+int mb_guess_model_create(const float* blob, mb_guess_model** out);
+int mb_guess_model_destroy(mb_guess_model* model);
+/* Predicts the context's starting density on the device (H and O only; other
+ * elements return MB_ERR_UNSUPPORTED and the caller keeps the standard guess).
+ * Use with opts.guess = 1. */
+int mb_ctx_guess(mb_ctx* ctx, const mb_guess_model* model);
+/* The steps, on device pointers.  Pairs: counts_host[NTYPES] receives the
+ * per-type counts; with pf == NULL only counting is done; otherwise pf/ps/pt
+ * (first atom, second atom, type) are filled type by type (order inside a
+ * type is unspecified).  work: 15 ints of device scratch. */
+int mb_guess_pairs_dev(int numat, const int* nat, const double* xyz, double rpair, int* counts_host,
+                       int max_pairs, int* pf, int* ps, int* pt, int* work, cudaStream_t stream);
+/* Frames (npairs x 9 doubles, axes as columns) and raw descriptors (npairs x DIN floats). */
+int mb_guess_features_dev(int numat, const int* nat, const double* xyz, int npairs, const int* pf,
+                          const int* ps, float* feat, double* frames, cudaStream_t stream);
+/* Raw descriptors -> normalised BF16 rows (uint16 bit patterns). */
+int mb_guess_normalize_dev(const mb_guess_model* model, int type, int n, const float* raw,
+                           unsigned short* x, cudaStream_t stream);
+/* Raw local blocks -> normalised targets (unused slots 0). */
+int mb_guess_norm_targets_dev(const mb_guess_model* model, int type, int n, const float* yraw,
+                              float* yt, cudaStream_t stream);
+/* Network of one type on n rows: y (n x 16, normalised).  ws: 2*n*128 BF16. */
+int mb_guess_forward_dev(const mb_guess_model* model, int type, int n, const unsigned short* x,
+                         float* y, void* ws, cudaStream_t stream);
+/* Local blocks (network output) -> packed density p (pairs not listed are
+ * left untouched); first (0-based) and nor per atom as in MbAtomsDev. */
+int mb_guess_assemble_dev(const mb_guess_model* model, int npairs, const int* pf, const int* ps,
+                          const int* pt, const double* frames, const float* y, const int* first,
+                          const int* nor, double* p, cudaStream_t stream);
+/* Training targets: each pair's block of a packed density in its frame (npairs x 16, raw). */
+int mb_guess_targets_dev(int npairs, const int* pf, const int* ps, const int* pt,
+                         const double* frames, const int* first, const int* nor, const double* p,
+                         float* yraw, cudaStream_t stream);
+/* All of the above for one molecule: p (mpack) is overwritten. */
+int mb_guess_predict_density_dev(const mb_guess_model* model, int numat, const int* nat,
+                                 const double* xyz, const int* first, const int* nor, int norbs,
+                                 double* p, cudaStream_t stream);
+/* Training on the device: FP32 master weights, BF16 copies for the GEMMs,
+ * Adam.  mb_guess_trainer_model returns a model view of the current weights. */
+typedef struct mb_guess_trainer mb_guess_trainer;
+int mb_guess_trainer_create(const float* blob, int max_rows, mb_guess_trainer** out);
+int mb_guess_trainer_destroy(mb_guess_trainer* trainer);
+const mb_guess_model* mb_guess_trainer_model(mb_guess_trainer* trainer);
+int mb_guess_trainer_set_norm(mb_guess_trainer* trainer, int type, const float* in_mean,
+                              const float* in_std, const float* out_mean, const float* out_std);
+/* Forward, MSE over the type's valid outputs, backward; update != 0 applies
+ * an Adam step (lr).  loss_out (optional) synchronises and returns the loss. */
+int mb_guess_trainer_step(mb_guess_trainer* trainer, int type, int n, const unsigned short* x,
+                          const float* yt, float lr, int update, double* loss_out,
+                          cudaStream_t stream);
+/* Copies the parameter blob and the last step's gradients (same layout) to host. */
+int mb_guess_trainer_get(mb_guess_trainer* trainer, float* params, float* grads);
 
 /* ------------------------------------- (1) reference bind(C) symbols */
 /* src/gpu/cuda_wrappers.cu:192 (cublas_interfaces.F90:9-21) */

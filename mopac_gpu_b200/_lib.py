@@ -46,7 +46,7 @@ class MbMzLmos(ctypes.Structure):
 class ScfOpts(ctypes.Structure):
     _fields_ = [("pseudo", ctypes.c_int), ("itrmax", ctypes.c_int), ("scfcrt", ctypes.c_double),
                 ("precision", ctypes.c_int), ("switch_pl", ctypes.c_double), ("verbose", ctypes.c_int),
-                ("pulay", ctypes.c_int)]
+                ("pulay", ctypes.c_int), ("guess", ctypes.c_int)]
 
 
 class ScfRes(ctypes.Structure):
@@ -155,6 +155,25 @@ SIGNATURES = {
     "density_for_gpu_": ([_P] * 10, None),
     "eigenvectors_lapack_": ([_P] * 4, None),
     "diag_for_gpu_": ([_P] * 6, None),
+    "mb_ctx_set_guess": ([_P, _P], _I),
+    "mb_ctx_guess": ([_P, _P], _I),
+    "mb_guess_blob_floats": ([], ctypes.c_size_t),
+    "mb_guess_model_create": ([_P, ctypes.POINTER(_P)], _I),
+    "mb_guess_model_destroy": ([_P], _I),
+    "mb_guess_pairs_dev": ([_I, _P, _P, _D, _P, _I, _P, _P, _P, _P, _P], _I),
+    "mb_guess_features_dev": ([_I, _P, _P, _I, _P, _P, _P, _P, _P], _I),
+    "mb_guess_normalize_dev": ([_P, _I, _I, _P, _P, _P], _I),
+    "mb_guess_norm_targets_dev": ([_P, _I, _I, _P, _P, _P], _I),
+    "mb_guess_forward_dev": ([_P, _I, _I, _P, _P, _P, _P], _I),
+    "mb_guess_assemble_dev": ([_P, _I, _P, _P, _P, _P, _P, _P, _P, _P, _P], _I),
+    "mb_guess_targets_dev": ([_I, _P, _P, _P, _P, _P, _P, _P, _P, _P], _I),
+    "mb_guess_predict_density_dev": ([_P, _I, _P, _P, _P, _P, _I, _P, _P], _I),
+    "mb_guess_trainer_create": ([_P, _I, ctypes.POINTER(_P)], _I),
+    "mb_guess_trainer_destroy": ([_P], _I),
+    "mb_guess_trainer_model": ([_P], _P),
+    "mb_guess_trainer_set_norm": ([_P, _I, _P, _P, _P, _P], _I),
+    "mb_guess_trainer_step": ([_P, _I, _I, _P, _P, ctypes.c_float, _I, ctypes.POINTER(_D), _P], _I),
+    "mb_guess_trainer_get": ([_P, _P, _P], _I),
 }
 
 

@@ -153,6 +153,9 @@ struct mb_ctx {
   void* tc_ws_raw = nullptr;
   void* tc_ws = nullptr;     // 1024-byte aligned inside tc_ws_raw
   size_t tc_ws_bytes = 0;
+  // starting density for opts.guess (mb_ctx_set_guess / mb_ctx_guess)
+  double* pguess = nullptr;
+  bool have_guess = false;
   cudaStream_t stream = nullptr;
 };
 
@@ -164,7 +167,7 @@ static void ctx_free(mb_ctx* c) {
   mb_atoms_destroy(&c->atoms);
   void* ptrs[] = {c->d_nat, c->d_coord, c->h, c->w, c->f, c->p, c->pa, c->pold, c->pold2, c->c, c->eigs,
                   c->fdiag, c->scal, c->hws, c->status, c->nrot, c->eig_ws, c->pseudo_ws,
-                  c->fppf_hist, c->fock_hist, c->tc_ws_raw};
+                  c->fppf_hist, c->fock_hist, c->tc_ws_raw, c->pguess};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -179,6 +182,7 @@ extern "C" void mb_scf_opts_default(mb_scf_opts* o) {
   o->switch_pl = 1.0e-4;
   o->verbose = 0;
   o->pulay = 0;
+  o->guess = 0;
 }
 
 extern "C" int mb_ctx_create(int numat, const int* nat, const double* coord, mb_ctx** out) {
@@ -345,6 +349,37 @@ extern "C" int mb_ctx_atoms_dev(mb_ctx* c, MbAtomsDev* out) {
   return MB_OK;
 }
 
+extern "C" int mb_guess_predict_density_dev(const mb_guess_model* m, int numat, const int* nat, const double* xyz,
+                                            const int* first, const int* nor, int norbs, double* p, cudaStream_t s);
+
+static int ensure_guess_buffer(mb_ctx* c) {
+  if (!c->pguess) MB_CUDA(cudaMalloc(&c->pguess, sizeof(double) * (size_t)c->mpack));
+  return MB_OK;
+}
+
+extern "C" int mb_ctx_set_guess(mb_ctx* c, const double* p) {
+  if (!c || !p) return mb_set_error(MB_ERR_ARG, "mb_ctx_set_guess: bad args");
+  MB_TRY(ensure_guess_buffer(c));
+  MB_CUDA(cudaMemcpyAsync(c->pguess, p, sizeof(double) * (size_t)c->mpack, cudaMemcpyHostToDevice, c->stream));
+  MB_CUDA(cudaStreamSynchronize(c->stream));
+  c->have_guess = true;
+  return MB_OK;
+}
+
+extern "C" int mb_ctx_guess(mb_ctx* c, const mb_guess_model* m) {
+  if (!c || !m) return mb_set_error(MB_ERR_ARG, "mb_ctx_guess: bad args");
+  for (int a = 0; a < c->numat; ++a)
+    if (c->nat[a] != 1 && c->nat[a] != 8)
+      return mb_set_error(MB_ERR_UNSUPPORTED, "mb_ctx_guess: the network is trained on H and O only");
+  MB_TRY(ensure_guess_buffer(c));
+  c->have_guess = false;
+  MB_TRY(mb_guess_predict_density_dev(m, c->numat, c->d_nat, c->d_coord, c->atoms.first, c->atoms.nor, c->norbs,
+                                      c->pguess, c->stream));
+  MB_CUDA(cudaStreamSynchronize(c->stream));
+  c->have_guess = true;
+  return MB_OK;
+}
+
 // ---------------------------------------------------------------- kernels
 namespace {
 __global__ void half_kernel(long long n, const double* __restrict__ p, double* __restrict__ pa) {
@@ -354,6 +389,20 @@ __global__ void half_kernel(long long n, const double* __restrict__ p, double* _
 __global__ void add_tail_kernel(int n, int from, double* e, double s) {
   int i = from + blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) e[i] = e[i] + s;
+}
+// Starting state from a supplied density, as iter sets it up after reading
+// one with OLDENS (iter.F90:151-158, RHF): pa = p/2 and pold = 2*pa.  That
+// branch leaves pold2 as allocated; here it starts as the diagonal of p.
+__global__ void guess_start_kernel(int n, long long mpack, const double* __restrict__ g, double* __restrict__ p,
+                                   double* __restrict__ pa, double* __restrict__ pold, double* __restrict__ pold2) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < mpack; i += (long long)gridDim.x * blockDim.x) {
+    double v = g[i];
+    p[i] = v;
+    pa[i] = v * 0.5;
+    pold[i] = (v * 0.5) * 2.0;
+  }
+  for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < n; r += (long long)gridDim.x * blockDim.x)
+    pold2[r] = g[r * (r + 1) / 2 + r];
 }
 }  // namespace
 
@@ -471,6 +520,11 @@ extern "C" int mb_scf_run(mb_ctx* c, const mb_scf_opts* opts_in, mb_scf_result* 
     MB_CUDA(cudaMemcpyAsync(pold, hpa.data(), sizeof(double) * mpack, cudaMemcpyHostToDevice, s));
     MB_CUDA(cudaMemcpyAsync(pold2, hpd.data(), sizeof(double) * n, cudaMemcpyHostToDevice, s));
     MB_CUDA(cudaStreamSynchronize(s));
+  }
+  if (opts.guess) {
+    if (!c->have_guess) return mb_set_error(MB_ERR_ARG, "mb_scf_run: opts.guess needs mb_ctx_set_guess or mb_ctx_guess");
+    guess_start_kernel<<<148, 256, 0, s>>>(n, mpack, c->pguess, c->p, c->pa, pold, pold2);
+    MB_LAUNCH_CHECK();
   }
   const double gnorm = 0.0;
   double selcon = opts.scfcrt;

@@ -68,8 +68,21 @@ class ScfContext:
         return h, w, e.value
 
     # -- SCF
+    def set_guess(self, p: np.ndarray) -> None:
+        """Starting density for ``run(guess=True)`` (packed, host), entered like
+        a density read with OLDENS (SCF/iter.F90:151-158)."""
+        p = np.ascontiguousarray(p, dtype=np.float64)
+        assert p.size == self.mpack
+        check(lib().mb_ctx_set_guess(self._h, p.ctypes.data))
+
+    def learned_guess(self, model) -> None:
+        """Starting density predicted on the device by the atom-pair network
+        (``guess.GuessModel``); use with ``run(guess=True)``."""
+        check(lib().mb_ctx_guess(self._h, model.handle))
+
     def run(self, pseudo: bool = False, scfcrt: float = 1.0e-4, itrmax: int = 2000, precision: int = 0,
-            switch_pl: float = 1.0e-4, verbose: bool = False, pulay: bool = False) -> ScfResult:
+            switch_pl: float = 1.0e-4, verbose: bool = False, pulay: bool = False,
+            guess: bool = False) -> ScfResult:
         o = ScfOpts()
         lib().mb_scf_opts_default(ctypes.byref(o))
         o.pseudo = int(pseudo)
@@ -79,6 +92,7 @@ class ScfContext:
         o.switch_pl = switch_pl
         o.verbose = int(verbose)
         o.pulay = int(pulay)
+        o.guess = int(guess)
         r = ScfRes()
         check(lib().mb_scf_run(self._h, ctypes.byref(o), ctypes.byref(r)))
         return ScfResult(r.escf, r.ee, r.niter, bool(r.converged), r.n_full_diag, r.n_pseudo_diag, r.pl,

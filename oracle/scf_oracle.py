@@ -423,9 +423,14 @@ class ScfResult:
 
 
 def iter_scf(s: System, pseudo: bool = False, scfcrt: float = 1.0e-4, itrmax: int = 2000,
-             gnorm: float = 0.0, trace: bool = False, pulay_on: bool = False) -> ScfResult:
+             gnorm: float = 0.0, trace: bool = False, pulay_on: bool = False,
+             p_guess: np.ndarray | None = None) -> ScfResult:
     """Closed-shell restatement of iter (SCF/iter.F90), 1SCF settings
-    (last = 1, nscf = 0, fulscf = .true.)."""
+    (last = 1, nscf = 0, fulscf = .true.).
+
+    p_guess: a starting total density (packed).  It enters like a density
+    read with OLDENS (iter.F90:151-158: pa = p/2, pold = 2*pa); pold2, which
+    that branch leaves as allocated, starts as the diagonal of p."""
     n = s.norbs
     mpack = s.mpack
     nclose = s.nclose
@@ -462,10 +467,16 @@ def iter_scf(s: System, pseudo: bool = False, scfcrt: float = 1.0e-4, itrmax: in
         p[j] = s.pdiag[i]
         pa[j] = p[j] * w1 * random
         random = 1.0 / random
-    if pst is not None:
+    if p_guess is not None:
+        p = np.array(p_guess, dtype=np.float64)
+        pa = p * 0.5
+    if p_guess is not None and pst is None:
+        pold = pa * 2.0
+        pold2 = pold[dix].copy()
+    elif pst is not None:
         # pold and pold2 are the heads of pulay's two history arrays
         pold = pst.fppf[:mpack]
-        pold[:] = pa
+        pold[:] = pa if p_guess is None else pa * 2.0
         pold2 = pst.fock[:n]
         pold2[:] = pold[dix]
     else:
