@@ -25,6 +25,13 @@ between steps anyway).  The headline metric is SCF single points per second
               times the CPU implementation of the same SCF (the oracle's C
               kernels with LAPACK dsyevd through numpy) on the host cores on a
               bounded sample and extrapolates to one SCF; N > 1: rank 0 only.
+--guess learned (default when the trained blob mopac_gpu_b200/data/
+              guess_pm7_water.npy exists) each step starts from the atom-pair
+              network's density (prediction on the device, inside the timed
+              region); standard: the reference's diagonal guess.  The line
+              also gives the SCF from the standard guess and a sample of the
+              learned-guess evaluation on held-out (H2O)_n lattice clusters
+              (n = 32..128) under "learned_guess".
 --batch N     also measure the batched workload (default 4096 seeded linear
               alkanes C3-C20, one persistent launch, a CTA per molecule SCF):
               batched SCFs/s on device-resident integrals, the same through
@@ -70,6 +77,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--batch", type=int, default=4096)
+    ap.add_argument("--guess", choices=["learned", "standard"], default="learned")
+    ap.add_argument("--guess-sample", type=int, default=40)
     return ap.parse_args()
 
 
@@ -325,6 +334,22 @@ def run_mine(args):
     ctx = ScfContext(nat, xyz)
     ctx.hcore()
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    from mopac_gpu_b200.guess import GuessModel
+    model = GuessModel() if args.guess == "learned" and GuessModel.available() else None
+    guess_note = "learned (atom-pair network, prediction inside the timed step)" if model else (
+        "standard diagonal guess" + (" (no trained blob found)" if args.guess == "learned" else ""))
+
+    def scf_step(c):
+        """One step: (prediction +) SCF; returns (result, step ms, prediction ms)."""
+        if model is None:
+            rr = c.run(pseudo=pseudo, precision=prec)
+            return rr, rr.t_total_ms, 0.0
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        c.learned_guess(model)
+        tp = (time.perf_counter() - t0) * 1e3
+        rr = c.run(pseudo=pseudo, precision=prec, guess=True)
+        return rr, tp + rr.t_total_ms, tp
 
     def barrier():
         torch.cuda.synchronize()
@@ -332,7 +357,7 @@ def run_mine(args):
             dist.barrier()
 
     for _ in range(args.warmup):
-        r = ctx.run(pseudo=pseudo, precision=prec)
+        r, _, _ = scf_step(ctx)
     # ---- timed region (device-resident inputs)
     clocks = ClockSampler(local)
     barrier()
@@ -341,12 +366,13 @@ def run_mine(args):
     L.mb_kstats_enable(1)
     clocks.start()
     l0 = L.mb_launch_count()
-    times, results = [], []
+    times, results, pred_ms = [], [], []
     for _ in range(args.steps):
         flush.fill_(1.0)
         torch.cuda.synchronize()
-        r = ctx.run(pseudo=pseudo, precision=prec)
-        times.append(r.t_total_ms)
+        r, tstep, tp = scf_step(ctx)
+        times.append(tstep)
+        pred_ms.append(tp)
         results.append(r)
     barrier()
     launches = L.mb_launch_count() - l0
@@ -376,7 +402,7 @@ def run_mine(args):
             barrier()
             t0 = time.perf_counter()
             L.mb_ctx_set_hw(ctx._h, hp.data_ptr(), wp.data_ptr(), enuc)
-            rr = ctx.run(pseudo=pseudo, precision=prec)
+            rr, _, _ = scf_step(ctx)
             L.mb_ctx_get_density(ctx._h, pout.data_ptr())
             torch.cuda.synchronize()
             if step > 0:
@@ -404,7 +430,29 @@ def run_mine(args):
             plain_ms.append(rp.t_total_ms)
         r64 = rp
     plain = {"scf_wall_s": statistics.mean(plain_ms) / 1000.0, "niter": r64.niter, "escf_kcal_mol": r64.escf,
-             "mode": "full FP64 eigensolve every iteration, FP64 GEMMs", "steps": len(plain_ms)}
+             "mode": "full FP64 eigensolve every iteration, FP64 GEMMs, standard guess", "steps": len(plain_ms)}
+    # the same fast path from the standard guess (what the network adds)
+    std = None
+    if model is not None:
+        sm = []
+        for i in range(3):
+            flush.fill_(1.0)
+            torch.cuda.synchronize()
+            rs = ctx.run(pseudo=pseudo, precision=prec)
+            if i > 0:
+                sm.append(rs.t_total_ms)
+        std = {"scf_wall_s": statistics.mean(sm) / 1000.0, "niter": rs.niter,
+               "abs_dHf_vs_learned_kcal_mol": abs(rs.escf - r.escf)}
+    guess_eval = None
+    if model is not None and args.guess_sample > 0 and rank == 0:
+        from mopac_gpu_b200.guess import evaluate
+        ev = evaluate(model, n_clusters=args.guess_sample, nmin=32, nmax=128, seed=777)
+        guess_eval = {"workload": "held-out (H2O)_n lattice clusters (as the 16-water case), n ~ U{32..128}, "
+                                  "PM7 1SCF, plain FP64 path, standard vs learned guess",
+                      "clusters": ev.n_clusters, "niter_standard": ev.niter_std, "niter_learned": ev.niter_learned,
+                      "ms_standard": ev.ms_std, "ms_learned_incl_prediction": ev.ms_learned,
+                      "speedup": ev.ms_std / ev.ms_learned, "max_abs_dHf_kcal_mol": ev.max_dhf,
+                      "fallbacks": ev.n_fallback}
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         os.environ.setdefault("OPENBLAS_NUM_THREADS", str(os.cpu_count()))
@@ -421,11 +469,15 @@ def run_mine(args):
             "warmup": args.warmup, "ms_per_step": t_ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64" if prec == 0 else "f64+bf16x3",
             "data": "synthetic (seeded water box, random sequential insertion)",
-            "config": {"workload": WORKLOAD, "mode": args.mode, "precision": args.precision,
+            "config": {"workload": WORKLOAD, "mode": args.mode, "precision": args.precision, "guess": args.guess,
                        "parallelism": f"replicas x{ws}",
                        "l2": "flushed between steps (256 MB write); W = 151 MB > L2",
                        "cell_edge_A": round(edge, 3)},
             "scf_wall_s": t_ms / 1000.0,
+            "guess": guess_note,
+            "guess_prediction_ms": statistics.mean(pred_ms),
+            "standard_guess_same_path": std,
+            "learned_guess": guess_eval,
             "scf": {"escf_kcal_mol": r.escf, "niter": r.niter, "full_diag": r.n_full_diag,
                     "pseudo_diag": r.n_pseudo_diag, "split_iterations": r.n_split, "converged": r.converged,
                     "abs_dHf_vs_fp64_kcal_mol": abs(r.escf - r64.escf),

@@ -166,6 +166,7 @@ def test_scf_from_supplied_density_follows_oracle(cluster):
     ro = so.iter_scf(s, p_guess=g)
     ctx = ScfContext(nat, xyz)
     ctx.set_hw(s.h, s.w, s.enuclr)
+    ctx.set_guess(g)
     rg = ctx.run(guess=True)
     assert rg.converged and rg.niter == ro.niter
     assert abs(rg.escf - ro.escf) < 1e-6
