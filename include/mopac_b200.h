@@ -401,7 +401,8 @@ int mb_dgemm_dev(char transa, char transb, int m, int n, int k, double alpha, co
 /* ------------------------------------------------ learned initial guess
  * No counterpart in the reference (which starts from moldat.F90:731-760 or an
  * OLDENS density): an atom-pair MLP predicts each pair's density block in a
- * local frame from radial/angular descriptors within 6 A.  Five pair types
+ * local frame from radial/angular descriptors within 6 A and each centre's
+ * long-range electrostatic environment (reference charges).  Five pair types
  * (0 heavy atom's own block, 1 hydrogen's own block, 2 heavy-heavy,
  * 3 heavy-hydrogen, 4 hydrogen-hydrogen), each with its own network
  * DIN -> 128 -> 128 -> 128 -> 16 (SiLU), BF16 weights and activations, FP32
@@ -409,11 +410,11 @@ int mb_dgemm_dev(char transa, char transb, int m, int n, int k, double alpha, co
  * MB_GUESS_PER_TYPE floats: in_mean[DIN], in_std[DIN], W1[128][DIN], b1[128],
  * W2[128][128], b2, W3[128][128], b3, W4[16][128], b4[16], out_mean[16],
  * out_std[16]. */
-#define MB_GUESS_DIN 336
+#define MB_GUESS_DIN 356
 #define MB_GUESS_HID 128
 #define MB_GUESS_DOUT 16
 #define MB_GUESS_NTYPES 5
-#define MB_GUESS_PER_TYPE 78928
+#define MB_GUESS_PER_TYPE 81528
 typedef struct mb_guess_model mb_guess_model;
 size_t mb_guess_blob_floats(void);
 int mb_guess_model_create(const float* blob, mb_guess_model** out);

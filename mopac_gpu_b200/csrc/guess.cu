@@ -17,7 +17,10 @@
 //      bond lengths pick a frame deterministically).  Descriptors: for each
 //      centre, Gaussian radial shells (8, cut off smoothly at 6 A) times ten
 //      angular monomials of the neighbour direction in the frame, per element
-//      class (H, heavy), plus 16 radial functions of the pair distance;
+//      class (H, heavy), plus 16 radial functions of the pair distance, plus
+//      each centre's long-range electrostatic environment (potential, field
+//      and field gradient of fixed reference charges on all other atoms, in
+//      the frame; no cutoff);
 //   3. normalisation to BF16 with per-type statistics;
 //   4. the MLP (DIN -> 128 -> 128 -> 128 -> 16, SiLU) as BF16 tensor-core
 //      GEMMs with FP32 accumulation (mma.sync m16n8k16), one weight set per
@@ -44,6 +47,12 @@ constexpr int PER_CENTER = 160;
 constexpr int NRAD = 8;
 constexpr int NANG = 10;
 constexpr int NPAIR_RBF = 16;
+constexpr int NLR = 10;
+constexpr int LR0 = 2 * PER_CENTER + NPAIR_RBF;
+// reference charges of the long-range descriptor: PM7 Mulliken charges of an
+// isolated water molecule
+constexpr double QREF_H = 0.32226;
+constexpr double QREF_HEAVY = -0.64452;
 constexpr double RC = 6.0;
 constexpr double RAD_SIG = 0.65;
 constexpr double PAIR_SIG = 0.35;
@@ -257,6 +266,35 @@ __global__ void __launch_bounds__(128) features_kernel(int numat, const int* __r
   }
   if (ncent == 1)
     for (int j = lane; j < PER_CENTER; j += 32) out[PER_CENTER + j] = 0.f;
+  // long-range electrostatic environment of each centre (warp-parallel sums)
+  for (int ci = 0; ci < 2; ++ci) {
+    if (ci == 1 && ncent == 1) {
+      if (lane < NLR) out[LR0 + NLR + lane] = 0.f;
+      continue;
+    }
+    const int c = ci == 0 ? f : s;
+    const double cx = xyz[3 * c], cy = xyz[3 * c + 1], cz = xyz[3 * c + 2];
+    double v[NLR];
+    for (int j = 0; j < NLR; ++j) v[j] = 0.0;
+    for (int k = lane; k < numat; k += 32) {
+      if (k == f || k == s) continue;
+      const double q = nat[k] == 1 ? QREF_H : QREF_HEAVY;
+      double gx = DSUB(xyz[3 * k], cx), gy = DSUB(xyz[3 * k + 1], cy), gz = DSUB(xyz[3 * k + 2], cz);
+      double x = DADD(DADD(DMUL(gx, R[0]), DMUL(gy, R[1])), DMUL(gz, R[2]));
+      double y = DADD(DADD(DMUL(gx, R[3]), DMUL(gy, R[4])), DMUL(gz, R[5]));
+      double z = DADD(DADD(DMUL(gx, R[6]), DMUL(gy, R[7])), DMUL(gz, R[8]));
+      double r2 = DADD(DADD(DMUL(x, x), DMUL(y, y)), DMUL(z, z));
+      double r = sqrt(r2), r3 = r2 * r, r5 = r3 * r2;
+      v[0] += q / r;
+      v[1] += q * x / r3; v[2] += q * y / r3; v[3] += q * z / r3;
+      v[4] += q * (3.0 * x * x - r2) / r5; v[5] += q * (3.0 * y * y - r2) / r5; v[6] += q * (3.0 * z * z - r2) / r5;
+      v[7] += q * 3.0 * x * y / r5; v[8] += q * 3.0 * x * z / r5; v[9] += q * 3.0 * y * z / r5;
+    }
+    for (int j = 0; j < NLR; ++j)
+      for (int o = 16; o > 0; o >>= 1) v[j] += __shfl_xor_sync(0xffffffffu, v[j], o);
+    if (lane == 0)
+      for (int j = 0; j < NLR; ++j) out[LR0 + ci * NLR + j] = (float)v[j];
+  }
   if (lane < NPAIR_RBF) {
     float v = 0.f;
     if (f != s) {

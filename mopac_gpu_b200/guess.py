@@ -28,7 +28,7 @@ from ._lib import check, lib
 from .scf import ScfContext
 from . import workloads
 
-DIN, HID, DOUT, NTYPES, PER_TYPE = 336, 128, 16, 5, 78928
+DIN, HID, DOUT, NTYPES, PER_TYPE = 356, 128, 16, 5, 81528
 NOUT = (10, 1, 16, 4, 1)
 TYPE_NAMES = ("O own", "H own", "O-O", "O-H", "H-H")
 RPAIR = 6.0

@@ -14,7 +14,9 @@ against:
     neighbour for an atom's own block; x towards the nearest neighbour with a
     clear perpendicular component);
   * radial/angular descriptors of each centre's neighbours within ``RC``,
-    expressed in that frame;
+    expressed in that frame, plus each centre's long-range electrostatic
+    environment (potential, field and field gradient of fixed reference
+    charges on every other atom, no cutoff);
   * a 3-hidden-layer MLP (width 128, SiLU) per pair type with BF16 weights and
     activations and FP32 accumulation, forward and backward, Adam;
   * the predicted local blocks rotated back and written into the packed
@@ -40,7 +42,12 @@ PER_CENTER = NELEM * NRAD * NANG       # 160
 NPAIR_RBF = 16
 PAIR_MU = np.linspace(0.8, RPAIR, NPAIR_RBF)
 PAIR_SIG = 0.35
-DIN = 2 * PER_CENTER + NPAIR_RBF       # 336
+NLR = 10          # per centre: potential, field (3), field gradient (6)
+# reference charges of the long-range descriptor: PM7 Mulliken charges of an
+# isolated water (0.322260 / -0.644520, tests/mopac_api_test.F90:61-104)
+QREF_H = 0.32226
+QREF_HEAVY = -0.64452
+DIN = 2 * PER_CENTER + NPAIR_RBF + 2 * NLR   # 356
 HID = 128
 DOUT = 16
 NTYPES = 5
@@ -220,6 +227,27 @@ def _center_features(c: int, excl, nat, xyz, R: np.ndarray) -> np.ndarray:
     return out.reshape(-1)
 
 
+def _center_longrange(c: int, excl, nat, xyz, R: np.ndarray) -> np.ndarray:
+    """Potential, field and field gradient (xx, yy, zz, xy, xz, yz; 3 d d^T -
+    r^2 I, over r^5) at centre c of reference charges on every atom not in
+    excl, in the frame R."""
+    out = np.zeros(NLR)
+    o = xyz[c]
+    for k in range(len(nat)):
+        if k in excl:
+            continue
+        q = QREF_H if nat[k] == 1 else QREF_HEAVY
+        d = (xyz[k] - o) @ R
+        r2 = d @ d
+        r = np.sqrt(r2)
+        r3 = r2 * r
+        r5 = r3 * r2
+        x, y, z = d
+        out += q * np.array([1.0 / r, x / r3, y / r3, z / r3, (3 * x * x - r2) / r5, (3 * y * y - r2) / r5,
+                             (3 * z * z - r2) / r5, 3 * x * y / r5, 3 * x * z / r5, 3 * y * z / r5])
+    return out
+
+
 def features(nat, xyz, F, S, T):
     """Raw descriptors (npairs x DIN, float64) and frames (npairs x 3 x 3)."""
     nat = np.asarray(nat)
@@ -229,15 +257,19 @@ def features(nat, xyz, F, S, T):
     for q, (f, s) in enumerate(zip(F, S)):
         R = frame(int(f), int(s), xyz)
         Rs[q] = R
+        lr0 = 2 * PER_CENTER + NPAIR_RBF
         if f == s:
             X[q, :PER_CENTER] = _center_features(int(f), (int(f),), nat, xyz, R)
+            X[q, lr0:lr0 + NLR] = _center_longrange(int(f), (int(f),), nat, xyz, R)
         else:
             ex = (int(f), int(s))
             X[q, :PER_CENTER] = _center_features(int(f), ex, nat, xyz, R)
             X[q, PER_CENTER:2 * PER_CENTER] = _center_features(int(s), ex, nat, xyz, R)
             d = xyz[s] - xyz[f]
             r = np.sqrt(d @ d)
-            X[q, 2 * PER_CENTER:] = np.exp(-(r - PAIR_MU) ** 2 / (2.0 * PAIR_SIG * PAIR_SIG))
+            X[q, 2 * PER_CENTER:lr0] = np.exp(-(r - PAIR_MU) ** 2 / (2.0 * PAIR_SIG * PAIR_SIG))
+            X[q, lr0:lr0 + NLR] = _center_longrange(int(f), ex, nat, xyz, R)
+            X[q, lr0 + NLR:] = _center_longrange(int(s), ex, nat, xyz, R)
     return X, Rs
 
 
