@@ -228,10 +228,18 @@ int mb_batch_destroy(mb_batch* batch);
 int mb_batch_nmol(const mb_batch* batch);
 /* Runs every molecule's SCF; per molecule escf (kcal/mol, iter's), niter,
  * converged (host arrays of nmol, each optional); *t_ms: CUDA-event time of
- * the launch. */
+ * the launch.  The launch sequence is captured into a CUDA graph on the first
+ * run of a configuration and replayed after that. */
 int mb_batch_run(mb_batch* batch, const mb_scf_opts* opts, double* escf, int* niter, int* converged,
                  double* t_ms);
 int mb_batch_get_density(mb_batch* batch, int m, double* p);
+/* Launch configuration: back-transformation block size nb (4, 8 or 16
+ * reflectors per compact-WY block) and CTAs per SM (0: as many as fit).
+ * mb_batch_autotune times all six on this batch (two runs each) and keeps the
+ * fastest; every configuration gives the same SCFs up to FP64 rounding. */
+int mb_batch_set_config(mb_batch* batch, int nb, int per_sm);
+int mb_batch_get_config(const mb_batch* batch, int* nb, int* grid);
+int mb_batch_autotune(mb_batch* batch, const mb_scf_opts* opts, int* nb, int* per_sm, double* ms);
 /* Phase timing (off by default): SM cycles summed over all CTAs of the last
  * run, out[8] = Fock, energy and control, Householder, bisection, inverse
  * iteration, back-transformation, density, cnvg. */

@@ -104,6 +104,10 @@ SIGNATURES = {
     "mb_batch_set_phase_timing": ([_P, _I], _I),
     "mb_batch_phase_cycles": ([_P, _P], _I),
     "mb_batch_get_hw": ([_P, _I, _P, _P, ctypes.POINTER(_D)], _I),
+    "mb_batch_set_config": ([_P, _I, _I], _I),
+    "mb_batch_get_config": ([_P, ctypes.POINTER(_I), ctypes.POINTER(_I)], _I),
+    "mb_batch_autotune": ([_P, ctypes.POINTER(ScfOpts), ctypes.POINTER(_I), ctypes.POINTER(_I),
+                           ctypes.POINTER(_D)], _I),
     "mb_mz_layout_create": ([_I, _P, _P, _D, _D, ctypes.POINTER(MbMzLayout), _P], _I),
     "mb_mz_layout_destroy": ([ctypes.POINTER(MbMzLayout)], _I),
     "mb_mz_idiag": ([ctypes.POINTER(MbMzLayout), _P], _I),

@@ -3,7 +3,9 @@
 ``Batch(molecules)`` takes a list of (atomic numbers, coordinates) pairs,
 computes every molecule's integrals on the GPU, and ``run()`` performs every
 molecule's SCF (iter, SCF/iter.F90, full diagonalisation each iteration) in
-one launch; it returns the heats of formation as iter computes them.
+one launch, replayed from a CUDA graph; it returns the heats of formation as
+iter computes them.  ``autotune()`` picks the launch configuration
+(back-transformation block size, CTAs per SM) by timing them on the batch.
 """
 from __future__ import annotations
 
@@ -40,6 +42,25 @@ class Batch:
         check(lib().mb_batch_run(self._h, ctypes.byref(o), escf.ctypes.data, niter.ctypes.data, conv.ctypes.data,
                                  ctypes.byref(t)))
         return escf, niter, conv.astype(bool), t.value
+
+    def set_config(self, nb: int = 8, per_sm: int = 0):
+        check(lib().mb_batch_set_config(self._h, int(nb), int(per_sm)))
+
+    def config(self):
+        nb, grid = ctypes.c_int(), ctypes.c_int()
+        check(lib().mb_batch_get_config(self._h, ctypes.byref(nb), ctypes.byref(grid)))
+        return nb.value, grid.value
+
+    def autotune(self, scfcrt: float = 1.0e-4, itrmax: int = 2000):
+        """Returns (block size, CTAs per SM (0 = all that fit), best ms)."""
+        o = ScfOpts()
+        lib().mb_scf_opts_default(ctypes.byref(o))
+        o.scfcrt = scfcrt
+        o.itrmax = itrmax
+        nb, per, ms = ctypes.c_int(), ctypes.c_int(), ctypes.c_double()
+        check(lib().mb_batch_autotune(self._h, ctypes.byref(o), ctypes.byref(nb), ctypes.byref(per),
+                                      ctypes.byref(ms)))
+        return nb.value, per.value, ms.value
 
     PHASES = ("fock", "energy", "householder", "bisection", "inverse_iteration", "back_transform", "density",
               "cnvg")

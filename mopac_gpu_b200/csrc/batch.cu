@@ -45,8 +45,9 @@ constexpr int BT_ZMAX = 11008;                            // n * nocc
 constexpr int BT_IMAX = 320;                              // diagonal-block elements, <= 2.5 n
 constexpr long long BT_LU = 5LL * BT_ZMAX;                // LU factors of T - lambda I, 5 n per vector
 constexpr long long BT_SCR = BT_LU + BT_AMAX + BT_ZMAX;   // + reflectors + oversized Z: doubles per CTA
-constexpr int BT_NB = 8;                                  // reflectors per back-transformation block
-constexpr int BT_TW = ((BT_NMAX - 2 + BT_NB - 1) / BT_NB) * BT_NB * BT_NB;  // T of every block
+// reflectors per back-transformation block: a template parameter of the
+// kernel (4, 8 or 16), chosen per batch by mb_batch_autotune (default 8)
+__host__ __device__ constexpr int bt_tw(int nb) { return ((BT_NMAX - 2 + nb - 1) / nb) * nb * nb; }  // T of every block
 constexpr int BT_PHASES = 8;
 static_assert(BT_T == 256, "the reduction tile is 16 x 16 threads");  // fock, energy, householder, bisection, inverse iteration, back-transform, density, cnvg
 
@@ -341,6 +342,7 @@ __device__ int sturm(int n, const double* d, const double* e2, double x, double 
 }
 
 // reltol: relative width at which an eigenvalue's bracket stops shrinking.
+template <int BT_NB>
 __device__ void cta_eigh(int n, int nz, bool vectors, double reltol, Smem& S, double* scr, long long* ph) {
   const int tid = threadIdx.x, lane = tid & 31, wp = tid >> 5, tr = tid >> 4, tc = tid & 15;
   double* A = S.A;
@@ -660,9 +662,9 @@ __device__ void cta_eigh(int n, int nz, bool vectors, double reltol, Smem& S, do
       const int kb = blk * BT_NB, nbb = min(BT_NB, nr - kb);
       for (int q = lane; q < BT_NB * BT_NB; q += 32) T[q] = 0.0;
       __syncwarp();
-      // Gram entries V(:, j)^T v_c, j < c < nbb, one lane each (28 pairs)
-      if (lane < BT_NB * (BT_NB - 1) / 2) {
-        int c = 1, j = lane;
+      // Gram entries V(:, j)^T v_c, j < c < nbb, one lane each
+      for (int pq = lane; pq < BT_NB * (BT_NB - 1) / 2; pq += 32) {
+        int c = 1, j = pq;
         while (j >= c) { j -= c; ++c; }
         if (c < nbb) {
           double g = 0.0;
@@ -867,6 +869,7 @@ __device__ void cta_density(int n, int nz, const Smem& S, double* p) {
   __syncthreads();
 }
 
+template <int BT_NB>
 __global__ void __launch_bounds__(BT_T, 2) scf_batch_kernel(BatchArgs B) {
   extern __shared__ double smem[];
   __shared__ int s_m, s_nitems;
@@ -886,7 +889,7 @@ __global__ void __launch_bounds__(BT_T, 2) scf_batch_kernel(BatchArgs B) {
   S.red = S.eig + BT_NMAX + 2;
   S.scal = S.red + 2 * BT_W;
   S.tw = S.scal + 16;
-  S.awrow = (long long*)(S.tw + BT_TW);
+  S.awrow = (long long*)(S.tw + bt_tw(BT_NB));
   S.afirst = (int*)(S.awrow + BT_NMAX);
   S.anor = S.afirst + BT_NMAX;
   S.acum = S.anor + BT_NMAX;
@@ -1007,7 +1010,7 @@ __global__ void __launch_bounds__(BT_T, 2) scf_batch_kernel(BatchArgs B) {
       eold = escf;
       ph_mark(ph, 1);
       load_perturbed(n, f, S, true);
-      cta_eigh(n, nclose, true, 1.0e-11, S, scr, ph);
+      cta_eigh<BT_NB>(n, nclose, true, 1.0e-11, S, scr, ph);
       eig_homo = S.eig[ihomo - 1];
       eig_lumo = ihomo < n ? S.eig[ihomo] : 0.0;
       cta_density(n, nclose, S, p);
@@ -1024,7 +1027,7 @@ __global__ void __launch_bounds__(BT_T, 2) scf_batch_kernel(BatchArgs B) {
     ee = cta_helect(n, p, cpa, h, f, S.red) * 2.0;
     load_perturbed(n, f, S, false);
     ph_mark(ph, 1);
-    cta_eigh(n, nclose, false, 4.4e-16, S, scr, ph);
+    cta_eigh<BT_NB>(n, nclose, false, 4.4e-16, S, scr, ph);
     if (ph && tid == 0)
       for (int q = 0; q < BT_PHASES; ++q) atomicAdd(B.phase + q, (unsigned long long)s_ph[q]);
     if (tid == 0) {
@@ -1039,9 +1042,31 @@ __global__ void __launch_bounds__(BT_T, 2) scf_batch_kernel(BatchArgs B) {
   }
 }
 
-size_t batch_smem() {
-  return sizeof(double) * ((size_t)BT_AMAX + 6 * BT_NMAX + BT_NMAX + 2 + 2 * BT_W + 16 + BT_TW) +
+size_t batch_smem(int nb) {
+  return sizeof(double) * ((size_t)BT_AMAX + 6 * BT_NMAX + BT_NMAX + 2 + 2 * BT_W + 16 + bt_tw(nb)) +
          sizeof(long long) * BT_NMAX + sizeof(int) * (4 * BT_NMAX + BT_IMAX);
+}
+
+// Kernel instance for a back-transformation block size (4, 8, 16).
+const void* batch_kernel(int nb) {
+  switch (nb) {
+    case 4: return (const void*)scf_batch_kernel<4>;
+    case 8: return (const void*)scf_batch_kernel<8>;
+    case 16: return (const void*)scf_batch_kernel<16>;
+    default: return nullptr;
+  }
+}
+
+// Opts the instance into its dynamic shared memory and returns how many of
+// its CTAs fit on one SM.
+int batch_kernel_setup(int nb, int* per_sm) {
+  const void* fn = batch_kernel(nb);
+  if (!fn) return mb_set_error(MB_ERR_ARG, "batched SCF: block size must be 4, 8 or 16");
+  const size_t smem = batch_smem(nb);
+  MB_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  MB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, fn, BT_T, smem));
+  if (*per_sm < 1) return mb_set_error(MB_ERR_CUDA, "batched SCF kernel does not fit on an SM");
+  return MB_OK;
 }
 
 }  // namespace
@@ -1060,6 +1085,12 @@ struct mb_batch {
          *lumo = nullptr, *enuc = nullptr, *epairs = nullptr;
   long long tot_mp = 0, tot_w = 0;
   int tot_n = 0, tot_at = 0, grid = 0;
+  int sms = 0, max_grid = 0;    // scratch is sized for max_grid CTAs
+  int nb = 8, per_sm = 0;       // launch configuration (per_sm 0: as many as fit)
+  // the run's launch sequence, captured once per configuration and replayed
+  cudaGraphExec_t graph = nullptr;
+  int g_nb = 0, g_grid = 0, g_timing = -1, g_itrmax = -1;
+  double g_scfcrt = -1.0;
   cudaStream_t stream = nullptr;
 };
 
@@ -1068,6 +1099,7 @@ static void batch_free(mb_batch* b) {
   void* ptrs[] = {b->mol, b->order, b->first, b->nor, b->lim, b->cum, b->nat, b->next, b->niter, b->conv, b->status, b->wrow,
                   b->coord, b->h, b->w, b->pdiag, b->f, b->p, b->pold, b->pold2, b->scratch, b->escf, b->ee,
                   b->homo, b->lumo, b->enuc, b->epairs, b->phase, b->offs};
+  if (b->graph) cudaGraphExecDestroy(b->graph);
   for (void* q : ptrs)
     if (q) cudaFree(q);
   if (b->stream) cudaStreamDestroy(b->stream);
@@ -1231,20 +1263,27 @@ extern "C" int mb_batch_create(int nmol, const int* numat, const int* nat, const
   std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return b->hmol[x].n > b->hmol[y].n; });
   e = cudaMemcpy(b->mol, b->hmol.data(), sizeof(Mol) * nmol, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(b->order, order.data(), sizeof(int) * nmol, cudaMemcpyHostToDevice);
-  int dev = 0, sms = 0, per = 0;
-  const size_t smem = batch_smem();
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(scf_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  int dev = 0, sms = 0, per = 0, maxper = 0;
   if (e == cudaSuccess) e = cudaGetDevice(&dev);
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, scf_batch_kernel, BT_T, smem);
-  if (e != cudaSuccess || per < 1) {
-    int r = e != cudaSuccess ? mb_set_cuda_error(e, "mb_batch_create kernel setup", __FILE__, __LINE__)
-                             : mb_set_error(MB_ERR_CUDA, "batched SCF kernel does not fit on an SM");
+  if (e != cudaSuccess) {
+    int r = mb_set_cuda_error(e, "mb_batch_create kernel setup", __FILE__, __LINE__);
     batch_free(b);
     return r;
   }
+  for (int nb : {4, 16, 8}) {  // the default (8) last: its attribute stays set
+    int rc = batch_kernel_setup(nb, &per);
+    if (rc != MB_OK) {
+      batch_free(b);
+      return rc;
+    }
+    maxper = std::max(maxper, per);
+  }
+  b->sms = sms;
+  b->nb = 8;
   b->grid = std::min(nmol, sms * per);
-  e = cudaMalloc((void**)&b->scratch, sizeof(double) * BT_SCR * (size_t)b->grid);
+  b->max_grid = std::min(nmol, sms * maxper);
+  e = cudaMalloc((void**)&b->scratch, sizeof(double) * BT_SCR * (size_t)b->max_grid);
   if (e != cudaSuccess) {
     int r = mb_set_cuda_error(e, "mb_batch_create scratch", __FILE__, __LINE__);
     batch_free(b);
@@ -1296,12 +1335,40 @@ extern "C" int mb_batch_run(mb_batch* b, const mb_scf_opts* opts_in, double* esc
   if (b->timing) MB_CUDA(cudaMemsetAsync(b->phase, 0, sizeof(unsigned long long) * BT_PHASES, b->stream));
   A.itrmax = o.itrmax;
   A.scfcrt = o.scfcrt;
+  // The launch sequence (clear the work counter, the persistent kernel) is
+  // captured into a CUDA graph once per configuration and replayed.
+  const int timing = b->timing ? 1 : 0;
+  if (!b->graph || b->g_nb != b->nb || b->g_grid != b->grid || b->g_timing != timing || b->g_itrmax != o.itrmax ||
+      b->g_scfcrt != o.scfcrt) {
+    if (b->graph) {
+      cudaGraphExecDestroy(b->graph);
+      b->graph = nullptr;
+    }
+    void* args[] = {&A};
+    cudaGraph_t g = nullptr;
+    MB_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+    cudaError_t ce = cudaMemsetAsync(b->next, 0, sizeof(int), b->stream);
+    if (ce == cudaSuccess)
+      ce = cudaLaunchKernel(batch_kernel(b->nb), dim3(b->grid), dim3(BT_T), args, batch_smem(b->nb), b->stream);
+    cudaError_t ee = cudaStreamEndCapture(b->stream, &g);
+    if (ce == cudaSuccess) ce = ee;
+    if (ce == cudaSuccess) ce = cudaGraphInstantiate(&b->graph, g, 0);
+    if (g) cudaGraphDestroy(g);
+    if (ce != cudaSuccess) {
+      b->graph = nullptr;
+      return mb_set_cuda_error(ce, "mb_batch_run graph capture", __FILE__, __LINE__);
+    }
+    b->g_nb = b->nb;
+    b->g_grid = b->grid;
+    b->g_timing = timing;
+    b->g_itrmax = o.itrmax;
+    b->g_scfcrt = o.scfcrt;
+  }
   cudaEvent_t e0, e1;
   MB_CUDA(cudaEventCreate(&e0));
   MB_CUDA(cudaEventCreate(&e1));
-  MB_CUDA(cudaMemsetAsync(b->next, 0, sizeof(int), b->stream));
   MB_CUDA(cudaEventRecord(e0, b->stream));
-  scf_batch_kernel<<<b->grid, BT_T, batch_smem(), b->stream>>>(A);
+  MB_CUDA(cudaGraphLaunch(b->graph, b->stream));
   MB_LAUNCH_CHECK();
   MB_CUDA(cudaEventRecord(e1, b->stream));
   MB_CUDA(cudaEventSynchronize(e1));
@@ -1313,6 +1380,53 @@ extern "C" int mb_batch_run(mb_batch* b, const mb_scf_opts* opts_in, double* esc
   if (escf) MB_CUDA(cudaMemcpy(escf, b->escf, sizeof(double) * b->nmol, cudaMemcpyDeviceToHost));
   if (niter) MB_CUDA(cudaMemcpy(niter, b->niter, sizeof(int) * b->nmol, cudaMemcpyDeviceToHost));
   if (converged) MB_CUDA(cudaMemcpy(converged, b->conv, sizeof(int) * b->nmol, cudaMemcpyDeviceToHost));
+  return MB_OK;
+}
+
+extern "C" int mb_batch_set_config(mb_batch* b, int nb, int per_sm) {
+  if (!b) return mb_set_error(MB_ERR_ARG, "mb_batch_set_config: null batch");
+  int per = 0;
+  MB_TRY(batch_kernel_setup(nb, &per));
+  if (per_sm < 0) return mb_set_error(MB_ERR_ARG, "mb_batch_set_config: per_sm < 0");
+  const int use = per_sm == 0 ? per : std::min(per_sm, per);
+  b->nb = nb;
+  b->per_sm = per_sm;
+  b->grid = std::min({b->nmol, b->sms * use, b->max_grid});
+  return MB_OK;
+}
+
+extern "C" int mb_batch_get_config(const mb_batch* b, int* nb, int* grid) {
+  if (!b) return mb_set_error(MB_ERR_ARG, "mb_batch_get_config: null batch");
+  if (nb) *nb = b->nb;
+  if (grid) *grid = b->grid;
+  return MB_OK;
+}
+
+// Times every configuration (block size 4, 8, 16 x one or as many CTAs per
+// SM as fit) on this batch -- one untimed and one timed run each -- and keeps
+// the fastest.  Every configuration computes the same SCFs (the block size
+// only regroups the back-transformation's FP64 sums).
+extern "C" int mb_batch_autotune(mb_batch* b, const mb_scf_opts* opts, int* nb_out, int* per_sm_out,
+                                 double* ms_out) {
+  if (!b) return mb_set_error(MB_ERR_ARG, "mb_batch_autotune: null batch");
+  double best = 1e300;
+  int bnb = 8, bper = 0;
+  for (int nb : {4, 8, 16})
+    for (int per : {1, 0}) {
+      MB_TRY(mb_batch_set_config(b, nb, per));
+      double ms = 0.0;
+      MB_TRY(mb_batch_run(b, opts, nullptr, nullptr, nullptr, &ms));
+      MB_TRY(mb_batch_run(b, opts, nullptr, nullptr, nullptr, &ms));
+      if (ms < best) {
+        best = ms;
+        bnb = nb;
+        bper = per;
+      }
+    }
+  MB_TRY(mb_batch_set_config(b, bnb, bper));
+  if (nb_out) *nb_out = bnb;
+  if (per_sm_out) *per_sm_out = bper;
+  if (ms_out) *ms_out = best;
   return MB_OK;
 }
 

@@ -73,3 +73,35 @@ def test_batch_repeat_is_deterministic():
     for k in range(4):
         assert e1[k] == e1[k + 4] == e1[k + 8]
     b.close()
+
+
+@pytest.mark.parametrize("nb,per_sm", [(4, 0), (16, 0), (8, 1)])
+def test_every_launch_configuration_gives_the_same_scfs(nb, per_sm):
+    """The back-transformation block size only regroups FP64 sums and the CTA
+    count only changes which CTA takes a molecule: heats agree to 1e-9
+    kcal/mol, iteration counts exactly, with the default configuration."""
+    from mopac_gpu_b200.batch import Batch
+    mols = _molecules()
+    b = Batch(mols)
+    e0, n0, c0, _ = b.run()
+    b.set_config(nb, per_sm)
+    assert b.config()[0] == nb
+    e1, n1, c1, _ = b.run()
+    e2, n2, _, _ = b.run()   # replay of the captured graph
+    assert c1.all() and np.array_equal(n0, n1) and np.array_equal(e1, e2)
+    assert np.abs(e1 - e0).max() < 1e-9
+    b.close()
+
+
+def test_autotune_picks_a_valid_configuration():
+    from mopac_gpu_b200.batch import Batch
+    mols = _molecules() * 4
+    b = Batch(mols)
+    nb, per, ms = b.autotune()
+    assert nb in (4, 8, 16) and per in (0, 1) and ms > 0
+    assert b.config()[0] == nb
+    e, n, c, _ = b.run()
+    assert c.all()
+    with pytest.raises(Exception):
+        b.set_config(5, 0)
+    b.close()
