@@ -437,9 +437,13 @@ int mb_ctx_guess(mb_ctx* ctx, const mb_guess_model* model);
  * type is unspecified).  work: 15 ints of device scratch. */
 int mb_guess_pairs_dev(int numat, const int* nat, const double* xyz, double rpair, int* counts_host,
                        int max_pairs, int* pf, int* ps, int* pt, int* work, cudaStream_t stream);
-/* Frames (npairs x 9 doubles, axes as columns) and raw descriptors (npairs x DIN floats). */
+/* Frames (npairs x 9 doubles, axes as columns) and raw descriptors (npairs x
+ * DIN floats).  ws: mb_guess_features_ws_bytes(numat) bytes of device scratch
+ * (per-atom neighbour lists within 6 A, at most 512 per atom; more returns
+ * MB_ERR_UNSUPPORTED).  Synchronises the stream. */
+size_t mb_guess_features_ws_bytes(int numat);
 int mb_guess_features_dev(int numat, const int* nat, const double* xyz, int npairs, const int* pf,
-                          const int* ps, float* feat, double* frames, cudaStream_t stream);
+                          const int* ps, float* feat, double* frames, void* ws, cudaStream_t stream);
 /* Raw descriptors -> normalised BF16 rows (uint16 bit patterns). */
 int mb_guess_normalize_dev(const mb_guess_model* model, int type, int n, const float* raw,
                            unsigned short* x, cudaStream_t stream);
@@ -458,7 +462,15 @@ int mb_guess_assemble_dev(const mb_guess_model* model, int npairs, const int* pf
 int mb_guess_targets_dev(int npairs, const int* pf, const int* ps, const int* pt,
                          const double* frames, const int* first, const int* nor, const double* p,
                          float* yraw, cudaStream_t stream);
-/* All of the above for one molecule: p (mpack) is overwritten. */
+/* All of the above for one molecule: p (mpack) is overwritten.  The _ws form
+ * takes its buffers from a grow-only workspace (mb_guess_ws_create; contexts
+ * keep one), the _dev form allocates and frees its own. */
+typedef struct mb_guess_ws mb_guess_ws;
+int mb_guess_ws_create(mb_guess_ws** out);
+int mb_guess_ws_destroy(mb_guess_ws* ws);
+int mb_guess_predict_density_ws(const mb_guess_model* model, int numat, const int* nat,
+                                const double* xyz, const int* first, const int* nor, int norbs,
+                                double* p, mb_guess_ws* ws, cudaStream_t stream);
 int mb_guess_predict_density_dev(const mb_guess_model* model, int numat, const int* nat,
                                  const double* xyz, const int* first, const int* nor, int norbs,
                                  double* p, cudaStream_t stream);

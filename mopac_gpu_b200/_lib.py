@@ -165,7 +165,11 @@ SIGNATURES = {
     "mb_guess_model_create": ([_P, ctypes.POINTER(_P)], _I),
     "mb_guess_model_destroy": ([_P], _I),
     "mb_guess_pairs_dev": ([_I, _P, _P, _D, _P, _I, _P, _P, _P, _P, _P], _I),
-    "mb_guess_features_dev": ([_I, _P, _P, _I, _P, _P, _P, _P, _P], _I),
+    "mb_guess_features_ws_bytes": ([_I], ctypes.c_size_t),
+    "mb_guess_features_dev": ([_I, _P, _P, _I, _P, _P, _P, _P, _P, _P], _I),
+    "mb_guess_ws_create": ([ctypes.POINTER(_P)], _I),
+    "mb_guess_ws_destroy": ([_P], _I),
+    "mb_guess_predict_density_ws": ([_P, _I, _P, _P, _P, _P, _I, _P, _P, _P], _I),
     "mb_guess_normalize_dev": ([_P, _I, _I, _P, _P, _P], _I),
     "mb_guess_norm_targets_dev": ([_P, _I, _I, _P, _P, _P], _I),
     "mb_guess_forward_dev": ([_P, _I, _I, _P, _P, _P, _P], _I),

@@ -141,6 +141,24 @@ __global__ void pairs_emit_kernel(int numat, const int* __restrict__ nat, const 
   }
 }
 
+// ---------------------------------------------------------- neighbour lists
+// Atoms within RC of each atom, ascending index (the order the descriptor
+// sums run in).  nbr_count[a] > NBR_MAX marks an overflow (the host refuses).
+constexpr int NBR_MAX = 512;
+
+__global__ void neighbours_kernel(int numat, const double* __restrict__ xyz, int* __restrict__ nbr_count,
+                                  int* __restrict__ nbr) {
+  int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= numat) return;
+  int c = 0;
+  for (int k = 0; k < numat; ++k) {
+    if (k == a || !(r2_of(xyz, k, a) < RC * RC)) continue;
+    if (c < NBR_MAX) nbr[(long long)a * NBR_MAX + c] = k;
+    ++c;
+  }
+  nbr_count[a] = c;
+}
+
 // --------------------------------------------------- frames + descriptors
 __device__ __forceinline__ unsigned long long rank_key(double r2, int k) {
   double q = floor(DADD(DMUL(r2, QSCALE), 0.5));
@@ -161,6 +179,7 @@ __device__ __forceinline__ unsigned long long warp_min_u64(unsigned long long v)
 __global__ void __launch_bounds__(128) features_kernel(int numat, const int* __restrict__ nat,
                                                        const double* __restrict__ xyz, int npairs,
                                                        const int* __restrict__ pf, const int* __restrict__ ps,
+                                                       const int* __restrict__ nbr_count, const int* __restrict__ nbr,
                                                        float* __restrict__ feat, double* __restrict__ frames) {
   const int lane = threadIdx.x & 31;
   const int q = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
@@ -241,7 +260,10 @@ __global__ void __launch_bounds__(128) features_kernel(int numat, const int* __r
     const int c = ci == 0 ? f : s;
     const double cx = xyz[3 * c], cy = xyz[3 * c + 1], cz = xyz[3 * c + 2];
     double acc[5] = {0, 0, 0, 0, 0};
-    for (int k = 0; k < numat; ++k) {
+    const int nn = min(nbr_count[c], NBR_MAX);  // an overflow is reported by the host after the launch
+    const int* nl = nbr + (long long)c * NBR_MAX;
+    for (int j = 0; j < nn; ++j) {
+      const int k = nl[j];
       if (k == f || k == s) continue;
       if ((nat[k] != 1) != (e == 1)) continue;
       double dx = DSUB(xyz[3 * k], cx), dy = DSUB(xyz[3 * k + 1], cy), dz = DSUB(xyz[3 * k + 2], cz);
@@ -690,13 +712,35 @@ extern "C" int mb_guess_pairs_dev(int numat, const int* nat, const double* xyz, 
   return MB_OK;
 }
 
-extern "C" int mb_guess_features_dev(int numat, const int* nat, const double* xyz, int npairs, const int* pf,
-                                     const int* ps, float* feat, double* frames, cudaStream_t s) {
-  if (npairs < 0 || numat >= (1 << 21)) return mb_set_error(MB_ERR_ARG, "mb_guess_features_dev: bad args");
-  if (npairs == 0) return MB_OK;
-  features_kernel<<<blocks_for(npairs, 4), 128, 0, s>>>(numat, nat, xyz, npairs, pf, ps, feat, frames);
+static int features_impl(int numat, const int* nat, const double* xyz, int npairs, const int* pf, const int* ps,
+                         float* feat, double* frames, int* nbr_count, int* nbr, cudaStream_t s) {
+  neighbours_kernel<<<blocks_for(numat, 128), 128, 0, s>>>(numat, xyz, nbr_count, nbr);
   MB_LAUNCH_CHECK();
+  features_kernel<<<blocks_for(npairs, 4), 128, 0, s>>>(numat, nat, xyz, npairs, pf, ps, nbr_count, nbr, feat, frames);
+  MB_LAUNCH_CHECK();
+  // an overflowing neighbour list is an error, not a silent truncation
+  int mx = 0;
+  std::vector<int> cnt(numat);
+  MB_CUDA(cudaMemcpyAsync(cnt.data(), nbr_count, sizeof(int) * numat, cudaMemcpyDeviceToHost, s));
+  MB_CUDA(cudaStreamSynchronize(s));
+  for (int a = 0; a < numat; ++a) mx = cnt[a] > mx ? cnt[a] : mx;
+  if (mx > NBR_MAX) return mb_set_error(MB_ERR_UNSUPPORTED, "learned guess: more than 512 atoms within 6 A of an atom");
   return MB_OK;
+}
+
+extern "C" size_t mb_guess_features_ws_bytes(int numat) {
+  return sizeof(int) * (size_t)numat * (NBR_MAX + 1);
+}
+
+// ws: mb_guess_features_ws_bytes(numat) bytes of device scratch (neighbour lists).
+extern "C" int mb_guess_features_dev(int numat, const int* nat, const double* xyz, int npairs, const int* pf,
+                                     const int* ps, float* feat, double* frames, void* ws, cudaStream_t s) {
+  if (npairs < 0 || numat <= 0 || numat >= (1 << 21) || !ws)
+    return mb_set_error(MB_ERR_ARG, "mb_guess_features_dev: bad args");
+  if (npairs == 0) return MB_OK;
+  int* nbr_count = (int*)ws;
+  int* nbr = nbr_count + numat;
+  return features_impl(numat, nat, xyz, npairs, pf, ps, feat, frames, nbr_count, nbr, s);
 }
 
 extern "C" int mb_guess_normalize_dev(const mb_guess_model* m, int type, int n, const float* raw, uint16_t* x,
@@ -781,34 +825,73 @@ extern "C" int mb_guess_targets_dev(int npairs, const int* pf, const int* ps, co
   return MB_OK;
 }
 
+// Grow-only device workspace of the prediction (a context keeps one, so a
+// prediction allocates only when a molecule needs more room than any before).
+struct mb_guess_ws {
+  char* buf = nullptr;
+  size_t bytes = 0;
+};
+
+static int ws_ensure(mb_guess_ws* w, size_t bytes) {
+  if (bytes <= w->bytes) return MB_OK;
+  if (w->buf) MB_CUDA(cudaFree(w->buf));
+  w->buf = nullptr;
+  w->bytes = 0;
+  MB_CUDA(cudaMalloc((void**)&w->buf, bytes));
+  w->bytes = bytes;
+  return MB_OK;
+}
+
+extern "C" int mb_guess_ws_create(mb_guess_ws** out) {
+  if (!out) return mb_set_error(MB_ERR_ARG, "mb_guess_ws_create: null");
+  *out = new mb_guess_ws();
+  return MB_OK;
+}
+
+extern "C" int mb_guess_ws_destroy(mb_guess_ws* w) {
+  if (w) {
+    if (w->buf) cudaFree(w->buf);
+    delete w;
+  }
+  return MB_OK;
+}
+
 // Whole prediction for one molecule into a packed density p (device, mpack
-// doubles, overwritten: pairs beyond rpair are zero).  Allocates and frees its
-// own buffers.
-extern "C" int mb_guess_predict_density_dev(const mb_guess_model* m, int numat, const int* nat, const double* xyz,
-                                            const int* first, const int* nor, int norbs, double* p,
-                                            cudaStream_t s) {
-  if (!m || numat <= 0 || norbs <= 0 || !p) return mb_set_error(MB_ERR_ARG, "mb_guess_predict_density_dev: bad args");
+// doubles, overwritten: pairs beyond 6 A are zero).  Two host synchronisations
+// (pair counts, neighbour-list check); buffers from the grow-only workspace.
+extern "C" int mb_guess_predict_density_ws(const mb_guess_model* m, int numat, const int* nat, const double* xyz,
+                                           const int* first, const int* nor, int norbs, double* p, mb_guess_ws* w,
+                                           cudaStream_t s) {
+  if (!m || !w || numat <= 0 || numat >= (1 << 21) || norbs <= 0 || !p)
+    return mb_set_error(MB_ERR_ARG, "mb_guess_predict_density_ws: bad args");
+  auto al = [](size_t v) { return (v + 255) & ~(size_t)255; };
+  const double r2 = 36.0;
+  MB_TRY(ws_ensure(w, 256));
+  int* work = (int*)w->buf;
   int counts[NT];
-  int* work = nullptr;
-  MB_CUDA(cudaMallocAsync((void**)&work, sizeof(int) * 3 * NT, s));
-  int rc = mb_guess_pairs_dev(numat, nat, xyz, 6.0, counts, 0, nullptr, nullptr, nullptr, work, s);
-  if (rc != MB_OK) { cudaFreeAsync(work, s); return rc; }
+  MB_CUDA(cudaMemsetAsync(work, 0, sizeof(int) * 3 * NT, s));
+  pairs_count_kernel<<<blocks_for(numat, 128), 128, 0, s>>>(numat, nat, xyz, r2, work);
+  MB_LAUNCH_CHECK();
+  MB_CUDA(cudaMemcpyAsync(counts, work, sizeof(int) * NT, cudaMemcpyDeviceToHost, s));
+  MB_CUDA(cudaStreamSynchronize(s));
   long long tot = 0;
-  int maxc = 0;
-  for (int t = 0; t < NT; ++t) { tot += counts[t]; maxc = counts[t] > maxc ? counts[t] : maxc; }
-  // one allocation for every buffer
+  int maxc = 0, segh[NT];
+  for (int t = 0; t < NT; ++t) {
+    segh[t] = (int)tot;
+    tot += counts[t];
+    maxc = counts[t] > maxc ? counts[t] : maxc;
+  }
+  const size_t b_work = 256;
   const size_t b_pairs = sizeof(int) * 3 * (size_t)tot;
   const size_t b_frames = sizeof(double) * 9 * (size_t)tot;
   const size_t b_feat = sizeof(float) * DIN * (size_t)tot;
   const size_t b_y = sizeof(float) * DOUT * (size_t)tot;
   const size_t b_x = sizeof(uint16_t) * DIN * (size_t)maxc;
   const size_t b_ws = sizeof(uint16_t) * 2 * HID * (size_t)maxc;
-  auto al = [](size_t v) { return (v + 255) & ~(size_t)255; };
-  const size_t total = al(b_pairs) + al(b_frames) + al(b_feat) + al(b_y) + al(b_x) + al(b_ws);
-  char* buf = nullptr;
-  cudaError_t e = cudaMallocAsync((void**)&buf, total, s);
-  if (e != cudaSuccess) { cudaFreeAsync(work, s); return mb_set_cuda_error(e, "cudaMallocAsync", __FILE__, __LINE__); }
-  char* cur = buf;
+  const size_t b_nbr = mb_guess_features_ws_bytes(numat);
+  MB_TRY(ws_ensure(w, b_work + al(b_pairs) + al(b_frames) + al(b_feat) + al(b_y) + al(b_x) + al(b_ws) + al(b_nbr)));
+  char* cur = w->buf;
+  work = (int*)cur; cur += b_work;
   int* pf = (int*)cur;
   int* ps = pf + tot;
   int* pt = ps + tot;
@@ -817,23 +900,35 @@ extern "C" int mb_guess_predict_density_dev(const mb_guess_model* m, int numat, 
   float* feat = (float*)cur; cur += al(b_feat);
   float* y = (float*)cur; cur += al(b_y);
   uint16_t* x = (uint16_t*)cur; cur += al(b_x);
-  uint16_t* ws = (uint16_t*)cur;
-  rc = mb_guess_pairs_dev(numat, nat, xyz, 6.0, counts, (int)tot, pf, ps, pt, work, s);
-  if (rc == MB_OK) rc = mb_guess_features_dev(numat, nat, xyz, (int)tot, pf, ps, feat, frames, s);
+  uint16_t* mlp_ws = (uint16_t*)cur; cur += al(b_ws);
+  int* nbr_count = (int*)cur;
+  int* nbr = nbr_count + numat;
+  // emit the pairs type by type
+  MB_CUDA(cudaMemcpyAsync(work + NT, segh, sizeof(int) * NT, cudaMemcpyHostToDevice, s));
+  MB_CUDA(cudaMemsetAsync(work + 2 * NT, 0, sizeof(int) * NT, s));
+  pairs_emit_kernel<<<blocks_for(numat, 128), 128, 0, s>>>(numat, nat, xyz, r2, work + NT, work + 2 * NT, pf, ps, pt);
+  MB_LAUNCH_CHECK();
+  MB_TRY(features_impl(numat, nat, xyz, (int)tot, pf, ps, feat, frames, nbr_count, nbr, s));  // syncs: segh is safe
   long long off = 0;
-  for (int t = 0; t < NT && rc == MB_OK; ++t) {
+  for (int t = 0; t < NT; ++t) {
     if (counts[t] == 0) continue;
-    rc = mb_guess_normalize_dev(m, t, counts[t], feat + off * DIN, x, s);
-    if (rc == MB_OK) rc = forward_impl(m->params, m->wbf, t, counts[t], x, y + off * DOUT, ws, nullptr, nullptr, s);
+    MB_TRY(mb_guess_normalize_dev(m, t, counts[t], feat + off * DIN, x, s));
+    MB_TRY(forward_impl(m->params, m->wbf, t, counts[t], x, y + off * DOUT, mlp_ws, nullptr, nullptr, s));
     off += counts[t];
   }
-  if (rc == MB_OK) {
-    e = cudaMemsetAsync(p, 0, sizeof(double) * (size_t)norbs * (norbs + 1) / 2, s);
-    if (e != cudaSuccess) rc = mb_set_cuda_error(e, "cudaMemsetAsync", __FILE__, __LINE__);
-  }
-  if (rc == MB_OK) rc = mb_guess_assemble_dev(m, (int)tot, pf, ps, pt, frames, y, first, nor, p, s);
-  cudaFreeAsync(buf, s);
-  cudaFreeAsync(work, s);
+  MB_CUDA(cudaMemsetAsync(p, 0, sizeof(double) * (size_t)norbs * (norbs + 1) / 2, s));
+  return mb_guess_assemble_dev(m, (int)tot, pf, ps, pt, frames, y, first, nor, p, s);
+}
+
+// The same with a workspace of its own (allocated and freed in the call).
+extern "C" int mb_guess_predict_density_dev(const mb_guess_model* m, int numat, const int* nat, const double* xyz,
+                                            const int* first, const int* nor, int norbs, double* p,
+                                            cudaStream_t s) {
+  mb_guess_ws w;
+  int rc = mb_guess_predict_density_ws(m, numat, nat, xyz, first, nor, norbs, p, &w, s);
+  cudaError_t e = cudaStreamSynchronize(s);
+  if (w.buf) cudaFree(w.buf);
+  if (rc == MB_OK && e != cudaSuccess) rc = mb_set_cuda_error(e, "mb_guess_predict_density_dev", __FILE__, __LINE__);
   return rc;
 }
 

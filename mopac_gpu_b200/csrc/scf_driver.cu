@@ -156,6 +156,7 @@ struct mb_ctx {
   // starting density for opts.guess (mb_ctx_set_guess / mb_ctx_guess)
   double* pguess = nullptr;
   bool have_guess = false;
+  mb_guess_ws* guess_ws = nullptr;  // the prediction's grow-only workspace
   cudaStream_t stream = nullptr;
 };
 
@@ -165,6 +166,7 @@ static const int kNpulay = 10;
 static void ctx_free(mb_ctx* c) {
   if (!c) return;
   mb_atoms_destroy(&c->atoms);
+  mb_guess_ws_destroy(c->guess_ws);
   void* ptrs[] = {c->d_nat, c->d_coord, c->h, c->w, c->f, c->p, c->pa, c->pold, c->pold2, c->c, c->eigs,
                   c->fdiag, c->scal, c->hws, c->status, c->nrot, c->eig_ws, c->pseudo_ws,
                   c->fppf_hist, c->fock_hist, c->tc_ws_raw, c->pguess};
@@ -349,8 +351,11 @@ extern "C" int mb_ctx_atoms_dev(mb_ctx* c, MbAtomsDev* out) {
   return MB_OK;
 }
 
-extern "C" int mb_guess_predict_density_dev(const mb_guess_model* m, int numat, const int* nat, const double* xyz,
-                                            const int* first, const int* nor, int norbs, double* p, cudaStream_t s);
+extern "C" int mb_guess_predict_density_ws(const mb_guess_model* m, int numat, const int* nat, const double* xyz,
+                                           const int* first, const int* nor, int norbs, double* p, mb_guess_ws* w,
+                                           cudaStream_t s);
+extern "C" int mb_guess_ws_create(mb_guess_ws** out);
+extern "C" int mb_guess_ws_destroy(mb_guess_ws* w);
 
 static int ensure_guess_buffer(mb_ctx* c) {
   if (!c->pguess) MB_CUDA(cudaMalloc(&c->pguess, sizeof(double) * (size_t)c->mpack));
@@ -372,9 +377,10 @@ extern "C" int mb_ctx_guess(mb_ctx* c, const mb_guess_model* m) {
     if (c->nat[a] != 1 && c->nat[a] != 8)
       return mb_set_error(MB_ERR_UNSUPPORTED, "mb_ctx_guess: the network is trained on H and O only");
   MB_TRY(ensure_guess_buffer(c));
+  if (!c->guess_ws) MB_TRY(mb_guess_ws_create(&c->guess_ws));
   c->have_guess = false;
-  MB_TRY(mb_guess_predict_density_dev(m, c->numat, c->d_nat, c->d_coord, c->atoms.first, c->atoms.nor, c->norbs,
-                                      c->pguess, c->stream));
+  MB_TRY(mb_guess_predict_density_ws(m, c->numat, c->d_nat, c->d_coord, c->atoms.first, c->atoms.nor, c->norbs,
+                                     c->pguess, c->guess_ws, c->stream));
   MB_CUDA(cudaStreamSynchronize(c->stream));
   c->have_guess = true;
   return MB_OK;

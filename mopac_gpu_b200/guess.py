@@ -33,7 +33,20 @@ NOUT = (10, 1, 16, 4, 1)
 TYPE_NAMES = ("O own", "H own", "O-O", "O-H", "H-H")
 RPAIR = 6.0
 HERE = os.path.dirname(os.path.abspath(__file__))
-DEFAULT_MODEL = os.path.join(HERE, "data", "guess_pm7_water.npy")
+DEFAULT_MODEL = os.path.join(HERE, "data", "guess_pm7_water.npy")          # lattice clusters
+BOX_MODEL = os.path.join(HERE, "data", "guess_pm7_waterbox.npy")           # liquid-density boxes
+
+
+def make_cluster(kind: str, nw: int, seed: int):
+    """(nat, xyz) of a seeded (H2O)_nw: "lattice" (cubic lattice, 2.9 A, the
+    16-water case's generator) or "box" (random sequential insertion at
+    1.0 g/cm^3, the 512-water box's generator)."""
+    if kind == "lattice":
+        return workloads.water_lattice(nw, seed=seed)
+    if kind == "box":
+        nat, xyz, _ = workloads.water_box(nw, seed=seed)
+        return nat, xyz
+    raise ValueError(kind)
 
 
 def init_blob(seed: int = 0) -> np.ndarray:
@@ -133,8 +146,9 @@ class PairSet:
                                    _ptr(self.ps), _ptr(self.pt), _ptr(work), s))
         self.feat = torch.empty((tot, DIN), dtype=torch.float32, device=dev)
         self.frames = torch.empty((tot, 9), dtype=torch.float64, device=dev)
+        self.ws = torch.empty(int(L.mb_guess_features_ws_bytes(self.numat)), dtype=torch.uint8, device=dev)
         check(L.mb_guess_features_dev(self.numat, _ptr(self.nat), _ptr(self.xyz), tot, _ptr(self.pf), _ptr(self.ps),
-                                      _ptr(self.feat), _ptr(self.frames), s))
+                                      _ptr(self.feat), _ptr(self.frames), _ptr(self.ws), s))
         self.offsets = np.concatenate([[0], np.cumsum(self.counts)]).astype(int)
 
     def targets(self, p_dev_ptr: int):
@@ -160,9 +174,9 @@ KEEP = (1.0, 1.0, 0.3, 0.1, 0.075)   # fraction of each type's pairs kept per cl
 
 
 def generate(n_clusters: int, nmin: int = 8, nmax: int = 64, seed: int = 100, keep=KEEP,
-             log_every: int = 0) -> DataSet:
-    """Converged densities of (H2O)_n lattice clusters, n ~ U{nmin..nmax}, from
-    the plain FP64 SCF; keeps a random fraction of each type's pair blocks."""
+             log_every: int = 0, kind: str = "lattice") -> DataSet:
+    """Converged densities of (H2O)_n clusters, n ~ U{nmin..nmax}, from the
+    plain FP64 SCF; keeps a random fraction of each type's pair blocks."""
     torch = _torch()
     rng = np.random.default_rng(seed)
     g = torch.Generator(device="cuda")
@@ -172,7 +186,7 @@ def generate(n_clusters: int, nmin: int = 8, nmax: int = 64, seed: int = 100, ke
     t_scf, iters = 0.0, []
     for c in range(n_clusters):
         nw = int(rng.integers(nmin, nmax + 1))
-        nat, xyz = workloads.water_lattice(nw, seed=int(rng.integers(1 << 30)))
+        nat, xyz = make_cluster(kind, nw, int(rng.integers(1 << 30)))
         t0 = time.perf_counter()
         ctx = ScfContext(nat, xyz)
         ctx.hcore()
@@ -322,16 +336,16 @@ class EvalResult:
 
 
 def evaluate(model: GuessModel, n_clusters: int = 1000, nmin: int = 32, nmax: int = 128, seed: int = 777,
-             log_every: int = 0, **run_kw) -> EvalResult:
-    """Held-out (H2O)_n lattice clusters: SCF from the standard guess and from
-    the network, same options otherwise."""
+             log_every: int = 0, kind: str = "lattice", **run_kw) -> EvalResult:
+    """Held-out (H2O)_n clusters (seeds disjoint from training): SCF from the
+    standard guess and from the network, same options otherwise."""
     import torch
     rng = np.random.default_rng(seed)
     rows = []
     nfb = 0
     for c in range(n_clusters):
         nw = int(rng.integers(nmin, nmax + 1))
-        nat, xyz = workloads.water_lattice(nw, seed=int(rng.integers(1 << 30)) + (1 << 30))
+        nat, xyz = make_cluster(kind, nw, int(rng.integers(1 << 30)) + (1 << 30))
         ctx = ScfContext(nat, xyz)
         ctx.hcore()
         r0 = ctx.run(**run_kw)
@@ -374,9 +388,12 @@ def main(argv=None):
     ap.add_argument("--eval", type=int, default=1000)
     ap.add_argument("--out", default=DEFAULT_MODEL)
     ap.add_argument("--report", default=None)
+    ap.add_argument("--kind", choices=["lattice", "box"], default="lattice")
+    ap.add_argument("--eval-nmin", type=int, default=32)
+    ap.add_argument("--eval-nmax", type=int, default=128)
     a = ap.parse_args(argv)
     t0 = time.perf_counter()
-    data = generate(a.clusters, a.nmin, a.nmax, log_every=max(1, a.clusters // 10))
+    data = generate(a.clusters, a.nmin, a.nmax, log_every=max(1, a.clusters // 10), kind=a.kind)
     t_data = time.perf_counter() - t0
     print(f"data: {a.clusters} clusters in {t_data:.1f} s (SCF {data.seconds_scf:.1f} s, mean "
           f"{data.mean_niter:.2f} iterations); rows per type {[int(x.shape[0]) for x in data.x]}", flush=True)
@@ -388,11 +405,11 @@ def main(argv=None):
     print(f"trained in {t_train:.1f} s -> {a.out}", flush=True)
     del data
     model = GuessModel(blob)
-    ev = evaluate(model, a.eval, log_every=max(1, a.eval // 10))
-    rep = dict(train_clusters=a.clusters, nmin=a.nmin, nmax=a.nmax, epochs=a.epochs, batch=a.batch,
+    ev = evaluate(model, a.eval, a.eval_nmin, a.eval_nmax, log_every=max(1, a.eval // 10), kind=a.kind)
+    rep = dict(kind=a.kind, train_clusters=a.clusters, nmin=a.nmin, nmax=a.nmax, epochs=a.epochs, batch=a.batch,
                data_s=t_data, train_s=t_train, final_loss=hist[-1], eval_clusters=ev.n_clusters,
                niter_std=ev.niter_std, niter_learned=ev.niter_learned, ms_std=ev.ms_std, ms_learned=ev.ms_learned,
-               max_dhf=ev.max_dhf, n_fallback=ev.n_fallback)
+               max_dhf=ev.max_dhf, n_fallback=ev.n_fallback, eval_nmin=a.eval_nmin, eval_nmax=a.eval_nmax)
     print(json.dumps(rep), flush=True)
     if a.report:
         with open(a.report, "w") as f:

@@ -22,6 +22,13 @@ Cases (sizes of the benchmark configurations):
                 (no SCF before it: the case to run under a launch-list capture)
   pseudo_diag   Fmo + rotation sweep, n = 3072, k = 2048
   pulay         one Pulay step with a full 10-entry history, n = 3072
+  guess_features  learned guess: pair frames + descriptors of the (H2O)512 box
+                (a warp per pair, three passes over the atoms)
+  guess_forward   the five networks on every pair of the (H2O)512 box:
+                2 rows (356*128 + 2*128*128 + 128*16) flops
+  guess_train     one training step (forward, backward, Adam) of the O-H
+                network on 2048 rows: 6 rows params flops
+  guess_predict   the whole prediction into a context (mb_ctx_guess), (H2O)512
   mz_density, mz_helecz, mz_cnvgz, mz_fock, mz_diagg1, mz_diagg2
                 MOZYME blocks, (H2O)4096, 9 A cutoff, synthetic unit LMOs
                 (occupied over 4 A, virtual over 3.2 A, two spare atom slots),
@@ -329,14 +336,78 @@ def run_cases(names, reps):
             qv.close()
         q.close()
         lay.close()
+    if any(c.startswith("guess_") for c in names):
+        out += guess_cases(names, reps, bf16, src)
     if c1 is not None:
         c1.ctx.close()
     return out
 
 
+def guess_cases(names, reps, bf16, src):
+    """Learned-guess kernels on the (H2O)512 box (an untrained, seeded blob:
+    the timing does not depend on the weights)."""
+    from . import guess as G
+    L = lib()
+    out = []
+    nat, xyz, _ = workloads.water_box(512)
+    ps = G.PairSet(nat, xyz)
+    model = G.GuessModel(G.init_blob(0)) if not G.GuessModel.available() else G.GuessModel()
+    DIN_BYTES = G.DIN + 18  # floats of descriptors + the frame's nine doubles
+
+    def hbm_peak():
+        return peaks()["hbm_gbs"]
+    if "guess_features" in names:
+        ms = timed(lambda: check(L.mb_guess_features_dev(ps.numat, ps.nat.data_ptr(), ps.xyz.data_ptr(), ps.n,
+                                                         ps.pf.data_ptr(), ps.ps.data_ptr(), ps.feat.data_ptr(),
+                                                         ps.frames.data_ptr(), ps.ws.data_ptr(), s())), reps)
+        work = 4.0 * ps.n * DIN_BYTES  # descriptors written (FP32) + frames
+        out.append(line("guess_features", ms, work, "GB/s", "FP64 issue / latency", hbm_peak(), src,
+                        pairs=ps.n, atoms=ps.numat,
+                        note="work = descriptor bytes written; the kernel is FP64-issue bound "
+                             "(neighbour lists within 6 A, all atoms for the frame and the long-range terms)"))
+    xs, ys, wss = [], [], []
+    for t in range(G.NTYPES):
+        a, b = ps.offsets[t], ps.offsets[t + 1]
+        x = torch.empty((b - a, G.DIN), dtype=torch.int16, device="cuda")
+        check(L.mb_guess_normalize_dev(model.handle, t, b - a, ps.feat[a:b].data_ptr(), x.data_ptr(), s()))
+        xs.append(x)
+        ys.append(torch.empty((b - a, G.DOUT), dtype=torch.float32, device="cuda"))
+        wss.append(torch.empty(2 * (b - a) * G.HID, dtype=torch.int16, device="cuda"))
+    rows = ps.n
+    flops_row = 2.0 * (G.DIN * G.HID + 2 * G.HID * G.HID + G.HID * G.DOUT)
+    if "guess_forward" in names:
+        def fwd():
+            for t in range(G.NTYPES):
+                if xs[t].shape[0]:
+                    check(L.mb_guess_forward_dev(model.handle, t, xs[t].shape[0], xs[t].data_ptr(),
+                                                 ys[t].data_ptr(), wss[t].data_ptr(), s()))
+        ms = timed(fwd, reps)
+        out.append(line("guess_forward", ms, flops_row * rows, "TFLOP/s", "BF16 tensor (mma.sync)", bf16, src,
+                        rows=rows, launches=4 * G.NTYPES))
+    if "guess_train" in names:
+        n = 2048
+        tr = G.Trainer(G.init_blob(1), n)
+        x = xs[3][:n].contiguous()
+        yt = torch.randn((n, G.DOUT), device="cuda")
+        ms = timed(lambda: tr.step(3, x, yt, 1e-4), reps)
+        params = G.DIN * G.HID + G.HID + 2 * (G.HID * G.HID + G.HID) + G.HID * G.DOUT + G.DOUT
+        out.append(line("guess_train", ms, 6.0 * n * params, "TFLOP/s", "BF16 tensor (mma.sync) / launches", bf16,
+                        src, rows=n, note="forward 2, backward 4 flops per row and parameter; 13 launches"))
+        tr.close()
+    if "guess_predict" in names:
+        ctx = ScfContext(nat, xyz)
+        ms = timed(lambda: ctx.learned_guess(model), reps)
+        out.append(line("guess_predict", ms, flops_row * rows, "TFLOP/s", "descriptors (FP64) + launches", bf16, src,
+                        pairs=rows, note="pairs, descriptors, five networks, assembly, with allocations"))
+        ctx.close()
+    model.close()
+    return out
+
+
 ALL = ["fock2", "helect", "cnvg", "density64", "density_split", "gemm64", "gemm_split", "eigh", "eigh_rand",
        "pseudo_diag",
-       "pulay", "mz_density", "mz_helecz", "mz_cnvgz", "mz_fock", "mz_diagg1", "mz_diagg2"]
+       "pulay", "mz_density", "mz_helecz", "mz_cnvgz", "mz_fock", "mz_diagg1", "mz_diagg2",
+       "guess_features", "guess_forward", "guess_train", "guess_predict"]
 
 
 def main(argv=None):
