@@ -25,13 +25,15 @@ between steps anyway).  The headline metric is SCF single points per second
               times the CPU implementation of the same SCF (the oracle's C
               kernels with LAPACK dsyevd through numpy) on the host cores on a
               bounded sample and extrapolates to one SCF; N > 1: rank 0 only.
---guess learned (default when the trained blob mopac_gpu_b200/data/
-              guess_pm7_water.npy exists) each step starts from the atom-pair
-              network's density (prediction on the device, inside the timed
-              region); standard: the reference's diagonal guess.  The line
-              also gives the SCF from the standard guess and a sample of the
-              learned-guess evaluation on held-out (H2O)_n lattice clusters
-              (n = 32..128) under "learned_guess".
+--converger pulay (default in fast mode) Pulay's DIIS once newdg is set,
+              like the PULAY keyword; cnvg: the default extrapolation.
+--guess standard (default) the reference's diagonal guess; learned: each step
+              starts from the atom-pair network trained on liquid-density
+              boxes (prediction on the device, inside the timed region).
+              Either way the line reports under "learned_guess" the box's
+              fast-path SCF from the network and a sample of the held-out
+              (H2O)_n lattice-cluster evaluation (n = 32..128, plain FP64 path,
+              standard vs learned guess).
 --batch N     also measure the batched workload (default 4096 seeded linear
               alkanes C3-C20, one persistent launch, a CTA per molecule SCF):
               batched SCFs/s on device-resident integrals, the same through
@@ -77,7 +79,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--batch", type=int, default=4096)
-    ap.add_argument("--guess", choices=["learned", "standard"], default="learned")
+    ap.add_argument("--guess", choices=["learned", "standard"], default="standard")
+    ap.add_argument("--converger", choices=["pulay", "cnvg"], default="pulay")
     ap.add_argument("--guess-sample", type=int, default=40)
     return ap.parse_args()
 
@@ -341,22 +344,27 @@ def run_mine(args):
     ctx = ScfContext(nat, xyz)
     ctx.hcore()
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
-    from mopac_gpu_b200.guess import GuessModel
-    model = GuessModel() if args.guess == "learned" and GuessModel.available() else None
-    guess_note = "learned (atom-pair network, prediction inside the timed step)" if model else (
-        "standard diagonal guess" + (" (no trained blob found)" if args.guess == "learned" else ""))
+    from mopac_gpu_b200.guess import BOX_MODEL, GuessModel
+    pul = pseudo and args.converger == "pulay"
+    box_model = GuessModel(path=BOX_MODEL) if GuessModel.available(BOX_MODEL) else None
+    model = box_model if args.guess == "learned" else None
+    guess_note = "learned (atom-pair network trained on liquid-density boxes, prediction inside the timed step)" \
+        if model else "standard diagonal guess" + (" (no trained blob found)" if args.guess == "learned" else "")
+
+    def learned_step(c, mdl):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        c.learned_guess(mdl)
+        tp = (time.perf_counter() - t0) * 1e3
+        rr = c.run(pseudo=pseudo, precision=prec, pulay=pul, guess=True)
+        return rr, tp + rr.t_total_ms, tp
 
     def scf_step(c):
         """One step: (prediction +) SCF; returns (result, step ms, prediction ms)."""
         if model is None:
-            rr = c.run(pseudo=pseudo, precision=prec)
+            rr = c.run(pseudo=pseudo, precision=prec, pulay=pul)
             return rr, rr.t_total_ms, 0.0
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        c.learned_guess(model)
-        tp = (time.perf_counter() - t0) * 1e3
-        rr = c.run(pseudo=pseudo, precision=prec, guess=True)
-        return rr, tp + rr.t_total_ms, tp
+        return learned_step(c, model)
 
     def barrier():
         torch.cuda.synchronize()
@@ -438,28 +446,35 @@ def run_mine(args):
         r64 = rp
     plain = {"scf_wall_s": statistics.mean(plain_ms) / 1000.0, "niter": r64.niter, "escf_kcal_mol": r64.escf,
              "mode": "full FP64 eigensolve every iteration, FP64 GEMMs, standard guess", "steps": len(plain_ms)}
-    # the same fast path from the standard guess (what the network adds)
-    std = None
-    if model is not None:
-        sm = []
-        for i in range(3):
-            flush.fill_(1.0)
-            torch.cuda.synchronize()
-            rs = ctx.run(pseudo=pseudo, precision=prec)
-            if i > 0:
-                sm.append(rs.t_total_ms)
-        std = {"scf_wall_s": statistics.mean(sm) / 1000.0, "niter": rs.niter,
-               "abs_dHf_vs_learned_kcal_mol": abs(rs.escf - r.escf)}
+    # the learned guess on this box (the fast path from the network trained on
+    # liquid-density boxes) and on held-out lattice clusters (its own case)
     guess_eval = None
-    if model is not None and args.guess_sample > 0 and rank == 0:
-        from mopac_gpu_b200.guess import evaluate
-        ev = evaluate(model, n_clusters=args.guess_sample, nmin=32, nmax=128, seed=777)
-        guess_eval = {"workload": "held-out (H2O)_n lattice clusters (as the 16-water case), n ~ U{32..128}, "
-                                  "PM7 1SCF, plain FP64 path, standard vs learned guess",
-                      "clusters": ev.n_clusters, "niter_standard": ev.niter_std, "niter_learned": ev.niter_learned,
-                      "ms_standard": ev.ms_std, "ms_learned_incl_prediction": ev.ms_learned,
-                      "speedup": ev.ms_std / ev.ms_learned, "max_abs_dHf_kcal_mol": ev.max_dhf,
-                      "fallbacks": ev.n_fallback}
+    if rank == 0 and (box_model is not None or GuessModel.available()):
+        guess_eval = {}
+        if box_model is not None:
+            lm = []
+            for i in range(2):
+                flush.fill_(1.0)
+                rl, tl, tpl = learned_step(ctx, box_model)
+                lm.append(tl)
+            guess_eval["box_fast_path"] = {
+                "scf_wall_s_incl_prediction": lm[-1] / 1000.0, "prediction_ms": tpl, "niter": rl.niter,
+                "full_diag": rl.n_full_diag, "pseudo_diag": rl.n_pseudo_diag,
+                "abs_dHf_vs_fp64_kcal_mol": abs(rl.escf - r64.escf),
+                "model": "guess_pm7_waterbox.npy (4000 seeded (H2O)16..64 boxes at 1.0 g/cm^3)",
+                "note": "more full eigensolves than from the standard guess: the prediction's first density change "
+                        "stays above iter's plchek (0.005), so the level shift freezes at the -20 eV of iteration 2"}
+        if GuessModel.available() and args.guess_sample > 0:
+            from mopac_gpu_b200.guess import evaluate
+            ev = evaluate(GuessModel(), n_clusters=args.guess_sample, nmin=32, nmax=128, seed=777)
+            guess_eval["held_out_lattice"] = {
+                "workload": "held-out (H2O)_n lattice clusters (as the 16-water case), n ~ U{32..128}, "
+                            "PM7 1SCF, plain FP64 path, standard vs learned guess",
+                "model": "guess_pm7_water.npy (20000 seeded (H2O)8..64 lattice clusters)",
+                "clusters": ev.n_clusters, "niter_standard": ev.niter_std, "niter_learned": ev.niter_learned,
+                "ms_standard": ev.ms_std, "ms_learned_incl_prediction": ev.ms_learned,
+                "speedup": ev.ms_std / ev.ms_learned, "max_abs_dHf_kcal_mol": ev.max_dhf,
+                "fallbacks": ev.n_fallback}
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         os.environ.setdefault("OPENBLAS_NUM_THREADS", str(os.cpu_count()))
@@ -477,13 +492,14 @@ def run_mine(args):
             "vs_baseline": None, "dtype": "f64" if prec == 0 else "f64+bf16x3",
             "data": "synthetic (seeded water box, random sequential insertion)",
             "config": {"workload": WORKLOAD, "mode": args.mode, "precision": args.precision, "guess": args.guess,
+                       "converger": "pulay" if pul else "cnvg",
                        "parallelism": f"replicas x{ws}",
                        "l2": "flushed between steps (256 MB write); W = 151 MB > L2",
                        "cell_edge_A": round(edge, 3)},
             "scf_wall_s": t_ms / 1000.0,
             "guess": guess_note,
+            "converger": "pulay" if pul else "cnvg",
             "guess_prediction_ms": statistics.mean(pred_ms),
-            "standard_guess_same_path": std,
             "learned_guess": guess_eval,
             "scf": {"escf_kcal_mol": r.escf, "niter": r.niter, "full_diag": r.n_full_diag,
                     "pseudo_diag": r.n_pseudo_diag, "split_iterations": r.n_split, "converged": r.converged,

@@ -22,6 +22,10 @@ Cases (sizes of the benchmark configurations):
                 (no SCF before it: the case to run under a launch-list capture)
   pseudo_diag   Fmo + rotation sweep, n = 3072, k = 2048
   pulay         one Pulay step with a full 10-entry history, n = 3072
+  batch         the batched SCF of seeded alkanes C3..C20 (--batch-n
+                molecules, default 4096), one persistent launch, default
+                launch configuration: SCF/s and FP64 flops of the reduction,
+                back-transformation and density per iteration
   guess_features  learned guess: pair frames + descriptors of the (H2O)512 box
                 (a warp per pair, three passes over the atoms)
   guess_forward   the five networks on every pair of the (H2O)512 box:
@@ -338,9 +342,39 @@ def run_cases(names, reps):
         lay.close()
     if any(c.startswith("guess_") for c in names):
         out += guess_cases(names, reps, bf16, src)
+    if "batch" in names:
+        out += batch_case(reps)
     if c1 is not None:
         c1.ctx.close()
     return out
+
+
+BATCH_N = 4096
+
+
+def batch_case(reps):
+    from .batch import Batch
+    mols = workloads.alkane_batch(BATCH_N)
+    b = Batch(mols)
+    res = {}
+
+    def run():
+        res["r"] = b.run()
+    ms = timed(run, reps)
+    escf, niter, conv, _ = res["r"]
+    flops = 0.0
+    for m, (nat, _) in enumerate(mols):
+        n = int(np.where(np.asarray(nat) == 1, 1, 4).sum())
+        k = n // 2  # alkanes: valence electrons = basis functions
+        flops += niter[m] * (4.0 * n ** 3 / 3.0 + 3.0 * n * n * k)
+    fp64 = fp64_peak_tflops()
+    nb, grid = b.config()
+    b.close()
+    return [line("batch", ms, flops, "TFLOP/s", "FP64 latency (barriers, dependent chains)", fp64, "measured here",
+                 molecules=len(mols), scf_per_s=len(mols) / (ms * 1e-3), niter_mean=float(np.mean(niter)),
+                 converged=bool(conv.all()), back_transform_block=nb, grid=grid,
+                 note="flops: per iteration 4n^3/3 (reduction) + 2n^2 nocc (back-transformation) + "
+                      "n^2 nocc (density); nocc = electrons/2 of an alkane = n/2")]
 
 
 def guess_cases(names, reps, bf16, src):
@@ -407,7 +441,7 @@ def guess_cases(names, reps, bf16, src):
 ALL = ["fock2", "helect", "cnvg", "density64", "density_split", "gemm64", "gemm_split", "eigh", "eigh_rand",
        "pseudo_diag",
        "pulay", "mz_density", "mz_helecz", "mz_cnvgz", "mz_fock", "mz_diagg1", "mz_diagg2",
-       "guess_features", "guess_forward", "guess_train", "guess_predict"]
+       "guess_features", "guess_forward", "guess_train", "guess_predict", "batch"]
 
 
 def main(argv=None):
@@ -415,7 +449,10 @@ def main(argv=None):
     ap.add_argument("cases", nargs="*", default=ALL)
     ap.add_argument("--reps", type=int, default=5)
     ap.add_argument("--out", default=None)
+    ap.add_argument("--batch-n", type=int, default=4096)
     a = ap.parse_args(argv)
+    global BATCH_N
+    BATCH_N = a.batch_n
     bad = [c for c in a.cases if c not in ALL]
     if bad:
         raise SystemExit(f"unknown cases {bad}; known: {ALL}")
