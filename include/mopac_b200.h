@@ -428,9 +428,17 @@ size_t mb_guess_blob_floats(void);
 int mb_guess_model_create(const float* blob, mb_guess_model** out);
 int mb_guess_model_destroy(mb_guess_model* model);
 /* Predicts the context's starting density on the device (H and O only; other
- * elements return MB_ERR_UNSUPPORTED and the caller keeps the standard guess).
- * Use with opts.guess = 1. */
-int mb_ctx_guess(mb_ctx* ctx, const mb_guess_model* model);
+ * elements return MB_ERR_UNSUPPORTED and the caller keeps the standard guess),
+ * then applies purify_steps McWeeny purifications (1 recommended; see
+ * mb_guess_purify_dev).  Use with opts.guess = 1. */
+int mb_ctx_guess(mb_ctx* ctx, const mb_guess_model* model, int purify_steps);
+/* McWeeny purification of a packed total density p (device, mpack): D = p/2,
+ * D <- 3 D^2 - 2 D^3 steps times (FP64 GEMMs), p = 2 D.  It moves D's
+ * eigenvalues towards 0 and 1, i.e. towards a closed-shell density, which
+ * keeps iter's first density change small.  ws: mb_guess_purify_ws_bytes(n)
+ * bytes of device scratch. */
+size_t mb_guess_purify_ws_bytes(int n);
+int mb_guess_purify_dev(int n, double* p, int steps, void* ws, cudaStream_t stream);
 /* The steps, on device pointers.  Pairs: counts_host[NTYPES] receives the
  * per-type counts; with pf == NULL only counting is done; otherwise pf/ps/pt
  * (first atom, second atom, type) are filled type by type (order inside a

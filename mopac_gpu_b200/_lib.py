@@ -160,7 +160,9 @@ SIGNATURES = {
     "eigenvectors_lapack_": ([_P] * 4, None),
     "diag_for_gpu_": ([_P] * 6, None),
     "mb_ctx_set_guess": ([_P, _P], _I),
-    "mb_ctx_guess": ([_P, _P], _I),
+    "mb_ctx_guess": ([_P, _P, _I], _I),
+    "mb_guess_purify_ws_bytes": ([_I], ctypes.c_size_t),
+    "mb_guess_purify_dev": ([_I, _P, _I, _P, _P], _I),
     "mb_guess_blob_floats": ([], ctypes.c_size_t),
     "mb_guess_model_create": ([_P, ctypes.POINTER(_P)], _I),
     "mb_guess_model_destroy": ([_P], _I),

@@ -932,6 +932,62 @@ extern "C" int mb_guess_predict_density_dev(const mb_guess_model* m, int numat, 
   return rc;
 }
 
+// ------------------------------------------------------------ purification
+// McWeeny purification of a predicted total density P: D = P/2 is replaced
+// by 3 D^2 - 2 D^3 (steps times), which pulls D's eigenvalues towards 0 and 1
+// -- a closed-shell density matrix -- with FP64 GEMMs.
+namespace {
+__global__ void unpack_half_kernel(int n, const double* __restrict__ pk, double* __restrict__ d) {
+  long long nn = (long long)n * n;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < nn; q += (long long)gridDim.x * blockDim.x) {
+    int i = (int)(q % n), j = (int)(q / n);
+    int r = i > j ? i : j, c = i > j ? j : i;
+    d[q] = pk[mb_tri(r, c)] * 0.5;
+  }
+}
+__global__ void mcweeny_kernel(long long nn, const double* __restrict__ d2, const double* __restrict__ d3,
+                               double* __restrict__ d) {
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < nn; q += (long long)gridDim.x * blockDim.x)
+    d[q] = 3.0 * d2[q] - 2.0 * d3[q];
+}
+__global__ void pack_twice_kernel(int n, const double* __restrict__ d, double* __restrict__ pk) {
+  long long mp = (long long)n * (n + 1) / 2;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < mp; q += (long long)gridDim.x * blockDim.x) {
+    int r = (int)((sqrt(8.0 * (double)q + 1.0) - 1.0) * 0.5);
+    while ((long long)r * (r + 1) / 2 > q) --r;
+    while ((long long)(r + 1) * (r + 2) / 2 <= q) ++r;
+    int c = (int)(q - (long long)r * (r + 1) / 2);
+    pk[q] = d[r + (long long)c * n] + d[c + (long long)r * n];  // 2 * the symmetric part
+  }
+}
+}  // namespace
+
+extern "C" int mb_dgemm_dev(char transa, char transb, int m, int n, int k, double alpha, const double* a, int lda,
+                            const double* b, int ldb, double beta, double* c, int ldc, cudaStream_t stream);
+
+extern "C" size_t mb_guess_purify_ws_bytes(int n) { return sizeof(double) * 3 * (size_t)n * n; }
+
+extern "C" int mb_guess_purify_dev(int n, double* p, int steps, void* ws, cudaStream_t s) {
+  if (n <= 0 || !p || steps < 0 || (steps > 0 && !ws)) return mb_set_error(MB_ERR_ARG, "mb_guess_purify_dev: bad args");
+  if (steps == 0) return MB_OK;
+  const long long nn = (long long)n * n;
+  double* d = (double*)ws;
+  double* d2 = d + nn;
+  double* d3 = d2 + nn;
+  const int grid = 148 * 8;
+  unpack_half_kernel<<<grid, 256, 0, s>>>(n, p, d);
+  MB_LAUNCH_CHECK();
+  for (int it = 0; it < steps; ++it) {
+    MB_TRY(mb_dgemm_dev('N', 'N', n, n, n, 1.0, d, n, d, n, 0.0, d2, n, s));
+    MB_TRY(mb_dgemm_dev('N', 'N', n, n, n, 1.0, d2, n, d, n, 0.0, d3, n, s));
+    mcweeny_kernel<<<grid, 256, 0, s>>>(nn, d2, d3, d);
+    MB_LAUNCH_CHECK();
+  }
+  pack_twice_kernel<<<grid, 256, 0, s>>>(n, d, p);
+  MB_LAUNCH_CHECK();
+  return MB_OK;
+}
+
 // ======================================================================
 //                                  trainer
 // ======================================================================

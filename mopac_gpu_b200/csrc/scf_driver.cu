@@ -157,6 +157,7 @@ struct mb_ctx {
   double* pguess = nullptr;
   bool have_guess = false;
   mb_guess_ws* guess_ws = nullptr;  // the prediction's grow-only workspace
+  void* purify_ws = nullptr;        // McWeeny matrices when eig_ws is too small
   cudaStream_t stream = nullptr;
 };
 
@@ -169,7 +170,7 @@ static void ctx_free(mb_ctx* c) {
   mb_guess_ws_destroy(c->guess_ws);
   void* ptrs[] = {c->d_nat, c->d_coord, c->h, c->w, c->f, c->p, c->pa, c->pold, c->pold2, c->c, c->eigs,
                   c->fdiag, c->scal, c->hws, c->status, c->nrot, c->eig_ws, c->pseudo_ws,
-                  c->fppf_hist, c->fock_hist, c->tc_ws_raw, c->pguess};
+                  c->fppf_hist, c->fock_hist, c->tc_ws_raw, c->pguess, c->purify_ws};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -371,8 +372,11 @@ extern "C" int mb_ctx_set_guess(mb_ctx* c, const double* p) {
   return MB_OK;
 }
 
-extern "C" int mb_ctx_guess(mb_ctx* c, const mb_guess_model* m) {
-  if (!c || !m) return mb_set_error(MB_ERR_ARG, "mb_ctx_guess: bad args");
+extern "C" size_t mb_guess_purify_ws_bytes(int n);
+extern "C" int mb_guess_purify_dev(int n, double* p, int steps, void* ws, cudaStream_t s);
+
+extern "C" int mb_ctx_guess(mb_ctx* c, const mb_guess_model* m, int purify_steps) {
+  if (!c || !m || purify_steps < 0) return mb_set_error(MB_ERR_ARG, "mb_ctx_guess: bad args");
   for (int a = 0; a < c->numat; ++a)
     if (c->nat[a] != 1 && c->nat[a] != 8)
       return mb_set_error(MB_ERR_UNSUPPORTED, "mb_ctx_guess: the network is trained on H and O only");
@@ -381,6 +385,17 @@ extern "C" int mb_ctx_guess(mb_ctx* c, const mb_guess_model* m) {
   c->have_guess = false;
   MB_TRY(mb_guess_predict_density_ws(m, c->numat, c->d_nat, c->d_coord, c->atoms.first, c->atoms.nor, c->norbs,
                                      c->pguess, c->guess_ws, c->stream));
+  if (purify_steps > 0) {
+    // the purification's three n x n matrices: the eigensolver workspace when
+    // it is large enough (idle before the SCF), else a buffer the context keeps
+    void* ws = c->eig_ws;
+    if (mb_guess_purify_ws_bytes(c->norbs) > mb_eigh_ws_bytes(c->norbs)) {
+      if (!c->purify_ws) MB_CUDA(cudaMalloc(&c->purify_ws, mb_guess_purify_ws_bytes(c->norbs)));
+      ws = c->purify_ws;
+    }
+    MB_TRY(mb_guess_purify_dev(c->norbs, c->pguess, purify_steps, ws, c->stream));
+    MB_CUDA(cudaStreamSynchronize(c->stream));
+  }
   MB_CUDA(cudaStreamSynchronize(c->stream));
   c->have_guess = true;
   return MB_OK;

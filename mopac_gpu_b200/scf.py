@@ -75,10 +75,11 @@ class ScfContext:
         assert p.size == self.mpack
         check(lib().mb_ctx_set_guess(self._h, p.ctypes.data))
 
-    def learned_guess(self, model) -> None:
+    def learned_guess(self, model, purify: int = 1) -> None:
         """Starting density predicted on the device by the atom-pair network
-        (``guess.GuessModel``); use with ``run(guess=True)``."""
-        check(lib().mb_ctx_guess(self._h, model.handle))
+        (``guess.GuessModel``), then ``purify`` McWeeny steps; use with
+        ``run(guess=True)``."""
+        check(lib().mb_ctx_guess(self._h, model.handle, int(purify)))
 
     def run(self, pseudo: bool = False, scfcrt: float = 1.0e-4, itrmax: int = 2000, precision: int = 0,
             switch_pl: float = 1.0e-4, verbose: bool = False, pulay: bool = False,

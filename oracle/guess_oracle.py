@@ -402,6 +402,17 @@ def adam(p, g, m, v, step: int, lr: float, b1: float = 0.9, b2: float = 0.999, e
         p[k][:] = p[k] - lr * (m[k] / c1) / (np.sqrt(v[k] / c2) + eps)
 
 
+def purify(p_packed, n: int, steps: int = 1) -> np.ndarray:
+    """McWeeny purification of a packed total density: D = P/2,
+    D <- 3 D^2 - 2 D^3 (steps times), P = 2 D (symmetric part)."""
+    from oracle.scf_oracle import pack, unpack
+    D = unpack(np.asarray(p_packed, np.float64), n) * 0.5
+    for _ in range(steps):
+        D2 = D @ D
+        D = 3.0 * D2 - 2.0 * (D2 @ D)
+    return pack(D + D.T)
+
+
 def predict_density(blob, nat, xyz) -> np.ndarray:
     """The learned guess end to end on the CPU (packed total density)."""
     types = unpack_blob(blob)

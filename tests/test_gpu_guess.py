@@ -213,6 +213,21 @@ def test_device_prediction_matches_oracle(cluster):
     ctx.close()
 
 
+def test_purification_matches_oracle(cluster):
+    from mopac_gpu_b200._lib import lib
+    nat, xyz, s, r = cluster
+    rng = np.random.default_rng(7)
+    g = r.p + rng.normal(scale=3e-3, size=r.p.shape) * (np.abs(r.p) > 1e-3)
+    for steps in (0, 1, 2):
+        p = torch.tensor(g, dtype=torch.float64, device="cuda")
+        ws = torch.empty(int(lib().mb_guess_purify_ws_bytes(s.norbs)), dtype=torch.uint8, device="cuda")
+        assert lib().mb_guess_purify_dev(s.norbs, p.data_ptr(), steps, ws.data_ptr(),
+                                         torch.cuda.current_stream().cuda_stream) == 0
+        torch.cuda.synchronize()
+        po = go.purify(g, s.norbs, steps) if steps else g
+        assert np.abs(p.cpu().numpy() - po).max() < 1e-10, steps
+
+
 def test_trained_network_cuts_iterations_and_keeps_the_heat():
     from mopac_gpu_b200.guess import GuessModel, evaluate
     if not GuessModel.available():

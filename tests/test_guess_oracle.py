@@ -132,3 +132,37 @@ def test_oracle_scf_from_converged_density_is_short(cluster):
     r2 = so.iter_scf(s, p_guess=r.p)
     assert r2.converged and abs(r2.escf - r.escf) < 1e-4
     assert r2.niter <= 6 < r.niter
+
+
+def test_mcweeny_purification_moves_towards_idempotent(cluster):
+    nat, xyz, s, r = cluster
+    rng = np.random.default_rng(6)
+    g = r.p + rng.normal(scale=3e-3, size=r.p.shape) * (np.abs(r.p) > 1e-3)
+    n = s.norbs
+
+    def idem(p):
+        D = so.unpack(p, n) / 2
+        return np.linalg.norm(D @ D - D)
+    pp = go.purify(g, n, 1)
+    assert idem(pp) < 0.2 * idem(g)
+    assert abs(so.unpack(pp, n).trace() - 2 * s.nclose) < 0.05
+    assert np.array_equal(go.purify(g, n, 0), so.pack(so.unpack(g, n)))
+
+
+def test_trained_network_guess_shortens_the_oracle_scf():
+    """The committed lattice network, purified once, seeds the oracle's iter:
+    same heat (1e-4 kcal/mol), fewer iterations than the diagonal guess."""
+    import os
+    from mopac_gpu_b200 import workloads
+    path = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "mopac_gpu_b200", "data",
+                        "guess_pm7_water.npy")
+    if not os.path.exists(path):
+        pytest.skip("no trained blob")
+    blob = np.load(path)
+    nat, xyz = workloads.water_lattice(16)
+    s = so.make_system(nat, xyz)
+    r0 = so.iter_scf(s)
+    g = go.purify(go.predict_density(blob, nat, xyz), s.norbs, 1)
+    r1 = so.iter_scf(s, p_guess=g)
+    assert r1.converged and abs(r1.escf - r0.escf) < 1e-4
+    assert r1.niter < r0.niter
