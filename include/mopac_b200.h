@@ -498,6 +498,26 @@ int mb_guess_trainer_step(mb_guess_trainer* trainer, int type, int n, const unsi
 /* Copies the parameter blob and the last step's gradients (same layout) to host. */
 int mb_guess_trainer_get(mb_guess_trainer* trainer, float* params, float* grads);
 
+/* ------------------------------------------- electronic-state exchange */
+/* DENOUT / OLDENS density restart file, den_in_out (SCF/iter.F90:1133-1227):
+ * one record "norbs, numat, pa(mpack)" with pa the alpha density (P/2 for a
+ * closed shell); formatted = 0 writes gfortran's unformatted sequential
+ * layout (4-byte length markers), 1 list-directed text (DENOUTF).  Reading
+ * tries *formatted first (0 if formatted is NULL) and the other format
+ * second; on return *formatted says which one was read.  A file for another
+ * system fails with "Density file read in does not match current data set",
+ * an unreadable one with "Density Restart File missing or corrupt". */
+int mb_den_write(const char* path, int norbs, int numat, const double* pa, int formatted);
+int mb_den_read(const char* path, int norbs, int numat, double* pa, int* formatted);
+/* struct mopac_state (include/mopac.h:123-132) save and load,
+ * mopac_save / mopac_load (interface/mopac_api_saveload.F90:26-78): save
+ * gives mpack, uhf (0) and pa = P/2 of the context's current density (pa NULL:
+ * size query); load makes pa the starting density of the next mb_scf_run with
+ * opts.guess = 1 (mpack 0: nothing to load; a state of another size or a UHF
+ * state: "Attempting to load incompatible MOPAC state"). */
+int mb_ctx_save_state(mb_ctx* ctx, int* mpack, int* uhf, double* pa);
+int mb_ctx_load_state(mb_ctx* ctx, int mpack, int uhf, const double* pa, const double* pb);
+
 /* ------------------------------------- (1) reference bind(C) symbols */
 /* src/gpu/cuda_wrappers.cu:192 (cublas_interfaces.F90:9-21) */
 void call_gemm_cublas(char tra, char trb, int m, int n, int k, double alpha, const double* A,

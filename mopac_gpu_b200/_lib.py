@@ -160,6 +160,10 @@ SIGNATURES = {
     "eigenvectors_lapack_": ([_P] * 4, None),
     "diag_for_gpu_": ([_P] * 6, None),
     "mb_ctx_set_guess": ([_P, _P], _I),
+    "mb_den_write": ([ctypes.c_char_p, _I, _I, _P, _I], _I),
+    "mb_den_read": ([ctypes.c_char_p, _I, _I, _P, ctypes.POINTER(_I)], _I),
+    "mb_ctx_save_state": ([_P, ctypes.POINTER(_I), ctypes.POINTER(_I), _P], _I),
+    "mb_ctx_load_state": ([_P, _I, _I, _P, _P], _I),
     "mb_ctx_guess": ([_P, _P, _I], _I),
     "mb_guess_purify_ws_bytes": ([_I], ctypes.c_size_t),
     "mb_guess_purify_dev": ([_I, _P, _I, _P, _P], _I),
