@@ -40,7 +40,9 @@ between steps anyway).  The headline metric is SCF single points per second
               the C ABI from host coordinates (integrals included), the plain
               FP64 GPU path (one molecule at a time) and the CPU oracle on
               samples; reported under "batched".  0 skips it.
-Multi-GPU: replicas only (independent SCFs per rank, no data-path collective).
+Multi-GPU: replicas only (independent SCFs per rank, no data-path
+collective); the batched workload gives each rank its share of a list of
+--batch x N alkanes (mopac_gpu_b200.replicas.shard), times are max over ranks.
 """
 from __future__ import annotations
 
@@ -199,20 +201,29 @@ def cpu_batch_rate(mols, nsample: int, workers: int):
     return len(sample) / dt, len(sample)
 
 
-def run_batch(args, flush, L):
-    """The batched workload on this GPU; returns the "batched" object."""
+def run_batch(args, flush, L, ws=1, rank=0, dist=None):
+    """The batched workload; returns the "batched" object on rank 0 (None on
+    the others).  Under torchrun the job is args.batch molecules per GPU: a
+    seeded list of args.batch * N alkanes split over the ranks by
+    replicas.shard (cost n^3, balanced), no data-path collective; times are
+    the max over ranks."""
     import numpy as np
     import torch
     from mopac_gpu_b200 import ScfContext, workloads
     from mopac_gpu_b200.batch import Batch
-    mols = workloads.alkane_batch(args.batch)
-    nat_tot = sum(len(m[0]) for m in mols)
+    from mopac_gpu_b200.replicas import max_over_ranks, shard
+    mols_all = workloads.alkane_batch(args.batch * ws)
+    costs = [float(np.where(np.asarray(m[0]) == 1, 1, 4).sum()) ** 3 for m in mols_all]
+    mols = [mols_all[i] for i in shard(costs, rank, ws)]
+    nat_tot = sum(len(m[0]) for m in mols_all)
     b = Batch(mols)
     # launch configuration chosen by the autotuner on this batch (untimed, like
     # the warm-up); the runs below replay the captured graph of that launch
     tuned_nb, tuned_per, tuned_ms = b.autotune()
     for _ in range(args.warmup):
         b.run()
+    if dist is not None:
+        dist.barrier()
     times = []
     l0 = L.mb_launch_count()
     for _ in range(args.steps):
@@ -221,7 +232,7 @@ def run_batch(args, flush, L):
         escf, niter, conv, t_ms = b.run()
         times.append(t_ms)
     launches = L.mb_launch_count() - l0
-    t_ms = statistics.mean(times)
+    t_ms = max_over_ranks(statistics.mean(times), dist, "cuda")
     b.set_phase_timing(True)
     b.run()
     ph = b.phase_cycles()
@@ -242,8 +253,10 @@ def run_batch(args, flush, L):
         torch.cuda.synchronize()
         if step > 0:
             e2e_t.append(time.perf_counter() - t0)
-    te = statistics.mean(e2e_t)
-    # the plain FP64 GPU path, one molecule at a time, on a sample
+    te = max_over_ranks(statistics.mean(e2e_t), dist, "cuda")
+    if rank != 0:
+        return None
+    # the plain FP64 GPU path, one molecule at a time, on a sample (rank 0)
     nplain = min(32, len(mols))
     stepp = max(1, len(mols) // nplain)
     idx = list(range(0, len(mols), stepp))[:nplain]
@@ -258,8 +271,8 @@ def run_batch(args, flush, L):
         ctx.close()
     plain_rate = len(idx) / (sum(plain_ms) / 1000.0)
     out = {
-        "workload": f"{len(mols)} {BATCH_WORKLOAD}",
-        "metric": "batched_scfs_per_s", "value": len(mols) / (t_ms / 1000.0), "unit": "SCF/s",
+        "workload": f"{len(mols_all)} {BATCH_WORKLOAD}" + (f", {args.batch} per GPU on {ws} GPUs" if ws > 1 else ""),
+        "metric": "batched_scfs_per_s", "value": len(mols_all) / (t_ms / 1000.0), "unit": "SCF/s",
         "ms_per_step": t_ms, "steps": args.steps, "warmup": args.warmup, "dtype": "f64",
         "l2": "flushed between steps (256 MB write)",
         "atoms": nat_tot, "niter_mean": float(np.mean(niter)), "niter_max": int(niter.max()),
@@ -273,9 +286,10 @@ def run_batch(args, flush, L):
                            "mode": "one molecule at a time through mb_scf_run, full FP64 eigensolve every "
                                    "iteration, integrals resident",
                            "max_abs_dHf_vs_batched_kcal_mol": float(max(dhf))},
-        "speedup_vs_plain_fp64": (len(mols) / (t_ms / 1000.0)) / plain_rate,
-        "e2e": {"value": len(mols) / te, "unit": "SCF/s", "h2d_bytes_per_step": 28 * nat_tot + 4 * len(mols),
-                "d2h_bytes_per_step": 8 * len(mols), "wall_s": te,
+        "speedup_vs_plain_fp64": (len(mols_all) / (t_ms / 1000.0)) / plain_rate,
+        "e2e": {"value": len(mols_all) / te, "unit": "SCF/s",
+                "h2d_bytes_per_step": 28 * nat_tot + 4 * len(mols_all),
+                "d2h_bytes_per_step": 8 * len(mols_all), "wall_s": te,
                 "includes": "batch creation (atoms to the device, integrals on the GPU), SCFs, heats to the host"},
     }
     if not args.no_cpu_baseline:
@@ -398,11 +412,8 @@ def run_mine(args):
         cnt, tot = ctypes.c_longlong(0), ctypes.c_double(0.0)
         L.mb_kstats_read(kid, ctypes.byref(cnt), ctypes.byref(tot))
         kst[name] = {"launches": cnt.value, "total_ms": tot.value}
-    t_ms = statistics.mean(times)
-    if dist is not None:
-        tt = torch.tensor([t_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_ms = float(tt.item())
+    from mopac_gpu_b200.replicas import max_over_ranks
+    t_ms = max_over_ranks(statistics.mean(times), dist, "cuda")
     r = results[-1]
     # ---- end to end through the C ABI with host buffers
     e2e = None
@@ -422,11 +433,7 @@ def run_mine(args):
             torch.cuda.synchronize()
             if step > 0:
                 e2e_t.append(time.perf_counter() - t0)
-        te = statistics.mean(e2e_t)
-        if dist is not None:
-            tt = torch.tensor([te], device="cuda", dtype=torch.float64)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            te = float(tt.item())
+        te = max_over_ranks(statistics.mean(e2e_t), dist, "cuda")
         e2e = {"value": ws / te, "unit": "SCF/s", "h2d_bytes_per_step": 8 * (ctx.mpack + ctx.n2elec),
                "d2h_bytes_per_step": 8 * ctx.mpack, "scf_wall_s": te}
     # ---- rooflines: the dominant kernel (Householder panel) from the events
@@ -446,6 +453,9 @@ def run_mine(args):
         r64 = rp
     plain = {"scf_wall_s": statistics.mean(plain_ms) / 1000.0, "niter": r64.niter, "escf_kcal_mol": r64.escf,
              "mode": "full FP64 eigensolve every iteration, FP64 GEMMs, standard guess", "steps": len(plain_ms)}
+    # the batched workload: every rank takes part (its collectives come before
+    # any rank-0-only work)
+    batched = run_batch(args, flush, L, ws, rank, dist) if args.batch > 0 else None
     # the learned guess on this box (the fast path from the network trained on
     # liquid-density boxes) and on held-out lattice clusters (its own case)
     guess_eval = None
@@ -485,8 +495,6 @@ def run_mine(args):
         cpu = {"value": 1.0 / t_scf, "unit": "SCF/s", "cores": os.cpu_count(), "kind": "port",
                "sample": f"one SCF iteration of the CPU oracle (fock2 in C, LAPACK dsyevd, density, cnvg) "
                          f"scaled by {CPU_NITER_FALLBACK} iterations", "scf_wall_s": t_scf}
-    # the batched workload is a one-GPU measurement (skipped under torchrun)
-    batched = run_batch(args, flush, L) if args.batch > 0 and ws == 1 else None
     if rank == 0:
         line = {
             "metric": METRIC, "value": ws * 1000.0 / t_ms, "unit": "SCF/s", "n_gpus": ws, "steps": args.steps,
