@@ -212,3 +212,233 @@ def diagg2(iorbs, occ, vir, ifmo, fmo, nij, eigs, eigv, idiagg, ctl, nrejct):
                            np.ascontiguousarray(eigs), np.ascontiguousarray(eigv), int(idiagg),
                            np.ascontiguousarray(ctl, np.float64), nrejct, ctypes.byref(nrej))
     return sumb, nrej.value
+
+
+# ------------------------------------------------------------ the SCF loop
+# The MOZYME SCF (iter_for_MOZYME) on the oracle's kernels, with the routines
+# its loop calls between them: check, eimp, hbonds/addhb, isitsc, and a
+# starting-LMO builder for water that stands in for makvec.
+
+def check_lmos(lmos, iorbs) -> float:
+    """check (MOZYME/check.F90:1-60): renormalise every LMO over its atoms;
+    returns the summed |1 - norm^2| (the reference stops above 0.1)."""
+    ncf, nncf, icocc, ncocc, cocc = lmos
+    err = 0.0
+    for i in range(len(ncf)):
+        n = int(sum(iorbs[icocc[nncf[i] + j] - 1] for j in range(ncf[i])))
+        seg = cocc[ncocc[i]:ncocc[i] + n]
+        ssum = float(np.sum(seg * seg))
+        err += abs(1.0 - ssum)
+        cocc[ncocc[i]:ncocc[i] + n] = seg * (1.0 / np.sqrt(ssum))
+    return err
+
+
+def eimp(iorbs, nijbo, p, f) -> None:
+    """eimp (MOZYME/eimp.F90): the first element of every stored
+    off-diagonal block of p becomes that block's sum of squared F elements,
+    the pair weight diagg1 reads (the next density build overwrites it)."""
+    for i in range(len(iorbs)):
+        for j in range(i):
+            k = int(nijbo[i, j])
+            if k >= 0:
+                m = int(iorbs[i] * iorbs[j])
+                p[k] = float(np.sum(f[k:k + m] ** 2))
+
+
+HB_LIMITS = (1.0, 0.1, 0.01, 0.001)   # addhb.F90: hblims
+
+
+def hbonds(iorbs, nijbo, fao, p, occ, vir, cutoff: float, cap: int):
+    """hbonds (MOZYME/hbonds.F90): for every stored atom pair (i > j) with no
+    density yet (sum P^2 < 1e-10) but a Fock block above cutoff, every
+    virtual LMO whose first or second atom is i or j paired with every
+    occupied LMO of that kind, with the nominal element 0.1, in the
+    reference's loop order.  Returns (nij, ifmo, fmo) in diagg1's layout."""
+    ncf, nncf, icocc = occ[0], occ[1], occ[2]
+    nce, nnce, icvir = vir[0], vir[1], vir[2]
+    ifmo = np.zeros(2 * cap, np.int32)
+    fmo = np.zeros(cap)
+    nij = 0
+    for i in range(len(iorbs)):
+        for j in range(i):
+            k = int(nijbo[i, j])
+            if k < 0:
+                continue
+            m = int(iorbs[i] * iorbs[j])
+            sumf = float(np.sum(fao[k:k + m] ** 2))
+            sump = float(np.sum(p[k:k + m] ** 2))
+            if not (sump < 1.0e-10 and sumf > cutoff):
+                continue
+            used = []
+            for q in range(len(ncf)):
+                kk = min(int(ncf[q]) - 1, 1)
+                l0 = int(nncf[q])
+                if icocc[l0] - 1 in (i, j) or icocc[l0 + kk] - 1 in (i, j):
+                    used.append(q)
+            for q in range(len(nce)):
+                kk = min(int(nce[q]) - 1, 1)
+                l0 = int(nnce[q])
+                if icvir[l0] - 1 in (i, j) or icvir[l0 + kk] - 1 in (i, j):
+                    for u in used:
+                        if nij >= cap:
+                            raise RuntimeError("hbonds: list capacity exceeded")
+                        fmo[nij] = 0.1
+                        ifmo[2 * nij] = q + 1
+                        ifmo[2 * nij + 1] = u + 1
+                        nij += 1
+    return nij, ifmo, fmo
+
+
+def _pipek_mezey(C: np.ndarray, atom_of: np.ndarray, natoms: int, sweeps: int = 100) -> np.ndarray:
+    """Pipek-Mezey localisation (Jacobi sweeps) of the columns of C in an
+    orthonormal AO basis (NDDO): maximises sum over MOs and atoms of the
+    squared atomic populations."""
+    C = C.copy()
+    n = C.shape[1]
+    masks = [atom_of == a for a in range(natoms)]
+    for _ in range(sweeps):
+        biggest = 0.0
+        for i in range(n):
+            for j in range(i + 1, n):
+                A = B = 0.0
+                for m in masks:
+                    qii = float(np.sum(C[m, i] ** 2))
+                    qjj = float(np.sum(C[m, j] ** 2))
+                    qij = float(np.sum(C[m, i] * C[m, j]))
+                    A += qij * qij - 0.25 * (qii - qjj) ** 2
+                    B += qij * (qii - qjj)
+                if A * A + B * B < 1.0e-24:
+                    continue
+                g = 0.25 * np.arccos(-A / np.hypot(A, B)) * (1.0 if B >= 0.0 else -1.0)
+                c, s = np.cos(g), np.sin(g)
+                ci, cj = C[:, i].copy(), C[:, j].copy()
+                C[:, i] = c * ci + s * cj
+                C[:, j] = -s * ci + c * cj
+                biggest = max(biggest, abs(g))
+        if biggest < 1.0e-10:
+            break
+    return C
+
+
+def water_lewis_lmos(nat, xyz, pad_atoms: int = 0):
+    """Starting LMOs for (H2O)_n in MOZYME_C's arrays, standing in for makvec
+    (its Lewis-structure builder is out of scope): per molecule, the isolated
+    molecule's occupied and virtual canonical MOs, Pipek-Mezey localised
+    (two O-H bonds + two lone pairs; two O-H antibonds), each LMO's atoms
+    listed by falling weight so its first two atoms are its bond's atoms, as
+    hbonds expects.  pad_atoms spare atom slots follow every LMO (room for
+    diagg2 to grow it).  Returns (iorbs, occ, vir)."""
+    nat = np.asarray(nat)
+    xyz = np.asarray(xyz, float).reshape(-1, 3)
+    iorbs = np.where(nat == 1, 1, 4).astype(np.int32)
+    occ = ([], [], [], [], [])
+    vir = ([], [], [], [], [])
+    atom_of = np.array([0, 0, 0, 0, 1, 2])
+    for m in range(len(nat) // 3):
+        a = [3 * m, 3 * m + 1, 3 * m + 2]
+        if not (nat[a[0]] == 8 and nat[a[1]] == 1 and nat[a[2]] == 1):
+            raise ValueError("water_lewis_lmos: atoms must come as O, H, H")
+        r1 = so.iter_scf(so.make_system(nat[a], xyz[a]), scfcrt=1.0e-8)
+        for C, dst in ((_pipek_mezey(r1.c[:, :4], atom_of, 3), occ), (_pipek_mezey(r1.c[:, 4:6], atom_of, 3), vir)):
+            for col in range(C.shape[1]):
+                v = C[:, col]
+                w = np.array([np.sum(v[:4] ** 2), v[4] ** 2, v[5] ** 2])
+                ncf, nncf, icocc, ncocc, cocc = dst
+                nncf.append(len(icocc))
+                ncocc.append(len(cocc))
+                ncf.append(3)
+                for o in np.argsort(-w, kind="stable"):
+                    icocc.append(a[o] + 1)
+                    cocc.extend(v[:4].tolist() if o == 0 else [float(v[3 + o])])
+                icocc.extend([0] * pad_atoms)
+                cocc.extend([0.0] * (4 * pad_atoms))
+    cast = lambda t: (np.array(t[0], np.int32), np.array(t[1], np.int32), np.array(t[2], np.int32),
+                      np.array(t[3], np.int32), np.array(t[4], np.float64))
+    return iorbs, cast(occ), cast(vir)
+
+
+def iter_for_mozyme(s, occ, vir, cutof1: float, cutof2: float, scfcrt: float = 1.0e-2, itrmax: int = 2000,
+                    trace: bool = False):
+    """The MOZYME SCF loop (MOZYME/iter_for_MOZYME.F90:218-630) for a whole
+    closed-shell system (numred = numat: no partial SCF, no setupk):
+    density, Fock and energy of the starting LMOs (:439-473); then per
+    iteration check (:482-484), eimp (:495), diagg = diagg1 + diagg2 +
+    density (diagg.F90), addhb every third iteration while nhb < 4
+    (:529-538, addhb.F90, hbonds.F90), cnvgz while the three-point
+    extrapolation is on (:549), buildf and helecz (:558-567), isitsc's 1SCF
+    test (isitsc.F90:34-44: ovmax below 5 selcon and |dE| below selcon on
+    two consecutive iterations; ovmax is diagg1's tiny, diagg1.F90:648), and
+    the shift control (:615-628).  selcon = scfcrt (scfcri's default 1e-2).
+    Not restated: tidy (storage compaction; the LMOs carry their own spare
+    slots), PLS_faulty's restart, COSMO.  occ and vir are updated in place.
+    Returns a dict: escf, ee, niter, converged, history."""
+    iorbs = (s.nlast - s.nfirst + 1).astype(np.int32)
+    mpack, nijbo = layout(iorbs, s.coord, cutof1, cutof2)
+    idg = idiag(iorbs, nijbo)
+    h = dense_to_blocks(so.unpack(s.h, s.norbs), iorbs, nijbo, mpack)
+    selcon = scfcrt
+    thresh = 1.0e-13
+    const = 1.0                          # DAMP for main-group atoms (diagg2.F90:56-63)
+    bigeps = 50.0 * np.sqrt(1.0e-39)
+    cap = 300 * s.norbs
+    st = np.array([10.0, 1.0, 0.0, 0.0])  # diagg1's fref, safety, oldlim, tiny
+    nfmo = np.zeros(len(vir[0]), np.int32)
+    ifmo = np.zeros(2 * cap, np.int32)
+    fmo = np.zeros(cap)
+    nrejct = np.zeros(2, np.int32)
+    eigs = np.zeros(len(occ[0]))
+    eigv = np.zeros(len(vir[0]))
+    p = density(iorbs, nijbo, occ, 0, mpack)
+    f = fock(s.nat, s.coord, iorbs, nijbo, s.w, p, h)
+    ee = helecz(iorbs, nijbo, p, h, f)
+    escf = (ee + s.enuclr) * so.FPC9 + s.atheat
+    pold = np.zeros(mpack)
+    p1, p2, p3 = np.zeros(s.norbs), np.zeros(s.norbs), np.zeros(s.norbs)
+    eold, niter, idiagg, shift, lstart, nhb = 0.0, 0, 0, 0.0, 0, 0
+    use3, scf1, converged = True, False, False
+    history = []
+    while True:
+        if check_lmos(occ, iorbs) > 0.1 or check_lmos(vir, iorbs) > 0.1:
+            raise RuntimeError("ERROR DETECTED IN SUBROUTINE CHECK")
+        eimp(iorbs, nijbo, p, f)
+        nij, eigv, eg, _ = diagg1(iorbs, nijbo, f, p, occ, vir, idiagg, st, nfmo, ifmo, fmo, cap)
+        if eg is not None:
+            eigs = eg
+        ovmax = float(st[3])
+        diagg2(iorbs, occ, vir, ifmo, fmo, nij, eigs, eigv, idiagg, [const, shift, thresh, st[3], bigeps], nrejct)
+        p = density(iorbs, nijbo, occ, 0, mpack)
+        idiagg += 1
+        niter += 1
+        nhb_ij = 0
+        if niter % 3 == 0 and nhb < 4:
+            nhb += 1
+            nhb_ij, hif, hfm = hbonds(iorbs, nijbo, f, p, occ, vir, HB_LIMITS[nhb - 1], cap)
+            if nhb_ij:
+                diagg2(iorbs, occ, vir, hif, hfm, nhb_ij, eigs, eigv, idiagg,
+                       [const, shift, thresh, st[3], bigeps], nrejct)
+                if idiagg % 2 == 1:
+                    idiagg += 1
+        if use3:
+            cnvgz(p, pold, p1, p2, p3, niter, idg)
+        f = fock(s.nat, s.coord, iorbs, nijbo, s.w, p, h)
+        ee = helecz(iorbs, nijbo, p, h, f)
+        escf = (ee + s.enuclr) * so.FPC9 + s.atheat
+        de = escf - eold
+        eold = escf
+        if abs(de) > 9999.0:
+            de = 0.0
+        if trace:
+            history.append(dict(niter=niter, escf=escf, de=de, ovmax=ovmax, nij=nij, hb=nhb_ij, shift=shift))
+        ok = ovmax < 5.0 * selcon and abs(de) < selcon
+        if (ok and scf1) or niter > itrmax:
+            if niter > 3:
+                converged = niter <= itrmax
+                break
+        scf1 = ok
+        if use3:
+            if niter % 3 == 2 and abs(de) < 0.1:
+                use3, lstart, shift = False, niter, 0.0
+        elif de > 0.0 and shift < 11.0 and niter > lstart + 2:
+            shift += 2.0
+            lstart = niter
+    return dict(escf=escf, ee=ee, niter=niter, converged=converged, history=history)
