@@ -377,6 +377,24 @@ size_t mb_mz_cnvgz_ws_bytes(void);
 int mb_mz_cnvgz_ws(int norbs, long long mpack, double* pnew, double* p, double* p1, double* p2,
                    double* p3, int niter, const long long* idiag, int use3, double* pmax_out, void* ws,
                    cudaStream_t stream);
+/* The routines iter_for_MOZYME calls between the kernels above.
+ * check (MOZYME/check.F90): renormalises every LMO in place; norm2[nlmo]
+ * (device) receives the squared norms before the scaling and *error (host,
+ * optional; synchronises) their summed |1 - norm2| (the reference stops above
+ * 0.1).  iorbs: device, per atom. */
+int mb_mz_check_dev(const MbMzLmos* lmos, const int* iorbs, double* norm2, double* error,
+                    cudaStream_t stream);
+/* eimp (MOZYME/eimp.F90): p's first element of every stored off-diagonal
+ * block becomes the block's sum of squared f elements. */
+int mb_mz_eimp_dev(const MbMzLayout* layout, double* p, const double* f, cudaStream_t stream);
+/* hbonds (MOZYME/hbonds.F90), called by addhb with cutoff 1, 0.1, 0.01, 1e-3
+ * on its first four calls: (virtual, occupied) LMO pairs (1-based, ifmo[2e],
+ * ifmo[2e+1]; fmo[e] = 0.1) around stored atom pairs with sum F^2 > cutoff
+ * and sum P^2 < 1e-10, in the reference's order; at most cap entries.
+ * Synchronises the stream. */
+int mb_mz_hbonds_dev(const MbMzLayout* layout, const MbMzLmos* occ, const MbMzLmos* vir,
+                     const double* f, const double* p, double cutoff, long long cap, int* ifmo,
+                     double* fmo, long long* nij, cudaStream_t stream);
 
 /* P (packed) = occ * C[:, 0:nocc] C[:, 0:nocc]^T, FP64. */
 int mb_density_dev(int n, int nocc, double occ, const double* c, int ldc, double* p,

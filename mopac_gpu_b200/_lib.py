@@ -128,6 +128,10 @@ SIGNATURES = {
     "mb_mz_helecz_ws": ([_LL, _I, _P, _P, _P, _P, _P, _P, _P], _I),
     "mb_mz_cnvgz_ws_bytes": ([], ctypes.c_size_t),
     "mb_mz_cnvgz_ws": ([_I, _LL, _P, _P, _P, _P, _P, _I, _P, _I, _P, _P, _P], _I),
+    "mb_mz_check_dev": ([ctypes.POINTER(MbMzLmos), _P, _P, ctypes.POINTER(_D), _P], _I),
+    "mb_mz_eimp_dev": ([ctypes.POINTER(MbMzLayout), _P, _P, _P], _I),
+    "mb_mz_hbonds_dev": ([ctypes.POINTER(MbMzLayout), ctypes.POINTER(MbMzLmos), ctypes.POINTER(MbMzLmos), _P, _P,
+                          _D, _LL, _P, _P, ctypes.POINTER(_LL), _P], _I),
     "mb_gemm_split_ws_bytes": ([_I, _I, _I], ctypes.c_size_t),
     "mb_gemm_split_ws": ([_C, _C, _I, _I, _I, _D, _P, _I, _P, _I, _D, _P, _I, _P, ctypes.c_size_t, _P, _P], _I),
     "mb_density_split_ws_bytes": ([_I, _I], ctypes.c_size_t),

@@ -183,3 +183,102 @@ def diagg2(layout: Layout, occ: Lmos, vir: Lmos, d1: "Diagg1", idiagg: int, ctl,
                                  c.ctypes.data, nrejct.ctypes.data, ctypes.byref(sumb), ctypes.byref(nrej),
                                  _stream()))
     return sumb.value, nrej.value
+
+
+HB_LIMITS = (1.0, 0.1, 0.01, 0.001)   # addhb's cutoffs on its first four calls
+
+
+class _HbList:
+    """hbonds' list in the shape diagg2 takes from Diagg1."""
+
+    def __init__(self, ifmo, fmo, nij, eigs, eigv):
+        self.ifmo, self.fmo, self.nij, self.eigs, self.eigv = ifmo, fmo, nij, eigs, eigv
+
+
+def iter_for_mozyme(layout: Layout, occ: Lmos, vir: Lmos, coord, w, h, enuclr: float, atheat: float,
+                    scfcrt: float = 1.0e-2, itrmax: int = 2000, cap: int | None = None, trace: bool = False):
+    """The MOZYME SCF loop (MOZYME/iter_for_MOZYME.F90:218-630) for a whole
+    closed-shell system on the device: density, Fock and energy of the
+    starting LMOs, then per iteration check, eimp, diagg (diagg1 + diagg2 +
+    density), addhb every third iteration while fewer than four were made,
+    cnvgz while the three-point extrapolation is on, buildf, helecz, isitsc's
+    1SCF test and the shift control.  coord (numat x 3), w (the stored pairs'
+    integrals) and h (pair blocks) are CUDA float64 tensors; occ and vir are
+    updated in place.  The host sees scalars each iteration (energy, diagg1's
+    tiny) and, four times per SCF, hbonds' atom-pair flags.  Returns a dict:
+    escf, ee, niter, converged, history, p, f."""
+    fpc9 = 23.060547830619029
+    n = layout.norbs
+    cap = cap or 300 * n
+    selcon = scfcrt
+    const, thresh, bigeps = 1.0, 1.0e-13, 50.0 * np.sqrt(1.0e-39)
+    D = Diagg1(layout, occ, vir, cap)
+    hb_ifmo = torch.zeros(2 * cap, dtype=torch.int32, device="cuda")
+    hb_fmo = torch.zeros(cap, dtype=torch.float64, device="cuda")
+    norm_o = torch.empty(max(1, int(occ.s.nlmo)), dtype=torch.float64, device="cuda")
+    norm_v = torch.empty(max(1, int(vir.s.nlmo)), dtype=torch.float64, device="cuda")
+    nrejct = np.zeros(2, np.int32)
+    L = lib()
+    p = density(layout, occ, 0)
+    f = fock(layout, coord, w, p, h)
+    ee = helecz(layout, p, h, f)
+    escf = (ee + enuclr) * fpc9 + atheat
+    pold = torch.zeros(layout.mpack, dtype=torch.float64, device="cuda")
+    p1, p2, p3 = (torch.zeros(n, dtype=torch.float64, device="cuda") for _ in range(3))
+    eold, niter, idiagg, shift, lstart, nhb = 0.0, 0, 0, 0.0, 0, 0
+    use3, scf1, converged = True, False, False
+    history = []
+    while True:
+        eo, ev = ctypes.c_double(), ctypes.c_double()
+        check(L.mb_mz_check_dev(ctypes.byref(occ.s), layout.s.iorbs, _ptr(norm_o), ctypes.byref(eo), _stream()))
+        check(L.mb_mz_check_dev(ctypes.byref(vir.s), layout.s.iorbs, _ptr(norm_v), ctypes.byref(ev), _stream()))
+        if eo.value > 0.1 or ev.value > 0.1:
+            raise RuntimeError("ERROR DETECTED IN SUBROUTINE CHECK")
+        check(L.mb_mz_eimp_dev(ctypes.byref(layout.s), _ptr(p), _ptr(f), _stream()))
+        nij, _, _ = D(f, p, idiagg)
+        ovmax = float(D.state[3])
+        diagg2(layout, occ, vir, D, idiagg, [const, shift, thresh, D.state[3], bigeps], nrejct)
+        occ.refresh()
+        vir.refresh()
+        p = density(layout, occ, 0)
+        idiagg += 1
+        niter += 1
+        nhb_ij = 0
+        if niter % 3 == 0 and nhb < 4:
+            nhb += 1
+            nn = ctypes.c_longlong(0)
+            check(L.mb_mz_hbonds_dev(ctypes.byref(layout.s), ctypes.byref(occ.s), ctypes.byref(vir.s), _ptr(f),
+                                     _ptr(p), HB_LIMITS[nhb - 1], cap, _ptr(hb_ifmo), _ptr(hb_fmo),
+                                     ctypes.byref(nn), _stream()))
+            nhb_ij = nn.value
+            if nhb_ij:
+                diagg2(layout, occ, vir, _HbList(hb_ifmo, hb_fmo, nhb_ij, D.eigs, D.eigv), idiagg,
+                       [const, shift, thresh, D.state[3], bigeps], nrejct)
+                occ.refresh()
+                vir.refresh()
+                if idiagg % 2 == 1:
+                    idiagg += 1
+        if use3:
+            cnvgz(layout, p, pold, p1, p2, p3, niter, True)
+        f = fock(layout, coord, w, p, h)
+        ee = helecz(layout, p, h, f)
+        escf = (ee + enuclr) * fpc9 + atheat
+        de = escf - eold
+        eold = escf
+        if abs(de) > 9999.0:
+            de = 0.0
+        if trace:
+            history.append(dict(niter=niter, escf=escf, de=de, ovmax=ovmax, nij=nij, hb=nhb_ij, shift=shift))
+        ok = ovmax < 5.0 * selcon and abs(de) < selcon
+        if (ok and scf1) or niter > itrmax:
+            if niter > 3:
+                converged = niter <= itrmax
+                break
+        scf1 = ok
+        if use3:
+            if niter % 3 == 2 and abs(de) < 0.1:
+                use3, lstart, shift = False, niter, 0.0
+        elif de > 0.0 and shift < 11.0 and niter > lstart + 2:
+            shift += 2.0
+            lstart = niter
+    return dict(escf=escf, ee=ee, niter=niter, converged=converged, history=history, p=p, f=f)

@@ -226,10 +226,11 @@ def check_lmos(lmos, iorbs) -> float:
     err = 0.0
     for i in range(len(ncf)):
         n = int(sum(iorbs[icocc[nncf[i] + j] - 1] for j in range(ncf[i])))
-        seg = cocc[ncocc[i]:ncocc[i] + n]
-        ssum = float(np.sum(seg * seg))
+        ssum = 0.0
+        for m in range(ncocc[i], ncocc[i] + n):   # the reference's order
+            ssum += float(cocc[m]) * float(cocc[m])
         err += abs(1.0 - ssum)
-        cocc[ncocc[i]:ncocc[i] + n] = seg * (1.0 / np.sqrt(ssum))
+        cocc[ncocc[i]:ncocc[i] + n] *= 1.0 / np.sqrt(ssum)
     return err
 
 
@@ -241,8 +242,10 @@ def eimp(iorbs, nijbo, p, f) -> None:
         for j in range(i):
             k = int(nijbo[i, j])
             if k >= 0:
-                m = int(iorbs[i] * iorbs[j])
-                p[k] = float(np.sum(f[k:k + m] ** 2))
+                acc = 0.0
+                for q in range(k, k + int(iorbs[i] * iorbs[j])):
+                    acc += float(f[q]) * float(f[q])
+                p[k] = acc
 
 
 HB_LIMITS = (1.0, 0.1, 0.01, 0.001)   # addhb.F90: hblims
@@ -264,9 +267,10 @@ def hbonds(iorbs, nijbo, fao, p, occ, vir, cutoff: float, cap: int):
             k = int(nijbo[i, j])
             if k < 0:
                 continue
-            m = int(iorbs[i] * iorbs[j])
-            sumf = float(np.sum(fao[k:k + m] ** 2))
-            sump = float(np.sum(p[k:k + m] ** 2))
+            sumf = sump = 0.0
+            for q in range(k, k + int(iorbs[i] * iorbs[j])):
+                sumf += float(fao[q]) * float(fao[q])
+                sump += float(p[q]) * float(p[q])
             if not (sump < 1.0e-10 and sumf > cutoff):
                 continue
             used = []
