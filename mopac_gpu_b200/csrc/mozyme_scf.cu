@@ -167,8 +167,9 @@ extern "C" int mb_mz_hbonds_dev(const MbMzLayout* L, const MbMzLmos* occ, const 
     e = cudaMemcpyAsync(heads.data(), dheads, sizeof(int) * heads.size(), cudaMemcpyDeviceToHost, s);
     if (e != cudaSuccess) rc = mb_set_cuda_error(e, "hbond copies", __FILE__, __LINE__);
   }
-  if (rc == MB_OK && (e = cudaStreamSynchronize(s)) != cudaSuccess)
-    rc = mb_set_cuda_error(e, "hbond sync", __FILE__, __LINE__);
+  // always wait: copies already queued write into the host vectors above
+  e = cudaStreamSynchronize(s);
+  if (rc == MB_OK && e != cudaSuccess) rc = mb_set_cuda_error(e, "hbond sync", __FILE__, __LINE__);
   cudaFreeAsync(dflag, s);
   cudaFreeAsync(dheads, s);
   if (rc != MB_OK) return rc;
