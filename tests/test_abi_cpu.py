@@ -64,3 +64,17 @@ def test_bad_arguments_fail_loudly_without_gpu_work(libpath):
     rc = L.mb_ctx_create(1, nat.ctypes.data, None, ctypes.byref(h))
     assert rc == 5
     assert b"element" in L.mb_last_error()
+
+
+def test_plain_c_client_links_and_runs(libpath, tmp_path):
+    """tests/c_abi_client.c, built with gcc against include/mopac_b200.h and
+    the in-tree library alone, runs its host-only checks."""
+    exe = tmp_path / "c_abi_client"
+    libdir = os.path.dirname(libpath)
+    r = subprocess.run(["gcc", "-std=c11", "-O1", "-I", os.path.join(ROOT, "include"),
+                        os.path.join(ROOT, "tests", "c_abi_client.c"), "-L", libdir, "-lmopac_b200",
+                        f"-Wl,-rpath,{libdir}", "-o", str(exe)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    run = subprocess.run([str(exe), str(tmp_path / "x.den")], capture_output=True, text=True, timeout=60)
+    assert run.returncode == 0, (run.returncode, run.stderr)
+    assert "c_abi_client ok" in run.stdout
