@@ -2129,3 +2129,106 @@ double orc_mz_diagg2(int numat, const int *iorbs, int norbs, int nocc, int *ncf,
     free(iused); free(latoms); free(storei); free(storej);
     return sumb;
 }
+
+/* ------------------------------------------------------------------ */
+/* hcore_for_MOZYME (MOZYME/hcore_for_MOZYME.F90), molecular (id = 0),   */
+/* mode 0, no field: H and W on fillij's pair-block storage.             */
+/* ------------------------------------------------------------------ */
+/* outer1 (MOZYME/outer1.F90, mode 0): pairs beyond cutof1, a feathered
+ * point charge; e1b/e2a: packed local diagonal (10 for sp). */
+static double outer1_pair(int ni, int nj, const double *ci, const double *cj, double *e1b, double *e2a) {
+  double rij = sqrt((ci[0] - cj[0]) * (ci[0] - cj[0]) + (ci[1] - cj[1]) * (ci[1] - cj[1]) +
+                    (ci[2] - cj[2]) * (ci[2] - cj[2]));
+  double r = rij / A0;
+  double aee = 0.5 / E[ni].am + 0.5 / E[nj].am;
+  aee = aee * aee;
+  double ww = EV / sqrt(r * r + aee);
+  double point, cst;
+  to_point(rij, &point, &cst);              /* l_feather: PM7 */
+  ww = ww * cst + (1.0 - cst) * point;
+  for (int k = 0; k < 10; ++k) { e1b[k] = 0.0; e2a[k] = 0.0; }
+  static const int dg[4] = {0, 2, 5, 9};
+  for (int k = 0; k < 4; ++k) {
+    e1b[dg[k]] = -ww * E[nj].tore;
+    e2a[dg[k]] = -ww * E[ni].tore;
+  }
+  return E[ni].tore * E[nj].tore * ww;
+}
+
+/* outer2 (MOZYME/outer2.F90, mode 0): pairs between cutof2 and cutof1,
+ * monopole and dipole terms from reppd along the unit vector j -> i. */
+static double outer2_pair(int ni, int nj, const double *ci, const double *cj, double *e1b, double *e2a) {
+  double x[3] = {ci[0] - cj[0], ci[1] - cj[1], ci[2] - cj[2]};
+  double rij = sqrt(x[0] * x[0] + x[1] * x[1] + x[2] * x[2]);
+  double ri[23], gab;
+  reppd(ni, nj, rij, ri, &gab);
+  double a = 1.0 / rij;
+  x[0] *= a; x[1] *= a; x[2] *= a;
+  if (fabs(x[2]) > 0.99999999) x[2] = x[2] >= 0.0 ? 1.0 : -1.0;
+  int si = E[ni].natorb > 1, sj = E[nj].natorb > 1;
+  double w1 = ri[1];
+  for (int k = 0; k < 10; ++k) { e1b[k] = 0.0; e2a[k] = 0.0; }
+  e1b[0] = -w1 * E[nj].tore;
+  e2a[0] = -w1 * E[ni].tore;
+  if (sj) {
+    double w2 = -ri[5] * x[0], w3 = -ri[5] * x[1], w4 = -ri[5] * x[2];
+    e2a[1] = -w2 * E[ni].tore; e2a[2] = -w1 * E[ni].tore; e2a[3] = -w3 * E[ni].tore;
+    e2a[5] = -w1 * E[ni].tore; e2a[6] = -w4 * E[ni].tore; e2a[9] = -w1 * E[ni].tore;
+  }
+  if (si) {
+    double w5 = -ri[2] * x[0], w6 = -ri[2] * x[1], w7 = -ri[2] * x[2];
+    e1b[1] = -w5 * E[nj].tore; e1b[2] = -w1 * E[nj].tore; e1b[3] = -w6 * E[nj].tore;
+    e1b[5] = -w1 * E[nj].tore; e1b[6] = -w7 * E[nj].tore; e1b[9] = -w1 * E[nj].tore;
+  }
+  return E[ni].tore * E[nj].tore * w1;
+}
+
+/* H on the pair blocks (mpack from orc_mz_layout, nijbo from it too), W of
+ * the stored pairs in the dense W's order (pairs at or beyond cutof2 left
+ * out; the Fock build treats them through the coordinates), enuclr over all
+ * pairs.  Returns the number of W values written. */
+long long orc_mz_hcore(int numat, const int *nat, const double *coord, const long long *nijbo, double *h,
+                       double *w, double *enuclr_out) {
+  init_params();
+  double enuclr = 0.0;
+  const double cutof1 = 225.0;  /* h1elec's overlap cutoff, as the dense hcore */
+  long long kr = 0, mp = 0;
+  for (int i = 0; i < numat; ++i) {
+    long long o = nijbo[(long long)i * numat + i] + E[nat[i]].natorb * (E[nat[i]].natorb + 1) / 2;
+    if (o > mp) mp = o;
+  }
+  for (long long q = 0; q < mp; ++q) h[q] = 0.0;
+  for (int i = 0; i < numat; ++i) {
+    const int ni = nat[i], io = E[ni].natorb;
+    const long long di = nijbo[(long long)i * numat + i];
+    for (int a = 0; a < io; ++a) h[di + (long long)a * (a + 1) / 2 + a] = a == 0 ? E[ni].uss : E[ni].upp;
+    const double *xi = coord + 3 * i;
+    for (int j = 0; j < i; ++j) {
+      const int nj = nat[j], jo = E[nj].natorb;
+      const double *xj = coord + 3 * j;
+      const long long bo = nijbo[(long long)i * numat + j];
+      double e1b[10], e2a[10], enuc;
+      if (bo >= 0) {
+        double dm[5][5];
+        h1elec(ni, nj, xi, xj, dm, cutof1);
+        for (int a = 0; a < io; ++a)
+          for (int b = 0; b < jo; ++b) h[bo + (long long)a * jo + b] = h[bo + (long long)a * jo + b] + dm[a + 1][b + 1];
+        enuc = rotate_pair(ni, nj, xi, xj, w + kr, e1b, e2a);
+        kr += (long long)indx_(io, io) * indx_(jo, jo);
+      } else if (bo == -2) {
+        enuc = outer2_pair(ni, nj, xi, xj, e1b, e2a);
+      } else {
+        enuc = outer1_pair(ni, nj, xi, xj, e1b, e2a);
+      }
+      enuclr = enuclr + enuc;
+      const long long dj = nijbo[(long long)j * numat + j];
+      for (int m = 0; m < indx_(io, io); ++m) h[di + m] = h[di + m] + e1b[m] * 1.0;
+      for (int m = 0; m < indx_(jo, jo); ++m) h[dj + m] = h[dj + m] + e2a[m] * 1.0;
+    }
+    wstore(ni, w + kr);
+    const int il = indx_(io, io);
+    kr += (long long)il * il;
+  }
+  *enuclr_out = enuclr;
+  return kr;
+}

@@ -446,3 +446,25 @@ def iter_for_mozyme(s, occ, vir, cutof1: float, cutof2: float, scfcrt: float = 1
             shift += 2.0
             lstart = niter
     return dict(escf=escf, ee=ee, niter=niter, converged=converged, history=history)
+
+
+def hcore(nat, coord, iorbs, nijbo, mpack: int, nw_max: int):
+    """hcore_for_MOZYME (MOZYME/hcore_for_MOZYME.F90, molecular, mode 0): H on
+    the pair blocks, W of the stored pairs (dense W order, far pairs left
+    out), enuclr.  Stored pairs get the full integrals (h1elec, rotate);
+    pairs between cutof2 and cutof1 outer2's monopole + dipole terms, pairs
+    beyond cutof1 outer1's feathered point charge."""
+    L = _lib()
+    if not hasattr(L, "_mz_hcore_bound"):
+        i32p = np.ctypeslib.ndpointer(np.int32, flags="C")
+        i64p = np.ctypeslib.ndpointer(np.int64, flags="C")
+        f64p = np.ctypeslib.ndpointer(np.float64, flags="C")
+        L.orc_mz_hcore.argtypes = [ctypes.c_int, i32p, f64p, i64p, f64p, f64p, ctypes.POINTER(ctypes.c_double)]
+        L.orc_mz_hcore.restype = ctypes.c_longlong
+        L._mz_hcore_bound = True
+    h = np.zeros(mpack)
+    w = np.zeros(nw_max)
+    en = ctypes.c_double()
+    nw = L.orc_mz_hcore(len(nat), np.ascontiguousarray(nat, np.int32), np.ascontiguousarray(coord, np.float64).ravel(),
+                        np.ascontiguousarray(nijbo.ravel()), h, w, ctypes.byref(en))
+    return h, w[:nw], en.value

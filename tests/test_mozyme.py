@@ -412,3 +412,30 @@ def test_gpu_mozyme_scf_follows_the_oracle_loop():
     Qo.close()
     Qv.close()
     L.close()
+
+
+@pytest.mark.parametrize("kind,nwater,cutoff", [("lattice", 8, None), ("box", 16, None), ("box", 32, 9.0)])
+def test_oracle_mozyme_hcore(kind, nwater, cutoff):
+    """hcore_for_MOZYME restated: with every pair stored it is the dense hcore
+    rearranged into blocks, bit for bit; with far pairs (outer1's point charge
+    beyond cutof1, outer2's dipoles in the band) H still matches the dense one
+    to rounding, because PM7's feathering makes the exact core attraction a
+    point charge beyond 7 A, and the core-core energy loses only its short-range
+    terms (< 1e-4 eV)."""
+    if kind == "lattice":
+        nat, xyz = workloads.water_lattice(nwater, seed=2)
+    else:
+        nat, xyz, _ = workloads.water_box(nwater, seed=3)
+    s = oracle_system(nat, xyz)
+    iorbs = (s.nlast - s.nfirst + 1).astype(np.int32)
+    c1, c2 = mo.cutoffs(len(nat), cutoff)
+    mp, nb = mo.layout(iorbs, s.coord, c1, c2)
+    h, w, en = mo.hcore(nat, xyz, iorbs, nb, mp, s.w.size)
+    hd = mo.dense_to_blocks(so.unpack(s.h, s.norbs), iorbs, nb, mp)
+    np.testing.assert_array_equal(w, mo.w_stored(iorbs, nb, s.w))
+    if (nb < 0).any():
+        assert np.abs(h - hd).max() < 1e-11
+        assert abs(en - s.enuclr) < 1e-4
+    else:
+        np.testing.assert_array_equal(h, hd)
+        assert en == s.enuclr
