@@ -298,6 +298,16 @@ typedef struct MbMzLmos {
 int mb_mz_layout_create(int numat, const int* iorbs, const double* coord, double cutof1, double cutof2,
                         MbMzLayout* out, long long* nijbo);
 int mb_mz_layout_destroy(MbMzLayout* layout);
+/* hcore_for_MOZYME (MOZYME/hcore_for_MOZYME.F90, molecular, mode 0) on the
+ * layout: h (mpack) the one-electron matrix in pair blocks, w (nw) the stored
+ * pairs' two-centre integrals and every atom's one-centre block,
+ * *enuclr_dev the core-core energy over every atom pair (pairs not stored:
+ * outer2's monopole in the cutof2-cutof1 band, outer1's feathered point
+ * charge beyond).  nat, coord: device (atomic numbers; Angstrom).  ws:
+ * mb_mz_hcore_ws_bytes(layout) bytes of device scratch. */
+size_t mb_mz_hcore_ws_bytes(const MbMzLayout* layout);
+int mb_mz_hcore_dev(const MbMzLayout* layout, const int* nat, const double* coord, double* h, double* w,
+                    double* enuclr, void* ws, cudaStream_t stream);
 /* idiag (host, norbs): 1-based position of each orbital's diagonal element,
  * as iter_for_MOZYME.F90:183-190. */
 int mb_mz_idiag(const MbMzLayout* layout, long long* idiag);

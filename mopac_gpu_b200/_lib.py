@@ -128,6 +128,8 @@ SIGNATURES = {
     "mb_mz_helecz_ws": ([_LL, _I, _P, _P, _P, _P, _P, _P, _P], _I),
     "mb_mz_cnvgz_ws_bytes": ([], ctypes.c_size_t),
     "mb_mz_cnvgz_ws": ([_I, _LL, _P, _P, _P, _P, _P, _I, _P, _I, _P, _P, _P], _I),
+    "mb_mz_hcore_ws_bytes": ([ctypes.POINTER(MbMzLayout)], ctypes.c_size_t),
+    "mb_mz_hcore_dev": ([ctypes.POINTER(MbMzLayout), _P, _P, _P, _P, _P, _P, _P], _I),
     "mb_mz_check_dev": ([ctypes.POINTER(MbMzLmos), _P, _P, ctypes.POINTER(_D), _P], _I),
     "mb_mz_eimp_dev": ([ctypes.POINTER(MbMzLayout), _P, _P, _P], _I),
     "mb_mz_hbonds_dev": ([ctypes.POINTER(MbMzLayout), ctypes.POINTER(MbMzLmos), ctypes.POINTER(MbMzLmos), _P, _P,

@@ -757,6 +757,122 @@ __global__ void enuc_sum_batch(MbHcoreBatch B) {
   if (threadIdx.x == 0) B.enuclr[m] = np > 0 ? sh[0] : 0.0;
 }
 
+// ---- hcore_for_MOZYME (MOZYME/hcore_for_MOZYME.F90, molecular, mode 0) on
+// fillij's pair-block storage.  Stored pairs get the full integrals (the
+// bodies above); the diagonal blocks take every partner's core attraction
+// in the reference's order (with PM7's feathering the exact term beyond 7 A
+// is the point charge outer1/outer2 use); the core-core energy of a pair
+// that is not stored is outer1's or outer2's (tore_i tore_j times the
+// point-charge or monopole integral).
+__global__ void mz_hcore_pairs(MbMzLayout L, const int* __restrict__ nat, const double* __restrict__ coord,
+                               double* __restrict__ h, double* __restrict__ w, double* __restrict__ enuc_entry) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < L.npairs;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int ia = L.pair_i[e], ja = L.pair_j[e];
+    if (ia == ja) {
+      enuc_entry[e] = 0.0;
+      continue;
+    }
+    const int ni = nat[ia], nj = nat[ja];
+    const double* xi = coord + 3 * ia;
+    const double* xj = coord + 3 * ja;
+    const int noi = L.iorbs[ia], noj = L.iorbs[ja];
+    double di[5][5];
+    h1elec(ni, nj, xi, xj, di);
+    double* hb = h + L.pair_off[e];
+    for (int a = 1; a <= noi; ++a)
+      for (int b = 1; b <= noj; ++b) hb[(a - 1) * noj + (b - 1)] = di[a][b];
+    const int li = noi * (noi + 1) / 2, lj = noj * (noj + 1) / 2;
+    double* wb = w + L.pair_woff[e];
+    const double dx = xi[0] - xj[0], dy = xi[1] - xj[1], dz = xi[2] - xj[2];
+    if (dx * dx + dy * dy + dz * dz < 0.00002) {
+      for (int x = 0; x < li * lj; ++x) wb[x] = 0.0;
+      enuc_entry[e] = 0.0;
+      continue;
+    }
+    double p[4][4];
+    const double r = rotmat(xi, xj, p);
+    double ri[23], gab;
+    reppd(ni, nj, r, ri, &gab);
+    w_block(ni, nj, p, ri, wb);
+    enuc_entry[e] = ccrep(ni, nj, r / PM7_A0, gab);
+  }
+}
+
+__global__ void mz_hcore_diag(MbMzLayout L, const int* __restrict__ nat, const double* __restrict__ coord,
+                              double* __restrict__ h, double* __restrict__ w, const double* __restrict__ enuc_entry,
+                              double* __restrict__ enuc_atom) {
+  const int A = blockIdx.x * blockDim.x + threadIdx.x;
+  if (A >= L.numat) return;
+  const int nA = nat[A], noA = L.iorbs[A], lA = noA * (noA + 1) / 2;
+  const Pm7Elem& E = c_P.el[nA];
+  double blk[10];
+  for (int x = 0; x < 10; ++x) blk[x] = 0.0;
+  blk[0] = E.uss;
+  if (noA == 4) { blk[2] = E.upp; blk[5] = E.upp; blk[9] = E.upp; }
+  const double* xa = coord + 3 * A;
+  int ep = L.pair_ptr[A];                 // A's stored partners (ascending), then its own block
+  const int ediag = L.pair_ptr[A + 1] - 1;
+  double en = 0.0;
+  for (int B = 0; B < L.numat; ++B) {
+    if (B == A) continue;
+    const double* xb = coord + 3 * B;
+    const double dx = xa[0] - xb[0], dy = xa[1] - xb[1], dz = xa[2] - xb[2];
+    const double r2 = dx * dx + dy * dy + dz * dz;
+    const int nB = nat[B];
+    if (B < A) {
+      // the pair's core-core energy (summed per atom over partners below it)
+      if (ep < ediag && L.pair_j[ep] == B) {
+        en += enuc_entry[ep];
+        ++ep;
+      } else if (r2 < L.cutof1) {       // outer2: monopole term
+        double ri[23], gab;
+        reppd(nA, nB, sqrt(r2), ri, &gab);
+        en += c_P.el[nA].tore * c_P.el[nB].tore * ri[1];
+      } else {                          // outer1: feathered point charge
+        const double rij = sqrt(r2), rb = rij / PM7_A0;
+        double aee = 0.5 / E.am + 0.5 / c_P.el[nB].am;
+        aee = aee * aee;
+        double ww = PM7_EV / sqrt(rb * rb + aee), point, cst;
+        to_point(rij, &point, &cst);
+        ww = ww * cst + (1.0 - cst) * point;
+        en += c_P.el[nA].tore * c_P.el[nB].tore * ww;
+      }
+    }
+    if (r2 < 0.00002) continue;
+    double p[4][4], core[5][3], e1b[10], e2a[10];
+    if (B < A) {
+      const double r = rotmat(xa, xb, p);
+      core_terms(nA, nB, r, core);
+      elenuc(p, core, noA, L.iorbs[B], e1b, e2a);
+      for (int x = 0; x < lA; ++x) blk[x] = blk[x] + e1b[x] * 1.0;
+    } else {
+      const double r = rotmat(xb, xa, p);
+      core_terms(nB, nA, r, core);
+      elenuc(p, core, L.iorbs[B], noA, e1b, e2a);
+      for (int x = 0; x < lA; ++x) blk[x] = blk[x] + e2a[x] * 1.0;
+    }
+  }
+  enuc_atom[A] = en;
+  double* hd = h + L.pair_off[ediag];
+  for (int x = 0; x < lA; ++x) hd[x] = blk[x];
+  double* w1 = w + L.pair_woff[ediag];
+  for (int x = 0; x < lA * lA; ++x) w1[x] = 0.0;
+#define WS(a, b) w1[((a) - 1) + lA * ((b) - 1)]
+  WS(1, 1) = E.gss;
+  if (noA == 4) {
+    const int ipx = 3, ipy = 6, ipz = 10;
+    WS(ipx, 1) = E.gsp; WS(ipy, 1) = E.gsp; WS(ipz, 1) = E.gsp;
+    WS(1, ipx) = E.gsp; WS(1, ipy) = E.gsp; WS(1, ipz) = E.gsp;
+    WS(ipx, ipx) = E.gpp; WS(ipy, ipy) = E.gpp; WS(ipz, ipz) = E.gpp;
+    WS(ipy, ipx) = E.gp2; WS(ipz, ipx) = E.gp2; WS(ipz, ipy) = E.gp2;
+    WS(ipx, ipy) = E.gp2; WS(ipx, ipz) = E.gp2; WS(ipy, ipz) = E.gp2;
+    WS(2, 2) = E.hsp; WS(4, 4) = E.hsp; WS(7, 7) = E.hsp;
+    WS(5, 5) = 0.5 * (E.gpp - E.gp2); WS(8, 8) = 0.5 * (E.gpp - E.gp2); WS(9, 9) = 0.5 * (E.gpp - E.gp2);
+  }
+#undef WS
+}
+
 bool g_params_uploaded = false;
 
 int upload_params() {
@@ -816,6 +932,33 @@ extern "C" int mb_hcore_finish(int numat, const MbAtomsDev* at, const int* nat_d
     return MB_OK;
   }
   enuc_sum<<<1, 1024, 0, stream>>>(npair, enuc_pairs, enuclr_dev);
+  MB_LAUNCH_CHECK();
+  return MB_OK;
+}
+
+// hcore_for_MOZYME on the pair blocks: h (layout mpack), w (layout nw: the
+// stored pairs' two-centre blocks and every atom's one-centre block),
+// *enuclr_dev (device) the core-core energy over every atom pair.  ws:
+// mb_mz_hcore_ws_bytes(layout) bytes of device scratch.
+extern "C" size_t mb_mz_hcore_ws_bytes(const MbMzLayout* L) {
+  return L ? sizeof(double) * (size_t)(L->npairs + L->numat) : 0;
+}
+
+extern "C" int mb_mz_hcore_dev(const MbMzLayout* L, const int* nat_d, const double* coord_d, double* h, double* w,
+                               double* enuclr_dev, void* ws, cudaStream_t stream) {
+  if (!L || !nat_d || !coord_d || !h || !w || !enuclr_dev || !ws || L->numat <= 0)
+    return mb_set_error(MB_ERR_ARG, "mb_mz_hcore_dev: bad args");
+  MB_TRY(upload_params());
+  double* enuc_entry = (double*)ws;
+  double* enuc_atom = enuc_entry + L->npairs;
+  if (L->npairs > 0) {
+    const int blocks = (int)std::min<long long>((L->npairs + 127) / 128, 148LL * 32);
+    mz_hcore_pairs<<<blocks, 128, 0, stream>>>(*L, nat_d, coord_d, h, w, enuc_entry);
+    MB_LAUNCH_CHECK();
+  }
+  mz_hcore_diag<<<(L->numat + 63) / 64, 64, 0, stream>>>(*L, nat_d, coord_d, h, w, enuc_entry, enuc_atom);
+  MB_LAUNCH_CHECK();
+  enuc_sum<<<1, 1024, 0, stream>>>(L->numat, enuc_atom, enuclr_dev);
   MB_LAUNCH_CHECK();
   return MB_OK;
 }

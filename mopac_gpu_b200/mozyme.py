@@ -127,6 +127,19 @@ def cnvgz(layout: Layout, pnew, p, p1, p2, p3, niter: int, use3: bool = True) ->
     return float(pm.item())
 
 
+def hcore(layout: Layout, nat, coord):
+    """hcore_for_MOZYME on the device: (h pair blocks, w stored-pair integrals,
+    enuclr).  nat (int32) and coord (numat x 3, float64): CUDA tensors."""
+    h = torch.empty(layout.mpack, dtype=torch.float64, device="cuda")
+    w = torch.empty(int(layout.s.nw), dtype=torch.float64, device="cuda")
+    en = torch.zeros(1, dtype=torch.float64, device="cuda")
+    ws = torch.empty(int(lib().mb_mz_hcore_ws_bytes(ctypes.byref(layout.s))) // 8 + 1, dtype=torch.float64,
+                     device="cuda")
+    check(lib().mb_mz_hcore_dev(ctypes.byref(layout.s), _ptr(nat.contiguous()), _ptr(coord.contiguous()), _ptr(h),
+                                _ptr(w), _ptr(en), _ptr(ws), _stream()))
+    return h, w, float(en.item())
+
+
 def fock(layout: Layout, coord, w, ptot, h, out=None):
     """buildf(f, partf, 0): F = H + G(P) over the pair-block storage.  coord
     (numat x 3, Angstrom), w (the stored pairs' integrals, layout.nw), ptot

@@ -439,3 +439,30 @@ def test_oracle_mozyme_hcore(kind, nwater, cutoff):
     else:
         np.testing.assert_array_equal(h, hd)
         assert en == s.enuclr
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kind,nwater,cutoff", [("lattice", 8, None), ("box", 32, 9.0)])
+def test_gpu_mozyme_hcore_matches_oracle(kind, nwater, cutoff):
+    """hcore_for_MOZYME on the device against the oracle's restatement: H and
+    W to the dense integrals' parity (1e-11 relative), the core-core energy
+    over all pairs (far ones through outer1/outer2) to 1e-10 relative."""
+    torch = _need_gpu()
+    from mopac_gpu_b200 import mozyme
+    if kind == "lattice":
+        nat, xyz = workloads.water_lattice(nwater, seed=2)
+    else:
+        nat, xyz, _ = workloads.water_box(nwater, seed=3)
+    s = oracle_system(nat, xyz)
+    iorbs = (s.nlast - s.nfirst + 1).astype(np.int32)
+    c1, c2 = mo.cutoffs(len(nat), cutoff)
+    mp, nb = mo.layout(iorbs, s.coord, c1, c2)
+    ho, wo, eo = mo.hcore(nat, xyz, iorbs, nb, mp, s.w.size)
+    L = mozyme.Layout(iorbs, s.coord, c1, c2)
+    assert L.mpack == mp and int(L.s.nw) == wo.size
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    hg, wg, eg = mozyme.hcore(L, dev(np.asarray(nat, np.int32)), dev(s.coord))
+    np.testing.assert_allclose(hg.cpu().numpy(), ho, rtol=1e-11, atol=1e-11)
+    np.testing.assert_allclose(wg.cpu().numpy(), wo, rtol=1e-11, atol=1e-12)
+    assert abs(eg - eo) <= 1e-10 * abs(eo)
+    L.close()
