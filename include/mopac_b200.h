@@ -93,6 +93,19 @@ typedef struct mb_scf_opts {
                         or predicted by mb_ctx_guess, entered like an OLDENS
                         density (SCF/iter.F90:151-158); 0: the standard
                         diagonal guess                                     */
+  double finish_dp;  /* FP64 finish (an addition to iter): once iter's test
+                        (SCF/iter.F90:675-690) passes in FP64, convergence
+                        is accepted only when the last density update moved
+                        no element of P by more than finish_dp; until then
+                        the loop goes on in FP64 with the rotation sweep's
+                        relative threshold bigeps at 0 and, from its first
+                        iteration, the orbital energies of the current
+                        vectors (diag C^T F C) in the rotation angles.  It
+                        takes the SCF to its self-consistent point instead
+                        of stopping inside iter's criterion.  < 0
+                        (default): 1e-7 when precision = 1, off when
+                        precision = 0; 0: off                              */
+  int finish_max;    /* cap on the iterations the finish adds (default 40) */
 } mb_scf_opts;
 
 typedef struct mb_scf_result {
@@ -109,6 +122,9 @@ typedef struct mb_scf_result {
   int n_pulay;       /* Pulay extrapolation steps taken                    */
   int n_split;       /* iterations whose density / Fmo GEMMs ran in the
                         split BF16 precision (opts.precision = 1)          */
+  int n_finish;      /* iterations the FP64 finish added                   */
+  double dp;         /* max|P_k - P_(k-1)| of the last density update
+                        (computed when the finish is on, else -1)          */
 } mb_scf_result;
 
 void mb_scf_opts_default(mb_scf_opts* o);

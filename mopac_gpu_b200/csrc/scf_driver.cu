@@ -33,7 +33,9 @@ extern "C" int mb_pseudo_diag_ws(int n, int nocc, const double* fpacked, double*
                                  unsigned long long* nrot_dev, void* ws, cudaStream_t stream);
 extern "C" int mb_pseudo_diag_ex(int n, int nocc, const double* fpacked, double* c, const double* eigs,
                                  unsigned long long* nrot_dev, void* ws, void* split_ws, size_t split_ws_bytes,
-                                 int* split_err, cudaStream_t stream);
+                                 int* split_err, double bigeps, cudaStream_t stream);
+extern "C" int mb_orbital_energies_ws(int n, const double* fpacked, const double* c, double* eigs, void* ws,
+                                      cudaStream_t stream);
 extern "C" size_t mb_gemm_split_ws_bytes(int m, int n, int k);
 extern "C" size_t mb_density_split_ws_bytes(int n, int nocc);
 extern "C" int mb_density_split_ws(int n, int nocc, double occ, const double* c, int ldc, double* p, void* ws,
@@ -156,6 +158,7 @@ struct mb_ctx {
   // starting density for opts.guess (mb_ctx_set_guess / mb_ctx_guess)
   double* pguess = nullptr;
   bool have_guess = false;
+  double* pprev = nullptr;          // previous density for the FP64 finish's max|dP|
   mb_guess_ws* guess_ws = nullptr;  // the prediction's grow-only workspace
   void* purify_ws = nullptr;        // McWeeny matrices when eig_ws is too small
   cudaStream_t stream = nullptr;
@@ -170,7 +173,7 @@ static void ctx_free(mb_ctx* c) {
   mb_guess_ws_destroy(c->guess_ws);
   void* ptrs[] = {c->d_nat, c->d_coord, c->h, c->w, c->f, c->p, c->pa, c->pold, c->pold2, c->c, c->eigs,
                   c->fdiag, c->scal, c->hws, c->status, c->nrot, c->eig_ws, c->pseudo_ws,
-                  c->fppf_hist, c->fock_hist, c->tc_ws_raw, c->pguess, c->purify_ws};
+                  c->fppf_hist, c->fock_hist, c->tc_ws_raw, c->pguess, c->purify_ws, c->pprev};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -186,6 +189,8 @@ extern "C" void mb_scf_opts_default(mb_scf_opts* o) {
   o->verbose = 0;
   o->pulay = 0;
   o->guess = 0;
+  o->finish_dp = -1.0;
+  o->finish_max = 40;
 }
 
 extern "C" int mb_ctx_create(int numat, const int* nat, const double* coord, mb_ctx** out) {
@@ -425,6 +430,21 @@ __global__ void guess_start_kernel(int n, long long mpack, const double* __restr
   for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < n; r += (long long)gridDim.x * blockDim.x)
     pold2[r] = g[r * (r + 1) / 2 + r];
 }
+// out = max|p - prev| over the packed matrix (out zeroed by the caller; the
+// values are >= 0, so their bit patterns order like the values), then
+// prev <- p for the next iteration.
+__global__ void maxdiff_copy_kernel(long long n, const double* __restrict__ p, double* __restrict__ prev,
+                                    unsigned long long* __restrict__ out) {
+  double m = 0.0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const double v = p[i];
+    m = fmax(m, fabs(v - prev[i]));
+    prev[i] = v;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
+}
 }  // namespace
 
 static int d2h(mb_ctx* c, double* dst, const double* src, int count) {
@@ -510,6 +530,13 @@ extern "C" int mb_scf_run(mb_ctx* c, const mb_scf_opts* opts_in, mb_scf_result* 
     }
     MB_CUDA(cudaMemsetAsync(c->status + 1, 0, sizeof(int), s));
   }
+  // FP64 finish: automatic (< 0) means on for the split precision only
+  const double finish_dp = opts.finish_dp < 0.0 ? (opts.precision != 0 ? 1.0e-7 : 0.0) : opts.finish_dp;
+  const int finish_max = opts.finish_max > 0 ? opts.finish_max : 0;
+  const bool finishing = finish_dp > 0.0 && finish_max > 0;
+  double dp = finishing ? INFINITY : -1.0;  // max|P_k - P_(k-1)| of the last update
+  bool refreshed = false;                   // orbital energies refreshed for the finish
+  if (finishing && !c->pprev) MB_CUDA(cudaMalloc(&c->pprev, sizeof(double) * (size_t)mpack));
   PhaseTimer t_fock(s), t_diag(s), t_dens(s);
   cudaEvent_t ev_begin, ev_end;
   MB_CUDA(cudaEventCreate(&ev_begin));
@@ -547,6 +574,7 @@ extern "C" int mb_scf_run(mb_ctx* c, const mb_scf_opts* opts_in, mb_scf_result* 
     guess_start_kernel<<<148, 256, 0, s>>>(n, mpack, c->pguess, c->p, c->pa, pold, pold2);
     MB_LAUNCH_CHECK();
   }
+  if (finishing) MB_CUDA(cudaMemcpyAsync(c->pprev, c->p, sizeof(double) * mpack, cudaMemcpyDeviceToDevice, s));
   const double gnorm = 0.0;
   double selcon = opts.scfcrt;
   selcon = fmin(fmin(opts.scfcrt * 100.0, 0.1), fmax(opts.scfcrt * gnorm * gnorm * gnorm, opts.scfcrt));
@@ -618,6 +646,10 @@ extern "C" int mb_scf_run(mb_ctx* c, const mb_scf_opts* opts_in, mb_scf_result* 
         use_split = false;
         conv = false;
       }
+      if (conv && finishing && dp > finish_dp && res->n_finish < finish_max) {
+        res->n_finish++;  // FP64 finish: go on until the density stops moving
+        conv = false;
+      }
       if (conv) {
         if (fabs(shift) < 1.0e-10) { converged = true; break; }
         shift = 0.0;
@@ -642,9 +674,14 @@ extern "C" int mb_scf_run(mb_ctx* c, const mb_scf_opts* opts_in, mb_scf_result* 
     }
     t_diag.start();
     if (newdg && opts.pseudo && !(halfe || camkin)) {
+      if (res->n_finish > 0 && !refreshed) {
+        // the finish's rotation angles use the energies of the current vectors
+        MB_TRY(mb_orbital_energies_ws(n, c->f, c->c, c->eigs, c->eig_ws, s));
+        refreshed = true;
+      }
       mb_kstat_mark(MB_KSTAT_PSEUDO, s, true);
       MB_TRY(mb_pseudo_diag_ex(n, na1el, c->f, c->c, c->eigs, c->nrot, c->pseudo_ws, use_split ? c->tc_ws : nullptr,
-                               c->tc_ws_bytes, c->status + 1, s));
+                               c->tc_ws_bytes, c->status + 1, res->n_finish > 0 ? 0.0 : 1.5e-7, s));
       mb_kstat_mark(MB_KSTAT_PSEUDO, s, false);
       res->n_pseudo_diag++;
     } else {
@@ -663,8 +700,15 @@ extern "C" int mb_scf_run(mb_ctx* c, const mb_scf_opts* opts_in, mb_scf_result* 
     if (do_cnvg) MB_TRY(mb_cnvg_ws(n, c->p, pold, pold2, niter, c->scal + 1, c->scal + 8, s));
     half_kernel<<<hblocks, 256, 0, s>>>(mpack, c->p, c->pa);
     MB_LAUNCH_CHECK();
+    if (finishing) {
+      unsigned long long* dpbits = (unsigned long long*)(c->scal + 2);
+      MB_CUDA(cudaMemsetAsync(dpbits, 0, sizeof(unsigned long long), s));
+      maxdiff_copy_kernel<<<hblocks, 256, 0, s>>>(mpack, c->p, c->pprev, dpbits);
+      MB_LAUNCH_CHECK();
+    }
     t_dens.stop();
     if (do_cnvg) MB_TRY(d2h(c, &pl, c->scal + 1, 1));
+    if (finishing) MB_TRY(d2h(c, &dp, c->scal + 2, 1));
     if (opts.precision != 0 && res->n_split > 0) {
       int terr = 0;
       MB_CUDA(cudaMemcpyAsync(&terr, c->status + 1, sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -693,6 +737,7 @@ extern "C" int mb_scf_run(mb_ctx* c, const mb_scf_opts* opts_in, mb_scf_result* 
   res->niter = niter;
   res->converged = converged ? 1 : 0;
   res->pl = pl;
+  res->dp = finishing ? dp : -1.0;
   res->t_fock_ms = t_fock.total;
   res->t_diag_ms = t_diag.total;
   res->t_density_ms = t_dens.total;

@@ -395,10 +395,12 @@ extern "C" int mb_gemm_split_ws(char transa, char transb, int m, int n, int k, d
                                 int* err_dev, cudaStream_t stream);
 
 // The Fmo GEMMs run in FP64, or -- when split_ws is given -- with the
-// three-product BF16 split on the tensor cores (mb_gemm_split_ws).
+// three-product BF16 split on the tensor cores (mb_gemm_split_ws).  bigeps is
+// the reference's relative rotation threshold (1.5e-7, diag_for_GPU.F90:33);
+// the SCF's FP64 finish passes 0 so that no rotation above tiny is skipped.
 extern "C" int mb_pseudo_diag_ex(int n, int nocc, const double* fpacked, double* c, const double* eigs,
                                  unsigned long long* nrot_dev, void* ws, void* split_ws, size_t split_ws_bytes,
-                                 int* split_err, cudaStream_t stream) {
+                                 int* split_err, double bigeps, cudaStream_t stream) {
   const int nvirt = n - nocc;
   if (nocc <= 0 || nvirt <= 0) return MB_OK;
   if (((uintptr_t)ws & 255) != 0) return mb_set_error(MB_ERR_ARG, "pseudo-diag workspace must be 256-byte aligned");
@@ -436,14 +438,48 @@ extern "C" int mb_pseudo_diag_ex(int n, int nocc, const double* fpacked, double*
   if (blocks > 148 * 8) blocks = 148 * 8;
   absmax_kernel<<<blocks, 256, 0, stream>>>((long long)kv, fmo, tiny);
   MB_LAUNCH_CHECK();
-  rot_coeff_kernel<<<blocks, 256, 0, stream>>>(nocc, nvirt, fmo, eigs, tiny, -1.0, 1.5e-7, al, be, act, tcnt, nrot_dev, tv);
+  rot_coeff_kernel<<<blocks, 256, 0, stream>>>(nocc, nvirt, fmo, eigs, tiny, -1.0, bigeps, al, be, act, tcnt, nrot_dev, tv);
   MB_LAUNCH_CHECK();
   return launch_wavefronts(n, nocc, nvirt, c, al, be, act, tcnt, to, tv, stream);
 }
 
+namespace {
+// e[j] = sum_r c[r, j] * g[r, j] for column-major c, g (one CTA per column).
+__global__ void coldot_kernel(int n, const double* __restrict__ c, const double* __restrict__ g,
+                              double* __restrict__ e) {
+  __shared__ double red[256];
+  const long long col = (long long)blockIdx.x * n;
+  double s = 0.0;
+  for (int r = threadIdx.x; r < n; r += blockDim.x) s += c[col + r] * g[col + r];
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+    if (threadIdx.x < h) red[threadIdx.x] += red[threadIdx.x + h];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) e[blockIdx.x] = red[0];
+}
+}  // namespace
+
+// Orbital energies of the current vectors, e_j = c_j^T F c_j (the diagonal of
+// C^T F C), for the SCF's FP64 finish: the pseudo-diagonalisation takes its
+// rotation angles from the energies of the last full diagonalisation, which
+// carry the level shift of that iteration; the finish refreshes them once.
+// ws: 2 n^2 doubles.
+extern "C" int mb_orbital_energies_ws(int n, const double* fpacked, const double* c, double* eigs, void* ws,
+                                      cudaStream_t stream) {
+  double* ff = (double*)ws;
+  double* g = ff + (size_t)n * n;
+  MB_TRY(mb_unpack_dev(n, fpacked, ff, n, 0, nullptr, stream));
+  MB_TRY(mb_dgemm_dev('N', 'N', n, n, n, 1.0, ff, n, c, n, 0.0, g, n, stream));
+  coldot_kernel<<<n, 256, 0, stream>>>(n, c, g, eigs);
+  MB_LAUNCH_CHECK();
+  return MB_OK;
+}
+
 extern "C" int mb_pseudo_diag_ws(int n, int nocc, const double* fpacked, double* c, const double* eigs,
                                  unsigned long long* nrot_dev, void* ws, cudaStream_t stream) {
-  return mb_pseudo_diag_ex(n, nocc, fpacked, c, eigs, nrot_dev, ws, nullptr, 0, nullptr, stream);
+  return mb_pseudo_diag_ex(n, nocc, fpacked, c, eigs, nrot_dev, ws, nullptr, 0, nullptr, 1.5e-7, stream);
 }
 
 // Rotation sweep alone with caller-given Fmo, tiny and bigeps (the arguments

@@ -34,6 +34,8 @@ class ScfResult:
     t_total_ms: float
     n_pulay: int = 0
     n_split: int = 0
+    n_finish: int = 0
+    dp: float = -1.0
 
 
 class ScfContext:
@@ -83,7 +85,11 @@ class ScfContext:
 
     def run(self, pseudo: bool = False, scfcrt: float = 1.0e-4, itrmax: int = 2000, precision: int = 0,
             switch_pl: float = 1.0e-4, verbose: bool = False, pulay: bool = False,
-            guess: bool = False) -> ScfResult:
+            guess: bool = False, finish_dp: float = -1.0, finish_max: int = 40) -> ScfResult:
+        """finish_dp: the FP64 finish (mb_scf_opts.finish_dp): < 0 automatic
+        (1e-7 with precision=1, off with precision=0), 0 off, > 0 the bound on
+        the last density update max|P_k - P_(k-1)| before convergence is
+        accepted."""
         o = ScfOpts()
         lib().mb_scf_opts_default(ctypes.byref(o))
         o.pseudo = int(pseudo)
@@ -94,10 +100,13 @@ class ScfContext:
         o.verbose = int(verbose)
         o.pulay = int(pulay)
         o.guess = int(guess)
+        o.finish_dp = float(finish_dp)
+        o.finish_max = int(finish_max)
         r = ScfRes()
         check(lib().mb_scf_run(self._h, ctypes.byref(o), ctypes.byref(r)))
         return ScfResult(r.escf, r.ee, r.niter, bool(r.converged), r.n_full_diag, r.n_pseudo_diag, r.pl,
-                         r.t_fock_ms, r.t_diag_ms, r.t_density_ms, r.t_other_ms, r.t_total_ms, r.n_pulay, r.n_split)
+                         r.t_fock_ms, r.t_diag_ms, r.t_density_ms, r.t_other_ms, r.t_total_ms, r.n_pulay, r.n_split,
+                         r.n_finish, r.dp)
 
     def density(self) -> np.ndarray:
         p = np.empty(self.mpack)

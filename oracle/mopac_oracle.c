@@ -33,9 +33,12 @@
  * Summation orders of fock2/jab/kab/fock1/helect are kept term by term; the
  * file is compiled with -ffp-contract=off so no FMA is introduced.
  */
+#define _GNU_SOURCE
 #include <math.h>
+#include <pthread.h>
 #include <stdlib.h>
 #include <string.h>
+#include <unistd.h>
 
 #define A0 0.529177210903
 #define EV 27.211386245988
@@ -2231,4 +2234,87 @@ long long orc_mz_hcore(int numat, const int *nat, const double *coord, const lon
   }
   *enuclr_out = enuclr;
   return kr;
+}
+
+/* diag_for_GPU.F90:151-206 (CPU branch): the ordered 2x2 rotation sweep over
+ * the columns of c (n x n, column-major), occupied i outer and virtual j
+ * inner.  fmo is nvirt x nocc column-major, eig holds the orbital energies.
+ * A pair is skipped when |x| < tiny or |x/d| < bigeps.  Every row of c sees
+ * the same rotations in the same order and rows never mix, so the rows are
+ * split over POSIX threads without changing any result.  Returns the number
+ * of rotations applied. */
+typedef struct {
+  int n, r0, r1;
+  long long cnt;
+  const double *al, *be;
+  const int *idx;
+  double *c;
+} RotJob;
+
+static void *rot_rows(void *arg) {
+  RotJob *j = (RotJob *)arg;
+  for (int b0 = j->r0; b0 < j->r1; b0 += 8) {
+    int b1 = b0 + 8 < j->r1 ? b0 + 8 : j->r1;
+    for (long long q = 0; q < j->cnt; ++q) {
+      double a = j->al[q], b = j->be[q];
+      double *ci = j->c + (long long)j->idx[2 * q] * j->n, *cj = j->c + (long long)j->idx[2 * q + 1] * j->n;
+      for (int r = b0; r < b1; ++r) {
+        double x = ci[r], y = cj[r];
+        ci[r] = a * x + b * y;
+        cj[r] = a * y - b * x;
+      }
+    }
+  }
+  return NULL;
+}
+
+long long orc_rot_sweep(int n, int nocc, const double *fmo, const double *eig, double *c, double bigeps,
+                        double tiny) {
+  const int nvirt = n - nocc;
+  if (nocc <= 0 || nvirt <= 0) return 0;
+  const long long kv = (long long)nocc * nvirt;
+  double *al = (double *)malloc(sizeof(double) * (size_t)kv);
+  double *be = (double *)malloc(sizeof(double) * (size_t)kv);
+  int *idx = (int *)malloc(sizeof(int) * 2 * (size_t)kv);
+  long long cnt = 0;
+  for (int i = 0; i < nocc; ++i)
+    for (int jv = 0; jv < nvirt; ++jv) {
+      double x = fmo[jv + (long long)nvirt * i];
+      if (fabs(x) < tiny) continue;
+      double d = eig[i] - eig[nocc + jv];
+      if (fabs(x / d) < bigeps) continue;
+      double e = copysign(sqrt(4.0 * x * x + d * d), d);
+      double a = sqrt(0.5 * (1.0 + d / e));
+      al[cnt] = a;
+      be[cnt] = -copysign(sqrt(1.0 - a * a), x);
+      idx[2 * cnt] = i;
+      idx[2 * cnt + 1] = nocc + jv;
+      ++cnt;
+    }
+  int nt = (int)sysconf(_SC_NPROCESSORS_ONLN);
+  const char *env = getenv("OMP_NUM_THREADS");
+  if (env && atoi(env) > 0) nt = atoi(env);
+  if (nt < 1) nt = 1;
+  if (nt > 64) nt = 64;
+  if (nt > (n + 7) / 8) nt = (n + 7) / 8;
+  pthread_t th[64];
+  RotJob jobs[64];
+  int chunk = ((n + nt - 1) / nt + 7) / 8 * 8;
+  int started = 0;
+  for (int t = 0; t < nt; ++t) {
+    int r0 = t * chunk, r1 = r0 + chunk < n ? r0 + chunk : n;
+    if (r0 >= r1) break;
+    RotJob jb = {n, r0, r1, cnt, al, be, idx, c};
+    jobs[t] = jb;
+    if (t == 0) continue;
+    if (pthread_create(&th[t], NULL, rot_rows, &jobs[t]) != 0) { rot_rows(&jobs[t]); th[t] = 0; }
+    started = t;
+  }
+  rot_rows(&jobs[0]);
+  for (int t = 1; t <= started; ++t)
+    if (th[t]) pthread_join(th[t], NULL);
+  free(al);
+  free(be);
+  free(idx);
+  return cnt;
 }

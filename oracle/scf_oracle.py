@@ -69,6 +69,9 @@ def lib():
         L.orc_disp_pm7.restype = ctypes.c_double
         L.orc_param.argtypes = [ctypes.c_int, ctypes.c_char_p]
         L.orc_param.restype = ctypes.c_double
+        f64f = np.ctypeslib.ndpointer(np.float64, flags="F")
+        L.orc_rot_sweep.argtypes = [ctypes.c_int, ctypes.c_int, f64f, f64p, f64f, ctypes.c_double, ctypes.c_double]
+        L.orc_rot_sweep.restype = ctypes.c_longlong
         _lib = L
     return _lib
 
@@ -196,6 +199,19 @@ def fmo_block(f: np.ndarray, c: np.ndarray, nocc: int) -> np.ndarray:
 
 def rotation_sweep(c: np.ndarray, fmo: np.ndarray, eig: np.ndarray, nocc: int,
                    bigeps: float = 1.5e-7, tiny: float | None = None) -> int:
+    """diag_for_GPU.F90:151-206 (CPU branch) in C (orc_rot_sweep): the same
+    rotations in the same order as ``rotation_sweep_py``, bit for bit, with
+    the rows of c split over threads.  c must be Fortran-ordered (n x n)."""
+    if tiny is None:
+        tiny = float(np.max(np.abs(fmo))) * 0.05
+    assert c.flags.f_contiguous and c.dtype == np.float64
+    fmo = np.asfortranarray(fmo, dtype=np.float64)
+    eig = np.ascontiguousarray(eig, dtype=np.float64)
+    return int(lib().orc_rot_sweep(c.shape[0], nocc, fmo, eig, c, float(bigeps), float(tiny)))
+
+
+def rotation_sweep_py(c: np.ndarray, fmo: np.ndarray, eig: np.ndarray, nocc: int,
+                      bigeps: float = 1.5e-7, tiny: float | None = None) -> int:
     """diag_for_GPU.F90:151-206 (CPU branch).  Rotates columns of c in place in
     the reference order (occupied i outer, virtual j inner); returns the count
     of rotations applied."""
@@ -224,9 +240,9 @@ def rotation_sweep(c: np.ndarray, fmo: np.ndarray, eig: np.ndarray, nocc: int,
     return done
 
 
-def pseudo_diag(f, c, nocc, eig):
+def pseudo_diag(f, c, nocc, eig, bigeps: float = 1.5e-7):
     fmo = fmo_block(f, c, nocc)
-    return rotation_sweep(c, fmo, eig, nocc)
+    return rotation_sweep(c, fmo, eig, nocc, bigeps=bigeps)
 
 
 # ---------------------------------------------------------------- pulay
@@ -420,17 +436,31 @@ class ScfResult:
     niter: int
     converged: bool
     history: list
+    n_finish: int = 0
 
 
 def iter_scf(s: System, pseudo: bool = False, scfcrt: float = 1.0e-4, itrmax: int = 2000,
              gnorm: float = 0.0, trace: bool = False, pulay_on: bool = False,
-             p_guess: np.ndarray | None = None) -> ScfResult:
+             p_guess: np.ndarray | None = None, finish_dp: float = 0.0,
+             finish_max: int = 40) -> ScfResult:
     """Closed-shell restatement of iter (SCF/iter.F90), 1SCF settings
     (last = 1, nscf = 0, fulscf = .true.).
 
     p_guess: a starting total density (packed).  It enters like a density
     read with OLDENS (iter.F90:151-158: pa = p/2, pold = 2*pa); pold2, which
-    that branch leaves as allocated, starts as the diagonal of p."""
+    that branch leaves as allocated, starts as the diagonal of p.
+
+    finish_dp > 0 adds the FP64 finish of the device SCF (mb_scf_opts
+    finish_dp): once iter's test (:675-690) passes, convergence is accepted
+    only when the last density update moved no element of P by more than
+    finish_dp (max|P_k - P_(k-1)| over all mpack elements); otherwise the
+    loop goes on, at most finish_max more iterations, and the rotation
+    sweep's relative threshold bigeps (diag_for_GPU.F90:33) is 0 in those
+    iterations.  The pseudo-diagonalisation takes its rotation angles from
+    the orbital energies of the last full diagonalisation, which carry that
+    iteration's level shift (-8 eV on the virtuals with Pulay); at its first
+    iteration the finish replaces them by the energies of the current
+    vectors, diag(C^T F C).  With finish_dp = 0 this is iter unchanged."""
     n = s.norbs
     mpack = s.mpack
     nclose = s.nclose
@@ -499,6 +529,9 @@ def iter_scf(s: System, pseudo: bool = False, scfcrt: float = 1.0e-4, itrmax: in
     ramp = np.arange(1, mpack + 1) * 1.0e-16
     f = None
     converged = False
+    dp = np.inf          # max|P_k - P_(k-1)| of the last density update
+    n_finish = 0         # iterations the finish added after iter's test passed
+    refreshed = False    # orbital energies refreshed for the finish
     while True:  # label 250
         niter += 1
         if niter > itrmax:
@@ -552,6 +585,9 @@ def iter_scf(s: System, pseudo: bool = False, scfcrt: float = 1.0e-4, itrmax: in
                 ten = ten * 0.975 + 0.05
             sellim = max(selcon, 1.0e-15 * max(abs(ee), 1.0))
             conv = niter > 4 and (pl == 0.0 or (pl < pltest and abs(diff) < sellim)) and ready
+            if conv and finish_dp > 0.0 and dp > finish_dp and n_finish < finish_max:
+                n_finish += 1
+                conv = False
             if conv:
                 if abs(shift) < 1.0e-10:
                     converged = True
@@ -571,12 +607,20 @@ def iter_scf(s: System, pseudo: bool = False, scfcrt: float = 1.0e-4, itrmax: in
         if newdg and okpuly and iredy > 1:
             pl = pulay(pst, f, pa)
         if newdg and pseudo and not (halfe or camkin):
-            pseudo_diag(f, c, na1el, eigs)
+            if n_finish > 0 and not refreshed:
+                # the finish refreshes the orbital energies the rotation
+                # angles use: eigs from the last full diagonalisation carry
+                # that iteration's level shift
+                eigs = np.einsum("ij,ij->j", c, unpack(f, n) @ c)
+                refreshed = True
+            pseudo_diag(f, c, na1el, eigs, bigeps=0.0 if n_finish > 0 else 1.5e-7)
         else:
             c, eigs = eigenvectors_lapack(f, n)
+        p_before = p
         p = density(c, nclose)
         if not (newdg and okpuly):
             pl = cnvg(n, p, pold, pold2, niter)
+        dp = float(np.max(np.abs(p - p_before)))
         pa = p * 0.5
         oknewd = pl < sellim or oknewd
         newdg = (pl < trans and oknewd) or newdg
@@ -588,7 +632,48 @@ def iter_scf(s: System, pseudo: bool = False, scfcrt: float = 1.0e-4, itrmax: in
     c, eigs = eigenvectors_lapack(fcopy, n)
     escf = (ee + s.enuclr) * enrgy + s.atheat
     return ScfResult(escf=escf, ee=ee, eigs=eigs, c=c, p=p, niter=niter, converged=converged,
-                     history=history)
+                     history=history, n_finish=n_finish)
+
+
+# ---------------------------------------------------------------- fixed point
+def roothaan_step(s: System, p: np.ndarray):
+    """One plain SCF step from the total density p: F(p) = H + fock2
+    (iter.F90:553), the heat at p (:641-659), the full diagonalisation with
+    the reference's perturbation (eigenvectors_LAPACK.F90:53-121) and the
+    closed-shell density of its eigenvectors (density_for_GPU.F90:102-108).
+    Returns (new density, eigenvalues of F(p), heat of formation at p)."""
+    f = s.h.copy()
+    fock2(s, f, p, p * 0.5)
+    ee = helect(s.norbs, p * 0.5, s.h, f) * 2.0
+    heat = (ee + s.enuclr) * FPC9 + s.atheat
+    c, e = eigenvectors_lapack(f, s.norbs)
+    return density(c, s.nclose), e, heat
+
+
+def fixed_point_certificate(s: System, p: np.ndarray, steps: int = 3) -> dict:
+    """How far a density p is from the oracle's self-consistent point P*.
+
+    Runs ``steps`` plain steps P_k = T(P_(k-1)) from P_0 = p and records
+    r_k = max|P_k - P_(k-1)|.  Near P* the step is a contraction with factor
+    rho (estimated as the largest r_(k+1)/r_k), so max|p - P*| <= r_1/(1 - rho);
+    for water clusters rho is about 0.6 and the bound matches the true
+    distance to within a few percent.  Also returns the orbital energies of
+    F(p) (what iter's exit diagonalisation gives for a converged p) and the
+    heat at p and at P_steps."""
+    rs, heats = [], []
+    pk = p
+    eigs0 = None
+    for k in range(steps):
+        pn, e, heat = roothaan_step(s, pk)
+        if k == 0:
+            eigs0 = e
+        heats.append(heat)
+        rs.append(float(np.max(np.abs(pn - pk))))
+        pk = pn
+    ratios = [rs[k + 1] / rs[k] for k in range(len(rs) - 1) if rs[k] > 0.0]
+    rho = max(ratios) if ratios else 0.0
+    bound = rs[0] / (1.0 - rho) if rho < 1.0 else float("inf")
+    return dict(r=rs, rho=rho, bound=bound, eigs=eigs0, heat_at_p=heats[0], heat_last=heats[-1], p_last=pk)
 
 
 # ---------------------------------------------------------------- properties

@@ -1,14 +1,16 @@
 """Split-precision tensor-core GEMMs (tcgen05, three BF16 products) and the
-SCF's precision switch.
+SCF's precision switch with its FP64 finish.
 
 Tolerance of the split products: |C - C_fp64| <= 1e-4 * (|A| |B|) element by
 element (three BF16 products leave ~2^-16 relative per product; FP32
-accumulation adds ~k 2^-24 in the worst case).  The SCF with the switch on
-takes a different trajectory from the FP64 one, so it lands on the same
-self-consistent state only to within the SCF's own convergence test: heat
-1e-4 kcal/mol, density and orbital energies 1e-4 (the bar the pseudo- and
-full-diagonalisation paths are held to against each other); convergence is
-only accepted after FP64 has taken over.
+accumulation adds ~k 2^-24 in the worst case).
+
+The SCF with the switch on takes a different path from the FP64 one; iter's
+own convergence test stops 1e-5..1e-4 away from the self-consistent density,
+so the split SCF finishes in FP64 (mb_scf_opts.finish_dp, 1e-7 by default
+with precision = 1) until the density stops moving, and is held to the
+self-consistent point of the FP64 oracle: heat 1e-4 kcal/mol, density 1e-6,
+orbital energies 1e-5 eV.
 """
 import ctypes
 
@@ -99,22 +101,63 @@ def test_matmul_split_wrapper():
     assert np.all(np.abs(c - a @ b) <= 1e-4 * (np.abs(a) @ np.abs(b)) + 1e-12)
 
 
-@pytest.mark.parametrize("name", ["water16", "propane", "heptane"])
-@pytest.mark.parametrize("pseudo", [False, True])
-def test_split_precision_scf_lands_on_fp64_oracle(name, pseudo):
+def _fixed_point(s):
+    """The oracle's self-consistent point: plain iter run to 1e-11 in P."""
+    return so.iter_scf(s, scfcrt=1.0e-12, finish_dp=1.0e-11, finish_max=200)
+
+
+@pytest.mark.parametrize("name", ["water16", "propane", "heptane", "co2_1scf"])
+@pytest.mark.parametrize("pseudo,pulay", [(False, False), (True, False), (True, True)])
+def test_split_precision_scf_lands_on_fp64_oracle(name, pseudo, pulay):
     from mopac_gpu_b200 import ScfContext
     nat, xyz = SYSTEMS[name]
     s = oracle_system(nat, xyz)
-    ref = so.iter_scf(s, pseudo=pseudo)
+    ref = _fixed_point(s)
     ctx = ScfContext(nat, xyz)
     ctx.set_hw(s.h, s.w, s.enuclr)
-    r = ctx.run(pseudo=pseudo, precision=1, switch_pl=1e-4)
+    r = ctx.run(pseudo=pseudo, pulay=pulay, precision=1, switch_pl=1e-4)
     p = ctx.density()
     _, e = ctx.vectors()
     ctx.close()
-    assert r.converged and r.n_split > 0
-    print(f"{name} pseudo={pseudo}: dHf {r.escf - ref.escf:.2e} kcal/mol, max|dP| {np.abs(p - ref.p).max():.2e}, "
-          f"max|de| {np.abs(e - ref.eigs).max():.2e} eV, split iterations {r.n_split} of {r.niter}")
+    assert r.converged and r.n_split > 0 and r.dp <= 1e-7
+    print(f"{name} pseudo={pseudo} pulay={pulay}: dHf {r.escf - ref.escf:.2e} kcal/mol, "
+          f"max|dP| {np.abs(p - ref.p).max():.2e}, max|de| {np.abs(e - ref.eigs).max():.2e} eV, "
+          f"split iterations {r.n_split}, finish {r.n_finish} of {r.niter}")
     assert abs(r.escf - ref.escf) < 1e-4
-    np.testing.assert_allclose(p, ref.p, atol=1e-4)
-    np.testing.assert_allclose(e, ref.eigs, atol=1e-4)
+    assert np.abs(p - ref.p).max() < 1e-6
+    assert np.abs(e - ref.eigs).max() < 1e-5
+
+
+def test_split_scf_matches_the_oracle_running_the_same_finish():
+    """Same algorithm on both sides (pseudo-diagonalisation, Pulay, finish):
+    the GPU's split SCF and the oracle's FP64 one end within 1e-6."""
+    from mopac_gpu_b200 import ScfContext, workloads
+    nat, xyz, _ = workloads.water_box(32)
+    s = oracle_system(nat, xyz)
+    ref = so.iter_scf(s, pseudo=True, pulay_on=True, finish_dp=1.0e-7)
+    ctx = ScfContext(nat, xyz)
+    ctx.set_hw(s.h, s.w, s.enuclr)
+    r = ctx.run(pseudo=True, pulay=True, precision=1)
+    p = ctx.density()
+    _, e = ctx.vectors()
+    ctx.close()
+    assert r.converged and ref.converged
+    assert abs(r.escf - ref.escf) < 1e-4
+    assert np.abs(p - ref.p).max() < 1e-6
+    assert np.abs(e - ref.eigs).max() < 1e-5
+
+
+def test_finish_off_keeps_iter_semantics():
+    """finish_dp = 0 on the FP64 path is iter unchanged: same iterations and
+    density as the oracle without the finish."""
+    from mopac_gpu_b200 import ScfContext
+    nat, xyz = SYSTEMS["water16"]
+    s = oracle_system(nat, xyz)
+    ref = so.iter_scf(s, pseudo=True, pulay_on=True)
+    ctx = ScfContext(nat, xyz)
+    ctx.set_hw(s.h, s.w, s.enuclr)
+    r = ctx.run(pseudo=True, pulay=True, precision=0, finish_dp=0.0)
+    p = ctx.density()
+    ctx.close()
+    assert r.n_finish == 0 and r.dp == -1.0 and r.niter == ref.niter
+    assert np.abs(p - ref.p).max() < 1e-7
