@@ -22,9 +22,12 @@ between steps anyway).  The headline metric is SCF single points per second
               of the plain FP64 path (full eigensolve every iteration, FP64
               GEMMs) on the same box.
 --impl reference
-              times the CPU implementation of the same SCF (the oracle's C
-              kernels with LAPACK dsyevd through numpy) on the host cores on a
-              bounded sample and extrapolates to one SCF; N > 1: rank 0 only.
+              times the CPU implementation of the same SCF (the oracle: C
+              Fock build and rotation sweep, LAPACK dsyevd and BLAS through
+              numpy) on the host cores: one complete SCF in the same mode
+              (pseudo-diagonalisation, Pulay, finish to max|dP| <= 1e-7, all
+              FP64), reported as --steps slices of that one timed SCF, plus a
+              complete plain-mode SCF beside it; N > 1: rank 0 only.
 --converger pulay (default in fast mode) Pulay's DIIS once newdg is set,
               like the PULAY keyword; cnvg: the default extrapolation.
 --guess standard (default) the reference's diagonal guess; learned: each step
@@ -63,10 +66,9 @@ WORKLOAD = "(H2O)512 water box, PM7 1SCF, RHF closed shell, 1536 atoms, 3072 bas
 METRIC = "scf_single_points_per_s"
 BATCH_WORKLOAD = ("linear alkanes C3H8..C20H42, seeded random staggered conformers (no syn-pentane pairs), "
                   "PM7 1SCF each, RHF closed shell, 11-62 atoms, 20-122 basis functions")
-# Iterations the reference algorithm needs on this input from the standard
-# guess with full diagonalisation each iteration (same for the CPU oracle and
-# the GPU plain path; used to scale the CPU sample to one SCF).
-CPU_NITER_FALLBACK = 15
+# FP64 finish of the split-precision SCF (mb_scf_opts.finish_dp), used by the
+# oracle runs in the same mode
+FINISH_DP = 1.0e-7
 
 
 def parse():
@@ -146,29 +148,36 @@ def dist_init():
     return ws, rank, local
 
 
-def cpu_sample(nwater: int, iters: int = 1):
-    """Time `iters` SCF iterations of the oracle (fock2 + LAPACK eigensolve +
-    density + cnvg) on the host cores; return seconds per iteration."""
-    import numpy as np
+def oracle_system(nwater: int):
+    """The water box in the CPU oracle (integrals on the host)."""
     from mopac_gpu_b200 import workloads as wl
     from oracle import scf_oracle as so
     nat, xyz, _ = wl.water_box(nwater)
-    s = so.make_system(nat, xyz)
+    return so.make_system(nat, xyz)
+
+
+def oracle_scf(s, mode: str):
+    """One complete oracle SCF from the standard guess, timed on the host:
+    mode "fast" is the GPU arm's default algorithm (pseudo-diagonalisation
+    once newdg is set, Pulay, FP64 finish to max|dP| <= FINISH_DP), "plain"
+    a full LAPACK eigensolve every iteration with cnvg (iter's default).
+    Returns (result, seconds)."""
+    from oracle import scf_oracle as so
+    kw = dict(pseudo=True, pulay_on=True, finish_dp=FINISH_DP) if mode == "fast" else {}
+    t0 = time.perf_counter()
+    r = so.iter_scf(s, **kw)
+    return r, time.perf_counter() - t0
+
+
+def warm_host(s, steps: int):
+    """Untimed plain oracle steps (Fock build, eigensolve, density) to start
+    the BLAS threads and page in the integrals."""
+    import numpy as np
+    from oracle import scf_oracle as so
     p = np.zeros(s.mpack)
     p[so.diag_index(s.norbs)] = s.pdiag
-    pa = p * 0.5
-    pold = pa.copy()
-    pold2 = pold[so.diag_index(s.norbs)].copy()
-    t0 = time.perf_counter()
-    for it in range(1, iters + 1):
-        f = s.h.copy()
-        so.fock2(s, f, p, pa)
-        so.helect(s.norbs, pa, s.h, f)
-        c, e = so.eigenvectors_lapack(f, s.norbs)
-        p = so.density(c, s.nclose)
-        so.cnvg(s.norbs, p, pold, pold2, it)
-        pa = p * 0.5
-    return (time.perf_counter() - t0) / iters
+    for _ in range(steps):
+        p, _, _ = so.roothaan_step(s, p)
 
 
 def _cpu_one(mol):
@@ -178,27 +187,33 @@ def _cpu_one(mol):
     return r.escf
 
 
+def batch_sample(n: int, nsample: int):
+    """Indices of an evenly spaced sample of a batch of n molecules."""
+    step = max(1, n // nsample)
+    return list(range(0, n, step))[:nsample]
+
+
 def cpu_batch_rate(mols, nsample: int, workers: int):
     """SCF/s of the CPU oracle over an evenly spaced sample of the molecules,
     `workers` processes (spawned) each running whole SCFs with one BLAS
-    thread; the pool is warmed on one molecule per worker first."""
+    thread; the pool is warmed on one molecule per worker first.  Returns
+    (rate, sample size, the sample's heats)."""
     import multiprocessing as mp
-    step = max(1, len(mols) // nsample)
-    sample = mols[::step][:nsample]
+    sample = [mols[i] for i in batch_sample(len(mols), nsample)]
     old = os.environ.get("OPENBLAS_NUM_THREADS")
     os.environ["OPENBLAS_NUM_THREADS"] = "1"
     try:
         with mp.get_context("spawn").Pool(workers) as pool:
             pool.map(_cpu_one, mols[:workers], chunksize=1)
             t0 = time.perf_counter()
-            pool.map(_cpu_one, sample, chunksize=1)
+            heats = pool.map(_cpu_one, sample, chunksize=1)
             dt = time.perf_counter() - t0
     finally:
         if old is None:
             os.environ.pop("OPENBLAS_NUM_THREADS", None)
         else:
             os.environ["OPENBLAS_NUM_THREADS"] = old
-    return len(sample) / dt, len(sample)
+    return len(sample) / dt, len(sample), heats
 
 
 def run_batch(args, flush, L, ws=1, rank=0, dist=None):
@@ -294,43 +309,72 @@ def run_batch(args, flush, L, ws=1, rank=0, dist=None):
     }
     if not args.no_cpu_baseline:
         workers = os.cpu_count() or 1
-        rate, ns = cpu_batch_rate(mols, 8 * workers, workers)
+        rate, ns, heats = cpu_batch_rate(mols, 8 * workers, workers)
+        sidx = batch_sample(len(mols), 8 * workers)
+        dh = np.abs(np.asarray(heats) - escf[sidx])
         out["cpu_baseline"] = {"value": rate, "unit": "SCF/s", "cores": workers, "kind": "port",
                                "sample": f"{ns} evenly spaced molecules of the batch, one whole oracle SCF per "
                                          f"task, {workers} spawned processes"}
+        out["parity_vs_oracle"] = {"molecules": ns, "max_abs_dHf_kcal_mol": float(dh.max()),
+                                   "mean_abs_dHf_kcal_mol": float(dh.mean()),
+                                   "what": "heat of every sampled molecule in the timed batched launch against "
+                                           "the oracle's complete SCF of the same molecule"}
     return out
 
 
+def bench_config(args, edge: float) -> dict:
+    """The workload description both arms print (the reference arm runs the
+    same SCF algorithm on the host, in FP64 throughout)."""
+    return {"workload": WORKLOAD, "mode": args.mode, "guess": args.guess,
+            "converger": "pulay" if (args.mode == "fast" and args.converger == "pulay") else "cnvg",
+            "finish_dp": FINISH_DP if args.precision == "split" else 0.0,
+            "parallelism": "replicas x1" if args.gpus == 1 else f"replicas x{args.gpus}",
+            "l2": "GPU: flushed between steps (256 MB write); W = 151 MB > L2",
+            "cell_edge_A": round(edge, 3)}
+
+
 def run_reference(args):
+    """The reference arm: the CPU implementation of the same SCF (the oracle)
+    on all host cores.  Its timed region is ONE complete SCF from the standard
+    guess in the GPU arm's mode (fast: pseudo-diagonalisation, Pulay, finish
+    to max|dP| <= FINISH_DP, FP64), because one SCF of the 3072-orbital box
+    takes about a minute on the host; it is reported as --steps slices of
+    that SCF (ms_per_step = SCF time / steps).  A complete plain-mode SCF
+    (full eigensolve every iteration, cnvg) is timed beside it."""
     ws, rank, _ = dist_init()
     if rank != 0:
         return 0
-    os.environ.setdefault("OPENBLAS_NUM_THREADS", str(os.cpu_count()))
     cores = os.cpu_count()
-    per_iter = []
-    for _ in range(args.warmup):
-        cpu_sample(args.nwater)
-    for _ in range(args.steps):
-        per_iter.append(cpu_sample(args.nwater))
-    t_iter = statistics.mean(per_iter)
-    t_scf = t_iter * CPU_NITER_FALLBACK
+    os.environ.setdefault("OPENBLAS_NUM_THREADS", str(cores))
+    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+    from mopac_gpu_b200 import workloads
+    _, _, edge = workloads.water_box(args.nwater)
+    s = oracle_system(args.nwater)
+    warm_host(s, min(args.warmup, 2))
+    r, t_scf = oracle_scf(s, args.mode)
+    rp, t_plain = oracle_scf(s, "plain") if args.mode == "fast" else (r, t_scf)
     val = 1.0 / t_scf
+    mode_txt = ("pseudo-diagonalisation once newdg is set, Pulay, FP64 finish to max|dP| <= 1e-7"
+                if args.mode == "fast" else "full eigensolve every iteration, cnvg")
     line = {
         "impl": "reference", "metric": METRIC, "value": val, "unit": "SCF/s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_scf * 1e3, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded water box)",
-        "config": {"workload": WORKLOAD, "mode": "plain (full diagonalisation every iteration)",
-                   "l2": "n/a (CPU)"},
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_scf * 1e3 / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded water box, random sequential insertion)",
+        "config": bench_config(args, edge),
         "scf_wall_s": t_scf,
+        "scf": {"escf_kcal_mol": r.escf, "niter": r.niter, "finish_iterations": r.n_finish, "converged": r.converged},
+        "plain_mode": {"scf_wall_s": t_plain, "niter": rp.niter, "escf_kcal_mol": rp.escf,
+                       "mode": "full LAPACK eigensolve every iteration, cnvg (iter's default)"},
         "cpu_baseline": {"value": val, "unit": "SCF/s", "cores": cores, "kind": "port",
-                         "sample": f"one SCF iteration (fock2 + LAPACK dsyevd + density + cnvg) per step, "
-                                   f"scaled by {CPU_NITER_FALLBACK} iterations to one SCF"},
+                         "sample": f"one complete oracle SCF of the box ({mode_txt}; C Fock build and rotation "
+                                   f"sweep, LAPACK dsyevd / BLAS on {cores} threads), timed whole; the line's "
+                                   f"{args.steps} steps are equal slices of it"},
         "e2e": {"value": val, "unit": "SCF/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     if args.batch > 0:
-        from mopac_gpu_b200 import workloads
         mols = workloads.alkane_batch(args.batch)
-        rate, ns = cpu_batch_rate(mols, 8 * cores, cores)
+        rate, ns, _ = cpu_batch_rate(mols, 8 * cores, cores)
         line["batched"] = {"workload": f"{len(mols)} {BATCH_WORKLOAD}", "metric": "batched_scfs_per_s",
                            "value": rate, "unit": "SCF/s", "cores": cores, "kind": "port",
                            "sample": f"{ns} evenly spaced molecules of the batch, one whole oracle SCF per "
@@ -415,6 +459,9 @@ def run_mine(args):
     from mopac_gpu_b200.replicas import max_over_ranks
     t_ms = max_over_ranks(statistics.mean(times), dist, "cuda")
     r = results[-1]
+    # the timed SCF's density and orbital energies, for the oracle comparison
+    p_fast = ctx.density()
+    _, e_fast = ctx.vectors()
     # ---- end to end through the C ABI with host buffers
     e2e = None
     if not args.no_e2e:
@@ -487,25 +534,43 @@ def run_mine(args):
                 "ms_standard": ev.ms_std, "ms_learned_incl_prediction": ev.ms_learned,
                 "speedup": ev.ms_std / ev.ms_learned, "max_abs_dHf_kcal_mol": ev.max_dhf,
                 "fallbacks": ev.n_fallback}
-    cpu = None
+    cpu, parity = None, None
     if rank == 0 and not args.no_cpu_baseline:
-        os.environ.setdefault("OPENBLAS_NUM_THREADS", str(os.cpu_count()))
-        t_iter = cpu_sample(args.nwater)
-        t_scf = t_iter * CPU_NITER_FALLBACK
-        cpu = {"value": 1.0 / t_scf, "unit": "SCF/s", "cores": os.cpu_count(), "kind": "port",
-               "sample": f"one SCF iteration of the CPU oracle (fock2 in C, LAPACK dsyevd, density, cnvg) "
-                         f"scaled by {CPU_NITER_FALLBACK} iterations", "scf_wall_s": t_scf}
+        # the CPU oracle: one complete SCF of the same box in the same mode on
+        # the host cores (the baseline), compared with the timed GPU SCF, and
+        # the fixed-point certificate of the GPU density (three plain oracle
+        # steps from it bound its distance to the self-consistent density)
+        import numpy as np
+        from oracle import scf_oracle as so
+        cores = os.cpu_count()
+        os.environ.setdefault("OPENBLAS_NUM_THREADS", str(cores))
+        s_or = oracle_system(args.nwater)
+        ro, t_or = oracle_scf(s_or, args.mode)
+        cpu = {"value": 1.0 / t_or, "unit": "SCF/s", "cores": cores, "kind": "port",
+               "sample": "one complete oracle SCF of the box in the same mode (C Fock build and rotation sweep, "
+                         f"LAPACK dsyevd / BLAS on {cores} threads), timed whole", "scf_wall_s": t_or,
+               "niter": ro.niter}
+        cert = so.fixed_point_certificate(s_or, p_fast, steps=3)
+        parity = {
+            "vs_oracle_same_mode": {"abs_dHf_kcal_mol": abs(r.escf - ro.escf),
+                                    "max_abs_dP": float(np.abs(p_fast - ro.p).max()),
+                                    "max_abs_deig_eV": float(np.abs(e_fast - ro.eigs).max()),
+                                    "oracle_niter": ro.niter, "gpu_niter": r.niter,
+                                    "what": "timed GPU SCF against the oracle's complete FP64 SCF of the box in the "
+                                            "same mode (both finish to max|dP| <= 1e-7)"},
+            "fixed_point_certificate": {"max_abs_dP_bound": cert["bound"], "rho": cert["rho"], "r": cert["r"],
+                                        "max_abs_deig_eV": float(np.abs(e_fast - cert["eigs"]).max()),
+                                        "abs_dHf_at_P_kcal_mol": abs(r.escf - cert["heat_at_p"]),
+                                        "what": "three plain oracle steps from the GPU density: r_1/(1-rho) bounds "
+                                                "max|P_gpu - P*|; eigenvalues of the oracle's F(P_gpu)"}}
     if rank == 0:
         line = {
             "metric": METRIC, "value": ws * 1000.0 / t_ms, "unit": "SCF/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64" if prec == 0 else "f64+bf16x3",
             "data": "synthetic (seeded water box, random sequential insertion)",
-            "config": {"workload": WORKLOAD, "mode": args.mode, "precision": args.precision, "guess": args.guess,
-                       "converger": "pulay" if pul else "cnvg",
-                       "parallelism": f"replicas x{ws}",
-                       "l2": "flushed between steps (256 MB write); W = 151 MB > L2",
-                       "cell_edge_A": round(edge, 3)},
+            "config": bench_config(args, edge),
+            "precision": args.precision,
             "scf_wall_s": t_ms / 1000.0,
             "guess": guess_note,
             "converger": "pulay" if pul else "cnvg",
@@ -513,6 +578,7 @@ def run_mine(args):
             "learned_guess": guess_eval,
             "scf": {"escf_kcal_mol": r.escf, "niter": r.niter, "full_diag": r.n_full_diag,
                     "pseudo_diag": r.n_pseudo_diag, "split_iterations": r.n_split, "converged": r.converged,
+                    "finish_iterations": r.n_finish, "last_max_abs_dP": r.dp,
                     "abs_dHf_vs_fp64_kcal_mol": abs(r.escf - r64.escf),
                     "phase_ms": {"fock": r.t_fock_ms, "diag": r.t_diag_ms, "density_cnvg": r.t_density_ms,
                                  "other": r.t_other_ms}},
@@ -525,6 +591,7 @@ def run_mine(args):
             "roofline_fock": roof_fock,
             "kernel_ms": {k: v["total_ms"] / max(1, args.steps) for k, v in kst.items()},
             "cpu_baseline": cpu,
+            "parity_vs_oracle": parity,
             "e2e": e2e,
             "batched": batched,
         }

@@ -925,6 +925,7 @@ extern "C" int mb_eigh_ws(int n, double* fpacked, int perturb, double* c, double
   double* Y = b; b += (size_t)BT * n;
   double* bnd = part + 2048;
 
+  MB_CUDA(cudaMemsetAsync(status_dev, 0, sizeof(int), stream));
   if (n == 1) {
     MB_TRY(mb_unpack_dev(1, fpacked, A, 1, perturb, fpacked, stream));
     MB_CUDA(cudaMemcpyAsync(eigs, A, sizeof(double), cudaMemcpyDeviceToDevice, stream));

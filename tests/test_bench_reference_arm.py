@@ -24,3 +24,8 @@ def test_reference_arm_prints_one_contract_line():
     assert d["cpu_baseline"]["value"] == d["value"] and d["cpu_baseline"]["cores"] >= 1
     assert d["e2e"] == {"value": d["value"], "unit": "SCF/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
     assert d["batched"]["value"] > 0
+    # one complete oracle SCF in the GPU arm's mode, reported as equal slices
+    assert d["scf"]["converged"] and d["scf"]["niter"] > 4
+    assert abs(d["ms_per_step"] * d["steps"] / 1e3 - d["scf_wall_s"]) < 1e-6
+    assert d["plain_mode"]["niter"] > 4
+    assert d["config"]["mode"] == "fast" and d["config"]["finish_dp"] == 1e-7
