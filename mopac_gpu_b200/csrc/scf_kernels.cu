@@ -6,7 +6,11 @@
 //   pseudo-diagonalisation, diag_for_GPU.F90:116-206: Fmo = C_v^T F C_o by
 //            FP64 GEMM, tiny = 0.05 max|Fmo|, rotation coefficients and the
 //            ordered 2x2 rotation sweep over the columns of C.
+#include <cooperative_groups.h>
+
 #include "mb_common.cuh"
+
+namespace cg = cooperative_groups;
 
 namespace {
 
@@ -196,106 +200,136 @@ __global__ void absmax_kernel(long long len, const double* __restrict__ x, unsig
 
 // Rotation coefficients for every (occupied i, virtual a) pair in the
 // reference's arithmetic (diag_for_GPU.F90:176-206).  act = 0 means skipped.
+// Layout is tile-major: the 16 x 16 tile (I, J) of pairs (occupied block I,
+// virtual block J) occupies the 256 entries from (I * ntile_v + J) * 256,
+// element (u, v) at u * 16 + v; positions past nocc or nvirt hold an inactive
+// identity rotation.
 __global__ void rot_coeff_kernel(int nocc, int nvirt, const double* __restrict__ fmo,
                                  const double* __restrict__ eig, const unsigned long long* tinybits,
                                  double tiny_direct, double bigeps, double* __restrict__ alpha, double* __restrict__ beta,
                                  unsigned char* __restrict__ act, unsigned int* __restrict__ tile_cnt,
-                                 unsigned long long* __restrict__ nrot, int ntile_v) {
+                                 unsigned long long* __restrict__ nrot, int ntile_o, int ntile_v) {
   // tiny = 0.05 * max|Fmo| (diag_for_GPU.F90:151-152) unless given directly
   const double tiny = tiny_direct >= 0.0 ? tiny_direct : __longlong_as_double(*tinybits) * 0.05;
-  const long long total = (long long)nocc * nvirt;
-  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < total; q += (long long)gridDim.x * blockDim.x) {
-    const int i = (int)(q / nvirt), av = (int)(q % nvirt);
-    const double x = fmo[av + (long long)nvirt * i];
+  const long long total = (long long)ntile_o * ntile_v * (RT * RT);
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < total; p += (long long)gridDim.x * blockDim.x) {
+    const long long tile = p / (RT * RT);
+    const int e = (int)(p % (RT * RT));
+    const int I = (int)(tile / ntile_v), J = (int)(tile % ntile_v);
+    const int i = I * RT + e / RT, av = J * RT + e % RT;
     unsigned char on = 0;
     double al = 1.0, be = 0.0;
-    if (!(fabs(x) < tiny)) {
-      const double d = DSUB(eig[i], eig[nocc + av]);
-      if (!(fabs(x / d) < bigeps)) {
-        const double e = copysign(sqrt(DADD(DMUL(DMUL(4.0, x), x), DMUL(d, d))), d);
-        al = sqrt(DMUL(0.5, DADD(1.0, d / e)));
-        be = -copysign(sqrt(DSUB(1.0, DMUL(al, al))), x);
-        on = 1;
+    if (i < nocc && av < nvirt) {
+      const double x = fmo[av + (long long)nvirt * i];
+      if (!(fabs(x) < tiny)) {
+        const double d = DSUB(eig[i], eig[nocc + av]);
+        if (!(fabs(x / d) < bigeps)) {
+          const double ee = copysign(sqrt(DADD(DMUL(DMUL(4.0, x), x), DMUL(d, d))), d);
+          al = sqrt(DMUL(0.5, DADD(1.0, d / ee)));
+          be = -copysign(sqrt(DSUB(1.0, DMUL(al, al))), x);
+          on = 1;
+        }
       }
     }
-    alpha[q] = al;
-    beta[q] = be;
-    act[q] = on;
+    alpha[p] = al;
+    beta[p] = be;
+    act[p] = on;
     if (on) {
-      atomicAdd(&tile_cnt[(i / RT) * ntile_v + av / RT], 1u);
+      atomicAdd(&tile_cnt[tile], 1u);
       atomicAdd(nrot, 1ull);
     }
   }
 }
 
-// Apply all active rotations to C in the reference order, one anti-diagonal of
-// 16x16 (occupied block I, virtual block J) tiles per launch.  Tile (I, J)
-// touches columns I (occupied) and J (virtual) only; it must follow (I, J-1),
-// which last touched columns I, and (I-1, J), which last touched columns J.
-// Tiles on one anti-diagonal I + J = t touch disjoint columns, so they run in
-// parallel, and every column still sees its rotations in the sequential
-// sweep's order (occupied i outer, virtual j inner) -- rotations on disjoint
-// column pairs commute exactly, so C is bit-identical to the sequential sweep.
-// Each thread owns one row of C; a CTA covers WROWS rows of one tile.
-constexpr int WROWS = 64;
+// Apply all active rotations to C in the reference order.  Tiles are 16 x 16
+// pairs (occupied block I, virtual block J); tile (I, J) touches columns I
+// (occupied) and J (virtual) only and must follow (I, J-1), which last
+// touched columns I, and (I-1, J), which last touched columns J.  Tiles on one
+// anti-diagonal I + J = t touch disjoint columns, so they run in parallel,
+// and every column still sees its rotations in the sequential sweep's order
+// (occupied i outer, virtual j inner) -- rotations on disjoint column pairs
+// commute exactly, so C is bit-identical to the sequential sweep.
+//
+// One cooperative launch per sweep: the anti-diagonals follow each other with
+// a grid barrier between them, and within one the CTAs take (tile, block of
+// CROWS rows) items in turn.  A CTA stages the tile's 256 coefficients in
+// shared memory (every thread reads them by broadcast) and each thread
+// rotates one row of the tile's 32 columns in registers.
+constexpr int CROWS = 128;
 
-__global__ void __launch_bounds__(WROWS) rot_wave_kernel(int n, int nocc, int nvirt, double* __restrict__ c,
+__global__ void __launch_bounds__(CROWS) rot_sweep_kernel(int n, int nocc, int nvirt, double* __restrict__ c,
                                                          const double* __restrict__ alpha,
                                                          const double* __restrict__ beta,
                                                          const unsigned char* __restrict__ act,
                                                          const unsigned int* __restrict__ tile_cnt, int ntile_o,
-                                                         int ntile_v, int t) {
-  const int jlo = t - (ntile_o - 1) > 0 ? t - (ntile_o - 1) : 0;
-  const int J = jlo + blockIdx.y;
-  const int I = t - J;
-  if (J >= ntile_v || I < 0 || I >= ntile_o) return;
-  if (tile_cnt[I * ntile_v + J] == 0) return;
-  __shared__ double s_al[RT][RT], s_be[RT][RT];
-  __shared__ unsigned char s_on[RT][RT];
-  const int i0 = I * RT, j0 = J * RT;
-  for (int e = threadIdx.x; e < RT * RT; e += WROWS) {
-    const int u = e / RT, v = e % RT;
-    const bool in = (i0 + u < nocc) && (j0 + v < nvirt);
-    const long long q = (long long)(i0 + u) * nvirt + (j0 + v);
-    s_on[u][v] = in ? act[q] : 0;
-    s_al[u][v] = in ? alpha[q] : 1.0;
-    s_be[u][v] = in ? beta[q] : 0.0;
-  }
-  __syncthreads();
-  const int r = blockIdx.x * WROWS + threadIdx.x;
-  if (r >= n) return;
-  double xi[RT], xj[RT];
-#pragma unroll
-  for (int u = 0; u < RT; ++u) xi[u] = (i0 + u < nocc) ? c[(long long)(i0 + u) * n + r] : 0.0;
-#pragma unroll
-  for (int v = 0; v < RT; ++v) xj[v] = (j0 + v < nvirt) ? c[(long long)(nocc + j0 + v) * n + r] : 0.0;
-#pragma unroll
-  for (int u = 0; u < RT; ++u)
-#pragma unroll
-    for (int v = 0; v < RT; ++v) {
-      if (s_on[u][v]) {
-        const double al = s_al[u][v], be = s_be[u][v];
-        const double a = xi[u], b = xj[v];
-        xi[u] = DADD(DMUL(al, a), DMUL(be, b));
-        xj[v] = DSUB(DMUL(al, b), DMUL(be, a));
+                                                         int ntile_v) {
+  cg::grid_group grid = cg::this_grid();
+  __shared__ double2 s_ab[RT * RT];       // (alpha, beta) of the tile's pairs
+  __shared__ int s_row[RT];               // occupied column u has an active pair
+  const int nrb = (n + CROWS - 1) / CROWS;
+  for (int t = 0; t < ntile_o + ntile_v - 1; ++t) {
+    const int jlo = t - (ntile_o - 1) > 0 ? t - (ntile_o - 1) : 0;
+    const int jhi = t < ntile_v - 1 ? t : ntile_v - 1;
+    const int items = (jhi - jlo + 1) * nrb;
+    for (int it = blockIdx.x; it < items; it += gridDim.x) {
+      const int J = jlo + it / nrb, rb = it % nrb;
+      const int I = t - J;
+      if (tile_cnt[I * ntile_v + J] == 0) continue;  // the same for the whole CTA
+      const long long tbase = ((long long)I * ntile_v + J) * (RT * RT);
+      __syncthreads();  // the previous item's coefficients are no longer read
+      for (int e = threadIdx.x; e < RT * RT; e += CROWS) s_ab[e] = make_double2(alpha[tbase + e], beta[tbase + e]);
+      if (threadIdx.x < RT) {
+        const uint4 w = *reinterpret_cast<const uint4*>(act + tbase + threadIdx.x * RT);
+        s_row[threadIdx.x] = (w.x | w.y | w.z | w.w) != 0u;
       }
+      __syncthreads();
+      const int r = rb * CROWS + threadIdx.x;
+      if (r >= n) continue;
+      const int i0 = I * RT, j0 = J * RT;
+      double xi[RT], xj[RT];
+#pragma unroll
+      for (int u = 0; u < RT; ++u) xi[u] = (i0 + u < nocc) ? c[(long long)(i0 + u) * n + r] : 0.0;
+#pragma unroll
+      for (int v = 0; v < RT; ++v) xj[v] = (j0 + v < nvirt) ? c[(long long)(nocc + j0 + v) * n + r] : 0.0;
+      // A skipped pair carries the identity (alpha 1, beta 0): applying it
+      // leaves both values equal (1*a + 0*b == a), so a row of the tile runs
+      // its 16 rotations without a branch per pair.
+#pragma unroll
+      for (int u = 0; u < RT; ++u) {
+        if (!s_row[u]) continue;
+#pragma unroll
+        for (int v = 0; v < RT; ++v) {
+          const double2 ab = s_ab[u * RT + v];
+          const double a = xi[u], b = xj[v];
+          xi[u] = DADD(DMUL(ab.x, a), DMUL(ab.y, b));
+          xj[v] = DSUB(DMUL(ab.x, b), DMUL(ab.y, a));
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < RT; ++u)
+        if (i0 + u < nocc) c[(long long)(i0 + u) * n + r] = xi[u];
+#pragma unroll
+      for (int v = 0; v < RT; ++v)
+        if (j0 + v < nvirt) c[(long long)(nocc + j0 + v) * n + r] = xj[v];
     }
-#pragma unroll
-  for (int u = 0; u < RT; ++u)
-    if (i0 + u < nocc) c[(long long)(i0 + u) * n + r] = xi[u];
-#pragma unroll
-  for (int v = 0; v < RT; ++v)
-    if (j0 + v < nvirt) c[(long long)(nocc + j0 + v) * n + r] = xj[v];
+    grid.sync();
+  }
 }
 
 int launch_wavefronts(int n, int nocc, int nvirt, double* c, const double* al, const double* be,
                       const unsigned char* act, const unsigned int* tcnt, int to, int tv, cudaStream_t stream) {
-  const int diag_len = to < tv ? to : tv;
-  dim3 grid((n + WROWS - 1) / WROWS, diag_len);
-  for (int t = 0; t < to + tv - 1; ++t) {
-    rot_wave_kernel<<<grid, WROWS, 0, stream>>>(n, nocc, nvirt, c, al, be, act, tcnt, to, tv, t);
-    MB_LAUNCH_CHECK();
+  static int grid = 0;
+  if (grid == 0) {
+    int dev = 0, sms = 0, per = 0;
+    MB_CUDA(cudaGetDevice(&dev));
+    MB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    MB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, rot_sweep_kernel, CROWS, 0));
+    if (per < 1) return mb_set_error(MB_ERR_CUDA, "rot_sweep_kernel: no CTA fits on an SM");
+    grid = sms * per;
   }
+  void* args[] = {&n, &nocc, &nvirt, &c, &al, &be, &act, &tcnt, &to, &tv};
+  MB_CUDA(cudaLaunchCooperativeKernel((void*)rot_sweep_kernel, grid, CROWS, args, 0, stream));
+  mb_count_launch();
   return MB_OK;
 }
 
@@ -374,8 +408,9 @@ extern "C" int mb_unpack_dev(int n, const double* pk, double* a, int lda, int pe
 static inline size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
 
 // Workspace layout for the pseudo-diagonalisation (bytes):
-//   F full n*n | fck n*max(k,v) | fmo v*k | alpha k*v | beta k*v | act k*v |
-//   tile counts | tiny bits | nrot
+//   F full n*n | fck n*max(k,v) | fmo v*k | alpha, beta, act over the
+//   ceil(k/16) x ceil(v/16) tiles of 256 pairs (tile-major) | tile counts |
+//   tiny bits | nrot
 extern "C" size_t mb_pseudo_ws_bytes(int n, int nocc) {
   size_t v = (size_t)(n - nocc), k = (size_t)nocc;
   size_t kv = k * v;
@@ -383,8 +418,10 @@ extern "C" size_t mb_pseudo_ws_bytes(int n, int nocc) {
   size_t b = 0;
   b += align256(sizeof(double) * (size_t)n * n);
   b += align256(sizeof(double) * (size_t)n * (k > v ? k : v));
-  b += 3 * align256(sizeof(double) * kv);
-  b += align256(kv);
+  const size_t kt = to * tv * (size_t)(RT * RT);  // tile-major coefficient entries
+  b += align256(sizeof(double) * kv);
+  b += 2 * align256(sizeof(double) * kt);
+  b += align256(kt);
   b += align256(sizeof(unsigned int) * (to * tv + 64));
   b += 256;
   return b;
@@ -408,11 +445,12 @@ extern "C" int mb_pseudo_diag_ex(int n, int nocc, const double* fpacked, double*
   char* b = (char*)ws;
   double* ff = (double*)b; b += align256(sizeof(double) * (size_t)n * n);
   double* fck = (double*)b; b += align256(sizeof(double) * (size_t)n * (nocc > nvirt ? nocc : nvirt));
-  double* fmo = (double*)b; b += align256(sizeof(double) * kv);
-  double* al = (double*)b; b += align256(sizeof(double) * kv);
-  double* be = (double*)b; b += align256(sizeof(double) * kv);
-  unsigned char* act = (unsigned char*)b; b += align256(kv);
   const int to = (nocc + RT - 1) / RT, tv = (nvirt + RT - 1) / RT;
+  const size_t kt = (size_t)to * tv * (RT * RT);
+  double* fmo = (double*)b; b += align256(sizeof(double) * kv);
+  double* al = (double*)b; b += align256(sizeof(double) * kt);
+  double* be = (double*)b; b += align256(sizeof(double) * kt);
+  unsigned char* act = (unsigned char*)b; b += align256(kt);
   unsigned int* tcnt = (unsigned int*)b; b += align256(sizeof(unsigned int) * ((size_t)to * tv + 64));
   unsigned long long* tiny = (unsigned long long*)b;
   MB_TRY(mb_unpack_dev(n, fpacked, ff, n, 0, nullptr, stream));
@@ -438,7 +476,10 @@ extern "C" int mb_pseudo_diag_ex(int n, int nocc, const double* fpacked, double*
   if (blocks > 148 * 8) blocks = 148 * 8;
   absmax_kernel<<<blocks, 256, 0, stream>>>((long long)kv, fmo, tiny);
   MB_LAUNCH_CHECK();
-  rot_coeff_kernel<<<blocks, 256, 0, stream>>>(nocc, nvirt, fmo, eigs, tiny, -1.0, bigeps, al, be, act, tcnt, nrot_dev, tv);
+  int cblocks = (int)((kt + 255) / 256);
+  if (cblocks > 148 * 8) cblocks = 148 * 8;
+  rot_coeff_kernel<<<cblocks, 256, 0, stream>>>(nocc, nvirt, fmo, eigs, tiny, -1.0, bigeps, al, be, act, tcnt, nrot_dev,
+                                                 to, tv);
   MB_LAUNCH_CHECK();
   return launch_wavefronts(n, nocc, nvirt, c, al, be, act, tcnt, to, tv, stream);
 }
@@ -490,21 +531,23 @@ extern "C" int mb_rot_sweep_ws(int n, int nocc, const double* fmo, const double*
   if (nocc <= 0 || nvirt <= 0) return MB_OK;
   if (((uintptr_t)ws & 255) != 0) return mb_set_error(MB_ERR_ARG, "rotation workspace must be 256-byte aligned");
   const size_t kvs = (size_t)nocc * nvirt;
+  const int to = (nocc + RT - 1) / RT, tv = (nvirt + RT - 1) / RT;
+  const size_t kt = (size_t)to * tv * (RT * RT);
   char* b = (char*)ws;
   b += align256(sizeof(double) * (size_t)n * n);
   b += align256(sizeof(double) * (size_t)n * (nocc > nvirt ? nocc : nvirt));
   b += align256(sizeof(double) * kvs);
-  double* al = (double*)b; b += align256(sizeof(double) * kvs);
-  double* be = (double*)b; b += align256(sizeof(double) * kvs);
-  unsigned char* act = (unsigned char*)b; b += align256(kvs);
-  const int to = (nocc + RT - 1) / RT, tv = (nvirt + RT - 1) / RT;
+  double* al = (double*)b; b += align256(sizeof(double) * kt);
+  double* be = (double*)b; b += align256(sizeof(double) * kt);
+  unsigned char* act = (unsigned char*)b; b += align256(kt);
   unsigned int* tcnt = (unsigned int*)b;
   MB_CUDA(cudaMemsetAsync(tcnt, 0, sizeof(unsigned int) * (size_t)to * tv, stream));
   MB_CUDA(cudaMemsetAsync(nrot_dev, 0, sizeof(unsigned long long), stream));
   const long long kv = (long long)nocc * nvirt;
-  int blocks = (int)((kv + 255) / 256);
-  if (blocks > 148 * 8) blocks = 148 * 8;
-  rot_coeff_kernel<<<blocks, 256, 0, stream>>>(nocc, nvirt, fmo, eigs, nullptr, tiny, bigeps, al, be, act, tcnt, nrot_dev, tv);
+  int cblocks = (int)((kt + 255) / 256);
+  if (cblocks > 148 * 8) cblocks = 148 * 8;
+  rot_coeff_kernel<<<cblocks, 256, 0, stream>>>(nocc, nvirt, fmo, eigs, nullptr, tiny, bigeps, al, be, act, tcnt,
+                                                 nrot_dev, to, tv);
   MB_LAUNCH_CHECK();
   return launch_wavefronts(n, nocc, nvirt, c, al, be, act, tcnt, to, tv, stream);
 }

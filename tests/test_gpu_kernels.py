@@ -139,13 +139,15 @@ def test_eigh_packed(n):
     assert np.abs(c.T @ c - np.eye(n)).max() < 1e-10
 
 
-def test_rotation_sweep_bit_identical_through_reference_symbol():
-    """call_rot_cuda_gpu (reference signature) vs the oracle's sequential sweep."""
+@pytest.mark.parametrize("n,nocc", [(150, 53), (3072, 2048), (3400, 1700)])
+def test_rotation_sweep_bit_identical_through_reference_symbol(n, nocc):
+    """call_rot_cuda_gpu (reference signature) vs the oracle's sequential sweep;
+    n = 3072 runs the one-launch row kernel at the benchmark's size, n = 3400
+    the per-wavefront fallback (rows too long for shared memory)."""
     from mopac_gpu_b200._lib import lib
     rng = np.random.default_rng(11)
-    n, nocc = 150, 53
     nv = n - nocc
-    c = np.asfortranarray(np.linalg.qr(rng.normal(size=(n, n)))[0])
+    c = np.asfortranarray(rng.normal(size=(n, n)) / np.sqrt(n))
     eig = np.sort(rng.normal(size=n) * 10)
     fmo = np.asfortranarray(rng.normal(size=(nv, nocc)) * 0.1)
     fmo[np.abs(fmo) < 0.08] *= 1e-3  # a mix of skipped and applied rotations
