@@ -30,13 +30,17 @@ between steps anyway).  The headline metric is SCF single points per second
               complete plain-mode SCF beside it; N > 1: rank 0 only.
 --converger pulay (default in fast mode) Pulay's DIIS once newdg is set,
               like the PULAY keyword; cnvg: the default extrapolation.
---guess standard (default) the reference's diagonal guess; learned: each step
-              starts from the atom-pair network trained on liquid-density
-              boxes (prediction on the device, inside the timed region).
-              Either way the line reports under "learned_guess" the box's
-              fast-path SCF from the network and a sample of the held-out
-              (H2O)_n lattice-cluster evaluation (n = 32..128, plain FP64 path,
-              standard vs learned guess).
+--guess learned (default): each step starts from the atom-pair network
+              trained on liquid-density boxes (prediction and one McWeeny step
+              on the device, inside the timed region), entered like an OLDENS
+              density; standard: the reference's diagonal guess.  The line
+              reports under "learned_guess" the fast path from the other guess
+              and a sample of the held-out (H2O)_n lattice-cluster evaluation
+              (n = 32..128, plain FP64 path, standard vs learned guess).
+--shift N     the reference's SHIFT=N keyword for the timed SCF (default 0 in
+              fast mode: no level shift, newdg from the first small density
+              change, SCF/iter.F90:131-136; "default" keeps iter's -80).  The
+              plain FP64 reference point always runs iter's default keywords.
 --batch N     also measure the batched workload (default 4096 seeded linear
               alkanes C3-C20, one persistent launch, a CTA per molecule SCF):
               batched SCFs/s on device-resident integrals, the same through
@@ -83,7 +87,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--batch", type=int, default=4096)
-    ap.add_argument("--guess", choices=["learned", "standard"], default="standard")
+    ap.add_argument("--guess", choices=["learned", "standard"], default="learned")
+    ap.add_argument("--shift", default="0")
     ap.add_argument("--converger", choices=["pulay", "cnvg"], default="pulay")
     ap.add_argument("--guess-sample", type=int, default=40)
     return ap.parse_args()
@@ -156,14 +161,19 @@ def oracle_system(nwater: int):
     return so.make_system(nat, xyz)
 
 
-def oracle_scf(s, mode: str):
+def shift_value(args):
+    """The SHIFT=n keyword of the timed SCF, or None for iter's default."""
+    return None if (args.mode != "fast" or args.shift == "default") else float(args.shift)
+
+
+def oracle_scf(s, mode: str, shift=None):
     """One complete oracle SCF from the standard guess, timed on the host:
-    mode "fast" is the GPU arm's default algorithm (pseudo-diagonalisation
-    once newdg is set, Pulay, FP64 finish to max|dP| <= FINISH_DP), "plain"
-    a full LAPACK eigensolve every iteration with cnvg (iter's default).
-    Returns (result, seconds)."""
+    mode "fast" is the GPU arm's algorithm (pseudo-diagonalisation once newdg
+    is set, Pulay, the SHIFT keyword, FP64 finish to max|dP| <= FINISH_DP),
+    "plain" a full LAPACK eigensolve every iteration with cnvg (iter's
+    default keywords).  Returns (result, seconds)."""
     from oracle import scf_oracle as so
-    kw = dict(pseudo=True, pulay_on=True, finish_dp=FINISH_DP) if mode == "fast" else {}
+    kw = dict(pseudo=True, pulay_on=True, finish_dp=FINISH_DP, shift_kw=shift) if mode == "fast" else {}
     t0 = time.perf_counter()
     r = so.iter_scf(s, **kw)
     return r, time.perf_counter() - t0
@@ -325,8 +335,9 @@ def run_batch(args, flush, L, ws=1, rank=0, dist=None):
 def bench_config(args, edge: float) -> dict:
     """The workload description both arms print (the reference arm runs the
     same SCF algorithm on the host, in FP64 throughout)."""
-    return {"workload": WORKLOAD, "mode": args.mode, "guess": args.guess,
+    return {"workload": WORKLOAD, "mode": args.mode,
             "converger": "pulay" if (args.mode == "fast" and args.converger == "pulay") else "cnvg",
+            "shift_keyword": "default (-80)" if shift_value(args) is None else shift_value(args),
             "finish_dp": FINISH_DP if args.precision == "split" else 0.0,
             "parallelism": "replicas x1" if args.gpus == 1 else f"replicas x{args.gpus}",
             "l2": "GPU: flushed between steps (256 MB write); W = 151 MB > L2",
@@ -351,17 +362,18 @@ def run_reference(args):
     _, _, edge = workloads.water_box(args.nwater)
     s = oracle_system(args.nwater)
     warm_host(s, min(args.warmup, 2))
-    r, t_scf = oracle_scf(s, args.mode)
+    r, t_scf = oracle_scf(s, args.mode, shift_value(args))
     rp, t_plain = oracle_scf(s, "plain") if args.mode == "fast" else (r, t_scf)
     val = 1.0 / t_scf
-    mode_txt = ("pseudo-diagonalisation once newdg is set, Pulay, FP64 finish to max|dP| <= 1e-7"
-                if args.mode == "fast" else "full eigensolve every iteration, cnvg")
+    mode_txt = ("pseudo-diagonalisation once newdg is set, Pulay, SHIFT keyword as in config, FP64 finish to "
+                "max|dP| <= 1e-7, standard guess" if args.mode == "fast" else "full eigensolve every iteration, cnvg")
     line = {
         "impl": "reference", "metric": METRIC, "value": val, "unit": "SCF/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_scf * 1e3 / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded water box, random sequential insertion)",
         "config": bench_config(args, edge),
+        "guess": "standard diagonal guess (the reference has no learned guess)",
         "scf_wall_s": t_scf,
         "scf": {"escf_kcal_mol": r.escf, "niter": r.niter, "finish_iterations": r.n_finish, "converged": r.converged},
         "plain_mode": {"scf_wall_s": t_plain, "niter": rp.niter, "escf_kcal_mol": rp.escf,
@@ -404,6 +416,7 @@ def run_mine(args):
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     from mopac_gpu_b200.guess import BOX_MODEL, GuessModel
     pul = pseudo and args.converger == "pulay"
+    shift = shift_value(args)
     box_model = GuessModel(path=BOX_MODEL) if GuessModel.available(BOX_MODEL) else None
     model = box_model if args.guess == "learned" else None
     guess_note = "learned (atom-pair network trained on liquid-density boxes, prediction inside the timed step)" \
@@ -414,14 +427,17 @@ def run_mine(args):
         t0 = time.perf_counter()
         c.learned_guess(mdl)
         tp = (time.perf_counter() - t0) * 1e3
-        rr = c.run(pseudo=pseudo, precision=prec, pulay=pul, guess=True)
+        rr = c.run(pseudo=pseudo, precision=prec, pulay=pul, guess=True, shift=shift)
         return rr, tp + rr.t_total_ms, tp
+
+    def standard_step(c):
+        rr = c.run(pseudo=pseudo, precision=prec, pulay=pul, shift=shift)
+        return rr, rr.t_total_ms, 0.0
 
     def scf_step(c):
         """One step: (prediction +) SCF; returns (result, step ms, prediction ms)."""
         if model is None:
-            rr = c.run(pseudo=pseudo, precision=prec, pulay=pul)
-            return rr, rr.t_total_ms, 0.0
+            return standard_step(c)
         return learned_step(c, model)
 
     def barrier():
@@ -509,20 +525,17 @@ def run_mine(args):
     if rank == 0 and (box_model is not None or GuessModel.available()):
         guess_eval = {}
         if box_model is not None:
+            # the same fast path from the other starting density
             lm = []
             for i in range(2):
                 flush.fill_(1.0)
-                rl, tl, tpl = learned_step(ctx, box_model)
+                rl, tl, tpl = standard_step(ctx) if model is not None else learned_step(ctx, box_model)
                 lm.append(tl)
-            guess_eval["box_fast_path"] = {
+            guess_eval["standard_guess_fast_path" if model is not None else "learned_guess_fast_path"] = {
                 "scf_wall_s_incl_prediction": lm[-1] / 1000.0, "prediction_ms": tpl, "niter": rl.niter,
-                "full_diag": rl.n_full_diag, "pseudo_diag": rl.n_pseudo_diag,
+                "full_diag": rl.n_full_diag, "pseudo_diag": rl.n_pseudo_diag, "finish_iterations": rl.n_finish,
                 "abs_dHf_vs_fp64_kcal_mol": abs(rl.escf - r64.escf),
-                "model": "guess_pm7_waterbox.npy (4000 seeded (H2O)16..64 boxes at 1.0 g/cm^3)",
-                "purify_steps": 1,
-                "note": "more full eigensolves than from the standard guess: on 1536 atoms the purified "
-                        "prediction's first density change (a maximum over 3072 diagonal elements) stays above "
-                        "iter's plchek (0.005), so the level shift freezes at the -20 eV of iteration 2"}
+                "model": "guess_pm7_waterbox.npy (4000 seeded (H2O)16..64 boxes at 1.0 g/cm^3), one McWeeny step"}
         if GuessModel.available() and args.guess_sample > 0:
             from mopac_gpu_b200.guess import evaluate
             ev = evaluate(GuessModel(), n_clusters=args.guess_sample, nmin=32, nmax=128, seed=777)
@@ -545,7 +558,7 @@ def run_mine(args):
         cores = os.cpu_count()
         os.environ.setdefault("OPENBLAS_NUM_THREADS", str(cores))
         s_or = oracle_system(args.nwater)
-        ro, t_or = oracle_scf(s_or, args.mode)
+        ro, t_or = oracle_scf(s_or, args.mode, shift)
         cpu = {"value": 1.0 / t_or, "unit": "SCF/s", "cores": cores, "kind": "port",
                "sample": "one complete oracle SCF of the box in the same mode (C Fock build and rotation sweep, "
                          f"LAPACK dsyevd / BLAS on {cores} threads), timed whole", "scf_wall_s": t_or,

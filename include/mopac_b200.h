@@ -106,6 +106,10 @@ typedef struct mb_scf_opts {
                         (default): 1e-7 when precision = 1, off when
                         precision = 0; 0: off                              */
   int finish_max;    /* cap on the iterations the finish adds (default 40) */
+  double bshift;     /* -n for the SHIFT=n keyword (SCF/iter.F90:119, :131);
+                        default -80 (no keyword).  0 (SHIFT=0) turns the
+                        level shift off and lets newdg switch on as soon as
+                        the density change falls below trans (:136)       */
 } mb_scf_opts;
 
 typedef struct mb_scf_result {
@@ -187,7 +191,10 @@ int mb_helect_dev(int n, const double* p, const double* h, const double* f, doub
  * latency loops).  Scratch is a fixed 256 KiB array inside the library, so
  * n <= 16384 (larger n: MB_ERR_ARG); calls share that array and must not
  * overlap on the GPU; the first call on a device resolves the array's address
- * and should happen outside stream capture. */
+ * and should happen outside stream capture.  That address is cached per
+ * device for the life of the process: a caller that resets the device
+ * (cudaDeviceReset, which destroys the primary context) leaves the cached
+ * address stale, so it must not call this entry point afterwards. */
 int mb_helect_noalloc(int n, const double* p, const double* h, const double* f, double* out,
                       cudaStream_t stream);
 
@@ -320,7 +327,10 @@ int mb_mz_layout_destroy(MbMzLayout* layout);
  * *enuclr_dev the core-core energy over every atom pair (pairs not stored:
  * outer2's monopole in the cutof2-cutof1 band, outer1's feathered point
  * charge beyond).  nat, coord: device (atomic numbers; Angstrom).  ws:
- * mb_mz_hcore_ws_bytes(layout) bytes of device scratch. */
+ * mb_mz_hcore_ws_bytes(layout) bytes of device scratch.  Needs cutof2 >= 49
+ * (7 A squared): below PM7's feathering distance the reference's far pairs
+ * carry dipole terms this path does not form, so the call returns
+ * MB_ERR_UNSUPPORTED, as mb_mz_fock_dev does. */
 size_t mb_mz_hcore_ws_bytes(const MbMzLayout* layout);
 int mb_mz_hcore_dev(const MbMzLayout* layout, const int* nat, const double* coord, double* h, double* w,
                     double* enuclr, void* ws, cudaStream_t stream);

@@ -47,7 +47,7 @@ class ScfOpts(ctypes.Structure):
     _fields_ = [("pseudo", ctypes.c_int), ("itrmax", ctypes.c_int), ("scfcrt", ctypes.c_double),
                 ("precision", ctypes.c_int), ("switch_pl", ctypes.c_double), ("verbose", ctypes.c_int),
                 ("pulay", ctypes.c_int), ("guess", ctypes.c_int), ("finish_dp", ctypes.c_double),
-                ("finish_max", ctypes.c_int)]
+                ("finish_max", ctypes.c_int), ("bshift", ctypes.c_double)]
 
 
 class ScfRes(ctypes.Structure):

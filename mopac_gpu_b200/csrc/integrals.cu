@@ -948,6 +948,11 @@ extern "C" int mb_mz_hcore_dev(const MbMzLayout* L, const int* nat_d, const doub
                                double* enuclr_dev, void* ws, cudaStream_t stream) {
   if (!L || !nat_d || !coord_d || !h || !w || !enuclr_dev || !ws || L->numat <= 0)
     return mb_set_error(MB_ERR_ARG, "mb_mz_hcore_dev: bad args");
+  // Far pairs get the full rotated core attraction and the point-charge
+  // core-core term; that is the reference's outer2/outer1 only when every
+  // pair beyond cutof2 is past PM7's 7 A feathering (mndod.F90:800-822).
+  if (!(L->cutof2 >= 49.0))
+    return mb_set_error(MB_ERR_UNSUPPORTED, "mb_mz_hcore_dev: needs cutof2 >= 49 (7 A); shorter cutoffs feather");
   MB_TRY(upload_params());
   double* enuc_entry = (double*)ws;
   double* enuc_atom = enuc_entry + L->npairs;

@@ -20,7 +20,10 @@
 //     give wrong energies; serialise them.
 //   * The first call on each device looks up the array's device address
 //     (cudaGetSymbolAddress) with that device current and caches it; make that
-//     first call outside any stream capture.
+//     first call outside any stream capture.  The cache is never refreshed:
+//     after a cudaDeviceReset (which destroys the primary context and the
+//     array with it) the cached address is stale, so a caller that resets
+//     the device must not use this entry point again in the same process.
 #include <mutex>
 
 #include "mb_common.cuh"

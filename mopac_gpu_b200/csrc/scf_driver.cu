@@ -191,6 +191,7 @@ extern "C" void mb_scf_opts_default(mb_scf_opts* o) {
   o->guess = 0;
   o->finish_dp = -1.0;
   o->finish_max = 40;
+  o->bshift = -80.0;
 }
 
 extern "C" int mb_ctx_create(int numat, const int* nat, const double* coord, mb_ctx** out) {
@@ -545,8 +546,10 @@ extern "C" int mb_scf_run(mb_ctx* c, const mb_scf_opts* opts_in, mb_scf_result* 
 
   // ---- first-call setup (iter.F90:123-221)
   const double enrgy = PM7_FPC9;
-  double shift = 1.0, shfmax = 20.0, pl = 1.0, bshift = -80.0, ten = bshift, shfto = 0.0, shftbo = 0.0,
-         shiftb = 0.0;
+  // bshift: -80 by default, -n with SHIFT=n (iter.F90:119, :131-132)
+  const double bshift = opts.bshift;
+  double shift = 1.0, shfmax = 20.0, pl = 1.0, ten = fabs(bshift) > 1.0e-20 ? bshift : 0.0, shfto = 0.0,
+         shftbo = 0.0, shiftb = 0.0;
   const double plchek = 0.005, trans = 0.2;
   bool newdg = false, oknewd = fabs(bshift) < 0.001;
   const bool halfe = false, camkin = false;
@@ -636,6 +639,9 @@ extern "C" int mb_scf_run(mb_ctx* c, const mb_scf_opts* opts_in, mb_scf_result* 
       double hee = 0.0;
       MB_TRY(d2h(c, &hee, c->scal, 1));
       ee = hee * 2.0;
+      // a NaN or Inf in H, W or the density shows in the energy first: stop
+      // before the eigensolver sees the Fock matrix
+      if (!isfinite(ee)) return mb_set_error(MB_ERR_NUMERIC, "non-finite electronic energy (H, W or P)");
       escf = (ee + c->enuclr) * enrgy + c->atheat + scorr;
       diff = escf - eold;
       if (diff > 0) ten = ten - 1.0;

@@ -85,11 +85,13 @@ class ScfContext:
 
     def run(self, pseudo: bool = False, scfcrt: float = 1.0e-4, itrmax: int = 2000, precision: int = 0,
             switch_pl: float = 1.0e-4, verbose: bool = False, pulay: bool = False,
-            guess: bool = False, finish_dp: float = -1.0, finish_max: int = 40) -> ScfResult:
+            guess: bool = False, finish_dp: float = -1.0, finish_max: int = 40,
+            shift: float | None = None) -> ScfResult:
         """finish_dp: the FP64 finish (mb_scf_opts.finish_dp): < 0 automatic
         (1e-7 with precision=1, off with precision=0), 0 off, > 0 the bound on
         the last density update max|P_k - P_(k-1)| before convergence is
-        accepted."""
+        accepted.  shift: the SHIFT=n keyword (None: the default level shift;
+        0: no level shift, SCF/iter.F90:131-136)."""
         o = ScfOpts()
         lib().mb_scf_opts_default(ctypes.byref(o))
         o.pseudo = int(pseudo)
@@ -102,6 +104,8 @@ class ScfContext:
         o.guess = int(guess)
         o.finish_dp = float(finish_dp)
         o.finish_max = int(finish_max)
+        if shift is not None:
+            o.bshift = -float(shift)
         r = ScfRes()
         check(lib().mb_scf_run(self._h, ctypes.byref(o), ctypes.byref(r)))
         return ScfResult(r.escf, r.ee, r.niter, bool(r.converged), r.n_full_diag, r.n_pseudo_diag, r.pl,

@@ -442,13 +442,16 @@ class ScfResult:
 def iter_scf(s: System, pseudo: bool = False, scfcrt: float = 1.0e-4, itrmax: int = 2000,
              gnorm: float = 0.0, trace: bool = False, pulay_on: bool = False,
              p_guess: np.ndarray | None = None, finish_dp: float = 0.0,
-             finish_max: int = 40) -> ScfResult:
+             finish_max: int = 40, shift_kw: float | None = None) -> ScfResult:
     """Closed-shell restatement of iter (SCF/iter.F90), 1SCF settings
     (last = 1, nscf = 0, fulscf = .true.).
 
     p_guess: a starting total density (packed).  It enters like a density
     read with OLDENS (iter.F90:151-158: pa = p/2, pold = 2*pa); pold2, which
     that branch leaves as allocated, starts as the diagonal of p.
+
+    shift_kw: the SHIFT=n keyword (iter.F90:131-136): bshift = -n; SHIFT=0
+    switches the level shift off and allows newdg from the first iteration.
 
     finish_dp > 0 adds the FP64 finish of the device SCF (mb_scf_opts
     finish_dp): once iter's test (:675-690) passes, convergence is accepted
@@ -472,7 +475,7 @@ def iter_scf(s: System, pseudo: bool = False, scfcrt: float = 1.0e-4, itrmax: in
     newdg = False
     plchek = 0.005
     pl = 1.0
-    bshift = -80.0
+    bshift = -80.0 if shift_kw is None else -float(shift_kw)
     ten = bshift
     tenold = ten
     shfto = 0.0

@@ -1,19 +1,24 @@
 """Extract golden values for the PM7 SCF path from the reference's own tests.
 
-Run in a container where the reference checkout is mounted; it writes
-tests/golden/reference_values.json.  Sources (paths inside the reference):
+Usage: python tests/golden/make_golden.py <reference checkout>
+
+It writes tests/golden/reference_values.json.  Sources (paths inside the
+reference checkout):
   tests/keywords/1SCF.mop / 1SCF.out   CO2 PM7 1SCF: heat (:70), eigenvalues
                                        (:118-120), net charges (:125-127)
   tests/keywords/VECTORS.mop / .out    propane PM7 (first job): heat (:91),
                                        eigenvalues (:156-159), charges (:164-174)
   tests/mopac_api_test.F90:61-104      H2O PM7 SCF: heat, charges
+  tests/mopac_api_test.F90:379-454     the same H2O through MOZYME: heat, charges
 """
 import json
 import os
 import re
 import sys
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) != 2:
+    sys.exit("usage: python tests/golden/make_golden.py <reference checkout>")
+REF = sys.argv[1]
 SYM = {"H": 1, "C": 6, "O": 8}
 
 
@@ -66,6 +71,12 @@ heat = float(re.search(r"test_target%heat = (-?[\d.]+)d0", blk).group(1))
 charge = [float(m) for m in re.findall(r"test_target%charge\(\d\) = (-?[\d.]+)d0", blk)]
 g["h2o_api"] = dict(nat=[1, 1, 8], xyz=[coord[0:3], coord[3:6], coord[6:9]], heat=heat, charges=charge,
                     source="tests/mopac_api_test.F90:61-104")
+blk = src[src.index("subroutine test_mozyme_scf1"):src.index("end subroutine test_mozyme_scf1")]
+coord = [float(m) for m in re.findall(r"test_in%coord\(\d\) = (-?[\d.]+)d0", blk)]
+heat = float(re.search(r"test_target%heat = (-?[\d.]+)d0", blk).group(1))
+charge = [float(m) for m in re.findall(r"test_target%charge\(\d\) = (-?[\d.]+)d0", blk)]
+g["h2o_mozyme"] = dict(nat=[1, 1, 8], xyz=[coord[0:3], coord[3:6], coord[6:9]], heat=heat, charges=charge,
+                       source="tests/mopac_api_test.F90:379-454")
 json.dump(g, open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_values.json"), "w"),
           indent=1)
 print({k: len(v.get("eigs", [])) for k, v in g.items()})

@@ -72,3 +72,48 @@ def test_h2o_heat_with_dispersion_matches_reference():
     r, p, e = _gpu_run(nat, xyz, pseudo=False)
     s = oracle_system(nat, xyz)
     assert abs(r.escf + so.disp_correction(s) - case["heat"]) < 1e-4
+
+
+def test_status_codes_for_nonconvergence_and_non_finite_input():
+    """Failures made on the host: an iteration cap the SCF cannot meet gives
+    MB_ERR_NOCONV (the reference's UNABLE TO ACHIEVE SELF-CONSISTENCE); a NaN
+    planted in H gives MB_ERR_NUMERIC at the first energy, before any
+    eigensolve sees the Fock matrix; the context stays usable after both."""
+    from mopac_gpu_b200 import ScfContext
+    from mopac_gpu_b200._lib import LibraryError
+    nat, xyz = SYSTEMS["water16"]
+    s = oracle_system(nat, xyz)
+    ctx = ScfContext(nat, xyz)
+    ctx.set_hw(s.h, s.w, s.enuclr)
+    with pytest.raises(LibraryError) as e:
+        ctx.run(itrmax=3)
+    assert e.value.code == 3
+    h = s.h.copy()
+    h[5] = np.nan
+    ctx.set_hw(h, s.w, s.enuclr)
+    with pytest.raises(LibraryError) as e:
+        ctx.run()
+    assert e.value.code == 6
+    ctx.set_hw(s.h, s.w, s.enuclr)
+    r = ctx.run()
+    assert r.converged and abs(r.escf - so.iter_scf(s).escf) < 1e-4
+    ctx.close()
+
+
+@pytest.mark.parametrize("pseudo", [False, True])
+def test_shift_keyword_zero_follows_the_oracle(pseudo):
+    """SHIFT=0 (bshift = 0, SCF/iter.F90:131-136): no level shift, newdg may
+    switch on from the first iterations; the device SCF follows the oracle's
+    iter with the same keyword iteration for iteration."""
+    nat, xyz = SYSTEMS["water16"]
+    s = oracle_system(nat, xyz)
+    ref = so.iter_scf(s, pseudo=pseudo, shift_kw=0.0)
+    from mopac_gpu_b200 import ScfContext
+    ctx = ScfContext(nat, xyz)
+    ctx.set_hw(s.h, s.w, s.enuclr)
+    r = ctx.run(pseudo=pseudo, shift=0.0)
+    p = ctx.density()
+    ctx.close()
+    assert r.converged and r.niter == ref.niter
+    assert abs(r.escf - ref.escf) < 1e-6
+    np.testing.assert_allclose(p, ref.p, atol=1e-7)
