@@ -257,60 +257,105 @@ __global__ void rot_coeff_kernel(int nocc, int nvirt, const double* __restrict__
 // rotates one row of the tile's 32 columns in registers.
 constexpr int CROWS = 128;
 
-__global__ void __launch_bounds__(CROWS) rot_sweep_kernel(int n, int nocc, int nvirt, double* __restrict__ c,
-                                                         const double* __restrict__ alpha,
-                                                         const double* __restrict__ beta,
-                                                         const unsigned char* __restrict__ act,
-                                                         const unsigned int* __restrict__ tile_cnt, int ntile_o,
-                                                         int ntile_v) {
+__global__ void __launch_bounds__(CROWS, 3) rot_sweep_kernel(int n, int nocc, int nvirt, double* __restrict__ c,
+                                                            const double* __restrict__ alpha,
+                                                            const double* __restrict__ beta,
+                                                            const unsigned int* __restrict__ tile_cnt, int ntile_o,
+                                                            int ntile_v) {
   cg::grid_group grid = cg::this_grid();
-  __shared__ double2 s_ab[RT * RT];       // (alpha, beta) of the tile's pairs
-  __shared__ int s_row[RT];               // occupied column u has an active pair
+  // (alpha, beta) of a tile's 256 pairs, double-buffered: the next item's
+  // coefficients are loaded while the current item's rotations run
+  __shared__ double2 s_ab[2][RT * RT];
+  __shared__ double s_xi[RT][CROWS];   // the occupied values of each thread's row
   const int nrb = (n + CROWS - 1) / CROWS;
+  constexpr int PER = RT * RT / CROWS;  // coefficients each thread stages
   for (int t = 0; t < ntile_o + ntile_v - 1; ++t) {
     const int jlo = t - (ntile_o - 1) > 0 ? t - (ntile_o - 1) : 0;
     const int jhi = t < ntile_v - 1 ? t : ntile_v - 1;
     const int items = (jhi - jlo + 1) * nrb;
-    for (int it = blockIdx.x; it < items; it += gridDim.x) {
-      const int J = jlo + it / nrb, rb = it % nrb;
-      const int I = t - J;
-      if (tile_cnt[I * ntile_v + J] == 0) continue;  // the same for the whole CTA
-      const long long tbase = ((long long)I * ntile_v + J) * (RT * RT);
-      __syncthreads();  // the previous item's coefficients are no longer read
-      for (int e = threadIdx.x; e < RT * RT; e += CROWS) s_ab[e] = make_double2(alpha[tbase + e], beta[tbase + e]);
-      if (threadIdx.x < RT) {
-        const uint4 w = *reinterpret_cast<const uint4*>(act + tbase + threadIdx.x * RT);
-        s_row[threadIdx.x] = (w.x | w.y | w.z | w.w) != 0u;
+    // items of this anti-diagonal that carry at least one rotation; the
+    // test is the same for every thread of the CTA
+    auto next_item = [&](int it) {
+      for (; it < items; it += gridDim.x) {
+        const int J = jlo + it / nrb, I = t - J;
+        if (tile_cnt[I * ntile_v + J] != 0) break;
       }
-      __syncthreads();
-      const int r = rb * CROWS + threadIdx.x;
-      if (r >= n) continue;
-      const int i0 = I * RT, j0 = J * RT;
-      double xi[RT], xj[RT];
+      return it;
+    };
+    auto tile_base = [&](int it) {
+      const int J = jlo + it / nrb, I = t - J;
+      return ((long long)I * ntile_v + J) * (RT * RT);
+    };
+    int it = next_item(blockIdx.x);
+    int buf = 0;
+    if (it < items) {
+      const long long tb = tile_base(it);
 #pragma unroll
-      for (int u = 0; u < RT; ++u) xi[u] = (i0 + u < nocc) ? c[(long long)(i0 + u) * n + r] : 0.0;
+      for (int q = 0; q < PER; ++q) {
+        const int e = threadIdx.x + q * CROWS;
+        s_ab[0][e] = make_double2(alpha[tb + e], beta[tb + e]);
+      }
+    }
+    __syncthreads();
+    while (it < items) {
+      const int nx = next_item(it + gridDim.x);
+      double2 pre[PER];
+      if (nx < items) {
+        const long long tb = tile_base(nx);
 #pragma unroll
-      for (int v = 0; v < RT; ++v) xj[v] = (j0 + v < nvirt) ? c[(long long)(nocc + j0 + v) * n + r] : 0.0;
-      // A skipped pair carries the identity (alpha 1, beta 0): applying it
-      // leaves both values equal (1*a + 0*b == a), so a row of the tile runs
-      // its 16 rotations without a branch per pair.
-#pragma unroll
-      for (int u = 0; u < RT; ++u) {
-        if (!s_row[u]) continue;
-#pragma unroll
-        for (int v = 0; v < RT; ++v) {
-          const double2 ab = s_ab[u * RT + v];
-          const double a = xi[u], b = xj[v];
-          xi[u] = DADD(DMUL(ab.x, a), DMUL(ab.y, b));
-          xj[v] = DSUB(DMUL(ab.x, b), DMUL(ab.y, a));
+        for (int q = 0; q < PER; ++q) {
+          const int e = threadIdx.x + q * CROWS;
+          pre[q] = make_double2(alpha[tb + e], beta[tb + e]);
         }
       }
+      const int J = jlo + it / nrb, rb = it % nrb;
+      const int I = t - J;
+      const int r = rb * CROWS + threadIdx.x;
+      if (r < n) {
+        const int i0 = I * RT, j0 = J * RT;
+        const double2* ab = s_ab[buf];
+        // All 32 values of the thread's row are loaded at once (one memory
+        // latency per item): the 16 virtual ones stay in registers for the
+        // tile, the 16 occupied ones wait in shared memory, since occupied
+        // column u is touched by row u of the tile only.  A skipped pair
+        // carries the identity (alpha 1, beta 0): applying it leaves both
+        // values equal (1*a + 0*b == a), so the rotations run without a
+        // branch, each row's coefficients read from shared memory ahead of
+        // its dependent chain.
+        double xj[RT];
 #pragma unroll
-      for (int u = 0; u < RT; ++u)
-        if (i0 + u < nocc) c[(long long)(i0 + u) * n + r] = xi[u];
+        for (int u = 0; u < RT; ++u) s_xi[u][threadIdx.x] = (i0 + u < nocc) ? c[(long long)(i0 + u) * n + r] : 0.0;
 #pragma unroll
-      for (int v = 0; v < RT; ++v)
-        if (j0 + v < nvirt) c[(long long)(nocc + j0 + v) * n + r] = xj[v];
+        for (int v = 0; v < RT; ++v) xj[v] = (j0 + v < nvirt) ? c[(long long)(nocc + j0 + v) * n + r] : 0.0;
+#pragma unroll 1
+        for (int u = 0; u < RT; ++u) {
+          double x = s_xi[u][threadIdx.x];
+          double2 w[RT];
+#pragma unroll
+          for (int v = 0; v < RT; ++v) w[v] = ab[u * RT + v];
+#pragma unroll
+          for (int v = 0; v < RT; ++v) {
+            const double b = xj[v];
+            const double na = DADD(DMUL(w[v].x, x), DMUL(w[v].y, b));
+            xj[v] = DSUB(DMUL(w[v].x, b), DMUL(w[v].y, x));
+            x = na;
+          }
+          s_xi[u][threadIdx.x] = x;
+        }
+#pragma unroll
+        for (int u = 0; u < RT; ++u)
+          if (i0 + u < nocc) c[(long long)(i0 + u) * n + r] = s_xi[u][threadIdx.x];
+#pragma unroll
+        for (int v = 0; v < RT; ++v)
+          if (j0 + v < nvirt) c[(long long)(nocc + j0 + v) * n + r] = xj[v];
+      }
+      if (nx < items) {
+#pragma unroll
+        for (int q = 0; q < PER; ++q) s_ab[buf ^ 1][threadIdx.x + q * CROWS] = pre[q];
+      }
+      __syncthreads();  // the next buffer is filled; the current one is free
+      buf ^= 1;
+      it = nx;
     }
     grid.sync();
   }
@@ -327,7 +372,8 @@ int launch_wavefronts(int n, int nocc, int nvirt, double* c, const double* al, c
     if (per < 1) return mb_set_error(MB_ERR_CUDA, "rot_sweep_kernel: no CTA fits on an SM");
     grid = sms * per;
   }
-  void* args[] = {&n, &nocc, &nvirt, &c, &al, &be, &act, &tcnt, &to, &tv};
+  (void)act;  // skipped pairs carry the identity rotation in al / be
+  void* args[] = {&n, &nocc, &nvirt, &c, &al, &be, &tcnt, &to, &tv};
   MB_CUDA(cudaLaunchCooperativeKernel((void*)rot_sweep_kernel, grid, CROWS, args, 0, stream));
   mb_count_launch();
   return MB_OK;

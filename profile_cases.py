@@ -18,6 +18,8 @@ Cases (sizes of the benchmark configurations):
   density_split same with the three-product BF16 split on tcgen05
   gemm64, gemm_split   3072^3 GEMM, 2 n^3 flops
   eigh          full eigensolve n = 3072 (the SCF's Fock matrix)
+  eigh_cusolver the same matrix through torch.linalg.eigh (cuSOLVER's syevd),
+                the library bar, beside this library's eigensolver
   eigh_rand     full eigensolve of a seeded random symmetric 3072 x 3072 matrix
                 (no SCF before it: the case to run under a launch-list capture)
   pseudo_diag   Fmo + rotation sweep, n = 3072, k = 2048
@@ -164,7 +166,7 @@ def run_cases(names, reps):
     pk = peaks()
     out = []
     hbm, bf16, src = pk["hbm_gbs"], pk["bf16_tflops"], pk["source"]
-    need_c1 = any(c in names for c in ("fock2", "helect", "cnvg", "density64", "density_split", "eigh",
+    need_c1 = any(c in names for c in ("fock2", "helect", "cnvg", "density64", "density_split", "eigh", "eigh_cusolver",
                                        "pseudo_diag", "pulay"))
     c1 = C1() if need_c1 else None
     fp64 = fp64_peak_tflops() if any(c in names for c in ("density64", "gemm64", "eigh")) else None
@@ -227,6 +229,29 @@ def run_cases(names, reps):
         out.append(line("eigh", ms, 4.5 * c1.n ** 3, "TFLOP/s", "fp64", fp64, "cuBLAS DGEMM here",
                         config="n = 3072 Fock matrix of (H2O)512", note="4.5 n^3 flop convention of the "
                         "reference's gpu_bench"))
+    if "eigh_cusolver" in names:
+        # the library bar: cuSOLVER's dsyevd through torch.linalg.eigh on the
+        # same Fock matrix (unpacked, with the reference's perturbation)
+        fpk = c1.f.clone()
+        work = fpk.clone()
+        cv = torch.empty(c1.n * c1.n, dtype=torch.float64, device="cuda")
+        ev = torch.empty(c1.n, dtype=torch.float64, device="cuda")
+        nb = int(L.mb_eigh_ws_bytes(c1.n))
+        buf, ws = kernels._aligned_ws(nb, "cuda", 256)
+        st = torch.zeros(4, dtype=torch.int32, device="cuda")
+        ms_ours = timed(lambda: check(L.mb_eigh_ws(c1.n, vp(work), 1, vp(cv), vp(ev), ws, vp(st), s())),
+                        max(2, reps // 2), setup=lambda: work.copy_(fpk))
+        a = torch.zeros(c1.n, c1.n, dtype=torch.float64, device="cuda")
+        rr, cc = torch.tril_indices(c1.n, c1.n, device="cuda")
+        a[rr, cc] = fpk
+        a[cc, rr] = fpk
+        a.diagonal().add_(torch.arange(1, c1.n + 1, dtype=torch.float64, device="cuda") * 1e-10)
+        ms_lib = timed(lambda: torch.linalg.eigh(a), max(2, reps // 2))
+        w_lib = torch.linalg.eigh(a)[0]
+        out.append(line("eigh_cusolver", ms_lib, 4.5 * c1.n ** 3, "TFLOP/s", "fp64", fp64_peak_tflops(),
+                        "cuBLAS DGEMM here", config="n = 3072 Fock matrix of (H2O)512",
+                        ours_ms=ms_ours, library="torch.linalg.eigh (cuSOLVER syevd)",
+                        max_abs_eig_diff=float((w_lib - ev).abs().max().item())))
     if "eigh_rand" in names:
         n = 3072
         rng = np.random.default_rng(0)
@@ -442,7 +467,7 @@ def guess_cases(names, reps, bf16, src):
     return out
 
 
-ALL = ["fock2", "helect", "cnvg", "density64", "density_split", "gemm64", "gemm_split", "eigh", "eigh_rand",
+ALL = ["fock2", "helect", "cnvg", "density64", "density_split", "gemm64", "gemm_split", "eigh", "eigh_cusolver", "eigh_rand",
        "pseudo_diag",
        "pulay", "mz_density", "mz_helecz", "mz_cnvgz", "mz_fock", "mz_diagg1", "mz_diagg2",
        "guess_features", "guess_forward", "guess_train", "guess_predict", "batch"]
