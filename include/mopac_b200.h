@@ -137,6 +137,11 @@ void mb_scf_opts_default(mb_scf_opts* o);
  * in Angstrom (numat x 3, host).  Computes nothing yet. */
 int mb_ctx_create(int numat, const int* nat, const double* coord, mb_ctx** out);
 int mb_ctx_destroy(mb_ctx* ctx);
+/* The atomic term of the heat of formation, sum over atoms of the
+ * experimental heat of atomisation minus eisol in kcal/mol
+ * (interface/mopac_api_initialize.F90:340-350); NaN for an element outside
+ * this build.  What iter adds to (ee + enuclr) * fpc_9. */
+double mb_atheat(int numat, const int* nat);
 int mb_ctx_norbs(const mb_ctx* ctx);
 long long mb_ctx_n2elec(const mb_ctx* ctx);
 int mb_ctx_nclose(const mb_ctx* ctx);
@@ -420,6 +425,12 @@ int mb_mz_cnvgz_ws(int norbs, long long mpack, double* pnew, double* p, double* 
  * 0.1).  iorbs: device, per atom. */
 int mb_mz_check_dev(const MbMzLmos* lmos, const int* iorbs, double* norm2, double* error,
                     cudaStream_t stream);
+/* tidy's compression step (MOZYME/tidy.F90:66-107): every LMO drops the
+ * atoms whose squared coefficients sum to thresh (1e-13 in iter_for_MOZYME)
+ * or less, keeping the order of the rest, within its own storage; call
+ * mb_mz_lmos_refresh afterwards.  The reference's repacking of the storage
+ * is not restated: every LMO keeps its own space.  iorbs: device. */
+int mb_mz_tidy_dev(MbMzLmos* lmos, const int* iorbs, double thresh, cudaStream_t stream);
 /* eimp (MOZYME/eimp.F90): p's first element of every stored off-diagonal
  * block becomes the block's sum of squared f elements. */
 int mb_mz_eimp_dev(const MbMzLayout* layout, double* p, const double* f, cudaStream_t stream);
@@ -431,6 +442,40 @@ int mb_mz_eimp_dev(const MbMzLayout* layout, double* p, const double* f, cudaStr
 int mb_mz_hbonds_dev(const MbMzLayout* layout, const MbMzLmos* occ, const MbMzLmos* vir,
                      const double* f, const double* p, double cutoff, long long cap, int* ifmo,
                      double* fmo, long long* nij, cudaStream_t stream);
+
+/* The whole MOZYME SCF on the device, iter_for_MOZYME
+ * (MOZYME/iter_for_MOZYME.F90:218-630) for a closed-shell system with every
+ * atom in the SCF (no partial SCF, no setupk): from the starting LMOs occ and
+ * vir (updated in place) and the pair-block integrals (h, w from
+ * mb_mz_hcore_dev; coord device, Angstrom), per iteration tidy's
+ * compression, check, eimp,
+ * diagg1 + diagg2 + density, addhb every third iteration (four at most),
+ * cnvgz while the three-point extrapolation is on, buildf, helecz, isitsc's
+ * 1SCF test (diagg1's tiny below 5 scfcrt and |dE| below scfcrt on two
+ * consecutive iterations) and the shift control.  p and f (device, mpack)
+ * are the working density and Fock matrix and hold the last ones on return.
+ * iorbs_host: orbitals per atom (host).  MB_ERR_NOCONV after itrmax
+ * iterations.  tidy's repacking of the storage is not restated: every LMO
+ * needs spare atom slots (the space mb_mz_lmos_create leaves after it); a
+ * rotation that would overflow one is rejected. */
+typedef struct mb_mz_scf_opts {
+  double scfcrt;   /* selcon, kcal/mol (default 1e-2)                       */
+  int itrmax;      /* iteration cap (default 2000)                           */
+  long long cap;   /* capacity of the interaction lists (0: 300 norbs)       */
+  int verbose;     /* one line per iteration to stderr                       */
+} mb_mz_scf_opts;
+typedef struct mb_mz_scf_result {
+  double escf;          /* heat of formation, kcal/mol (no post-SCF terms)   */
+  double ee;            /* electronic energy, eV                             */
+  int niter, converged;
+  double t_total_ms;    /* CUDA events on the stream around the SCF          */
+  long long nrejected;  /* rotations diagg2 rejected for want of space       */
+} mb_mz_scf_result;
+void mb_mz_scf_opts_default(mb_mz_scf_opts* o);
+int mb_mz_scf_run(const MbMzLayout* layout, const int* iorbs_host, MbMzLmos* occ, MbMzLmos* vir,
+                  const double* coord, const double* w, const double* h, double enuclr, double atheat,
+                  const mb_mz_scf_opts* opts, double* p, double* f, mb_mz_scf_result* res,
+                  cudaStream_t stream);
 
 /* P (packed) = occ * C[:, 0:nocc] C[:, 0:nocc]^T, FP64. */
 int mb_density_dev(int n, int nocc, double occ, const double* c, int ldc, double* p,

@@ -43,6 +43,16 @@ class MbMzLmos(ctypes.Structure):
                 ("nentries", ctypes.c_longlong), ("ncoeff", ctypes.c_longlong)]
 
 
+class MzScfOpts(ctypes.Structure):
+    _fields_ = [("scfcrt", ctypes.c_double), ("itrmax", ctypes.c_int), ("cap", ctypes.c_longlong),
+                ("verbose", ctypes.c_int)]
+
+
+class MzScfRes(ctypes.Structure):
+    _fields_ = [("escf", ctypes.c_double), ("ee", ctypes.c_double), ("niter", ctypes.c_int),
+                ("converged", ctypes.c_int), ("t_total_ms", ctypes.c_double), ("nrejected", ctypes.c_longlong)]
+
+
 class ScfOpts(ctypes.Structure):
     _fields_ = [("pseudo", ctypes.c_int), ("itrmax", ctypes.c_int), ("scfcrt", ctypes.c_double),
                 ("precision", ctypes.c_int), ("switch_pl", ctypes.c_double), ("verbose", ctypes.c_int),
@@ -134,6 +144,11 @@ SIGNATURES = {
     "mb_mz_hcore_dev": ([ctypes.POINTER(MbMzLayout), _P, _P, _P, _P, _P, _P, _P], _I),
     "mb_mz_check_dev": ([ctypes.POINTER(MbMzLmos), _P, _P, ctypes.POINTER(_D), _P], _I),
     "mb_mz_eimp_dev": ([ctypes.POINTER(MbMzLayout), _P, _P, _P], _I),
+    "mb_mz_scf_opts_default": ([ctypes.POINTER(MzScfOpts)], None),
+    "mb_atheat": ([_I, _P], _D),
+    "mb_mz_tidy_dev": ([ctypes.POINTER(MbMzLmos), _P, _D, _P], _I),
+    "mb_mz_scf_run": ([ctypes.POINTER(MbMzLayout), _P, ctypes.POINTER(MbMzLmos), ctypes.POINTER(MbMzLmos), _P, _P,
+                       _P, _D, _D, ctypes.POINTER(MzScfOpts), _P, _P, ctypes.POINTER(MzScfRes), _P], _I),
     "mb_mz_hbonds_dev": ([ctypes.POINTER(MbMzLayout), ctypes.POINTER(MbMzLmos), ctypes.POINTER(MbMzLmos), _P, _P,
                           _D, _LL, _P, _P, ctypes.POINTER(_LL), _P], _I),
     "mb_gemm_split_ws_bytes": ([_I, _I, _I], ctypes.c_size_t),

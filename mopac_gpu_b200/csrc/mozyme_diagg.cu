@@ -21,7 +21,7 @@
 
 namespace {
 
-constexpr int MZ_MAXA = 256;  // atoms per virtual LMO handled by one CTA
+constexpr int MZ_MAXA = 512;  // atoms per virtual LMO handled by one CTA
 constexpr int MZ_T = 128;
 
 __device__ long long pair_offset(const MbMzLayout& L, int a, int b) {
@@ -437,7 +437,7 @@ extern "C" int mb_mz_diagg1_dev(const MbMzLayout* L, const MbMzLmos* occ, const 
   MB_CUDA(cudaMemcpyAsync(&tb, tiny_bits, sizeof(tb), cudaMemcpyDeviceToHost, stream));
   MB_CUDA(cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, stream));
   MB_CUDA(cudaStreamSynchronize(stream));
-  if (herr) return mb_set_error(MB_ERR_UNSUPPORTED, "mb_mz_diagg1_dev: a virtual LMO covers more than 256 atoms");
+  if (herr) return mb_set_error(MB_ERR_UNSUPPORTED, "mb_mz_diagg1_dev: a virtual LMO covers more than 512 atoms");
   double st = 0.0;
   for (int i = 0; i < nvir; ++i) st += sp[i];
   *sumt = st;
@@ -496,6 +496,40 @@ __device__ __forceinline__ int find_atom(const int* ic, int nn, int cnt, const i
   return -1;
 }
 
+// Atom -> coefficient offset of one LMO's atoms (the first cnt of its list),
+// open addressing in thread-local memory, so each test "is atom a in this
+// LMO" is a few probes instead of a scan of the list.  Built in list order, so
+// a repeated atom resolves to its first slot, as the scan does.  At most half
+// full, so every probe sequence ends; LMOs past that size use the scan.
+constexpr int AMAP = 1024;
+struct AtomMap {
+  int key[AMAP];
+  int val[AMAP];
+  bool ok;
+  __device__ void build(const int* ic, int nn, int cnt, const int* iorbs) {
+    ok = cnt <= AMAP / 2;
+    if (!ok) return;
+    for (int q = 0; q < AMAP; ++q) key[q] = -1;
+    int off = 0;
+    for (int t = nn; t < nn + cnt; ++t) {
+      const int b = ic[t] - 1;
+      unsigned h = ((unsigned)b * 2654435761u) & (AMAP - 1);
+      while (key[h] >= 0) h = (h + 1) & (AMAP - 1);
+      key[h] = b;
+      val[h] = off;
+      off += iorbs[b];
+    }
+  }
+  __device__ int find(int a) const {
+    unsigned h = ((unsigned)a * 2654435761u) & (AMAP - 1);
+    while (key[h] >= 0) {
+      if (key[h] == a) return val[h];
+      h = (h + 1) & (AMAP - 1);
+    }
+    return -1;
+  }
+};
+
 // One thread per rotation of the level.  Whether a rotation is rejected
 // depends only on coefficients it has not yet touched (those of atoms in one
 // LMO only), so a dry run decides it first; modifying and then restoring, as
@@ -533,6 +567,11 @@ __global__ void mzd2_level(D2Args A) {
   jur = jlr + A.norbs - 1 < jur ? jlr + A.norbs - 1 : jur;
   iur = ilr + A.norbs - 1 < iur ? ilr + A.norbs - 1 : iur;
   const int ncf0 = ncf[j], nce0 = nce[i];
+  AtomMap mj, mi;
+  mj.build(icocc, nncf[j], ncf0, A.iorbs);
+  mi.build(icvir, nnce[i], nce0, A.iorbs);
+  auto findj = [&](int a) { return mj.ok ? mj.find(a) : find_atom(icocc, nncf[j], ncf0, A.iorbs, a); };
+  auto findi = [&](int a) { return mi.ok ? mi.find(a) : find_atom(icvir, nnce[i], nce0, A.iorbs, a); };
   const double ee = copysign(sqrt(DADD(DMUL(DMUL(4.0, c), c), DMUL(d, d))), d);
   double alpha = sqrt(DMUL(0.5, DADD(1.0, d / ee)));
   for (;;) {
@@ -546,7 +585,7 @@ __global__ void mzd2_level(D2Args A) {
     for (int le = nnce[i]; le < nnce[i] + nce0; ++le) {
       const int mie = icvir[le] - 1;
       const int no = A.iorbs[mie];
-      if (find_atom(icocc, nncf[j], ncf0, A.iorbs, mie) < 0) {
+      if (findj(mie) < 0) {
         double sum = 0.0;
         for (int k = 0; k < no; ++k) {
           const double t = DMUL(beta, cvir[loopi + mle + k]);
@@ -567,7 +606,7 @@ __global__ void mzd2_level(D2Args A) {
       for (int lf = nncf[j]; lf < nncf[j] + ncf0; ++lf) {
         const int ii = icocc[lf] - 1;
         const int no = A.iorbs[ii];
-        if (find_atom(icvir, nnce[i], nce0, A.iorbs, ii) < 0) {
+        if (findi(ii) < 0) {
           double sum = 0.0;
           for (int k = 0; k < no; ++k) {
             const double t = DMUL(beta, cocc[loopj + off + k]);
@@ -595,7 +634,7 @@ __global__ void mzd2_level(D2Args A) {
     for (int le = nnce[i]; le < nnce[i] + nce0; ++le) {
       const int mie = icvir[le] - 1;
       const int no = A.iorbs[mie];
-      const int uj = find_atom(icocc, nncf[j], ncf0, A.iorbs, mie);
+      const int uj = findj(mie);
       if (uj >= 0) {
         for (int k = 0; k < no; ++k) {
           const long long pj = loopj + uj + k, pi = loopi + mle + k;
@@ -627,7 +666,7 @@ __global__ void mzd2_level(D2Args A) {
     for (int lf = nncf[j]; lf < nncf[j] + ncf0; ++lf) {
       const int ii = icocc[lf] - 1;
       const int no = A.iorbs[ii];
-      if (find_atom(icvir, nnce[i], nce0, A.iorbs, ii) < 0) {
+      if (findi(ii) < 0) {
         double sum = 0.0;
         for (int k = 0; k < no; ++k) {
           const double t = DMUL(beta, cocc[loopj + off + k]);

@@ -273,6 +273,20 @@ extern "C" int mb_ctx_create(int numat, const int* nat, const double* coord, mb_
   return MB_OK;
 }
 
+extern "C" double mb_atheat(int numat, const int* nat) {
+  static Pm7Params P;
+  static bool pinit = false;
+  if (!pinit) { pm7_init(&P); pinit = true; }
+  if (numat <= 0 || !nat) return 0.0;
+  double atheat = 0.0, eat = 0.0;
+  for (int a = 0; a < numat; ++a) {
+    if (!pm7_supported(nat[a])) return NAN;
+    atheat += P.el[nat[a]].eheat;
+    eat += P.el[nat[a]].eisol;
+  }
+  return atheat - eat * PM7_FPC9;
+}
+
 extern "C" int mb_ctx_destroy(mb_ctx* c) {
   if (c) {
     cudaStreamSynchronize(c->stream);

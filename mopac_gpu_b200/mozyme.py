@@ -12,7 +12,7 @@ import ctypes
 import numpy as np
 import torch
 
-from ._lib import MbMzLayout, MbMzLmos, check, lib
+from ._lib import MbMzLayout, MbMzLmos, MzScfOpts, MzScfRes, check, lib
 
 
 def _stream():
@@ -212,7 +212,8 @@ def iter_for_mozyme(layout: Layout, occ: Lmos, vir: Lmos, coord, w, h, enuclr: f
                     scfcrt: float = 1.0e-2, itrmax: int = 2000, cap: int | None = None, trace: bool = False):
     """The MOZYME SCF loop (MOZYME/iter_for_MOZYME.F90:218-630) for a whole
     closed-shell system on the device: density, Fock and energy of the
-    starting LMOs, then per iteration check, eimp, diagg (diagg1 + diagg2 +
+    starting LMOs, then per iteration tidy's compression, check, eimp, diagg
+    (diagg1 + diagg2 +
     density), addhb every third iteration while fewer than four were made,
     cnvgz while the three-point extrapolation is on, buildf, helecz, isitsc's
     1SCF test and the shift control.  coord (numat x 3), w (the stored pairs'
@@ -242,6 +243,11 @@ def iter_for_mozyme(layout: Layout, occ: Lmos, vir: Lmos, coord, w, h, enuclr: f
     use3, scf1, converged = True, False, False
     history = []
     while True:
+        # tidy's compression step (iter_for_MOZYME.F90:221, :326)
+        check(L.mb_mz_tidy_dev(ctypes.byref(occ.s), layout.s.iorbs, thresh, _stream()))
+        check(L.mb_mz_tidy_dev(ctypes.byref(vir.s), layout.s.iorbs, thresh, _stream()))
+        occ.refresh()
+        vir.refresh()
         eo, ev = ctypes.c_double(), ctypes.c_double()
         check(L.mb_mz_check_dev(ctypes.byref(occ.s), layout.s.iorbs, _ptr(norm_o), ctypes.byref(eo), _stream()))
         check(L.mb_mz_check_dev(ctypes.byref(vir.s), layout.s.iorbs, _ptr(norm_v), ctypes.byref(ev), _stream()))
@@ -295,3 +301,132 @@ def iter_for_mozyme(layout: Layout, occ: Lmos, vir: Lmos, coord, w, h, enuclr: f
             shift += 2.0
             lstart = niter
     return dict(escf=escf, ee=ee, niter=niter, converged=converged, history=history, p=p, f=f)
+
+
+def scf_run(layout: Layout, occ: Lmos, vir: Lmos, coord, w, h, enuclr: float, atheat: float,
+            scfcrt: float = 1.0e-2, itrmax: int = 2000, cap: int | None = None, verbose: bool = False):
+    """The MOZYME SCF behind its C entry (mb_mz_scf_run): the loop of
+    ``iter_for_mozyme`` run by the library.  Returns a dict: escf, ee, niter,
+    converged, t_total_ms, nrejected, p, f."""
+    o = MzScfOpts()
+    lib().mb_mz_scf_opts_default(ctypes.byref(o))
+    o.scfcrt = float(scfcrt)
+    o.itrmax = int(itrmax)
+    o.cap = int(cap or 0)
+    o.verbose = int(verbose)
+    p = torch.empty(layout.mpack, dtype=torch.float64, device="cuda")
+    f = torch.empty(layout.mpack, dtype=torch.float64, device="cuda")
+    r = MzScfRes()
+    check(lib().mb_mz_scf_run(ctypes.byref(layout.s), layout.iorbs.ctypes.data, ctypes.byref(occ.s),
+                              ctypes.byref(vir.s), _ptr(coord.contiguous()), _ptr(w), _ptr(h), float(enuclr),
+                              float(atheat), ctypes.byref(o), _ptr(p), _ptr(f), ctypes.byref(r), _stream()))
+    return dict(escf=r.escf, ee=r.ee, niter=r.niter, converged=bool(r.converged), t_total_ms=r.t_total_ms,
+                nrejected=r.nrejected, p=p, f=f)
+
+
+# ------------------------------------------------------------ starting LMOs
+def _pipek_mezey(C: np.ndarray, atom_of: np.ndarray, natoms: int, sweeps: int = 200) -> np.ndarray:
+    """Pipek-Mezey localisation of the columns of C (orthonormal NDDO AO
+    basis): 2x2 Jacobi rotations that maximise the sum over orbitals and
+    atoms of the squared atomic populations."""
+    C = C.copy()
+    n = C.shape[1]
+    masks = [atom_of == a for a in range(natoms)]
+    for _ in range(sweeps):
+        largest = 0.0
+        for i in range(n):
+            for j in range(i + 1, n):
+                A = B = 0.0
+                for m in masks:
+                    pii, pjj, pij = float(C[m, i] @ C[m, i]), float(C[m, j] @ C[m, j]), float(C[m, i] @ C[m, j])
+                    A += pij * pij - 0.25 * (pii - pjj) ** 2
+                    B += pij * (pii - pjj)
+                if A * A + B * B < 1.0e-24:
+                    continue
+                g = 0.25 * np.arccos(-A / np.hypot(A, B)) * (1.0 if B >= 0.0 else -1.0)
+                c, s = np.cos(g), np.sin(g)
+                ci, cj = C[:, i].copy(), C[:, j].copy()
+                C[:, i] = c * ci + s * cj
+                C[:, j] = -s * ci + c * cj
+                largest = max(largest, abs(g))
+        if largest < 1.0e-12:
+            break
+    return C
+
+
+def _water_frame_axes(o, h1, h2) -> np.ndarray:
+    """Orthonormal axes (columns) of a water molecule: the HOH bisector, the
+    H1-H2 direction, their cross product."""
+    e1 = (h1 - o) + (h2 - o)
+    e1 /= np.linalg.norm(e1)
+    e2 = h1 - h2
+    e2 -= (e2 @ e1) * e1
+    e2 /= np.linalg.norm(e2)
+    return np.stack([e1, e2, np.cross(e1, e2)], axis=1)
+
+
+def water_lmos(nat, xyz, pad_atoms: int = 0, scfcrt: float = 1.0e-8):
+    """Starting LMOs for (H2O)_n, atoms given as O, H, H per molecule: the work
+    makvec (MOZYME/makvec.F90:16-143) does from a Lewis structure, done here
+    from the isolated molecule -- two O-H bonds and two lone pairs occupied,
+    two O-H antibonds virtual -- as the SCF orbitals of one water (this
+    library's dense SCF on the GPU), Pipek-Mezey localised, then carried into
+    every molecule's orientation (s coefficients unchanged, p coefficients
+    rotated with the molecule).  The molecules must share one rigid internal
+    geometry (checked to 1e-8 A).  Each LMO lists its atoms by falling weight
+    (its bond's atoms first, as hbonds expects) and is followed by pad_atoms
+    spare atom slots for diagg2 to grow it.  Returns (iorbs, occ, vir) in the
+    reference's arrays (ncf, nncf, icocc, ncocc, cocc)."""
+    from .scf import ScfContext
+    nat = np.asarray(nat)
+    xyz = np.asarray(xyz, float).reshape(-1, 3)
+    nmol = len(nat) // 3
+    if len(nat) != 3 * nmol or np.any(nat[0::3] != 8) or np.any(nat[1::3] != 1) or np.any(nat[2::3] != 1):
+        raise ValueError("water_lmos: atoms must come as O, H, H per molecule")
+    o, h1, h2 = xyz[0::3], xyz[1::3], xyz[2::3]
+    geo = np.stack([np.linalg.norm(h1 - o, axis=1), np.linalg.norm(h2 - o, axis=1),
+                    np.linalg.norm(h1 - h2, axis=1)], axis=1)
+    if np.abs(geo - geo[0]).max() > 1.0e-8:
+        raise ValueError("water_lmos: the molecules do not share one rigid geometry")
+    ctx = ScfContext(nat[:3], xyz[:3])
+    ctx.hcore()
+    ctx.run(pseudo=False, scfcrt=scfcrt, finish_dp=1.0e-10, finish_max=200)
+    c, _ = ctx.vectors()
+    ctx.close()
+    atom_of = np.array([0, 0, 0, 0, 1, 2])
+    loc = [_pipek_mezey(c[:, :4], atom_of, 3), _pipek_mezey(c[:, 4:6], atom_of, 3)]
+    R0 = _water_frame_axes(o[0], h1[0], h2[0])
+    # per LMO: the atoms in falling weight (the same in every molecule)
+    orders = []
+    for C in loc:
+        orders.append([np.argsort(-np.array([np.sum(C[:4, k] ** 2), C[4, k] ** 2, C[5, k] ** 2]), kind="stable")
+                       for k in range(C.shape[1])])
+    iorbs = np.where(nat == 1, 1, 4).astype(np.int32)
+    out = []
+    for C, order in zip(loc, orders):
+        nl = C.shape[1]
+        per_icocc = 3 + pad_atoms
+        per_cocc = 6 + 4 * pad_atoms
+        ncf = np.full(nmol * nl, 3, np.int32)
+        nncf = (np.arange(nmol * nl) * per_icocc).astype(np.int32)
+        ncocc = (np.arange(nmol * nl) * per_cocc).astype(np.int32)
+        icocc = np.zeros(nmol * nl * per_icocc, np.int32)
+        cocc = np.zeros(nmol * nl * per_cocc)
+        # p coefficients in the molecule frame, then into each molecule's axes
+        q = np.einsum("ji,jk->ik", R0, C[1:4, :])              # (3, nl): frame components
+        Rm = np.stack([_water_frame_axes(o[m], h1[m], h2[m]) for m in range(nmol)])  # (nmol, 3, 3)
+        pm = np.einsum("mij,jk->mik", Rm, q)                    # (nmol, 3, nl)
+        for k in range(nl):
+            for m in range(nmol):
+                lm = m * nl + k
+                ia, ic = nncf[lm], ncocc[lm]
+                for slot, a in enumerate(order[k]):
+                    icocc[ia + slot] = 3 * m + a + 1
+                    if a == 0:
+                        cocc[ic:ic + 4] = [C[0, k], pm[m, 0, k], pm[m, 1, k], pm[m, 2, k]]
+                        ic += 4
+                    else:
+                        cocc[ic] = C[3 + a, k]
+                        ic += 1
+        out.append((ncf, nncf, icocc, ncocc, cocc))
+    return iorbs, out[0], out[1]

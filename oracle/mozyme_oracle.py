@@ -234,6 +234,32 @@ def check_lmos(lmos, iorbs) -> float:
     return err
 
 
+def tidy(lmos, iorbs, thresh: float = 1.0e-13) -> None:
+    """The compression step of tidy (MOZYME/tidy.F90:66-107): every LMO drops
+    the atoms whose squared coefficients sum to thresh or less, keeping the
+    order of the rest, in place within its own storage.  (The reference then
+    repacks all LMOs and spreads the free space evenly, :133-213; here every
+    LMO keeps its own fixed space, so only the counts and contents change.)"""
+    ncf, nncf, icocc, ncocc, cocc = lmos
+    for i in range(len(ncf)):
+        mm = ncocc[i]
+        mn = ncocc[i]
+        kept = 0
+        for j1 in range(ncf[i]):
+            a = icocc[nncf[i] + j1]
+            no = int(iorbs[a - 1])
+            ssum = 0.0
+            for k in range(no):
+                ssum += float(cocc[mm + k]) ** 2
+            if ssum > thresh:
+                cocc[mn:mn + no] = cocc[mm:mm + no].copy()
+                icocc[nncf[i] + kept] = a
+                mn += no
+                kept += 1
+            mm += no
+        ncf[i] = kept
+
+
 def eimp(iorbs, nijbo, p, f) -> None:
     """eimp (MOZYME/eimp.F90): the first element of every stored
     off-diagonal block of p becomes that block's sum of squared F elements,
@@ -373,8 +399,10 @@ def iter_for_mozyme(s, occ, vir, cutof1: float, cutof2: float, scfcrt: float = 1
     test (isitsc.F90:34-44: ovmax below 5 selcon and |dE| below selcon on
     two consecutive iterations; ovmax is diagg1's tiny, diagg1.F90:648), and
     the shift control (:615-628).  selcon = scfcrt (scfcri's default 1e-2).
-    Not restated: tidy (storage compaction; the LMOs carry their own spare
-    slots), PLS_faulty's restart, COSMO.  occ and vir are updated in place.
+    tidy's compression step (atoms with negligible coefficients dropped)
+    runs at the top of every iteration (:221, :326); not restated: tidy's
+    repacking of the storage (the LMOs carry their own spare slots),
+    PLS_faulty's restart, COSMO.  occ and vir are updated in place.
     Returns a dict: escf, ee, niter, converged, history."""
     iorbs = (s.nlast - s.nfirst + 1).astype(np.int32)
     mpack, nijbo = layout(iorbs, s.coord, cutof1, cutof2)
@@ -402,6 +430,8 @@ def iter_for_mozyme(s, occ, vir, cutof1: float, cutof2: float, scfcrt: float = 1
     use3, scf1, converged = True, False, False
     history = []
     while True:
+        tidy(occ, iorbs, thresh)                      # iter_for_MOZYME.F90:221, :326
+        tidy(vir, iorbs, thresh)
         if check_lmos(occ, iorbs) > 0.1 or check_lmos(vir, iorbs) > 0.1:
             raise RuntimeError("ERROR DETECTED IN SUBROUTINE CHECK")
         eimp(iorbs, nijbo, p, f)
