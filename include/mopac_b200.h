@@ -680,6 +680,37 @@ void eigenvectors_lapack_(double* eigenvecs, double* xmat, double* eigvals, cons
 void diag_for_gpu_(const double* fao, double* vector, const int* nocc, const double* eig,
                    const int* norbs, const int* mpack);
 
+/* MOZYME's routines read module MOZYME_C and common_arrays_C, which a C
+ * library cannot see; the host registers them (by reference, Fortran-style),
+ * then calls the shims with the reference's argument lists.  Each call stages
+ * the registered host arrays through the device kernels and writes the
+ * results back into them. */
+/* After fillij and hcore_for_MOZYME: the atoms (iorbs, coord in Angstrom),
+ * fillij's cutoffs (squared), H in pair blocks (mpack) and the stored pairs'
+ * two-electron integrals (nw, the layout's order). */
+int mb_mz_bind_system_(const int* numat, const int* iorbs, const double* coord, const double* cutof1,
+                       const double* cutof2, const double* h, const double* w, const long long* nw);
+/* Whenever the LMO arrays are (re)allocated or repacked: MOZYME_C's ncf,
+ * nncf, icocc, ncocc, cocc and nce, nnce, icvir, ncvir, cvir with their
+ * dimensions, common_arrays_C's p and eigs, and fmo_dim.  The pointers are
+ * kept and read / written by the shims. */
+int mb_mz_bind_lmos_(const int* nocc, int* ncf, int* nncf, int* icocc, int* ncocc, double* cocc,
+                     const long long* icocc_dim, const long long* cocc_dim, const int* nvir, int* nce,
+                     int* nnce, int* icvir, int* ncvir, double* cvir, const long long* icvir_dim,
+                     const long long* cvir_dim, double* p, double* eigs, const long long* fmo_dim);
+/* MOZYME_C's shift and thresh, read at every diagg_ call. */
+int mb_mz_bind_controls_(const double* shift, const double* thresh);
+/* density_for_MOZYME(p, mode, nclose_loc, partp), MOZYME/density_for_MOZYME.F90:16 */
+void density_for_mozyme_(double* p, const int* mode, const int* nclose_loc, const double* partp);
+/* buildf(f, partf, mode), MOZYME/buildf.F90:16; P is the registered p; mode 0
+ * (whole F) only, other modes report MB_ERR_UNSUPPORTED */
+void buildf_(double* f, const double* partf, const int* mode);
+/* diagg(fao, nocc, nvir, idiagg, partp, indi), MOZYME/diagg.F90: diagg1,
+ * diagg2 and density_for_MOZYME(p, indi, nocc, partp); diagg1's and diagg2's
+ * saved state is kept by the library between calls */
+void diagg_(const double* fao, const int* nocc, const int* nvir, const int* idiagg, double* partp,
+            const int* indi);
+
 #ifdef __cplusplus
 }
 #endif

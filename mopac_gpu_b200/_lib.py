@@ -182,6 +182,12 @@ SIGNATURES = {
     "density_for_gpu_": ([_P] * 10, None),
     "eigenvectors_lapack_": ([_P] * 4, None),
     "diag_for_gpu_": ([_P] * 6, None),
+    "mb_mz_bind_system_": ([_P] * 8, _I),
+    "mb_mz_bind_lmos_": ([_P] * 19, _I),
+    "mb_mz_bind_controls_": ([_P, _P], _I),
+    "density_for_mozyme_": ([_P] * 4, None),
+    "buildf_": ([_P] * 3, None),
+    "diagg_": ([_P] * 6, None),
     "mb_ctx_set_guess": ([_P, _P], _I),
     "mb_den_write": ([ctypes.c_char_p, _I, _I, _P, _I], _I),
     "mb_den_read": ([ctypes.c_char_p, _I, _I, _P, ctypes.POINTER(_I)], _I),

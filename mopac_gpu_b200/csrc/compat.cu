@@ -271,9 +271,12 @@ extern "C" void set_mozyme_gpu_pair(int dev0, int dev1) { (void)dev0; (void)dev1
 extern "C" void create_handle(void) {}
 extern "C" void destroy_handle(void) {}
 
+void mz_release_bound();  // the MOZYME shims' registered system (below)
+
 extern "C" void mopac_cuda_destroy_resources(void) {
   std::lock_guard<std::mutex> lk(g_mu);
   g_a.release(); g_b.release(); g_c.release(); g_d.release(); g_ws.release();
+  mz_release_bound();
   if (g_stream) { cudaStreamDestroy(g_stream); g_stream = nullptr; }
 }
 
@@ -468,4 +471,257 @@ extern "C" void pulay_(double* f, const double* p, const int* n, double* fppf, d
     rc = MB_ERR_CUDA;
   if (rc == MB_OK && cudaStreamSynchronize(g_stream) != cudaSuccess) rc = MB_ERR_CUDA;
   report(rc, "pulay_");
+}
+
+// ====================================================== (2) MOZYME shims
+// The reference's MOZYME routines read their LMOs and storage tables from
+// module MOZYME_C and common_arrays_C.  A C library cannot see Fortran
+// module variables, so the host registers them once (mb_mz_bind_system_ after
+// fillij / hcore_for_MOZYME, mb_mz_bind_lmos_ whenever the arrays are
+// (re)allocated, e.g. after tidy repacks them) and the three shims then take
+// the reference's own argument lists.  Every call stages the registered host
+// arrays through the device kernels and writes the results back to them, as
+// the reference's own GPU layer stages its matrices: the host arrays stay the
+// truth between calls.
+extern "C" int mb_mz_layout_create(int numat, const int* iorbs, const double* coord, double cutof1, double cutof2,
+                                   MbMzLayout* out, long long* nijbo);
+extern "C" int mb_mz_layout_destroy(MbMzLayout* layout);
+extern "C" int mb_mz_lmos_create(int numat, const int* iorbs, int nlmo, const int* ncf, const int* nncf,
+                                 const int* icocc, const int* ncocc, const double* cocc, long long icocc_dim,
+                                 long long cocc_dim, MbMzLmos* out);
+extern "C" int mb_mz_lmos_refresh(int numat, const int* iorbs_host, MbMzLmos* lmos);
+extern "C" int mb_mz_lmos_destroy(MbMzLmos* lmos);
+extern "C" int mb_mz_density_dev(const MbMzLayout* layout, const MbMzLmos* lmos, int mode, const double* partp,
+                                 double* p, cudaStream_t stream);
+extern "C" size_t mb_mz_fock_ws_bytes(const MbMzLayout* layout);
+extern "C" int mb_mz_fock_dev(const MbMzLayout* layout, const double* coord, const double* w, const double* ptot,
+                              const double* h, double* f, void* ws, cudaStream_t stream);
+extern "C" size_t mb_mz_diagg1_ws_bytes(const MbMzLayout* layout, const MbMzLmos* occ, const MbMzLmos* vir);
+extern "C" int mb_mz_diagg1_dev(const MbMzLayout* layout, const MbMzLmos* occ, const MbMzLmos* vir, const double* fao,
+                                const double* p, int idiagg, double* state, int* nfmo, int* ifmo, double* fmo,
+                                long long* nij, double* eigv, double* eigs, int* eigs_done, double* sumt, void* ws,
+                                cudaStream_t stream);
+extern "C" int mb_mz_diagg2_dev(const MbMzLayout* layout, MbMzLmos* occ, MbMzLmos* vir, const int* ifmo,
+                                const double* fmo, long long nij, const double* eigs, const double* eigv, int idiagg,
+                                const double* ctl, int* nrejct, double* sumb, long long* nrej, cudaStream_t stream);
+
+namespace {
+struct MzBound {
+  bool have_system = false, have_lmos = false;
+  int numat = 0, norbs = 0;
+  long long mpack = 0, nw = 0;
+  std::vector<int> iorbs;
+  MbMzLayout L{};
+  double *coord = nullptr, *h = nullptr, *w = nullptr;  // device copies
+  // host arrays of MOZYME_C / common_arrays_C (the caller's, not copied)
+  int nocc = 0, nvir = 0;
+  int *ncf = nullptr, *nncf = nullptr, *icocc = nullptr, *ncocc = nullptr;
+  int *nce = nullptr, *nnce = nullptr, *icvir = nullptr, *ncvir = nullptr;
+  double *cocc = nullptr, *cvir = nullptr, *p = nullptr, *eigs = nullptr;
+  long long icocc_dim = 0, cocc_dim = 0, icvir_dim = 0, cvir_dim = 0;
+  double thresh = 1.0e-13, cst = 1.0;
+  const double* shift = nullptr;         // MOZYME_C's shift, read at every diagg
+  const double* thresh_p = nullptr;      // MOZYME_C's thresh
+  // diagg1's and diagg2's saved variables (the Fortran save state)
+  double state[4] = {10.0, 1.0, 0.0, 0.0};
+  int nrejct[2] = {0, 0};
+  long long cap = 0;
+  Buf nfmo, ifmo, fmo;
+};
+MzBound g_mz;
+
+void mz_release_system() {
+  if (g_mz.have_system) mb_mz_layout_destroy(&g_mz.L);
+  cudaFree(g_mz.coord);
+  cudaFree(g_mz.h);
+  cudaFree(g_mz.w);
+  g_mz.coord = g_mz.h = g_mz.w = nullptr;
+  g_mz.have_system = false;
+}
+
+}  // namespace
+
+void mz_release_bound() {
+  mz_release_system();
+  g_mz.nfmo.release();
+  g_mz.ifmo.release();
+  g_mz.fmo.release();
+  g_mz.have_lmos = false;
+}
+
+namespace {
+int mz_upload(double** dst, const double* src, size_t count) {
+  MB_CUDA(cudaMalloc(dst, sizeof(double) * (count > 0 ? count : 1)));
+  if (count) MB_CUDA(cudaMemcpy(*dst, src, sizeof(double) * count, cudaMemcpyHostToDevice));
+  return MB_OK;
+}
+
+// device copies of the registered LMOs (occupied first nocc_use of them)
+int mz_lmos(int nocc_use, MbMzLmos* occ, MbMzLmos* vir) {
+  MB_TRY(mb_mz_lmos_create(g_mz.numat, g_mz.iorbs.data(), nocc_use, g_mz.ncf, g_mz.nncf, g_mz.icocc, g_mz.ncocc,
+                           g_mz.cocc, g_mz.icocc_dim, g_mz.cocc_dim, occ));
+  if (vir) {
+    int rc = mb_mz_lmos_create(g_mz.numat, g_mz.iorbs.data(), g_mz.nvir, g_mz.nce, g_mz.nnce, g_mz.icvir, g_mz.ncvir,
+                               g_mz.cvir, g_mz.icvir_dim, g_mz.cvir_dim, vir);
+    if (rc != MB_OK) { mb_mz_lmos_destroy(occ); return rc; }
+  }
+  return MB_OK;
+}
+
+int mz_download(const MbMzLmos* Q, int nlmo, int* ncf, int* ic, long long icdim, double* c, long long cdim) {
+  MB_CUDA(cudaMemcpy(ncf, Q->ncf, sizeof(int) * nlmo, cudaMemcpyDeviceToHost));
+  MB_CUDA(cudaMemcpy(ic, Q->icocc, sizeof(int) * icdim, cudaMemcpyDeviceToHost));
+  MB_CUDA(cudaMemcpy(c, Q->cocc, sizeof(double) * cdim, cudaMemcpyDeviceToHost));
+  return MB_OK;
+}
+}  // namespace
+
+extern "C" int mb_mz_bind_system_(const int* numat, const int* iorbs, const double* coord, const double* cutof1,
+                                  const double* cutof2, const double* h, const double* w, const long long* nw) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  mz_release_system();
+  const int n = *numat;
+  g_mz.numat = n;
+  g_mz.iorbs.assign(iorbs, iorbs + n);
+  MB_TRY(mb_mz_layout_create(n, iorbs, coord, *cutof1, *cutof2, &g_mz.L, nullptr));
+  g_mz.have_system = true;
+  if (*nw != g_mz.L.nw) return mb_set_error(MB_ERR_ARG, "mb_mz_bind_system_: w length differs from the layout's");
+  g_mz.norbs = g_mz.L.norbs;
+  g_mz.mpack = g_mz.L.mpack;
+  g_mz.nw = *nw;
+  MB_TRY(mz_upload(&g_mz.coord, coord, 3 * (size_t)n));
+  MB_TRY(mz_upload(&g_mz.h, h, (size_t)g_mz.mpack));
+  MB_TRY(mz_upload(&g_mz.w, w, (size_t)g_mz.nw));
+  g_mz.state[0] = 10.0; g_mz.state[1] = 1.0; g_mz.state[2] = 0.0; g_mz.state[3] = 0.0;
+  g_mz.nrejct[0] = g_mz.nrejct[1] = 0;
+  return MB_OK;
+}
+
+extern "C" int mb_mz_bind_lmos_(const int* nocc, int* ncf, int* nncf, int* icocc, int* ncocc, double* cocc,
+                                const long long* icocc_dim, const long long* cocc_dim, const int* nvir, int* nce,
+                                int* nnce, int* icvir, int* ncvir, double* cvir, const long long* icvir_dim,
+                                const long long* cvir_dim, double* p, double* eigs, const long long* fmo_dim) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  g_mz.nocc = *nocc; g_mz.ncf = ncf; g_mz.nncf = nncf; g_mz.icocc = icocc; g_mz.ncocc = ncocc; g_mz.cocc = cocc;
+  g_mz.icocc_dim = *icocc_dim; g_mz.cocc_dim = *cocc_dim;
+  g_mz.nvir = *nvir; g_mz.nce = nce; g_mz.nnce = nnce; g_mz.icvir = icvir; g_mz.ncvir = ncvir; g_mz.cvir = cvir;
+  g_mz.icvir_dim = *icvir_dim; g_mz.cvir_dim = *cvir_dim;
+  g_mz.p = p;
+  g_mz.eigs = eigs;
+  g_mz.cap = *fmo_dim;
+  g_mz.have_lmos = true;
+  return MB_OK;
+}
+
+extern "C" int mb_mz_bind_controls_(const double* shift, const double* thresh) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  g_mz.shift = shift;
+  g_mz.thresh_p = thresh;
+  return MB_OK;
+}
+
+extern "C" void density_for_mozyme_(double* p, const int* mode, const int* nclose_loc, const double* partp) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  int rc = (!g_mz.have_system || !g_mz.have_lmos)
+               ? mb_set_error(MB_ERR_ARG, "density_for_mozyme_: call mb_mz_bind_system_ and mb_mz_bind_lmos_ first")
+               : ensure_stream();
+  MbMzLmos occ{};
+  bool have = false;
+  if (rc == MB_OK) rc = mz_lmos(*nclose_loc, &occ, nullptr);
+  have = rc == MB_OK;
+  const size_t mp = (size_t)g_mz.mpack;
+  if (rc == MB_OK) rc = g_a.get(sizeof(double) * 2 * mp);
+  double* dp = (double*)g_a.p;
+  if (rc == MB_OK && *mode != 0 &&
+      cudaMemcpyAsync(dp + mp, partp, sizeof(double) * mp, cudaMemcpyHostToDevice, g_stream) != cudaSuccess)
+    rc = MB_ERR_CUDA;
+  if (rc == MB_OK) rc = mb_mz_density_dev(&g_mz.L, &occ, *mode, *mode != 0 ? dp + mp : nullptr, dp, g_stream);
+  if (rc == MB_OK && cudaMemcpyAsync(p, dp, sizeof(double) * mp, cudaMemcpyDeviceToHost, g_stream) != cudaSuccess)
+    rc = MB_ERR_CUDA;
+  if (rc == MB_OK && cudaStreamSynchronize(g_stream) != cudaSuccess) rc = MB_ERR_CUDA;
+  if (have) mb_mz_lmos_destroy(&occ);
+  report(rc, "density_for_mozyme_");
+}
+
+extern "C" void buildf_(double* f, const double* partf, const int* mode) {
+  (void)partf;
+  std::lock_guard<std::mutex> lk(g_mu);
+  int rc = (!g_mz.have_system || !g_mz.have_lmos)
+               ? mb_set_error(MB_ERR_ARG, "buildf_: call mb_mz_bind_system_ and mb_mz_bind_lmos_ first")
+               : (*mode != 0 ? mb_set_error(MB_ERR_UNSUPPORTED, "buildf_: whole-F mode 0 only") : ensure_stream());
+  const size_t mp = (size_t)g_mz.mpack;
+  if (rc == MB_OK) rc = g_a.get(sizeof(double) * 2 * mp);
+  if (rc == MB_OK) rc = g_ws.get(mb_mz_fock_ws_bytes(&g_mz.L) + 256);
+  double* dp = (double*)g_a.p;
+  double* df = dp + mp;
+  if (rc == MB_OK && cudaMemcpyAsync(dp, g_mz.p, sizeof(double) * mp, cudaMemcpyHostToDevice, g_stream) != cudaSuccess)
+    rc = MB_ERR_CUDA;
+  if (rc == MB_OK) rc = mb_mz_fock_dev(&g_mz.L, g_mz.coord, g_mz.w, dp, g_mz.h, df, g_ws.p, g_stream);
+  if (rc == MB_OK && cudaMemcpyAsync(f, df, sizeof(double) * mp, cudaMemcpyDeviceToHost, g_stream) != cudaSuccess)
+    rc = MB_ERR_CUDA;
+  if (rc == MB_OK && cudaStreamSynchronize(g_stream) != cudaSuccess) rc = MB_ERR_CUDA;
+  report(rc, "buildf_");
+}
+
+extern "C" void diagg_(const double* fao, const int* nocc, const int* nvir, const int* idiagg, double* partp,
+                       const int* indi) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  int rc = (!g_mz.have_system || !g_mz.have_lmos)
+               ? mb_set_error(MB_ERR_ARG, "diagg_: call mb_mz_bind_system_ and mb_mz_bind_lmos_ first")
+               : ensure_stream();
+  if (rc == MB_OK && (*nocc != g_mz.nocc || *nvir != g_mz.nvir))
+    rc = mb_set_error(MB_ERR_ARG, "diagg_: nocc / nvir differ from the bound LMOs");
+  MbMzLmos occ{}, vir{};
+  bool have = false;
+  if (rc == MB_OK) rc = mz_lmos(g_mz.nocc, &occ, &vir);
+  have = rc == MB_OK;
+  const size_t mp = (size_t)g_mz.mpack;
+  const long long cap = g_mz.cap > 0 ? g_mz.cap : 300LL * g_mz.norbs;
+  if (rc == MB_OK) rc = g_a.get(sizeof(double) * 3 * mp);
+  if (rc == MB_OK) rc = g_b.get(sizeof(double) * ((size_t)g_mz.nocc + g_mz.nvir + 2));
+  if (rc == MB_OK) rc = g_ws.get(mb_mz_diagg1_ws_bytes(&g_mz.L, &occ, &vir) + 256);
+  if (rc == MB_OK) rc = g_mz.nfmo.get(sizeof(int) * ((size_t)g_mz.nvir + 1));
+  if (rc == MB_OK) rc = g_mz.ifmo.get(sizeof(int) * 2 * (size_t)cap);
+  if (rc == MB_OK) rc = g_mz.fmo.get(sizeof(double) * (size_t)cap);
+  double *dfao = (double*)g_a.p, *dp = dfao + mp, *dpart = dp + mp;
+  double *deigs = (double*)g_b.p, *deigv = deigs + g_mz.nocc;
+  if (rc == MB_OK && (cudaMemcpyAsync(dfao, fao, sizeof(double) * mp, cudaMemcpyHostToDevice, g_stream) != cudaSuccess ||
+                      cudaMemcpyAsync(dp, g_mz.p, sizeof(double) * mp, cudaMemcpyHostToDevice, g_stream) != cudaSuccess ||
+                      cudaMemcpyAsync(deigs, g_mz.eigs, sizeof(double) * ((size_t)g_mz.nocc + g_mz.nvir),
+                                      cudaMemcpyHostToDevice, g_stream) != cudaSuccess ||
+                      (*indi != 0 && cudaMemcpyAsync(dpart, partp, sizeof(double) * mp, cudaMemcpyHostToDevice,
+                                                     g_stream) != cudaSuccess)))
+    rc = MB_ERR_CUDA;
+  // diagg.F90: diagg1 (list, energies), diagg2 (rotations), density_for_MOZYME
+  long long nij = cap;
+  int done = 0;
+  double sumt = 0.0, sumb = 0.0;
+  long long nrej = 0;
+  void* ws = (void*)(((uintptr_t)g_ws.p + 255) & ~(uintptr_t)255);
+  if (rc == MB_OK)
+    rc = mb_mz_diagg1_dev(&g_mz.L, &occ, &vir, dfao, dp, *idiagg, g_mz.state, (int*)g_mz.nfmo.p, (int*)g_mz.ifmo.p,
+                          (double*)g_mz.fmo.p, &nij, deigv, deigs, &done, &sumt, ws, g_stream);
+  // diagg2's controls as iter_for_MOZYME sets them: damping, the current
+  // shift and thresh (registered by mb_mz_bind_controls_; 0 and 1e-13
+  // otherwise), diagg1's tiny and bigeps (diagg2.F90:56-63,
+  // iter_for_MOZYME.F90:86-97)
+  const double ctl[5] = {g_mz.cst, g_mz.shift ? *g_mz.shift : 0.0, g_mz.thresh_p ? *g_mz.thresh_p : g_mz.thresh,
+                         g_mz.state[3], 50.0 * sqrt(1.0e-39)};
+  if (rc == MB_OK)
+    rc = mb_mz_diagg2_dev(&g_mz.L, &occ, &vir, (const int*)g_mz.ifmo.p, (const double*)g_mz.fmo.p, nij, deigs, deigv,
+                          *idiagg, ctl, g_mz.nrejct, &sumb, &nrej, g_stream);
+  if (rc == MB_OK) rc = mb_mz_lmos_refresh(g_mz.numat, g_mz.iorbs.data(), &occ);
+  if (rc == MB_OK) rc = mb_mz_density_dev(&g_mz.L, &occ, *indi, *indi != 0 ? dpart : nullptr, dp, g_stream);
+  if (rc == MB_OK && cudaStreamSynchronize(g_stream) != cudaSuccess) rc = MB_ERR_CUDA;
+  if (rc == MB_OK) rc = mz_download(&occ, g_mz.nocc, g_mz.ncf, g_mz.icocc, g_mz.icocc_dim, g_mz.cocc, g_mz.cocc_dim);
+  if (rc == MB_OK) rc = mz_download(&vir, g_mz.nvir, g_mz.nce, g_mz.icvir, g_mz.icvir_dim, g_mz.cvir, g_mz.cvir_dim);
+  if (rc == MB_OK && (cudaMemcpy(g_mz.p, dp, sizeof(double) * mp, cudaMemcpyDeviceToHost) != cudaSuccess ||
+                      cudaMemcpy(g_mz.eigs, deigs, sizeof(double) * ((size_t)g_mz.nocc + g_mz.nvir),
+                                 cudaMemcpyDeviceToHost) != cudaSuccess))
+    rc = MB_ERR_CUDA;
+  if (have) {
+    mb_mz_lmos_destroy(&occ);
+    mb_mz_lmos_destroy(&vir);
+  }
+  report(rc, "diagg_");
 }

@@ -189,3 +189,67 @@ def test_helect_and_cnvg_shims():
     _L().cnvg_(_p(pn), _p(po), _p(p1), _i(6), ctypes.byref(pl))
     assert pl.value == plr
     assert np.array_equal(pn, rn) and np.array_equal(po, ro_) and np.array_equal(p1, r1)
+
+
+def test_mozyme_shims_with_registered_arrays():
+    """density_for_MOZYME(p, mode, nclose, partp), buildf(f, partf, 0) and
+    diagg(fao, nocc, nvir, idiagg, partp, indi) (MOZYME/density_for_MOZYME.F90,
+    buildf.F90, diagg.F90) through their gfortran names, after the host has
+    registered its MOZYME_C arrays (mb_mz_bind_system_, mb_mz_bind_lmos_,
+    mb_mz_bind_controls_): each against the oracle's restatement, bit for bit,
+    and the host arrays hold diagg's results afterwards."""
+    from mopac_gpu_b200 import workloads
+    from oracle import mozyme_oracle as mo
+    nat, xyz, _ = workloads.water_box(32)
+    s = oracle_system(nat, xyz)
+    iorbs = np.ascontiguousarray((s.nlast - s.nfirst + 1).astype(np.int32))
+    c1, c2 = mo.cutoffs(len(nat), 9.0)
+    mp, nb = mo.layout(iorbs, s.coord, c1, c2)
+    h = np.ascontiguousarray(mo.dense_to_blocks(so.unpack(s.h, s.norbs), iorbs, nb, mp))
+    w = np.ascontiguousarray(mo.w_stored(iorbs, nb, s.w))
+    _, occ = workloads.mozyme_lmos(nat, xyz, radius=4.0, seed=3, per_heavy=4, pad_atoms=2)
+    _, vir = workloads.mozyme_lmos(nat, xyz, radius=3.2, seed=4, per_heavy=2, pad_atoms=2)
+    occ = [np.ascontiguousarray(x) for x in occ]
+    vir = [np.ascontiguousarray(x) for x in vir]
+    L = _L()
+    coord = np.ascontiguousarray(s.coord.reshape(-1))
+    nw = ctypes.c_longlong(w.size)
+    assert L.mb_mz_bind_system_(_i(len(nat)), _p(iorbs), _p(coord), _d(c1), _d(c2), _p(h), _p(w),
+                                ctypes.byref(nw)) == 0
+    p = np.zeros(mp)
+    eigs = np.zeros(len(occ[0]) + len(vir[0]))
+    cap = 300 * s.norbs
+    ll = lambda v: ctypes.byref(ctypes.c_longlong(int(v)))
+    assert L.mb_mz_bind_lmos_(_i(len(occ[0])), _p(occ[0]), _p(occ[1]), _p(occ[2]), _p(occ[3]), _p(occ[4]),
+                              ll(occ[2].size), ll(occ[4].size), _i(len(vir[0])), _p(vir[0]), _p(vir[1]),
+                              _p(vir[2]), _p(vir[3]), _p(vir[4]), ll(vir[2].size), ll(vir[4].size), _p(p),
+                              _p(eigs), ll(cap)) == 0
+    shift, thresh = ctypes.c_double(0.0), ctypes.c_double(1.0e-13)
+    assert L.mb_mz_bind_controls_(ctypes.byref(shift), ctypes.byref(thresh)) == 0
+    partp = np.zeros(mp)
+    # density_for_MOZYME
+    L.density_for_mozyme_(_p(p), _i(0), _i(len(occ[0])), _p(partp))
+    p_ref = mo.density(iorbs, nb, tuple(occ), 0, mp)
+    assert np.array_equal(p, p_ref)
+    # buildf (whole F from the registered p)
+    f = np.zeros(mp)
+    L.buildf_(_p(f), _p(partp), _i(0))
+    f_ref = mo.fock(s.nat, s.coord, iorbs, nb, s.w, p_ref, h)
+    assert np.array_equal(f, f_ref)
+    # diagg: diagg1 + diagg2 + density, the host arrays updated in place
+    o_ref, v_ref = tuple(x.copy() for x in occ), tuple(x.copy() for x in vir)
+    st = np.array([10.0, 1.0, 0.0, 0.0])
+    nfmo = np.zeros(len(vir[0]), np.int32)
+    ifmo = np.zeros(2 * cap, np.int32)
+    fmo = np.zeros(cap)
+    nij, eigv, eg, _ = mo.diagg1(iorbs, nb, f_ref, p_ref, o_ref, v_ref, 0, st, nfmo, ifmo, fmo, cap)
+    mo.diagg2(iorbs, o_ref, v_ref, ifmo, fmo, nij, eg, eigv, 0, [1.0, 0.0, 1e-13, st[3], 50 * np.sqrt(1e-39)],
+              np.zeros(2, np.int32))
+    p2_ref = mo.density(iorbs, nb, o_ref, 0, mp)
+    L.diagg_(_p(f), _i(len(occ[0])), _i(len(vir[0])), _i(0), _p(partp), _i(0))
+    for got, ref in zip(occ + vir, o_ref + v_ref):
+        assert np.array_equal(got, ref)
+    assert np.array_equal(p, p2_ref)
+    np.testing.assert_array_equal(eigs[:len(occ[0])], eg)
+    np.testing.assert_array_equal(eigs[len(occ[0]):], eigv)
+    L.mopac_cuda_destroy_resources()
