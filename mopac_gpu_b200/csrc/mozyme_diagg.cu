@@ -496,59 +496,112 @@ __device__ __forceinline__ int find_atom(const int* ic, int nn, int cnt, const i
   return -1;
 }
 
-// Atom -> coefficient offset of one LMO's atoms (the first cnt of its list),
-// open addressing in thread-local memory, so each test "is atom a in this
-// LMO" is a few probes instead of a scan of the list.  Built in list order, so
-// a repeated atom resolves to its first slot, as the scan does.  At most half
-// full, so every probe sequence ends; LMOs past that size use the scan.
-constexpr int AMAP = 1024;
-struct AtomMap {
-  int key[AMAP];
-  int val[AMAP];
+// Whether a rotation is rejected depends only on coefficients it has not yet
+// touched (those of atoms in one LMO only), so a dry run decides it first;
+// modifying and then restoring, as the reference does, leaves the same
+// coefficients as not modifying.  The atom numbers it appends before a
+// rejection stay in the LMOs' spare slots in the reference (it restores the
+// counts, not the slots); the dry run writes them too.
+// ---------------------------------------------------------- warp per rotation
+// diagg2's 2x2 rotation (diagg2.F90:180-345), one warp per rotation: the atom lists of
+// the two LMOs are walked 32 atoms at a time, one lane per atom, and what the
+// sequential loop carries from atom to atom -- the running coefficient offset,
+// the number of atoms appended so far and their coefficient count -- is a
+// warp prefix sum, so every lane knows where its atom's coefficients sit and
+// where an appended atom goes.  Membership ("is atom a in the other LMO, and
+// at which offset") goes through a per-warp hash map in shared memory.  Each
+// atom's own arithmetic (its squared-sum test over its orbitals, its 2x2
+// rotations) is the sequential loop's, in the same order, and atoms touch
+// disjoint coefficients, so the result is bit for bit the sequential loop's.  An
+// overflow check fails first at the same atom as in the sequential loop:
+// the running totals only grow.
+constexpr int WMAP = 1024;            // slots per map; at most WMAP / 2 atoms mapped
+constexpr int D2W = 4;                // warps (rotations) per CTA
+constexpr unsigned FULLW = 0xffffffffu;
+constexpr size_t D2_SMEM = sizeof(int) * 4 * WMAP * D2W;  // two maps (keys, values) per warp
+
+struct WMap {
+  int* key;
+  int* val;
   bool ok;
-  __device__ void build(const int* ic, int nn, int cnt, const int* iorbs) {
-    ok = cnt <= AMAP / 2;
-    if (!ok) return;
-    for (int q = 0; q < AMAP; ++q) key[q] = -1;
-    int off = 0;
-    for (int t = nn; t < nn + cnt; ++t) {
-      const int b = ic[t] - 1;
-      unsigned h = ((unsigned)b * 2654435761u) & (AMAP - 1);
-      while (key[h] >= 0) h = (h + 1) & (AMAP - 1);
-      key[h] = b;
-      val[h] = off;
-      off += iorbs[b];
-    }
+};
+
+__device__ __forceinline__ unsigned wmap_hash(int a) { return ((unsigned)a * 2654435761u) & (WMAP - 1); }
+
+// Inclusive warp scan of x.
+__device__ __forceinline__ long long warp_scan(long long x, int lane) {
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const long long y = __shfl_up_sync(FULLW, x, o);
+    if (lane >= o) x += y;
   }
-  __device__ int find(int a) const {
-    unsigned h = ((unsigned)a * 2654435761u) & (AMAP - 1);
-    while (key[h] >= 0) {
-      if (key[h] == a) return val[h];
-      h = (h + 1) & (AMAP - 1);
+  return x;
+}
+
+// Map atom -> coefficient offset over the first cnt atoms of a list; returns
+// the list's total coefficient count.
+__device__ long long wmap_build(WMap& m, const int* ic, int nn, int cnt, const int* iorbs, int lane) {
+  m.ok = cnt <= WMAP / 2;
+  if (m.ok)
+    for (int q = lane; q < WMAP; q += 32) { m.key[q] = -1; m.val[q] = 0x7fffffff; }
+  __syncwarp();
+  long long carry = 0;
+  for (int base = 0; base < cnt; base += 32) {
+    const int t = base + lane;
+    int b = -1, no = 0;
+    if (t < cnt) { b = ic[nn + t] - 1; no = iorbs[b]; }
+    const long long inc = warp_scan(no, lane);
+    const long long off = carry + inc - no;
+    if (m.ok && t < cnt) {
+      unsigned h = wmap_hash(b);
+      for (;;) {
+        const int prev = atomicCAS(&m.key[h], -1, b);
+        if (prev == -1 || prev == b) break;
+        h = (h + 1) & (WMAP - 1);
+      }
+      atomicMin(&m.val[h], (int)off);  // a repeated atom keeps its first slot
+    }
+    carry += __shfl_sync(FULLW, inc, 31);
+  }
+  __syncwarp();
+  return carry;
+}
+
+__device__ __forceinline__ int wmap_find(const WMap& m, int a, const int* ic, int nn, int cnt, const int* iorbs) {
+  if (m.ok) {
+    unsigned h = wmap_hash(a);
+    while (m.key[h] >= 0) {
+      if (m.key[h] == a) return m.val[h];
+      h = (h + 1) & (WMAP - 1);
     }
     return -1;
   }
-};
+  return find_atom(ic, nn, cnt, iorbs, a);
+}
 
-// One thread per rotation of the level.  Whether a rotation is rejected
-// depends only on coefficients it has not yet touched (those of atoms in one
-// LMO only), so a dry run decides it first; modifying and then restoring, as
-// the reference does, leaves the same coefficients as not modifying.  The
-// atom numbers it appends before a rejection stay in the LMOs' spare slots
-// in the reference (it restores the counts, not the slots); the dry run
-// writes them too.
-__global__ void mzd2_level(D2Args A) {
-  const long long q = A.lo + blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (q >= A.hi) return;
+__global__ void __launch_bounds__(32 * D2W) mzd2_level_warp(D2Args A) {
+  extern __shared__ int d2_smem[];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const long long q = A.lo + (long long)blockIdx.x * D2W + wid;
+  if (q >= A.hi) return;  // whole warp
+  WMap mj, mi;
+  mj.key = d2_smem + wid * 4 * WMAP;
+  mj.val = mj.key + WMAP;
+  mi.key = mj.val + WMAP;
+  mi.val = mi.key + WMAP;
   const long long e = A.order[q];
   const int i = A.ifmo[2 * e] - 1, j = A.ifmo[2 * e + 1] - 1;
-  double bs = 0.0;
-  int rj = 0;
   const double fm = A.fmo[e];
-  if (!(fabs(fm) >= A.tiny)) { A.beta_sum[e] = 0.0; A.rej[e] = 0; return; }
+  if (!(fabs(fm) >= A.tiny)) {
+    if (lane == 0) { A.beta_sum[e] = 0.0; A.rej[e] = 0; }
+    return;
+  }
   const double c = DMUL(fm, A.cst);
   const double d = DSUB(DSUB(A.eigs[j], A.eigv[i]), A.shift);
-  if (!(fabs(c / d) >= A.biglim)) { A.beta_sum[e] = 0.0; A.rej[e] = 0; return; }
+  if (!(fabs(c / d) >= A.biglim)) {
+    if (lane == 0) { A.beta_sum[e] = 0.0; A.rej[e] = 0; }
+    return;
+  }
   int* ncf = const_cast<int*>(A.occ.ncf);
   int* icocc = const_cast<int*>(A.occ.icocc);
   double* cocc = const_cast<double*>(A.occ.cocc);
@@ -558,7 +611,6 @@ __global__ void mzd2_level(D2Args A) {
   const int* nncf = A.occ.nncf;
   const int* nnce = A.vir.nncf;
   const long long loopj = A.occ.ncocc[j], loopi = A.vir.ncocc[i];
-  // spaces, 1-based ends as in the reference
   const long long jlr = loopj + 1, ilr = loopi + 1;
   long long jur = (j != A.nocc - 1) ? A.occ.ncocc[j + 1] : A.occ.ncoeff;
   const long long jncf = (j != A.nocc - 1) ? nncf[j + 1] : A.occ.nentries;
@@ -567,59 +619,79 @@ __global__ void mzd2_level(D2Args A) {
   jur = jlr + A.norbs - 1 < jur ? jlr + A.norbs - 1 : jur;
   iur = ilr + A.norbs - 1 < iur ? ilr + A.norbs - 1 : iur;
   const int ncf0 = ncf[j], nce0 = nce[i];
-  AtomMap mj, mi;
-  mj.build(icocc, nncf[j], ncf0, A.iorbs);
-  mi.build(icvir, nnce[i], nce0, A.iorbs);
-  auto findj = [&](int a) { return mj.ok ? mj.find(a) : find_atom(icocc, nncf[j], ncf0, A.iorbs, a); };
-  auto findi = [&](int a) { return mi.ok ? mi.find(a) : find_atom(icvir, nnce[i], nce0, A.iorbs, a); };
+  const int nnj = nncf[j], nni = nnce[i];
+  const long long mlf0 = wmap_build(mj, icocc, nnj, ncf0, A.iorbs, lane);  // coefficients of LMO j
+  const long long mle0 = wmap_build(mi, icvir, nni, nce0, A.iorbs, lane);  // coefficients of LMO i
   const double ee = copysign(sqrt(DADD(DMUL(DMUL(4.0, c), c), DMUL(d, d))), d);
   double alpha = sqrt(DMUL(0.5, DADD(1.0, d / ee)));
+  double bs = 0.0;
+  int rj = 0;
+  const unsigned lt = (1u << lane) - 1u;
+  double beta = 0.0;
   for (;;) {
-    const double beta = -copysign(sqrt(DSUB(1.0, DMUL(alpha, alpha))), c);
+    beta = -copysign(sqrt(DSUB(1.0, DMUL(alpha, alpha))), c);
     bs = DADD(bs, fabs(beta));
-    // ---- dry run: growth decisions and the space checks, in the reference's order
+    // ---- dry run 1: atoms of LMO i that would join LMO j
     bool rejected = false;
-    long long mlf = 0;
-    for (int t = nncf[j]; t < nncf[j] + ncf0; ++t) mlf += A.iorbs[icocc[t] - 1];
-    long long nfj = ncf0, mle = 0;
-    for (int le = nnce[i]; le < nnce[i] + nce0; ++le) {
-      const int mie = icvir[le] - 1;
-      const int no = A.iorbs[mie];
-      if (findj(mie) < 0) {
-        double sum = 0.0;
-        for (int k = 0; k < no; ++k) {
-          const double t = DMUL(beta, cvir[loopi + mle + k]);
-          sum = DADD(sum, DMUL(t, t));
-        }
-        if (sum > A.thresh) {
-          if (nncf[j] + nfj >= jncf || mlf + no + loopj > jur) { rejected = true; break; }
-          ++nfj;
-          icocc[nncf[j] + nfj - 1] = mie + 1;  // the reference leaves these in place if it rejects later
-          mlf += no;
-        }
-      }
-      mle += no;
-    }
-    long long nfi = nce0;
-    if (!rejected) {
-      long long off = 0;
-      for (int lf = nncf[j]; lf < nncf[j] + ncf0; ++lf) {
-        const int ii = icocc[lf] - 1;
-        const int no = A.iorbs[ii];
-        if (findi(ii) < 0) {
+    {
+      long long nfj = ncf0, mlf = mlf0, moff = 0;
+      for (int base = 0; base < nce0 && !rejected; base += 32) {
+        const int t = base + lane;
+        int mie = -1, no = 0;
+        if (t < nce0) { mie = icvir[nni + t] - 1; no = A.iorbs[mie]; }
+        const long long inc = warp_scan(no, lane);
+        const long long off = moff + inc - no;
+        bool cand = false;
+        if (t < nce0 && wmap_find(mj, mie, icocc, nnj, ncf0, A.iorbs) < 0) {
           double sum = 0.0;
           for (int k = 0; k < no; ++k) {
-            const double t = DMUL(beta, cocc[loopj + off + k]);
-            sum = DADD(sum, DMUL(t, t));
+            const double tt = DMUL(beta, cvir[loopi + off + k]);
+            sum = DADD(sum, DMUL(tt, tt));
           }
-          if (sum > A.thresh) {
-            if (nnce[i] + nfi >= incv || mle + no + loopi > iur) { rejected = true; break; }
-            ++nfi;
-            icvir[nnce[i] + nfi - 1] = ii + 1;
-            mle += no;
-          }
+          cand = sum > A.thresh;
         }
-        off += no;
+        const unsigned bal = __ballot_sync(FULLW, cand);
+        const long long cno = warp_scan(cand ? no : 0, lane);
+        const long long pos_n = nfj + __popc(bal & lt), pos_m = mlf + cno - (cand ? no : 0);
+        const bool over = cand && (nnj + pos_n >= jncf || pos_m + no + loopj > jur);
+        const unsigned ob = __ballot_sync(FULLW, over);
+        const int first = ob ? __ffs(ob) - 1 : 32;
+        if (cand && lane < first) icocc[nnj + pos_n] = mie + 1;  // as the reference leaves them
+        if (ob) rejected = true;
+        nfj += __popc(bal);
+        mlf += __shfl_sync(FULLW, cno, 31);
+        moff += __shfl_sync(FULLW, inc, 31);
+      }
+    }
+    // ---- dry run 2: atoms of LMO j that would join LMO i
+    if (!rejected) {
+      long long nfi = nce0, mle = mle0, joff = 0;
+      for (int base = 0; base < ncf0 && !rejected; base += 32) {
+        const int t = base + lane;
+        int ii = -1, no = 0;
+        if (t < ncf0) { ii = icocc[nnj + t] - 1; no = A.iorbs[ii]; }
+        const long long inc = warp_scan(no, lane);
+        const long long off = joff + inc - no;
+        bool cand = false;
+        if (t < ncf0 && wmap_find(mi, ii, icvir, nni, nce0, A.iorbs) < 0) {
+          double sum = 0.0;
+          for (int k = 0; k < no; ++k) {
+            const double tt = DMUL(beta, cocc[loopj + off + k]);
+            sum = DADD(sum, DMUL(tt, tt));
+          }
+          cand = sum > A.thresh;
+        }
+        const unsigned bal = __ballot_sync(FULLW, cand);
+        const long long cno = warp_scan(cand ? no : 0, lane);
+        const long long pos_n = nfi + __popc(bal & lt), pos_m = mle + cno - (cand ? no : 0);
+        const bool over = cand && (nni + pos_n >= incv || pos_m + no + loopi > iur);
+        const unsigned ob = __ballot_sync(FULLW, over);
+        const int first = ob ? __ffs(ob) - 1 : 32;
+        if (cand && lane < first) icvir[nni + pos_n] = ii + 1;
+        if (ob) rejected = true;
+        nfi += __popc(bal);
+        mle += __shfl_sync(FULLW, cno, 31);
+        joff += __shfl_sync(FULLW, inc, 31);
       }
     }
     if (rejected) {
@@ -627,70 +699,95 @@ __global__ void mzd2_level(D2Args A) {
       if (A.retry) { alpha = DMUL(0.5, DADD(alpha, 1.0)); continue; }
       break;
     }
-    // ---- apply: rotations and the atoms added to LMO j (loop over LMO i's atoms)
-    mlf = 0;
-    for (int t = nncf[j]; t < nncf[j] + ncf0; ++t) mlf += A.iorbs[icocc[t] - 1];
-    mle = 0;
-    for (int le = nnce[i]; le < nnce[i] + nce0; ++le) {
-      const int mie = icvir[le] - 1;
-      const int no = A.iorbs[mie];
-      const int uj = findj(mie);
-      if (uj >= 0) {
-        for (int k = 0; k < no; ++k) {
-          const long long pj = loopj + uj + k, pi = loopi + mle + k;
-          const double a = cocc[pj], b = cvir[pi];
-          cocc[pj] = DADD(DMUL(alpha, a), DMUL(beta, b));
-          cvir[pi] = DSUB(DMUL(alpha, b), DMUL(beta, a));
-        }
-      } else {
-        double sum = 0.0;
-        for (int k = 0; k < no; ++k) {
-          const double t = DMUL(beta, cvir[loopi + mle + k]);
-          sum = DADD(sum, DMUL(t, t));
-        }
-        if (sum > A.thresh) {
-          ncf[j] = ncf[j] + 1;
-          icocc[nncf[j] + ncf[j] - 1] = mie + 1;
+    // ---- apply 1: LMO i's atoms -- rotate the shared ones, append the rest to j
+    int addj = 0;
+    {
+      long long mlf = mlf0, moff = 0;
+      for (int base = 0; base < nce0; base += 32) {
+        const int t = base + lane;
+        int mie = -1, no = 0;
+        if (t < nce0) { mie = icvir[nni + t] - 1; no = A.iorbs[mie]; }
+        const long long inc = warp_scan(no, lane);
+        const long long off = moff + inc - no;
+        const int uj = t < nce0 ? wmap_find(mj, mie, icocc, nnj, ncf0, A.iorbs) : 0;
+        bool cand = false;
+        if (t < nce0 && uj >= 0) {
           for (int k = 0; k < no; ++k) {
-            const long long pi = loopi + mle + k;
-            cocc[loopj + mlf + k] = DMUL(beta, cvir[pi]);
+            const long long pj = loopj + uj + k, pi = loopi + off + k;
+            const double a = cocc[pj], b = cvir[pi];
+            cocc[pj] = DADD(DMUL(alpha, a), DMUL(beta, b));
+            cvir[pi] = DSUB(DMUL(alpha, b), DMUL(beta, a));
+          }
+        } else if (t < nce0) {
+          double sum = 0.0;
+          for (int k = 0; k < no; ++k) {
+            const double tt = DMUL(beta, cvir[loopi + off + k]);
+            sum = DADD(sum, DMUL(tt, tt));
+          }
+          cand = sum > A.thresh;
+        }
+        const unsigned bal = __ballot_sync(FULLW, cand);
+        const long long cno = warp_scan(cand ? no : 0, lane);
+        if (cand) {
+          const long long pos_m = mlf + cno - no;
+          icocc[nnj + ncf0 + addj + __popc(bal & lt)] = mie + 1;
+          for (int k = 0; k < no; ++k) {
+            const long long pi = loopi + off + k;
+            cocc[loopj + pos_m + k] = DMUL(beta, cvir[pi]);
             cvir[pi] = DMUL(alpha, cvir[pi]);
           }
-          mlf += no;
         }
+        addj += __popc(bal);
+        mlf += __shfl_sync(FULLW, cno, 31);
+        moff += __shfl_sync(FULLW, inc, 31);
       }
-      mle += no;
     }
-    // atoms added to LMO i (loop over LMO j's original atoms not in LMO i)
-    long long off = 0;
-    for (int lf = nncf[j]; lf < nncf[j] + ncf0; ++lf) {
-      const int ii = icocc[lf] - 1;
-      const int no = A.iorbs[ii];
-      if (findi(ii) < 0) {
-        double sum = 0.0;
-        for (int k = 0; k < no; ++k) {
-          const double t = DMUL(beta, cocc[loopj + off + k]);
-          sum = DADD(sum, DMUL(t, t));
+    // ---- apply 2: LMO j's original atoms not in i join LMO i
+    int addi = 0;
+    {
+      long long mle = mle0, joff = 0;
+      for (int base = 0; base < ncf0; base += 32) {
+        const int t = base + lane;
+        int ii = -1, no = 0;
+        if (t < ncf0) { ii = icocc[nnj + t] - 1; no = A.iorbs[ii]; }
+        const long long inc = warp_scan(no, lane);
+        const long long off = joff + inc - no;
+        bool cand = false;
+        if (t < ncf0 && wmap_find(mi, ii, icvir, nni, nce0, A.iorbs) < 0) {
+          double sum = 0.0;
+          for (int k = 0; k < no; ++k) {
+            const double tt = DMUL(beta, cocc[loopj + off + k]);
+            sum = DADD(sum, DMUL(tt, tt));
+          }
+          cand = sum > A.thresh;
         }
-        if (sum > A.thresh) {
-          nce[i] = nce[i] + 1;
-          icvir[nnce[i] + nce[i] - 1] = ii + 1;
+        const unsigned bal = __ballot_sync(FULLW, cand);
+        const long long cno = warp_scan(cand ? no : 0, lane);
+        if (cand) {
+          const long long pos_m = mle + cno - no;
+          icvir[nni + nce0 + addi + __popc(bal & lt)] = ii + 1;
           for (int k = 0; k < no; ++k) {
             const long long pj = loopj + off + k;
-            cvir[loopi + mle + k] = DMUL(-beta, cocc[pj]);
+            cvir[loopi + pos_m + k] = DMUL(-beta, cocc[pj]);
             cocc[pj] = DMUL(alpha, cocc[pj]);
           }
-          mle += no;
         }
+        addi += __popc(bal);
+        mle += __shfl_sync(FULLW, cno, 31);
+        joff += __shfl_sync(FULLW, inc, 31);
       }
-      off += no;
+    }
+    if (lane == 0) {
+      ncf[j] = ncf0 + addj;
+      nce[i] = nce0 + addi;
     }
     break;
   }
-  A.beta_sum[e] = bs;
-  A.rej[e] = rj;
+  if (lane == 0) {
+    A.beta_sum[e] = bs;
+    A.rej[e] = rj;
+  }
 }
-
 }  // namespace
 
 extern "C" int mb_mz_diagg2_dev(const MbMzLayout* L, MbMzLmos* occ, MbMzLmos* vir, const int* ifmo, const double* fmo,
@@ -764,12 +861,17 @@ extern "C" int mb_mz_diagg2_dev(const MbMzLayout* L, MbMzLmos* occ, MbMzLmos* vi
   A.norbs = L->norbs;
   A.beta_sum = d_bs;
   A.rej = d_rej;
+  static bool d2_attr = false;
+  if (!d2_attr) {
+    MB_CUDA(cudaFuncSetAttribute(mzd2_level_warp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)D2_SMEM));
+    d2_attr = true;
+  }
   for (int v = 1; v <= nlev && rc == MB_OK; ++v) {
     A.lo = start[v];
     A.hi = start[v + 1];
     const long long cnt = A.hi - A.lo;
     if (cnt <= 0) continue;
-    mzd2_level<<<(unsigned)((cnt + 127) / 128), 128, 0, stream>>>(A);
+    mzd2_level_warp<<<(unsigned)((cnt + D2W - 1) / D2W), 32 * D2W, D2_SMEM, stream>>>(A);
     mb_count_launch();
     if (cudaGetLastError() != cudaSuccess) rc = mb_set_error(MB_ERR_CUDA, "diagg2: launch");
   }
