@@ -186,6 +186,16 @@ int mb_fock2_dev(const MbAtomsDev* atoms, double* f, const double* h, const doub
                  const double* pa, const double* w, double shift, int use_shift,
                  cudaStream_t stream);
 
+/* The same Fock build with a caller-owned device workspace of at least
+ * mb_fock2_ws_bytes(numat) bytes, 256-byte aligned (mb_fock2_dev takes one
+ * from the stream-ordered allocator per call).  The workspace holds every
+ * atom's staged partner contributions (10 numat^2 doubles); calls that
+ * overlap in time need separate workspaces. */
+size_t mb_fock2_ws_bytes(int numat);
+int mb_fock2_ws(const MbAtomsDev* atoms, double* f, const double* h, const double* ptot,
+                const double* pa, const double* w, double shift, int use_shift, void* ws,
+                size_t ws_bytes, cudaStream_t stream);
+
 /* helect: sum_{i>j} P(H+F) + 0.5 sum_i P(H+F), written to *out (device). */
 int mb_helect_dev(int n, const double* p, const double* h, const double* f, double* out,
                   cudaStream_t stream);

@@ -101,6 +101,8 @@ SIGNATURES = {
     "mb_atoms_create": ([_I, _P, _P, ctypes.POINTER(MbAtomsDev)], _I),
     "mb_atoms_destroy": ([ctypes.POINTER(MbAtomsDev)], _I),
     "mb_fock2_dev": ([ctypes.POINTER(MbAtomsDev), _P, _P, _P, _P, _P, _D, _I, _P], _I),
+    "mb_fock2_ws_bytes": ([_I], ctypes.c_size_t),
+    "mb_fock2_ws": ([ctypes.POINTER(MbAtomsDev), _P, _P, _P, _P, _P, _D, _I, _P, ctypes.c_size_t, _P], _I),
     "mb_helect_dev": ([_I, _P, _P, _P, _P, _P], _I),
     "mb_helect_noalloc": ([_I, _P, _P, _P, _P, _P], _I),
     "mb_cnvg_dev": ([_I, _P, _P, _P, _I, _P, _P], _I),

@@ -29,6 +29,10 @@ extern "C" size_t mb_eigh_ws_bytes(int n);
 extern "C" int mb_eigh_ws(int n, double* fpacked, int perturb, double* c, double* eigs, void* ws, int* status_dev,
                           cudaStream_t stream);
 extern "C" size_t mb_pseudo_ws_bytes(int n, int nocc);
+extern "C" size_t mb_fock2_ws_bytes(int numat);
+extern "C" int mb_fock2_ws(const MbAtomsDev* atoms, double* f, const double* h, const double* ptot, const double* pa,
+                           const double* w, double shift, int use_shift, void* ws, size_t ws_bytes,
+                           cudaStream_t stream);
 extern "C" int mb_pseudo_diag_ws(int n, int nocc, const double* fpacked, double* c, const double* eigs,
                                  unsigned long long* nrot_dev, void* ws, cudaStream_t stream);
 extern "C" int mb_pseudo_diag_ex(int n, int nocc, const double* fpacked, double* c, const double* eigs,
@@ -149,6 +153,7 @@ struct mb_ctx {
   unsigned long long* nrot = nullptr;
   void* eig_ws = nullptr;
   void* pseudo_ws = nullptr;
+  void* fock_ws = nullptr;  // the Fock build's staging (mb_fock2_ws_bytes(numat)), allocated on the first SCF
   // Pulay histories (npulay * mpack each), allocated on the first Pulay run
   double *fppf_hist = nullptr, *fock_hist = nullptr;
   // BF16 plane buffers of the split-precision GEMMs, allocated on first use
@@ -173,7 +178,7 @@ static void ctx_free(mb_ctx* c) {
   mb_guess_ws_destroy(c->guess_ws);
   void* ptrs[] = {c->d_nat, c->d_coord, c->h, c->w, c->f, c->p, c->pa, c->pold, c->pold2, c->c, c->eigs,
                   c->fdiag, c->scal, c->hws, c->status, c->nrot, c->eig_ws, c->pseudo_ws,
-                  c->fppf_hist, c->fock_hist, c->tc_ws_raw, c->pguess, c->purify_ws, c->pprev};
+                  c->fock_ws, c->fppf_hist, c->fock_hist, c->tc_ws_raw, c->pguess, c->purify_ws, c->pprev};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -512,6 +517,7 @@ extern "C" int mb_scf_run(mb_ctx* c, const mb_scf_opts* opts_in, mb_scf_result* 
   const int nclose = c->nclose;
   cudaStream_t s = c->stream;
   if (opts.pseudo && !c->pseudo_ws) MB_CUDA(cudaMalloc(&c->pseudo_ws, mb_pseudo_ws_bytes(n, nclose)));
+  if (!c->fock_ws) MB_CUDA(cudaMalloc(&c->fock_ws, mb_fock2_ws_bytes(c->numat)));
   const bool okpuly = opts.pulay != 0;
   if (okpuly) {
     if (!c->fppf_hist) MB_CUDA(cudaMalloc(&c->fppf_hist, sizeof(double) * kNpulay * (size_t)mpack));
@@ -647,7 +653,8 @@ extern "C" int mb_scf_run(mb_ctx* c, const mb_scf_opts* opts_in, mb_scf_result* 
     double cur_shift = shift;
     for (;;) {  // label 320
       t_fock.start();
-      MB_TRY(mb_fock2_dev(&c->atoms, c->f, c->h, c->p, c->pa, c->w, cur_shift, use_shift ? 1 : 0, s));
+      MB_TRY(mb_fock2_ws(&c->atoms, c->f, c->h, c->p, c->pa, c->w, cur_shift, use_shift ? 1 : 0, c->fock_ws,
+                         mb_fock2_ws_bytes(c->numat), s));
       t_fock.stop();
       MB_TRY(mb_helect_ws(n, c->pa, c->h, c->f, c->scal, c->hws, s));
       double hee = 0.0;

@@ -172,8 +172,10 @@ def run_cases(names, reps):
     fp64 = fp64_peak_tflops() if any(c in names for c in ("density64", "gemm64", "eigh")) else None
     if "fock2" in names:
         f = c1.f.clone()
-        ms = timed(lambda: check(L.mb_fock2_dev(ctypes.byref(c1.atoms), vp(f), vp(c1.h), vp(c1.p), vp(c1.pa),
-                                                vp(c1.w), 0.0, 0, s())), reps)
+        wsb = L.mb_fock2_ws_bytes(len(c1.ctx.nat))
+        ws = torch.empty(wsb, dtype=torch.uint8, device="cuda")
+        ms = timed(lambda: check(L.mb_fock2_ws(ctypes.byref(c1.atoms), vp(f), vp(c1.h), vp(c1.p), vp(c1.pa),
+                                               vp(c1.w), 0.0, 0, vp(ws), wsb, s())), reps)
         out.append(line("fock2", ms, 8 * (c1.ctx.n2elec + 4 * c1.mpack), "GB/s", "hbm", hbm, src,
                         config="(H2O)512, n = 3072"))
     if "helect" in names:

@@ -95,3 +95,28 @@ def test_mozyme_hcore_refuses_cutoffs_below_the_feathering_distance(libpath):
     rc = L.mb_mz_hcore_dev(ctypes.byref(lay), fake, fake, fake, fake, fake, fake, None)
     assert rc == 5  # MB_ERR_UNSUPPORTED
     assert b"cutof2" in L.mb_last_error()
+
+
+def test_fock2_workspace_is_checked_before_any_gpu_work(libpath):
+    """mb_fock2_ws refuses a missing, short or misaligned workspace with
+    MB_ERR_ARG before it touches the device; the size is 10 numat^2 doubles
+    of staging plus the two atom lists and a 256-byte header."""
+    from mopac_gpu_b200._lib import MbAtomsDev
+    L = ctypes.CDLL(libpath)
+    L.mb_fock2_ws_bytes.restype = ctypes.c_size_t
+    L.mb_fock2_ws_bytes.argtypes = [ctypes.c_int]
+    L.mb_last_error.restype = ctypes.c_char_p
+    numat = 5
+    need = L.mb_fock2_ws_bytes(numat)
+    assert need == 256 + 2 * 256 + 8 * 10 * numat * numat
+    assert L.mb_fock2_ws_bytes(0) == 0
+    at = MbAtomsDev()
+    at.numat = numat
+    fake = ctypes.c_void_p(4096)
+    args = [ctypes.byref(at), fake, fake, fake, fake, fake, ctypes.c_double(0.0), ctypes.c_int(0)]
+    L.mb_fock2_ws.restype = ctypes.c_int
+    assert L.mb_fock2_ws(*args, None, ctypes.c_size_t(need), None) == 1
+    assert L.mb_fock2_ws(*args, fake, ctypes.c_size_t(need - 8), None) == 1
+    assert b"mb_fock2_ws_bytes" in L.mb_last_error()
+    assert L.mb_fock2_ws(*args, ctypes.c_void_p(4096 + 8), ctypes.c_size_t(need), None) == 1
+    assert b"aligned" in L.mb_last_error()

@@ -50,6 +50,45 @@ def test_fock2_bit_identical(name, use_shift):
     assert np.array_equal(got, f), np.abs(got - f).max()
 
 
+def _heavy_lattice(n, seed=9, spacing=1.6):
+    """n carbon atoms on a jittered cubic grid: every pair heavy-heavy, so a
+    CTA's partner chunks are bounded by the W stage, not by the thread count."""
+    rng = np.random.default_rng(seed)
+    side = int(np.ceil(n ** (1 / 3)))
+    pts = np.array([(i, j, k) for i in range(side) for j in range(side) for k in range(side)][:n], float)
+    return np.full(n, 6, np.int32), pts * spacing + rng.uniform(-0.1, 0.1, (n, 3))
+
+
+def _large_fock_systems():
+    from mopac_gpu_b200 import workloads as wl
+    nat, xyz = wl.water_lattice(200)
+    order = np.argsort(nat != 8, kind="stable")  # the same waters, oxygens first
+    return {"water200": (nat, xyz), "water200_o_first": (nat[order], xyz[order]),
+            "carbon160": _heavy_lattice(160)}
+
+
+@pytest.mark.parametrize("name", ["water200", "water200_o_first", "carbon160"])
+def test_fock2_bit_identical_multichunk(name):
+    """Systems larger than one partner chunk: water (a third heavy, mixed in
+    every chunk), the same waters with all oxygens first (chunks of one kind),
+    and an all-carbon lattice (chunks cut by the W stage)."""
+    from mopac_gpu_b200 import kernels as K
+    s = oracle_system(*_large_fock_systems()[name])
+    rng = np.random.default_rng(11)
+    p = rng.normal(scale=0.1, size=s.mpack)
+    p[so.diag_index(s.norbs)] = rng.uniform(0.0, 2.0, s.norbs)
+    pa = p * 0.5
+    shift = -20.0
+    f = s.h + shift * pa + np.arange(1, s.mpack + 1) * 1.0e-16
+    f[so.diag_index(s.norbs)] -= shift
+    so.fock2(s, f, p, pa)
+    at = K.Atoms(s.nfirst, s.nlast)
+    fd = torch.empty(s.mpack, dtype=torch.float64, device="cuda")
+    K.fock2(at, fd, _dev(s.h), _dev(p), _dev(pa), _dev(s.w), shift, True)
+    got = fd.cpu().numpy()
+    assert np.array_equal(got, f), np.abs(got - f).max()
+
+
 def test_cnvg_bit_identical():
     from mopac_gpu_b200 import kernels as K
     rng = np.random.default_rng(3)
