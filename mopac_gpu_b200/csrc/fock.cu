@@ -47,6 +47,7 @@ namespace {
 
 constexpr int kWarps = 4;          // warps per CTA of the pair pass
 constexpr int kDepth = 4;          // tiles in flight per warp
+static_assert(kDepth >= 4 && kDepth <= 4, "an HX item stages its four tiles at once, and cp_async_wait takes n <= 3");
 constexpr int kSlot = 11;          // doubles per lane slot in a tile
 constexpr int kTile = 32 * kSlot;  // doubles per tile
 constexpr int kStageW = 10;        // staged doubles per (A, B) record of a heavy A (a light A uses 2)
@@ -119,16 +120,16 @@ __device__ __forceinline__ long long rec_off(int A, int numat, int B, bool heavy
 }
 
 __device__ __forceinline__ double f_start(const FockArgs& a, long long idx, bool diag) {
-  if (!a.use_shift) return a.h[idx];
-  double v = DADD(DADD(a.h[idx], DMUL(a.shift, a.pa[idx])), DMUL((double)(idx + 1), 1.0e-16));
+  if (!a.use_shift) return __ldg(a.h + idx);
+  double v = DADD(DADD(__ldg(a.h + idx), DMUL(a.shift, __ldg(a.pa + idx))), DMUL((double)(idx + 1), 1.0e-16));
   if (diag) v = DSUB(v, a.shift);
   return v;
 }
 
 // f_start with PA(idx) already in a register.
 __device__ __forceinline__ double f_start_pa(const FockArgs& a, long long idx, double pa_idx) {
-  if (!a.use_shift) return a.h[idx];
-  return DADD(DADD(a.h[idx], DMUL(a.shift, pa_idx)), DMUL((double)(idx + 1), 1.0e-16));
+  if (!a.use_shift) return __ldg(a.h + idx);
+  return DADD(DADD(__ldg(a.h + idx), DMUL(a.shift, pa_idx)), DMUL((double)(idx + 1), 1.0e-16));
 }
 
 // Heavy atom B's diagonal density block in jab's 4 x 4 gather order,
@@ -139,7 +140,7 @@ __device__ __forceinline__ void diag_block(const FockArgs& a, int fB, double* pj
 #pragma unroll
     for (int y = 0; y < 4; ++y) {
       const int r = fB + (x > y ? x : y), cc = fB + (x < y ? x : y);
-      pjb[x * 4 + y] = a.ptot[mb_tri(r, cc)];
+      pjb[x * 4 + y] = __ldg(a.ptot + mb_tri(r, cc));
     }
 }
 
@@ -152,9 +153,9 @@ __device__ __forceinline__ void light_from_heavy(const FockArgs& a, int fB, cons
 #pragma unroll
   for (int i = 0; i <= 3; ++i) {
 #pragma unroll
-    for (int j = 1; j <= i; ++j) sumoff = DADD(sumoff, DMUL(a.ptot[mb_tri(fB + i, fB + j - 1)], wk[j + k - 1]));
+    for (int j = 1; j <= i; ++j) sumoff = DADD(sumoff, DMUL(__ldg(a.ptot + mb_tri(fB + i, fB + j - 1)), __ldg(wk + j + k - 1)));
     k += i + 1;
-    sumdia = DADD(sumdia, DMUL(a.ptot[mb_tri(fB + i, fB + i)], wk[k - 1]));
+    sumdia = DADD(sumdia, DMUL(__ldg(a.ptot + mb_tri(fB + i, fB + i)), __ldg(wk + k - 1)));
   }
   c[0] = DMUL(sumoff, 2.0);
   c[1] = sumdia;
@@ -177,26 +178,27 @@ __device__ __forceinline__ void issue_win10(double* tile, const unsigned long lo
 // (B's pair index fastest), else the lB x lA block of row B.
 __device__ __forceinline__ const double* w_block(const FockArgs& a, int A, int lA, long long wrowA, int B,
                                                  int lB) {
-  return B < A ? a.w + wrowA + (long long)lA * a.at.cum[B] : a.w + a.at.wrow[B] + (long long)lB * a.at.cum[A];
+  return B < A ? a.w + wrowA + (long long)lA * __ldg(a.at.cum + B)
+               : a.w + __ldg(a.at.wrow + B) + (long long)lB * __ldg(a.at.cum + A);
 }
 
-// One pair with at least one light atom, W block in shared memory.
+// One pair with at least one light atom, W block read from global memory.
 __device__ __forceinline__ void pair_x(const FockArgs& a, int A, int fA, int nA, int B, const double* wk,
                                        double* out) {
-  const int fB = a.at.first[B], nB = a.at.nor[B];
+  const int fB = __ldg(a.at.first + B), nB = __ldg(a.at.nor + B);
   if (nA == 4) {  // heavy A, light B: ten Coulomb terms
-    const double pb = a.ptot[mb_tri(fB, fB)];
+    const double pb = __ldg(a.ptot + (mb_tri(fB, fB)));
 #pragma unroll
-    for (int q = 0; q < 10; ++q) out[q] = DMUL(pb, wk[q]);
+    for (int q = 0; q < 10; ++q) out[q] = DMUL(pb, __ldg(wk + q));
     if (B < A) {  // kab on the 4 x 1 block
       double pj[4];
 #pragma unroll
-      for (int j = 0; j < 4; ++j) pj[j] = a.pa[mb_tri(fA + j, fB)];
+      for (int j = 0; j < 4; ++j) pj[j] = __ldg(a.pa + (mb_tri(fA + j, fB)));
 #pragma unroll
       for (int i = 1; i <= 4; ++i) {
         double sum = 0.0;
 #pragma unroll
-        for (int j = 1; j <= 4; ++j) sum = DADD(sum, DMUL(pj[j - 1], wk[pair1(i, j) - 1]));
+        for (int j = 1; j <= 4; ++j) sum = DADD(sum, DMUL(pj[j - 1], __ldg(wk + pair1(i, j) - 1)));
         const long long idx = mb_tri(fA + i - 1, fB);
         a.f[idx] = DSUB(f_start(a, idx, false), sum);
       }
@@ -206,22 +208,22 @@ __device__ __forceinline__ void pair_x(const FockArgs& a, int A, int fA, int nA,
     if (B < A) {  // kab on the 1 x 4 block
       double pl[4];
 #pragma unroll
-      for (int l = 0; l < 4; ++l) pl[l] = a.pa[mb_tri(fA, fB + l)];
+      for (int l = 0; l < 4; ++l) pl[l] = __ldg(a.pa + (mb_tri(fA, fB + l)));
 #pragma unroll
       for (int i = 0; i < 4; ++i) {
         double sum = 0.0;
 #pragma unroll
-        for (int l = 1; l <= 4; ++l) sum = DADD(sum, DMUL(pl[l - 1], wk[pair1(i + 1, l) - 1]));
+        for (int l = 1; l <= 4; ++l) sum = DADD(sum, DMUL(pl[l - 1], __ldg(wk + pair1(i + 1, l) - 1)));
         const long long idx = mb_tri(fA, fB + i);
         a.f[idx] = DSUB(f_start(a, idx, false), sum);
       }
     }
   } else {  // two light atoms: one addition
-    out[0] = DMUL(a.ptot[mb_tri(fB, fB)], wk[0]);
+    out[0] = DMUL(__ldg(a.ptot + (mb_tri(fB, fB))), __ldg(wk));
     out[1] = -0.0;
     if (B < A) {
       const long long idx = mb_tri(fA, fB);
-      a.f[idx] = DSUB(f_start(a, idx, false), DMUL(a.pa[idx], wk[0]));
+      a.f[idx] = DSUB(f_start(a, idx, false), DMUL(__ldg(a.pa + idx), __ldg(wk)));
     }
   }
 }
@@ -280,12 +282,12 @@ __global__ void __launch_bounds__(32 * kWarps, 3) fock2_pairs(FockArgs a, FockWs
 
     if (item < r1) {
       // HH: heavy A, heavy partners hlist[32 t + lane]; W rows through the tile ring
-      const int A = ws.hlist[item / th];
+      const int A = __ldg(ws.hlist + (item / th));
       const int hi = 32 * (int)(item % th) + lane;
-      const int B = hi < nh ? ws.hlist[hi] : A;
+      const int B = hi < nh ? __ldg(ws.hlist + hi) : A;
       const bool act = B != A, lower = B < A;
-      const int fA = a.at.first[A], fB = a.at.first[B];
-      s_src[warp][0][lane] = (unsigned long long)(act ? w_block(a, A, 10, a.at.wrow[A], B, 10) : a.w);
+      const int fA = __ldg(a.at.first + A), fB = __ldg(a.at.first + B);
+      s_src[warp][0][lane] = (unsigned long long)(act ? w_block(a, A, 10, __ldg(a.at.wrow + A), B, 10) : a.w);
       __syncwarp();
 #pragma unroll
       for (int m = 0; m < kDepth; ++m) {
@@ -300,7 +302,7 @@ __global__ void __launch_bounds__(32 * kWarps, 3) fock2_pairs(FockArgs a, FockWs
 #pragma unroll
           for (int x = 0; x < 4; ++x)
 #pragma unroll
-            for (int y = 0; y < 4; ++y) pk[x * 4 + y] = a.pa[mb_tri(fA + x, fB + y)];
+            for (int y = 0; y < 4; ++y) pk[x * 4 + y] = __ldg(a.pa + (mb_tri(fA + x, fB + y)));
         }
       }
 #pragma unroll
@@ -308,7 +310,7 @@ __global__ void __launch_bounds__(32 * kWarps, 3) fock2_pairs(FockArgs a, FockWs
         const int x = m / 4, y = m % 4;
         if (act && lower && y == 0) {
 #pragma unroll
-          for (int nu = 0; nu < 4; ++nu) hm[nu] = a.h[mb_tri(fA + x, fB + nu)];
+          for (int nu = 0; nu < 4; ++nu) hm[nu] = __ldg(a.h + (mb_tri(fA + x, fB + nu)));
         }
         cp_async_wait(m + kDepth <= 16 ? kDepth - 1 : 15 - m);
         __syncwarp();
@@ -361,15 +363,15 @@ __global__ void __launch_bounds__(32 * kWarps, 3) fock2_pairs(FockArgs a, FockWs
     } else if (item < r2) {
       // HX: heavy A, light partners llist[128 t + 32 g + lane]; one ten-double block each
       const long long j = item - r1;
-      const int A = ws.hlist[j / tl];
+      const int A = __ldg(ws.hlist + (j / tl));
       const int base = (int)(j % tl) * 128;
-      const int fA = a.at.first[A];
-      const long long wrowA = a.at.wrow[A];
+      const int fA = __ldg(a.at.first + A);
+      const long long wrowA = __ldg(a.at.wrow + A);
       int Bs[4];
 #pragma unroll
       for (int g = 0; g < 4; ++g) {
         const int idx = base + 32 * g + lane;
-        const int B = idx < nl ? ws.llist[idx] : -1;
+        const int B = idx < nl ? __ldg(ws.llist + idx) : -1;
         Bs[g] = B;
         s_src[warp][g][lane] = (unsigned long long)(B >= 0 ? w_block(a, A, 10, wrowA, B, 1) : a.w);
       }
@@ -385,11 +387,11 @@ __global__ void __launch_bounds__(32 * kWarps, 3) fock2_pairs(FockArgs a, FockWs
         double pb = 0.0, pj[4];
         int fB = 0;
         if (B >= 0) {
-          fB = a.at.first[B];
-          pb = a.ptot[mb_tri(fB, fB)];
+          fB = __ldg(a.at.first + B);
+          pb = __ldg(a.ptot + (mb_tri(fB, fB)));
           if (B < A) {
 #pragma unroll
-            for (int jj = 0; jj < 4; ++jj) pj[jj] = a.pa[mb_tri(fA + jj, fB)];
+            for (int jj = 0; jj < 4; ++jj) pj[jj] = __ldg(a.pa + (mb_tri(fA + jj, fB)));
           }
         }
         cp_async_wait(3 - g);
@@ -416,15 +418,15 @@ __global__ void __launch_bounds__(32 * kWarps, 3) fock2_pairs(FockArgs a, FockWs
       // LX: light A, partners 128 t + 32 g + lane; blocks of at most ten
       // doubles read straight from W (row A's are contiguous over B < A)
       const long long j = item - r2;
-      const int A = ws.llist[j / ta];
+      const int A = __ldg(ws.llist + (j / ta));
       const int base = (int)(j % ta) * 128;
-      const int fA = a.at.first[A];
-      const long long wrowA = a.at.wrow[A];
+      const int fA = __ldg(a.at.first + A);
+      const long long wrowA = __ldg(a.at.wrow + A);
 #pragma unroll 1
       for (int g = 0; g < 4; ++g) {
         const int B = base + 32 * g + lane;
         if (B < numat && B != A) {
-          const double* wk = w_block(a, A, 1, wrowA, B, a.at.lim[B]);
+          const double* wk = w_block(a, A, 1, wrowA, B, __ldg(a.at.lim + B));
           double out[10];
           pair_x(a, A, fA, 1, B, wk, out);
           double* rec = ws.stage + rec_off(A, numat, B, false);
@@ -441,10 +443,10 @@ __global__ void __launch_bounds__(kFoldThreads) fock2_fold(FockArgs a, FockWs ws
   extern __shared__ double s_buf[];  // kFoldDepth chunks of kFoldThreads records
   const int A = blockIdx.x, tid = threadIdx.x;
   const int numat = a.at.numat;
-  const int fA = a.at.first[A], nA = a.at.nor[A], lA = a.at.lim[A];
+  const int fA = __ldg(a.at.first + A), nA = __ldg(a.at.nor + A), lA = __ldg(a.at.lim + A);
   const bool heavy = nA == 4;
   const int wv = heavy ? kStageW : 2;
-  const long long wrowA = a.at.wrow[A];
+  const long long wrowA = __ldg(a.at.wrow + A);
   const double* src = ws.stage + rec_off(A, numat, 0, heavy);
 
   double run = 0.0, f1 = 0.0;
@@ -459,7 +461,7 @@ __global__ void __launch_bounds__(kFoldThreads) fock2_fold(FockArgs a, FockWs ws
     own_idx = mb_tri(fA + iw - 1, fA + jw - 1);
     run = f_start(a, own_idx, iw == jw);
     // fock1 (SCF/fock1.F90): one-centre Coulomb and exchange for element (iw, jw)
-    const double* w1 = a.w + wrowA + (long long)lA * a.at.cum[A];
+    const double* w1 = a.w + wrowA + (long long)lA * __ldg(a.at.cum + A);
     const int ilim = lA;
     const int ijw = iw * (iw - 1) / 2 + jw;
     double sum = 0.0;
@@ -472,8 +474,8 @@ __global__ void __launch_bounds__(kFoldThreads) fock2_fold(FockArgs a, FockWs ws
         int ikw = im * (im - 1) / 2 + jm;
         im = lw > iw ? lw : iw; jm = lw < iw ? lw : iw;
         int jlw = im * (im - 1) / 2 + jm;
-        sum = DSUB(DADD(sum, DMUL(a.ptot[ijp], w1[(ijw - 1) + ilim * (klw - 1)])),
-                   DMUL(a.pa[ijp], w1[(ikw - 1) + ilim * (jlw - 1)]));
+        sum = DSUB(DADD(sum, DMUL(__ldg(a.ptot + ijp), w1[(ijw - 1) + ilim * (klw - 1)])),
+                   DMUL(__ldg(a.pa + ijp), w1[(ikw - 1) + ilim * (jlw - 1)]));
       }
     f1 = sum;
   }
