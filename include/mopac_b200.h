@@ -491,6 +491,18 @@ int mb_mz_scf_run(const MbMzLayout* layout, const int* iorbs_host, MbMzLmos* occ
 int mb_density_dev(int n, int nocc, double occ, const double* c, int ldc, double* p,
                    cudaStream_t stream);
 
+/* density_for_GPU (matrix/density_for_GPU.F90:16-130) with every occupation
+ * it handles: ndubl doubly occupied MOs, MOs ndubl+1..nsingl holding fract
+ * electrons, occ = 2 (RHF) or 1 (one spin of UHF); mode 2 forbids the
+ * positron equivalent (:32).  iopc selects the reference's form: 2 or 3 the
+ * two DGEMMs (2*sign*G2 + frac*sign*G1 + cst*I), 4 occ*C_d C_d^T, 5 that
+ * below fract 0.01 and the explicit sums sign*(occ*G2 + frac*G1) + cst*I
+ * above; 6 (no reference iopc) the explicit sums at any fract, which is
+ * densit (matrix/densit.F90).  c: n x n column-major device matrix of all
+ * MOs (ldc >= n); p: packed device output.  FP64 on the DMMA engine. */
+int mb_density_occ_dev(int n, int ndubl, int nsingl, double occ, double fract, int mode, int iopc,
+                       const double* c, int ldc, double* p, cudaStream_t stream);
+
 /* Full eigensolve of a packed symmetric matrix after adding i*1e-10 to
  * diagonal element i (eigenvectors_LAPACK.F90:53-55; the packed input is
  * modified like the reference's xmat).  Ascending eigenvalues, vectors in
@@ -679,7 +691,9 @@ void pulay_(double* f, const double* p, const int* n, double* fppf, double* fock
             int* lfock, int* nfock, const int* msize, int* start, double* pl);
 void mb_set_npulay_(const int* npulay);
 /* density_for_GPU(c, fract, ndubl, nsingl, occ, mpack, norbs, mode, pp, iopc),
- * matrix/density_for_GPU.F90:16; closed shell (fract = 0) */
+ * matrix/density_for_GPU.F90:16: every occupation (closed shell, fractional,
+ * one UHF spin) and every iopc it takes (2..5), through mb_density_occ_dev;
+ * c holds all norbs MOs (the positron equivalent reads the virtual ones) */
 void density_for_gpu_(const double* c, const double* fract, const int* ndubl, const int* nsingl,
                       const double* occ, const int* mpack, const int* norbs, const int* mode,
                       double* pp, const int* iopc);

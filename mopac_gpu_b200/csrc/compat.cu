@@ -18,6 +18,8 @@
 extern "C" int mb_eigh_ws(int n, double* fpacked, int perturb, double* c, double* eigs, void* ws, int* status_dev,
                           cudaStream_t stream);
 extern "C" size_t mb_eigh_ws_bytes(int n);
+extern "C" int mb_density_occ_dev(int n, int ndubl, int nsingl, double occ, double fract, int mode, int iopc,
+                                  const double* c, int ldc, double* p, cudaStream_t stream);
 extern "C" size_t mb_pseudo_ws_bytes(int n, int nocc);
 extern "C" int mb_pseudo_diag_ws(int n, int nocc, const double* fpacked, double* c, const double* eigs,
                                  unsigned long long* nrot_dev, void* ws, cudaStream_t stream);
@@ -371,21 +373,18 @@ extern "C" void cnvg_(double* pnew, double* p, double* p1, const int* niter, dou
 extern "C" void density_for_gpu_(const double* c, const double* fract, const int* ndubl, const int* nsingl,
                                  const double* occ, const int* mpack, const int* norbs, const int* mode, double* pp,
                                  const int* iopc) {
-  (void)nsingl; (void)mode; (void)iopc; (void)mpack;
+  (void)mpack;
   std::lock_guard<std::mutex> lk(g_mu);
-  if (fract && *fract >= 1.0e-2) {
-    report(mb_set_error(MB_ERR_UNSUPPORTED, "density_for_gpu_: fractional occupancy not in this build"),
-           "density_for_gpu_");
-    return;
-  }
-  const int n = *norbs, k = *ndubl;
+  const int n = *norbs;
   const size_t mp = (size_t)n * (n + 1) / 2;
   int rc = ensure_stream();
-  if (rc == MB_OK) rc = g_a.get(sizeof(double) * ((size_t)n * (k > 0 ? k : 1)));
+  if (rc == MB_OK) rc = g_a.get(sizeof(double) * (size_t)n * n);
   if (rc == MB_OK) rc = g_b.get(sizeof(double) * mp);
-  if (rc == MB_OK && k > 0 && cudaMemcpyAsync(g_a.p, c, sizeof(double) * (size_t)n * k, cudaMemcpyHostToDevice, g_stream) != cudaSuccess)
+  if (rc == MB_OK && cudaMemcpyAsync(g_a.p, c, sizeof(double) * (size_t)n * n, cudaMemcpyHostToDevice, g_stream) != cudaSuccess)
     rc = MB_ERR_CUDA;
-  if (rc == MB_OK) rc = mb_density_dev(n, k, *occ, (const double*)g_a.p, n, (double*)g_b.p, g_stream);
+  if (rc == MB_OK)
+    rc = mb_density_occ_dev(n, *ndubl, *nsingl, *occ, *fract, *mode, *iopc, (const double*)g_a.p, n, (double*)g_b.p,
+                            g_stream);
   if (rc == MB_OK && cudaMemcpyAsync(pp, g_b.p, sizeof(double) * mp, cudaMemcpyDeviceToHost, g_stream) != cudaSuccess)
     rc = MB_ERR_CUDA;
   if (rc == MB_OK && cudaStreamSynchronize(g_stream) != cudaSuccess) rc = MB_ERR_CUDA;

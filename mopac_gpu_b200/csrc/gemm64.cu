@@ -245,9 +245,9 @@ __global__ void __launch_bounds__(NT) dgemm_dmma_kernel(int m, int n, int k, dou
   }
 }
 
-// Packed lower P = occ * A A^T on the DMMA engine (tiles meeting the lower triangle).
+// Packed lower P = occ * A A^T (+ P when acc) on the DMMA engine (tiles meeting the lower triangle).
 __global__ void __launch_bounds__(NT) syrk_packed_dmma_kernel(int n, int k, double occ, const double* __restrict__ a,
-                                                              int lda, double* __restrict__ p) {
+                                                              int lda, double* __restrict__ p, int acc_p) {
   const int bm = blockIdx.y * DBM, bn = blockIdx.x * DBN;
   if (bn > bm + DBM - 1) return;
   double acc[8][4][2];
@@ -264,7 +264,8 @@ __global__ void __launch_bounds__(NT) syrk_packed_dmma_kernel(int n, int k, doub
       for (int t = 0; t < 2; ++t) {
         const int cc = c0 + 8 * j + t;
         if (cc > r) continue;
-        p[mb_tri(r, cc)] = occ * acc[i][j][t];
+        const long long q = mb_tri(r, cc);
+        p[q] = acc_p ? occ * acc[i][j][t] + p[q] : occ * acc[i][j][t];
       }
   }
 }
@@ -295,10 +296,10 @@ __global__ void splitk_reduce(int m, int n, int nz, double alpha, const double* 
   }
 }
 
-// P(packed lower) = occ * A A^T with A = c[:, 0:k] (n x k, column-major).
-// Grid over 64x64 tiles intersecting the lower triangle.
+// P(packed lower) = occ * A A^T (+ P when acc) with A = c[:, 0:k] (n x k,
+// column-major).  Grid over 64x64 tiles intersecting the lower triangle.
 __global__ void __launch_bounds__(NT) syrk_packed_kernel(int n, int k, double occ, const double* __restrict__ a,
-                                                         int lda, double* __restrict__ p, int ntn) {
+                                                         int lda, double* __restrict__ p, int ntn, int acc_p) {
   const int bm = blockIdx.y * BM, bn = blockIdx.x * BN;
   if (bn > bm + BM - 1) return;  // tile entirely above the diagonal
   double acc[TM][TN];
@@ -312,9 +313,16 @@ __global__ void __launch_bounds__(NT) syrk_packed_kernel(int n, int k, double oc
     for (int j = 0; j < TN; ++j) {
       int cc = bn + tx + 16 * j;
       if (cc > r) continue;
-      p[mb_tri(r, cc)] = occ * acc[i][j];
+      const long long q = mb_tri(r, cc);
+      p[q] = acc_p ? occ * acc[i][j] + p[q] : occ * acc[i][j];
     }
   }
+}
+
+// P_ii = cst + P_ii (the constant of the positron-equivalent density).
+__global__ void add_diag_kernel(int n, double cst, double* __restrict__ p) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) p[mb_tri(i, i)] = cst + p[mb_tri(i, i)];
 }
 
 }  // namespace
@@ -371,6 +379,28 @@ extern "C" int mb_dgemm_dev(char transa, char transb, int m, int n, int k, doubl
   return mb_dgemm_ws(transa, transb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, nullptr, 0, stream);
 }
 
+namespace {
+
+// P = alpha * C[:, k0:k1] C[:, k0:k1]^T (+ P when acc), packed lower.  An
+// empty column range gives alpha * 0 (+ P), as a GEMM with k = 0 does.
+int syrk_range(int n, int k0, int k1, double alpha, const double* c, int ldc, double* p, bool acc,
+               cudaStream_t stream) {
+  const int k = k1 > k0 ? k1 - k0 : 0;
+  const double* a = c + (long long)(k > 0 ? k0 : 0) * ldc;
+  if (n > BM) {
+    dim3 grid((n + DBN - 1) / DBN, (n + DBM - 1) / DBM);
+    MB_TRY(dmma_attrs());
+    syrk_packed_dmma_kernel<<<grid, NT, DMMA_SMEM, stream>>>(n, k, alpha, a, ldc, p, acc ? 1 : 0);
+  } else {
+    dim3 grid((n + BN - 1) / BN, (n + BM - 1) / BM);
+    syrk_packed_kernel<<<grid, NT, 0, stream>>>(n, k, alpha, a, ldc, p, grid.x, acc ? 1 : 0);
+  }
+  MB_LAUNCH_CHECK();
+  return MB_OK;
+}
+
+}  // namespace
+
 extern "C" int mb_density_dev(int n, int nocc, double occ, const double* c, int ldc, double* p,
                               cudaStream_t stream) {
   if (n <= 0 || nocc < 0 || nocc > n) return mb_set_error(MB_ERR_ARG, "mb_density_dev: bad size");
@@ -379,15 +409,47 @@ extern "C" int mb_density_dev(int n, int nocc, double occ, const double* c, int 
     return MB_OK;
   }
   mb_kstat_mark(MB_KSTAT_DENSITY, stream, true);
-  if (n > BM) {
-    dim3 grid((n + DBN - 1) / DBN, (n + DBM - 1) / DBM);
-    MB_TRY(dmma_attrs());
-    syrk_packed_dmma_kernel<<<grid, NT, DMMA_SMEM, stream>>>(n, nocc, occ, c, ldc, p);
-  } else {
-    dim3 grid((n + BN - 1) / BN, (n + BM - 1) / BM);
-    syrk_packed_kernel<<<grid, NT, 0, stream>>>(n, nocc, occ, c, ldc, p, grid.x);
-  }
+  const int rc = syrk_range(n, 0, nocc, occ, c, ldc, p, false, stream);
   mb_kstat_mark(MB_KSTAT_DENSITY, stream, false);
-  MB_LAUNCH_CHECK();
+  return rc;
+}
+
+// density_for_GPU (matrix/density_for_GPU.F90:16-130) and densit
+// (matrix/densit.F90): closed-shell, fractional and UHF occupations.
+// iopc 2, 3: the DGEMM form; 4: occ * C_d C_d^T; 5: that below fract 0.01,
+// else the explicit sums; 6 (no reference iopc): densit, the explicit sums
+// at any fract.
+extern "C" int mb_density_occ_dev(int n, int ndubl, int nsingl, double occ, double fract, int mode, int iopc,
+                                  const double* c, int ldc, double* p, cudaStream_t stream) {
+  if (n <= 0 || ldc < n || ndubl < 0 || ndubl > n || nsingl < 0 || nsingl > n || !c || !p)
+    return mb_set_error(MB_ERR_ARG, "mb_density_occ_dev: bad size");
+  if (iopc < 2 || iopc > 6) return mb_set_error(MB_ERR_ARG, "mb_density_occ_dev: iopc must be 2..6");
+  // iopc 4 (and 5 below fract 0.01): the closed-shell product occ * C_d C_d^T
+  if (iopc == 4 || (iopc == 5 && fract < 1.0e-2)) return mb_density_dev(n, ndubl, occ, c, ldc, p, stream);
+  // electron or positron equivalent (density_for_GPU.F90:32-54, densit.F90:19-36)
+  double sign = 1.0, frac = fract, cst = 0.0;
+  int nl2 = 1, nu2 = ndubl, nl1 = ndubl + 1, nu1 = nsingl;
+  if (ndubl != 0 && nsingl > n / 2 && mode != 2) {
+    sign = -1.0;
+    frac = occ - fract;
+    cst = occ;
+    nl2 = nsingl + 1;
+    nu2 = n;
+    nl1 = ndubl + 1;
+    nu1 = nsingl;
+  }
+  // iopc 2/3 (the DGEMM form): 2*sign*G2, then + frac*sign*G1; iopc 5/6 (the
+  // explicit sums, densit): sign*(occ*G2 + frac*G1).  G = C C^T over the
+  // 1-based column ranges [nl, nu]; then P_ii = cst + P_ii.
+  const double a2 = (iopc <= 3 ? 2.0 : occ) * sign, a1 = frac * sign;
+  mb_kstat_mark(MB_KSTAT_DENSITY, stream, true);
+  int rc = syrk_range(n, nl2 - 1, nu2, a2, c, ldc, p, false, stream);
+  if (rc == MB_OK) rc = syrk_range(n, nl1 - 1, nu1, a1, c, ldc, p, true, stream);
+  mb_kstat_mark(MB_KSTAT_DENSITY, stream, false);
+  if (rc != MB_OK) return rc;
+  if (cst != 0.0) {
+    add_diag_kernel<<<(n + 255) / 256, 256, 0, stream>>>(n, cst, p);
+    MB_LAUNCH_CHECK();
+  }
   return MB_OK;
 }

@@ -188,6 +188,34 @@ def density(c: np.ndarray, nclose: int) -> np.ndarray:
     return pack(2.0 * (co @ co.T))
 
 
+def density_for_gpu(c: np.ndarray, fract: float, ndubl: int, nsingl: int, occ: float, mode: int,
+                    iopc: int) -> np.ndarray:
+    """matrix/density_for_GPU.F90:16-130 (iopc 2..5) and matrix/densit.F90
+    (iopc 6 here: the explicit sums at any fract).  c: (norbs, norbs), column
+    k = MO k.  Returns the packed lower triangle (= dtrttp('u') of the
+    symmetric result)."""
+    n = c.shape[0]
+    if iopc == 4 or (iopc == 5 and fract < 1.0e-2):           # :96-106 (dsyrk)
+        cd = c[:, :ndubl]
+        return pack(occ * (cd @ cd.T))
+    if ndubl != 0 and nsingl > n // 2 and mode != 2:           # :32-43 positron equivalent
+        sign, frac, cst = -1.0, occ - fract, occ
+        nl2, nu2, nl1, nu1 = nsingl + 1, n, ndubl + 1, nsingl
+    else:                                                      # :44-54 electron equivalent
+        sign, frac, cst = 1.0, fract, 0.0
+        nl2, nu2, nl1, nu1 = 1, ndubl, ndubl + 1, nsingl
+    c2 = c[:, nl2 - 1:nu2] if nu2 >= nl2 else c[:, :0]
+    c1 = c[:, nl1 - 1:nu1] if nu1 >= nl1 else c[:, :0]
+    g2, g1 = c2 @ c2.T, c1 @ c1.T
+    if iopc in (2, 3):                                         # :57-87 (two dgemm)
+        x = (2.0 * sign) * g2
+        x = (frac * sign) * g1 + x
+    else:                                                      # :107-124, densit.F90:37-48
+        x = (occ * g2 + g1 * frac) * sign
+    x[np.diag_indices(n)] = cst + x[np.diag_indices(n)]
+    return pack(x)
+
+
 def fmo_block(f: np.ndarray, c: np.ndarray, nocc: int) -> np.ndarray:
     """diag_for_GPU.F90:101-150: Fmo (nvirt x nocc) = C_v^T F C_o."""
     n = c.shape[0]
