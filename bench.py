@@ -755,6 +755,7 @@ def fock_roofline(ctx):
     pt.copy_(torch.from_numpy(ctx.density()))
     pa.copy_(pt * 0.5)
     reps = 10
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     wsb = lib().mb_fock2_ws_bytes(len(ctx.nat))
     ws = torch.empty(wsb, dtype=torch.uint8, device="cuda")
 
