@@ -200,6 +200,13 @@ int mb_fock2_ws(const MbAtomsDev* atoms, double* f, const double* h, const doubl
 int mb_helect_dev(int n, const double* p, const double* h, const double* f, double* out,
                   cudaStream_t stream);
 
+/* Self-test of the bounded mbarrier wait the tcgen05 GEMM uses: waits
+ * limit_ns (1 ns .. 0.1 s, else MB_ERR_ARG) on a barrier that never
+ * completes and writes out_dev[0] = 1 (the wait gave up) and out_dev[1] =
+ * nanoseconds waited.  No reference counterpart: it exercises this library's
+ * failure path without faulting or hanging anything. */
+int mb_selftest_bounded_wait(unsigned long long limit_ns, long long* out_dev, cudaStream_t stream);
+
 /* helect without any device allocation.  No counterpart in the reference: it
  * exists for callers that cannot allocate device memory where they need the
  * energy (a host arena that owns all device memory, stream capture, hard

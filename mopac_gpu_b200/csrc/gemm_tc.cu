@@ -77,17 +77,34 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
 }
 
 // Wait for the phase of `bar` with the given parity; false (and *flag set) on
-// expiry or when another role has already flagged an error.
-__device__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* flag) {
+// expiry (limit_ns of %globaltimer) or when another role has already flagged
+// an error.
+__device__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* flag,
+                          unsigned long long limit_ns = WAIT_NS) {
   if (mbar_try_wait(bar, parity)) return true;
   const unsigned long long t0 = gtimer();
   for (uint32_t it = 1; it != 0; ++it) {
     if (mbar_try_wait(bar, parity)) return true;
     if (*flag) return false;
-    if ((it & 255u) == 0 && gtimer() - t0 > WAIT_NS) break;
+    if ((it & 255u) == 0 && gtimer() - t0 > limit_ns) break;
   }
   *flag = 1;
   return false;
+}
+
+// Self-test of the bounded wait: one thread waits on an mbarrier that nothing
+// arrives at.  out[0] = 1 when the wait gave up, out[1] = nanoseconds waited.
+__global__ void bounded_wait_selftest(unsigned long long limit_ns, long long* out) {
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ int flag;
+  if (threadIdx.x != 0) return;
+  mbar_init(&bar, 1);
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  flag = 0;
+  const unsigned long long t0 = gtimer();
+  const bool ok = mbar_wait(&bar, 0, &flag, limit_ns);
+  out[0] = ok ? 0 : 1;
+  out[1] = (long long)(gtimer() - t0);
 }
 
 // Same, but does not give up because of another role's error (used to drain).
@@ -426,5 +443,17 @@ extern "C" int mb_density_split_ws(int n, int nocc, double occ, const double* c,
       mc, mc, n, n, pad_to(nocc, TK) / TK, occ, 0.0, p, 0, err_dev);
   MB_LAUNCH_CHECK();
   mb_kstat_mark(MB_KSTAT_DENSITY, stream, false);
+  return MB_OK;
+}
+
+// The GEMM's bounded mbarrier wait, made to run out: limit_ns (at most 0.1 s)
+// on a barrier that never completes.  out_dev: two long longs (gave up,
+// nanoseconds waited).  No reference counterpart: a check of this library's
+// failure path that faults nothing.
+extern "C" int mb_selftest_bounded_wait(unsigned long long limit_ns, long long* out_dev, cudaStream_t stream) {
+  if (!out_dev || limit_ns == 0 || limit_ns > 100000000ull)
+    return mb_set_error(MB_ERR_ARG, "mb_selftest_bounded_wait: limit must be 1 ns .. 0.1 s");
+  bounded_wait_selftest<<<1, 32, 0, stream>>>(limit_ns, out_dev);
+  MB_LAUNCH_CHECK();
   return MB_OK;
 }

@@ -120,3 +120,13 @@ def test_fock2_workspace_is_checked_before_any_gpu_work(libpath):
     assert b"mb_fock2_ws_bytes" in L.mb_last_error()
     assert L.mb_fock2_ws(*args, ctypes.c_void_p(4096 + 8), ctypes.c_size_t(need), None) == 1
     assert b"aligned" in L.mb_last_error()
+
+
+def test_bounded_wait_selftest_checks_its_limit_before_any_gpu_work(libpath):
+    L = ctypes.CDLL(libpath)
+    L.mb_selftest_bounded_wait.restype = ctypes.c_int
+    L.mb_selftest_bounded_wait.argtypes = [ctypes.c_ulonglong, ctypes.c_void_p, ctypes.c_void_p]
+    fake = ctypes.c_void_p(4096)
+    assert L.mb_selftest_bounded_wait(0, fake, None) == 1
+    assert L.mb_selftest_bounded_wait(200000000, fake, None) == 1
+    assert L.mb_selftest_bounded_wait(1000, None, None) == 1
