@@ -47,12 +47,22 @@ def test_h2o_heat_matches_reference_exactly():
 
 
 @pytest.mark.parametrize("name", ["co2_1scf", "propane"])
-def test_carbon_heats_within_known_residual(name):
-    # Carbon-containing heats carry a residual of <1e-3 kcal/mol that sits in
-    # the geometry-only terms (the SCF observables above match every digit).
+def test_keyword_output_heats_within_the_reference_suites_bound(name):
+    """The keyword outputs (tests/keywords/1SCF.out, VECTORS.out) were written
+    by MOPAC2016 21.298M (2021, their banner); the source is 23.1.2
+    (CITATION.cff).  The reference's own harness checks these stored heats
+    against the current build with HOF_ERROR = 0.01 kcal/mol
+    (tests/CMakeLists.txt:18, compare_output.py:244) and warns above 1e-4
+    (compare_output.py:29, :245).  The oracle lands 3.1e-4 (CO2) and 7.9e-4
+    (propane) from them, inside that bound, while the ionisation potentials of
+    the same files match to 1e-7 eV and the current-source API heat (water,
+    above) to 4e-6; the bar here is the reference suite's own 0.01, with the
+    measured residual pinned below 1e-3 so a regression shows."""
     case = G[name]
     s, r = _run(case)
-    assert abs(so.heat_of_formation(s, r) - case["heat"]) < 1.0e-3
+    d = abs(so.heat_of_formation(s, r) - case["heat"])
+    assert d < 1.0e-2
+    assert d < 1.0e-3
 
 
 def test_tight_convergence_is_stable():
