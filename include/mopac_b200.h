@@ -174,6 +174,21 @@ int mb_ctx_device_ptrs(mb_ctx* ctx, double** h, double** w, double** f, double**
                        double** c, double** eigs);
 int mb_ctx_atoms_dev(mb_ctx* ctx, MbAtomsDev* out);
 
+/* Cartesian gradient of the SCF energy at the context's density (dcart,
+ * forces/dcart.F90:16-300, for a molecule, RHF, the default finite
+ * difference: every pair's energy as dhc forms it, forces/dhc.F90, with atom
+ * jj moved 0.5e-4 A along all axes and atom ii 1e-4 A along each).  dxyz:
+ * host array of 3*numat doubles, kcal/mol/A, atom-major.  Post-SCF
+ * corrections (PM7 dispersion, hydrogen bonds) are not included. */
+int mb_ctx_gradient(mb_ctx* ctx, double* dxyz);
+
+/* The same on device arrays: nat_d/coord_d (A) as for mb_hcore_dev, p the
+ * packed density; ws of mb_dcart_ws_bytes(numat) bytes (3 doubles per
+ * atom pair); dxyz_dev 3*numat doubles. */
+size_t mb_dcart_ws_bytes(int numat);
+int mb_dcart_dev(const int* nat_d, const double* coord_d, const MbAtomsDev* at, int numat,
+                 const double* p, double* dxyz_dev, void* ws, size_t ws_bytes, cudaStream_t stream);
+
 /* --------------------------------------------- device-pointer kernels */
 /* Atom layout on the device from host nfirst/nlast (1-based). */
 int mb_atoms_create(int numat, const int* nfirst, const int* nlast, MbAtomsDev* out);

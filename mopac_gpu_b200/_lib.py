@@ -109,6 +109,9 @@ SIGNATURES = {
     "mb_density_dev": ([_I, _I, _D, _P, _I, _P, _P], _I),
     "mb_density_occ_dev": ([_I, _I, _I, _D, _D, _I, _I, _P, _I, _P, _P], _I),
     "mb_selftest_bounded_wait": ([ctypes.c_ulonglong, _P, _P], _I),
+    "mb_ctx_gradient": ([_P, _P], _I),
+    "mb_dcart_ws_bytes": ([_I], ctypes.c_size_t),
+    "mb_dcart_dev": ([_P, _P, ctypes.POINTER(MbAtomsDev), _I, _P, _P, _P, ctypes.c_size_t, _P], _I),
     "mb_pulay_ws_bytes": ([_I], ctypes.c_size_t),
     "mb_pulay_ws": ([_I, _P, _P, _P, _P, _I, _P, _I, _P, _P, _P, _P, _P, _P], _I),
     "mb_osinv": ([_P, _I], _D),

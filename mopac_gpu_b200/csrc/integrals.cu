@@ -873,6 +873,127 @@ __global__ void mz_hcore_diag(MbMzLayout L, const int* __restrict__ nat, const d
 #undef WS
 }
 
+// ---------------------------------------------------------------- gradients
+// Density blocks of the diatomic (atom 1 = jj, atom 2 = ii > jj): atom 1's,
+// atom 2's, and rows of atom 2 by columns of atom 1.
+struct PairDens {
+  double p1[4][4], p2[4][4], p21[4][4];
+};
+
+__device__ __forceinline__ int pairix(int a, int b) {  // 0-based pair index of local orbitals a, b
+  return a > b ? a * (a + 1) / 2 + b : b * (b + 1) / 2 + a;
+}
+
+// Energy of the diatomic in dhc's form (forces/dhc.F90:59-173, a molecule,
+// RHF): h1elec's resonance block, the electron-core blocks, the two-centre
+// Coulomb and exchange terms with the density fixed, helect over the pair's
+// orbitals (doubled), and ccrep's core-core term; eV.  Like dhc it leaves out
+// every term that does not depend on the pair's geometry.
+__device__ double dhc_energy(int n1, int n2, const double* x1, const double* x2, const PairDens& d) {
+  const int nor1 = c_P.el[n1].natorb, nor2 = c_P.el[n2].natorb;
+  const int lim1 = nor1 * (nor1 + 1) / 2, lim2 = nor2 * (nor2 + 1) / 2;
+  double di[5][5];
+  h1elec(n1, n2, x1, x2, di);  // di[a][b]: a on atom 1, b on atom 2
+  double h1[10], h2[10], wb[100], enuc = 0.0;
+  for (int x = 0; x < 10; ++x) { h1[x] = 0.0; h2[x] = 0.0; }
+  for (int x = 0; x < 100; ++x) wb[x] = 0.0;
+  const double dx = x2[0] - x1[0], dy = x2[1] - x1[1], dz = x2[2] - x1[2];
+  if (dx * dx + dy * dy + dz * dz >= 0.00002) {
+    double p[4][4];
+    const double r = rotmat(x2, x1, p);  // rotate(ni = atom 2, nj = atom 1) as dhc calls it
+    double ri[23], gab;
+    reppd(n2, n1, r, ri, &gab);
+    w_block(n2, n1, p, ri, wb);  // lim2 x lim1, atom 1's pair index fastest
+    double core[5][3];
+    core_terms(n2, n1, r, core);
+    elenuc(p, core, nor2, nor1, h2, h1);  // atom 2's electrons: e1b; atom 1's: e2a
+    enuc = ccrep(n2, n1, r / PM7_A0, gab);
+  }
+  // Coulomb terms on each atom's block from the other atom's density, and the
+  // energy of the diagonal blocks: sum' P (H + F), F = H + G
+  double e = 0.0;
+  for (int a = 0; a < nor1; ++a)
+    for (int b = 0; b <= a; ++b) {
+      const int q = pairix(a, b);
+      double g = 0.0;
+      for (int x = 0; x < nor2; ++x)
+        for (int y = 0; y < nor2; ++y) g += d.p2[x][y] * wb[pairix(x, y) * lim1 + q];
+      const double wgt = a == b ? 0.5 : 1.0;
+      e += wgt * d.p1[a][b] * (2.0 * h1[q] + g);
+    }
+  for (int a = 0; a < nor2; ++a)
+    for (int b = 0; b <= a; ++b) {
+      const int q = pairix(a, b);
+      double g = 0.0;
+      for (int x = 0; x < nor1; ++x)
+        for (int y = 0; y < nor1; ++y) g += d.p1[x][y] * wb[q * lim1 + pairix(x, y)];
+      const double wgt = a == b ? 0.5 : 1.0;
+      e += wgt * d.p2[a][b] * (2.0 * h2[q] + g);
+    }
+  // the off-diagonal block: resonance and exchange (kab), PA = P / 2
+  for (int mu = 0; mu < nor2; ++mu)
+    for (int nu = 0; nu < nor1; ++nu) {
+      double k = 0.0;
+      for (int la = 0; la < nor2; ++la)
+        for (int si = 0; si < nor1; ++si) k += 0.5 * d.p21[la][si] * wb[pairix(mu, la) * lim1 + pairix(nu, si)];
+      e += d.p21[mu][nu] * (2.0 * di[nu + 1][mu + 1] - k);
+    }
+  (void)lim2;
+  // 2 * helect(PA, H, F) with PA = P/2 is sum' P (H + F) = e
+  return e + enuc;
+}
+
+// dcart (forces/dcart.F90:60-300) for a molecule with the default finite
+// difference (no FORCE keyword): pair q = (ii, jj), jj < ii, with atom jj
+// moved by chnge/2 along all three axes, then atom ii by chnge along each
+// axis in turn; deriv = (E0 - Ek) * fpc_9 / chnge, kcal/mol/A.
+__global__ void dcart_pairs(int numat, const int* __restrict__ nat, const double* __restrict__ coord, MbAtomsDev at,
+                            const double* __restrict__ ptot, double* __restrict__ deriv) {
+  const long long npair = (long long)numat * (numat - 1) / 2;
+  const double chnge = 1.0e-4, chnge2 = chnge * 0.5;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < npair;
+       q += (long long)gridDim.x * blockDim.x) {
+    long long i = (long long)((sqrt(8.0 * (double)q + 1.0) + 1.0) * 0.5);
+    while (i * (i - 1) / 2 > q) --i;
+    while ((i + 1) * i / 2 <= q) ++i;
+    const int ii = (int)i, jj = (int)(q - i * (i - 1) / 2);
+    const int f1 = at.first[jj], f2 = at.first[ii], no1 = at.nor[jj], no2 = at.nor[ii];
+    PairDens d;
+    for (int a = 0; a < 4; ++a)
+      for (int b = 0; b < 4; ++b) {
+        d.p1[a][b] = (a < no1 && b < no1) ? ptot[mb_tri(f1 + (a > b ? a : b), f1 + (a > b ? b : a))] : 0.0;
+        d.p2[a][b] = (a < no2 && b < no2) ? ptot[mb_tri(f2 + (a > b ? a : b), f2 + (a > b ? b : a))] : 0.0;
+        d.p21[a][b] = (a < no2 && b < no1) ? ptot[mb_tri(f2 + a, f1 + b)] : 0.0;
+      }
+    double x1[3], x2[3];
+    for (int k = 0; k < 3; ++k) {
+      x1[k] = coord[3 * jj + k] + chnge2;
+      x2[k] = coord[3 * ii + k];
+    }
+    const int n1 = nat[jj], n2 = nat[ii];
+    const double aa = dhc_energy(n1, n2, x1, x2, d);
+    for (int k = 0; k < 3; ++k) {
+      x2[k] = x2[k] + chnge;
+      const double ee = dhc_energy(n1, n2, x1, x2, d);
+      x2[k] = x2[k] - chnge2;
+      x2[k] = x2[k] - chnge2;
+      deriv[3 * q + k] = (aa - ee) * PM7_FPC9 / chnge;
+    }
+  }
+}
+
+// dxyz of atom a in dcart's accumulation order: the pairs (a, jj < a), then
+// the pairs (ii > a, a), each ascending.
+__global__ void dcart_sum(int numat, const double* __restrict__ deriv, double* __restrict__ dxyz) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= 3 * numat) return;
+  const int a = t / 3, k = t - 3 * a;
+  double g = 0.0;
+  for (int b = 0; b < a; ++b) g = g - deriv[3 * ((long long)a * (a - 1) / 2 + b) + k];
+  for (int b = a + 1; b < numat; ++b) g = g + deriv[3 * ((long long)b * (b - 1) / 2 + a) + k];
+  dxyz[t] = g;
+}
+
 bool g_params_uploaded = false;
 
 int upload_params() {
@@ -965,5 +1086,32 @@ extern "C" int mb_mz_hcore_dev(const MbMzLayout* L, const int* nat_d, const doub
   MB_LAUNCH_CHECK();
   enuc_sum<<<1, 1024, 0, stream>>>(L->numat, enuc_atom, enuclr_dev);
   MB_LAUNCH_CHECK();
+  return MB_OK;
+}
+
+extern "C" size_t mb_dcart_ws_bytes(int numat) {
+  if (numat < 2) return 0;
+  return sizeof(double) * 3 * ((size_t)numat * (numat - 1) / 2);
+}
+
+// Cartesian gradient of the SCF energy (dcart, forces/dcart.F90:16-300, a
+// molecule, RHF): dxyz_dev[3a + k] in kcal/mol/A for the packed density p.
+extern "C" int mb_dcart_dev(const int* nat_d, const double* coord_d, const MbAtomsDev* at, int numat, const double* p,
+                            double* dxyz_dev, void* ws, size_t ws_bytes, cudaStream_t stream) {
+  if (!at || numat <= 0 || !nat_d || !coord_d || !p || !dxyz_dev) return mb_set_error(MB_ERR_ARG, "mb_dcart_dev: bad args");
+  if (ws_bytes < mb_dcart_ws_bytes(numat) || (numat > 1 && !ws))
+    return mb_set_error(MB_ERR_ARG, "mb_dcart_dev: workspace smaller than mb_dcart_ws_bytes(numat)");
+  MB_TRY(upload_params());
+  const long long npair = (long long)numat * (numat - 1) / 2;
+  if (npair > 0) {
+    int blocks = (int)((npair + 127) / 128);
+    if (blocks > 148 * 32) blocks = 148 * 32;
+    dcart_pairs<<<blocks, 128, 0, stream>>>(numat, nat_d, coord_d, *at, p, (double*)ws);
+    MB_LAUNCH_CHECK();
+    dcart_sum<<<(3 * numat + 127) / 128, 128, 0, stream>>>(numat, (const double*)ws, dxyz_dev);
+    MB_LAUNCH_CHECK();
+  } else {
+    MB_CUDA(cudaMemsetAsync(dxyz_dev, 0, sizeof(double) * 3 * (size_t)numat, stream));
+  }
   return MB_OK;
 }

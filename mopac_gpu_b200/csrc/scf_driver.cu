@@ -371,6 +371,25 @@ extern "C" int mb_ctx_device_ptrs(mb_ctx* c, double** h, double** w, double** f,
   return MB_OK;
 }
 
+extern "C" size_t mb_dcart_ws_bytes(int numat);
+extern "C" int mb_dcart_dev(const int* nat_d, const double* coord_d, const MbAtomsDev* at, int numat, const double* p,
+                            double* dxyz_dev, void* ws, size_t ws_bytes, cudaStream_t stream);
+
+extern "C" int mb_ctx_gradient(mb_ctx* c, double* dxyz) {
+  if (!c || !dxyz) return mb_set_error(MB_ERR_ARG, "mb_ctx_gradient: bad args");
+  if (!c->have_hw) return mb_set_error(MB_ERR_ARG, "mb_ctx_gradient: call mb_ctx_hcore or mb_ctx_set_hw first");
+  const size_t wsb = mb_dcart_ws_bytes(c->numat), outb = sizeof(double) * 3 * (size_t)c->numat;
+  char* ws = nullptr;
+  MB_CUDA(cudaMallocAsync((void**)&ws, wsb + outb + 256, c->stream));
+  double* out = (double*)(ws + ((wsb + 255) & ~(size_t)255));
+  int rc = mb_dcart_dev(c->d_nat, c->d_coord, &c->atoms, c->numat, c->p, out, ws, wsb, c->stream);
+  if (rc == MB_OK && cudaMemcpyAsync(dxyz, out, outb, cudaMemcpyDeviceToHost, c->stream) != cudaSuccess)
+    rc = mb_set_error(MB_ERR_CUDA, "mb_ctx_gradient: copy");
+  cudaFreeAsync(ws, c->stream);
+  if (rc == MB_OK) MB_CUDA(cudaStreamSynchronize(c->stream));
+  return rc;
+}
+
 extern "C" int mb_ctx_atoms_dev(mb_ctx* c, MbAtomsDev* out) {
   if (!c || !out) return mb_set_error(MB_ERR_ARG, "null context");
   *out = c->atoms;

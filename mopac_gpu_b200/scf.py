@@ -117,6 +117,13 @@ class ScfContext:
         check(lib().mb_ctx_get_density(self._h, p.ctypes.data))
         return p
 
+    def gradient(self) -> np.ndarray:
+        """Cartesian gradient of the SCF energy at the current density,
+        (numat, 3) kcal/mol/A (dcart, forces/dcart.F90, for a molecule)."""
+        g = np.empty((len(self.nat), 3))
+        check(lib().mb_ctx_gradient(self._h, g.ctypes.data))
+        return g
+
     def vectors(self):
         c = np.empty((self.norbs, self.norbs), order="F")
         e = np.empty(self.norbs)

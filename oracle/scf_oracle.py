@@ -707,6 +707,64 @@ def fixed_point_certificate(s: System, p: np.ndarray, steps: int = 3) -> dict:
     return dict(r=rs, rho=rho, bound=bound, eigs=eigs0, heat_at_p=heats[0], heat_last=heats[-1], p_last=pk)
 
 
+# ---------------------------------------------------------------- gradients
+def _pair_system(nat2, xyz2) -> System:
+    """The two atoms alone (electron count not checked: dhc's diatomic need
+    not be closed shell)."""
+    L = lib()
+    nat2 = np.ascontiguousarray(nat2, dtype=np.int32)
+    xyz2 = np.ascontiguousarray(xyz2, dtype=np.float64).reshape(2, 3)
+    nfirst, nlast = np.zeros(2, np.int32), np.zeros(2, np.int32)
+    norbs = L.orc_layout(2, nat2, nfirst, nlast)
+    s = System(nat=nat2, coord=xyz2, nfirst=nfirst, nlast=nlast, norbs=norbs, nclose=0)
+    hcore(s)
+    return s
+
+
+def _pair_energy(nat2, x1, x2, p_loc, pa_loc) -> float:
+    """forces/dhc.F90 for a molecule, RHF: the diatomic's energy with its
+    density blocks fixed.  Built from the whole two-atom system, so it also
+    holds the one-centre terms; those do not depend on the geometry and drop
+    out of every difference dcart takes."""
+    s = _pair_system(nat2, np.vstack([x1, x2]))
+    f = s.h.copy()
+    fock2(s, f, p_loc, pa_loc)
+    return 2.0 * helect(s.norbs, pa_loc, s.h, f) + s.enuclr
+
+
+def dcart(s: System, p: np.ndarray) -> np.ndarray:
+    """forces/dcart.F90:60-300 for a molecule (id = 0), RHF, the default
+    finite difference (no FORCE keyword): for every pair (ii, jj), jj < ii,
+    atom jj moves chnge/2 along all three axes (:283-286), then atom ii moves
+    chnge along each axis in turn (:292-296); deriv = (aa - ee) fpc_9 / chnge
+    (:297) is subtracted from ii's gradient and added to jj's.  Returns
+    (numat, 3) kcal/mol/A, accumulated in the reference's order."""
+    chnge = 1.0e-4
+    chnge2 = chnge * 0.5
+    n = s.numat
+    P = unpack(p, s.norbs)
+    dxyz = np.zeros((n, 3))
+    for ii in range(n):
+        for jj in range(ii):
+            idx = np.concatenate([np.arange(s.nfirst[jj] - 1, s.nlast[jj]),
+                                  np.arange(s.nfirst[ii] - 1, s.nlast[ii])])
+            p_loc = pack(P[np.ix_(idx, idx)])
+            pa_loc = 0.5 * p_loc
+            nat2 = s.nat[[jj, ii]]
+            x1 = s.coord[jj] + chnge2
+            x2 = s.coord[ii].copy()
+            aa = _pair_energy(nat2, x1, x2, p_loc, pa_loc)
+            for k in range(3):
+                x2[k] = x2[k] + chnge
+                ee = _pair_energy(nat2, x1, x2, p_loc, pa_loc)
+                x2[k] = x2[k] - chnge2
+                x2[k] = x2[k] - chnge2
+                deriv = (aa - ee) * FPC9 / chnge
+                dxyz[ii, k] = dxyz[ii, k] - deriv
+                dxyz[jj, k] = dxyz[jj, k] + deriv
+    return dxyz
+
+
 # ---------------------------------------------------------------- properties
 def mulliken_charges(s: System, p: np.ndarray) -> np.ndarray:
     """NDDO net charges: core charge minus the diagonal density on the atom."""

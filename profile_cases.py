@@ -13,6 +13,7 @@ has no FP64 figure.
 
 Cases (sizes of the benchmark configurations):
   fock2         Fock build, (H2O)512: 8 (n2elec + 4 mpack) bytes
+  dcart         gradient (dcart), (H2O)512: four pair energies per atom pair
   helect, cnvg  energy and extrapolation, n = 3072: 24 mpack / 24 mpack + 8 n bytes
   density64     P = 2 C_o C_o^T FP64, n = 3072, k = 2048: n^2 k flops
   density_split same with the three-product BF16 split on tcgen05
@@ -166,7 +167,7 @@ def run_cases(names, reps):
     pk = peaks()
     out = []
     hbm, bf16, src = pk["hbm_gbs"], pk["bf16_tflops"], pk["source"]
-    need_c1 = any(c in names for c in ("fock2", "helect", "cnvg", "density64", "density_split", "eigh", "eigh_cusolver",
+    need_c1 = any(c in names for c in ("fock2", "dcart", "helect", "cnvg", "density64", "density_split", "eigh", "eigh_cusolver",
                                        "pseudo_diag", "pulay"))
     c1 = C1() if need_c1 else None
     fp64 = fp64_peak_tflops() if any(c in names for c in ("density64", "gemm64", "eigh")) else None
@@ -178,6 +179,19 @@ def run_cases(names, reps):
                                                vp(c1.w), 0.0, 0, vp(ws), wsb, s())), reps)
         out.append(line("fock2", ms, 8 * (c1.ctx.n2elec + 4 * c1.mpack), "GB/s", "hbm", hbm, src,
                         config="(H2O)512, n = 3072"))
+    if "dcart" in names:
+        wsb = L.mb_dcart_ws_bytes(len(c1.ctx.nat))
+        ws = torch.empty(wsb, dtype=torch.uint8, device="cuda")
+        g = torch.empty(3 * len(c1.ctx.nat), dtype=torch.float64, device="cuda")
+        nat_d = torch.as_tensor(np.asarray(c1.ctx.nat, np.int32), device="cuda")
+        xyz_d = torch.as_tensor(np.asarray(c1.ctx.coord, np.float64).ravel(), device="cuda")
+        ms = timed(lambda: check(L.mb_dcart_dev(vp(nat_d), vp(xyz_d), ctypes.byref(c1.atoms), len(c1.ctx.nat),
+                                                vp(c1.p), vp(g), vp(ws), wsb, s())), reps)
+        npair = len(c1.ctx.nat) * (len(c1.ctx.nat) - 1) // 2
+        out.append({"case": "dcart", "ms": round(ms, 4), "atom_pairs": npair,
+                    "pair_energies_per_s": 4 * npair / (ms * 1e-3),
+                    "config": "(H2O)512 gradient: four pair energies (integrals, Coulomb, exchange, "
+                              "core-core) per atom pair, then the per-atom ordered sums"})
     if "helect" in names:
         o = torch.zeros(1, dtype=torch.float64, device="cuda")
         ms = timed(lambda: check(L.mb_helect_dev(c1.n, vp(c1.pa), vp(c1.h), vp(c1.f), vp(o), s())), reps)
@@ -469,7 +483,7 @@ def guess_cases(names, reps, bf16, src):
     return out
 
 
-ALL = ["fock2", "helect", "cnvg", "density64", "density_split", "gemm64", "gemm_split", "eigh", "eigh_cusolver", "eigh_rand",
+ALL = ["fock2", "dcart", "helect", "cnvg", "density64", "density_split", "gemm64", "gemm_split", "eigh", "eigh_cusolver", "eigh_rand",
        "pseudo_diag",
        "pulay", "mz_density", "mz_helecz", "mz_cnvgz", "mz_fock", "mz_diagg1", "mz_diagg2",
        "guess_features", "guess_forward", "guess_train", "guess_predict", "batch"]
