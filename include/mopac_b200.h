@@ -384,6 +384,11 @@ int mb_mz_lmos_create(int numat, const int* iorbs, int nlmo, const int* ncf, con
 /* Rebuilds the per-atom index after diagg2 has grown LMOs (mb_mz_density_dev
  * reads it). */
 int mb_mz_lmos_refresh(int numat, const int* iorbs_host, MbMzLmos* lmos);
+/* The same index built on the device, in place, on `stream` (iorbs_dev: a
+ * device array, e.g. MbMzLayout.iorbs): each atom's LMOs ascending, as the
+ * host version orders them.  Synchronises the stream once to report
+ * malformed LMOs (MB_ERR_ARG). */
+int mb_mz_lmos_refresh_dev(int numat, const int* iorbs_dev, MbMzLmos* lmos, cudaStream_t stream);
 int mb_mz_lmos_destroy(MbMzLmos* lmos);
 /* density_for_MOZYME(p, mode, nclose, partp) (MOZYME/density_for_MOZYME.F90:16):
  * mode 0: P = 2 sum_LMO c c^T; -1: P = -2 (sum - partp/2); 1: P = 2 (sum +

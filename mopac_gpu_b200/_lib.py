@@ -132,6 +132,7 @@ SIGNATURES = {
     "mb_mz_idiag": ([ctypes.POINTER(MbMzLayout), _P], _I),
     "mb_mz_lmos_create": ([_I, _P, _I, _P, _P, _P, _P, _P, _LL, _LL, ctypes.POINTER(MbMzLmos)], _I),
     "mb_mz_lmos_refresh": ([_I, _P, ctypes.POINTER(MbMzLmos)], _I),
+    "mb_mz_lmos_refresh_dev": ([_I, _P, ctypes.POINTER(MbMzLmos), _P], _I),
     "mb_mz_diagg2_dev": ([ctypes.POINTER(MbMzLayout), ctypes.POINTER(MbMzLmos), ctypes.POINTER(MbMzLmos), _P, _P,
                           _LL, _P, _P, _I, _P, _P, ctypes.POINTER(_D), ctypes.POINTER(_LL), _P], _I),
     "mb_mz_lmos_destroy": ([ctypes.POINTER(MbMzLmos)], _I),

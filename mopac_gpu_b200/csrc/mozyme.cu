@@ -392,14 +392,116 @@ int grid_for(long long n) {
 }
 
 template <class T>
-int upload(const std::vector<T>& v, const T** out) {
+int upload(const std::vector<T>& v, const T** out, size_t capacity = 0) {
   T* d = nullptr;
-  if (!v.empty()) {
-    MB_CUDA(cudaMalloc(&d, sizeof(T) * v.size()));
-    MB_CUDA(cudaMemcpy(d, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice));
+  const size_t n = v.size() > capacity ? v.size() : capacity;
+  if (n > 0) {
+    MB_CUDA(cudaMalloc(&d, sizeof(T) * n));
+    if (!v.empty()) MB_CUDA(cudaMemcpy(d, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice));
   }
   *out = d;
   return MB_OK;
+}
+
+// ---------------------------------------------------------------- LMO index on the device
+// The per-atom index (atom_ptr, atom_lmo, atom_coff) rebuilt from the LMOs'
+// own arrays, as build_atom_index does on the host: each atom's LMOs in
+// ascending order with the offset of the atom's coefficients in the LMO.
+
+// Per LMO: count its atoms, and the coefficient offset of every entry.
+__global__ void mzr_count(int numat, int nlmo, const int* __restrict__ iorbs, const int* __restrict__ ncf,
+                          const int* __restrict__ nncf, const int* __restrict__ icocc, const int* __restrict__ ncocc,
+                          long long nentries, long long ncoeff, int* __restrict__ cnt, int* __restrict__ ecoff,
+                          int* __restrict__ err) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nlmo) return;
+  long long c = ncocc[i];
+  const long long j0 = nncf[i], j1 = j0 + ncf[i];
+  if (j0 < 0 || j1 > nentries) { atomicOr(err, 1); return; }
+  for (long long jj = j0; jj < j1; ++jj) {
+    const int a = icocc[jj] - 1;
+    if (a < 0 || a >= numat) { atomicOr(err, 1); continue; }
+    atomicAdd(&cnt[a], 1);
+    ecoff[jj] = (int)c;
+    c += iorbs[a];
+  }
+  if (c > ncoeff) atomicOr(err, 2);
+}
+
+// Exclusive scan of the counts into atom_ptr (numat + 1 entries); one CTA.
+__global__ void mzr_scan(int numat, const int* __restrict__ cnt, int* __restrict__ ptr) {
+  __shared__ int s_warp[32];
+  __shared__ int s_carry;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+  if (tid == 0) s_carry = 0;
+  __syncthreads();
+  for (int b0 = 0; b0 < numat; b0 += blockDim.x) {
+    const int a = b0 + tid;
+    int v = a < numat ? cnt[a] : 0;
+    int incl = v;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const int t = __shfl_up_sync(0xffffffffu, incl, d);
+      if (lane >= d) incl += t;
+    }
+    if (lane == 31) s_warp[warp] = incl;
+    __syncthreads();
+    int off = s_carry;
+    for (int w = 0; w < warp; ++w) off += s_warp[w];
+    if (a < numat) ptr[a] = off + incl - v;
+    __syncthreads();
+    if (tid == 0) {
+      int tot = 0;
+      for (int w = 0; w < nw; ++w) tot += s_warp[w];
+      s_carry += tot;
+    }
+    __syncthreads();
+  }
+  if (tid == 0) ptr[numat] = s_carry;
+}
+
+// Per LMO: drop every entry into its atom's segment (any order).
+__global__ void mzr_scatter(int numat, int nlmo, const int* __restrict__ ncf, const int* __restrict__ nncf,
+                            const int* __restrict__ icocc, long long nentries, const int* __restrict__ ptr,
+                            const int* __restrict__ ecoff, int* __restrict__ cursor,
+                            unsigned long long* __restrict__ tmp, int* __restrict__ err) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nlmo) return;
+  const long long j0 = nncf[i], j1 = j0 + ncf[i];
+  if (j0 < 0 || j1 > nentries) return;
+  for (long long jj = j0; jj < j1; ++jj) {
+    const int a = icocc[jj] - 1;
+    if (a < 0 || a >= numat) continue;
+    const long long at = (long long)ptr[a] + atomicAdd(&cursor[a], 1);
+    if (at >= nentries) { atomicOr(err, 4); continue; }  // overlapping atom lists
+    tmp[at] = ((unsigned long long)(unsigned)i << 32) | (unsigned)ecoff[jj];
+  }
+}
+
+// Per atom: each entry's place is the number of entries with a smaller LMO
+// index (ties, which well-formed LMOs do not have, broken by position).
+__global__ void mzr_order(const int* __restrict__ ptr, const unsigned long long* __restrict__ tmp, long long nentries,
+                          int* __restrict__ atom_lmo, int* __restrict__ atom_coff) {
+  constexpr int kStage = 2048;
+  __shared__ unsigned s_key[kStage];
+  const int a = blockIdx.x;
+  const int b = ptr[a], m = ptr[a + 1] - b;
+  if ((long long)b + m > nentries) return;  // flagged by mzr_scatter
+  const bool staged = m <= kStage;
+  if (staged)
+    for (int e = threadIdx.x; e < m; e += blockDim.x) s_key[e] = (unsigned)(tmp[b + e] >> 32);
+  __syncthreads();
+  for (int e = threadIdx.x; e < m; e += blockDim.x) {
+    const unsigned long long v = tmp[b + e];
+    const unsigned key = (unsigned)(v >> 32);
+    int rank = 0;
+    for (int f = 0; f < m; ++f) {
+      const unsigned k2 = staged ? s_key[f] : (unsigned)(tmp[b + f] >> 32);
+      rank += (k2 < key) || (k2 == key && f < e);
+    }
+    atom_lmo[b + rank] = (int)key;
+    atom_coff[b + rank] = (int)(unsigned)(v & 0xffffffffull);
+  }
 }
 
 }  // namespace
@@ -568,9 +670,10 @@ extern "C" int mb_mz_lmos_create(int numat, const int* iorbs, int nlmo, const in
   out->nlmo = nlmo;
   out->nentries = icocc_dim;
   out->ncoeff = cocc_dim;
+  // the index arrays hold up to icocc_dim entries, so a refresh never reallocates them
   int rc = upload(cnt, &out->atom_ptr);
-  if (rc == MB_OK) rc = upload(lmo, &out->atom_lmo);
-  if (rc == MB_OK) rc = upload(coff, &out->atom_coff);
+  if (rc == MB_OK) rc = upload(lmo, &out->atom_lmo, (size_t)icocc_dim);
+  if (rc == MB_OK) rc = upload(coff, &out->atom_coff, (size_t)icocc_dim);
   if (rc == MB_OK) rc = upload(cv, &out->cocc);
   if (rc == MB_OK) rc = upload(vncf, &out->ncf);
   if (rc == MB_OK) rc = upload(vnncf, &out->nncf);
@@ -596,8 +699,59 @@ extern "C" int mb_mz_lmos_refresh(int numat, const int* iorbs, MbMzLmos* Q) {
   cudaFree((void*)Q->atom_coff);
   Q->atom_ptr = Q->atom_lmo = Q->atom_coff = nullptr;
   MB_TRY(upload(cnt, &Q->atom_ptr));
-  MB_TRY(upload(lmo, &Q->atom_lmo));
-  MB_TRY(upload(coff, &Q->atom_coff));
+  MB_TRY(upload(lmo, &Q->atom_lmo, (size_t)Q->nentries));
+  MB_TRY(upload(coff, &Q->atom_coff, (size_t)Q->nentries));
+  return MB_OK;
+}
+
+// mb_mz_lmos_refresh on the device: the same index, in place (the index
+// arrays hold nentries entries from mb_mz_lmos_create), on `stream`, with
+// iorbs a device array.  Synchronises the stream once to report malformed
+// LMOs as the host version does.
+extern "C" int mb_mz_lmos_refresh_dev(int numat, const int* iorbs_dev, MbMzLmos* Q, cudaStream_t stream) {
+  if (!Q || !iorbs_dev || numat <= 0) return mb_set_error(MB_ERR_ARG, "mb_mz_lmos_refresh_dev: bad args");
+  const int n = Q->nlmo;
+  const long long ne = Q->nentries;
+  const size_t bytes = sizeof(int) * (2 * (size_t)numat + (size_t)ne + 8) + sizeof(unsigned long long) * (size_t)ne;
+  char* ws = nullptr;
+  MB_CUDA(cudaMallocAsync((void**)&ws, bytes, stream));
+  unsigned long long* tmp = (unsigned long long*)ws;
+  int* cnt = (int*)(tmp + ne);
+  int* cursor = cnt + numat;
+  int* ecoff = cursor + numat;
+  int* err = ecoff + ne;
+  int rc = MB_OK;
+  if (cudaMemsetAsync(cnt, 0, sizeof(int) * 2 * (size_t)numat, stream) != cudaSuccess ||
+      cudaMemsetAsync(err, 0, sizeof(int), stream) != cudaSuccess)
+    rc = mb_set_error(MB_ERR_CUDA, "mb_mz_lmos_refresh_dev: memset");
+  const int nb = (n + 127) / 128;
+  if (rc == MB_OK && n > 0) {
+    mzr_count<<<nb, 128, 0, stream>>>(numat, n, iorbs_dev, Q->ncf, Q->nncf, Q->icocc, Q->ncocc, ne, Q->ncoeff, cnt,
+                                      ecoff, err);
+    if (cudaGetLastError() != cudaSuccess) rc = mb_set_error(MB_ERR_CUDA, "mb_mz_lmos_refresh_dev: count");
+  }
+  if (rc == MB_OK) {
+    mzr_scan<<<1, 1024, 0, stream>>>(numat, cnt, (int*)Q->atom_ptr);
+    if (cudaGetLastError() != cudaSuccess) rc = mb_set_error(MB_ERR_CUDA, "mb_mz_lmos_refresh_dev: scan");
+  }
+  if (rc == MB_OK && n > 0) {
+    mzr_scatter<<<nb, 128, 0, stream>>>(numat, n, Q->ncf, Q->nncf, Q->icocc, ne, Q->atom_ptr, ecoff, cursor, tmp,
+                                        err);
+    if (cudaGetLastError() != cudaSuccess) rc = mb_set_error(MB_ERR_CUDA, "mb_mz_lmos_refresh_dev: scatter");
+  }
+  if (rc == MB_OK) {
+    mzr_order<<<numat, 128, 0, stream>>>(Q->atom_ptr, tmp, ne, (int*)Q->atom_lmo, (int*)Q->atom_coff);
+    if (cudaGetLastError() != cudaSuccess) rc = mb_set_error(MB_ERR_CUDA, "mb_mz_lmos_refresh_dev: order");
+  }
+  int herr = 0;
+  if (rc == MB_OK && (cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
+                      cudaStreamSynchronize(stream) != cudaSuccess))
+    rc = mb_set_error(MB_ERR_CUDA, "mb_mz_lmos_refresh_dev: status");
+  cudaFreeAsync(ws, stream);
+  if (rc != MB_OK) return rc;
+  if (herr & 1) return mb_set_error(MB_ERR_ARG, "MOZYME LMOs: atom number out of range");
+  if (herr & 2) return mb_set_error(MB_ERR_ARG, "MOZYME LMOs: cocc too short for the atom lists");
+  if (herr & 4) return mb_set_error(MB_ERR_ARG, "MOZYME LMOs: atom lists overlap in icocc");
   return MB_OK;
 }
 

@@ -281,6 +281,7 @@ extern "C" int mb_mz_cnvgz_ws(int norbs, long long mpack, double* pnew, double* 
                               cudaStream_t stream);
 extern "C" int mb_mz_idiag(const MbMzLayout* layout, long long* idiag);
 extern "C" int mb_mz_lmos_refresh(int numat, const int* iorbs_host, MbMzLmos* lmos);
+extern "C" int mb_mz_lmos_refresh_dev(int numat, const int* iorbs_dev, MbMzLmos* lmos, cudaStream_t stream);
 
 extern "C" void mb_mz_scf_opts_default(mb_mz_scf_opts* o) {
   o->scfcrt = 1.0e-2;
@@ -388,8 +389,8 @@ extern "C" int mb_mz_scf_run(const MbMzLayout* L, const int* iorbs_host, MbMzLmo
     // tidy's compression (iter_for_MOZYME.F90:221, :326), then the index
     MB_TRY(mb_mz_tidy_dev(occ, L->iorbs, thresh, s));
     MB_TRY(mb_mz_tidy_dev(vir, L->iorbs, thresh, s));
-    MB_TRY(mb_mz_lmos_refresh(numat, iorbs_host, occ));
-    MB_TRY(mb_mz_lmos_refresh(numat, iorbs_host, vir));
+    MB_TRY(mb_mz_lmos_refresh_dev(numat, L->iorbs, occ, s));
+    MB_TRY(mb_mz_lmos_refresh_dev(numat, L->iorbs, vir, s));
     double eo = 0.0, ev = 0.0;
     MB_TRY(mb_mz_check_dev(occ, L->iorbs, norm_o, &eo, s));
     MB_TRY(mb_mz_check_dev(vir, L->iorbs, norm_v, &ev, s));
@@ -406,8 +407,8 @@ extern "C" int mb_mz_scf_run(const MbMzLayout* L, const int* iorbs_host, MbMzLmo
     long long nrej = 0;
     MB_TRY(mb_mz_diagg2_dev(L, occ, vir, ifmo, fmo, nij, eigs, eigv, idiagg, ctl, nrejct, &sumb, &nrej, s));
     nrej_total += nrej;
-    MB_TRY(mb_mz_lmos_refresh(numat, iorbs_host, occ));
-    MB_TRY(mb_mz_lmos_refresh(numat, iorbs_host, vir));
+    MB_TRY(mb_mz_lmos_refresh_dev(numat, L->iorbs, occ, s));
+    MB_TRY(mb_mz_lmos_refresh_dev(numat, L->iorbs, vir, s));
     MB_TRY(mb_mz_density_dev(L, occ, 0, nullptr, p, s));
     ++idiagg;
     ++niter;
@@ -420,8 +421,8 @@ extern "C" int mb_mz_scf_run(const MbMzLayout* L, const int* iorbs_host, MbMzLmo
         MB_TRY(mb_mz_diagg2_dev(L, occ, vir, hb_ifmo, hb_fmo, nhb_ij, eigs, eigv, idiagg, ctl2, nrejct, &sumb, &nrej,
                                 s));
         nrej_total += nrej;
-        MB_TRY(mb_mz_lmos_refresh(numat, iorbs_host, occ));
-        MB_TRY(mb_mz_lmos_refresh(numat, iorbs_host, vir));
+        MB_TRY(mb_mz_lmos_refresh_dev(numat, L->iorbs, occ, s));
+        MB_TRY(mb_mz_lmos_refresh_dev(numat, L->iorbs, vir, s));
         if (idiagg % 2 == 1) ++idiagg;
       }
     }

@@ -616,3 +616,44 @@ def test_gpu_water_lmos_are_the_isolated_molecule_lmos():
     Qo.close()
     Qv.close()
     L.close()
+
+
+@pytest.mark.gpu
+def test_gpu_lmo_index_refresh_on_the_device_is_the_host_one():
+    """mb_mz_lmos_refresh_dev (count, scan, scatter, rank by LMO) rebuilds the
+    per-atom LMO index exactly as the host builder does, on LMOs that the
+    SCF's rotations have grown."""
+    torch = _need_gpu()
+    import ctypes
+    from mopac_gpu_b200 import mozyme
+    from mopac_gpu_b200._lib import check, lib
+    from mopac_gpu_b200.mozyme import _device_view
+    nat, xyz, _ = workloads.water_box(32, seed=3)
+    s = oracle_system(nat, xyz)
+    iorbs, occ, vir = mozyme.water_lmos(nat, xyz, pad_atoms=40)
+    c1, c2 = mo.cutoffs(len(nat))
+    mp, nb = mo.layout(iorbs, s.coord, c1, c2)
+    hb = mo.dense_to_blocks(so.unpack(s.h, s.norbs), iorbs, nb, mp)
+    wz = mo.w_stored(iorbs, nb, s.w)
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    L = mozyme.Layout(iorbs, s.coord, c1, c2)
+    Qo, Qv = mozyme.Lmos(L, occ), mozyme.Lmos(L, vir)
+    mozyme.scf_run(L, Qo, Qv, dev(s.coord), dev(wz), dev(hb), s.enuclr, s.atheat)
+
+    def index(Q):
+        torch.cuda.synchronize()
+        ptr = _device_view(Q.s.atom_ptr, len(nat) + 1, "<i4").cpu().numpy().copy()
+        tot = int(ptr[-1])
+        return (ptr, _device_view(Q.s.atom_lmo, tot, "<i4").cpu().numpy().copy(),
+                _device_view(Q.s.atom_coff, tot, "<i4").cpu().numpy().copy())
+
+    for Q in (Qo, Qv):
+        Q.refresh()
+        host = index(Q)
+        check(lib().mb_mz_lmos_refresh_dev(len(nat), ctypes.c_void_p(L.s.iorbs), ctypes.byref(Q.s), None))
+        devi = index(Q)
+        for a, b in zip(host, devi):
+            np.testing.assert_array_equal(a, b)
+    Qo.close()
+    Qv.close()
+    L.close()
