@@ -628,9 +628,9 @@ def test_gpu_lmo_index_refresh_on_the_device_is_the_host_one():
     from mopac_gpu_b200 import mozyme
     from mopac_gpu_b200._lib import check, lib
     from mopac_gpu_b200.mozyme import _device_view
-    nat, xyz, _ = workloads.water_box(32, seed=3)
+    nat, xyz, _ = workloads.water_box(16, seed=3)
     s = oracle_system(nat, xyz)
-    iorbs, occ, vir = mozyme.water_lmos(nat, xyz, pad_atoms=40)
+    iorbs, occ, vir = mozyme.water_lmos(nat, xyz, pad_atoms=len(nat) - 3)
     c1, c2 = mo.cutoffs(len(nat))
     mp, nb = mo.layout(iorbs, s.coord, c1, c2)
     hb = mo.dense_to_blocks(so.unpack(s.h, s.norbs), iorbs, nb, mp)
