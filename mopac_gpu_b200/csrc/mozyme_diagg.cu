@@ -130,24 +130,33 @@ __global__ void __launch_bounds__(MZ_T) mzd_virtual(DiagArgs A) {
   unsigned* near2 = s_bits + 2 * words;
   for (int w = tid; w < 3 * words; w += MZ_T) s_bits[w] = 0u;
   __syncthreads();
+  for (int t = tid; t < nce; t += MZ_T) s_atom[t] = A.vir.icocc[nn + t] - 1;
+  __syncthreads();
   if (tid == 0) {
     int pos = 0;
     for (int t = 0; t < nce; ++t) {
-      const int a = A.vir.icocc[nn + t] - 1;
-      s_atom[t] = a;
       s_wpos[t] = pos;
-      for (int x = 0; x < L.iorbs[a]; ++x) s_eat[pos + x] = t;
-      pos += L.iorbs[a];
-      // insertion into the sorted copy (short lists)
-      int q = t;
-      while (q > 0 && s_sorted[q - 1] > a) { s_sorted[q] = s_sorted[q - 1]; s_sidx[q] = s_sidx[q - 1]; --q; }
-      s_sorted[q] = a;
-      s_sidx[q] = t;
+      pos += L.iorbs[s_atom[t]];
     }
     s_wpos[nce] = pos;
     s_sumt = 0.0;
     s_tiny = 0.0;
   }
+  // the sorted copy: each atom's place is the number of atoms before it in
+  // order (ties by list position, which an LMO's distinct atoms never need)
+  for (int t = tid; t < nce; t += MZ_T) {
+    const int a = s_atom[t];
+    int r = 0;
+    for (int u = 0; u < nce; ++u) {
+      const int b = s_atom[u];
+      r += (b < a) || (b == a && u < t);
+    }
+    s_sorted[r] = a;
+    s_sidx[r] = t;
+  }
+  __syncthreads();
+  for (int t = tid; t < nce; t += MZ_T)
+    for (int x = 0; x < L.iorbs[s_atom[t]]; ++x) s_eat[s_wpos[t] + x] = t;
   __syncthreads();
   for (int t = tid; t < nce; t += MZ_T) {
     const int a = s_atom[t];
@@ -263,31 +272,36 @@ __global__ void __launch_bounds__(MZ_T) mzd_virtual(DiagArgs A) {
         }
       }
     }
+    // evaluated and appended entries of this chunk as warp masks: the
+    // ordered fold visits only the evaluated ones, in j order
+    const int lane = tid & 31, wid = tid >> 5;
+    const unsigned evm = __ballot_sync(0xffffffffu, ev), apm = __ballot_sync(0xffffffffu, app);
     __syncthreads();
-    s_val[tid] = ev ? fabs(val) : -1.0;
-    s_flag[tid] = app;
+    s_val[tid] = fabs(val);
+    if (lane == 0) { s_flag[wid] = (int)evm; s_scan[wid] = (int)apm; }
     __syncthreads();
-    if (tid == 0) {  // ordered fold of |fmo| for sumt, max for tiny, running ranks
-      int run = 0;
-      const int m = min(MZ_T, nocc - j0);
-      for (int t = 0; t < m; ++t) {
-        if (s_val[t] >= 0.0) {
-          s_sumt = DADD(s_sumt, s_val[t]);
-          s_tiny = fmax(s_tiny, s_val[t]);
+    if (tid == 0) {  // ordered fold of |fmo| for sumt, max for tiny
+      for (int w = 0; w < MZ_T / 32; ++w)
+        for (unsigned m = (unsigned)s_flag[w]; m; m &= m - 1) {
+          const double v = s_val[32 * w + __ffs((int)m) - 1];
+          s_sumt = DADD(s_sumt, v);
+          s_tiny = fmax(s_tiny, v);
         }
-        s_scan[t] = run;
-        run += s_flag[t];
-      }
     }
-    __syncthreads();
+    int before = __popc(apm & ((1u << lane) - 1u)), total = 0;
+    for (int w = 0; w < MZ_T / 32; ++w) {
+      const int c = __popc((unsigned)s_scan[w]);
+      if (w < wid) before += c;
+      total += c;
+    }
     if (A.mode == 1 && app) {
-      const long long pos = s_base + count + s_scan[tid];
+      const long long pos = s_base + count + before;
       A.ifmo[2 * pos] = i + 1;
       A.ifmo[2 * pos + 1] = j + 1;
       A.fmo[pos] = val;
     }
-    const int m = min(MZ_T, nocc - j0);
-    count += s_scan[m - 1] + s_flag[m - 1];
+    count += total;
+    __syncthreads();
   }
   __syncthreads();
   if (tid == 0) {
