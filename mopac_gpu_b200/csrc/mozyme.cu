@@ -408,24 +408,42 @@ int upload(const std::vector<T>& v, const T** out, size_t capacity = 0) {
 // own arrays, as build_atom_index does on the host: each atom's LMOs in
 // ascending order with the offset of the atom's coefficients in the LMO.
 
-// Per LMO: count its atoms, and the coefficient offset of every entry.
+// Per LMO (one warp, lanes over its atoms): count its atoms, and the
+// coefficient offset of every entry (a warp scan of the atoms' orbital counts).
 __global__ void mzr_count(int numat, int nlmo, const int* __restrict__ iorbs, const int* __restrict__ ncf,
                           const int* __restrict__ nncf, const int* __restrict__ icocc, const int* __restrict__ ncocc,
                           long long nentries, long long ncoeff, int* __restrict__ cnt, int* __restrict__ ecoff,
                           int* __restrict__ err) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= nlmo) return;
-  long long c = ncocc[i];
+  const int lane = threadIdx.x & 31;
+  const int i = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5);
+  if (i >= nlmo) return;  // warp-uniform
   const long long j0 = nncf[i], j1 = j0 + ncf[i];
-  if (j0 < 0 || j1 > nentries) { atomicOr(err, 1); return; }
-  for (long long jj = j0; jj < j1; ++jj) {
-    const int a = icocc[jj] - 1;
-    if (a < 0 || a >= numat) { atomicOr(err, 1); continue; }
-    atomicAdd(&cnt[a], 1);
-    ecoff[jj] = (int)c;
-    c += iorbs[a];
+  if (j0 < 0 || j1 > nentries) {
+    if (lane == 0) atomicOr(err, 1);
+    return;
   }
-  if (c > ncoeff) atomicOr(err, 2);
+  long long c = ncocc[i];
+  for (long long q0 = j0; q0 < j1; q0 += 32) {
+    const long long jj = q0 + lane;
+    int a = -1, no = 0;
+    if (jj < j1) {
+      a = icocc[jj] - 1;
+      if (a < 0 || a >= numat) atomicOr(err, 1);
+      else no = iorbs[a];
+    }
+    int incl = no;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const int t = __shfl_up_sync(0xffffffffu, incl, d);
+      if (lane >= d) incl += t;
+    }
+    if (jj < j1 && a >= 0 && a < numat) {
+      atomicAdd(&cnt[a], 1);
+      ecoff[jj] = (int)(c + incl - no);
+    }
+    c += __shfl_sync(0xffffffffu, incl, 31);
+  }
+  if (lane == 0 && c > ncoeff) atomicOr(err, 2);
 }
 
 // Exclusive scan of the counts into atom_ptr (numat + 1 entries); one CTA.
@@ -460,16 +478,18 @@ __global__ void mzr_scan(int numat, const int* __restrict__ cnt, int* __restrict
   if (tid == 0) ptr[numat] = s_carry;
 }
 
-// Per LMO: drop every entry into its atom's segment (any order).
+// Per LMO (one warp, lanes over its atoms): drop every entry into its atom's
+// segment (any order).
 __global__ void mzr_scatter(int numat, int nlmo, const int* __restrict__ ncf, const int* __restrict__ nncf,
                             const int* __restrict__ icocc, long long nentries, const int* __restrict__ ptr,
                             const int* __restrict__ ecoff, int* __restrict__ cursor,
                             unsigned long long* __restrict__ tmp, int* __restrict__ err) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane = threadIdx.x & 31;
+  const int i = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5);
   if (i >= nlmo) return;
   const long long j0 = nncf[i], j1 = j0 + ncf[i];
   if (j0 < 0 || j1 > nentries) return;
-  for (long long jj = j0; jj < j1; ++jj) {
+  for (long long jj = j0 + lane; jj < j1; jj += 32) {
     const int a = icocc[jj] - 1;
     if (a < 0 || a >= numat) continue;
     const long long at = (long long)ptr[a] + atomicAdd(&cursor[a], 1);
@@ -724,7 +744,7 @@ extern "C" int mb_mz_lmos_refresh_dev(int numat, const int* iorbs_dev, MbMzLmos*
   if (cudaMemsetAsync(cnt, 0, sizeof(int) * 2 * (size_t)numat, stream) != cudaSuccess ||
       cudaMemsetAsync(err, 0, sizeof(int), stream) != cudaSuccess)
     rc = mb_set_error(MB_ERR_CUDA, "mb_mz_lmos_refresh_dev: memset");
-  const int nb = (n + 127) / 128;
+  const int nb = (int)(((long long)n * 32 + 127) / 128);  // a warp per LMO
   if (rc == MB_OK && n > 0) {
     mzr_count<<<nb, 128, 0, stream>>>(numat, n, iorbs_dev, Q->ncf, Q->nncf, Q->icocc, Q->ncocc, ne, Q->ncoeff, cnt,
                                       ecoff, err);
