@@ -23,6 +23,11 @@ namespace {
 
 constexpr int MZ_MAXA = 512;  // atoms per virtual LMO handled by one CTA
 constexpr int MZ_T = 128;
+// diagg1's rebuild: evaluated candidates each warp keeps in shared memory
+constexpr int MZD_CAND = 256;
+// 32-bit words of diagg1's three atom bitmaps, rounded to an even count so the
+// candidate values after them are 8-byte aligned
+__host__ __device__ __forceinline__ int mzd_bits_words(int numat) { return (3 * ((numat + 31) / 32) + 1) & ~1; }
 
 __device__ long long pair_offset(const MbMzLayout& L, int a, int b) {
   if (a == b) return L.pair_off[L.pair_ptr[a + 1] - 1];
@@ -249,59 +254,122 @@ __global__ void __launch_bounds__(MZ_T) mzd_virtual(DiagArgs A) {
   __syncthreads();
   int count = 0;
   const int nocc = A.occ.nlmo;
-  for (int j0 = 0; j0 < nocc; j0 += MZ_T) {
-    const int j = j0 + tid;
-    int app = 0, ev = 0;
-    double val = 0.0;
-    if (j < nocc) {
-      const int j1 = A.occ.icocc[A.occ.nncf[j]] - 1;
-      const int j2 = A.occ.ncf[j] > 1 ? A.occ.icocc[A.occ.nncf[j] + 1] - 1 : j1;
-      const bool b11 = bit_test(near1, j1), b12 = bit_test(near1, j2), b21 = bit_test(near2, j1),
-                 b22 = bit_test(near2, j2);
-      if (b11 || b12 || b21 || b22) {
-        double s = 0.0;
-        if (b11) s = fabs(A.fao[pair_offset(L, i1, j1)]);
-        if (b12) s = DADD(s, fabs(A.fao[pair_offset(L, i1, j2)]));
-        if (b21) s = DADD(s, fabs(A.fao[pair_offset(L, i2, j1)]));
-        if (b22) s = DADD(s, fabs(A.fao[pair_offset(L, i2, j2)]));
-        if (s >= A.flim) {
-          bool lij;
-          val = mzd_fmo(A, j, lat, s_sorted, s_sidx, nce, s_aov, s_wpos, s_ws, &lij);
-          ev = 1;
-          app = (lij && fabs(val) > A.oldlim) ? 1 : 0;
-        }
-      }
+  // Candidate j of virtual LMO i: evaluated (ev) when its first two atoms see
+  // i's first two within the neighbour lists and the F elements between them
+  // reach flim; appended (app) when fmo(i, j) also clears oldlim.
+  auto candidate = [&](int j, int& ev, int& app, double& val) {
+    ev = 0;
+    app = 0;
+    val = 0.0;
+    if (j >= nocc) return;
+    const int j1 = A.occ.icocc[A.occ.nncf[j]] - 1;
+    const int j2 = A.occ.ncf[j] > 1 ? A.occ.icocc[A.occ.nncf[j] + 1] - 1 : j1;
+    const bool b11 = bit_test(near1, j1), b12 = bit_test(near1, j2), b21 = bit_test(near2, j1),
+               b22 = bit_test(near2, j2);
+    if (!(b11 || b12 || b21 || b22)) return;
+    double s = 0.0;
+    if (b11) s = fabs(A.fao[pair_offset(L, i1, j1)]);
+    if (b12) s = DADD(s, fabs(A.fao[pair_offset(L, i1, j2)]));
+    if (b21) s = DADD(s, fabs(A.fao[pair_offset(L, i2, j1)]));
+    if (b22) s = DADD(s, fabs(A.fao[pair_offset(L, i2, j2)]));
+    if (s >= A.flim) {
+      bool lij;
+      val = mzd_fmo(A, j, lat, s_sorted, s_sidx, nce, s_aov, s_wpos, s_ws, &lij);
+      ev = 1;
+      app = (lij && fabs(val) > A.oldlim) ? 1 : 0;
     }
-    // evaluated and appended entries of this chunk as warp masks: the
-    // ordered fold visits only the evaluated ones, in j order
+  };
+  // Fast path: each warp scans a contiguous quarter of the occupied LMOs and
+  // compacts its evaluated candidates, in j order, into shared memory (s_eat
+  // is free after the ws build); one barrier, then thread 0 folds them all in
+  // j order and ranks the appended ones.  A warp with more than kCand
+  // candidates sends the CTA to the chunked loop below.
+  static_assert(MZ_T == 128 && 4 * MZD_CAND <= 4 * MZ_MAXA, "four warps share s_eat");
+  constexpr int kCand = MZD_CAND;
+  double* s_cv = (double*)(s_bits + mzd_bits_words(L.numat));  // 4 * kCand values after the bitmaps
+  __shared__ int s_cn[4];
+  {
     const int lane = tid & 31, wid = tid >> 5;
-    const unsigned evm = __ballot_sync(0xffffffffu, ev), apm = __ballot_sync(0xffffffffu, app);
-    __syncthreads();
-    s_val[tid] = fabs(val);
-    if (lane == 0) { s_flag[wid] = (int)evm; s_scan[wid] = (int)apm; }
-    __syncthreads();
-    if (tid == 0) {  // ordered fold of |fmo| for sumt, max for tiny
-      for (int w = 0; w < MZ_T / 32; ++w)
-        for (unsigned m = (unsigned)s_flag[w]; m; m &= m - 1) {
-          const double v = s_val[32 * w + __ffs((int)m) - 1];
-          s_sumt = DADD(s_sumt, v);
-          s_tiny = fmax(s_tiny, v);
+    int* cj = s_eat + wid * kCand;  // j + 1, negated when appended
+    double* cv = s_cv + wid * kCand;
+    const int per = (nocc + 3) / 4, jb = wid * per, je = min(nocc, jb + per);
+    int nc = 0;
+    for (int j0 = jb; j0 < je; j0 += 32) {
+      int ev, app;
+      double val;
+      candidate(j0 + lane < je ? j0 + lane : nocc, ev, app, val);
+      const unsigned evm = __ballot_sync(0xffffffffu, ev);
+      const int pos = nc + __popc(evm & ((1u << lane) - 1u));
+      if (ev && pos < kCand) {
+        cj[pos] = app ? -(j0 + lane + 1) : (j0 + lane + 1);
+        cv[pos] = val;
+      }
+      nc += __popc(evm);
+    }
+    if (lane == 0) s_cn[wid] = nc;
+  }
+  __syncthreads();
+  if (s_cn[0] <= kCand && s_cn[1] <= kCand && s_cn[2] <= kCand && s_cn[3] <= kCand) {
+    if (tid == 0) {  // the ordered fold, and the appended entries in j order
+      long long pos = s_base;
+      int run = 0;
+      for (int w = 0; w < 4; ++w)
+        for (int q = 0; q < s_cn[w]; ++q) {
+          const double v = s_cv[w * kCand + q];
+          s_sumt = DADD(s_sumt, fabs(v));
+          s_tiny = fmax(s_tiny, fabs(v));
+          const int cj = s_eat[w * kCand + q];
+          if (cj < 0) {
+            if (A.mode == 1) {
+              A.ifmo[2 * pos] = i + 1;
+              A.ifmo[2 * pos + 1] = -cj;
+              A.fmo[pos] = v;
+              ++pos;
+            }
+            ++run;
+          }
         }
+      s_scan[0] = run;
     }
-    int before = __popc(apm & ((1u << lane) - 1u)), total = 0;
-    for (int w = 0; w < MZ_T / 32; ++w) {
-      const int c = __popc((unsigned)s_scan[w]);
-      if (w < wid) before += c;
-      total += c;
-    }
-    if (A.mode == 1 && app) {
-      const long long pos = s_base + count + before;
-      A.ifmo[2 * pos] = i + 1;
-      A.ifmo[2 * pos + 1] = j + 1;
-      A.fmo[pos] = val;
-    }
-    count += total;
     __syncthreads();
+    count = s_scan[0];
+  } else {
+    for (int j0 = 0; j0 < nocc; j0 += MZ_T) {
+      const int j = j0 + tid;
+      int app, ev;
+      double val;
+      candidate(j, ev, app, val);
+      // evaluated and appended entries of this chunk as warp masks: the
+      // ordered fold visits only the evaluated ones, in j order
+      const int lane = tid & 31, wid = tid >> 5;
+      const unsigned evm = __ballot_sync(0xffffffffu, ev), apm = __ballot_sync(0xffffffffu, app);
+      __syncthreads();
+      s_val[tid] = fabs(val);
+      if (lane == 0) { s_flag[wid] = (int)evm; s_scan[wid] = (int)apm; }
+      __syncthreads();
+      if (tid == 0) {  // ordered fold of |fmo| for sumt, max for tiny
+        for (int w = 0; w < MZ_T / 32; ++w)
+          for (unsigned m = (unsigned)s_flag[w]; m; m &= m - 1) {
+            const double v = s_val[32 * w + __ffs((int)m) - 1];
+            s_sumt = DADD(s_sumt, v);
+            s_tiny = fmax(s_tiny, v);
+          }
+      }
+      int before = __popc(apm & ((1u << lane) - 1u)), total = 0;
+      for (int w = 0; w < MZ_T / 32; ++w) {
+        const int c = __popc((unsigned)s_scan[w]);
+        if (w < wid) before += c;
+        total += c;
+      }
+      if (A.mode == 1 && app) {
+        const long long pos = s_base + count + before;
+        A.ifmo[2 * pos] = i + 1;
+        A.ifmo[2 * pos + 1] = j + 1;
+        A.fmo[pos] = val;
+      }
+      count += total;
+      __syncthreads();
+    }
   }
   __syncthreads();
   if (tid == 0) {
@@ -408,7 +476,7 @@ extern "C" int mb_mz_diagg1_dev(const MbMzLayout* L, const MbMzLmos* occ, const 
   A.sumt_part = sumt_part;
   A.tiny_bits = tiny_bits;
   A.err = err;
-  const size_t smem = sizeof(unsigned) * 3 * (size_t)((L->numat + 31) / 32);
+  const size_t smem = sizeof(unsigned) * (size_t)mzd_bits_words(L->numat) + sizeof(double) * 4 * MZD_CAND;
   if (smem > 160 * 1024) return mb_set_error(MB_ERR_UNSUPPORTED, "mb_mz_diagg1_dev: too many atoms for the bitmaps");
   static bool attr = false;
   if (!attr) {
