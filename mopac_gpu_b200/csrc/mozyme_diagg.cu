@@ -17,6 +17,8 @@
 
 #include <vector>
 
+#include <algorithm>
+
 #include "mb_common.cuh"
 
 namespace {
@@ -67,6 +69,9 @@ struct DiagArgs {
   const double* aocc;
   double cutoff, flim, oldlim;
   int mode;                       // 0: count, 1: write (rebuild), 2: recompute on the old list
+  int* stash_j;                   // count pass: the appended entries of LMO i (j + 1) at i * stash_cap ..,
+  double* stash_v;                //   their values; the write pass then only has to copy them
+  int stash_cap;                  //   0: no stash.  Write pass: LMOs with nfmo <= stash_cap are skipped
   const long long* list_off;      // write / recompute: first list position of each virtual LMO
   int* nfmo;                      // count pass: entries per virtual LMO
   int* ifmo;
@@ -123,6 +128,7 @@ __global__ void __launch_bounds__(MZ_T) mzd_virtual(DiagArgs A) {
   __shared__ long long s_base;
   __shared__ double s_sumt, s_tiny;
   const int i = blockIdx.x, tid = threadIdx.x;
+  if (A.mode == 1 && A.stash_cap > 0 && A.nfmo[i] <= A.stash_cap) return;  // copied from the stash
   const MbMzLayout& L = A.L;
   const int nce = A.vir.ncf[i], nn = A.vir.nncf[i], loopi = A.vir.ncocc[i];
   if (nce > MZ_MAXA) {  // uniform over the CTA
@@ -325,6 +331,9 @@ __global__ void __launch_bounds__(MZ_T) mzd_virtual(DiagArgs A) {
               A.ifmo[2 * pos + 1] = -cj;
               A.fmo[pos] = v;
               ++pos;
+            } else if (run < A.stash_cap) {
+              A.stash_j[(long long)i * A.stash_cap + run] = -cj;
+              A.stash_v[(long long)i * A.stash_cap + run] = v;
             }
             ++run;
           }
@@ -366,6 +375,9 @@ __global__ void __launch_bounds__(MZ_T) mzd_virtual(DiagArgs A) {
         A.ifmo[2 * pos] = i + 1;
         A.ifmo[2 * pos + 1] = j + 1;
         A.fmo[pos] = val;
+      } else if (A.mode == 0 && app && count + before < A.stash_cap) {
+        A.stash_j[(long long)i * A.stash_cap + count + before] = j + 1;
+        A.stash_v[(long long)i * A.stash_cap + count + before] = val;
       }
       count += total;
       __syncthreads();
@@ -432,6 +444,25 @@ extern "C" size_t mb_mz_diagg1_ws_bytes(const MbMzLayout* L, const MbMzLmos* occ
          256;
 }
 
+namespace {
+// The write pass for stashed LMOs: entries of virtual LMO i (count pass, j
+// order) into the list at list_off[i].
+__global__ void mzd_copy_stash(int nvir, const int* __restrict__ nfmo, const long long* __restrict__ list_off,
+                               const int* __restrict__ sj, const double* __restrict__ sv, int stash_cap,
+                               int* __restrict__ ifmo, double* __restrict__ fmo) {
+  const int i = blockIdx.x;
+  if (i >= nvir) return;
+  const int n = nfmo[i];
+  if (n > stash_cap) return;
+  const long long b = list_off[i];
+  for (int k = threadIdx.x; k < n; k += blockDim.x) {
+    ifmo[2 * (b + k)] = i + 1;
+    ifmo[2 * (b + k) + 1] = sj[(long long)i * stash_cap + k];
+    fmo[b + k] = sv[(long long)i * stash_cap + k];
+  }
+}
+}  // namespace
+
 extern "C" int mb_mz_diagg1_dev(const MbMzLayout* L, const MbMzLmos* occ, const MbMzLmos* vir, const double* fao,
                                 const double* p, int idiagg, double* state, int* nfmo, int* ifmo, double* fmo,
                                 long long* nij, double* eigv, double* eigs, int* eigs_done, double* sumt, void* ws,
@@ -470,6 +501,9 @@ extern "C" int mb_mz_diagg1_dev(const MbMzLayout* L, const MbMzLmos* occ, const 
   A.oldlim = oldlim;
   A.list_off = list_off;
   A.nfmo = nfmo;
+  A.stash_j = nullptr;
+  A.stash_v = nullptr;
+  A.stash_cap = 0;
   A.ifmo = ifmo;
   A.fmo = fmo;
   A.eigv = eigv;
@@ -488,20 +522,43 @@ extern "C" int mb_mz_diagg1_dev(const MbMzLayout* L, const MbMzLmos* occ, const 
   std::vector<long long> off(nvir + 1, 0);
   long long total = 0;
   if (rebuild) {
+    // the count pass also keeps each LMO's appended entries (up to stash_cap,
+    // at most 512 MB in all); the write pass then copies them and recomputes
+    // only the LMOs that had more
+    const int stash_cap = (int)std::min<long long>(1024, (512ll << 20) / (12ll * std::max(nvir, 1)));
+    char* stash = nullptr;
+    if (stash_cap >= 16) {
+      MB_CUDA(cudaMallocAsync((void**)&stash, (size_t)nvir * stash_cap * 12, stream));
+      A.stash_v = (double*)stash;
+      A.stash_j = (int*)(stash + (size_t)nvir * stash_cap * 8);
+      A.stash_cap = stash_cap;
+    }
     A.mode = 0;
     mzd_virtual<<<nvir, MZ_T, smem, stream>>>(A);
     MB_LAUNCH_CHECK();
     MB_CUDA(cudaMemcpyAsync(cnt.data(), nfmo, sizeof(int) * nvir, cudaMemcpyDeviceToHost, stream));
     MB_CUDA(cudaStreamSynchronize(stream));
-    for (int i = 0; i < nvir; ++i) off[i + 1] = off[i] + cnt[i];
+    bool over = false;
+    for (int i = 0; i < nvir; ++i) {
+      off[i + 1] = off[i] + cnt[i];
+      over = over || cnt[i] > A.stash_cap;
+    }
     total = off[nvir];
-    if (total > cap)
+    if (total > cap) {
+      if (stash) cudaFreeAsync(stash, stream);
       return mb_set_error(MB_ERR_UNSUPPORTED, "mb_mz_diagg1_dev: interaction list exceeds its capacity");
+    }
     MB_CUDA(cudaMemcpyAsync(list_off, off.data(), sizeof(long long) * nvir, cudaMemcpyHostToDevice, stream));
-    MB_CUDA(cudaMemsetAsync(tiny_bits, 0, sizeof(unsigned long long), stream));
-    A.mode = 1;
-    mzd_virtual<<<nvir, MZ_T, smem, stream>>>(A);
-    MB_LAUNCH_CHECK();
+    if (A.stash_cap > 0) {
+      mzd_copy_stash<<<nvir, 128, 0, stream>>>(nvir, nfmo, list_off, A.stash_j, A.stash_v, A.stash_cap, ifmo, fmo);
+      MB_LAUNCH_CHECK();
+    }
+    if (over) {  // recomputes the same values, sums and maxima for the LMOs past the stash
+      A.mode = 1;
+      mzd_virtual<<<nvir, MZ_T, smem, stream>>>(A);
+      MB_LAUNCH_CHECK();
+    }
+    if (stash) MB_CUDA(cudaFreeAsync(stash, stream));
   } else {
     MB_CUDA(cudaMemcpyAsync(cnt.data(), nfmo, sizeof(int) * nvir, cudaMemcpyDeviceToHost, stream));
     MB_CUDA(cudaStreamSynchronize(stream));
