@@ -595,7 +595,7 @@ extern "C" int mb_fock2_dev(const MbAtomsDev* atoms, double* f, const double* h,
   if (!atoms || atoms->numat <= 0) return mb_set_error(MB_ERR_ARG, "mb_fock2_dev: no atoms");
   const size_t bytes = mb_fock2_ws_bytes(atoms->numat);
   void* ws = nullptr;
-  MB_CUDA(cudaMallocAsync(&ws, bytes, stream));
+  MB_CUDA(mb_malloc_async(&ws, bytes, stream));
   const int rc = mb_fock2_ws(atoms, f, h, ptot, pa, w, shift, use_shift, ws, bytes, stream);
   const cudaError_t fe = cudaFreeAsync(ws, stream);
   if (rc != MB_OK) return rc;

@@ -62,3 +62,23 @@ extern "C" int mb_kstats_read(int id, long long* count, double* total_ms) {
   if (total_ms) *total_ms = t;
   return MB_OK;
 }
+
+cudaError_t mb_malloc_async(void** p, size_t bytes, cudaStream_t s) {
+  static std::mutex mu;
+  static bool kept[64] = {};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev >= 0 && dev < 64) {
+    std::lock_guard<std::mutex> lk(mu);
+    if (!kept[dev]) {
+      cudaMemPool_t pool;
+      if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+        unsigned long long thr = ~0ull;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+      }
+      kept[dev] = true;
+    }
+  }
+  return cudaMallocAsync(p, bytes, s);
+}

@@ -35,6 +35,16 @@ void mb_count_launch();
 #define MB_KSTAT_IDS 8
 void mb_kstat_mark(int id, cudaStream_t s, bool begin);
 
+// cudaMallocAsync from the device's default pool, which on first use per
+// device is told to keep freed memory (release threshold: unlimited), so the
+// library's per-call scratch is not unmapped and remapped at every
+// synchronisation.  Process-local; changes no device setting.
+cudaError_t mb_malloc_async(void** p, size_t bytes, cudaStream_t s);
+template <class T>
+inline cudaError_t mb_malloc_async(T** p, size_t bytes, cudaStream_t s) {
+  return mb_malloc_async((void**)p, bytes, s);
+}
+
 #define MB_TRY(expr)            \
   do {                          \
     int _rc = (expr);           \

@@ -734,7 +734,7 @@ extern "C" int mb_mz_lmos_refresh_dev(int numat, const int* iorbs_dev, MbMzLmos*
   const long long ne = Q->nentries;
   const size_t bytes = sizeof(int) * (2 * (size_t)numat + (size_t)ne + 8) + sizeof(unsigned long long) * (size_t)ne;
   char* ws = nullptr;
-  MB_CUDA(cudaMallocAsync((void**)&ws, bytes, stream));
+  MB_CUDA(mb_malloc_async((void**)&ws, bytes, stream));
   unsigned long long* tmp = (unsigned long long*)ws;
   int* cnt = (int*)(tmp + ne);
   int* cursor = cnt + numat;

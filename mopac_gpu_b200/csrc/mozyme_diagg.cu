@@ -528,7 +528,7 @@ extern "C" int mb_mz_diagg1_dev(const MbMzLayout* L, const MbMzLmos* occ, const 
     const int stash_cap = (int)std::min<long long>(1024, (512ll << 20) / (12ll * std::max(nvir, 1)));
     char* stash = nullptr;
     if (stash_cap >= 16) {
-      MB_CUDA(cudaMallocAsync((void**)&stash, (size_t)nvir * stash_cap * 12, stream));
+      MB_CUDA(mb_malloc_async((void**)&stash, (size_t)nvir * stash_cap * 12, stream));
       A.stash_v = (double*)stash;
       A.stash_j = (int*)(stash + (size_t)nvir * stash_cap * 8);
       A.stash_cap = stash_cap;
@@ -974,9 +974,9 @@ extern "C" int mb_mz_diagg2_dev(const MbMzLayout* L, MbMzLmos* occ, MbMzLmos* vi
   long long* d_order = nullptr;
   double* d_bs = nullptr;
   int* d_rej = nullptr;
-  MB_CUDA(cudaMallocAsync((void**)&d_order, sizeof(long long) * nij, stream));
-  MB_CUDA(cudaMallocAsync((void**)&d_bs, sizeof(double) * nij, stream));
-  MB_CUDA(cudaMallocAsync((void**)&d_rej, sizeof(int) * nij, stream));
+  MB_CUDA(mb_malloc_async((void**)&d_order, sizeof(long long) * nij, stream));
+  MB_CUDA(mb_malloc_async((void**)&d_bs, sizeof(double) * nij, stream));
+  MB_CUDA(mb_malloc_async((void**)&d_rej, sizeof(int) * nij, stream));
   int rc = MB_OK;
   if (cudaMemcpyAsync(d_order, order.data(), sizeof(long long) * nij, cudaMemcpyHostToDevice, stream) != cudaSuccess)
     rc = mb_set_error(MB_ERR_CUDA, "diagg2: upload");

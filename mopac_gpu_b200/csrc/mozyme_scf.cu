@@ -169,8 +169,8 @@ extern "C" int mb_mz_hbonds_dev(const MbMzLayout* L, const MbMzLmos* occ, const 
   const int no = occ->nlmo, nv = vir->nlmo;
   unsigned char* dflag = nullptr;
   int* dheads = nullptr;
-  MB_CUDA(cudaMallocAsync((void**)&dflag, (size_t)(np > 0 ? np : 1), s));
-  cudaError_t e = cudaMallocAsync((void**)&dheads, sizeof(int) * 2 * (size_t)(no + nv + 1), s);
+  MB_CUDA(mb_malloc_async((void**)&dflag, (size_t)(np > 0 ? np : 1), s));
+  cudaError_t e = mb_malloc_async((void**)&dheads, sizeof(int) * 2 * (size_t)(no + nv + 1), s);
   if (e != cudaSuccess) {
     cudaFreeAsync(dflag, s);
     return mb_set_cuda_error(e, "mb_mz_hbonds_dev", __FILE__, __LINE__);

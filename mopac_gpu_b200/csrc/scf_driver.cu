@@ -380,7 +380,7 @@ extern "C" int mb_ctx_gradient(mb_ctx* c, double* dxyz) {
   if (!c->have_hw) return mb_set_error(MB_ERR_ARG, "mb_ctx_gradient: call mb_ctx_hcore or mb_ctx_set_hw first");
   const size_t wsb = mb_dcart_ws_bytes(c->numat), outb = sizeof(double) * 3 * (size_t)c->numat;
   char* ws = nullptr;
-  MB_CUDA(cudaMallocAsync((void**)&ws, wsb + outb + 256, c->stream));
+  MB_CUDA(mb_malloc_async((void**)&ws, wsb + outb + 256, c->stream));
   double* out = (double*)(ws + ((wsb + 255) & ~(size_t)255));
   int rc = mb_dcart_dev(c->d_nat, c->d_coord, &c->atoms, c->numat, c->p, out, ws, wsb, c->stream);
   if (rc == MB_OK && cudaMemcpyAsync(dxyz, out, outb, cudaMemcpyDeviceToHost, c->stream) != cudaSuccess)

@@ -386,7 +386,7 @@ extern "C" int mb_helect_dev(int n, const double* p, const double* h, const doub
                              cudaStream_t stream) {
   if (n <= 0) return mb_set_error(MB_ERR_ARG, "mb_helect_dev: n <= 0");
   double* tmp = nullptr;
-  MB_CUDA(cudaMallocAsync(&tmp, sizeof(double) * 2 * (size_t)n, stream));
+  MB_CUDA(mb_malloc_async(&tmp, sizeof(double) * 2 * (size_t)n, stream));
   const int threads = 256;
   const int blocks = (int)(((long long)n * 32 + threads - 1) / threads);
   helect_rows<<<blocks, threads, 0, stream>>>(n, p, h, f, tmp, tmp + n);
@@ -432,7 +432,7 @@ extern "C" int mb_cnvg_dev(int norbs, double* pnew, double* p, double* p1, int n
                            cudaStream_t stream) {
   if (norbs <= 0) return mb_set_error(MB_ERR_ARG, "mb_cnvg_dev: norbs <= 0");
   double* ws = nullptr;
-  MB_CUDA(cudaMallocAsync(&ws, sizeof(double) * 4, stream));
+  MB_CUDA(mb_malloc_async(&ws, sizeof(double) * 4, stream));
   int rc = mb_cnvg_ws(norbs, pnew, p, p1, niter, pl_out, ws, stream);
   cudaFreeAsync(ws, stream);
   return rc;
@@ -603,8 +603,8 @@ extern "C" int mb_pseudo_diag_dev(int n, int nocc, const double* fpacked, double
   if (n <= 0 || nocc < 0 || nocc > n) return mb_set_error(MB_ERR_ARG, "mb_pseudo_diag_dev: bad size");
   void* ws = nullptr;
   unsigned long long* nrot = nullptr;
-  MB_CUDA(cudaMallocAsync(&ws, mb_pseudo_ws_bytes(n, nocc), stream));
-  MB_CUDA(cudaMallocAsync((void**)&nrot, sizeof(unsigned long long), stream));
+  MB_CUDA(mb_malloc_async(&ws, mb_pseudo_ws_bytes(n, nocc), stream));
+  MB_CUDA(mb_malloc_async((void**)&nrot, sizeof(unsigned long long), stream));
   MB_CUDA(cudaMemsetAsync(nrot, 0, sizeof(unsigned long long), stream));
   int rc = mb_pseudo_diag_ws(n, nocc, fpacked, c, eigs, nrot, ws, stream);
   unsigned long long h = 0;
