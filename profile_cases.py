@@ -36,6 +36,9 @@ Cases (sizes of the benchmark configurations):
   guess_train     one training step (forward, backward, Adam) of the O-H
                 network on 2048 rows: 6 rows params flops
   guess_predict   the whole prediction into a context (mb_ctx_guess), (H2O)512
+  mz_scf_split  the MOZYME SCF of the (H2O)4096 box (CUTOFF=9, the bench's
+                starting LMOs) through the host loop with every step
+                synchronised and timed: seconds per step over the SCF
   mz_density, mz_helecz, mz_cnvgz, mz_fock, mz_diagg1, mz_diagg2
                 MOZYME blocks, (H2O)4096, 9 A cutoff, synthetic unit LMOs
                 (occupied over 4 A, virtual over 3.2 A, two spare atom slots),
@@ -162,6 +165,71 @@ class C1:
         check(lib().mb_ctx_atoms_dev(self.ctx._h, ctypes.byref(self.atoms)))
 
 
+def mz_scf_split(nwater: int = 4096) -> dict:
+    """Per-step seconds of mozyme.iter_for_mozyme on the (H2O)_n box, each
+    step wrapped in torch.cuda.synchronize() (the loop mb_mz_scf_run runs in
+    C, composed of the same entry points)."""
+    import collections
+    import time
+    from mopac_gpu_b200 import mozyme as mz
+    T = collections.defaultdict(float)
+
+    def timed(name, fn):
+        def w(*a, **k):
+            torch.cuda.synchronize()
+            t = time.perf_counter()
+            r = fn(*a, **k)
+            torch.cuda.synchronize()
+            T[name] += time.perf_counter() - t
+            return r
+        return w
+
+    L_ = lib()
+    saved = []
+    for nm in ("mb_mz_tidy_dev", "mb_mz_check_dev", "mb_mz_eimp_dev", "mb_mz_hbonds_dev"):
+        saved.append((L_, nm, getattr(L_, nm)))
+        setattr(L_, nm, timed(nm.replace("mb_mz_", "").replace("_dev", ""), getattr(L_, nm)))
+    for nm in ("diagg2", "density", "cnvgz", "fock", "helecz"):
+        saved.append((mz, nm, getattr(mz, nm)))
+        setattr(mz, nm, timed(nm, getattr(mz, nm)))
+
+    def refresh_dev(self):
+        check(lib().mb_mz_lmos_refresh_dev(self.numat, ctypes.c_void_p(self.layout_iorbs), ctypes.byref(self.s), None))
+
+    saved.append((mz.Lmos, "refresh", mz.Lmos.refresh))
+    mz.Lmos.refresh = timed("lmo_index_refresh", refresh_dev)
+    base = mz.Diagg1
+
+    class TimedDiagg1(base):
+        def __call__(self, *a, **k):
+            return timed("diagg1", super().__call__)(*a, **k)
+
+    saved.append((mz, "Diagg1", base))
+    mz.Diagg1 = TimedDiagg1
+    try:
+        nat, xyz, _ = workloads.water_box(nwater)
+        L = mz.Layout(np.where(np.asarray(nat) == 1, 1, 4).astype(np.int32), xyz, 81.0, 8.9 ** 2)
+        nat_d = torch.from_numpy(np.ascontiguousarray(nat, np.int32)).cuda()
+        coord_d = torch.from_numpy(np.ascontiguousarray(xyz, np.float64)).cuda()
+        h, w, enuclr = mz.hcore(L, nat_d, coord_d)
+        iorbs, occ, vir = mz.water_lmos(nat, xyz, pad_atoms=400)
+        Qo, Qv = mz.Lmos(L, occ), mz.Lmos(L, vir)
+        Qo.layout_iorbs = Qv.layout_iorbs = L.s.iorbs
+        atheat = lib().mb_atheat(len(nat), np.ascontiguousarray(nat, np.int32).ctypes.data)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r = mz.iter_for_mozyme(L, Qo, Qv, coord_d, w, h, enuclr, atheat)
+        torch.cuda.synchronize()
+        total = time.perf_counter() - t0
+    finally:
+        for obj, nm, v in saved:
+            setattr(obj, nm, v)
+    return {"case": "mz_scf_split", "total_s": round(total, 3), "niter": r["niter"],
+            "escf_per_water_kcal_mol": r["escf"] / nwater,
+            "steps_s": {k: round(v, 3) for k, v in sorted(T.items(), key=lambda x: -x[1])},
+            "config": f"(H2O){nwater} box, CUTOFF=9, host loop with synchronised steps"}
+
+
 def run_cases(names, reps):
     L = lib()
     pk = peaks()
@@ -179,6 +247,8 @@ def run_cases(names, reps):
                                                vp(c1.w), 0.0, 0, vp(ws), wsb, s())), reps)
         out.append(line("fock2", ms, 8 * (c1.ctx.n2elec + 4 * c1.mpack), "GB/s", "hbm", hbm, src,
                         config="(H2O)512, n = 3072"))
+    if "mz_scf_split" in names:
+        out.append(mz_scf_split())
     if "dcart" in names:
         wsb = L.mb_dcart_ws_bytes(len(c1.ctx.nat))
         ws = torch.empty(wsb, dtype=torch.uint8, device="cuda")
