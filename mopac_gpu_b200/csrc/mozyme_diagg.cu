@@ -122,7 +122,7 @@ __global__ void __launch_bounds__(MZ_T) mzd_virtual(DiagArgs A) {
   extern __shared__ unsigned s_bits[];  // lat | near1 | near2, ceil(numat/32) words each
   __shared__ int s_atom[MZ_MAXA], s_wpos[MZ_MAXA + 1], s_sorted[MZ_MAXA], s_sidx[MZ_MAXA];
   __shared__ double s_avir[MZ_MAXA], s_aov[MZ_MAXA], s_ws[4 * MZ_MAXA];
-  __shared__ int s_eat[4 * MZ_MAXA];
+  __shared__ int s_eat[4 * MZ_MAXA];  // the rebuild's candidates (j, appended flag), per warp
   __shared__ double s_val[MZ_T];
   __shared__ int s_flag[MZ_T], s_scan[MZ_T];
   __shared__ long long s_base;
@@ -166,8 +166,6 @@ __global__ void __launch_bounds__(MZ_T) mzd_virtual(DiagArgs A) {
     s_sidx[r] = t;
   }
   __syncthreads();
-  for (int t = tid; t < nce; t += MZ_T)
-    for (int x = 0; x < L.iorbs[s_atom[t]]; ++x) s_eat[s_wpos[t] + x] = t;
   __syncthreads();
   for (int t = tid; t < nce; t += MZ_T) {
     const int a = s_atom[t];
@@ -180,29 +178,30 @@ __global__ void __launch_bounds__(MZ_T) mzd_virtual(DiagArgs A) {
     atomicOr(&lat[a >> 5], 1u << (a & 31));
   }
   __syncthreads();
-  // ws(orbital of atom j1, jx) = sum over the LMO's atoms k1 (in order) of F(k1, j1) psi(k1)
-  const int nws = s_wpos[nce];
-  for (int e = tid; e < nws; e += MZ_T) {
-    const int jjl = s_eat[e];
-    const int j1 = s_atom[jjl], jx = e - s_wpos[jjl] + 1;
+  // ws(orbital of atom j1, jx) = sum over the LMO's atoms k1 (in order) of
+  // F(k1, j1) psi(k1).  One thread per atom j1: its orbitals share every
+  // pair lookup and density test, and each orbital's sum keeps the k1 order.
+  for (int jjl = tid; jjl < nce; jjl += MZ_T) {
+    const int j1 = s_atom[jjl];
     const int nj = L.iorbs[j1];
-    double acc = 0.0;
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
     for (int kk = 0; kk < nce; ++kk) {
       const int k1 = s_atom[kk];
       const long long kj = pair_offset(L, k1, j1);
       if (kj < 0 || !(DMUL(s_avir[kk], A.p[kj]) > A.cutoff)) continue;
       const int nk = L.iorbs[k1];
       const double* cv = A.vir.cocc + loopi + s_wpos[kk];
-      for (int i4 = 1; i4 <= nk; ++i4) {
-        long long ii;
-        if (nk == 1 && nj == 1) ii = kj + 1;
-        else if (k1 > j1) ii = kj + (long long)(i4 - 1) * nj + jx;
-        else if (k1 < j1) ii = kj + (long long)(jx - 1) * nk + i4;
-        else ii = i4 > jx ? kj + (i4 * (i4 - 1)) / 2 + jx : kj + (jx * (jx - 1)) / 2 + i4;
-        acc = DADD(acc, DMUL(A.fao[ii - 1], cv[i4 - 1]));
-      }
+      for (int jx = 1; jx <= nj; ++jx)
+        for (int i4 = 1; i4 <= nk; ++i4) {
+          long long ii;
+          if (nk == 1 && nj == 1) ii = kj + 1;
+          else if (k1 > j1) ii = kj + (long long)(i4 - 1) * nj + jx;
+          else if (k1 < j1) ii = kj + (long long)(jx - 1) * nk + i4;
+          else ii = i4 > jx ? kj + (i4 * (i4 - 1)) / 2 + jx : kj + (jx * (jx - 1)) / 2 + i4;
+          acc[jx - 1] = DADD(acc[jx - 1], DMUL(A.fao[ii - 1], cv[i4 - 1]));
+        }
     }
-    s_ws[e] = acc;
+    for (int jx = 0; jx < nj; ++jx) s_ws[s_wpos[jjl] + jx] = acc[jx];
   }
   __syncthreads();
   for (int t = tid; t < nce; t += MZ_T) {
@@ -286,8 +285,8 @@ __global__ void __launch_bounds__(MZ_T) mzd_virtual(DiagArgs A) {
     }
   };
   // Fast path: each warp scans a contiguous quarter of the occupied LMOs and
-  // compacts its evaluated candidates, in j order, into shared memory (s_eat
-  // is free after the ws build); one barrier, then thread 0 folds them all in
+  // compacts its evaluated candidates, in j order, into shared memory; one
+  // barrier, then thread 0 folds them all in
   // j order and ranks the appended ones.  A warp with more than kCand
   // candidates sends the CTA to the chunked loop below.
   static_assert(MZ_T == 128 && 4 * MZD_CAND <= 4 * MZ_MAXA, "four warps share s_eat");
