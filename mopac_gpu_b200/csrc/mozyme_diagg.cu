@@ -43,48 +43,6 @@ __device__ long long pair_offset(const MbMzLayout& L, int a, int b) {
   return -1;  // outside cutof2: the reference's nijbo is -1 or -2, tested as < 0
 }
 
-// pair_offset for four partners of b at once: the four binary searches
-// advance in lockstep, so their dependent loads overlap.
-__device__ void pair_offset4(const MbMzLayout& L, const int a[4], int b, long long out[4]) {
-  int lo[4], hi[4];
-  bool live[4];
-#pragma unroll
-  for (int q = 0; q < 4; ++q) {
-    out[q] = -1;
-    live[q] = a[q] >= 0;
-    if (live[q] && a[q] == b) {
-      out[q] = L.pair_off[L.pair_ptr[b + 1] - 1];
-      live[q] = false;
-    }
-    lo[q] = live[q] ? L.nbr_ptr[a[q]] : 0;
-    hi[q] = live[q] ? L.nbr_ptr[a[q] + 1] - 1 : -1;
-  }
-  for (;;) {
-    bool any = false;
-#pragma unroll
-    for (int q = 0; q < 4; ++q) any |= live[q] && lo[q] <= hi[q];
-    if (!any) break;
-    int v[4], mid[4];
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      mid[q] = (lo[q] + hi[q]) >> 1;
-      v[q] = (live[q] && lo[q] <= hi[q]) ? L.nbr_atom[mid[q]] : 0;
-    }
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      if (!(live[q] && lo[q] <= hi[q])) continue;
-      if (v[q] == b) {
-        out[q] = L.pair_off[L.nbr_entry[mid[q]]];
-        live[q] = false;
-      } else if (v[q] < b) {
-        lo[q] = mid[q] + 1;
-      } else {
-        hi[q] = mid[q] - 1;
-      }
-    }
-  }
-}
-
 // aocc(kk) = sum of squared coefficients of entry kk (one thread per LMO).
 __global__ void mzd_aocc(MbMzLmos Q, const int* __restrict__ iorbs, double* __restrict__ aocc) {
   for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < Q.nlmo; j += gridDim.x * blockDim.x) {
@@ -227,28 +185,21 @@ __global__ void __launch_bounds__(MZ_T) mzd_virtual(DiagArgs A) {
     const int j1 = s_atom[jjl];
     const int nj = L.iorbs[j1];
     double acc[4] = {0.0, 0.0, 0.0, 0.0};
-    for (int k0 = 0; k0 < nce; k0 += 4) {
-      int ka[4];
-      long long kjs[4];
-#pragma unroll
-      for (int q = 0; q < 4; ++q) ka[q] = k0 + q < nce ? s_atom[k0 + q] : -1;
-      pair_offset4(L, ka, j1, kjs);
-      for (int q = 0; q < 4 && k0 + q < nce; ++q) {  // the partners in order
-        const int kk = k0 + q, k1 = ka[q];
-        const long long kj = kjs[q];
-        if (kj < 0 || !(DMUL(s_avir[kk], A.p[kj]) > A.cutoff)) continue;
-        const int nk = L.iorbs[k1];
-        const double* cv = A.vir.cocc + loopi + s_wpos[kk];
-        for (int jx = 1; jx <= nj; ++jx)
-          for (int i4 = 1; i4 <= nk; ++i4) {
-            long long ii;
-            if (nk == 1 && nj == 1) ii = kj + 1;
-            else if (k1 > j1) ii = kj + (long long)(i4 - 1) * nj + jx;
-            else if (k1 < j1) ii = kj + (long long)(jx - 1) * nk + i4;
-            else ii = i4 > jx ? kj + (i4 * (i4 - 1)) / 2 + jx : kj + (jx * (jx - 1)) / 2 + i4;
-            acc[jx - 1] = DADD(acc[jx - 1], DMUL(A.fao[ii - 1], cv[i4 - 1]));
-          }
-      }
+    for (int kk = 0; kk < nce; ++kk) {
+      const int k1 = s_atom[kk];
+      const long long kj = pair_offset(L, k1, j1);
+      if (kj < 0 || !(DMUL(s_avir[kk], A.p[kj]) > A.cutoff)) continue;
+      const int nk = L.iorbs[k1];
+      const double* cv = A.vir.cocc + loopi + s_wpos[kk];
+      for (int jx = 1; jx <= nj; ++jx)
+        for (int i4 = 1; i4 <= nk; ++i4) {
+          long long ii;
+          if (nk == 1 && nj == 1) ii = kj + 1;
+          else if (k1 > j1) ii = kj + (long long)(i4 - 1) * nj + jx;
+          else if (k1 < j1) ii = kj + (long long)(jx - 1) * nk + i4;
+          else ii = i4 > jx ? kj + (i4 * (i4 - 1)) / 2 + jx : kj + (jx * (jx - 1)) / 2 + i4;
+          acc[jx - 1] = DADD(acc[jx - 1], DMUL(A.fao[ii - 1], cv[i4 - 1]));
+        }
     }
     for (int jx = 0; jx < nj; ++jx) s_ws[s_wpos[jjl] + jx] = acc[jx];
   }
