@@ -577,8 +577,9 @@ int mb_guess_model_create(const float* blob, mb_guess_model** out);
 int mb_guess_model_destroy(mb_guess_model* model);
 /* Predicts the context's starting density on the device (H and O only; other
  * elements return MB_ERR_UNSUPPORTED and the caller keeps the standard guess),
- * then applies purify_steps McWeeny purifications (1 recommended; see
- * mb_guess_purify_dev).  Use with opts.guess = 1. */
+ * then applies purify_steps McWeeny purifications (1 recommended) with the
+ * split-precision products of mb_guess_purify_split_dev.  Use with
+ * opts.guess = 1. */
 int mb_ctx_guess(mb_ctx* ctx, const mb_guess_model* model, int purify_steps);
 /* McWeeny purification of a packed total density p (device, mpack): D = p/2,
  * D <- 3 D^2 - 2 D^3 steps times (FP64 GEMMs), p = 2 D.  It moves D's
@@ -587,6 +588,13 @@ int mb_ctx_guess(mb_ctx* ctx, const mb_guess_model* model, int purify_steps);
  * bytes of device scratch. */
 size_t mb_guess_purify_ws_bytes(int n);
 int mb_guess_purify_dev(int n, double* p, int steps, void* ws, cudaStream_t stream);
+/* The same with both products of each step as three-product BF16 splits on
+ * the tensor cores (mb_gemm_split_ws's accuracy, about 1e-5 of |A||B|; the
+ * result only seeds the SCF).  tc_ws: mb_gemm_split_ws_bytes(n, n, n) bytes, 1024-byte aligned;
+ * err_dev: device int, zeroed by the caller, nonzero after the stream is
+ * synchronised if a tensor-core pipeline wait expired. */
+int mb_guess_purify_split_dev(int n, double* p, int steps, void* ws, void* tc_ws, size_t tc_ws_bytes, int* err_dev,
+                              cudaStream_t stream);
 /* The steps, on device pointers.  Pairs: counts_host[NTYPES] receives the
  * per-type counts; with pf == NULL only counting is done; otherwise pf/ps/pt
  * (first atom, second atom, type) are filled type by type (order inside a

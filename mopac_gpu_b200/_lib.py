@@ -204,6 +204,7 @@ SIGNATURES = {
     "mb_ctx_guess": ([_P, _P, _I], _I),
     "mb_guess_purify_ws_bytes": ([_I], ctypes.c_size_t),
     "mb_guess_purify_dev": ([_I, _P, _I, _P, _P], _I),
+    "mb_guess_purify_split_dev": ([_I, _P, _I, _P, _P, ctypes.c_size_t, _P, _P], _I),
     "mb_guess_blob_floats": ([], ctypes.c_size_t),
     "mb_guess_model_create": ([_P, ctypes.POINTER(_P)], _I),
     "mb_guess_model_destroy": ([_P], _I),

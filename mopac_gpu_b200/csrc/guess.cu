@@ -174,13 +174,88 @@ __device__ __forceinline__ unsigned long long warp_min_u64(unsigned long long v)
   return v;
 }
 
+// Smallest rank key over the atoms k != f that key_of accepts (key_of returns
+// ~0 for the others), over the whole molecule.  The search runs over f's
+// neighbour list first: every atom off that list has r2 >= RC^2 by the same
+// arithmetic (r2_of), so its key's distance part is at least that of RC^2,
+// and a list minimum strictly below it is the global minimum.  Otherwise (no
+// candidate on the list, a tie at the boundary, an overflowing list) the
+// whole molecule is scanned.
+template <class KeyOf>
+__device__ __forceinline__ unsigned long long nearest_key(int lane, int numat, int f, const int* __restrict__ nbr_count,
+                                                          const int* __restrict__ nbr, KeyOf key_of) {
+  const unsigned long long NONE = ~0ull;
+  const int nn = nbr_count[f];
+  if (nn <= NBR_MAX) {
+    unsigned long long best = NONE;
+    const int* nl = nbr + (long long)f * NBR_MAX;
+    for (int j = lane; j < nn; j += 32) {
+      const unsigned long long key = key_of(nl[j]);
+      best = key < best ? key : best;
+    }
+    best = warp_min_u64(best);
+    const unsigned long long q_rc = (unsigned long long)floor(DADD(DMUL(RC * RC, QSCALE), 0.5));
+    if (best != NONE && (best >> 21) < q_rc) return best;
+  }
+  unsigned long long best = NONE;
+  for (int k = lane; k < numat; k += 32) {
+    if (k == f) continue;
+    const unsigned long long key = key_of(k);
+    best = key < best ? key : best;
+  }
+  return warp_min_u64(best);
+}
+
+// Long-range moments of the reference charges seen from atom c (all k != c,
+// g = x_k - x_c, r = |g|): m[0] = sum q/r, m[1..3] = sum q g/r^3, m[4] = sum
+// q/r^3, m[5..10] = sum q g g^T/r^5 (xx, yy, zz, xy, xz, yz).  The frame-local
+// multipoles of a pair follow from these by one rotation (features_kernel).
+constexpr int NMOM = 11;
+__device__ __forceinline__ void lr_contrib(const double* __restrict__ xyz, int k, int c, double q, double* m) {
+  const double gx = DSUB(xyz[3 * k], xyz[3 * c]), gy = DSUB(xyz[3 * k + 1], xyz[3 * c + 1]),
+               gz = DSUB(xyz[3 * k + 2], xyz[3 * c + 2]);
+  const double r2 = DADD(DADD(DMUL(gx, gx), DMUL(gy, gy)), DMUL(gz, gz));
+  const double r = sqrt(r2), ir = 1.0 / r, ir3 = ir / r2, ir5 = ir3 / r2;
+  m[0] = q * ir;
+  m[1] = q * gx * ir3; m[2] = q * gy * ir3; m[3] = q * gz * ir3;
+  m[4] = q * ir3;
+  m[5] = q * gx * gx * ir5; m[6] = q * gy * gy * ir5; m[7] = q * gz * gz * ir5;
+  m[8] = q * gx * gy * ir5; m[9] = q * gx * gz * ir5; m[10] = q * gy * gz * ir5;
+}
+
+// One warp per atom.
+__global__ void __launch_bounds__(128) lr_moments_kernel(int numat, const int* __restrict__ nat,
+                                                         const double* __restrict__ xyz, double* __restrict__ mom) {
+  const int lane = threadIdx.x & 31;
+  const int c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (c >= numat) return;
+  double acc[NMOM];
+#pragma unroll
+  for (int j = 0; j < NMOM; ++j) acc[j] = 0.0;
+  for (int k = lane; k < numat; k += 32) {
+    if (k == c) continue;
+    double m[NMOM];
+    lr_contrib(xyz, k, c, nat[k] == 1 ? QREF_H : QREF_HEAVY, m);
+#pragma unroll
+    for (int j = 0; j < NMOM; ++j) acc[j] += m[j];
+  }
+#pragma unroll
+  for (int j = 0; j < NMOM; ++j)
+    for (int o = 16; o > 0; o >>= 1) acc[j] += __shfl_xor_sync(0xffffffffu, acc[j], o);
+  double mine = 0.0;  // acc[lane] without a dynamically indexed (local-memory) array
+#pragma unroll
+  for (int j = 0; j < NMOM; ++j) mine = lane == j ? acc[j] : mine;
+  if (lane < NMOM) mom[(long long)c * NMOM + lane] = mine;
+}
+
 // One warp per pair.  Writes the frame (columns x, y, z: frames[9q + 3c + r]
 // = component r of axis c) and the raw descriptors feat[q * DIN + j].
 __global__ void __launch_bounds__(128) features_kernel(int numat, const int* __restrict__ nat,
                                                        const double* __restrict__ xyz, int npairs,
                                                        const int* __restrict__ pf, const int* __restrict__ ps,
                                                        const int* __restrict__ nbr_count, const int* __restrict__ nbr,
-                                                       float* __restrict__ feat, double* __restrict__ frames) {
+                                                       const double* __restrict__ mom, float* __restrict__ feat,
+                                                       double* __restrict__ frames) {
   const int lane = threadIdx.x & 31;
   const int q = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (q >= npairs) return;
@@ -193,13 +268,8 @@ __global__ void __launch_bounds__(128) features_kernel(int numat, const int* __r
   if (f != s) {
     zx = DSUB(xyz[3 * s], ox); zy = DSUB(xyz[3 * s + 1], oy); zz = DSUB(xyz[3 * s + 2], oz);
   } else {
-    unsigned long long best = NONE;
-    for (int k = lane; k < numat; k += 32) {
-      if (k == f) continue;
-      unsigned long long key = rank_key(r2_of(xyz, k, f), k);
-      best = key < best ? key : best;
-    }
-    best = warp_min_u64(best);
+    const unsigned long long best =
+        nearest_key(lane, numat, f, nbr_count, nbr, [&](int k) { return rank_key(r2_of(xyz, k, f), k); });
     if (best == NONE) {
       have_z = false;
       zx = 0.0; zy = 0.0; zz = 1.0;
@@ -216,18 +286,15 @@ __global__ void __launch_bounds__(128) features_kernel(int numat, const int* __r
   } else {
     double zn = sqrt(DADD(DADD(DMUL(zx, zx), DMUL(zy, zy)), DMUL(zz, zz)));
     zx = zx / zn; zy = zy / zn; zz = zz / zn;
-    unsigned long long best = NONE;
-    for (int k = lane; k < numat; k += 32) {
-      if (k == f || k == ex2) continue;
+    const unsigned long long best = nearest_key(lane, numat, f, nbr_count, nbr, [&](int k) {
+      if (k == ex2) return NONE;
       double dx = DSUB(xyz[3 * k], ox), dy = DSUB(xyz[3 * k + 1], oy), dz = DSUB(xyz[3 * k + 2], oz);
       double r2 = DADD(DADD(DMUL(dx, dx), DMUL(dy, dy)), DMUL(dz, dz));
       double dd = DADD(DADD(DMUL(dx, zx), DMUL(dy, zy)), DMUL(dz, zz));
       double p2 = DSUB(r2, DMUL(dd, dd));
-      if (!(p2 > DMUL(PERP_MIN2, r2))) continue;
-      unsigned long long key = rank_key(r2, k);
-      best = key < best ? key : best;
-    }
-    best = warp_min_u64(best);
+      if (!(p2 > DMUL(PERP_MIN2, r2))) return NONE;
+      return rank_key(r2, k);
+    });
     double px, py, pz;
     if (best == NONE) {
       double ax = fabs(zx), ay = fabs(zy), az = fabs(zz);
@@ -288,34 +355,41 @@ __global__ void __launch_bounds__(128) features_kernel(int numat, const int* __r
   }
   if (ncent == 1)
     for (int j = lane; j < PER_CENTER; j += 32) out[PER_CENTER + j] = 0.f;
-  // long-range electrostatic environment of each centre (warp-parallel sums)
+  // long-range electrostatic environment of each centre: the centre's
+  // moments over all other atoms less the pair partner's share, rotated into
+  // the pair frame (x = a_x . g, so sum q x/r^3 = a_x . m[1..3] and sum q (3 x
+  // x' - r^2 d)/r^5 = 3 a^T M a' - d m[4])
   for (int ci = 0; ci < 2; ++ci) {
     if (ci == 1 && ncent == 1) {
       if (lane < NLR) out[LR0 + NLR + lane] = 0.f;
       continue;
     }
-    const int c = ci == 0 ? f : s;
-    const double cx = xyz[3 * c], cy = xyz[3 * c + 1], cz = xyz[3 * c + 2];
-    double v[NLR];
-    for (int j = 0; j < NLR; ++j) v[j] = 0.0;
-    for (int k = lane; k < numat; k += 32) {
-      if (k == f || k == s) continue;
-      const double q = nat[k] == 1 ? QREF_H : QREF_HEAVY;
-      double gx = DSUB(xyz[3 * k], cx), gy = DSUB(xyz[3 * k + 1], cy), gz = DSUB(xyz[3 * k + 2], cz);
-      double x = DADD(DADD(DMUL(gx, R[0]), DMUL(gy, R[1])), DMUL(gz, R[2]));
-      double y = DADD(DADD(DMUL(gx, R[3]), DMUL(gy, R[4])), DMUL(gz, R[5]));
-      double z = DADD(DADD(DMUL(gx, R[6]), DMUL(gy, R[7])), DMUL(gz, R[8]));
-      double r2 = DADD(DADD(DMUL(x, x), DMUL(y, y)), DMUL(z, z));
-      double r = sqrt(r2), r3 = r2 * r, r5 = r3 * r2;
-      v[0] += q / r;
-      v[1] += q * x / r3; v[2] += q * y / r3; v[3] += q * z / r3;
-      v[4] += q * (3.0 * x * x - r2) / r5; v[5] += q * (3.0 * y * y - r2) / r5; v[6] += q * (3.0 * z * z - r2) / r5;
-      v[7] += q * 3.0 * x * y / r5; v[8] += q * 3.0 * x * z / r5; v[9] += q * 3.0 * y * z / r5;
+    const int c = ci == 0 ? f : s, o = ci == 0 ? s : f;
+    double m[NMOM];
+    for (int j = 0; j < NMOM; ++j) m[j] = mom[(long long)c * NMOM + j];
+    if (ncent == 2) {
+      double mo[NMOM];
+      lr_contrib(xyz, o, c, nat[o] == 1 ? QREF_H : QREF_HEAVY, mo);
+      for (int j = 0; j < NMOM; ++j) m[j] -= mo[j];
     }
-    for (int j = 0; j < NLR; ++j)
-      for (int o = 16; o > 0; o >>= 1) v[j] += __shfl_xor_sync(0xffffffffu, v[j], o);
-    if (lane == 0)
-      for (int j = 0; j < NLR; ++j) out[LR0 + ci * NLR + j] = (float)v[j];
+    // M a for the three axes a = R[0..2], R[3..5], R[6..8]
+    double Ma[9];
+    for (int a = 0; a < 3; ++a) {
+      const double ax = R[3 * a], ay = R[3 * a + 1], az = R[3 * a + 2];
+      Ma[3 * a] = m[5] * ax + m[8] * ay + m[9] * az;
+      Ma[3 * a + 1] = m[8] * ax + m[6] * ay + m[10] * az;
+      Ma[3 * a + 2] = m[9] * ax + m[10] * ay + m[7] * az;
+    }
+    auto aMb = [&](int a, int b) { return R[3 * a] * Ma[3 * b] + R[3 * a + 1] * Ma[3 * b + 1] + R[3 * a + 2] * Ma[3 * b + 2]; };
+    if (lane == 0) {
+      float* lr = out + LR0 + ci * NLR;
+      lr[0] = (float)m[0];
+      for (int a = 0; a < 3; ++a) lr[1 + a] = (float)(R[3 * a] * m[1] + R[3 * a + 1] * m[2] + R[3 * a + 2] * m[3]);
+      for (int a = 0; a < 3; ++a) lr[4 + a] = (float)(3.0 * aMb(a, a) - m[4]);
+      lr[7] = (float)(3.0 * aMb(0, 1));
+      lr[8] = (float)(3.0 * aMb(0, 2));
+      lr[9] = (float)(3.0 * aMb(1, 2));
+    }
   }
   if (lane < NPAIR_RBF) {
     float v = 0.f;
@@ -712,11 +786,21 @@ extern "C" int mb_guess_pairs_dev(int numat, const int* nat, const double* xyz, 
   return MB_OK;
 }
 
+static size_t nbr_bytes(int numat) { return ((sizeof(int) * (size_t)numat * (NBR_MAX + 1)) + 255) & ~(size_t)255; }
+
+// fws: mb_guess_features_ws_bytes(numat) bytes, 256-byte aligned: the
+// neighbour counts and lists, then the atoms' long-range moments.
 static int features_impl(int numat, const int* nat, const double* xyz, int npairs, const int* pf, const int* ps,
-                         float* feat, double* frames, int* nbr_count, int* nbr, cudaStream_t s) {
+                         float* feat, double* frames, void* fws, cudaStream_t s) {
+  int* nbr_count = (int*)fws;
+  int* nbr = nbr_count + numat;
+  double* mom = (double*)((char*)fws + nbr_bytes(numat));
   neighbours_kernel<<<blocks_for(numat, 128), 128, 0, s>>>(numat, xyz, nbr_count, nbr);
   MB_LAUNCH_CHECK();
-  features_kernel<<<blocks_for(npairs, 4), 128, 0, s>>>(numat, nat, xyz, npairs, pf, ps, nbr_count, nbr, feat, frames);
+  lr_moments_kernel<<<blocks_for(numat, 4), 128, 0, s>>>(numat, nat, xyz, mom);
+  MB_LAUNCH_CHECK();
+  features_kernel<<<blocks_for(npairs, 4), 128, 0, s>>>(numat, nat, xyz, npairs, pf, ps, nbr_count, nbr, mom, feat,
+                                                        frames);
   MB_LAUNCH_CHECK();
   // an overflowing neighbour list is an error, not a silent truncation
   int mx = 0;
@@ -729,18 +813,18 @@ static int features_impl(int numat, const int* nat, const double* xyz, int npair
 }
 
 extern "C" size_t mb_guess_features_ws_bytes(int numat) {
-  return sizeof(int) * (size_t)numat * (NBR_MAX + 1);
+  return nbr_bytes(numat) + sizeof(double) * NMOM * (size_t)numat;
 }
 
-// ws: mb_guess_features_ws_bytes(numat) bytes of device scratch (neighbour lists).
+// ws: mb_guess_features_ws_bytes(numat) bytes of device scratch, 256-byte
+// aligned (neighbour lists and long-range moments).
 extern "C" int mb_guess_features_dev(int numat, const int* nat, const double* xyz, int npairs, const int* pf,
                                      const int* ps, float* feat, double* frames, void* ws, cudaStream_t s) {
   if (npairs < 0 || numat <= 0 || numat >= (1 << 21) || !ws)
     return mb_set_error(MB_ERR_ARG, "mb_guess_features_dev: bad args");
   if (npairs == 0) return MB_OK;
-  int* nbr_count = (int*)ws;
-  int* nbr = nbr_count + numat;
-  return features_impl(numat, nat, xyz, npairs, pf, ps, feat, frames, nbr_count, nbr, s);
+  if (((uintptr_t)ws & 255) != 0) return mb_set_error(MB_ERR_ARG, "mb_guess_features_dev: ws must be 256-byte aligned");
+  return features_impl(numat, nat, xyz, npairs, pf, ps, feat, frames, ws, s);
 }
 
 extern "C" int mb_guess_normalize_dev(const mb_guess_model* m, int type, int n, const float* raw, uint16_t* x,
@@ -901,14 +985,13 @@ extern "C" int mb_guess_predict_density_ws(const mb_guess_model* m, int numat, c
   float* y = (float*)cur; cur += al(b_y);
   uint16_t* x = (uint16_t*)cur; cur += al(b_x);
   uint16_t* mlp_ws = (uint16_t*)cur; cur += al(b_ws);
-  int* nbr_count = (int*)cur;
-  int* nbr = nbr_count + numat;
+  void* fws = cur;
   // emit the pairs type by type
   MB_CUDA(cudaMemcpyAsync(work + NT, segh, sizeof(int) * NT, cudaMemcpyHostToDevice, s));
   MB_CUDA(cudaMemsetAsync(work + 2 * NT, 0, sizeof(int) * NT, s));
   pairs_emit_kernel<<<blocks_for(numat, 128), 128, 0, s>>>(numat, nat, xyz, r2, work + NT, work + 2 * NT, pf, ps, pt);
   MB_LAUNCH_CHECK();
-  MB_TRY(features_impl(numat, nat, xyz, (int)tot, pf, ps, feat, frames, nbr_count, nbr, s));  // syncs: segh is safe
+  MB_TRY(features_impl(numat, nat, xyz, (int)tot, pf, ps, feat, frames, fws, s));  // syncs: segh is safe
   long long off = 0;
   for (int t = 0; t < NT; ++t) {
     if (counts[t] == 0) continue;
@@ -980,6 +1063,40 @@ extern "C" int mb_guess_purify_dev(int n, double* p, int steps, void* ws, cudaSt
   for (int it = 0; it < steps; ++it) {
     MB_TRY(mb_dgemm_dev('N', 'N', n, n, n, 1.0, d, n, d, n, 0.0, d2, n, s));
     MB_TRY(mb_dgemm_dev('N', 'N', n, n, n, 1.0, d2, n, d, n, 0.0, d3, n, s));
+    mcweeny_kernel<<<grid, 256, 0, s>>>(nn, d2, d3, d);
+    MB_LAUNCH_CHECK();
+  }
+  pack_twice_kernel<<<grid, 256, 0, s>>>(n, d, p);
+  MB_LAUNCH_CHECK();
+  return MB_OK;
+}
+
+extern "C" size_t mb_gemm_split_ws_bytes(int m, int n, int k);
+extern "C" int mb_gemm_split_ws(char transa, char transb, int m, int n, int k, double alpha, const double* a, int lda,
+                                const double* b, int ldb, double beta, double* c, int ldc, void* ws, size_t ws_bytes,
+                                int* err_dev, cudaStream_t stream);
+
+// The same purification with the two products on the tensor cores (two BF16
+// planes per operand, three products accumulated in FP32: about 1e-5 of
+// |A||B| per element): the result only seeds the SCF, which converges to the
+// same fixed point from it.  tc_ws: mb_gemm_split_ws_bytes(n, n, n) bytes, 1024-byte aligned;
+// err_dev: the GEMM pipeline's error flag (zeroed by the caller, read after
+// the stream is synchronised).
+extern "C" int mb_guess_purify_split_dev(int n, double* p, int steps, void* ws, void* tc_ws, size_t tc_ws_bytes,
+                                         int* err_dev, cudaStream_t s) {
+  if (n <= 0 || !p || steps < 0 || (steps > 0 && (!ws || !tc_ws || !err_dev)))
+    return mb_set_error(MB_ERR_ARG, "mb_guess_purify_split_dev: bad args");
+  if (steps == 0) return MB_OK;
+  const long long nn = (long long)n * n;
+  double* d = (double*)ws;
+  double* d2 = d + nn;
+  double* d3 = d2 + nn;
+  const int grid = 148 * 8;
+  unpack_half_kernel<<<grid, 256, 0, s>>>(n, p, d);
+  MB_LAUNCH_CHECK();
+  for (int it = 0; it < steps; ++it) {
+    MB_TRY(mb_gemm_split_ws('N', 'N', n, n, n, 1.0, d, n, d, n, 0.0, d2, n, tc_ws, tc_ws_bytes, err_dev, s));
+    MB_TRY(mb_gemm_split_ws('N', 'N', n, n, n, 1.0, d2, n, d, n, 0.0, d3, n, tc_ws, tc_ws_bytes, err_dev, s));
     mcweeny_kernel<<<grid, 256, 0, s>>>(nn, d2, d3, d);
     MB_LAUNCH_CHECK();
   }

@@ -145,6 +145,7 @@ struct mb_ctx {
   MbAtomsDev atoms{};
   int* d_nat = nullptr;
   double* d_coord = nullptr;
+  double* d_pdiag = nullptr;  // the diagonal guess on the device (norbs)
   double *h = nullptr, *w = nullptr, *f = nullptr, *p = nullptr, *pa = nullptr, *pold = nullptr, *pold2 = nullptr,
          *c = nullptr, *eigs = nullptr, *fdiag = nullptr;
   double* scal = nullptr;   // device scalars: [0] ee, [1] pl, [8..] scratch
@@ -176,7 +177,7 @@ static void ctx_free(mb_ctx* c) {
   if (!c) return;
   mb_atoms_destroy(&c->atoms);
   mb_guess_ws_destroy(c->guess_ws);
-  void* ptrs[] = {c->d_nat, c->d_coord, c->h, c->w, c->f, c->p, c->pa, c->pold, c->pold2, c->c, c->eigs,
+  void* ptrs[] = {c->d_nat, c->d_coord, c->d_pdiag, c->h, c->w, c->f, c->p, c->pa, c->pold, c->pold2, c->c, c->eigs,
                   c->fdiag, c->scal, c->hws, c->status, c->nrot, c->eig_ws, c->pseudo_ws,
                   c->fock_ws, c->fppf_hist, c->fock_hist, c->tc_ws_raw, c->pguess, c->purify_ws, c->pprev};
   for (void* q : ptrs)
@@ -248,6 +249,7 @@ extern "C" int mb_ctx_create(int numat, const int* nat, const double* coord, mb_
 #define ALLOC(ptr, bytes) if (e == cudaSuccess) e = cudaMalloc((void**)&(ptr), (bytes))
   ALLOC(c->d_nat, sizeof(int) * numat);
   ALLOC(c->d_coord, sizeof(double) * 3 * numat);
+  ALLOC(c->d_pdiag, sizeof(double) * n);
   ALLOC(c->h, sizeof(double) * mp);
   ALLOC(c->w, sizeof(double) * (size_t)c->n2elec);
   ALLOC(c->f, sizeof(double) * mp);
@@ -267,6 +269,7 @@ extern "C" int mb_ctx_create(int numat, const int* nat, const double* coord, mb_
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaMemcpy(c->d_nat, nat, sizeof(int) * numat, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(c->d_coord, c->coord.data(), sizeof(double) * 3 * numat, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(c->d_pdiag, c->pdiag.data(), sizeof(double) * n, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemset(c->c, 0, sizeof(double) * nn);
   if (e == cudaSuccess) e = cudaMemset(c->eigs, 0, sizeof(double) * n);
   if (e != cudaSuccess) {
@@ -418,6 +421,8 @@ extern "C" int mb_ctx_set_guess(mb_ctx* c, const double* p) {
 
 extern "C" size_t mb_guess_purify_ws_bytes(int n);
 extern "C" int mb_guess_purify_dev(int n, double* p, int steps, void* ws, cudaStream_t s);
+extern "C" int mb_guess_purify_split_dev(int n, double* p, int steps, void* ws, void* tc_ws, size_t tc_ws_bytes,
+                                         int* err_dev, cudaStream_t s);
 
 extern "C" int mb_ctx_guess(mb_ctx* c, const mb_guess_model* m, int purify_steps) {
   if (!c || !m || purify_steps < 0) return mb_set_error(MB_ERR_ARG, "mb_ctx_guess: bad args");
@@ -437,8 +442,25 @@ extern "C" int mb_ctx_guess(mb_ctx* c, const mb_guess_model* m, int purify_steps
       if (!c->purify_ws) MB_CUDA(cudaMalloc(&c->purify_ws, mb_guess_purify_ws_bytes(c->norbs)));
       ws = c->purify_ws;
     }
-    MB_TRY(mb_guess_purify_dev(c->norbs, c->pguess, purify_steps, ws, c->stream));
+    // the two products per step on the tensor cores, in the split GEMM
+    // workspace the SCF uses afterwards (grown here if it is smaller)
+    const int n = c->norbs;
+    const size_t need = mb_gemm_split_ws_bytes(n, n, n);
+    if (need > c->tc_ws_bytes) {
+      if (c->tc_ws_raw) cudaFree(c->tc_ws_raw);
+      c->tc_ws_raw = c->tc_ws = nullptr;
+      c->tc_ws_bytes = 0;
+      MB_CUDA(cudaMalloc(&c->tc_ws_raw, need + 1024));
+      c->tc_ws = (void*)(((uintptr_t)c->tc_ws_raw + 1023) & ~(uintptr_t)1023);
+      c->tc_ws_bytes = need;
+    }
+    MB_CUDA(cudaMemsetAsync(c->status + 1, 0, sizeof(int), c->stream));
+    MB_TRY(mb_guess_purify_split_dev(n, c->pguess, purify_steps, ws, c->tc_ws, c->tc_ws_bytes, c->status + 1,
+                                     c->stream));
+    int terr = 0;
+    MB_CUDA(cudaMemcpyAsync(&terr, c->status + 1, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
     MB_CUDA(cudaStreamSynchronize(c->stream));
+    if (terr) return mb_set_error(MB_ERR_CUDA, "mb_ctx_guess: tensor-core GEMM pipeline wait expired");
   }
   MB_CUDA(cudaStreamSynchronize(c->stream));
   c->have_guess = true;
@@ -458,6 +480,17 @@ __global__ void add_tail_kernel(int n, int from, double* e, double s) {
 // Starting state from a supplied density, as iter sets it up after reading
 // one with OLDENS (iter.F90:151-158, RHF): pa = p/2 and pold = 2*pa.  That
 // branch leaves pold2 as allocated; here it starts as the diagonal of p.
+__global__ void diag_start_kernel(int n, const double* __restrict__ pdiag, double w1, double* __restrict__ p,
+                                  double* __restrict__ pa, double* __restrict__ pold, double* __restrict__ pold2) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const long long j = (long long)i * (i + 1) / 2 + i;
+  const double d = pdiag[i], da = (d * w1) * 1.0;
+  p[j] = d;
+  pa[j] = da;
+  pold[j] = da;
+  pold2[i] = da;
+}
 __global__ void guess_start_kernel(int n, long long mpack, const double* __restrict__ g, double* __restrict__ p,
                                    double* __restrict__ pa, double* __restrict__ pold, double* __restrict__ pold2) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < mpack; i += (long long)gridDim.x * blockDim.x) {
@@ -595,21 +628,15 @@ extern "C" int mb_scf_run(mb_ctx* c, const mb_scf_opts* opts_in, mb_scf_result* 
   const int na1el = nclose, nb1el = nclose;
   const int ihomo = nclose > 1 ? nclose : 1;
   {
-    std::vector<double> hp(mpack, 0.0), hpa(mpack, 0.0), hpd(n);
+    // the diagonal guess: P = diag(pdiag), alpha and old densities scaled by
+    // w1 (iter.F90:168-189; the reference's `random` factor alternates
+    // between 1 and 1/1, so it is 1 for every orbital)
     const double w1 = na1el / (na1el + 1.0e-6 + nb1el);
-    double random = 1.0;
-    for (int i = 0; i < n; ++i) {
-      long long j = (long long)i * (i + 1) / 2 + i;
-      hp[j] = c->pdiag[i];
-      hpa[j] = hp[j] * w1 * random;
-      random = 1.0 / random;
-      hpd[i] = hpa[j];
-    }
-    MB_CUDA(cudaMemcpyAsync(c->p, hp.data(), sizeof(double) * mpack, cudaMemcpyHostToDevice, s));
-    MB_CUDA(cudaMemcpyAsync(c->pa, hpa.data(), sizeof(double) * mpack, cudaMemcpyHostToDevice, s));
-    MB_CUDA(cudaMemcpyAsync(pold, hpa.data(), sizeof(double) * mpack, cudaMemcpyHostToDevice, s));
-    MB_CUDA(cudaMemcpyAsync(pold2, hpd.data(), sizeof(double) * n, cudaMemcpyHostToDevice, s));
-    MB_CUDA(cudaStreamSynchronize(s));
+    MB_CUDA(cudaMemsetAsync(c->p, 0, sizeof(double) * mpack, s));
+    MB_CUDA(cudaMemsetAsync(c->pa, 0, sizeof(double) * mpack, s));
+    MB_CUDA(cudaMemsetAsync(pold, 0, sizeof(double) * mpack, s));
+    diag_start_kernel<<<(n + 255) / 256, 256, 0, s>>>(n, c->d_pdiag, w1, c->p, c->pa, pold, pold2);
+    MB_LAUNCH_CHECK();
   }
   if (opts.guess) {
     if (!c->have_guess) return mb_set_error(MB_ERR_ARG, "mb_scf_run: opts.guess needs mb_ctx_set_guess or mb_ctx_guess");

@@ -228,6 +228,30 @@ def test_purification_matches_oracle(cluster):
         assert np.abs(p.cpu().numpy() - po).max() < 1e-10, steps
 
 
+def test_split_purification_matches_oracle_to_the_split_gemm_bound(cluster):
+    """mb_ctx_guess's purification: the same McWeeny steps with the products
+    as three-product BF16 splits (about 1e-5 of |A||B| per element)."""
+    from mopac_gpu_b200._lib import lib
+    nat, xyz, s, r = cluster
+    rng = np.random.default_rng(7)
+    g = r.p + rng.normal(scale=3e-3, size=r.p.shape) * (np.abs(r.p) > 1e-3)
+    n = s.norbs
+    tc = torch.empty(int(lib().mb_gemm_split_ws_bytes(n, n, n)) + 1024, dtype=torch.uint8, device="cuda")
+    tc_ptr = (tc.data_ptr() + 1023) & ~1023
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    for steps in (0, 1, 2):
+        p = torch.tensor(g, dtype=torch.float64, device="cuda")
+        ws = torch.empty(int(lib().mb_guess_purify_ws_bytes(n)), dtype=torch.uint8, device="cuda")
+        assert lib().mb_guess_purify_split_dev(n, p.data_ptr(), steps, ws.data_ptr(), tc_ptr,
+                                               int(lib().mb_gemm_split_ws_bytes(n, n, n)), err.data_ptr(),
+                                               torch.cuda.current_stream().cuda_stream) == 0
+        torch.cuda.synchronize()
+        assert int(err.item()) == 0
+        po = go.purify(g, n, steps) if steps else g
+        dev = np.abs(p.cpu().numpy() - po).max()
+        assert dev < (1e-12 if steps == 0 else 1e-4), (steps, dev)
+
+
 def test_trained_network_cuts_iterations_and_keeps_the_heat():
     from mopac_gpu_b200.guess import GuessModel, evaluate
     if not GuessModel.available():
