@@ -110,6 +110,16 @@ typedef struct mb_scf_opts {
                         default -80 (no keyword).  0 (SHIFT=0) turns the
                         level shift off and lets newdg switch on as soon as
                         the density change falls below trans (:136)       */
+  int camp;          /* 1: the CAMP keyword (SCF/iter.F90:134): Camp-King's
+                        interp (matrix/interp.F90) on the vectors from the
+                        third iteration, a full diagonalisation in every
+                        iteration; an interpolated pass (interp's mode 3)
+                        builds the rotated vectors' density without Pulay,
+                        diagonalisation or cnvg and is not counted.
+                        Independently of it, iter's forced switch-on of all
+                        convergers (:351-372) runs when niter passes
+                        itrmax - 10: Pulay and Camp-King on, bshift = 4.44,
+                        the count restarts.  Default 0                    */
 } mb_scf_opts;
 
 typedef struct mb_scf_result {
@@ -129,6 +139,9 @@ typedef struct mb_scf_result {
   int n_finish;      /* iterations the FP64 finish added                   */
   double dp;         /* max|P_k - P_(k-1)| of the last density update
                         (computed when the finish is on, else -1)          */
+  int n_interp;      /* Camp-King interpolated passes (interp mode 3)      */
+  int forced_on;     /* 1 when iter forced all convergers on (niter passed
+                        itrmax - 10, SCF/iter.F90:351-372)                 */
 } mb_scf_result;
 
 void mb_scf_opts_default(mb_scf_opts* o);

@@ -57,7 +57,7 @@ class ScfOpts(ctypes.Structure):
     _fields_ = [("pseudo", ctypes.c_int), ("itrmax", ctypes.c_int), ("scfcrt", ctypes.c_double),
                 ("precision", ctypes.c_int), ("switch_pl", ctypes.c_double), ("verbose", ctypes.c_int),
                 ("pulay", ctypes.c_int), ("guess", ctypes.c_int), ("finish_dp", ctypes.c_double),
-                ("finish_max", ctypes.c_int), ("bshift", ctypes.c_double)]
+                ("finish_max", ctypes.c_int), ("bshift", ctypes.c_double), ("camp", ctypes.c_int)]
 
 
 class ScfRes(ctypes.Structure):
@@ -66,7 +66,7 @@ class ScfRes(ctypes.Structure):
                 ("pl", ctypes.c_double), ("t_fock_ms", ctypes.c_double), ("t_diag_ms", ctypes.c_double),
                 ("t_density_ms", ctypes.c_double), ("t_other_ms", ctypes.c_double), ("t_total_ms", ctypes.c_double),
                 ("n_pulay", ctypes.c_int), ("n_split", ctypes.c_int), ("n_finish", ctypes.c_int),
-                ("dp", ctypes.c_double)]
+                ("dp", ctypes.c_double), ("n_interp", ctypes.c_int), ("forced_on", ctypes.c_int)]
 
 
 _lib = None

@@ -47,6 +47,11 @@ extern "C" int mb_density_split_ws(int n, int nocc, double occ, const double* c,
 extern "C" size_t mb_pulay_ws_bytes(int n);
 extern "C" int mb_pulay_ws(int n, double* f, const double* p, double* fppf, double* fock, int mfock, double* emat,
                            int ldemat, int* lfock, int* nfock, int* start, double* pl, void* ws, cudaStream_t stream);
+struct mb_campking;
+extern "C" int mb_campking_create(int n, mb_campking** out);
+extern "C" void mb_campking_destroy(mb_campking* ck);
+extern "C" int mb_campking_interp(mb_campking* ck, int np_, int mode, double e, const double* fp, double* cp,
+                                  void* eig_ws, int* status, cudaStream_t s, int* mode_out, int* rotated);
 extern "C" int mb_hcore_dev(const int* nat_d, const double* coord_d, const MbAtomsDev* at, int numat, double* h,
                             double* w, double* enuc_pairs, cudaStream_t stream);
 extern "C" int mb_hcore_finish(int numat, const MbAtomsDev* at, const int* nat_d, double* h, const double* e1b,
@@ -167,6 +172,7 @@ struct mb_ctx {
   double* pprev = nullptr;          // previous density for the FP64 finish's max|dP|
   mb_guess_ws* guess_ws = nullptr;  // the prediction's grow-only workspace
   void* purify_ws = nullptr;        // McWeeny matrices when eig_ws is too small
+  mb_campking* ck = nullptr;        // Camp-King's state, made on its first use
   cudaStream_t stream = nullptr;
 };
 
@@ -177,6 +183,7 @@ static void ctx_free(mb_ctx* c) {
   if (!c) return;
   mb_atoms_destroy(&c->atoms);
   mb_guess_ws_destroy(c->guess_ws);
+  mb_campking_destroy(c->ck);
   void* ptrs[] = {c->d_nat, c->d_coord, c->d_pdiag, c->h, c->w, c->f, c->p, c->pa, c->pold, c->pold2, c->c, c->eigs,
                   c->fdiag, c->scal, c->hws, c->status, c->nrot, c->eig_ws, c->pseudo_ws,
                   c->fock_ws, c->fppf_hist, c->fock_hist, c->tc_ws_raw, c->pguess, c->purify_ws, c->pprev};
@@ -198,6 +205,7 @@ extern "C" void mb_scf_opts_default(mb_scf_opts* o) {
   o->finish_dp = -1.0;
   o->finish_max = 40;
   o->bshift = -80.0;
+  o->camp = 0;
 }
 
 extern "C" int mb_ctx_create(int numat, const int* nat, const double* coord, mb_ctx** out) {
@@ -570,7 +578,11 @@ extern "C" int mb_scf_run(mb_ctx* c, const mb_scf_opts* opts_in, mb_scf_result* 
   cudaStream_t s = c->stream;
   if (opts.pseudo && !c->pseudo_ws) MB_CUDA(cudaMalloc(&c->pseudo_ws, mb_pseudo_ws_bytes(n, nclose)));
   if (!c->fock_ws) MB_CUDA(cudaMalloc(&c->fock_ws, mb_fock2_ws_bytes(c->numat)));
-  const bool okpuly = opts.pulay != 0;
+  if (c->ck) {  // interp's saved state belongs to one SCF
+    mb_campking_destroy(c->ck);
+    c->ck = nullptr;
+  }
+  bool okpuly = opts.pulay != 0;
   if (okpuly) {
     if (!c->fppf_hist) MB_CUDA(cudaMalloc(&c->fppf_hist, sizeof(double) * kNpulay * (size_t)mpack));
     if (!c->fock_hist) MB_CUDA(cudaMalloc(&c->fock_hist, sizeof(double) * kNpulay * (size_t)mpack));
@@ -582,6 +594,7 @@ extern "C" int mb_scf_run(mb_ctx* c, const mb_scf_opts* opts_in, mb_scf_result* 
   // (setup_mopac_arrays.F90:148, iter.F90:826-831): keep that aliasing.
   double* pold = okpuly ? c->fppf_hist : c->pold;
   double* pold2 = okpuly ? c->fock_hist : c->pold2;
+  int modea = opts.camp ? 1 : 0;  // interp's mode (iter.F90:322-330)
   std::vector<double> emat((size_t)(kNpulay + 1) * (kNpulay + 1), 0.0);
   int lfock = 0, nfock = 0, frst = 1;
   // Split precision: density and Fmo GEMMs on the tensor cores until pl falls
@@ -619,12 +632,14 @@ extern "C" int mb_scf_run(mb_ctx* c, const mb_scf_opts* opts_in, mb_scf_result* 
   // ---- first-call setup (iter.F90:123-221)
   const double enrgy = PM7_FPC9;
   // bshift: -80 by default, -n with SHIFT=n (iter.F90:119, :131-132)
-  const double bshift = opts.bshift;
+  double bshift = opts.bshift;
   double shift = 1.0, shfmax = 20.0, pl = 1.0, ten = fabs(bshift) > 1.0e-20 ? bshift : 0.0, shfto = 0.0,
          shftbo = 0.0, shiftb = 0.0;
   const double plchek = 0.005, trans = 0.2;
   bool newdg = false, oknewd = fabs(bshift) < 0.001;
-  const bool halfe = false, camkin = false;
+  const bool halfe = false;
+  bool camkin = opts.camp != 0;
+  bool allcon = okpuly || camkin;  // iter.F90:142
   const int na1el = nclose, nb1el = nclose;
   const int ihomo = nclose > 1 ? nclose : 1;
   {
@@ -656,8 +671,39 @@ extern "C" int mb_scf_run(mb_ctx* c, const mb_scf_opts* opts_in, mb_scf_result* 
   const int hblocks = (int)((mpack + 255) / 256 > 148 * 16 ? 148 * 16 : (mpack + 255) / 256);
 
   for (;;) {  // label 250
-    ++niter;
+    const bool incitr = modea != 3;  // an interpolated pass is not an iteration (iter.F90:342-343)
+    if (incitr) ++niter;
     if (niter > opts.itrmax) break;
+    if (niter > opts.itrmax - 10 && !allcon) {
+      // SWITCH ON ALL CONVERGERS (iter.F90:351-372): Pulay and Camp-King on,
+      // a constant shift, and the iteration count restarts (label 180)
+      if (!c->fppf_hist || !c->fock_hist) {
+        if (mb_pulay_ws_bytes(n) > mb_eigh_ws_bytes(n))
+          return mb_set_error(MB_ERR_ARG, "mb_scf_run: Pulay workspace exceeds the eigensolver workspace");
+        if (!c->fppf_hist) MB_CUDA(cudaMalloc(&c->fppf_hist, sizeof(double) * kNpulay * (size_t)mpack));
+        if (!c->fock_hist) MB_CUDA(cudaMalloc(&c->fock_hist, sizeof(double) * kNpulay * (size_t)mpack));
+      }
+      if (pold != c->fppf_hist) {
+        // pulay's histories start at pold and pold2 (one pair of arrays in
+        // the reference): carry cnvg's heads over
+        MB_CUDA(cudaMemcpyAsync(c->fppf_hist, pold, sizeof(double) * mpack, cudaMemcpyDeviceToDevice, s));
+        MB_CUDA(cudaMemcpyAsync(c->fock_hist, pold2, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+        pold = c->fppf_hist;
+        pold2 = c->fock_hist;
+      }
+      okpuly = true;
+      camkin = !halfe;
+      allcon = true;
+      bshift = 4.44;
+      iredy = -4;
+      eold = 100.0;
+      newdg = false;
+      frst = 1;
+      niter = 0;
+      modea = camkin ? 1 : 0;
+      res->forced_on = 1;
+      continue;
+    }
     bool use_shift = false;
     if (fabs(shift) > 1.0e-10 && bshift != 0.0) {
       if (niter > 1) {
@@ -710,6 +756,7 @@ extern "C" int mb_scf_run(mb_ctx* c, const mb_scf_opts* opts_in, mb_scf_result* 
       // before the eigensolver sees the Fock matrix
       if (!isfinite(ee)) return mb_set_error(MB_ERR_NUMERIC, "non-finite electronic energy (H, W or P)");
       escf = (ee + c->enuclr) * enrgy + c->atheat + scorr;
+      if (!incitr) break;  // an interpolated point: no energy test (iter.F90:662)
       diff = escf - eold;
       if (diff > 0) ten = ten - 1.0;
       else ten = ten * 0.975 + 0.05;
@@ -734,19 +781,31 @@ extern "C" int mb_scf_run(mb_ctx* c, const mb_scf_opts* opts_in, mb_scf_result* 
       break;
     }
     if (converged) break;
-    ready = iredy > 0 && (fabs(diff) < sellim * 10.0 || pl == 0.0);
-    ++iredy;
-    eold = escf;
+    if (incitr) {
+      ready = iredy > 0 && (fabs(diff) < sellim * 10.0 || pl == 0.0);
+      ++iredy;
+      eold = escf;
+    }
     if (opts.verbose)
-      fprintf(stderr, " ITERATION %4d PLS=%10.3e ENERGY %14.6f DELTAE %13.7f shift %8.3f %s\n", niter, pl, escf, diff,
-              shift, newdg ? "newdg" : "");
-    if (newdg && okpuly && iredy > 1) {  // iter.F90:815-831
+      fprintf(stderr, " ITERATION %4d PLS=%10.3e ENERGY %14.6f DELTAE %13.7f shift %8.3f %s%s\n", niter, pl, escf,
+              diff, shift, newdg ? "newdg" : "", incitr ? "" : " (interpolated)");
+    if (niter > 2 && camkin) {  // Camp-King on the alpha vectors (iter.F90:781-798; makea is always set for RHF)
+      if (!c->ck) MB_TRY(mb_campking_create(n, &c->ck));
+      int mnew = modea, rot = 0;
+      MB_TRY(mb_campking_interp(c->ck, na1el, modea, escf / enrgy, c->f, c->c, c->eig_ws, c->status, s, &mnew, &rot));
+      modea = mnew;
+      if (rot) res->n_interp++;
+    }
+    const bool interpolated = modea == 3;  // no Pulay, no diagonalisation, no cnvg (iter.F90:800, :888)
+    if (!interpolated && newdg && okpuly && iredy > 1) {  // iter.F90:815-831
       MB_TRY(mb_pulay_ws(n, c->f, c->pa, c->fppf_hist, c->fock_hist, kNpulay, emat.data(), kNpulay + 1, &lfock,
                          &nfock, &frst, &pl, c->eig_ws, s));
       res->n_pulay++;
     }
     t_diag.start();
-    if (newdg && opts.pseudo && !(halfe || camkin)) {
+    if (interpolated) {
+      // the density of the interpolated vectors
+    } else if (newdg && opts.pseudo && !(halfe || camkin)) {
       if (res->n_finish > 0 && !refreshed) {
         // the finish's rotation angles use the energies of the current vectors
         MB_TRY(mb_orbital_energies_ws(n, c->f, c->c, c->eigs, c->eig_ws, s));
@@ -769,7 +828,7 @@ extern "C" int mb_scf_run(mb_ctx* c, const mb_scf_opts* opts_in, mb_scf_result* 
     } else {
       MB_TRY(mb_density_dev(n, nclose, 2.0, c->c, n, c->p, s));
     }
-    const bool do_cnvg = !(newdg && okpuly);  // iter.F90:899
+    const bool do_cnvg = !interpolated && !(newdg && okpuly);  // iter.F90:899
     if (do_cnvg) MB_TRY(mb_cnvg_ws(n, c->p, pold, pold2, niter, c->scal + 1, c->scal + 8, s));
     half_kernel<<<hblocks, 256, 0, s>>>(mpack, c->p, c->pa);
     MB_LAUNCH_CHECK();

@@ -36,6 +36,8 @@ class ScfResult:
     n_split: int = 0
     n_finish: int = 0
     dp: float = -1.0
+    n_interp: int = 0        # Camp-King interpolated passes
+    forced_on: bool = False  # iter forced all convergers on (niter > itrmax - 10)
 
 
 class ScfContext:
@@ -86,12 +88,13 @@ class ScfContext:
     def run(self, pseudo: bool = False, scfcrt: float = 1.0e-4, itrmax: int = 2000, precision: int = 0,
             switch_pl: float = 1.0e-4, verbose: bool = False, pulay: bool = False,
             guess: bool = False, finish_dp: float = -1.0, finish_max: int = 40,
-            shift: float | None = None) -> ScfResult:
+            shift: float | None = None, camp: bool = False) -> ScfResult:
         """finish_dp: the FP64 finish (mb_scf_opts.finish_dp): < 0 automatic
         (1e-7 with precision=1, off with precision=0), 0 off, > 0 the bound on
         the last density update max|P_k - P_(k-1)| before convergence is
         accepted.  shift: the SHIFT=n keyword (None: the default level shift;
-        0: no level shift, SCF/iter.F90:131-136)."""
+        0: no level shift, SCF/iter.F90:131-136).  camp: the CAMP keyword
+        (Camp-King's interp, mb_scf_opts.camp)."""
         o = ScfOpts()
         lib().mb_scf_opts_default(ctypes.byref(o))
         o.pseudo = int(pseudo)
@@ -106,11 +109,12 @@ class ScfContext:
         o.finish_max = int(finish_max)
         if shift is not None:
             o.bshift = -float(shift)
+        o.camp = int(camp)
         r = ScfRes()
         check(lib().mb_scf_run(self._h, ctypes.byref(o), ctypes.byref(r)))
         return ScfResult(r.escf, r.ee, r.niter, bool(r.converged), r.n_full_diag, r.n_pseudo_diag, r.pl,
                          r.t_fock_ms, r.t_diag_ms, r.t_density_ms, r.t_other_ms, r.t_total_ms, r.n_pulay, r.n_split,
-                         r.n_finish, r.dp)
+                         r.n_finish, r.dp, r.n_interp, bool(r.forced_on))
 
     def density(self) -> np.ndarray:
         p = np.empty(self.mpack)

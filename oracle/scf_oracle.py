@@ -6,7 +6,8 @@ thing measured or shipped.
 
 What it restates:
   * ``iter`` (SCF/iter.F90:16-1107) for closed-shell RHF with the default
-    keywords (no UHF, no Camp-King, no C.I., id = 0): level-shift control
+    keywords (no UHF, no C.I., id = 0), Camp-King optional (``camp``,
+    oracle/campking_oracle.py, and iter's forced switch-on): level-shift control
     (:273-325), Fock build (:553), energy (:641-659), convergence test
     (:675-690), full diagonalisation (:849) or, in ``pseudo`` mode, the
     pseudo-diagonalisation the reference comments out (:847-861), density
@@ -465,12 +466,14 @@ class ScfResult:
     converged: bool
     history: list
     n_finish: int = 0
+    n_interp: int = 0       # interpolated iterations (Camp-King's mode 3)
+    forced_on: bool = False  # iter forced all convergers on (niter > itrmax - 10)
 
 
 def iter_scf(s: System, pseudo: bool = False, scfcrt: float = 1.0e-4, itrmax: int = 2000,
              gnorm: float = 0.0, trace: bool = False, pulay_on: bool = False,
              p_guess: np.ndarray | None = None, finish_dp: float = 0.0,
-             finish_max: int = 40, shift_kw: float | None = None) -> ScfResult:
+             finish_max: int = 40, shift_kw: float | None = None, camp: bool = False) -> ScfResult:
     """Closed-shell restatement of iter (SCF/iter.F90), 1SCF settings
     (last = 1, nscf = 0, fulscf = .true.).
 
@@ -487,7 +490,16 @@ def iter_scf(s: System, pseudo: bool = False, scfcrt: float = 1.0e-4, itrmax: in
     finish_dp (max|P_k - P_(k-1)| over all mpack elements); otherwise the
     loop goes on, at most finish_max more iterations, and the rotation
     sweep's relative threshold bigeps (diag_for_GPU.F90:33) is 0 in those
-    iterations.  The pseudo-diagonalisation takes its rotation angles from
+    iterations.
+
+    camp: the CAMP keyword (iter.F90:134): Camp-King's interp on the alpha
+    vectors from the third iteration (:781-798), a full diagonalisation in
+    every iteration, and an interpolated iteration (interp's mode 3) neither
+    counts nor tests convergence (:342-343, :662) and skips Pulay, the
+    diagonalisation and cnvg (:800, :888).  Without it iter still forces all
+    convergers on when niter passes itrmax - 10 (:351-372): Pulay and
+    Camp-King on, a constant shift (bshift = 4.44), iredy = -4, and the
+    iteration count restarts.  The pseudo-diagonalisation takes its rotation angles from
     the orbital energies of the last full diagonalisation, which carry that
     iteration's level shift (-8 eV on the virtuals with Pulay); at its first
     iteration the finish replaces them by the energies of the current
@@ -513,7 +525,10 @@ def iter_scf(s: System, pseudo: bool = False, scfcrt: float = 1.0e-4, itrmax: in
     okpuly = pulay_on
     pst = PulayState(s.norbs) if pulay_on else None
     halfe = False
-    camkin = False
+    camkin = bool(camp)
+    allcon = okpuly or camkin           # iter.F90:142
+    modea = 1 if camkin else 0          # label 180 (:322-330)
+    ck = None                           # interp's state, made on its first call
     trans = 0.2
     na1el = nclose
     nb1el = nclose
@@ -563,10 +578,38 @@ def iter_scf(s: System, pseudo: bool = False, scfcrt: float = 1.0e-4, itrmax: in
     dp = np.inf          # max|P_k - P_(k-1)| of the last density update
     n_finish = 0         # iterations the finish added after iter's test passed
     refreshed = False    # orbital energies refreshed for the finish
+    n_interp = 0                        # interpolated passes (interp mode 3)
+    forced_on = False
     while True:  # label 250
-        niter += 1
+        incitr = modea != 3
+        if incitr:
+            niter += 1
         if niter > itrmax:
             break
+        if niter > itrmax - 10 and not allcon:
+            # SWITCH ON ALL CONVERGERS (:351-372), then label 180
+            okpuly = True
+            camkin = not halfe
+            allcon = True
+            bshift = 4.44
+            iredy = -4
+            eold = 100.0
+            newdg = False
+            if pst is None:
+                # pulay's histories start at pold and pold2 (the same arrays
+                # in the reference): carry cnvg's heads over
+                pst = PulayState(s.norbs)
+                pst.fppf[:mpack] = pold
+                pst.fock[:n] = pold2
+                pold = pst.fppf[:mpack]
+                pold2 = pst.fock[:n]
+            pst.start = True
+            niter = 0
+            modea = 1 if camkin else 0
+            forced_on = True
+            if trace:
+                history.append(dict(niter=0, escf=None, pl=pl, shift=shift, newdg=newdg, allcon=True))
+            continue
         if abs(shift) > 1.0e-10 and bshift != 0.0:
             if niter > 1:
                 if newdg and not (halfe or camkin):
@@ -609,6 +652,8 @@ def iter_scf(s: System, pseudo: bool = False, scfcrt: float = 1.0e-4, itrmax: in
             fock2(s, f, p, pa)
             ee = helect(n, pa, h, f) * 2.0
             escf = (ee + s.enuclr) * enrgy + s.atheat + scorr
+            if not incitr:      # an interpolated point: no energy test (:662)
+                break
             diff = escf - eold
             if diff > 0:
                 ten = ten - 1.0
@@ -630,11 +675,29 @@ def iter_scf(s: System, pseudo: bool = False, scfcrt: float = 1.0e-4, itrmax: in
             break
         if converged:
             break
-        ready = iredy > 0 and (abs(diff) < sellim * 10.0 or pl == 0.0)
-        iredy += 1
-        eold = escf
+        if incitr:
+            ready = iredy > 0 and (abs(diff) < sellim * 10.0 or pl == 0.0)
+            iredy += 1
+            eold = escf
         if trace:
-            history.append(dict(niter=niter, escf=escf, pl=pl, shift=shift, newdg=newdg))
+            history.append(dict(niter=niter, escf=escf, pl=pl, shift=shift, newdg=newdg, mode=modea))
+        if niter > 2 and camkin:        # :781-798 (makea is always true for RHF)
+            if ck is None:
+                from oracle.campking_oracle import CampKing
+                ck = CampKing(n)
+            modea = ck.interp(na1el, n - na1el, modea, escf / enrgy, f, c)
+            if modea == 3:
+                n_interp += 1
+        p_before = p
+        if modea == 3:                  # interpolated vectors: no Pulay, no diagonalisation, no cnvg
+            p = density(c, nclose)
+            dp = float(np.max(np.abs(p - p_before)))
+            pa = p * 0.5
+            oknewd = pl < sellim or oknewd
+            newdg = (pl < trans and oknewd) or newdg
+            if pl < trans * 0.3333:
+                oknewd = True
+            continue
         if newdg and okpuly and iredy > 1:
             pl = pulay(pst, f, pa)
         if newdg and pseudo and not (halfe or camkin):
@@ -647,7 +710,6 @@ def iter_scf(s: System, pseudo: bool = False, scfcrt: float = 1.0e-4, itrmax: in
             pseudo_diag(f, c, na1el, eigs, bigeps=0.0 if n_finish > 0 else 1.5e-7)
         else:
             c, eigs = eigenvectors_lapack(f, n)
-        p_before = p
         p = density(c, nclose)
         if not (newdg and okpuly):
             pl = cnvg(n, p, pold, pold2, niter)
@@ -663,7 +725,7 @@ def iter_scf(s: System, pseudo: bool = False, scfcrt: float = 1.0e-4, itrmax: in
     c, eigs = eigenvectors_lapack(fcopy, n)
     escf = (ee + s.enuclr) * enrgy + s.atheat
     return ScfResult(escf=escf, ee=ee, eigs=eigs, c=c, p=p, niter=niter, converged=converged,
-                     history=history, n_finish=n_finish)
+                     history=history, n_finish=n_finish, n_interp=n_interp, forced_on=forced_on)
 
 
 # ---------------------------------------------------------------- fixed point
