@@ -195,6 +195,15 @@ int mb_ctx_atoms_dev(mb_ctx* ctx, MbAtomsDev* out);
  * corrections (PM7 dispersion, hydrogen bonds) are not included. */
 int mb_ctx_gradient(mb_ctx* ctx, double* dxyz);
 
+/* dfock2 (forces/dfock2.F90:16-279) on device arrays: f (in/out), ptot, p
+ * packed (mpack), w the derivative integrals of the pairs (nati, jj) in
+ * partner order, mb_dfock2_w_len values (100 / 10 / 1 per heavy-heavy /
+ * heavy-light / light-light pair); nfirst, nlast host, 1-based; nati
+ * 1-based.  Bit-identical to the reference's loop.  mb_dfock2_w_len returns
+ * -1 for bad arguments or d orbitals. */
+long long mb_dfock2_w_len(int numat, const int* nfirst, const int* nlast, int nati);
+int mb_dfock2_dev(int numat, const int* nfirst, const int* nlast, int nati, double* f, const double* ptot,
+                  const double* p, const double* w, cudaStream_t stream);
 /* The same on device arrays: nat_d/coord_d (A) as for mb_hcore_dev, p the
  * packed density; ws of mb_dcart_ws_bytes(numat) bytes (3 doubles per
  * atom pair); dxyz_dev 3*numat doubles. */
@@ -727,6 +736,11 @@ void fock2_(double* f, const double* ptot, const double* p, const double* w, con
             const int* mode);
 /* helect(n, p, h, f), integrals/helect.F90:16 */
 double helect_(const int* n, const double* p, const double* h, const double* f);
+/* dfock2(f, ptot, p, w, numat, nfirst, nlast, nati), forces/dfock2.F90:16
+ * (called at forces/deri1.F90:107): the two-centre Fock-matrix derivative
+ * of atom nati (1-based) added to f; host arrays, s and sp atoms. */
+void dfock2_(double* f, const double* ptot, const double* p, const double* w, const int* numat,
+             const int* nfirst, const int* nlast, const int* nati);
 /* cnvg(pnew, p, p1, niter, pl), SCF/cnvg.F90:16 (RHF).  norbs comes from
  * molkst_C in the reference; a Fortran host sets it once with mb_set_norbs. */
 void cnvg_(double* pnew, double* p, double* p1, const int* niter, double* pl);

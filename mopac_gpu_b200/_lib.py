@@ -182,6 +182,9 @@ SIGNATURES = {
     "destroy_handle": ([], None),
     "mopac_cuda_destroy_resources": ([], None),
     "fock2_": ([_P] * 10, None),
+    "dfock2_": ([_P] * 8, None),
+    "mb_dfock2_w_len": ([_I, _P, _P, _I], ctypes.c_longlong),
+    "mb_dfock2_dev": ([_I, _P, _P, _I, _P, _P, _P, _P, _P], _I),
     "helect_": ([_P] * 4, _D),
     "cnvg_": ([_P] * 5, None),
     "mb_set_norbs_": ([_P], None),

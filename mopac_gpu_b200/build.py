@@ -21,7 +21,8 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I", os.path.join(ROOT, "include"), "-I", CSRC]
 # Kernels whose FP64 arithmetic must follow the reference's operation order
 # exactly are built without multiply-add contraction.
-NO_FMA = {"fock.cu", "scf_kernels.cu", "mozyme.cu", "mozyme_diagg.cu", "batch.cu", "guess.cu", "mozyme_scf.cu"}
+NO_FMA = {"fock.cu", "dfock.cu", "scf_kernels.cu", "mozyme.cu", "mozyme_diagg.cu", "batch.cu", "guess.cu",
+          "mozyme_scf.cu"}
 
 
 def sources():

@@ -324,6 +324,38 @@ extern "C" void fock2_(double* f, const double* ptot, const double* p, const dou
   report(rc, "fock2_");
 }
 
+extern "C" long long mb_dfock2_w_len(int numat, const int* nfirst, const int* nlast, int nati);
+extern "C" int mb_dfock2_dev(int numat, const int* nfirst, const int* nlast, int nati, double* f, const double* ptot,
+                             const double* p, const double* w, cudaStream_t s);
+
+extern "C" void dfock2_(double* f, const double* ptot, const double* p, const double* w, const int* numat,
+                        const int* nfirst, const int* nlast, const int* nati) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  const int na = numat ? *numat : 0;
+  const long long nw = (na > 0 && nati) ? mb_dfock2_w_len(na, nfirst, nlast, *nati) : -1;
+  if (nw < 0 || !f || !ptot || !p || !w) {
+    report(mb_set_error(MB_ERR_ARG, "dfock2_: bad arguments or an atom with d orbitals"), "dfock2_");
+    return;
+  }
+  const int norbs = nlast[na - 1];
+  const size_t mp = (size_t)norbs * (norbs + 1) / 2;
+  int rc = ensure_stream();
+  if (rc == MB_OK) rc = g_a.get(sizeof(double) * mp * 3);
+  if (rc == MB_OK) rc = g_b.get(sizeof(double) * (size_t)(nw > 0 ? nw : 1));
+  double *df = (double*)g_a.p, *dpt = df + mp, *dp = dpt + mp;
+  if (rc == MB_OK && (cudaMemcpyAsync(df, f, sizeof(double) * mp, cudaMemcpyHostToDevice, g_stream) != cudaSuccess ||
+                      cudaMemcpyAsync(dpt, ptot, sizeof(double) * mp, cudaMemcpyHostToDevice, g_stream) != cudaSuccess ||
+                      cudaMemcpyAsync(dp, p, sizeof(double) * mp, cudaMemcpyHostToDevice, g_stream) != cudaSuccess ||
+                      (nw > 0 && cudaMemcpyAsync(g_b.p, w, sizeof(double) * (size_t)nw, cudaMemcpyHostToDevice,
+                                                 g_stream) != cudaSuccess)))
+    rc = MB_ERR_CUDA;
+  if (rc == MB_OK) rc = mb_dfock2_dev(na, nfirst, nlast, *nati, df, dpt, dp, (const double*)g_b.p, g_stream);
+  if (rc == MB_OK && cudaMemcpyAsync(f, df, sizeof(double) * mp, cudaMemcpyDeviceToHost, g_stream) != cudaSuccess)
+    rc = MB_ERR_CUDA;
+  if (rc == MB_OK && cudaStreamSynchronize(g_stream) != cudaSuccess) rc = MB_ERR_CUDA;
+  report(rc, "dfock2_");
+}
+
 extern "C" double helect_(const int* n, const double* p, const double* h, const double* f) {
   std::lock_guard<std::mutex> lk(g_mu);
   const int nn = *n;
