@@ -386,10 +386,10 @@ int mb_mz_layout_destroy(MbMzLayout* layout);
  * *enuclr_dev the core-core energy over every atom pair (pairs not stored:
  * outer2's monopole in the cutof2-cutof1 band, outer1's feathered point
  * charge beyond).  nat, coord: device (atomic numbers; Angstrom).  ws:
- * mb_mz_hcore_ws_bytes(layout) bytes of device scratch.  Needs cutof2 >= 49
- * (7 A squared): below PM7's feathering distance the reference's far pairs
- * carry dipole terms this path does not form, so the call returns
- * MB_ERR_UNSUPPORTED, as mb_mz_fock_dev does. */
+ * mb_mz_hcore_ws_bytes(layout) bytes of device scratch.  Any cutoff: a far
+ * pair inside PM7's 7 A feathering radius takes outer1's or outer2's
+ * diagonal terms (MOZYME/outer1.F90, outer2.F90), one beyond it the rotated
+ * core attraction, which is the same point charge there. */
 size_t mb_mz_hcore_ws_bytes(const MbMzLayout* layout);
 int mb_mz_hcore_dev(const MbMzLayout* layout, const int* nat, const double* coord, double* h, double* w,
                     double* enuclr, void* ws, cudaStream_t stream);
@@ -425,10 +425,18 @@ int mb_mz_density_dev(const MbMzLayout* layout, const MbMzLmos* lmos, int mode, 
  * other pair, then each atom's one-centre terms.  coord: device, numat x 3
  * Angstrom.  Needs cutof2 >= 49 (7 A), where the reference's feathering
  * weight is exactly zero for every pair outside the cutoff, so its dipole
- * terms vanish.  Bit-identical to the reference's loop. */
+ * terms vanish (mb_mz_fock_nat_dev takes shorter cutoffs).  Bit-identical
+ * to the reference's loop. */
 size_t mb_mz_fock_ws_bytes(const MbMzLayout* layout);
 int mb_mz_fock_dev(const MbMzLayout* layout, const double* coord, const double* w, const double* ptot,
                    const double* h, double* f, void* ws, cudaStream_t stream);
+/* The same with the atomic numbers (device, numat ints), which a cutoff
+ * below 7 A needs: a pair outside cutof2 but inside PM7's 7 A feathering
+ * radius takes fock2z's feathered monopole and, inside cutof1, its dipole
+ * terms (MOZYME/fock2z.F90:440-634); mb_mz_fock_dev (nat = NULL) refuses
+ * such cutoffs with MB_ERR_UNSUPPORTED. */
+int mb_mz_fock_nat_dev(const MbMzLayout* layout, const int* nat, const double* coord, const double* w,
+                       const double* ptot, const double* h, double* f, void* ws, cudaStream_t stream);
 
 /* diagg1 (MOZYME/diagg1.F90:16-503): F psi for every virtual LMO, the virtual
  * LMO energies eigv, the occupied-virtual interaction list (fmo) -- rebuilt
@@ -522,6 +530,8 @@ typedef struct mb_mz_scf_opts {
   int itrmax;      /* iteration cap (default 2000)                           */
   long long cap;   /* capacity of the interaction lists (0: 300 norbs)       */
   int verbose;     /* one line per iteration to stderr                       */
+  const int* nat;  /* atomic numbers on the device, or NULL; needed for a
+                      cutoff below 7 A (mb_mz_fock_nat_dev)                  */
 } mb_mz_scf_opts;
 typedef struct mb_mz_scf_result {
   double escf;          /* heat of formation, kcal/mol (no post-SCF terms)   */

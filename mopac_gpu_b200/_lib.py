@@ -45,7 +45,7 @@ class MbMzLmos(ctypes.Structure):
 
 class MzScfOpts(ctypes.Structure):
     _fields_ = [("scfcrt", ctypes.c_double), ("itrmax", ctypes.c_int), ("cap", ctypes.c_longlong),
-                ("verbose", ctypes.c_int)]
+                ("verbose", ctypes.c_int), ("nat", ctypes.c_void_p)]
 
 
 class MzScfRes(ctypes.Structure):
@@ -144,6 +144,7 @@ SIGNATURES = {
                           _I, _P, _P, _P, _P, ctypes.POINTER(_LL), _P, _P, ctypes.POINTER(_I),
                           ctypes.POINTER(_D), _P, _P], _I),
     "mb_mz_fock_dev": ([ctypes.POINTER(MbMzLayout), _P, _P, _P, _P, _P, _P, _P], _I),
+    "mb_mz_fock_nat_dev": ([ctypes.POINTER(MbMzLayout)] + [_P] * 8, _I),
     "mb_mz_helecz_ws_bytes": ([], ctypes.c_size_t),
     "mb_mz_helecz_ws": ([_LL, _I, _P, _P, _P, _P, _P, _P, _P], _I),
     "mb_mz_cnvgz_ws_bytes": ([], ctypes.c_size_t),

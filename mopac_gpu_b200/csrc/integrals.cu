@@ -799,6 +799,53 @@ __global__ void mz_hcore_pairs(MbMzLayout L, const int* __restrict__ nat, const 
   }
 }
 
+// The diagonal-block terms of a pair outside cutof2: outer2 (MOZYME/outer2.F90,
+// mode 0: reppd's monopole and dipoles along the unit vector j -> i) in
+// cutof1's band, outer1 (MOZYME/outer1.F90, mode 0: a feathered point charge)
+// beyond it.  e1b: atom i's block, e2a: atom j's (packed, 10 for sp).
+__device__ void mz_outer_terms(int ni, int nj, const double* ci, const double* cj, bool band, double* e1b,
+                               double* e2a) {
+  for (int k = 0; k < 10; ++k) { e1b[k] = 0.0; e2a[k] = 0.0; }
+  const Pm7Elem& I = c_P.el[ni];
+  const Pm7Elem& J = c_P.el[nj];
+  if (!band) {
+    const double rij = sqrt((ci[0] - cj[0]) * (ci[0] - cj[0]) + (ci[1] - cj[1]) * (ci[1] - cj[1]) +
+                            (ci[2] - cj[2]) * (ci[2] - cj[2]));
+    const double r = rij / PM7_A0;
+    double aee = 0.5 / I.am + 0.5 / J.am;
+    aee = aee * aee;
+    double ww = PM7_EV / sqrt(r * r + aee), point, cst;
+    to_point(rij, &point, &cst);
+    ww = ww * cst + (1.0 - cst) * point;
+    const int dg[4] = {0, 2, 5, 9};
+    for (int k = 0; k < 4; ++k) {
+      e1b[dg[k]] = -ww * J.tore;
+      e2a[dg[k]] = -ww * I.tore;
+    }
+    return;
+  }
+  double x[3] = {ci[0] - cj[0], ci[1] - cj[1], ci[2] - cj[2]};
+  const double rij = sqrt(x[0] * x[0] + x[1] * x[1] + x[2] * x[2]);
+  double ri[23], gab;
+  reppd(ni, nj, rij, ri, &gab);
+  const double a = 1.0 / rij;
+  x[0] *= a; x[1] *= a; x[2] *= a;
+  if (fabs(x[2]) > 0.99999999) x[2] = x[2] >= 0.0 ? 1.0 : -1.0;
+  const double w1 = ri[1];
+  e1b[0] = -w1 * J.tore;
+  e2a[0] = -w1 * I.tore;
+  if (J.natorb > 1) {
+    const double w2 = -ri[5] * x[0], w3 = -ri[5] * x[1], w4 = -ri[5] * x[2];
+    e2a[1] = -w2 * I.tore; e2a[2] = -w1 * I.tore; e2a[3] = -w3 * I.tore;
+    e2a[5] = -w1 * I.tore; e2a[6] = -w4 * I.tore; e2a[9] = -w1 * I.tore;
+  }
+  if (I.natorb > 1) {
+    const double w5 = -ri[2] * x[0], w6 = -ri[2] * x[1], w7 = -ri[2] * x[2];
+    e1b[1] = -w5 * J.tore; e1b[2] = -w1 * J.tore; e1b[3] = -w6 * J.tore;
+    e1b[5] = -w1 * J.tore; e1b[6] = -w7 * J.tore; e1b[9] = -w1 * J.tore;
+  }
+}
+
 __global__ void mz_hcore_diag(MbMzLayout L, const int* __restrict__ nat, const double* __restrict__ coord,
                               double* __restrict__ h, double* __restrict__ w, const double* __restrict__ enuc_entry,
                               double* __restrict__ enuc_atom) {
@@ -841,6 +888,19 @@ __global__ void mz_hcore_diag(MbMzLayout L, const int* __restrict__ nat, const d
     }
     if (r2 < 0.00002) continue;
     double p[4][4], core[5][3], e1b[10], e2a[10];
+    if (!(r2 < L.cutof2) && sqrt(r2) < 7.0) {
+      // a far pair inside PM7's 7 A feathering radius (a cutoff below 7 A):
+      // outer1's or outer2's terms; beyond 7 A elenuc's feathered integrals
+      // are the same point charges
+      if (B < A) {
+        mz_outer_terms(nA, nB, xa, xb, r2 < L.cutof1, e1b, e2a);
+        for (int x = 0; x < lA; ++x) blk[x] = blk[x] + e1b[x] * 1.0;
+      } else {
+        mz_outer_terms(nB, nA, xb, xa, r2 < L.cutof1, e1b, e2a);
+        for (int x = 0; x < lA; ++x) blk[x] = blk[x] + e2a[x] * 1.0;
+      }
+      continue;
+    }
     if (B < A) {
       const double r = rotmat(xa, xb, p);
       core_terms(nA, nB, r, core);
@@ -1069,11 +1129,10 @@ extern "C" int mb_mz_hcore_dev(const MbMzLayout* L, const int* nat_d, const doub
                                double* enuclr_dev, void* ws, cudaStream_t stream) {
   if (!L || !nat_d || !coord_d || !h || !w || !enuclr_dev || !ws || L->numat <= 0)
     return mb_set_error(MB_ERR_ARG, "mb_mz_hcore_dev: bad args");
-  // Far pairs get the full rotated core attraction and the point-charge
-  // core-core term; that is the reference's outer2/outer1 only when every
-  // pair beyond cutof2 is past PM7's 7 A feathering (mndod.F90:800-822).
-  if (!(L->cutof2 >= 49.0))
-    return mb_set_error(MB_ERR_UNSUPPORTED, "mb_mz_hcore_dev: needs cutof2 >= 49 (7 A); shorter cutoffs feather");
+  // Far pairs past PM7's 7 A feathering (mndod.F90:800-822) take the
+  // rotated core attraction, which there is outer1's and outer2's point
+  // charge; those inside 7 A (a cutoff below 7 A) take outer1's and outer2's
+  // own terms, and every far pair the outer core-core term.
   MB_TRY(upload_params());
   double* enuc_entry = (double*)ws;
   double* enuc_atom = enuc_entry + L->npairs;

@@ -20,9 +20,11 @@
 #include <string.h>
 
 #include <algorithm>
+#include <mutex>
 #include <vector>
 
 #include "mb_common.cuh"
+#include "pm7_params.h"
 
 namespace {
 
@@ -195,6 +197,38 @@ __global__ void __launch_bounds__(256) copy_kernel(long long n, const double* __
 // ------------------------------------------------------------- fock2z
 constexpr double MZ_EV = 27.211386245988;
 constexpr double MZ_A0 = 0.529177210903;
+
+// The element parameters of fock2z's far-pair terms inside PM7's 7 A
+// feathering radius (am, ad, dd by atomic number), for cutoffs below 7 A.
+struct MzFar {
+  double am[9], ad[9], dd[9];
+};
+__constant__ MzFar c_far;
+
+int far_params_init() {
+  static std::mutex mu;
+  static bool done = false;
+  std::lock_guard<std::mutex> lk(mu);
+  if (done) return MB_OK;
+  Pm7Params P;
+  pm7_init(&P);
+  MzFar h;
+  for (int z = 0; z < 9; ++z) {
+    h.am[z] = P.el[z].am;
+    h.ad[z] = P.el[z].ad;
+    h.dd[z] = P.el[z].dd;
+  }
+  MB_CUDA(cudaMemcpyToSymbol(c_far, &h, sizeof(h)));
+  done = true;
+  return MB_OK;
+}
+
+// to_point (integrals/mndod.F90:3462-3486) with trunc_1 = 7, trunc_2 = 0.22:
+// the point-charge repulsion and the NDDO weight.
+__device__ __forceinline__ double mz_feather(double r, double* point) {
+  *point = DMUL(MZ_EV, MZ_A0) / r;
+  return r < 7.0 ? 1.0 - exp(-(r - 7.0) * (r - 7.0) * 0.22) : 0.0;
+}
 __constant__ int c_pidx[16] = {1, 2, 4, 7, 2, 3, 5, 8, 4, 5, 6, 9, 7, 8, 9, 10};
 
 __device__ __forceinline__ int tri1(int i, int j) {  // 1-based packed index of (i, j)
@@ -266,13 +300,18 @@ __device__ double mz_pair_diag_term(int a, int b, int t, const MbMzLayout& L, co
 // and p diagonal), then lane t folds element t over the 32 partners in
 // ascending order -- the order in which fz2n's pair loop reaches atom a -- and
 // the one-centre terms come last.
-__global__ void __launch_bounds__(128) mz_fock_diag(MbMzLayout L, const double* __restrict__ coord,
+// nat (device, may be null) is read only for far pairs inside 7 A, which a
+// cutoff of 7 A or more never has.
+__global__ void __launch_bounds__(128) mz_fock_diag(MbMzLayout L, const int* __restrict__ nat,
+                                                   const double* __restrict__ coord,
                                                    const double* __restrict__ w, const double* __restrict__ p,
                                                    const double* __restrict__ qe, const double* __restrict__ h,
                                                    double* __restrict__ f) {
   __shared__ double s_c[4][32][10];
   __shared__ double s_x[4][32];          // second addition (light atom, heavy partner)
-  __shared__ unsigned short s_m[4][32];  // bit t: element t gets s_c; bit 15: then s_x on element 0
+  __shared__ double s_d[4][32][3];       // a far pair's three dipole additions on every diagonal element
+  __shared__ unsigned short s_m[4][32];  // bit t: element t gets s_c; bit 14: diagonal elements then get
+                                         // s_d[0..2]; bit 15: element 0 then gets s_x
   const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
   const int a = blockIdx.x * 4 + wl;
   if (a >= L.numat) return;
@@ -312,13 +351,70 @@ __global__ void __launch_bounds__(128) mz_fock_diag(MbMzLayout L, const double* 
           }
         }
       } else {
-        // point-charge monopole (feathering weight zero beyond 7 A): w1 = ev a0 / r
-        const double point = evA0 / sqrt(r2);
-        const double c = DMUL(qe[b], point);
+        // a pair outside cutof2 (fock2z.F90:440-634): the point-charge
+        // monopole w1 = ev a0 / r, feathered inside 7 A (w1 const + (1 -
+        // const) point, which is the point charge itself where const = 0),
+        // and inside cutof1 the dipole terms, which vanish beyond 7 A
+        const double rij = sqrt(r2);
+        double point;
+        const double cst = mz_feather(rij, &point);
+        double w1 = point;
+        const int ii = a > b ? a : b, jj = a > b ? b : a;  // the pair loop's roles
+        if (cst != 0.0) {
+          const int ni = nat[ii], nj = nat[jj];
+          const double aee = 0.5 / c_far.am[ni] + 0.5 / c_far.am[nj];
+          w1 = MZ_EV / sqrt(r2 / (MZ_A0 * MZ_A0) + aee * aee);
+          w1 = w1 * cst + (1.0 - cst) * point;
+        }
+        const double c = DMUL(qe[b], w1);
         const int dg[4] = {0, 2, 5, 9};
         for (int q = 0; q < ia; ++q) {
           s_c[wl][lane][dg[q]] = c;
           mask |= (unsigned short)(1u << dg[q]);
+        }
+        if (cst != 0.0 && r2 < L.cutof1) {  // fock2z.F90:490-634
+          const int ni = nat[ii], nj = nat[jj];
+          const int iab = L.iorbs[ii], jba = L.iorbs[jj];
+          const double ux = dx / rij, uy = dy / rij;
+          double uz = dz / rij;
+          if (fabs(uz) > 0.99999999) uz = copysign(1.0, uz);
+          double w2 = 0.0, w3 = 0.0, w4 = 0.0, w5 = 0.0, w6 = 0.0, w7 = 0.0;
+          if (iab > 1) {
+            const double da = c_far.dd[ni], ade = 0.5 / c_far.ad[ni] + 0.5 / c_far.am[nj];
+            const double rp = sqrt((rij / MZ_A0 + da) * (rij / MZ_A0 + da) + ade * ade);
+            const double rm = sqrt((rij / MZ_A0 - da) * (rij / MZ_A0 - da) + ade * ade);
+            const double ri2 = MZ_EV * (0.5 / rp - 0.5 / rm) * cst;
+            w5 = ri2 * ux; w6 = ri2 * uy; w7 = ri2 * uz;
+          }
+          if (jba > 1) {
+            const double da = c_far.dd[nj], ade = 0.5 / c_far.am[ni] + 0.5 / c_far.ad[nj];
+            const double rp = sqrt((rij / MZ_A0 + da) * (rij / MZ_A0 + da) + ade * ade);
+            const double rm = sqrt((rij / MZ_A0 - da) * (rij / MZ_A0 - da) + ade * ade);
+            const double ri5 = -MZ_EV * (0.5 / rp - 0.5 / rm) * cst;
+            w2 = ri5 * ux; w3 = ri5 * uy; w4 = ri5 * uz;
+          }
+          // this atom's p-s elements take the partner's charge times its own
+          // dipole integrals; its diagonal takes the partner's p-s densities
+          // times the partner's, doubled
+          const bool mine_p = a == ii ? iab > 1 : jba > 1;
+          const bool part_p = a == ii ? jba > 1 : iab > 1;
+          const double qa = qe[b];
+          const double ma[3] = {a == ii ? w5 : w2, a == ii ? w6 : w3, a == ii ? w7 : w4};
+          const double mb[3] = {a == ii ? w2 : w5, a == ii ? w3 : w6, a == ii ? w4 : w7};
+          if (mine_p) {
+            const int sp[3] = {1, 3, 6};
+            for (int q = 0; q < 3; ++q) {
+              s_c[wl][lane][sp[q]] = DMUL(qa, ma[q]);
+              mask |= (unsigned short)(1u << sp[q]);
+            }
+          }
+          if (part_p) {
+            const long long pb = L.pair_off[L.pair_ptr[b + 1] - 1];
+            s_d[wl][lane][0] = DMUL(DMUL(p[pb + 1], mb[0]), 2.0);
+            s_d[wl][lane][1] = DMUL(DMUL(p[pb + 3], mb[1]), 2.0);
+            s_d[wl][lane][2] = DMUL(DMUL(p[pb + 6], mb[2]), 2.0);
+            mask |= (unsigned short)0x4000u;
+          }
         }
       }
     }
@@ -329,6 +425,11 @@ __global__ void __launch_bounds__(128) mz_fock_diag(MbMzLayout L, const double* 
       for (int t = 0; t < nt; ++t) {
         const unsigned mk = s_m[wl][t];
         if (mk & (1u << lane)) acc = DADD(acc, s_c[wl][t][lane]);
+        if ((mk & 0x4000u) && (lane == 0 || lane == 2 || lane == 5 || lane == 9)) {
+          acc = DADD(acc, s_d[wl][t][0]);
+          acc = DADD(acc, s_d[wl][t][1]);
+          acc = DADD(acc, s_d[wl][t][2]);
+        }
         if ((mk & 0x8000u) && lane == 0) acc = DADD(acc, s_x[wl][t]);
       }
     }
@@ -844,18 +945,25 @@ extern "C" size_t mb_mz_fock_ws_bytes(const MbMzLayout* L) {
   return L ? sizeof(double) * (size_t)L->numat : 0;
 }
 
-extern "C" int mb_mz_fock_dev(const MbMzLayout* L, const double* coord, const double* w, const double* ptot,
-                              const double* h, double* f, void* ws, cudaStream_t stream) {
+extern "C" int mb_mz_fock_nat_dev(const MbMzLayout* L, const int* nat, const double* coord, const double* w,
+                                  const double* ptot, const double* h, double* f, void* ws, cudaStream_t stream) {
   if (!L || !coord || !w || !ptot || !h || !f || !ws) return mb_set_error(MB_ERR_ARG, "mb_mz_fock_dev: bad args");
-  if (!(L->cutof2 >= 49.0))
-    return mb_set_error(MB_ERR_UNSUPPORTED, "mb_mz_fock_dev: needs cutof2 >= 49 (7 A); shorter cutoffs feather");
+  // far pairs inside PM7's 7 A feathering radius need the elements
+  if (!(L->cutof2 >= 49.0) && !nat)
+    return mb_set_error(MB_ERR_UNSUPPORTED, "mb_mz_fock_dev: cutof2 < 49 (7 A) needs nat (mb_mz_fock_nat_dev)");
+  if (nat) MB_TRY(far_params_init());
   double* qe = (double*)ws;
   mz_chrge<<<grid_for(L->numat), 256, 0, stream>>>(*L, ptot, qe);
   MB_LAUNCH_CHECK();
-  mz_fock_diag<<<(L->numat + 3) / 4, 128, 0, stream>>>(*L, coord, w, ptot, qe, h, f);
+  mz_fock_diag<<<(L->numat + 3) / 4, 128, 0, stream>>>(*L, nat, coord, w, ptot, qe, h, f);
   MB_LAUNCH_CHECK();
   const long long thr = L->npairs * 16;
   mz_fock_pairs<<<(unsigned)((thr + 255) / 256), 256, 0, stream>>>(*L, w, ptot, h, f);
   MB_LAUNCH_CHECK();
   return MB_OK;
+}
+
+extern "C" int mb_mz_fock_dev(const MbMzLayout* L, const double* coord, const double* w, const double* ptot,
+                              const double* h, double* f, void* ws, cudaStream_t stream) {
+  return mb_mz_fock_nat_dev(L, nullptr, coord, w, ptot, h, f, ws, stream);
 }

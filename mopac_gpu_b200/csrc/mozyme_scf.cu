@@ -260,6 +260,8 @@ extern "C" int mb_mz_hbonds_dev(const MbMzLayout* L, const MbMzLmos* occ, const 
 // consecutive iterations; ovmax is diagg1's tiny) and the shift control
 // (:615-628).  The host sees a few scalars per iteration.
 extern "C" size_t mb_mz_fock_ws_bytes(const MbMzLayout* layout);
+extern "C" int mb_mz_fock_nat_dev(const MbMzLayout* layout, const int* nat, const double* coord, const double* w,
+                                  const double* ptot, const double* h, double* f, void* ws, cudaStream_t stream);
 extern "C" int mb_mz_fock_dev(const MbMzLayout* layout, const double* coord, const double* w, const double* ptot,
                               const double* h, double* f, void* ws, cudaStream_t stream);
 extern "C" int mb_mz_density_dev(const MbMzLayout* layout, const MbMzLmos* lmos, int mode, const double* partp,
@@ -288,6 +290,7 @@ extern "C" void mb_mz_scf_opts_default(mb_mz_scf_opts* o) {
   o->itrmax = 2000;
   o->cap = 0;
   o->verbose = 0;
+  o->nat = nullptr;
 }
 
 namespace {
@@ -375,7 +378,7 @@ extern "C" int mb_mz_scf_run(const MbMzLayout* L, const int* iorbs_host, MbMzLmo
   };
   // the starting LMOs' density, Fock matrix and energy (iter_for_MOZYME.F90:439-473)
   MB_TRY(mb_mz_density_dev(L, occ, 0, nullptr, p, s));
-  MB_TRY(mb_mz_fock_dev(L, coord, w, p, h, f, fws, s));
+  MB_TRY(mb_mz_fock_nat_dev(L, opts.nat, coord, w, p, h, f, fws, s));
   double ee = 0.0;
   MB_TRY(energy(&ee));
   double escf = (ee + enuclr) * fpc9 + atheat;
@@ -427,7 +430,7 @@ extern "C" int mb_mz_scf_run(const MbMzLayout* L, const int* iorbs_host, MbMzLmo
       }
     }
     if (use3) MB_TRY(mb_mz_cnvgz_ws(n, mpack, p, pold, p1, p2, p3, niter, idiag, 1, scal + 1, cws, s));
-    MB_TRY(mb_mz_fock_dev(L, coord, w, p, h, f, fws, s));
+    MB_TRY(mb_mz_fock_nat_dev(L, opts.nat, coord, w, p, h, f, fws, s));
     MB_TRY(energy(&ee));
     if (!isfinite(ee)) return mb_set_error(MB_ERR_NUMERIC, "mb_mz_scf_run: non-finite energy");
     escf = (ee + enuclr) * fpc9 + atheat;

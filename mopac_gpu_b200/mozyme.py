@@ -140,16 +140,21 @@ def hcore(layout: Layout, nat, coord):
     return h, w, float(en.item())
 
 
-def fock(layout: Layout, coord, w, ptot, h, out=None):
+def fock(layout: Layout, coord, w, ptot, h, out=None, nat=None):
     """buildf(f, partf, 0): F = H + G(P) over the pair-block storage.  coord
     (numat x 3, Angstrom), w (the stored pairs' integrals, layout.nw), ptot
-    and h: CUDA float64 tensors."""
+    and h: CUDA float64 tensors; nat (CUDA int32 atomic numbers) is needed
+    for a cutoff below 7 A."""
     f = out if out is not None else torch.empty(layout.mpack, dtype=torch.float64, device="cuda")
     ws = torch.empty(int(lib().mb_mz_fock_ws_bytes(ctypes.byref(layout.s))) // 8 + 1, dtype=torch.float64,
                      device="cuda")
     c = coord.contiguous()
-    check(lib().mb_mz_fock_dev(ctypes.byref(layout.s), _ptr(c), _ptr(w), _ptr(ptot), _ptr(h), _ptr(f), _ptr(ws),
-                               _stream()))
+    if nat is None:
+        check(lib().mb_mz_fock_dev(ctypes.byref(layout.s), _ptr(c), _ptr(w), _ptr(ptot), _ptr(h), _ptr(f),
+                                   _ptr(ws), _stream()))
+    else:
+        check(lib().mb_mz_fock_nat_dev(ctypes.byref(layout.s), _ptr(nat.contiguous()), _ptr(c), _ptr(w), _ptr(ptot),
+                                       _ptr(h), _ptr(f), _ptr(ws), _stream()))
     return f
 
 
@@ -209,7 +214,8 @@ class _HbList:
 
 
 def iter_for_mozyme(layout: Layout, occ: Lmos, vir: Lmos, coord, w, h, enuclr: float, atheat: float,
-                    scfcrt: float = 1.0e-2, itrmax: int = 2000, cap: int | None = None, trace: bool = False):
+                    scfcrt: float = 1.0e-2, itrmax: int = 2000, cap: int | None = None, trace: bool = False,
+                    nat=None):
     """The MOZYME SCF loop (MOZYME/iter_for_MOZYME.F90:218-630) for a whole
     closed-shell system on the device: density, Fock and energy of the
     starting LMOs, then per iteration tidy's compression, check, eimp, diagg
@@ -219,7 +225,8 @@ def iter_for_mozyme(layout: Layout, occ: Lmos, vir: Lmos, coord, w, h, enuclr: f
     1SCF test and the shift control.  coord (numat x 3), w (the stored pairs'
     integrals) and h (pair blocks) are CUDA float64 tensors; occ and vir are
     updated in place.  The host sees scalars each iteration (energy, diagg1's
-    tiny) and, four times per SCF, hbonds' atom-pair flags.  Returns a dict:
+    tiny) and, four times per SCF, hbonds' atom-pair flags.  nat (CUDA
+    int32 atomic numbers) is needed for a cutoff below 7 A.  Returns a dict:
     escf, ee, niter, converged, history, p, f."""
     fpc9 = 23.060547830619029
     n = layout.norbs
@@ -234,7 +241,7 @@ def iter_for_mozyme(layout: Layout, occ: Lmos, vir: Lmos, coord, w, h, enuclr: f
     nrejct = np.zeros(2, np.int32)
     L = lib()
     p = density(layout, occ, 0)
-    f = fock(layout, coord, w, p, h)
+    f = fock(layout, coord, w, p, h, nat=nat)
     ee = helecz(layout, p, h, f)
     escf = (ee + enuclr) * fpc9 + atheat
     pold = torch.zeros(layout.mpack, dtype=torch.float64, device="cuda")
@@ -279,7 +286,7 @@ def iter_for_mozyme(layout: Layout, occ: Lmos, vir: Lmos, coord, w, h, enuclr: f
                     idiagg += 1
         if use3:
             cnvgz(layout, p, pold, p1, p2, p3, niter, True)
-        f = fock(layout, coord, w, p, h)
+        f = fock(layout, coord, w, p, h, nat=nat)
         ee = helecz(layout, p, h, f)
         escf = (ee + enuclr) * fpc9 + atheat
         de = escf - eold
@@ -304,7 +311,8 @@ def iter_for_mozyme(layout: Layout, occ: Lmos, vir: Lmos, coord, w, h, enuclr: f
 
 
 def scf_run(layout: Layout, occ: Lmos, vir: Lmos, coord, w, h, enuclr: float, atheat: float,
-            scfcrt: float = 1.0e-2, itrmax: int = 2000, cap: int | None = None, verbose: bool = False):
+            scfcrt: float = 1.0e-2, itrmax: int = 2000, cap: int | None = None, verbose: bool = False,
+            nat=None):
     """The MOZYME SCF behind its C entry (mb_mz_scf_run): the loop of
     ``iter_for_mozyme`` run by the library.  Returns a dict: escf, ee, niter,
     converged, t_total_ms, nrejected, p, f."""
@@ -314,6 +322,8 @@ def scf_run(layout: Layout, occ: Lmos, vir: Lmos, coord, w, h, enuclr: float, at
     o.itrmax = int(itrmax)
     o.cap = int(cap or 0)
     o.verbose = int(verbose)
+    nat_d = None if nat is None else nat.contiguous()
+    o.nat = None if nat_d is None else nat_d.data_ptr()
     p = torch.empty(layout.mpack, dtype=torch.float64, device="cuda")
     f = torch.empty(layout.mpack, dtype=torch.float64, device="cuda")
     r = MzScfRes()

@@ -80,19 +80,20 @@ def test_plain_c_client_links_and_runs(libpath, tmp_path):
     assert "c_abi_client ok" in run.stdout
 
 
-def test_mozyme_hcore_refuses_cutoffs_below_the_feathering_distance(libpath):
-    """A 6 A cutoff puts far pairs inside PM7's point-charge feathering, which
-    the pair-block hcore does not form: the call is refused before it touches
-    the device (the pointers below are never dereferenced)."""
+def test_mozyme_fock_without_elements_refuses_cutoffs_below_the_feathering_distance(libpath):
+    """A 6 A cutoff puts far pairs inside PM7's point-charge feathering, whose
+    terms need the elements: mb_mz_fock_dev (no atomic numbers) refuses it
+    before it touches the device (the pointers below are never
+    dereferenced); mb_mz_fock_nat_dev takes it."""
     from mopac_gpu_b200._lib import MbMzLayout
     L = ctypes.CDLL(libpath)
-    L.mb_mz_hcore_dev.restype = ctypes.c_int
+    L.mb_mz_fock_dev.restype = ctypes.c_int
     L.mb_last_error.restype = ctypes.c_char_p
     lay = MbMzLayout()
     lay.numat = 3
     lay.cutof1, lay.cutof2 = 6.0, 5.9 ** 2
     fake = ctypes.c_void_p(256)
-    rc = L.mb_mz_hcore_dev(ctypes.byref(lay), fake, fake, fake, fake, fake, fake, None)
+    rc = L.mb_mz_fock_dev(ctypes.byref(lay), fake, fake, fake, fake, fake, fake, None)
     assert rc == 5  # MB_ERR_UNSUPPORTED
     assert b"cutof2" in L.mb_last_error()
 

@@ -302,16 +302,75 @@ def test_gpu_diagg2_bit_identical(nwater, padv):
 
 
 @pytest.mark.gpu
-def test_gpu_mozyme_fock_rejects_short_cutoff():
+@pytest.mark.parametrize("cut", [6.0, 5.0, 4.0])
+def test_gpu_mozyme_short_cutoff_matches_oracle(cut):
+    """Cutoffs below PM7's 7 A feathering radius: far pairs inside 7 A take
+    hcore's outer1 / outer2 terms and fock2z's feathered monopole and, in the
+    cutof2-cutof1 band (0.5 A wide here), its dipole terms.  H, W and the
+    core-core energy against the oracle to the integrals' parity; F to 1e-12
+    (the feathering weight's exp is CUDA's here, the C library's there);
+    without the elements the Fock build refuses such a cutoff."""
     torch = _need_gpu()
     from mopac_gpu_b200 import mozyme
     from mopac_gpu_b200._lib import LibraryError
-    nat, xyz = small_systems()["water16"]
-    iorbs = np.where(np.asarray(nat) == 1, 1, 4).astype(np.int32)
-    L = mozyme.Layout(iorbs, xyz, 6.0 ** 2 + 1e-4, 6.0 ** 2)
-    z = torch.zeros(max(L.mpack, int(L.s.nw), 3 * len(nat)), dtype=torch.float64, device="cuda")
+    nat, xyz, _ = workloads.water_box(64)
+    s = oracle_system(nat, xyz)
+    iorbs = (s.nlast - s.nfirst + 1).astype(np.int32)
+    c1, c2 = cut ** 2, (cut - 0.5) ** 2
+    mp, nb = mo.layout(iorbs, s.coord, c1, c2)
+    r = np.linalg.norm(s.coord[:, None, :] - s.coord[None, :, :], axis=-1)
+    assert ((nb == -2) & (r < 7.0)).sum() > 0 and ((nb == -1) & (r < 7.0)).sum() > 0
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    L = mozyme.Layout(iorbs, s.coord, c1, c2)
+    natd = dev(np.asarray(nat, np.int32))
+    ho, wo, eo = mo.hcore(nat, xyz, iorbs, nb, mp, s.w.size)
+    hg, wg, eg = mozyme.hcore(L, natd, dev(s.coord))
+    np.testing.assert_allclose(hg.cpu().numpy(), ho, rtol=1e-11, atol=1e-11)
+    np.testing.assert_allclose(wg.cpu().numpy(), wo, rtol=1e-11, atol=1e-12)
+    assert abs(eg - eo) <= 1e-10 * abs(eo)
+    rng = np.random.default_rng(int(cut))
+    x = rng.normal(size=(s.norbs, s.norbs)) * 0.1
+    pd = x + x.T + np.diag(rng.uniform(0.2, 1.8, s.norbs))
+    pb = mo.dense_to_blocks(pd, iorbs, nb, mp)
+    ref = mo.fock(s.nat, s.coord, iorbs, nb, s.w, pb, ho)
+    wz = mo.w_stored(iorbs, nb, s.w)
+    f = mozyme.fock(L, dev(s.coord), dev(wz), dev(pb), dev(ho), nat=natd).cpu().numpy()
+    np.testing.assert_allclose(f, ref, rtol=1e-12, atol=1e-12)
     with pytest.raises(LibraryError):
-        mozyme.fock(L, z[:3 * len(nat)], z, z[:L.mpack], z[:L.mpack])
+        mozyme.fock(L, dev(s.coord), dev(wz), dev(pb), dev(ho))
+    L.close()
+
+
+@pytest.mark.gpu
+def test_gpu_mozyme_scf_with_a_short_cutoff_follows_the_oracle_loop():
+    """The device MOZYME SCF with a 4 A cutoff (0.5 A dipole band) on an
+    eight-water lattice, against the oracle's loop from the same starting
+    LMOs: the same iterations and energies to 1e-8 kcal/mol."""
+    torch = _need_gpu()
+    from mopac_gpu_b200 import mozyme
+    nat, xyz = workloads.water_lattice(8, seed=2)
+    s = oracle_system(nat, xyz)
+    iorbs, occ, vir = mo.water_lewis_lmos(nat, xyz, pad_atoms=len(nat) - 3)
+    c1, c2 = 4.0 ** 2, 3.5 ** 2
+    mp, nb = mo.layout(iorbs, s.coord, c1, c2)
+    assert (nb == -2).sum() > 0 and (nb == -1).sum() > 0
+    hb = mo.dense_to_blocks(so.unpack(s.h, s.norbs), iorbs, nb, mp)
+    wz = mo.w_stored(iorbs, nb, s.w)
+    L = mozyme.Layout(iorbs, s.coord, c1, c2)
+    Qo, Qv = mozyme.Lmos(L, _copy_lmos(occ)), mozyme.Lmos(L, _copy_lmos(vir))
+    Ro, Rv = mozyme.Lmos(L, _copy_lmos(occ)), mozyme.Lmos(L, _copy_lmos(vir))  # before the oracle moves them
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    natd = dev(np.asarray(nat, np.int32))
+    rg = mozyme.iter_for_mozyme(L, Qo, Qv, dev(s.coord), dev(wz), dev(hb), s.enuclr, s.atheat, trace=True,
+                                nat=natd)
+    ro = mo.iter_for_mozyme(s, occ, vir, c1, c2, trace=True)
+    assert rg["converged"] and rg["niter"] == ro["niter"]
+    for a, b in zip(rg["history"], ro["history"]):
+        assert abs(a["escf"] - b["escf"]) < 1e-8
+    rb = mozyme.scf_run(L, Ro, Rv, dev(s.coord), dev(wz), dev(hb), s.enuclr, s.atheat, nat=natd)
+    assert rb["converged"] and rb["niter"] == rg["niter"] and abs(rb["escf"] - rg["escf"]) < 1e-9
+    for q in (Qo, Qv, Ro, Rv):
+        q.close()
     L.close()
 
 
