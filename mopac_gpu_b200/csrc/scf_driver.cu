@@ -614,8 +614,9 @@ extern "C" int mb_scf_run(mb_ctx* c, const mb_scf_opts* opts_in, mb_scf_result* 
       c->tc_ws = (void*)(((uintptr_t)c->tc_ws_raw + 1023) & ~(uintptr_t)1023);
       c->tc_ws_bytes = need;
     }
-    MB_CUDA(cudaMemsetAsync(c->status + 1, 0, sizeof(int), s));
   }
+  // the device wait flag of the split GEMMs and the rotation sweep
+  MB_CUDA(cudaMemsetAsync(c->status + 1, 0, sizeof(int), s));
   // FP64 finish: automatic (< 0) means on for the split precision only
   const double finish_dp = opts.finish_dp < 0.0 ? (opts.precision != 0 ? 1.0e-7 : 0.0) : opts.finish_dp;
   const int finish_max = opts.finish_max > 0 ? opts.finish_max : 0;
@@ -841,10 +842,11 @@ extern "C" int mb_scf_run(mb_ctx* c, const mb_scf_opts* opts_in, mb_scf_result* 
     t_dens.stop();
     if (do_cnvg) MB_TRY(d2h(c, &pl, c->scal + 1, 1));
     if (finishing) MB_TRY(d2h(c, &dp, c->scal + 2, 1));
-    if (opts.precision != 0 && res->n_split > 0) {
+    if (res->n_pseudo_diag > 0 || (opts.precision != 0 && res->n_split > 0)) {
       int terr = 0;
       MB_CUDA(cudaMemcpyAsync(&terr, c->status + 1, sizeof(int), cudaMemcpyDeviceToHost, s));
       MB_CUDA(cudaStreamSynchronize(s));
+      if (terr & 4) return mb_set_error(MB_ERR_CUDA, "rotation sweep: a dependency wait expired");
       if (terr) return mb_set_error(MB_ERR_CUDA, "tensor-core GEMM pipeline wait expired");
     }
     if (use_split && pl < opts.switch_pl) use_split = false;

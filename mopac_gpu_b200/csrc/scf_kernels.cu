@@ -250,119 +250,206 @@ __global__ void rot_coeff_kernel(int nocc, int nvirt, const double* __restrict__
 // (occupied i outer, virtual j inner) -- rotations on disjoint column pairs
 // commute exactly, so C is bit-identical to the sequential sweep.
 //
-// One cooperative launch per sweep: the anti-diagonals follow each other with
-// a grid barrier between them, and within one the CTAs take (tile, block of
-// CROWS rows) items in turn.  A CTA stages the tile's 256 coefficients in
-// shared memory (every thread reads them by broadcast) and each thread
-// rotates one row of the tile's 32 columns in registers.
+// One cooperative launch per sweep, scheduled as a dataflow graph: rows are
+// independent (a rotation mixes two columns of each row separately), so the
+// work item is (tile (I, J), block rb of CROWS rows), and item (I, J, rb)
+// depends on (I - 1, J, rb) and (I, J - 1, rb) only.  CTAs take items from a
+// queue ordered by anti-diagonal I + J, wait for the item's two predecessors'
+// done flags, rotate, and set the item's own flag -- no grid barrier, so
+// blocks of rows run ahead on later anti-diagonals while others finish the
+// current one.  Every predecessor of an item sits earlier in the queue and
+// was taken by a resident CTA (a CTA takes its next item only while working
+// on the current one), so the smallest unfinished item always has its inputs
+// and the sweep cannot stall; each wait is still bounded (2 s of
+// %globaltimer), after which the kernel raises an abort flag that ends every
+// CTA's loop and sets bit 4 of *err.  A CTA stages the tile's 256
+// coefficients in shared memory (every thread reads them by broadcast) and
+// each thread rotates one row of the tile's 32 columns in registers; the
+// arithmetic of every element is that of the sequential sweep, so C is
+// bit-identical to it.
 constexpr int CROWS = 128;
+constexpr unsigned long long kFlowWaitNs = 2000000000ull;
 
+__device__ __forceinline__ int ld_acquire_gpu(const int* p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release_gpu(int* p, int v) {
+  asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// sync[0]: queue head; sync[1]: abort; sync[2 + (I * ntile_v + J) * nrb + rb]:
+// done flag of item (I, J, rb).  All zero at launch.
 __global__ void __launch_bounds__(CROWS, 3) rot_sweep_kernel(int n, int nocc, int nvirt, double* __restrict__ c,
                                                             const double* __restrict__ alpha,
                                                             const double* __restrict__ beta,
                                                             const unsigned int* __restrict__ tile_cnt, int ntile_o,
-                                                            int ntile_v) {
-  cg::grid_group grid = cg::this_grid();
-  // (alpha, beta) of a tile's 256 pairs, double-buffered: the next item's
-  // coefficients are loaded while the current item's rotations run
+                                                            int ntile_v, int* __restrict__ sync,
+                                                            int* __restrict__ err) {
   __shared__ double2 s_ab[2][RT * RT];
   __shared__ double s_xi[RT][CROWS];   // the occupied values of each thread's row
+  __shared__ int s_next[4];            // the next item: I, J, rb, valid
+  __shared__ int s_go;                 // 0 once the sweep is aborted
   const int nrb = (n + CROWS - 1) / CROWS;
+  const int ndiag = ntile_o + ntile_v - 1;
+  int* const head = sync;
+  int* const abort_flag = sync + 1;
+  int* const done = sync + 2;
   constexpr int PER = RT * RT / CROWS;  // coefficients each thread stages
-  for (int t = 0; t < ntile_o + ntile_v - 1; ++t) {
+  // thread 0's cursor over the queue: items of anti-diagonal t are
+  // [t_start, t_start + width(t) * nrb), taken in increasing order
+  int t_cur = 0;
+  long long t_start = 0;
+  auto width = [&](int t) {
     const int jlo = t - (ntile_o - 1) > 0 ? t - (ntile_o - 1) : 0;
     const int jhi = t < ntile_v - 1 ? t : ntile_v - 1;
-    const int items = (jhi - jlo + 1) * nrb;
-    // items of this anti-diagonal that carry at least one rotation; the
-    // test is the same for every thread of the CTA
-    auto next_item = [&](int it) {
-      for (; it < items; it += gridDim.x) {
-        const int J = jlo + it / nrb, I = t - J;
-        if (tile_cnt[I * ntile_v + J] != 0) break;
-      }
-      return it;
-    };
-    auto tile_base = [&](int it) {
-      const int J = jlo + it / nrb, I = t - J;
-      return ((long long)I * ntile_v + J) * (RT * RT);
-    };
-    int it = next_item(blockIdx.x);
-    int buf = 0;
-    if (it < items) {
-      const long long tb = tile_base(it);
+    return jhi - jlo + 1;
+  };
+  auto take = [&]() {  // thread 0: the next item into s_next
+    const long long q = atomicAdd(head, 1);
+    while (t_cur < ndiag && q >= t_start + (long long)width(t_cur) * nrb) {
+      t_start += (long long)width(t_cur) * nrb;
+      ++t_cur;
+    }
+    if (t_cur >= ndiag) {
+      s_next[3] = 0;
+      return;
+    }
+    const long long loc = q - t_start;
+    const int jlo = t_cur - (ntile_o - 1) > 0 ? t_cur - (ntile_o - 1) : 0;
+    const int J = jlo + (int)(loc / nrb);
+    s_next[0] = t_cur - J;
+    s_next[1] = J;
+    s_next[2] = (int)(loc % nrb);
+    s_next[3] = 1;
+  };
+  auto stage = [&](int I, int J, double2* pre) {
+    const long long tb = ((long long)I * ntile_v + J) * (RT * RT);
 #pragma unroll
-      for (int q = 0; q < PER; ++q) {
-        const int e = threadIdx.x + q * CROWS;
-        s_ab[0][e] = make_double2(alpha[tb + e], beta[tb + e]);
+    for (int q = 0; q < PER; ++q) {
+      const int e = threadIdx.x + q * CROWS;
+      pre[q] = make_double2(alpha[tb + e], beta[tb + e]);
+    }
+  };
+  if (threadIdx.x == 0) {
+    take();
+    s_go = 1;
+  }
+  __syncthreads();
+  int I = s_next[0], J = s_next[1], rb = s_next[2], valid = s_next[3];
+  int buf = 0;
+  if (valid) {
+    double2 pre[PER];
+    stage(I, J, pre);
+#pragma unroll
+    for (int q = 0; q < PER; ++q) s_ab[0][threadIdx.x + q * CROWS] = pre[q];
+  }
+  __syncthreads();
+  while (valid) {
+    // the next item, and its coefficients in flight while this one runs
+    if (threadIdx.x == 0) take();
+    __syncthreads();
+    const int nI = s_next[0], nJ = s_next[1], nrb_ = s_next[2], nvalid = s_next[3];
+    double2 pre[PER];
+    if (nvalid) stage(nI, nJ, pre);
+    // wait for the item's predecessors
+    if (threadIdx.x == 0) {
+      bool ok = true;
+      const int* deps[2] = {I > 0 ? done + ((long long)(I - 1) * ntile_v + J) * nrb + rb : nullptr,
+                            J > 0 ? done + ((long long)I * ntile_v + (J - 1)) * nrb + rb : nullptr};
+      for (int d = 0; d < 2 && ok; ++d) {
+        if (!deps[d]) continue;
+        const unsigned long long t0 = global_ns();
+        while (ld_acquire_gpu(deps[d]) == 0) {
+          if (ld_acquire_gpu(abort_flag) != 0 || global_ns() - t0 > kFlowWaitNs) {
+            ok = false;
+            break;
+          }
+          __nanosleep(32);
+        }
+      }
+      if (!ok) {
+        atomicExch(abort_flag, 1);
+        if (err) atomicOr(err, 4);
+        s_go = 0;
       }
     }
     __syncthreads();
-    while (it < items) {
-      const int nx = next_item(it + gridDim.x);
-      double2 pre[PER];
-      if (nx < items) {
-        const long long tb = tile_base(nx);
+    if (!s_go) break;
+    const int r = rb * CROWS + threadIdx.x;
+    if (tile_cnt[I * ntile_v + J] != 0 && r < n) {
+      const int i0 = I * RT, j0 = J * RT;
+      const double2* ab = s_ab[buf];
+      // All 32 values of the thread's row are loaded at once (one memory
+      // latency per item; past L1, which may hold lines another SM has
+      // since rewritten): the 16 virtual ones stay in registers for the
+      // tile, the 16 occupied ones wait in shared memory, since occupied
+      // column u is touched by row u of the tile only.  A skipped pair
+      // carries the identity (alpha 1, beta 0): applying it leaves both
+      // values equal (1*a + 0*b == a), so the rotations run without a
+      // branch, each row's coefficients read from shared memory ahead of
+      // its dependent chain.
+      double xj[RT];
 #pragma unroll
-        for (int q = 0; q < PER; ++q) {
-          const int e = threadIdx.x + q * CROWS;
-          pre[q] = make_double2(alpha[tb + e], beta[tb + e]);
-        }
-      }
-      const int J = jlo + it / nrb, rb = it % nrb;
-      const int I = t - J;
-      const int r = rb * CROWS + threadIdx.x;
-      if (r < n) {
-        const int i0 = I * RT, j0 = J * RT;
-        const double2* ab = s_ab[buf];
-        // All 32 values of the thread's row are loaded at once (one memory
-        // latency per item): the 16 virtual ones stay in registers for the
-        // tile, the 16 occupied ones wait in shared memory, since occupied
-        // column u is touched by row u of the tile only.  A skipped pair
-        // carries the identity (alpha 1, beta 0): applying it leaves both
-        // values equal (1*a + 0*b == a), so the rotations run without a
-        // branch, each row's coefficients read from shared memory ahead of
-        // its dependent chain.
-        double xj[RT];
+      for (int u = 0; u < RT; ++u)
+        s_xi[u][threadIdx.x] = (i0 + u < nocc) ? __ldcg(c + (long long)(i0 + u) * n + r) : 0.0;
 #pragma unroll
-        for (int u = 0; u < RT; ++u) s_xi[u][threadIdx.x] = (i0 + u < nocc) ? c[(long long)(i0 + u) * n + r] : 0.0;
-#pragma unroll
-        for (int v = 0; v < RT; ++v) xj[v] = (j0 + v < nvirt) ? c[(long long)(nocc + j0 + v) * n + r] : 0.0;
+      for (int v = 0; v < RT; ++v) xj[v] = (j0 + v < nvirt) ? __ldcg(c + (long long)(nocc + j0 + v) * n + r) : 0.0;
 #pragma unroll 1
-        for (int u = 0; u < RT; ++u) {
-          double x = s_xi[u][threadIdx.x];
-          double2 w[RT];
+      for (int u = 0; u < RT; ++u) {
+        double x = s_xi[u][threadIdx.x];
+        double2 w[RT];
 #pragma unroll
-          for (int v = 0; v < RT; ++v) w[v] = ab[u * RT + v];
+        for (int v = 0; v < RT; ++v) w[v] = ab[u * RT + v];
 #pragma unroll
-          for (int v = 0; v < RT; ++v) {
-            const double b = xj[v];
-            const double na = DADD(DMUL(w[v].x, x), DMUL(w[v].y, b));
-            xj[v] = DSUB(DMUL(w[v].x, b), DMUL(w[v].y, x));
-            x = na;
-          }
-          s_xi[u][threadIdx.x] = x;
+        for (int v = 0; v < RT; ++v) {
+          const double b = xj[v];
+          const double na = DADD(DMUL(w[v].x, x), DMUL(w[v].y, b));
+          xj[v] = DSUB(DMUL(w[v].x, b), DMUL(w[v].y, x));
+          x = na;
         }
-#pragma unroll
-        for (int u = 0; u < RT; ++u)
-          if (i0 + u < nocc) c[(long long)(i0 + u) * n + r] = s_xi[u][threadIdx.x];
-#pragma unroll
-        for (int v = 0; v < RT; ++v)
-          if (j0 + v < nvirt) c[(long long)(nocc + j0 + v) * n + r] = xj[v];
+        s_xi[u][threadIdx.x] = x;
       }
-      if (nx < items) {
 #pragma unroll
-        for (int q = 0; q < PER; ++q) s_ab[buf ^ 1][threadIdx.x + q * CROWS] = pre[q];
-      }
-      __syncthreads();  // the next buffer is filled; the current one is free
-      buf ^= 1;
-      it = nx;
+      for (int u = 0; u < RT; ++u)
+        if (i0 + u < nocc) c[(long long)(i0 + u) * n + r] = s_xi[u][threadIdx.x];
+#pragma unroll
+      for (int v = 0; v < RT; ++v)
+        if (j0 + v < nvirt) c[(long long)(nocc + j0 + v) * n + r] = xj[v];
     }
-    grid.sync();
+    if (nvalid) {
+#pragma unroll
+      for (int q = 0; q < PER; ++q) s_ab[buf ^ 1][threadIdx.x + q * CROWS] = pre[q];
+    }
+    __syncthreads();  // the item's rows are written; the next buffer is filled
+    if (threadIdx.x == 0) {
+      __threadfence();
+      st_release_gpu(done + ((long long)I * ntile_v + J) * nrb + rb, 1);
+    }
+    buf ^= 1;
+    I = nI;
+    J = nJ;
+    rb = nrb_;
+    valid = nvalid;
   }
 }
 
+// sync ints a sweep needs: the queue head, the abort flag and a done flag per
+// (tile, row block) item.
+size_t flow_sync_ints(int n, int nocc) {
+  const size_t to = (size_t)(nocc + RT - 1) / RT, tv = (size_t)(n - nocc + RT - 1) / RT;
+  return 2 + to * tv * (size_t)((n + CROWS - 1) / CROWS);
+}
+
 int launch_wavefronts(int n, int nocc, int nvirt, double* c, const double* al, const double* be,
-                      const unsigned char* act, const unsigned int* tcnt, int to, int tv, cudaStream_t stream) {
+                      const unsigned char* act, const unsigned int* tcnt, int to, int tv, int* sync, int* err,
+                      cudaStream_t stream) {
   static int grid = 0;
   if (grid == 0) {
     int dev = 0, sms = 0, per = 0;
@@ -373,7 +460,9 @@ int launch_wavefronts(int n, int nocc, int nvirt, double* c, const double* al, c
     grid = sms * per;
   }
   (void)act;  // skipped pairs carry the identity rotation in al / be
-  void* args[] = {&n, &nocc, &nvirt, &c, &al, &be, &tcnt, &to, &tv};
+  MB_CUDA(cudaMemsetAsync(sync, 0, sizeof(int) * flow_sync_ints(n, nocc), stream));
+  void* args[] = {&n, &nocc, &nvirt, &c, &al, &be, &tcnt, &to, &tv, &sync, &err};
+  // cooperative: every CTA resident, which the dataflow queue relies on
   MB_CUDA(cudaLaunchCooperativeKernel((void*)rot_sweep_kernel, grid, CROWS, args, 0, stream));
   mb_count_launch();
   return MB_OK;
@@ -470,6 +559,7 @@ extern "C" size_t mb_pseudo_ws_bytes(int n, int nocc) {
   b += align256(kt);
   b += align256(sizeof(unsigned int) * (to * tv + 64));
   b += 256;
+  b += align256(sizeof(int) * flow_sync_ints(n, nocc));  // the sweep's queue and done flags
   return b;
 }
 
@@ -499,6 +589,7 @@ extern "C" int mb_pseudo_diag_ex(int n, int nocc, const double* fpacked, double*
   unsigned char* act = (unsigned char*)b; b += align256(kt);
   unsigned int* tcnt = (unsigned int*)b; b += align256(sizeof(unsigned int) * ((size_t)to * tv + 64));
   unsigned long long* tiny = (unsigned long long*)b;
+  int* sync = (int*)(b + 256);
   MB_TRY(mb_unpack_dev(n, fpacked, ff, n, 0, nullptr, stream));
   // diag_for_GPU.F90:116-150
   auto gemm = [&](char ta, char tb, int m, int nn, int k, const double* a, int lda, const double* bb, int ldb,
@@ -527,7 +618,7 @@ extern "C" int mb_pseudo_diag_ex(int n, int nocc, const double* fpacked, double*
   rot_coeff_kernel<<<cblocks, 256, 0, stream>>>(nocc, nvirt, fmo, eigs, tiny, -1.0, bigeps, al, be, act, tcnt, nrot_dev,
                                                  to, tv);
   MB_LAUNCH_CHECK();
-  return launch_wavefronts(n, nocc, nvirt, c, al, be, act, tcnt, to, tv, stream);
+  return launch_wavefronts(n, nocc, nvirt, c, al, be, act, tcnt, to, tv, sync, split_err, stream);
 }
 
 namespace {
@@ -587,6 +678,8 @@ extern "C" int mb_rot_sweep_ws(int n, int nocc, const double* fmo, const double*
   double* be = (double*)b; b += align256(sizeof(double) * kt);
   unsigned char* act = (unsigned char*)b; b += align256(kt);
   unsigned int* tcnt = (unsigned int*)b;
+  b += align256(sizeof(unsigned int) * ((size_t)to * tv + 64));
+  int* sync = (int*)(b + 256);
   MB_CUDA(cudaMemsetAsync(tcnt, 0, sizeof(unsigned int) * (size_t)to * tv, stream));
   MB_CUDA(cudaMemsetAsync(nrot_dev, 0, sizeof(unsigned long long), stream));
   const long long kv = (long long)nocc * nvirt;
@@ -595,7 +688,7 @@ extern "C" int mb_rot_sweep_ws(int n, int nocc, const double* fmo, const double*
   rot_coeff_kernel<<<cblocks, 256, 0, stream>>>(nocc, nvirt, fmo, eigs, nullptr, tiny, bigeps, al, be, act, tcnt,
                                                  nrot_dev, to, tv);
   MB_LAUNCH_CHECK();
-  return launch_wavefronts(n, nocc, nvirt, c, al, be, act, tcnt, to, tv, stream);
+  return launch_wavefronts(n, nocc, nvirt, c, al, be, act, tcnt, to, tv, sync, nullptr, stream);
 }
 
 extern "C" int mb_pseudo_diag_dev(int n, int nocc, const double* fpacked, double* c, const double* eigs,
