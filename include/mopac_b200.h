@@ -97,8 +97,9 @@ typedef struct mb_scf_opts {
                         (SCF/iter.F90:675-690) passes in FP64, convergence
                         is accepted only when the last density update moved
                         no element of P by more than finish_dp; until then
-                        the loop goes on in FP64 with the rotation sweep's
-                        relative threshold bigeps at 0 and, from its first
+                        the loop goes on in FP64 with both of the rotation
+                        sweep's thresholds (bigeps and 0.05 max|Fmo|) at 0,
+                        every occupied-virtual pair rotated, and, from its first
                         iteration, the orbital energies of the current
                         vectors (diag C^T F C) in the rotation angles.  It
                         takes the SCF to its self-consistent point instead
@@ -142,6 +143,16 @@ typedef struct mb_scf_result {
   int n_interp;      /* Camp-King interpolated passes (interp mode 3)      */
   int forced_on;     /* 1 when iter forced all convergers on (niter passed
                         itrmax - 10, SCF/iter.F90:351-372)                 */
+  int exit_split;    /* 1 when the exit diagonalisation (SCF/iter.F90 label
+                        600) was solved as the occupied and virtual blocks
+                        of C^T F C after the FP64 finish (an addition to
+                        iter: the two blocks' eigenvalues differ from the
+                        whole matrix's by at most ||B||_F^2 / gap, accepted
+                        below 1e-8 eV, and a first-order rotation takes the
+                        coupling B out of the vectors); 0: the full
+                        eigensolve, counted in n_full_diag                 */
+  double exit_coupling; /* ||C_v^T F C_o||_F at the exit (eV) when the split
+                        was tried, else -1                                 */
 } mb_scf_result;
 
 void mb_scf_opts_default(mb_scf_opts* o);

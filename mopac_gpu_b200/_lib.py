@@ -66,7 +66,8 @@ class ScfRes(ctypes.Structure):
                 ("pl", ctypes.c_double), ("t_fock_ms", ctypes.c_double), ("t_diag_ms", ctypes.c_double),
                 ("t_density_ms", ctypes.c_double), ("t_other_ms", ctypes.c_double), ("t_total_ms", ctypes.c_double),
                 ("n_pulay", ctypes.c_int), ("n_split", ctypes.c_int), ("n_finish", ctypes.c_int),
-                ("dp", ctypes.c_double), ("n_interp", ctypes.c_int), ("forced_on", ctypes.c_int)]
+                ("dp", ctypes.c_double), ("n_interp", ctypes.c_int), ("forced_on", ctypes.c_int),
+                ("exit_split", ctypes.c_int), ("exit_coupling", ctypes.c_double)]
 
 
 _lib = None

@@ -29,6 +29,10 @@ extern "C" size_t mb_eigh_ws_bytes(int n);
 extern "C" int mb_eigh_ws(int n, double* fpacked, int perturb, double* c, double* eigs, void* ws, int* status_dev,
                           cudaStream_t stream);
 extern "C" size_t mb_pseudo_ws_bytes(int n, int nocc);
+extern "C" int mb_dgemm_dev(char transa, char transb, int m, int n, int k, double alpha, const double* a, int lda,
+                            const double* b, int ldb, double beta, double* c, int ldc, cudaStream_t stream);
+extern "C" int mb_unpack_dev(int n, const double* pk, double* a, int lda, int perturb, double* pk_mut,
+                             cudaStream_t stream);
 extern "C" size_t mb_fock2_ws_bytes(int numat);
 extern "C" int mb_fock2_ws(const MbAtomsDev* atoms, double* f, const double* h, const double* ptot, const double* pa,
                            const double* w, double shift, int use_shift, void* ws, size_t ws_bytes,
@@ -37,7 +41,7 @@ extern "C" int mb_pseudo_diag_ws(int n, int nocc, const double* fpacked, double*
                                  unsigned long long* nrot_dev, void* ws, cudaStream_t stream);
 extern "C" int mb_pseudo_diag_ex(int n, int nocc, const double* fpacked, double* c, const double* eigs,
                                  unsigned long long* nrot_dev, void* ws, void* split_ws, size_t split_ws_bytes,
-                                 int* split_err, double bigeps, cudaStream_t stream);
+                                 int* split_err, double bigeps, double tiny_direct, cudaStream_t stream);
 extern "C" int mb_orbital_energies_ws(int n, const double* fpacked, const double* c, double* eigs, void* ws,
                                       cudaStream_t stream);
 extern "C" size_t mb_gemm_split_ws_bytes(int m, int n, int k);
@@ -173,6 +177,7 @@ struct mb_ctx {
   mb_guess_ws* guess_ws = nullptr;  // the prediction's grow-only workspace
   void* purify_ws = nullptr;        // McWeeny matrices when eig_ws is too small
   mb_campking* ck = nullptr;        // Camp-King's state, made on its first use
+  double* exit_ws = nullptr;        // the split exit diagonalisation's matrices, made on its first use
   cudaStream_t stream = nullptr;
 };
 
@@ -186,7 +191,8 @@ static void ctx_free(mb_ctx* c) {
   mb_campking_destroy(c->ck);
   void* ptrs[] = {c->d_nat, c->d_coord, c->d_pdiag, c->h, c->w, c->f, c->p, c->pa, c->pold, c->pold2, c->c, c->eigs,
                   c->fdiag, c->scal, c->hws, c->status, c->nrot, c->eig_ws, c->pseudo_ws,
-                  c->fock_ws, c->fppf_hist, c->fock_hist, c->tc_ws_raw, c->pguess, c->purify_ws, c->pprev};
+                  c->fock_ws, c->fppf_hist, c->fock_hist, c->tc_ws_raw, c->pguess, c->purify_ws, c->pprev,
+                  c->exit_ws};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -525,6 +531,60 @@ __global__ void maxdiff_copy_kernel(long long n, const double* __restrict__ p, d
   for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
   if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
 }
+
+// The m x m diagonal block of M (column-major, leading dimension ld) that
+// starts at (r0, r0), symmetrised and packed by rows as the eigensolver reads
+// it: pk[i(i+1)/2 + j] = (M(i, j) + M(j, i)) / 2 for i >= j.  Grid (x over j,
+// y = row i).
+__global__ void pack_block_kernel(int m, int r0, const double* __restrict__ M, int ld, double* __restrict__ pk) {
+  const int i = blockIdx.y;
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m || j > i) return;
+  const double a = M[(size_t)(r0 + i) + (size_t)(r0 + j) * ld];
+  const double b = M[(size_t)(r0 + j) + (size_t)(r0 + i) * ld];
+  pk[(long long)i * (i + 1) / 2 + j] = 0.5 * (a + b);
+}
+
+// Per-block partial sums of squares of the rows x cols block of M starting
+// at M[0] (leading dimension ld); a fixed grid and a fixed tree, so the sum
+// below is the same in every run.
+__global__ void __launch_bounds__(256) block_sumsq_partials(int rows, int cols, const double* __restrict__ M, int ld,
+                                                            double* __restrict__ part) {
+  __shared__ double red[256];
+  double s = 0.0;
+  const long long total = (long long)rows * cols;
+  for (long long q = blockIdx.x * 256LL + threadIdx.x; q < total; q += (long long)gridDim.x * 256) {
+    const long long col = q / rows, row = q - col * rows;
+    const double x = M[row + col * ld];
+    s += x * x;
+  }
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int h = 128; h > 0; h >>= 1) {
+    if (threadIdx.x < h) red[threadIdx.x] += red[threadIdx.x + h];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) part[blockIdx.x] = red[0];
+}
+
+__global__ void sum_partials_kernel(int nb, const double* __restrict__ part, double* __restrict__ out) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    double s = 0.0;
+    for (int b = 0; b < nb; ++b) s += part[b];
+    *out = s;
+  }
+}
+
+// X(a, i) = B'(a, i) / (e_i - e_(no + a)) in place over the nv x no coupling
+// in the two blocks' eigenbases: the first-order rotation between occupied
+// orbital i and virtual orbital a that removes it.
+__global__ void coupling_rotation_kernel(int nv, int no, const double* __restrict__ eigs, double* __restrict__ b) {
+  const long long total = (long long)nv * no;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < total; q += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(q / nv), a = (int)(q - (long long)i * nv);
+    b[q] = b[q] / (eigs[i] - eigs[no + a]);
+  }
+}
 }  // namespace
 
 static int d2h(mb_ctx* c, double* dst, const double* src, int count) {
@@ -549,9 +609,9 @@ struct PhaseTimer {
   }
 };
 
-static int full_diag(mb_ctx* c, double* fpacked, double* eig_homo, double* eig_lumo, int ihomo) {
+static int full_diag(mb_ctx* c, double* fpacked, double* eig_homo, double* eig_lumo, int ihomo, int perturb = 1) {
   mb_kstat_mark(MB_KSTAT_EIGH, c->stream, true);
-  MB_TRY(mb_eigh_ws(c->norbs, fpacked, 1, c->c, c->eigs, c->eig_ws, c->status, c->stream));
+  MB_TRY(mb_eigh_ws(c->norbs, fpacked, perturb, c->c, c->eigs, c->eig_ws, c->status, c->stream));
   mb_kstat_mark(MB_KSTAT_EIGH, c->stream, false);
   int st = 0;
   MB_CUDA(cudaMemcpyAsync(&st, c->status, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
@@ -563,6 +623,107 @@ static int full_diag(mb_ctx* c, double* fpacked, double* eig_homo, double* eig_l
   if (st != 0) return mb_set_error(MB_ERR_NUMERIC, "eigensolver failed (inverse iteration)");
   *eig_homo = hl[0];
   *eig_lumo = hl[1];
+  return MB_OK;
+}
+
+static inline size_t pad32(size_t x) { return (x + 31) & ~(size_t)31; }  // doubles, to 256 bytes
+
+// The exit diagonalisation of an SCF that ended in the FP64 finish of the
+// pseudo-diagonalisation.  There the current vectors C split F into its
+// occupied and virtual invariant subspaces up to a small coupling
+// B = C_v^T F C_o (the finish has rotated it down with every pair active), so
+// the eigenproblem of F is solved as the two diagonal blocks of M = C^T F C,
+// nclose and n - nclose orbitals, on this library's eigensolver, and the
+// first-order rotation X = B' / (e_o - e_v) (B' = B in the blocks'
+// eigenbases) then takes the coupling out of the vectors.  The eigenvalues
+// differ from those of the whole matrix by at most ||B||_2^2 / gap <=
+// ||B||_F^2 / gap (the gap between the highest occupied and lowest virtual
+// block eigenvalue); the split is used only when that bound is below
+// 1e-8 eV, otherwise *done stays 0 and the caller runs the full eigensolve on
+// fpacked, which then already carries the perturbation.  F gets the
+// reference's perturbation i * 1e-10 on its diagonal first
+// (eigenvectors_LAPACK.F90:53-121), in place, as the full eigensolve does.
+// *coupling receives ||B||_F (eV).
+static int exit_block_diag(mb_ctx* c, double* fpacked, double* eig_homo, double* eig_lumo, int* done,
+                           double* coupling) {
+  *done = 0;
+  *coupling = -1.0;
+  const int n = c->norbs, no = c->nclose, nv = n - no;
+  cudaStream_t s = c->stream;
+  const size_t nn = (size_t)n * n;
+  const size_t o_m = 0, o_g = o_m + pad32(nn), o_ap = o_g + pad32(nn),
+               o_dp = o_ap + pad32((size_t)no * (no + 1) / 2), o_qa = o_dp + pad32((size_t)nv * (nv + 1) / 2),
+               o_qd = o_qa + pad32((size_t)no * no), o_t = o_qd + pad32((size_t)nv * nv),
+               o_x = o_t + pad32((size_t)nv * no), o_part = o_x + pad32((size_t)nv * no), total = o_part + 1024;
+  if (!c->exit_ws) MB_CUDA(cudaMalloc(&c->exit_ws, sizeof(double) * total));
+  double* M = c->exit_ws + o_m;   // F full, then C^T F C
+  double* G = c->exit_ws + o_g;   // F C, then the block vectors C Q
+  double* Ap = c->exit_ws + o_ap;
+  double* Dp = c->exit_ws + o_dp;
+  double* Qa = c->exit_ws + o_qa;
+  double* Qd = c->exit_ws + o_qd;
+  double* T = c->exit_ws + o_t;
+  double* X = c->exit_ws + o_x;
+  double* part = c->exit_ws + o_part;
+  mb_kstat_mark(MB_KSTAT_EIGH, s, true);
+  MB_TRY(mb_unpack_dev(n, fpacked, M, n, 1, fpacked, s));
+  MB_TRY(mb_dgemm_dev('N', 'N', n, n, n, 1.0, M, n, c->c, n, 0.0, G, n, s));
+  MB_TRY(mb_dgemm_dev('T', 'N', n, n, n, 1.0, c->c, n, G, n, 0.0, M, n, s));
+  const int nb = 148 * 4;
+  block_sumsq_partials<<<nb, 256, 0, s>>>(nv, no, M + no, n, part);
+  MB_LAUNCH_CHECK();
+  sum_partials_kernel<<<1, 32, 0, s>>>(nb, part, part + nb);
+  MB_LAUNCH_CHECK();
+  double b2 = 0.0;
+  MB_TRY(d2h(c, &b2, part + nb, 1));
+  *coupling = sqrt(b2);
+  const double tol_ev = 1.0e-8;
+  // the gap is at least 1 eV wherever the split can pass the test below
+  if (!(b2 <= tol_ev * 1.0e3)) {
+    mb_kstat_mark(MB_KSTAT_EIGH, s, false);
+    return MB_OK;
+  }
+  {
+    dim3 ga((no + 255) / 256, no), gd((nv + 255) / 256, nv);
+    pack_block_kernel<<<ga, 256, 0, s>>>(no, 0, M, n, Ap);
+    MB_LAUNCH_CHECK();
+    pack_block_kernel<<<gd, 256, 0, s>>>(nv, no, M, n, Dp);
+    MB_LAUNCH_CHECK();
+  }
+  int st[2] = {0, 0};
+  MB_TRY(mb_eigh_ws(no, Ap, 0, Qa, c->eigs, c->eig_ws, c->status, s));
+  MB_CUDA(cudaMemcpyAsync(&st[0], c->status, sizeof(int), cudaMemcpyDeviceToHost, s));
+  MB_TRY(mb_eigh_ws(nv, Dp, 0, Qd, c->eigs + no, c->eig_ws, c->status, s));
+  MB_CUDA(cudaMemcpyAsync(&st[1], c->status, sizeof(int), cudaMemcpyDeviceToHost, s));
+  double hl[2] = {0.0, 0.0};
+  MB_CUDA(cudaMemcpyAsync(hl, c->eigs + (no - 1), sizeof(double) * 2, cudaMemcpyDeviceToHost, s));
+  MB_CUDA(cudaStreamSynchronize(s));
+  const double gap = hl[1] - hl[0];
+  if (st[0] != 0 || st[1] != 0 || !(gap > 0.0) || !(b2 <= tol_ev * gap)) {
+    mb_kstat_mark(MB_KSTAT_EIGH, s, false);
+    return MB_OK;  // the full eigensolve takes over (c->c is untouched)
+  }
+  // B' = Qd^T B Qa (nv x no), then X = B' / (e_o - e_v)
+  MB_TRY(mb_dgemm_dev('N', 'N', nv, no, no, 1.0, M + no, n, Qa, no, 0.0, T, nv, s));
+  MB_TRY(mb_dgemm_dev('T', 'N', nv, no, nv, 1.0, Qd, nv, T, nv, 0.0, X, nv, s));
+  {
+    const long long kv = (long long)nv * no;
+    int blocks = (int)((kv + 255) / 256);
+    if (blocks > 148 * 8) blocks = 148 * 8;
+    coupling_rotation_kernel<<<blocks, 256, 0, s>>>(nv, no, c->eigs, X);
+    MB_LAUNCH_CHECK();
+  }
+  // block vectors [C_o Qa | C_v Qd], then C_o' = C_o Qa + C_v Qd X and
+  // C_v' = C_v Qd - C_o Qa X^T
+  MB_TRY(mb_dgemm_dev('N', 'N', n, no, no, 1.0, c->c, n, Qa, no, 0.0, G, n, s));
+  MB_TRY(mb_dgemm_dev('N', 'N', n, nv, nv, 1.0, c->c + (size_t)no * n, n, Qd, nv, 0.0, G + (size_t)no * n, n, s));
+  MB_CUDA(cudaMemcpyAsync(c->c, G, sizeof(double) * nn, cudaMemcpyDeviceToDevice, s));
+  MB_TRY(mb_dgemm_dev('N', 'N', n, no, nv, 1.0, G + (size_t)no * n, n, X, nv, 1.0, c->c, n, s));
+  MB_TRY(mb_dgemm_dev('N', 'T', n, nv, no, -1.0, G, n, X, nv, 1.0, c->c + (size_t)no * n, n, s));
+  mb_kstat_mark(MB_KSTAT_EIGH, s, false);
+  *eig_homo = hl[0];
+  *eig_lumo = hl[1];
+  *done = 1;
   return MB_OK;
 }
 
@@ -813,8 +974,12 @@ extern "C" int mb_scf_run(mb_ctx* c, const mb_scf_opts* opts_in, mb_scf_result* 
         refreshed = true;
       }
       mb_kstat_mark(MB_KSTAT_PSEUDO, s, true);
+      // the finish rotates every occupied-virtual pair: neither the relative
+      // threshold bigeps nor the absolute 0.05 max|Fmo| skips any (fewer
+      // finish iterations to the same fixed point)
+      const bool fin = res->n_finish > 0;
       MB_TRY(mb_pseudo_diag_ex(n, na1el, c->f, c->c, c->eigs, c->nrot, c->pseudo_ws, use_split ? c->tc_ws : nullptr,
-                               c->tc_ws_bytes, c->status + 1, res->n_finish > 0 ? 0.0 : 1.5e-7, s));
+                               c->tc_ws_bytes, c->status + 1, fin ? 0.0 : 1.5e-7, fin ? 0.0 : -1.0, s));
       mb_kstat_mark(MB_KSTAT_PSEUDO, s, false);
       res->n_pseudo_diag++;
     } else {
@@ -862,9 +1027,21 @@ extern "C" int mb_scf_run(mb_ctx* c, const mb_scf_opts* opts_in, mb_scf_result* 
   ee = hee * 2.0;
   MB_CUDA(cudaMemcpyAsync(c->fdiag, c->f, sizeof(double) * mpack, cudaMemcpyDeviceToDevice, s));
   t_diag.start();
-  MB_TRY(full_diag(c, c->fdiag, &eig_homo, &eig_lumo, ihomo));
+  int split_exit = 0;
+  bool split_tried = false;
+  res->exit_coupling = -1.0;
+  if (converged && finishing && res->n_finish > 0 && newdg && opts.pseudo && !camkin && nclose > 0 && nclose < n) {
+    split_tried = true;
+    MB_TRY(exit_block_diag(c, c->fdiag, &eig_homo, &eig_lumo, &split_exit, &res->exit_coupling));
+  }
+  if (split_exit) {
+    res->exit_split = 1;
+  } else {
+    // a declined split has perturbed fdiag already
+    MB_TRY(full_diag(c, c->fdiag, &eig_homo, &eig_lumo, ihomo, split_tried ? 0 : 1));
+    res->n_full_diag++;
+  }
   t_diag.stop();
-  res->n_full_diag++;
   escf = (ee + c->enuclr) * enrgy + c->atheat;
   res->escf = escf;
   res->ee = ee;

@@ -569,11 +569,13 @@ extern "C" int mb_gemm_split_ws(char transa, char transb, int m, int n, int k, d
 
 // The Fmo GEMMs run in FP64, or -- when split_ws is given -- with the
 // three-product BF16 split on the tensor cores (mb_gemm_split_ws).  bigeps is
-// the reference's relative rotation threshold (1.5e-7, diag_for_GPU.F90:33);
-// the SCF's FP64 finish passes 0 so that no rotation above tiny is skipped.
+// the reference's relative rotation threshold (1.5e-7, diag_for_GPU.F90:33)
+// and tiny_direct < 0 selects its absolute one, 0.05 max|Fmo|
+// (diag_for_GPU.F90:151-152); the SCF's FP64 finish passes 0 for both, so
+// that every occupied-virtual pair is rotated.
 extern "C" int mb_pseudo_diag_ex(int n, int nocc, const double* fpacked, double* c, const double* eigs,
                                  unsigned long long* nrot_dev, void* ws, void* split_ws, size_t split_ws_bytes,
-                                 int* split_err, double bigeps, cudaStream_t stream) {
+                                 int* split_err, double bigeps, double tiny_direct, cudaStream_t stream) {
   const int nvirt = n - nocc;
   if (nocc <= 0 || nvirt <= 0) return MB_OK;
   if (((uintptr_t)ws & 255) != 0) return mb_set_error(MB_ERR_ARG, "pseudo-diag workspace must be 256-byte aligned");
@@ -615,8 +617,8 @@ extern "C" int mb_pseudo_diag_ex(int n, int nocc, const double* fpacked, double*
   MB_LAUNCH_CHECK();
   int cblocks = (int)((kt + 255) / 256);
   if (cblocks > 148 * 8) cblocks = 148 * 8;
-  rot_coeff_kernel<<<cblocks, 256, 0, stream>>>(nocc, nvirt, fmo, eigs, tiny, -1.0, bigeps, al, be, act, tcnt, nrot_dev,
-                                                 to, tv);
+  rot_coeff_kernel<<<cblocks, 256, 0, stream>>>(nocc, nvirt, fmo, eigs, tiny, tiny_direct, bigeps, al, be, act, tcnt,
+                                                 nrot_dev, to, tv);
   MB_LAUNCH_CHECK();
   return launch_wavefronts(n, nocc, nvirt, c, al, be, act, tcnt, to, tv, sync, split_err, stream);
 }
@@ -657,7 +659,7 @@ extern "C" int mb_orbital_energies_ws(int n, const double* fpacked, const double
 
 extern "C" int mb_pseudo_diag_ws(int n, int nocc, const double* fpacked, double* c, const double* eigs,
                                  unsigned long long* nrot_dev, void* ws, cudaStream_t stream) {
-  return mb_pseudo_diag_ex(n, nocc, fpacked, c, eigs, nrot_dev, ws, nullptr, 0, nullptr, 1.5e-7, stream);
+  return mb_pseudo_diag_ex(n, nocc, fpacked, c, eigs, nrot_dev, ws, nullptr, 0, nullptr, 1.5e-7, -1.0, stream);
 }
 
 // Rotation sweep alone with caller-given Fmo, tiny and bigeps (the arguments

@@ -38,6 +38,8 @@ class ScfResult:
     dp: float = -1.0
     n_interp: int = 0        # Camp-King interpolated passes
     forced_on: bool = False  # iter forced all convergers on (niter > itrmax - 10)
+    exit_split: bool = False  # exit diagonalisation solved as the occupied and virtual blocks
+    exit_coupling: float = -1.0  # ||C_v^T F C_o||_F at the exit when the split was tried (eV)
 
 
 class ScfContext:
@@ -114,7 +116,7 @@ class ScfContext:
         check(lib().mb_scf_run(self._h, ctypes.byref(o), ctypes.byref(r)))
         return ScfResult(r.escf, r.ee, r.niter, bool(r.converged), r.n_full_diag, r.n_pseudo_diag, r.pl,
                          r.t_fock_ms, r.t_diag_ms, r.t_density_ms, r.t_other_ms, r.t_total_ms, r.n_pulay, r.n_split,
-                         r.n_finish, r.dp, r.n_interp, bool(r.forced_on))
+                         r.n_finish, r.dp, r.n_interp, bool(r.forced_on), bool(r.exit_split), r.exit_coupling)
 
     def density(self) -> np.ndarray:
         p = np.empty(self.mpack)

@@ -269,9 +269,9 @@ def rotation_sweep_py(c: np.ndarray, fmo: np.ndarray, eig: np.ndarray, nocc: int
     return done
 
 
-def pseudo_diag(f, c, nocc, eig, bigeps: float = 1.5e-7):
+def pseudo_diag(f, c, nocc, eig, bigeps: float = 1.5e-7, tiny: float | None = None):
     fmo = fmo_block(f, c, nocc)
-    return rotation_sweep(c, fmo, eig, nocc, bigeps=bigeps)
+    return rotation_sweep(c, fmo, eig, nocc, bigeps=bigeps, tiny=tiny)
 
 
 # ---------------------------------------------------------------- pulay
@@ -488,9 +488,10 @@ def iter_scf(s: System, pseudo: bool = False, scfcrt: float = 1.0e-4, itrmax: in
     finish_dp): once iter's test (:675-690) passes, convergence is accepted
     only when the last density update moved no element of P by more than
     finish_dp (max|P_k - P_(k-1)| over all mpack elements); otherwise the
-    loop goes on, at most finish_max more iterations, and the rotation
-    sweep's relative threshold bigeps (diag_for_GPU.F90:33) is 0 in those
-    iterations.
+    loop goes on, at most finish_max more iterations, and in those
+    iterations the rotation sweep's relative threshold bigeps
+    (diag_for_GPU.F90:33) and its absolute one, tiny = 0.05 max|Fmo|
+    (:151-152), are both 0: every occupied-virtual pair is rotated.
 
     camp: the CAMP keyword (iter.F90:134): Camp-King's interp on the alpha
     vectors from the third iteration (:781-798), a full diagonalisation in
@@ -707,7 +708,10 @@ def iter_scf(s: System, pseudo: bool = False, scfcrt: float = 1.0e-4, itrmax: in
                 # that iteration's level shift
                 eigs = np.einsum("ij,ij->j", c, unpack(f, n) @ c)
                 refreshed = True
-            pseudo_diag(f, c, na1el, eigs, bigeps=0.0 if n_finish > 0 else 1.5e-7)
+            if n_finish > 0:    # the finish rotates every occupied-virtual pair
+                pseudo_diag(f, c, na1el, eigs, bigeps=0.0, tiny=0.0)
+            else:
+                pseudo_diag(f, c, na1el, eigs)
         else:
             c, eigs = eigenvectors_lapack(f, n)
         p = density(c, nclose)
@@ -726,6 +730,36 @@ def iter_scf(s: System, pseudo: bool = False, scfcrt: float = 1.0e-4, itrmax: in
     escf = (ee + s.enuclr) * enrgy + s.atheat
     return ScfResult(escf=escf, ee=ee, eigs=eigs, c=c, p=p, niter=niter, converged=converged,
                      history=history, n_finish=n_finish, n_interp=n_interp, forced_on=forced_on)
+
+
+def exit_block_diag(f: np.ndarray, c: np.ndarray, nocc: int, tol_ev: float = 1.0e-8):
+    """The device SCF's exit diagonalisation after the FP64 finish (an
+    addition to iter's label 600, which calls eigenvectors_LAPACK on the whole
+    F): F gets the reference's perturbation i * 1e-10 (in place, as
+    eigenvectors_lapack does), M = C^T F C is split into its occupied and
+    virtual diagonal blocks, each block is diagonalised, and the first-order
+    rotation X = B' / (e_o - e_v) with B' = Q_v^T B Q_o, B = M[nocc:, :nocc],
+    takes the remaining coupling out of the vectors.  Returns (c, eigs,
+    ||B||_F), or (None, None, ||B||_F) when the eigenvalue bound
+    ||B||_F^2 / gap exceeds tol_ev and the whole matrix must be solved."""
+    n = c.shape[0]
+    f[diag_index(n)] += np.arange(1, n + 1) * 1.0e-10
+    ff = unpack(f, n)
+    m = c.T @ (ff @ c)
+    b = m[nocc:, :nocc]
+    b2 = float(np.sum(b * b))
+    if not b2 <= tol_ev * 1.0e3:
+        return None, None, np.sqrt(b2)
+    ea, qa = np.linalg.eigh(0.5 * (m[:nocc, :nocc] + m[:nocc, :nocc].T))
+    ed, qd = np.linalg.eigh(0.5 * (m[nocc:, nocc:] + m[nocc:, nocc:].T))
+    gap = ed[0] - ea[-1]
+    if not (gap > 0.0 and b2 <= tol_ev * gap):
+        return None, None, np.sqrt(b2)
+    x = (qd.T @ b @ qa) / (ea[None, :] - ed[:, None])
+    co = c[:, :nocc] @ qa
+    cv = c[:, nocc:] @ qd
+    cn = np.hstack([co + cv @ x, cv - co @ x.T])
+    return np.asfortranarray(cn), np.concatenate([ea, ed]), np.sqrt(b2)
 
 
 # ---------------------------------------------------------------- fixed point

@@ -67,7 +67,18 @@ def test_fast_split_path_lands_on_the_oracle_fixed_point(box):
     s, ctx = box
     r = ctx.run(pseudo=True, pulay=True, precision=1)
     p = ctx.density()
-    _, e = ctx.vectors()
+    c, e = ctx.vectors()
+    # the exit diagonalisation as the occupied and virtual blocks of C^T F C:
+    # orthonormal eigenvectors of the perturbed F, as for the whole eigensolve
+    cd = torch.from_numpy(np.ascontiguousarray(c)).cuda()
+    orth = (cd.T @ cd - torch.eye(s.norbs, dtype=torch.float64, device="cuda")).abs().max().item()
+    fd = torch.from_numpy(so.unpack(ctx.fock(), s.norbs)).cuda()
+    fd.diagonal().add_(torch.arange(1, s.norbs + 1, dtype=torch.float64, device="cuda") * 1e-10)
+    resid = (fd @ cd - cd * torch.from_numpy(e).cuda()).abs().max().item()
+    print(f"exit split {r.exit_split}, ||B||_F {r.exit_coupling:.2e} eV: max|C^T C - I| {orth:.2e}, "
+          f"max|F C - C e| {resid:.2e}")
+    assert r.exit_split and orth < 1e-10 and resid < 1e-9
+    del cd, fd
     cert = so.fixed_point_certificate(s, p, steps=3)
     print(f"fast: {r.niter} iterations ({r.n_full_diag} full, {r.n_pseudo_diag} pseudo, {r.n_split} split, "
           f"{r.n_finish} finish), last dP {r.dp:.2e}; oracle steps r {cert['r']}, rho {cert['rho']:.3f}, "

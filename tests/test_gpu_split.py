@@ -139,12 +139,23 @@ def test_split_scf_matches_the_oracle_running_the_same_finish():
     ctx.set_hw(s.h, s.w, s.enuclr)
     r = ctx.run(pseudo=True, pulay=True, precision=1)
     p = ctx.density()
-    _, e = ctx.vectors()
+    c, e = ctx.vectors()
+    fk = ctx.fock()
     ctx.close()
     assert r.converged and ref.converged
     assert abs(r.escf - ref.escf) < 1e-4
     assert np.abs(p - ref.p).max() < 1e-6
     assert np.abs(e - ref.eigs).max() < 1e-5
+    # the exit diagonalisation ran as the occupied and virtual blocks: its
+    # vectors are eigenvectors of the (perturbed) F as tightly as the whole
+    # eigensolve's, and orthonormal
+    fp = so.unpack(fk, s.norbs)
+    fp[np.diag_indices(s.norbs)] += np.arange(1, s.norbs + 1) * 1.0e-10
+    print(f"exit split {r.exit_split}, ||B||_F {r.exit_coupling:.2e} eV, "
+          f"max|F C - C e| {np.abs(fp @ c - c * e).max():.2e}")
+    assert r.exit_split and 0.0 <= r.exit_coupling < 1e-3
+    assert np.abs(fp @ c - c * e).max() < 1e-9
+    assert np.abs(c.T @ c - np.eye(s.norbs)).max() < 1e-10
 
 
 def test_finish_off_keeps_iter_semantics():

@@ -74,3 +74,42 @@ def test_certificate_estimates_the_distance_to_the_fixed_point():
         # orbital energies of F(p) are what the exit diagonalisation returns
         np.testing.assert_allclose(cert["eigs"], r.eigs, atol=1e-12)
         assert abs(cert["heat_at_p"] - r.escf) < 1e-9
+
+
+def test_split_exit_diagonalisation_matches_the_whole_eigensolve():
+    """After the finish, the exit diagonalisation solved as the occupied and
+    virtual blocks of C^T F C (plus the first-order rotation of the
+    remaining coupling) gives the whole eigensolve's eigenvalues and vectors
+    that satisfy F C = C e as tightly as it does."""
+    nat, xyz, _ = wl.water_box(32)
+    s = oracle_system(nat, xyz)
+    cap = {}
+    orig = so.pseudo_diag
+
+    def keep(f, c, nocc, eig, **kw):
+        r = orig(f, c, nocc, eig, **kw)
+        cap["c"] = c.copy(order="F")
+        cap["f"] = f.copy()
+        return r
+
+    so.pseudo_diag = keep
+    try:
+        r = so.iter_scf(s, pseudo=True, pulay_on=True, finish_dp=1.0e-7, shift_kw=0.0)
+    finally:
+        so.pseudo_diag = orig
+    assert r.converged and r.n_finish > 0
+    # F of the last iteration is the exit's F (iter.F90 label 600)
+    f = s.h.copy()
+    so.fock2(s, f, r.p, r.p * 0.5)
+    fk = f.copy()
+    c, e, bnorm = so.exit_block_diag(fk, cap["c"], s.nclose)
+    assert c is not None and bnorm < 1e-3
+    np.testing.assert_allclose(e, r.eigs, rtol=0, atol=1e-10)
+    fp = so.unpack(fk, s.norbs)
+    assert np.abs(fp @ c - c * e).max() < 1e-9
+    assert np.abs(c.T @ c - np.eye(s.norbs)).max() < 1e-10
+    # the same occupied subspace as the whole eigensolve's
+    np.testing.assert_allclose(so.density(c, s.nclose), so.density(r.c, s.nclose), atol=1e-9)
+    # a coupling above the bound is declined
+    c2, e2, _ = so.exit_block_diag(f.copy(), np.asfortranarray(np.eye(s.norbs)), s.nclose)
+    assert c2 is None and e2 is None
