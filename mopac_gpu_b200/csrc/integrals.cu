@@ -846,11 +846,18 @@ __device__ void mz_outer_terms(int ni, int nj, const double* ci, const double* c
   }
 }
 
-__global__ void mz_hcore_diag(MbMzLayout L, const int* __restrict__ nat, const double* __restrict__ coord,
-                              double* __restrict__ h, double* __restrict__ w, const double* __restrict__ enuc_entry,
-                              double* __restrict__ enuc_atom) {
-  const int A = blockIdx.x * blockDim.x + threadIdx.x;
-  if (A >= L.numat) return;
+// A warp per atom A; the partners B are taken 32 at a time, one per lane,
+// and every lane's terms are then added in lane order, so the one-centre
+// block and the core-core energy are summed over B in ascending order, the
+// reference loop's order, bit for bit.
+__global__ void __launch_bounds__(128) mz_hcore_diag(MbMzLayout L, const int* __restrict__ nat,
+                                                     const double* __restrict__ coord, double* __restrict__ h,
+                                                     double* __restrict__ w, const double* __restrict__ enuc_entry,
+                                                     double* __restrict__ enuc_atom) {
+  __shared__ int entry_of[4][32];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int A = blockIdx.x * 4 + wib;
+  if (A >= L.numat) return;  // warp-uniform
   const int nA = nat[A], noA = L.iorbs[A], lA = noA * (noA + 1) / 2;
   const Pm7Elem& E = c_P.el[nA];
   double blk[10];
@@ -861,58 +868,93 @@ __global__ void mz_hcore_diag(MbMzLayout L, const int* __restrict__ nat, const d
   int ep = L.pair_ptr[A];                 // A's stored partners (ascending), then its own block
   const int ediag = L.pair_ptr[A + 1] - 1;
   double en = 0.0;
-  for (int B = 0; B < L.numat; ++B) {
-    if (B == A) continue;
-    const double* xb = coord + 3 * B;
-    const double dx = xa[0] - xb[0], dy = xa[1] - xb[1], dz = xa[2] - xb[2];
-    const double r2 = dx * dx + dy * dy + dz * dz;
-    const int nB = nat[B];
-    if (B < A) {
-      // the pair's core-core energy (summed per atom over partners below it)
-      if (ep < ediag && L.pair_j[ep] == B) {
-        en += enuc_entry[ep];
-        ++ep;
-      } else if (r2 < L.cutof1) {       // outer2: monopole term
-        double ri[23], gab;
-        reppd(nA, nB, sqrt(r2), ri, &gab);
-        en += c_P.el[nA].tore * c_P.el[nB].tore * ri[1];
-      } else {                          // outer1: feathered point charge
-        const double rij = sqrt(r2), rb = rij / PM7_A0;
-        double aee = 0.5 / E.am + 0.5 / c_P.el[nB].am;
-        aee = aee * aee;
-        double ww = PM7_EV / sqrt(rb * rb + aee), point, cst;
-        to_point(rij, &point, &cst);
-        ww = ww * cst + (1.0 - cst) * point;
-        en += c_P.el[nA].tore * c_P.el[nB].tore * ww;
-      }
+  for (int b0 = 0; b0 < L.numat; b0 += 32) {
+    const int B = b0 + lane;
+    // which partners of this chunk are stored pairs, and their entries
+    entry_of[wib][lane] = -1;
+    __syncwarp();
+    {
+      const int e = ep + lane;
+      const int pj = e < ediag ? L.pair_j[e] : -1;
+      const bool in = pj >= b0 && pj < b0 + 32;
+      if (in) entry_of[wib][pj - b0] = e;
+      ep += __popc(__ballot_sync(0xffffffffu, in));
     }
-    if (r2 < 0.00002) continue;
-    double p[4][4], core[5][3], e1b[10], e2a[10];
-    if (!(r2 < L.cutof2) && sqrt(r2) < 7.0) {
-      // a far pair inside PM7's 7 A feathering radius (a cutoff below 7 A):
-      // outer1's or outer2's terms; beyond 7 A elenuc's feathered integrals
-      // are the same point charges
+    __syncwarp();
+    const int my_entry = entry_of[wib][lane];
+    double cen = 0.0;        // this lane's core-core term (B < A)
+    double c[10];            // this lane's contribution to A's one-centre block
+    for (int x = 0; x < 10; ++x) c[x] = 0.0;
+    bool has_c = false;
+    if (B < L.numat && B != A) {
+      const double* xb = coord + 3 * B;
+      const double dx = xa[0] - xb[0], dy = xa[1] - xb[1], dz = xa[2] - xb[2];
+      const double r2 = dx * dx + dy * dy + dz * dz;
+      const int nB = nat[B];
       if (B < A) {
-        mz_outer_terms(nA, nB, xa, xb, r2 < L.cutof1, e1b, e2a);
-        for (int x = 0; x < lA; ++x) blk[x] = blk[x] + e1b[x] * 1.0;
-      } else {
-        mz_outer_terms(nB, nA, xb, xa, r2 < L.cutof1, e1b, e2a);
-        for (int x = 0; x < lA; ++x) blk[x] = blk[x] + e2a[x] * 1.0;
+        if (my_entry >= 0) {
+          cen = enuc_entry[my_entry];
+        } else if (r2 < L.cutof1) {       // outer2: monopole term
+          double ri[23], gab;
+          reppd(nA, nB, sqrt(r2), ri, &gab);
+          cen = c_P.el[nA].tore * c_P.el[nB].tore * ri[1];
+        } else {                          // outer1: feathered point charge
+          const double rij = sqrt(r2), rb = rij / PM7_A0;
+          double aee = 0.5 / E.am + 0.5 / c_P.el[nB].am;
+          aee = aee * aee;
+          double ww = PM7_EV / sqrt(rb * rb + aee), point, cst;
+          to_point(rij, &point, &cst);
+          ww = ww * cst + (1.0 - cst) * point;
+          cen = c_P.el[nA].tore * c_P.el[nB].tore * ww;
+        }
       }
-      continue;
+      if (!(r2 < 0.00002)) {
+        double e1b[10], e2a[10];
+        has_c = true;
+        if (!(r2 < L.cutof2) && sqrt(r2) < 7.0) {
+          // a far pair inside PM7's 7 A feathering radius (a cutoff below
+          // 7 A): outer1's or outer2's terms; beyond 7 A elenuc's feathered
+          // integrals are the same point charges
+          if (B < A) {
+            mz_outer_terms(nA, nB, xa, xb, r2 < L.cutof1, e1b, e2a);
+            for (int x = 0; x < 10; ++x) if (x < lA) c[x] = e1b[x];
+          } else {
+            mz_outer_terms(nB, nA, xb, xa, r2 < L.cutof1, e1b, e2a);
+            for (int x = 0; x < 10; ++x) if (x < lA) c[x] = e2a[x];
+          }
+        } else {
+          double p[4][4], core[5][3];
+          if (B < A) {
+            const double r = rotmat(xa, xb, p);
+            core_terms(nA, nB, r, core);
+            elenuc(p, core, noA, L.iorbs[B], e1b, e2a);
+            for (int x = 0; x < 10; ++x) if (x < lA) c[x] = e1b[x];
+          } else {
+            const double r = rotmat(xb, xa, p);
+            core_terms(nB, nA, r, core);
+            elenuc(p, core, L.iorbs[B], noA, e1b, e2a);
+            for (int x = 0; x < 10; ++x) if (x < lA) c[x] = e2a[x];
+          }
+        }
+      }
     }
-    if (B < A) {
-      const double r = rotmat(xa, xb, p);
-      core_terms(nA, nB, r, core);
-      elenuc(p, core, noA, L.iorbs[B], e1b, e2a);
-      for (int x = 0; x < lA; ++x) blk[x] = blk[x] + e1b[x] * 1.0;
-    } else {
-      const double r = rotmat(xb, xa, p);
-      core_terms(nB, nA, r, core);
-      elenuc(p, core, L.iorbs[B], noA, e1b, e2a);
-      for (int x = 0; x < lA; ++x) blk[x] = blk[x] + e2a[x] * 1.0;
+    // the lanes' terms in ascending B
+    const unsigned cmask = __ballot_sync(0xffffffffu, has_c);
+    const unsigned emask = __ballot_sync(0xffffffffu, B < A);
+    for (int src = 0; src < 32; ++src) {
+      const double ce = __shfl_sync(0xffffffffu, cen, src);
+      if ((emask >> src) & 1u) en += ce;
+#pragma unroll
+      for (int x = 0; x < 10; ++x) {
+        if (x < lA) {  // lA is the warp's own, so every lane takes the shuffle or none
+          const double v = __shfl_sync(0xffffffffu, c[x], src);
+          if ((cmask >> src) & 1u) blk[x] = blk[x] + v * 1.0;
+        }
+      }
     }
+    __syncwarp();
   }
+  if (lane != 0) return;
   enuc_atom[A] = en;
   double* hd = h + L.pair_off[ediag];
   for (int x = 0; x < lA; ++x) hd[x] = blk[x];
@@ -1141,7 +1183,7 @@ extern "C" int mb_mz_hcore_dev(const MbMzLayout* L, const int* nat_d, const doub
     mz_hcore_pairs<<<blocks, 128, 0, stream>>>(*L, nat_d, coord_d, h, w, enuc_entry);
     MB_LAUNCH_CHECK();
   }
-  mz_hcore_diag<<<(L->numat + 63) / 64, 64, 0, stream>>>(*L, nat_d, coord_d, h, w, enuc_entry, enuc_atom);
+  mz_hcore_diag<<<(L->numat + 3) / 4, 128, 0, stream>>>(*L, nat_d, coord_d, h, w, enuc_entry, enuc_atom);
   MB_LAUNCH_CHECK();
   enuc_sum<<<1, 1024, 0, stream>>>(L->numat, enuc_atom, enuclr_dev);
   MB_LAUNCH_CHECK();

@@ -636,30 +636,103 @@ extern "C" int mb_mz_layout_create(int numat, const int* iorbs, const double* co
   std::vector<int> pi, pj, ptr(numat + 1, 0);
   std::vector<long long> po;
   long long mpack = 0;
-  for (int i = 0; i < numat; ++i) {
-    ptr[i] = (int)pi.size();
-    const int io = iorbs[i];
-    for (int j = 0; j < i; ++j) {
-      const double dx = coord[3 * i] - coord[3 * j], dy = coord[3 * i + 1] - coord[3 * j + 1],
-                   dz = coord[3 * i + 2] - coord[3 * j + 2];
-      const double r = dx * dx + dy * dy + dz * dz;
-      long long v;
-      if (r < cutof2) {
-        v = mpack;
+  auto r2_of = [&](int i, int j) {
+    const double dx = coord[3 * i] - coord[3 * j], dy = coord[3 * i + 1] - coord[3 * j + 1],
+                 dz = coord[3 * i + 2] - coord[3 * j + 2];
+    return dx * dx + dy * dy + dz * dz;
+  };
+  if (nijbo) {
+    // every pair's class is wanted: the full triangle
+    for (int i = 0; i < numat; ++i) {
+      ptr[i] = (int)pi.size();
+      const int io = iorbs[i];
+      for (int j = 0; j < i; ++j) {
+        const double r = r2_of(i, j);
+        long long v;
+        if (r < cutof2) {
+          v = mpack;
+          pi.push_back(i);
+          pj.push_back(j);
+          po.push_back(mpack);
+          mpack += (long long)io * iorbs[j];
+        } else {
+          v = r < cutof1 ? -2 : -1;
+        }
+        nijbo[(long long)i * numat + j] = nijbo[(long long)j * numat + i] = v;
+      }
+      pi.push_back(i);
+      pj.push_back(i);
+      po.push_back(mpack);
+      nijbo[(long long)i * numat + i] = mpack;
+      mpack += (long long)io * (io + 1) / 2;
+    }
+  } else {
+    // Only the stored pairs (r^2 < cutof2) are wanted: candidates come from a
+    // grid of cells at least the cutoff wide (a partner within the cutoff is
+    // in the same or a neighbouring cell), each atom's stored partners j < i
+    // sorted ascending, so the entries are the full triangle's, in its order.
+    double lo[3] = {coord[0], coord[1], coord[2]}, hi[3] = {coord[0], coord[1], coord[2]};
+    for (int i = 1; i < numat; ++i)
+      for (int d = 0; d < 3; ++d) {
+        lo[d] = std::min(lo[d], coord[3 * i + d]);
+        hi[d] = std::max(hi[d], coord[3 * i + d]);
+      }
+    const double rc = cutof2 > 0.0 ? sqrt(cutof2) : 0.0;
+    int nc[3];
+    double edge[3];
+    long long ncell = 1;
+    for (int d = 0; d < 3; ++d) {
+      const double ext = hi[d] - lo[d];
+      int k = rc > 0.0 ? (int)std::min(256.0, floor(ext / (rc * (1.0 + 1.0e-9) + 1.0e-9))) : 1;
+      if (k < 1) k = 1;
+      nc[d] = k;
+      edge[d] = std::max(ext / k, rc * (1.0 + 1.0e-9) + 1.0e-9);
+      ncell *= k;
+    }
+    auto cell_of = [&](int i, int d) {
+      int c = (int)((coord[3 * i + d] - lo[d]) / edge[d]);
+      return c < 0 ? 0 : (c >= nc[d] ? nc[d] - 1 : c);
+    };
+    std::vector<int> cstart(ncell + 1, 0), catom(numat), acell(numat);
+    for (int i = 0; i < numat; ++i) {
+      acell[i] = (cell_of(i, 0) * nc[1] + cell_of(i, 1)) * nc[2] + cell_of(i, 2);
+      cstart[acell[i] + 1]++;
+    }
+    for (long long c = 0; c < ncell; ++c) cstart[c + 1] += cstart[c];
+    {
+      std::vector<int> fill(cstart.begin(), cstart.end() - 1);
+      for (int i = 0; i < numat; ++i) catom[fill[acell[i]]++] = i;  // ascending atoms in every cell
+    }
+    std::vector<int> cand;
+    for (int i = 0; i < numat; ++i) {
+      ptr[i] = (int)pi.size();
+      const int io = iorbs[i];
+      cand.clear();
+      if (rc > 0.0) {
+        const int cx = cell_of(i, 0), cy = cell_of(i, 1), cz = cell_of(i, 2);
+        for (int x = std::max(cx - 1, 0); x <= std::min(cx + 1, nc[0] - 1); ++x)
+          for (int y = std::max(cy - 1, 0); y <= std::min(cy + 1, nc[1] - 1); ++y)
+            for (int z = std::max(cz - 1, 0); z <= std::min(cz + 1, nc[2] - 1); ++z) {
+              const long long c = ((long long)x * nc[1] + y) * nc[2] + z;
+              for (int q = cstart[c]; q < cstart[c + 1]; ++q) {
+                const int j = catom[q];
+                if (j >= i) break;
+                if (r2_of(i, j) < cutof2) cand.push_back(j);
+              }
+            }
+        std::sort(cand.begin(), cand.end());
+      }
+      for (int j : cand) {
         pi.push_back(i);
         pj.push_back(j);
         po.push_back(mpack);
         mpack += (long long)io * iorbs[j];
-      } else {
-        v = r < cutof1 ? -2 : -1;
       }
-      if (nijbo) nijbo[(long long)i * numat + j] = nijbo[(long long)j * numat + i] = v;
+      pi.push_back(i);
+      pj.push_back(i);
+      po.push_back(mpack);
+      mpack += (long long)io * (io + 1) / 2;
     }
-    pi.push_back(i);
-    pj.push_back(i);
-    po.push_back(mpack);
-    if (nijbo) nijbo[(long long)i * numat + i] = mpack;
-    mpack += (long long)io * (io + 1) / 2;
   }
   ptr[numat] = (int)pi.size();
   // integral blocks in entry order: the dense W's layout without the far pairs

@@ -375,6 +375,52 @@ def _water_frame_axes(o, h1, h2) -> np.ndarray:
     return np.stack([e1, e2, np.cross(e1, e2)], axis=1)
 
 
+def _water_frames(o, h1, h2) -> np.ndarray:
+    """_water_frame_axes for every molecule at once: (nmol, 3, 3)."""
+    e1 = (h1 - o) + (h2 - o)
+    e1 = e1 / np.sqrt(np.einsum("mi,mi->m", e1, e1))[:, None]
+    e2 = h1 - h2
+    e2 = e2 - np.einsum("mi,mi->m", e2, e1)[:, None] * e1
+    e2 = e2 / np.sqrt(np.einsum("mi,mi->m", e2, e2))[:, None]
+    return np.stack([e1, e2, np.cross(e1, e2)], axis=2)
+
+
+def _water_lmo_arrays(C, o, h1, h2, pad_atoms: int):
+    """The reference's LMO arrays (ncf, nncf, icocc, ncocc, cocc) for one
+    water's localised orbitals C (6 x nl: O s, px, py, pz, H1 s, H2 s)
+    carried into every molecule (O at o[m], hydrogens at h1[m], h2[m]): the s
+    coefficients as they are, the p coefficients rotated from the first
+    molecule's frame into each molecule's.  LMO m * nl + k lists its three
+    atoms by falling weight in C[:, k], followed by pad_atoms spare slots."""
+    nmol, nl = len(o), C.shape[1]
+    R0 = _water_frames(o[:1], h1[:1], h2[:1])[0]
+    Rm = _water_frames(o, h1, h2)                            # (nmol, 3, 3)
+    q = np.einsum("ji,jk->ik", R0, C[1:4, :])                # (3, nl): frame components
+    pm = np.einsum("mij,jk->mik", Rm, q)                     # (nmol, 3, nl)
+    per_icocc = 3 + pad_atoms
+    per_cocc = 6 + 4 * pad_atoms
+    nlmo = nmol * nl
+    ncf = np.full(nlmo, 3, np.int32)
+    nncf = (np.arange(nlmo) * per_icocc).astype(np.int32)
+    ncocc = (np.arange(nlmo) * per_cocc).astype(np.int32)
+    icocc = np.zeros((nmol, nl, per_icocc), np.int32)
+    cocc = np.zeros((nmol, nl, per_cocc))
+    mol = np.arange(nmol)
+    for k in range(nl):
+        weights = np.array([np.sum(C[:4, k] ** 2), C[4, k] ** 2, C[5, k] ** 2])
+        pos = 0
+        for slot, a in enumerate(np.argsort(-weights, kind="stable")):
+            icocc[:, k, slot] = 3 * mol + a + 1
+            if a == 0:
+                cocc[:, k, pos] = C[0, k]
+                cocc[:, k, pos + 1:pos + 4] = pm[:, :, k]
+                pos += 4
+            else:
+                cocc[:, k, pos] = C[3 + a, k]
+                pos += 1
+    return ncf, nncf, icocc.reshape(-1), ncocc, cocc.reshape(-1)
+
+
 def water_lmos(nat, xyz, pad_atoms: int = 0, scfcrt: float = 1.0e-8):
     """Starting LMOs for (H2O)_n, atoms given as O, H, H per molecule: the work
     makvec (MOZYME/makvec.F90:16-143) does from a Lewis structure, done here
@@ -405,38 +451,6 @@ def water_lmos(nat, xyz, pad_atoms: int = 0, scfcrt: float = 1.0e-8):
     ctx.close()
     atom_of = np.array([0, 0, 0, 0, 1, 2])
     loc = [_pipek_mezey(c[:, :4], atom_of, 3), _pipek_mezey(c[:, 4:6], atom_of, 3)]
-    R0 = _water_frame_axes(o[0], h1[0], h2[0])
-    # per LMO: the atoms in falling weight (the same in every molecule)
-    orders = []
-    for C in loc:
-        orders.append([np.argsort(-np.array([np.sum(C[:4, k] ** 2), C[4, k] ** 2, C[5, k] ** 2]), kind="stable")
-                       for k in range(C.shape[1])])
     iorbs = np.where(nat == 1, 1, 4).astype(np.int32)
-    out = []
-    for C, order in zip(loc, orders):
-        nl = C.shape[1]
-        per_icocc = 3 + pad_atoms
-        per_cocc = 6 + 4 * pad_atoms
-        ncf = np.full(nmol * nl, 3, np.int32)
-        nncf = (np.arange(nmol * nl) * per_icocc).astype(np.int32)
-        ncocc = (np.arange(nmol * nl) * per_cocc).astype(np.int32)
-        icocc = np.zeros(nmol * nl * per_icocc, np.int32)
-        cocc = np.zeros(nmol * nl * per_cocc)
-        # p coefficients in the molecule frame, then into each molecule's axes
-        q = np.einsum("ji,jk->ik", R0, C[1:4, :])              # (3, nl): frame components
-        Rm = np.stack([_water_frame_axes(o[m], h1[m], h2[m]) for m in range(nmol)])  # (nmol, 3, 3)
-        pm = np.einsum("mij,jk->mik", Rm, q)                    # (nmol, 3, nl)
-        for k in range(nl):
-            for m in range(nmol):
-                lm = m * nl + k
-                ia, ic = nncf[lm], ncocc[lm]
-                for slot, a in enumerate(order[k]):
-                    icocc[ia + slot] = 3 * m + a + 1
-                    if a == 0:
-                        cocc[ic:ic + 4] = [C[0, k], pm[m, 0, k], pm[m, 1, k], pm[m, 2, k]]
-                        ic += 4
-                    else:
-                        cocc[ic] = C[3 + a, k]
-                        ic += 1
-        out.append((ncf, nncf, icocc, ncocc, cocc))
+    out = [_water_lmo_arrays(C, o, h1, h2, pad_atoms) for C in loc]
     return iorbs, out[0], out[1]

@@ -111,6 +111,38 @@ def _water_case(nwater, radius=4.0):
     return nat, xyz, iorbs, lmos
 
 
+def test_water_lmo_arrays_carry_one_molecule_into_every_orientation():
+    """The starting LMOs' arrays, built for all molecules at once, are those
+    of the per-molecule construction: each LMO's atoms by falling weight,
+    the s coefficients as given, the p coefficients rotated from the first
+    molecule's frame into the molecule's own, spare slots after every LMO."""
+    from mopac_gpu_b200 import mozyme
+    nat, xyz, _ = workloads.water_box(24, seed=5)
+    xyz = np.asarray(xyz, float).reshape(-1, 3)
+    o, h1, h2 = xyz[0::3], xyz[1::3], xyz[2::3]
+    rng = np.random.default_rng(1)
+    C = np.linalg.qr(rng.normal(size=(6, 6)))[0][:, :4]
+    pad = 5
+    ncf, nncf, icocc, ncocc, cocc = mozyme._water_lmo_arrays(C, o, h1, h2, pad)
+    R0 = mozyme._water_frame_axes(o[0], h1[0], h2[0])
+    nmol, nl = len(o), C.shape[1]
+    assert np.all(ncf == 3) and len(nncf) == nmol * nl
+    for m in range(nmol):
+        Rm = mozyme._water_frame_axes(o[m], h1[m], h2[m])
+        pm = Rm @ (R0.T @ C[1:4, :])
+        for k in range(nl):
+            lm = m * nl + k
+            order = np.argsort(-np.array([np.sum(C[:4, k] ** 2), C[4, k] ** 2, C[5, k] ** 2]), kind="stable")
+            ia, ic = nncf[lm], ncocc[lm]
+            assert ia == lm * (3 + pad) and ic == lm * (6 + 4 * pad)
+            want = []
+            for slot, a in enumerate(order):
+                assert icocc[ia + slot] == 3 * m + a + 1
+                want += [C[0, k], *pm[:, k]] if a == 0 else [C[3 + a, k]]
+            np.testing.assert_allclose(cocc[ic:ic + 6], want, rtol=0, atol=1e-14)
+            assert np.all(icocc[ia + 3:ia + 3 + pad] == 0) and np.all(cocc[ic + 6:ic + 6 + 4 * pad] == 0.0)
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("nwater", [16, 128, 512])
 def test_gpu_layout_matches_fillij(nwater):
@@ -124,6 +156,33 @@ def test_gpu_layout_matches_fillij(nwater):
     np.testing.assert_array_equal(L.nijbo, nijbo)
     np.testing.assert_array_equal(L.idiag_host, mo.idiag(iorbs, nijbo))
     L.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("nwater,cut", [(16, 9.0), (512, 9.0), (512, 4.0), (2048, 9.0)])
+def test_gpu_layout_from_cells_is_the_full_triangle(nwater, cut):
+    """Without nijbo the stored pairs come from a grid of cells: the same
+    entries, offsets, integral offsets and neighbour lists as the scan of
+    the whole triangle that fills nijbo."""
+    torch = _need_gpu()
+    from mopac_gpu_b200.mozyme import Layout, _device_view
+    nat, xyz, _ = workloads.water_box(nwater)
+    iorbs = np.where(np.asarray(nat) == 1, 1, 4).astype(np.int32)
+    c1, c2 = mo.cutoffs(len(nat), cut)
+    a = Layout(iorbs, xyz, c1, c2, want_nijbo=True)
+    b = Layout(iorbs, xyz, c1, c2)
+    assert (a.mpack, a.s.npairs, a.s.nw) == (b.mpack, b.s.npairs, b.s.nw)
+    n, e = len(nat), int(a.s.npairs)
+    nb = int(_device_view(a.s.nbr_ptr + 4 * n, 1, "<i4").item())
+    for name, count, ty in (("pair_ptr", n + 1, "<i4"), ("pair_i", e, "<i4"), ("pair_j", e, "<i4"),
+                            ("pair_off", e, "<i8"), ("pair_woff", e, "<i8"), ("nbr_ptr", n + 1, "<i4"),
+                            ("nbr_atom", nb, "<i4"), ("nbr_entry", nb, "<i8")):
+        x = _device_view(getattr(a.s, name), count, ty)
+        y = _device_view(getattr(b.s, name), count, ty)
+        assert torch.equal(x, y), name
+    np.testing.assert_array_equal(a.idiag_host, b.idiag_host)
+    a.close()
+    b.close()
 
 
 @pytest.mark.gpu
