@@ -30,7 +30,37 @@ namespace {
 
 __device__ __forceinline__ int pair_elems(int io, int jo, bool diag) { return diag ? io * (io + 1) / 2 : io * jo; }
 
-// One warp per stored block (grid-stride over pair entries).
+// Adds the contributions of the LMOs matched in this chunk (bit m of mask:
+// lane m holds the match's coefficient offsets on atom i, my_ca, and on atom
+// j, my_cb), in lane order, to this lane's element (j1, k1).  Eight matches'
+// coefficients are loaded before their products are added, so the loads
+// overlap; the additions keep the reference's order.
+__device__ __forceinline__ void mz_density_add(unsigned mask, int my_ca, int my_cb, bool act, int j1, int k1,
+                                               const double* __restrict__ cocc, double& acc) {
+  while (mask) {  // warp-uniform
+    double va[8], vb[8];
+    bool hv[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      hv[q] = mask != 0;
+      const int src = hv[q] ? __ffs(mask) - 1 : 0;
+      if (hv[q]) mask &= mask - 1;
+      const int ca = __shfl_sync(0xffffffffu, my_ca, src), cb = __shfl_sync(0xffffffffu, my_cb, src);
+      va[q] = (hv[q] && act) ? __ldg(cocc + ca + j1) : 0.0;
+      vb[q] = (hv[q] && act) ? __ldg(cocc + cb + k1) : 0.0;
+    }
+#pragma unroll
+    for (int q = 0; q < 8; ++q)
+      if (hv[q] && act) acc = DADD(acc, DMUL(vb[q], va[q]));
+  }
+}
+
+// One warp per stored block (grid-stride over pair entries).  The block's
+// element (j1, k1) sums c(LMO, j1 on atom i) c(LMO, k1 on atom j) over the
+// LMOs on both atoms in ascending LMO order (density_for_MOZYME.F90's order):
+// the shorter of the two atoms' ascending LMO lists is taken 32 entries at a
+// time, one per lane, each searched in the longer list, and the matches of
+// the chunk are added in order.
 __global__ void __launch_bounds__(256) mz_density_kernel(MbMzLayout L, MbMzLmos Q, int mode, const double* __restrict__ partp,
                                                         double* __restrict__ p, double spinfa, int scale) {
   const int lane = threadIdx.x & 31;
@@ -57,18 +87,40 @@ __global__ void __launch_bounds__(256) mz_density_kernel(MbMzLayout L, MbMzLmos 
       if (mode == -1) acc = DMUL(-0.5, partp[off + lane]);
       else if (mode != 0) acc = DMUL(0.5, partp[off + lane]);
     }
-    int a = Q.atom_ptr[i], ae = Q.atom_ptr[i + 1];
-    int b = Q.atom_ptr[j], be = Q.atom_ptr[j + 1];
-    while (a < ae && b < be) {  // warp-uniform merge of two ascending LMO lists
-      const int la = Q.atom_lmo[a], lb = Q.atom_lmo[b];
-      if (la == lb) {
-        if (act) acc = DADD(acc, DMUL(Q.cocc[Q.atom_coff[b] + k1], Q.cocc[Q.atom_coff[a] + j1]));
-        ++a;
-        ++b;
-      } else if (la < lb) {
-        ++a;
-      } else {
-        ++b;
+    const int a0 = Q.atom_ptr[i], ae = Q.atom_ptr[i + 1];
+    if (diag) {
+      // every LMO on the atom meets itself
+      for (int base = a0; base < ae; base += 32) {
+        const int idx = base + lane;
+        const int c = idx < ae ? Q.atom_coff[idx] : 0;
+        const unsigned mask = __ballot_sync(0xffffffffu, idx < ae);
+        mz_density_add(mask, c, c, act, j1, k1, Q.cocc, acc);
+      }
+    } else {
+      const int b0 = Q.atom_ptr[j], be = Q.atom_ptr[j + 1];
+      const bool short_i = (ae - a0) <= (be - b0);  // walk atom i's list, search atom j's
+      const int s0 = short_i ? a0 : b0, se = short_i ? ae : be;
+      int lo = short_i ? b0 : a0;
+      const int le = short_i ? be : ae;
+      for (int base = s0; base < se && lo < le; base += 32) {
+        const int idx = base + lane;
+        const int x = idx < se ? __ldg(Q.atom_lmo + idx) : 0x7fffffff;
+        int lb = lo, ub = le;  // first entry >= x in the longer list
+        while (lb < ub) {
+          const int mid = (lb + ub) >> 1;
+          if (__ldg(Q.atom_lmo + mid) < x) lb = mid + 1;
+          else ub = mid;
+        }
+        const bool hit = idx < se && lb < le && __ldg(Q.atom_lmo + lb) == x;
+        int my_ca = 0, my_cb = 0;
+        if (hit) {
+          const int cs = Q.atom_coff[idx], cl = Q.atom_coff[lb];
+          my_ca = short_i ? cs : cl;
+          my_cb = short_i ? cl : cs;
+        }
+        const unsigned mask = __ballot_sync(0xffffffffu, hit);
+        lo = __shfl_sync(0xffffffffu, lb, 31);  // the chunk's largest entry bounds the next search
+        mz_density_add(mask, my_ca, my_cb, act, j1, k1, Q.cocc, acc);
       }
     }
     if (act) p[off + lane] = scale ? DMUL(spinfa, acc) : acc;
