@@ -29,3 +29,27 @@ def test_reference_arm_prints_one_contract_line():
     assert abs(d["ms_per_step"] * d["steps"] / 1e3 - d["scf_wall_s"]) < 1e-6
     assert d["plain_mode"]["niter"] > 4
     assert d["config"]["mode"] == "fast" and d["config"]["finish_dp"] == 1e-7
+
+
+def test_panel_roofline_counts_every_eigensolve_order():
+    """The dominant kernel's algorithmic bytes cover every eigensolve of the
+    timed SCFs: the whole n for each full eigensolve, and the occupied and
+    virtual orders for an exit diagonalisation solved as the two blocks."""
+    from types import SimpleNamespace
+    sys.path.insert(0, ROOT)
+    import bench
+    ctx = SimpleNamespace(norbs=3072, nclose=2048)
+    results = [SimpleNamespace(n_full_diag=1, exit_split=True), SimpleNamespace(n_full_diag=2, exit_split=False)]
+    sizes = bench.eigh_sizes(ctx, results)
+    assert sizes == [3072, 2048, 1024, 3072, 3072]
+    panels = sum((m - 2) // 32 + 1 for m in sizes)
+    kst = {"tridiag_panel": {"launches": panels, "total_ms": 100.0}}
+    r = bench.panel_roofline(ctx, kst, sizes)
+    algo = sum(8.0 * (m - 1) * m * (2 * m - 1) / 6.0 for m in sizes)
+    assert r["launches"] == r["launches_expected"] == panels
+    assert abs(r["achieved"] - algo / 0.1 / 1e9) < 1e-6 * r["achieved"]
+    assert abs(r["frac"] - r["achieved"] / r["peak"]) < 1e-12
+    assert r["eigensolve_orders"] == [1024, 2048, 3072]
+    # the DRAM traffic of a 3072 panel, scaled by algorithmic bytes
+    one = bench.panel_roofline(ctx, {"tridiag_panel": {"launches": 96, "total_ms": 40.0}}, [3072])
+    assert abs(one["traffic"] - bench.PANEL_DRAM_BYTES) < 1.0
