@@ -180,7 +180,11 @@ int mb_ctx_get_hw(mb_ctx* ctx, double* h, double* w, double* enuclr);
 
 /* Closed-shell RHF SCF (iter, SCF/iter.F90) from the standard diagonal guess
  * (moldat.F90:731-760).  The whole loop runs on the device; only scalars
- * cross to the host each iteration. */
+ * cross to the host each iteration.  Work arrays are allocated in the
+ * context on first use and kept for later calls (the pseudo-diagonalisation,
+ * the split-precision planes, Pulay's histories, and for an SCF that ends in
+ * the FP64 finish the split exit diagonalisation's 2 n^2 + ~(3/2)(k^2 + v^2)
+ * + 2 k v doubles, k = nclose, v = norbs - nclose). */
 int mb_scf_run(mb_ctx* ctx, const mb_scf_opts* opts, mb_scf_result* res);
 
 /* Starting density for opts.guess = 1: a host packed total density (mpack)
