@@ -685,6 +685,8 @@ extern "C" int mb_mz_layout_create(int numat, const int* iorbs, const double* co
   memset(out, 0, sizeof(*out));
   for (int i = 0; i < numat; ++i)
     if (iorbs[i] < 0 || iorbs[i] > 4) return mb_set_error(MB_ERR_UNSUPPORTED, "MOZYME layout: s and p shells only");
+  for (long long q = 0; q < 3LL * numat; ++q)
+    if (!isfinite(coord[q])) return mb_set_error(MB_ERR_ARG, "MOZYME layout: non-finite coordinate");
   std::vector<int> pi, pj, ptr(numat + 1, 0);
   std::vector<long long> po;
   long long mpack = 0;

@@ -131,3 +131,21 @@ def test_bounded_wait_selftest_checks_its_limit_before_any_gpu_work(libpath):
     assert L.mb_selftest_bounded_wait(0, fake, None) == 1
     assert L.mb_selftest_bounded_wait(200000000, fake, None) == 1
     assert L.mb_selftest_bounded_wait(1000, None, None) == 1
+
+
+def test_mozyme_layout_refuses_non_finite_coordinates_before_any_gpu_work(libpath):
+    """A NaN or infinite coordinate is refused before the pair search (the
+    cell grid needs finite extents) and before any device allocation."""
+    import numpy as np
+    from mopac_gpu_b200._lib import MbMzLayout
+    L = ctypes.CDLL(libpath)
+    L.mb_mz_layout_create.restype = ctypes.c_int
+    L.mb_last_error.restype = ctypes.c_char_p
+    iorbs = np.array([4, 1, 1], np.int32)
+    for bad in (np.nan, np.inf):
+        xyz = np.array([0.0, 0.0, 0.0, 0.96, 0.0, 0.0, bad, 0.9, 0.0])
+        lay = MbMzLayout()
+        rc = L.mb_mz_layout_create(3, iorbs.ctypes.data, xyz.ctypes.data, ctypes.c_double(100.0),
+                                   ctypes.c_double(98.0), ctypes.byref(lay), None)
+        assert rc == 1  # MB_ERR_ARG
+        assert b"non-finite" in L.mb_last_error()
