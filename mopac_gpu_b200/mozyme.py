@@ -421,6 +421,138 @@ def _water_lmo_arrays(C, o, h1, h2, pad_atoms: int):
     return ncf, nncf, icocc.reshape(-1), ncocc, cocc.reshape(-1)
 
 
+# covalent radii (A) of the bond graph that splits a system into molecules
+_COVALENT = {1: 0.31, 6: 0.76, 8: 0.66}
+
+
+def molecules(nat, xyz, scale: float = 1.25) -> list:
+    """The molecules of a system: the connected components of its bond graph,
+    atoms A and B bonded when r_AB < scale (R_A + R_B) with the covalent radii
+    R of H, C and O (0.31, 0.76, 0.66 A).  Each molecule is the ascending
+    array of its atoms (0-based); molecules come in order of their first
+    atom."""
+    from scipy.spatial import cKDTree
+    nat = np.asarray(nat)
+    xyz = np.asarray(xyz, float).reshape(-1, 3)
+    try:
+        rad = np.array([_COVALENT[int(z)] for z in nat])
+    except KeyError as e:
+        raise ValueError(f"molecules: element {e} outside H, C, O") from None
+    parent = np.arange(len(nat))
+
+    def root(a):
+        while parent[a] != a:
+            parent[a] = parent[parent[a]]
+            a = parent[a]
+        return a
+
+    if len(nat) > 1:
+        pairs = cKDTree(xyz).query_pairs(r=2.0 * scale * rad.max(), output_type="ndarray")
+        if len(pairs):
+            d = np.linalg.norm(xyz[pairs[:, 0]] - xyz[pairs[:, 1]], axis=1)
+            for a, b in pairs[d < scale * (rad[pairs[:, 0]] + rad[pairs[:, 1]])]:
+                ra, rb = root(a), root(b)
+                if ra != rb:
+                    parent[max(ra, rb)] = min(ra, rb)
+    roots = np.array([root(a) for a in range(len(nat))])
+    return [np.flatnonzero(roots == r) for r in np.unique(roots)]
+
+
+def _kabsch(p: np.ndarray, q: np.ndarray):
+    """The proper rotation R (det +1) that best maps the centred points p onto
+    the centred points q (rows), and the RMS distance left."""
+    u, _, vt = np.linalg.svd(p.T @ q)
+    d = np.sign(np.linalg.det(vt.T @ u.T)) or 1.0
+    r = vt.T @ np.diag([1.0, 1.0, d]) @ u.T
+    return r, float(np.sqrt(np.mean(np.sum((p @ r.T - q) ** 2, axis=1))))
+
+
+def _pack_lmos(iorbs: np.ndarray, lmos: list, pad_atoms: int):
+    """The reference's LMO arrays (ncf, nncf, icocc, ncocc, cocc) for LMOs
+    given as (atoms, coefficients over those atoms' orbitals in that order):
+    each LMO lists its atoms by falling weight (its bond's atoms first, as
+    hbonds expects), followed by pad_atoms spare atom slots."""
+    ncf, nncf, icocc, ncocc, cocc = [], [], [], [], []
+    for atoms, vec in lmos:
+        offs = np.concatenate([[0], np.cumsum(iorbs[atoms])])
+        w = np.array([np.sum(vec[offs[k]:offs[k + 1]] ** 2) for k in range(len(atoms))])
+        nncf.append(len(icocc))
+        ncocc.append(len(cocc))
+        ncf.append(len(atoms))
+        for k in np.argsort(-w, kind="stable"):
+            icocc.append(int(atoms[k]) + 1)
+            cocc.extend(vec[offs[k]:offs[k + 1]].tolist())
+        icocc.extend([0] * pad_atoms)
+        cocc.extend([0.0] * (4 * pad_atoms))
+    return (np.array(ncf, np.int32), np.array(nncf, np.int32), np.array(icocc, np.int32),
+            np.array(ncocc, np.int32), np.array(cocc, np.float64))
+
+
+def molecule_lmos(nat, xyz, pad_atoms: int = 0, scfcrt: float = 1.0e-8, orbitals=None, same_tol: float = 1.0e-6):
+    """Starting LMOs for a system of separate H, C, O molecules (a liquid, a
+    mixture, a molecular crystal): the work makvec (MOZYME/makvec.F90:16-143)
+    does from a Lewis structure, done from the isolated molecules.  The
+    system is split into molecules by its bond graph (``molecules``); each
+    distinct molecule's SCF orbitals (this library's dense SCF on the GPU, or
+    ``orbitals(nat, xyz) -> (C, nclose)`` when given) are Pipek-Mezey
+    localised, occupied and virtual separately, and carried into every copy
+    of that molecule: a copy has the same elements in the same order and the
+    same shape up to a proper rotation (RMS <= same_tol A after the best
+    rotation); its LMOs keep the s coefficients and rotate the p ones.  A
+    molecule with no copy earlier in the system gets its own SCF.  LMOs come
+    molecule by molecule; an LMO lists all atoms of its molecule by falling
+    weight and is followed by pad_atoms spare atom slots for diagg2 to grow
+    it.  Returns (iorbs, occ, vir) in the reference's arrays (ncf, nncf,
+    icocc, ncocc, cocc)."""
+    nat = np.asarray(nat).astype(np.int32)
+    xyz = np.asarray(xyz, float).reshape(-1, 3)
+    if np.any((nat != 1) & (nat != 6) & (nat != 8)):
+        raise ValueError("molecule_lmos: elements outside H, C, O")
+    iorbs = np.where(nat == 1, 1, 4).astype(np.int32)
+
+    def scf_orbitals(zn, r):
+        if orbitals is not None:
+            return orbitals(zn, r)
+        from .scf import ScfContext
+        ctx = ScfContext(zn, r)
+        try:
+            ctx.hcore()
+            ctx.run(pseudo=False, scfcrt=scfcrt, finish_dp=1.0e-10, finish_max=200)
+            c, _ = ctx.vectors()
+            return c, ctx.nclose
+        finally:
+            ctx.close()
+
+    templates = []  # (elements, centred coordinates, localised occupied, localised virtual)
+    occ, vir = [], []
+    for atoms in molecules(nat, xyz):
+        zn, r = nat[atoms], xyz[atoms]
+        centred = r - r.mean(axis=0)
+        rot = None
+        for tz, tc, tocc, tvir in templates:
+            if len(tz) == len(zn) and np.array_equal(tz, zn):
+                R, rms = _kabsch(tc, centred)
+                if rms <= same_tol:
+                    rot, lo, lv = R, tocc, tvir
+                    break
+        if rot is None:
+            c, nclose = scf_orbitals(zn, r)
+            atom_of = np.repeat(np.arange(len(atoms)), iorbs[atoms])
+            lo = _pipek_mezey(c[:, :nclose], atom_of, len(atoms)) if nclose > 0 else c[:, :0]
+            lv = _pipek_mezey(c[:, nclose:], atom_of, len(atoms)) if nclose < c.shape[0] else c[:, :0]
+            templates.append((zn.copy(), centred, lo, lv))
+            rot = np.eye(3)
+        # the p rows of every heavy atom rotate with the molecule
+        prow = np.concatenate([[0], np.cumsum(iorbs[atoms])])[:-1][iorbs[atoms] == 4]
+        for src, dst in ((lo, occ), (lv, vir)):
+            v = src.copy()
+            for o in prow:
+                v[o + 1:o + 4, :] = rot @ src[o + 1:o + 4, :]
+            for k in range(v.shape[1]):
+                dst.append((atoms, v[:, k]))
+    return iorbs, _pack_lmos(iorbs, occ, pad_atoms), _pack_lmos(iorbs, vir, pad_atoms)
+
+
 def water_lmos(nat, xyz, pad_atoms: int = 0, scfcrt: float = 1.0e-8):
     """Starting LMOs for (H2O)_n, atoms given as O, H, H per molecule: the work
     makvec (MOZYME/makvec.F90:16-143) does from a Lewis structure, done here

@@ -143,6 +143,77 @@ def test_water_lmo_arrays_carry_one_molecule_into_every_orientation():
             assert np.all(icocc[ia + 3:ia + 3 + pad] == 0) and np.all(cocc[ic + 6:ic + 6 + 4 * pad] == 0.0)
 
 
+def _mixed_system():
+    """Two propanes (the second rotated and shifted) and a hydrogen-bonded
+    4-water lattice 7 A away: 34 atoms in six molecules."""
+    pn, px = small_systems()["propane"]
+    rng = np.random.default_rng(4)
+    q, _ = np.linalg.qr(rng.normal(size=(3, 3)))
+    if np.linalg.det(q) < 0:
+        q[:, 0] *= -1.0
+    px2 = (px - px.mean(axis=0)) @ q.T + np.array([7.0, 0.0, 0.0])
+    wn, wx = workloads.water_lattice(4, seed=3)
+    wx = np.asarray(wx, float).reshape(-1, 3) + np.array([0.0, 7.0, 0.0])
+    return np.concatenate([pn, pn, wn]).astype(np.int32), np.concatenate([px, px2, wx])
+
+
+def _oracle_orbitals(zn, r):
+    s = so.make_system(zn, r)
+    return so.iter_scf(s, scfcrt=1.0e-8).c, s.nclose
+
+
+def test_molecules_are_the_bond_graph_components():
+    from mopac_gpu_b200 import mozyme
+    nat, xyz = _mixed_system()
+    mols = mozyme.molecules(nat, xyz)
+    assert [len(m) for m in mols] == [11, 11, 3, 3, 3, 3]
+    assert np.array_equal(np.concatenate(mols), np.arange(len(nat)))
+    nat, xyz, _ = workloads.water_box(64, seed=2)
+    assert [len(m) for m in mozyme.molecules(nat, xyz)] == [3] * 64
+    with pytest.raises(ValueError):
+        mozyme.molecules(np.array([7, 1]), np.zeros((2, 3)))
+
+
+def test_molecule_lmos_start_from_the_isolated_molecules_and_reach_the_dense_heat():
+    """The starting LMOs of a mixed system (the isolated molecules' SCF
+    orbitals, localised, a rotated copy carried over from the first propane)
+    give the sum of the isolated molecules' densities, the copy's LMOs are
+    those of its own SCF, and the oracle's MOZYME loop from them reaches the
+    dense SCF's heat."""
+    from mopac_gpu_b200 import mozyme
+    nat, xyz = _mixed_system()
+    iorbs, occ, vir = mozyme.molecule_lmos(nat, xyz, pad_atoms=len(nat), orbitals=_oracle_orbitals)
+    _, occ_own, _ = mozyme.molecule_lmos(nat, xyz, pad_atoms=len(nat), orbitals=_oracle_orbitals, same_tol=-1.0)
+    assert len(occ[0]) == 2 * 10 + 4 * 4 and len(vir[0]) == 2 * 10 + 4 * 2
+    n = int(iorbs.sum())
+    first = np.concatenate([[0], np.cumsum(iorbs)])
+
+    def lmo_density(lmos):
+        ncf, nncf, icocc, ncocc, cocc = lmos
+        P = np.zeros((n, n))
+        for k in range(len(ncf)):
+            v = np.zeros(n)
+            ic = ncocc[k]
+            for a in icocc[nncf[k]:nncf[k] + ncf[k]] - 1:
+                v[first[a]:first[a] + iorbs[a]] = cocc[ic:ic + iorbs[a]]
+                ic += iorbs[a]
+            P += 2.0 * np.outer(v, v)
+        return P
+
+    want = np.zeros((n, n))
+    for atoms in mozyme.molecules(nat, xyz):
+        rows = np.concatenate([np.arange(first[a], first[a + 1]) for a in atoms])
+        c, nclose = _oracle_orbitals(nat[atoms], xyz[atoms])
+        want[np.ix_(rows, rows)] = 2.0 * c[:, :nclose] @ c[:, :nclose].T
+    np.testing.assert_allclose(lmo_density(occ), want, atol=1e-6)
+    np.testing.assert_allclose(lmo_density(occ), lmo_density(occ_own), atol=1e-6)
+    s = oracle_system(nat, xyz)
+    c1, c2 = mo.cutoffs(len(nat))
+    r = mo.iter_for_mozyme(s, occ, vir, c1, c2, scfcrt=1.0e-5, itrmax=20)
+    dense = so.iter_scf(s, scfcrt=1.0e-6)
+    assert abs(r["escf"] - dense.escf) < 2.0e-3
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("nwater", [16, 128, 512])
 def test_gpu_layout_matches_fillij(nwater):
