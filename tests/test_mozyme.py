@@ -215,6 +215,35 @@ def test_molecule_lmos_start_from_the_isolated_molecules_and_reach_the_dense_hea
 
 
 @pytest.mark.gpu
+def test_gpu_molecule_lmos_are_those_of_the_oracle_orbitals():
+    """On the GPU the starting LMOs come from this library's dense SCF of each
+    distinct molecule: the same LMO density as from the oracle's orbitals."""
+    _need_gpu()
+    from mopac_gpu_b200 import mozyme
+    nat, xyz = _mixed_system()
+    iorbs, occ, vir = mozyme.molecule_lmos(nat, xyz, pad_atoms=4)
+    _, occ_o, vir_o = mozyme.molecule_lmos(nat, xyz, pad_atoms=4, orbitals=_oracle_orbitals)
+    n = int(iorbs.sum())
+    first = np.concatenate([[0], np.cumsum(iorbs)])
+
+    def lmo_density(lmos):
+        ncf, nncf, icocc, ncocc, cocc = lmos
+        P = np.zeros((n, n))
+        for k in range(len(ncf)):
+            v = np.zeros(n)
+            ic = ncocc[k]
+            for a in icocc[nncf[k]:nncf[k] + ncf[k]] - 1:
+                v[first[a]:first[a] + iorbs[a]] = cocc[ic:ic + iorbs[a]]
+                ic += iorbs[a]
+            P += 2.0 * np.outer(v, v)
+        return P
+
+    assert len(occ[0]) == len(occ_o[0]) and len(vir[0]) == len(vir_o[0])
+    np.testing.assert_allclose(lmo_density(occ), lmo_density(occ_o), atol=1e-6)
+    np.testing.assert_allclose(lmo_density(vir), lmo_density(vir_o), atol=1e-6)
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("nwater", [16, 128, 512])
 def test_gpu_layout_matches_fillij(nwater):
     _need_gpu()
