@@ -431,13 +431,7 @@ def molecules(nat, xyz, scale: float = 1.25) -> list:
     R of H, C and O (0.31, 0.76, 0.66 A).  Each molecule is the ascending
     array of its atoms (0-based); molecules come in order of their first
     atom."""
-    from scipy.spatial import cKDTree
     nat = np.asarray(nat)
-    xyz = np.asarray(xyz, float).reshape(-1, 3)
-    try:
-        rad = np.array([_COVALENT[int(z)] for z in nat])
-    except KeyError as e:
-        raise ValueError(f"molecules: element {e} outside H, C, O") from None
     parent = np.arange(len(nat))
 
     def root(a):
@@ -446,16 +440,100 @@ def molecules(nat, xyz, scale: float = 1.25) -> list:
             a = parent[a]
         return a
 
-    if len(nat) > 1:
-        pairs = cKDTree(xyz).query_pairs(r=2.0 * scale * rad.max(), output_type="ndarray")
-        if len(pairs):
-            d = np.linalg.norm(xyz[pairs[:, 0]] - xyz[pairs[:, 1]], axis=1)
-            for a, b in pairs[d < scale * (rad[pairs[:, 0]] + rad[pairs[:, 1]])]:
-                ra, rb = root(a), root(b)
-                if ra != rb:
-                    parent[max(ra, rb)] = min(ra, rb)
+    for a, b in bonds(nat, xyz, scale):
+        ra, rb = root(a), root(b)
+        if ra != rb:
+            parent[max(ra, rb)] = min(ra, rb)
     roots = np.array([root(a) for a in range(len(nat))])
     return [np.flatnonzero(roots == r) for r in np.unique(roots)]
+
+
+def bonds(nat, xyz, scale: float = 1.25) -> np.ndarray:
+    """The bond graph's edges (a, b), a < b, in ascending order: atoms closer
+    than scale times the sum of their covalent radii (H 0.31, C 0.76,
+    O 0.66 A)."""
+    from scipy.spatial import cKDTree
+    nat = np.asarray(nat)
+    xyz = np.asarray(xyz, float).reshape(-1, 3)
+    try:
+        rad = np.array([_COVALENT[int(z)] for z in nat])
+    except KeyError as e:
+        raise ValueError(f"element {e} outside H, C, O") from None
+    if len(nat) < 2:
+        return np.zeros((0, 2), np.int64)
+    pairs = cKDTree(xyz).query_pairs(r=2.0 * scale * rad.max(), output_type="ndarray")
+    if len(pairs) == 0:
+        return np.zeros((0, 2), np.int64)
+    pairs = np.sort(pairs, axis=1)
+    d = np.linalg.norm(xyz[pairs[:, 0]] - xyz[pairs[:, 1]], axis=1)
+    pairs = pairs[d < scale * (rad[pairs[:, 0]] + rad[pairs[:, 1]])]
+    return pairs[np.lexsort((pairs[:, 1], pairs[:, 0]))]
+
+
+def lewis_lmos(nat, xyz, pad_atoms: int = 0, scale: float = 1.25):
+    """Starting LMOs from the Lewis structure of a saturated H, C, O system
+    (alkanes, alcohols, ethers, water; one large molecule or many), the job
+    makvec (MOZYME/makvec.F90:16-143) does, here from the bond directions
+    rather than from makvec's Fock-matrix hybrids.  Every C must have four
+    single bonds, every O two and every H one (``bonds``); anything else
+    (a double bond, a radical, an ion) raises ValueError.  A heavy atom's
+    four sp3 hybrids point along its bonds and, for O, along the two lone
+    pairs that complete its tetrahedron (on the far side of the bisector of
+    its bonds, 54.74 degrees either side of their plane), orthonormalised
+    symmetrically (Loewdin); an H's hybrid is its s orbital.  A bond A-B
+    (A < B) gives the occupied LMO (h_A + h_B)/sqrt(2) and the virtual LMO
+    (h_A - h_B)/sqrt(2) on atoms A, B; a lone pair is the occupied LMO h_A on
+    its atom alone.  All LMOs are orthonormal, and a saturated closed-shell
+    system has exactly its nclose occupied and norbs - nclose virtual ones.
+    LMOs come atom by atom: the atom's bonds to higher atoms, then its lone
+    pairs.  Returns (iorbs, occ, vir) in the reference's arrays (ncf, nncf,
+    icocc, ncocc, cocc), pad_atoms spare atom slots after every LMO."""
+    nat = np.asarray(nat).astype(np.int32)
+    xyz = np.asarray(xyz, float).reshape(-1, 3)
+    iorbs = np.where(nat == 1, 1, 4).astype(np.int32)
+    edges = bonds(nat, xyz, scale)
+    nbr = [[] for _ in range(len(nat))]
+    for a, b in edges:
+        nbr[a].append(int(b))
+        nbr[b].append(int(a))
+    valence = {1: 1, 6: 4, 8: 2}
+    for a, z in enumerate(nat):
+        if len(nbr[a]) != valence[int(z)]:
+            raise ValueError(f"lewis_lmos: atom {a + 1} (Z = {z}) has {len(nbr[a])} bonds; "
+                             "only saturated H, C, O systems have a single-bond Lewis structure here")
+    half = np.arccos(-1.0 / 3.0) / 2.0      # half the tetrahedral angle
+    hyb = {}                                # (atom, partner or -1 - lone pair index) -> hybrid coefficients
+    for a, z in enumerate(nat):
+        if z == 1:
+            hyb[(a, nbr[a][0])] = np.array([1.0])
+            continue
+        dirs = [(xyz[b] - xyz[a]) / np.linalg.norm(xyz[b] - xyz[a]) for b in nbr[a]]
+        keys = [(a, b) for b in nbr[a]]
+        if z == 8:
+            bis = -(dirs[0] + dirs[1])
+            bis /= np.linalg.norm(bis)
+            nrm = np.cross(dirs[0], dirs[1])
+            nrm /= np.linalg.norm(nrm)
+            dirs += [np.cos(half) * bis + np.sin(half) * nrm, np.cos(half) * bis - np.sin(half) * nrm]
+            keys += [(a, -1), (a, -2)]
+        v = np.array([[0.5, *(np.sqrt(0.75) * d)] for d in dirs])   # rows: s, px, py, pz
+        w, u = np.linalg.eigh(v @ v.T)
+        if w.min() < 1.0e-3:
+            raise ValueError(f"lewis_lmos: the bonds of atom {a + 1} are coplanar")
+        h = (u @ np.diag(w ** -0.5) @ u.T) @ v                      # Loewdin: orthonormal rows
+        for key, row in zip(keys, h):
+            hyb[key] = row
+    occ, vir = [], []
+    r2 = np.sqrt(0.5)
+    for a in range(len(nat)):
+        for b in sorted(x for x in nbr[a] if x > a):
+            atoms = np.array([a, b])
+            occ.append((atoms, np.concatenate([r2 * hyb[(a, b)], r2 * hyb[(b, a)]])))
+            vir.append((atoms, np.concatenate([r2 * hyb[(a, b)], -r2 * hyb[(b, a)]])))
+        if nat[a] == 8:
+            for lp in (-1, -2):
+                occ.append((np.array([a]), hyb[(a, lp)].copy()))
+    return iorbs, _pack_lmos(iorbs, occ, pad_atoms), _pack_lmos(iorbs, vir, pad_atoms)
 
 
 def _kabsch(p: np.ndarray, q: np.ndarray):

@@ -214,6 +214,47 @@ def test_molecule_lmos_start_from_the_isolated_molecules_and_reach_the_dense_hea
     assert abs(r["escf"] - dense.escf) < 2.0e-3
 
 
+def _lmo_matrix(iorbs, lmos):
+    """The LMOs as columns of a dense norbs x nlmo coefficient matrix."""
+    ncf, nncf, icocc, ncocc, cocc = lmos
+    first = np.concatenate([[0], np.cumsum(iorbs)])
+    c = np.zeros((int(iorbs.sum()), len(ncf)))
+    for k in range(len(ncf)):
+        ic = ncocc[k]
+        for a in icocc[nncf[k]:nncf[k] + ncf[k]] - 1:
+            c[first[a]:first[a + 1], k] = cocc[ic:ic + iorbs[a]]
+            ic += iorbs[a]
+    return c
+
+
+@pytest.mark.parametrize("name", ["heptane", "water16", "propane"])
+def test_lewis_lmos_are_an_orthonormal_start_that_reaches_the_dense_heat(name):
+    """The Lewis-structure LMOs of a saturated system are orthonormal, number
+    nclose occupied and norbs - nclose virtual, and the oracle's MOZYME loop
+    from them reaches the dense SCF's heat."""
+    from mopac_gpu_b200 import mozyme
+    nat, xyz = small_systems()[name]
+    nat = np.asarray(nat)
+    xyz = np.asarray(xyz, float).reshape(-1, 3)
+    iorbs, occ, vir = mozyme.lewis_lmos(nat, xyz, pad_atoms=len(nat))
+    s = oracle_system(nat, xyz)
+    c = np.hstack([_lmo_matrix(iorbs, occ), _lmo_matrix(iorbs, vir)])
+    assert len(occ[0]) == s.nclose and c.shape == (s.norbs, s.norbs)
+    np.testing.assert_allclose(c.T @ c, np.eye(s.norbs), atol=1e-12)
+    assert set(np.unique(occ[0])) <= {1, 2} and set(np.unique(vir[0])) == {2}  # atoms per LMO
+    c1, c2 = mo.cutoffs(len(nat))
+    r = mo.iter_for_mozyme(s, occ, vir, c1, c2, scfcrt=1.0e-5, itrmax=40)
+    dense = so.iter_scf(s, scfcrt=1.0e-6)
+    assert abs(r["escf"] - dense.escf) < 1.0e-3
+
+
+def test_lewis_lmos_refuse_what_has_no_single_bond_structure():
+    from mopac_gpu_b200 import mozyme
+    nat, xyz = small_systems()["co2_1scf"]   # two C=O double bonds
+    with pytest.raises(ValueError):
+        mozyme.lewis_lmos(nat, xyz)
+
+
 @pytest.mark.gpu
 def test_gpu_molecule_lmos_are_those_of_the_oracle_orbitals():
     """On the GPU the starting LMOs come from this library's dense SCF of each
