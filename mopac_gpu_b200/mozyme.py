@@ -470,24 +470,70 @@ def bonds(nat, xyz, scale: float = 1.25) -> np.ndarray:
     return pairs[np.lexsort((pairs[:, 1], pairs[:, 0]))]
 
 
+def _perpendicular(axis: np.ndarray) -> np.ndarray:
+    """A unit vector perpendicular to the unit vector axis."""
+    t = np.eye(3)[int(np.argmin(np.abs(axis)))]
+    v = t - (t @ axis) * axis
+    return v / np.linalg.norm(v)
+
+
+def _pi_bonds(nat, nbr, valence):
+    """Multiple bonds of a neutral closed-shell H, C, O Lewis structure: each
+    atom's missing valence (valence - sigma bonds) is paired along its bonds,
+    first where an atom has a single bonded partner with missing valence,
+    then in ascending atom order.  Returns the pi bonds (a, b), a < b, a
+    double bond once and a triple bond twice."""
+    need = [valence[int(z)] - len(nbr[a]) for a, z in enumerate(nat)]
+    if min(need, default=0) < 0:
+        a = int(np.argmin(need))
+        raise ValueError(f"lewis_lmos: atom {a + 1} has more bonds than its valence")
+    pis = []
+    while any(need):
+        pick = None
+        for a in range(len(nat)):
+            if need[a] > 0:
+                cand = [b for b in nbr[a] if need[b] > 0]
+                if not cand:
+                    raise ValueError(f"lewis_lmos: atom {a + 1} has no partner for a multiple bond "
+                                     "(a radical or an ion)")
+                if len(cand) == 1:
+                    pick = (a, cand[0])
+                    break
+        if pick is None:
+            a = next(x for x in range(len(nat)) if need[x] > 0)
+            pick = (a, min(b for b in nbr[a] if need[b] > 0))
+        a, b = pick
+        need[a] -= 1
+        need[b] -= 1
+        pis.append((min(a, b), max(a, b)))
+    return sorted(pis)
+
+
 def lewis_lmos(nat, xyz, pad_atoms: int = 0, scale: float = 1.25):
-    """Starting LMOs from the Lewis structure of a saturated H, C, O system
-    (alkanes, alcohols, ethers, water; one large molecule or many), the job
-    makvec (MOZYME/makvec.F90:16-143) does, here from the bond directions
-    rather than from makvec's Fock-matrix hybrids.  Every C must have four
-    single bonds, every O two and every H one (``bonds``); anything else
-    (a double bond, a radical, an ion) raises ValueError.  A heavy atom's
-    four sp3 hybrids point along its bonds and, for O, along the two lone
-    pairs that complete its tetrahedron (on the far side of the bisector of
-    its bonds, 54.74 degrees either side of their plane), orthonormalised
-    symmetrically (Loewdin); an H's hybrid is its s orbital.  A bond A-B
-    (A < B) gives the occupied LMO (h_A + h_B)/sqrt(2) and the virtual LMO
-    (h_A - h_B)/sqrt(2) on atoms A, B; a lone pair is the occupied LMO h_A on
-    its atom alone.  All LMOs are orthonormal, and a saturated closed-shell
-    system has exactly its nclose occupied and norbs - nclose virtual ones.
-    LMOs come atom by atom: the atom's bonds to higher atoms, then its lone
-    pairs.  Returns (iorbs, occ, vir) in the reference's arrays (ncf, nncf,
-    icocc, ncocc, cocc), pad_atoms spare atom slots after every LMO."""
+    """Starting LMOs from the Lewis structure of a neutral closed-shell H, C, O
+    system (one large molecule or many), the job makvec
+    (MOZYME/makvec.F90:16-143) does, here from the bond directions rather
+    than from makvec's Fock-matrix hybrids.  Bonds come from ``bonds``;
+    missing valence (C 4, O 2, H 1) is paired into double and triple bonds
+    (``_pi_bonds``); an atom with missing valence and no partner for it (a
+    radical, an ion) raises ValueError.  Every O carries two lone pairs.
+
+    A heavy atom's sigma hybrids point along its bonds and lone pairs: sp3
+    for four of them (an O's two lone pairs complete the tetrahedron of its
+    two bonds, 54.74 degrees either side of their plane, on the far side of
+    their bisector), sp2 for three (a carbonyl O's lone pairs at 120 degrees
+    from its bond, in the plane perpendicular to the pi orbital), sp for two;
+    the remaining p orbitals carry the pi bonds, perpendicular to the sp2
+    plane or to the sp axis, the same direction on both atoms of a pi bond;
+    the atom's hybrids and p orbitals are orthonormalised symmetrically
+    (Loewdin).  An H's hybrid is its s orbital.  A bond A-B (sigma or pi,
+    A < B) gives the occupied LMO (h_A + h_B)/sqrt(2) and the virtual LMO
+    (h_A - h_B)/sqrt(2) on atoms A, B; a lone pair is the occupied LMO h_A
+    on its atom alone.  The LMOs are orthonormal, nclose occupied and
+    norbs - nclose virtual.  They come atom by atom: the atom's sigma bonds
+    to higher atoms, then its pi bonds to higher atoms, then its lone pairs.
+    Returns (iorbs, occ, vir) in the reference's arrays (ncf, nncf, icocc,
+    ncocc, cocc), pad_atoms spare atom slots after every LMO."""
     nat = np.asarray(nat).astype(np.int32)
     xyz = np.asarray(xyz, float).reshape(-1, 3)
     iorbs = np.where(nat == 1, 1, 4).astype(np.int32)
@@ -497,42 +543,110 @@ def lewis_lmos(nat, xyz, pad_atoms: int = 0, scale: float = 1.25):
         nbr[a].append(int(b))
         nbr[b].append(int(a))
     valence = {1: 1, 6: 4, 8: 2}
-    for a, z in enumerate(nat):
-        if len(nbr[a]) != valence[int(z)]:
-            raise ValueError(f"lewis_lmos: atom {a + 1} (Z = {z}) has {len(nbr[a])} bonds; "
-                             "only saturated H, C, O systems have a single-bond Lewis structure here")
-    half = np.arccos(-1.0 / 3.0) / 2.0      # half the tetrahedral angle
-    hyb = {}                                # (atom, partner or -1 - lone pair index) -> hybrid coefficients
+    pis = _pi_bonds(nat, nbr, valence)
+    if any(int(nat[a]) == 1 or int(nat[b]) == 1 for a, b in pis):
+        raise ValueError("lewis_lmos: hydrogen in a multiple bond")
+    npi = [0] * len(nat)
+    for a, b in pis:
+        npi[a] += 1
+        npi[b] += 1
+    unit = lambda v: v / np.linalg.norm(v)
+    sdir = [[unit(xyz[b] - xyz[a]) for b in nbr[a]] for a in range(len(nat))]
+    lone = [2 if z == 8 else 0 for z in nat]
+    # pi directions: from the atoms whose sigma frame fixes them, then carried
+    # to their partners; pdir[a] lists atom a's pi directions in use order
+    pdir = [None] * len(nat)
+    for a in range(len(nat)):
+        ns = len(nbr[a]) + lone[a]
+        if npi[a] == 0:
+            continue
+        if npi[a] == 1 and len(nbr[a]) >= 2:      # sp2 with two or three sigma bonds
+            d = np.array(sdir[a])
+            # the normal of the bonds' plane: the direction they span least
+            pdir[a] = [unit(np.linalg.svd(d)[2][-1])] if len(d) > 2 else [unit(np.cross(d[0], d[1]))]
+        elif npi[a] == 2 and ns == 2:               # sp: two pi orbitals around the axis
+            ax = sdir[a][0]
+            p1 = _perpendicular(ax)
+            pdir[a] = [p1, unit(np.cross(ax, p1))]
+    bond_dir = {}
+    todo = list(pis)
+    for _ in range(2 * len(pis) + 2):
+        left = []
+        for k, (a, b) in enumerate(todo):
+            src = a if pdir[a] is not None else (b if pdir[b] is not None else None)
+            if src is None:
+                left.append((a, b))
+                continue
+            used = sum(1 for key in bond_dir if src in key[:2])
+            d = pdir[src][min(used, len(pdir[src]) - 1)]
+            other = b if src == a else a
+            ax = sdir[other][nbr[other].index(src)]
+            d = unit(d - (d @ ax) * ax)
+            bond_dir[(a, b, len(bond_dir))] = d
+            if pdir[other] is None:
+                pdir[other] = [d] if npi[other] == 1 else [d, unit(np.cross(ax, d))]
+        todo = left
+        if not todo:
+            break
+    for a, b in todo:                               # neither atom fixes it: any direction off the bond
+        ax = sdir[a][nbr[a].index(b)]
+        d = _perpendicular(ax)
+        bond_dir[(a, b, len(bond_dir))] = d
+        pdir[a] = pdir[a] or [d]
+        pdir[b] = pdir[b] or [d]
+    half = np.arccos(-1.0 / 3.0) / 2.0
+    hyb = {}   # (atom, partner) for sigma, (atom, partner, 'pi', k) for pi, (atom, -1/-2) for lone pairs
+    pi_of = {}  # atom -> [(key, direction)] of its pi orbitals
+    for key, d in bond_dir.items():
+        a, b, k = key
+        pi_of.setdefault(a, []).append(((a, b, "pi", k), d))
+        pi_of.setdefault(b, []).append(((b, a, "pi", k), d))
     for a, z in enumerate(nat):
         if z == 1:
             hyb[(a, nbr[a][0])] = np.array([1.0])
             continue
-        dirs = [(xyz[b] - xyz[a]) / np.linalg.norm(xyz[b] - xyz[a]) for b in nbr[a]]
+        dirs = list(sdir[a])
         keys = [(a, b) for b in nbr[a]]
-        if z == 8:
-            bis = -(dirs[0] + dirs[1])
-            bis /= np.linalg.norm(bis)
-            nrm = np.cross(dirs[0], dirs[1])
-            nrm /= np.linalg.norm(nrm)
-            dirs += [np.cos(half) * bis + np.sin(half) * nrm, np.cos(half) * bis - np.sin(half) * nrm]
+        ns = len(dirs) + lone[a]
+        pis_a = pi_of.get(a, [])
+        if lone[a]:
+            if len(dirs) == 2:                      # sp3 O: lone pairs complete the tetrahedron
+                bis = unit(-(dirs[0] + dirs[1]))
+                nrm = unit(np.cross(dirs[0], dirs[1]))
+                dirs += [np.cos(half) * bis + np.sin(half) * nrm, np.cos(half) * bis - np.sin(half) * nrm]
+            elif len(dirs) == 1 and len(pis_a) == 1:  # sp2 O: lone pairs in the plane off the pi orbital
+                d0, pp = dirs[0], pis_a[0][1]
+                q = unit(np.cross(pp, d0))
+                c120, s120 = -0.5, np.sqrt(0.75)
+                dirs += [c120 * d0 + s120 * q, c120 * d0 - s120 * q]
+            else:
+                raise ValueError(f"lewis_lmos: oxygen {a + 1} is neither sp3 nor sp2")
             keys += [(a, -1), (a, -2)]
-        v = np.array([[0.5, *(np.sqrt(0.75) * d)] for d in dirs])   # rows: s, px, py, pz
+        if ns + len(pis_a) != 4:
+            raise ValueError(f"lewis_lmos: atom {a + 1} has {ns} sigma and {len(pis_a)} pi orbitals")
+        cs = np.sqrt(1.0 / ns)                      # s share of an sp^(ns-1) hybrid
+        rows = [[cs, *(np.sqrt(1.0 - cs * cs) * d)] for d in dirs]
+        rows += [[0.0, *d] for _, d in pis_a]
+        keys += [k for k, _ in pis_a]
+        v = np.array(rows)
         w, u = np.linalg.eigh(v @ v.T)
         if w.min() < 1.0e-3:
-            raise ValueError(f"lewis_lmos: the bonds of atom {a + 1} are coplanar")
-        h = (u @ np.diag(w ** -0.5) @ u.T) @ v                      # Loewdin: orthonormal rows
+            raise ValueError(f"lewis_lmos: the orbitals of atom {a + 1} are not independent")
+        h = (u @ np.diag(w ** -0.5) @ u.T) @ v
         for key, row in zip(keys, h):
             hyb[key] = row
     occ, vir = [], []
     r2 = np.sqrt(0.5)
     for a in range(len(nat)):
-        for b in sorted(x for x in nbr[a] if x > a):
+        pairs = [((a, b), (b, a)) for b in sorted(x for x in nbr[a] if x > a)]
+        pairs += [((a, b, "pi", k), (b, a, "pi", k)) for (a2, b, k) in bond_dir if a2 == a]
+        for ka, kb in pairs:
+            b = ka[1]
             atoms = np.array([a, b])
-            occ.append((atoms, np.concatenate([r2 * hyb[(a, b)], r2 * hyb[(b, a)]])))
-            vir.append((atoms, np.concatenate([r2 * hyb[(a, b)], -r2 * hyb[(b, a)]])))
-        if nat[a] == 8:
-            for lp in (-1, -2):
-                occ.append((np.array([a]), hyb[(a, lp)].copy()))
+            occ.append((atoms, np.concatenate([r2 * hyb[ka], r2 * hyb[kb]])))
+            vir.append((atoms, np.concatenate([r2 * hyb[ka], -r2 * hyb[kb]])))
+        for lp in range(lone[a]):
+            occ.append((np.array([a]), hyb[(a, -1 - lp)].copy()))
     return iorbs, _pack_lmos(iorbs, occ, pad_atoms), _pack_lmos(iorbs, vir, pad_atoms)
 
 

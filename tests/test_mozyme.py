@@ -227,13 +227,30 @@ def _lmo_matrix(iorbs, lmos):
     return c
 
 
-@pytest.mark.parametrize("name", ["heptane", "water16", "propane"])
+def _planar_sp2(heavy2):
+    """Ethylene (heavy2 = 6) or formaldehyde (heavy2 = 8) in the xy plane:
+    double bond along x, CH2 at 121.5 degrees."""
+    d2, ch, ang = (1.34, 1.09, np.radians(121.5)) if heavy2 == 6 else (1.21, 1.09, np.radians(121.5))
+    hx, hy = -ch * np.cos(np.pi - ang), ch * np.sin(np.pi - ang)
+    xyz = [[0, 0, 0], [d2, 0, 0], [hx, hy, 0], [hx, -hy, 0]]
+    nat = [6, heavy2, 1, 1]
+    if heavy2 == 6:
+        xyz += [[d2 - hx, hy, 0], [d2 - hx, -hy, 0]]
+        nat += [1, 1]
+    return np.array(nat, np.int32), np.array(xyz, float)
+
+
+@pytest.mark.parametrize("name", ["heptane", "water16", "propane", "co2_1scf", "ethylene", "formaldehyde"])
 def test_lewis_lmos_are_an_orthonormal_start_that_reaches_the_dense_heat(name):
-    """The Lewis-structure LMOs of a saturated system are orthonormal, number
-    nclose occupied and norbs - nclose virtual, and the oracle's MOZYME loop
-    from them reaches the dense SCF's heat."""
+    """The Lewis-structure LMOs (sigma bonds, pi bonds of double bonds, the
+    oxygen lone pairs) are orthonormal, number nclose occupied and
+    norbs - nclose virtual, and the oracle's MOZYME loop from them reaches
+    the dense SCF's heat."""
     from mopac_gpu_b200 import mozyme
-    nat, xyz = small_systems()[name]
+    if name in ("ethylene", "formaldehyde"):
+        nat, xyz = _planar_sp2(6 if name == "ethylene" else 8)
+    else:
+        nat, xyz = small_systems()[name]
     nat = np.asarray(nat)
     xyz = np.asarray(xyz, float).reshape(-1, 3)
     iorbs, occ, vir = mozyme.lewis_lmos(nat, xyz, pad_atoms=len(nat))
@@ -243,16 +260,20 @@ def test_lewis_lmos_are_an_orthonormal_start_that_reaches_the_dense_heat(name):
     np.testing.assert_allclose(c.T @ c, np.eye(s.norbs), atol=1e-12)
     assert set(np.unique(occ[0])) <= {1, 2} and set(np.unique(vir[0])) == {2}  # atoms per LMO
     c1, c2 = mo.cutoffs(len(nat))
-    r = mo.iter_for_mozyme(s, occ, vir, c1, c2, scfcrt=1.0e-5, itrmax=40)
+    r = mo.iter_for_mozyme(s, occ, vir, c1, c2, scfcrt=1.0e-5, itrmax=60)
     dense = so.iter_scf(s, scfcrt=1.0e-6)
     assert abs(r["escf"] - dense.escf) < 1.0e-3
 
 
-def test_lewis_lmos_refuse_what_has_no_single_bond_structure():
+def test_lewis_lmos_refuse_what_has_no_closed_shell_structure():
+    """A methyl radical (a carbon short of a bond with no partner for it) and
+    a hydroxyl radical have no closed-shell Lewis structure."""
     from mopac_gpu_b200 import mozyme
-    nat, xyz = small_systems()["co2_1scf"]   # two C=O double bonds
-    with pytest.raises(ValueError):
-        mozyme.lewis_lmos(nat, xyz)
+    ch3 = (np.array([6, 1, 1, 1]), np.array([[0, 0, 0], [1.08, 0, 0], [-0.54, 0.935, 0], [-0.54, -0.935, 0]]))
+    oh = (np.array([8, 1]), np.array([[0, 0, 0], [0.97, 0, 0]]))
+    for nat, xyz in (ch3, oh):
+        with pytest.raises(ValueError):
+            mozyme.lewis_lmos(nat, xyz)
 
 
 @pytest.mark.gpu
