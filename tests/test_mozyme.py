@@ -240,7 +240,8 @@ def _planar_sp2(heavy2):
     return np.array(nat, np.int32), np.array(xyz, float)
 
 
-@pytest.mark.parametrize("name", ["heptane", "water16", "propane", "co2_1scf", "ethylene", "formaldehyde"])
+@pytest.mark.parametrize("name", ["heptane", "water16", "propane", "co2_1scf", "ethylene", "formaldehyde",
+                                  "acetylene"])
 def test_lewis_lmos_are_an_orthonormal_start_that_reaches_the_dense_heat(name):
     """The Lewis-structure LMOs (sigma bonds, pi bonds of double bonds, the
     oxygen lone pairs) are orthonormal, number nclose occupied and
@@ -249,6 +250,8 @@ def test_lewis_lmos_are_an_orthonormal_start_that_reaches_the_dense_heat(name):
     from mopac_gpu_b200 import mozyme
     if name in ("ethylene", "formaldehyde"):
         nat, xyz = _planar_sp2(6 if name == "ethylene" else 8)
+    elif name == "acetylene":  # a triple bond: two pi bonds on perpendicular p orbitals
+        nat, xyz = np.array([6, 6, 1, 1]), np.array([[0, 0, 0], [1.20, 0, 0], [-1.06, 0, 0], [2.26, 0, 0]])
     else:
         nat, xyz = small_systems()[name]
     nat = np.asarray(nat)
