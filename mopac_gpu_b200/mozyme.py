@@ -664,20 +664,23 @@ def _pack_lmos(iorbs: np.ndarray, lmos: list, pad_atoms: int):
     given as (atoms, coefficients over those atoms' orbitals in that order):
     each LMO lists its atoms by falling weight (its bond's atoms first, as
     hbonds expects), followed by pad_atoms spare atom slots."""
-    ncf, nncf, icocc, ncocc, cocc = [], [], [], [], []
-    for atoms, vec in lmos:
-        offs = np.concatenate([[0], np.cumsum(iorbs[atoms])])
-        w = np.array([np.sum(vec[offs[k]:offs[k + 1]] ** 2) for k in range(len(atoms))])
-        nncf.append(len(icocc))
-        ncocc.append(len(cocc))
-        ncf.append(len(atoms))
-        for k in np.argsort(-w, kind="stable"):
-            icocc.append(int(atoms[k]) + 1)
-            cocc.extend(vec[offs[k]:offs[k + 1]].tolist())
-        icocc.extend([0] * pad_atoms)
-        cocc.extend([0.0] * (4 * pad_atoms))
-    return (np.array(ncf, np.int32), np.array(nncf, np.int32), np.array(icocc, np.int32),
-            np.array(ncocc, np.int32), np.array(cocc, np.float64))
+    nl = len(lmos)
+    ncf = np.array([len(atoms) for atoms, _ in lmos], np.int32)
+    ncoef = np.array([len(vec) for _, vec in lmos], np.int64)
+    nncf = np.concatenate([[0], np.cumsum(ncf + pad_atoms)])[:nl].astype(np.int32)
+    ncocc = np.concatenate([[0], np.cumsum(ncoef + 4 * pad_atoms)])[:nl].astype(np.int32)
+    icocc = np.zeros(int(ncf.sum()) + nl * pad_atoms, np.int32)
+    cocc = np.zeros(int(ncoef.sum()) + nl * 4 * pad_atoms, np.float64)
+    for m, (atoms, vec) in enumerate(lmos):
+        atoms = np.asarray(atoms)
+        no = iorbs[atoms]
+        offs = np.concatenate([[0], np.cumsum(no)])
+        w = np.add.reduceat(vec * vec, offs[:-1]) if len(atoms) else np.zeros(0)
+        order = np.argsort(-w, kind="stable")
+        icocc[nncf[m]:nncf[m] + len(atoms)] = atoms[order] + 1
+        sel = np.concatenate([np.arange(offs[k], offs[k + 1]) for k in order]) if len(atoms) else np.zeros(0, int)
+        cocc[ncocc[m]:ncocc[m] + len(sel)] = vec[sel]
+    return ncf, nncf, icocc, ncocc, cocc
 
 
 def molecule_lmos(nat, xyz, pad_atoms: int = 0, scfcrt: float = 1.0e-8, orbitals=None, same_tol: float = 1.0e-6):
